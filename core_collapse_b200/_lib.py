@@ -1,0 +1,128 @@
+"""ctypes binding of libcc_b200.so (the C ABI declared in include/cc_step.h and
+include/cc_ic.h).  Loading fails loudly: there is no CPU fallback."""
+from __future__ import annotations
+
+import ctypes as C
+from pathlib import Path
+
+LIB_PATH = Path(__file__).resolve().parent / "libcc_b200.so"
+
+CC_OK = 0
+CC_ERR_ARG = -1
+CC_ERR_CUDA = -2
+CC_ERR_STATE = -3
+CC_ERR_NONFINITE = -4
+CC_ERR_NOT_CONVERGED = -5
+CC_ERR_UNSUPPORTED = -6
+
+CC_FP64 = 0
+CC_FP32 = 1
+CC_POISSON_SOR = 0
+CC_POISSON_FFT = 1
+
+
+class CcMhd2dParams(C.Structure):
+    _fields_ = [
+        ("gamma", C.c_double), ("cfl", C.c_double),
+        ("x0", C.c_double), ("x1", C.c_double), ("y0", C.c_double), ("y1", C.c_double),
+        ("Nx", C.c_int32), ("Ny", C.c_int32),
+        ("t_end", C.c_double), ("dt_store", C.c_double),
+        ("floor_rho", C.c_double), ("floor_P", C.c_double),
+        ("periodic_x", C.c_int32), ("periodic_y", C.c_int32),
+        ("eta", C.c_double),
+        ("gravity_on", C.c_int32),
+        ("G", C.c_double), ("softening", C.c_double),
+        ("sor_iters", C.c_int32), ("sor_omega", C.c_double),
+        ("sor_tol", C.c_double),
+        ("poisson_kind", C.c_int32), ("precision", C.c_int32), ("reserved", C.c_int32),
+    ]
+
+
+class CcMhd3dParams(C.Structure):
+    _fields_ = [
+        ("gamma1", C.c_double), ("gamma2", C.c_double), ("K1", C.c_double), ("rho_nuc", C.c_double),
+        ("gamma_th", C.c_double), ("rho_bounce", C.c_double), ("gamma_bounce", C.c_double),
+        ("Kbounce", C.c_double), ("gamma_init", C.c_double), ("cfl", C.c_double),
+        ("x0", C.c_double), ("x1", C.c_double), ("y0", C.c_double), ("y1", C.c_double),
+        ("z0", C.c_double), ("z1", C.c_double),
+        ("Nx", C.c_int32), ("Ny", C.c_int32), ("Nz", C.c_int32), ("precision", C.c_int32),
+        ("t_end", C.c_double), ("dt_store", C.c_double),
+        ("floor_rho", C.c_double), ("floor_P", C.c_double),
+        ("periodic_x", C.c_int32), ("periodic_y", C.c_int32), ("periodic_z", C.c_int32), ("reserved", C.c_int32),
+        ("eta", C.c_double),
+    ]
+
+
+class CcEuler2dParams(C.Structure):
+    _fields_ = [
+        ("gamma", C.c_double), ("cfl", C.c_double),
+        ("x0", C.c_double), ("x1", C.c_double), ("y0", C.c_double), ("y1", C.c_double),
+        ("Nx", C.c_int32), ("Ny", C.c_int32),
+        ("t_end", C.c_double), ("dt_store", C.c_double),
+        ("floor_rho", C.c_double), ("floor_P", C.c_double),
+        ("periodic_x", C.c_int32), ("periodic_y", C.c_int32),
+        ("gravity_on", C.c_int32), ("sor_max_iter", C.c_int32),
+        ("G", C.c_double), ("softening", C.c_double),
+        ("sor_tol", C.c_double), ("sor_omega", C.c_double),
+        ("poisson_kind", C.c_int32), ("precision", C.c_int32),
+    ]
+
+
+class CcDiag(C.Structure):
+    _fields_ = [
+        ("mass", C.c_double), ("mom_x", C.c_double), ("mom_y", C.c_double), ("mom_z", C.c_double),
+        ("energy", C.c_double), ("max_divB", C.c_double), ("t", C.c_double), ("dt_last", C.c_double),
+        ("steps", C.c_int64), ("poisson_iters", C.c_int32), ("nonfinite", C.c_int32),
+        ("poisson_residual", C.c_double),
+    ]
+
+
+class CcIcKnobs(C.Structure):
+    _fields_ = [
+        ("rho_bg", C.c_double), ("rho_core", C.c_double), ("r_core", C.c_double), ("r_edge", C.c_double),
+        ("P0", C.c_double), ("vin", C.c_double), ("rot_omega", C.c_double),
+        ("B0x", C.c_double), ("Bshear", C.c_double), ("gamma_eff", C.c_double),
+    ]
+
+
+_DP = C.POINTER(C.c_double)
+_H = C.c_void_p
+
+# name -> (restype, argtypes); every symbol declared in include/*.h
+SIGNATURES = {
+    "cc_mhd2d_params_default": (None, [C.POINTER(CcMhd2dParams)]),
+    "cc_mhd2d_create": (C.c_int, [C.POINTER(CcMhd2dParams), C.POINTER(_H)]),
+    "cc_destroy": (C.c_int, [_H]),
+    "cc_last_error": (C.c_char_p, [_H]),
+    "cc_set_stream": (C.c_int, [_H, C.c_void_p]),
+    "cc_synchronize": (C.c_int, [_H]),
+    "cc_mhd2d_upload": (C.c_int, [_H] + [_DP] * 8),
+    "cc_mhd2d_download": (C.c_int, [_H] + [_DP] * 8),
+    "cc_mhd2d_compute_gravity": (C.c_int, [_H, _DP, _DP]),
+    "cc_mhd2d_compute_dt": (C.c_int, [_H, _DP]),
+    "cc_mhd2d_rk2_step": (C.c_int, [_H, _DP, _DP, C.c_double]),
+    "cc_mhd2d_advance": (C.c_int, [_H, C.c_int, _DP]),
+    "cc_mhd2d_diagnostics": (C.c_int, [_H, C.POINTER(CcDiag)]),
+    "cc_mhd2d_ic_knobs_default": (None, [C.POINTER(CcIcKnobs)]),
+    "cc_ic_mhd2d_reference": (C.c_int, [C.POINTER(CcMhd2dParams), C.POINTER(CcIcKnobs), C.POINTER(_DP)]),
+    "cc_ic_mhd2d_collapse": (C.c_int, [C.POINTER(CcMhd2dParams), C.c_double, C.c_double, C.c_double, C.c_uint32,
+                                       C.c_double, C.c_double, C.c_double, C.POINTER(_DP)]),
+    "cc_ic_mhd2d_orszag_tang": (C.c_int, [C.POINTER(CcMhd2dParams), C.c_double, C.c_double, C.POINTER(_DP)]),
+}
+
+_lib = None
+
+
+def lib() -> C.CDLL:
+    """Load libcc_b200.so (built by core_collapse_b200.build).  Raises if absent."""
+    global _lib
+    if _lib is None:
+        if not LIB_PATH.exists():
+            raise ImportError(f"{LIB_PATH} is missing: run `python -m core_collapse_b200.build` (no CPU fallback)")
+        L = C.CDLL(str(LIB_PATH))
+        for name, (res, args) in SIGNATURES.items():
+            fn = getattr(L, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = L
+    return _lib

@@ -1,0 +1,92 @@
+"""Build libcc_b200.so in-tree with nvcc for sm_100a.
+
+    python -m core_collapse_b200.build [-v]
+
+Translation units and their floating-point contract:
+  mhd2d_f64.cu, common_kernels.cu   -fmad=false: FP64 kernels round exactly like
+                                     the reference's x86-64 build (no FMA)
+  mhd2d_f32.cu                       FMA contraction on (the FP32 bulk path)
+  capi.cu, ic.cpp                    host code
+"""
+from __future__ import annotations
+
+import concurrent.futures as cf
+import os
+import shutil
+import subprocess
+import sys
+from pathlib import Path
+
+PKG = Path(__file__).resolve().parent
+CSRC = PKG / "csrc"
+INCLUDE = PKG.parent / "include"
+BUILD = PKG / "_build"
+LIB = PKG / "libcc_b200.so"
+
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-I", str(INCLUDE)]
+
+UNITS = [
+    ("mhd2d_f64.cu", ["-fmad=false"]),
+    ("common_kernels.cu", ["-fmad=false"]),
+    ("mhd2d_f32.cu", []),
+    ("capi.cu", []),
+    ("ic.cpp", []),
+]
+
+
+def nvcc() -> str:
+    for cand in (os.environ.get("NVCC"), shutil.which("nvcc"), "/usr/local/cuda/bin/nvcc"):
+        if cand and Path(cand).exists():
+            return cand
+    raise RuntimeError("nvcc not found")
+
+
+def _deps(src: Path) -> list[Path]:
+    return [src] + sorted(CSRC.glob("*.cuh")) + sorted(CSRC.glob("*.h")) + sorted(INCLUDE.glob("*.h"))
+
+
+def _stale(obj: Path, src: Path) -> bool:
+    if not obj.exists():
+        return True
+    t = obj.stat().st_mtime
+    return any(d.stat().st_mtime > t for d in _deps(src))
+
+
+def build(verbose: bool = False, force: bool = False) -> Path:
+    BUILD.mkdir(exist_ok=True)
+    nv = nvcc()
+    jobs = []
+    for name, flags in UNITS:
+        src = CSRC / name
+        obj = BUILD / (name + ".o")
+        cmd = [nv, *ARCH, *COMMON, *flags, "-c", str(src), "-o", str(obj)]
+        if name.endswith(".cpp"):
+            cmd = [nv, *COMMON, "-x", "c++", "-c", str(src), "-o", str(obj)]
+        if verbose and name.endswith(".cu"):
+            cmd.insert(1, "-Xptxas=-v")
+        jobs.append((obj, src, cmd))
+    todo = [(o, s, c) for o, s, c in jobs if force or _stale(o, s)]
+
+    def run(job):
+        obj, src, cmd = job
+        r = subprocess.run(cmd, capture_output=True, text=True)
+        if r.returncode != 0:
+            raise RuntimeError(f"nvcc failed for {src.name}:\n{r.stdout}\n{r.stderr}")
+        return src.name, r.stderr
+
+    with cf.ThreadPoolExecutor(max_workers=min(8, max(1, len(todo)))) as ex:
+        for name, err in ex.map(run, todo):
+            if verbose and err:
+                print(f"--- {name}\n{err}", file=sys.stderr)
+    objs = [str(o) for o, _, _ in jobs]
+    if todo or not LIB.exists() or any(Path(o).stat().st_mtime > LIB.stat().st_mtime for o in objs):
+        cmd = [nv, *ARCH, "-shared", "-o", str(LIB), *objs, "-lcudart_static"]
+        r = subprocess.run(cmd, capture_output=True, text=True)
+        if r.returncode != 0:
+            raise RuntimeError(f"link failed:\n{r.stdout}\n{r.stderr}")
+    return LIB
+
+
+if __name__ == "__main__":
+    print(build(verbose="-v" in sys.argv, force="-f" in sys.argv))

@@ -1,0 +1,143 @@
+// Definitions of M2Launch<T>; included once per precision TU.
+#pragma once
+#include "mhd2d_launch.h"
+
+namespace ccb {
+
+namespace {
+inline int grid_for(size_t n, int nt, int cap) {
+    size_t g = (n + nt - 1) / nt;
+    if (g < 1) g = 1;
+    if (g > (size_t)cap) g = cap;
+    return (int)g;
+}
+}  // namespace
+
+template <class T>
+cudaError_t M2Launch<T>::prepare(int nx, int ny) {
+    const int smem = (int)m2_stage_smem<T>();
+    cudaError_t e;
+#define CC_ATTR(K, BYTES)                                                                              \
+    if ((e = cudaFuncSetAttribute(K, cudaFuncAttributeMaxDynamicSharedMemorySize, (BYTES))) != cudaSuccess) \
+        return e;
+    CC_ATTR((m2_stage_kernel<T, false, GRAV_NONE>), smem)
+    CC_ATTR((m2_stage_kernel<T, false, GRAV_ARRAYS>), smem)
+    CC_ATTR((m2_stage_kernel<T, false, GRAV_PHI>), smem)
+    CC_ATTR((m2_stage_kernel<T, true, GRAV_NONE>), smem)
+    CC_ATTR((m2_stage_kernel<T, true, GRAV_ARRAYS>), smem)
+    CC_ATTR((m2_stage_kernel<T, true, GRAV_PHI>), smem)
+    constexpr int CW = (sizeof(T) == 8) ? 2 : 4;
+    const int smem_row = (int)(sizeof(Cplx<T>) * (size_t)nx);
+    const int smem_col = (int)(sizeof(Cplx<T>) * (size_t)ny * CW);
+    if (smem_row <= 227 * 1024 && smem_col <= 227 * 1024) {  // larger lines are rejected by the solver set-up
+        CC_ATTR(fft_rows_fwd_kernel<T>, smem_row)
+        CC_ATTR(fft_rows_inv_kernel<T>, smem_row)
+        CC_ATTR((fft_cols_solve_kernel<T, CW>), smem_col)
+    }
+#undef CC_ATTR
+    return cudaSuccess;
+}
+
+template <class T>
+cudaError_t M2Launch<T>::stage(const M2Const<T>& c, const Fields<T>& in, const Fields<T>& out, bool defer, int gmode,
+                               const T* ga, const T* gb, const double* dt, const int* active, cudaStream_t s) {
+    const size_t smem = m2_stage_smem<T>();
+    dim3 grid((c.nx + M2_TX - 1) / M2_TX, (c.ny + M2_TY - 1) / M2_TY);
+#define CC_STAGE_CASE(D, G)                                                                 \
+    if (defer == D && gmode == G) {                                                         \
+        m2_stage_kernel<T, D, G><<<grid, M2_NT, smem, s>>>(c, in, out, ga, gb, dt, active); \
+        return cudaGetLastError();                                                          \
+    }
+    CC_STAGE_CASE(false, GRAV_NONE)
+    CC_STAGE_CASE(false, GRAV_ARRAYS)
+    CC_STAGE_CASE(false, GRAV_PHI)
+    CC_STAGE_CASE(true, GRAV_NONE)
+    CC_STAGE_CASE(true, GRAV_ARRAYS)
+    CC_STAGE_CASE(true, GRAV_PHI)
+#undef CC_STAGE_CASE
+    return cudaErrorInvalidValue;
+}
+
+template <class T>
+cudaError_t M2Launch<T>::average(const M2Const<T>& c, const Fields<T>& un, const Fields<T>& s2, const Fields<T>& out,
+                                 const double* dt, const int* active, double* spd_part, double* rho_part,
+                                 cudaStream_t s) {
+    m2_average_kernel<T, RED_NT><<<RED_BLOCKS, RED_NT, 0, s>>>(c, un, s2, out, dt, active, spd_part, rho_part);
+    return cudaGetLastError();
+}
+
+template <class T>
+cudaError_t M2Launch<T>::speeds(const M2Const<T>& c, const Fields<T>& st, double* spd_part, double* rho_part,
+                                cudaStream_t s) {
+    m2_speed_kernel<T, RED_NT><<<RED_BLOCKS, RED_NT, 0, s>>>(c, st, spd_part, rho_part);
+    return cudaGetLastError();
+}
+
+template <class T>
+cudaError_t M2Launch<T>::rho_sum(const M2Const<T>& c, const T* rho, double* rho_part, cudaStream_t s) {
+    m2_rho_sum_kernel<T, RED_NT><<<RED_BLOCKS, RED_NT, 0, s>>>(c, rho, rho_part);
+    return cudaGetLastError();
+}
+
+template <class T>
+cudaError_t M2Launch<T>::diag(const M2Const<T>& c, const Fields<T>& st, double* part, cudaStream_t s) {
+    m2_diag_kernel<T, RED_NT><<<RED_BLOCKS, RED_NT, 0, s>>>(c, st, part);
+    return cudaGetLastError();
+}
+
+template <class T>
+cudaError_t M2Launch<T>::pack_in(const double* src, T* dst, int w, int h, int pitch, cudaStream_t s) {
+    pack_in_kernel<T><<<grid_for((size_t)w * h, 256, 4096), 256, 0, s>>>(src, dst, w, h, pitch);
+    return cudaGetLastError();
+}
+
+template <class T>
+cudaError_t M2Launch<T>::pack_out(const T* src, double* dst, int w, int h, int pitch, cudaStream_t s) {
+    pack_out_kernel<T><<<grid_for((size_t)w * h, 256, 4096), 256, 0, s>>>(src, dst, w, h, pitch);
+    return cudaGetLastError();
+}
+
+template <class T>
+cudaError_t M2Launch<T>::fft_solve(const T* rho, int pitch, const double* rho_part, int nx, int ny, int lognx,
+                                   int logny, const Cplx<T>* twx_f, const Cplx<T>* twx_i, const Cplx<T>* twy_f,
+                                   const Cplx<T>* twy_i, double Lx, double Ly, double G, Cplx<T>* A, T* phi,
+                                   const int* active, cudaStream_t s) {
+    constexpr int CW = (sizeof(T) == 8) ? 2 : 4;  // 32-byte column strips
+    const size_t smem_row = sizeof(Cplx<T>) * (size_t)nx;
+    const size_t smem_col = sizeof(Cplx<T>) * (size_t)ny * CW;
+    cudaError_t e;
+    const int nt_row = nx >= 1024 ? 512 : (nx >= 256 ? 256 : 128);
+    fft_rows_fwd_kernel<T><<<ny, nt_row, smem_row, s>>>(rho, pitch, rho_part, RED_BLOCKS, (double)nx * (double)ny, A,
+                                                         nx, lognx, twx_f, active);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    const int ncolblk = (nx + CW - 1) / CW;
+    fft_cols_solve_kernel<T, CW><<<ncolblk, 512, smem_col, s>>>(A, nx, ny, logny, twy_f, twy_i, Lx, Ly, G, active);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    fft_rows_inv_kernel<T><<<ny, nt_row, smem_row, s>>>(A, nx, lognx, twx_i, phi, pitch, active);
+    return cudaGetLastError();
+}
+
+template <class T>
+cudaError_t M2Launch<T>::sor_rhs(const T* rho, int nx, int ny, int pitch, const double* rho_part, double fourpiG,
+                                 double* rhs, const int* active, cudaStream_t s) {
+    sor_rhs_kernel<T><<<grid_for((size_t)nx * ny, 256, 2048), 256, 0, s>>>(rho, nx, ny, pitch, rho_part, RED_BLOCKS,
+                                                                          fourpiG, rhs, active);
+    return cudaGetLastError();
+}
+
+template <class T>
+cudaError_t M2Launch<T>::phi_to_field(const double* phi, int nx, int ny, T* out, int pitch, const int* active,
+                                      cudaStream_t s) {
+    phi_to_field_kernel<T><<<grid_for((size_t)nx * ny, 256, 2048), 256, 0, s>>>(phi, nx, ny, out, pitch, active);
+    return cudaGetLastError();
+}
+
+template <class T>
+cudaError_t M2Launch<T>::gravity_from_phi(const T* phi, int nx, int ny, int pitch, AxisMap ax, AxisMap ay, T two_dx,
+                                          T two_dy, T* gx, T* gy, cudaStream_t s) {
+    gravity_from_phi_kernel<T><<<grid_for((size_t)nx * ny, 256, 2048), 256, 0, s>>>(phi, nx, ny, pitch, ax, ay,
+                                                                                   two_dx, two_dy, gx, gy);
+    return cudaGetLastError();
+}
+
+}  // namespace ccb

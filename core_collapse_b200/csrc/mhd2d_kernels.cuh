@@ -1,0 +1,416 @@
+// 2D resistive-MHD step kernels (templated on T; instantiated per precision in
+// mhd2d_f64.cu / mhd2d_f32.cu).
+//
+// Device layout: every field is a pitched 2D array with the same pitch P
+// (elements, multiple of 32) and ny+1 rows:
+//   cells  c[j*P + i]          i < nx,  j < ny
+//   Bx     bx[j*P + i_face]    i_face <= nx, j < ny
+//   By     by[j_face*P + i]    i < nx, j_face <= ny
+//
+// One RK stage of the reference (advance_stage, M2:690-834) is ONE kernel here:
+// a CTA owns a TX x TY tile of cells, builds primitives on a halo-2 region in
+// shared memory, computes the x and y HLLD face fluxes it needs, the FV update,
+// the edge EMFs, the CT face update and the gravity kick, and writes the stage
+// output.  The reference's last sub-step, Joule heating + Bz diffusion + floors
+// (M2:631-686), needs post-update Bz of neighbouring cells; instead of a second
+// pass it is applied lazily by whichever kernel next reads the stage output
+// (the stage-2 prologue, and the RK-average kernel), from the stored pre-Joule
+// state.  Because that function depends only on global arrays addressed with
+// the reference's own wrap rules, the value every reader computes for a cell is
+// the reference's value, also across the periodic seam where the reference's
+// face arrays wrap modulo N+1.
+#pragma once
+#include "mhd2d_physics.cuh"
+
+namespace ccb {
+
+template <class T> struct Fields {
+    T* rho; T* mx; T* my; T* mz; T* E; T* Bz; T* bx; T* by;
+};
+
+enum GravMode { GRAV_NONE = 0, GRAV_ARRAYS = 1, GRAV_PHI = 2 };
+
+constexpr int M2_TX = 32, M2_TY = 8, M2_HALO = 2;
+constexpr int M2_RX = M2_TX + 2 * M2_HALO, M2_RY = M2_TY + 2 * M2_HALO;
+constexpr int M2_RR = M2_RX * M2_RY;
+constexpr int M2_NT = M2_TX * M2_TY;
+constexpr int M2_NFX = (M2_TX + 1) * (M2_TY + 2);   // x faces: TX+1 per row, rows -1..TY
+constexpr int M2_NGY = (M2_TX + 2) * (M2_TY + 1);   // y faces: cols -1..TX, TY+1 per col
+constexpr int M2_NE = (M2_TX + 1) * (M2_TY + 1);    // edges
+
+template <class T> constexpr size_t m2_stage_smem() {
+    return sizeof(T) * (size_t)(8 * M2_RR + 7 * M2_NFX + 7 * M2_NGY + M2_NE + 6 * M2_NT);
+}
+
+// Joule heating, explicit Bz diffusion and floors of one cell
+// (add_joule_heating_and_Bz_resistive, M2:631-686), applied to the stored
+// pre-Joule state s at cell (i,j); the cell's own values are passed in and
+// E, Bz, rho are updated.  Bx, By are the cell-centred stage-output B.
+template <class T>
+__device__ __forceinline__ void joule_cell(const M2Const<T>& c, const Fields<T>& s, int i, int j, T dt,
+                                           T& rho, T mx, T my, T mz, T& E, T& Bz, T Bx, T By) {
+    if (!c.resistive) return;
+    const int P = c.pitch;
+    const int iE = c.ax.cell(i + 1), iW = c.ax.cell(i - 1);
+    const int jN = c.ay.cell(j + 1), jS = c.ay.cell(j - 1);
+    const T bzC = Bz;
+    const T bzE = s.Bz[(size_t)j * P + iE], bzW = s.Bz[(size_t)j * P + iW];
+    const T bzN = s.Bz[(size_t)jN * P + i], bzS = s.Bz[(size_t)jS * P + i];
+    const T dBzdy = (bzN - bzS) / c.two_dy;
+    const T dBzdx = (bzE - bzW) / c.two_dx;
+    const T dBydx = (s.by[(size_t)j * P + iE] - s.by[(size_t)j * P + i]) / c.dx;
+    const T dBxdy = (s.bx[(size_t)jN * P + i] - s.bx[(size_t)j * P + i]) / c.dy;
+    const T Jx = dBzdy, Jy = -dBzdx, Jz = dBydx - dBxdy;
+    const T J2 = Jx * Jx + Jy * Jy + Jz * Jz;
+    E = E + dt * c.eta * J2;
+    const T lap = (bzE - T(2) * bzC + bzW) * c.idx2 + (bzN - T(2) * bzC + bzS) * c.idy2;
+    Bz = bzC + dt * c.eta * lap;
+    floors(c, rho, mx, my, mz, E, Bx, By, Bz);
+}
+
+// ---------------------------------------------------------------------------
+// One RK stage.  DEFER: the input is a stored pre-Joule stage output whose
+// Joule sub-step must be applied first.  GMODE selects the gravity source.
+// ---------------------------------------------------------------------------
+template <class T, bool DEFER, int GMODE>
+__global__ void __launch_bounds__(M2_NT, 2)
+m2_stage_kernel(const M2Const<T> c, const Fields<T> in, const Fields<T> out, const T* __restrict__ ga,
+                const T* __restrict__ gb, const double* __restrict__ dtp, const int* __restrict__ active) {
+    if (active && *active == 0) return;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    T* sm = reinterpret_cast<T*>(smem_raw);
+    T* s_r = sm;            T* s_u = s_r + M2_RR;   T* s_v = s_u + M2_RR;   T* s_w = s_v + M2_RR;
+    T* s_P = s_w + M2_RR;   T* s_bx = s_P + M2_RR;  T* s_by = s_bx + M2_RR; T* s_bz = s_by + M2_RR;
+    T* fx = s_bz + M2_RR;       // 7 planes of M2_NFX
+    T* gy = fx + 7 * M2_NFX;    // 7 planes of M2_NGY
+    T* ez = gy + 7 * M2_NGY;    // M2_NE
+    T* own = ez + M2_NE;        // 6 planes of M2_NT
+
+    const int tid = threadIdx.x;
+    const int i0 = blockIdx.x * M2_TX, j0 = blockIdx.y * M2_TY;
+    const int P = c.pitch;
+    const T dt = (T)(*dtp);
+
+    // ---- A: primitives on the halo-2 region (get_prim_cc, M2:278-286) ----
+    for (int k = tid; k < M2_RR; k += M2_NT) {
+        const int rx = k % M2_RX, ry = k / M2_RX;
+        const int gi = i0 - M2_HALO + rx, gj = j0 - M2_HALO + ry;
+        const int ci = c.ax.cell(gi), cj = c.ay.cell(gj);
+        const size_t q = (size_t)cj * P + ci;
+        T rho = in.rho[q], mx = in.mx[q], my = in.my[q], mz = in.mz[q], E = in.E[q], Bz = in.Bz[q];
+        const T Bx = T(0.5) * (in.bx[q] + in.bx[q + 1]);
+        const T By = T(0.5) * (in.by[q] + in.by[q + P]);
+        if (DEFER) joule_cell(c, in, ci, cj, dt, rho, mx, my, mz, E, Bz, Bx, By);
+        const Prim<T> W = to_prim(c, rho, mx, my, mz, E, Bx, By, Bz);
+        s_r[k] = W.r; s_u[k] = W.u; s_v[k] = W.v; s_w[k] = W.w;
+        s_P[k] = W.P; s_bx[k] = W.bx; s_by[k] = W.by; s_bz[k] = W.bz;
+        const int ox = rx - M2_HALO, oy = ry - M2_HALO;
+        if (ox >= 0 && ox < M2_TX && oy >= 0 && oy < M2_TY) {
+            const int o = oy * M2_TX + ox;
+            own[o] = rho; own[M2_NT + o] = mx; own[2 * M2_NT + o] = my;
+            own[3 * M2_NT + o] = mz; own[4 * M2_NT + o] = E; own[5 * M2_NT + o] = Bz;
+        }
+    }
+    __syncthreads();
+
+    auto load_prim = [&](int k) {
+        Prim<T> W;
+        W.r = s_r[k]; W.u = s_u[k]; W.v = s_v[k]; W.w = s_w[k];
+        W.P = s_P[k]; W.bx = s_bx[k]; W.by = s_by[k]; W.bz = s_bz[k];
+        return W;
+    };
+    // MUSCL-MC face state of the cell at region index k, stencil stride st
+    // (1: x, M2_RX: y); side +1 gives the state at the cell's upper face,
+    // -1 at its lower face (recon_x / recon_y, M2:290-336).
+    auto face_state = [&](int k, int st, bool ydir, T side) {
+        const Prim<T> Wc = load_prim(k);
+        Prim<T> W = Wc;
+        const T h = T(0.5) * side;
+        W.r = Wc.r + h * mc_slope(s_r[k - st], Wc.r, s_r[k + st]);
+        W.u = Wc.u + h * mc_slope(s_u[k - st], Wc.u, s_u[k + st]);
+        W.v = Wc.v + h * mc_slope(s_v[k - st], Wc.v, s_v[k + st]);
+        W.w = Wc.w + h * mc_slope(s_w[k - st], Wc.w, s_w[k + st]);
+        W.P = Wc.P + h * mc_slope(s_P[k - st], Wc.P, s_P[k + st]);
+        if (ydir) W.bx = Wc.bx + h * mc_slope(s_bx[k - st], Wc.bx, s_bx[k + st]);
+        else      W.by = Wc.by + h * mc_slope(s_by[k - st], Wc.by, s_by[k + st]);
+        W.bz = Wc.bz + h * mc_slope(s_bz[k - st], Wc.bz, s_bz[k + st]);
+        W.r = vmax(W.r, c.floor_rho);
+        W.P = vmax(W.P, c.floor_P);
+        return W;
+    };
+
+    // ---- B: x-face fluxes, faces i0..i0+TX, rows j0-1..j0+TY (M2:706-725) ----
+    for (int k = tid; k < M2_NFX; k += M2_NT) {
+        const int f = k % (M2_TX + 1), r = k / (M2_TX + 1) - 1;
+        const int gi = i0 + f;
+        if (gi > c.nx) continue;
+        const int cj = c.ay.cell(j0 + r);
+        const int kl = (r + M2_HALO) * M2_RX + (f - 1 + M2_HALO);   // left cell
+        const Prim<T> WL = face_state(kl, 1, false, T(1));
+        const Prim<T> WR = face_state(kl + 1, 1, false, T(-1));
+        const Flux<T> F = hlld_x(c, WL, WR, in.bx[(size_t)cj * P + gi]);
+        fx[k] = F.f0; fx[M2_NFX + k] = F.f1; fx[2 * M2_NFX + k] = F.f2; fx[3 * M2_NFX + k] = F.f3;
+        fx[4 * M2_NFX + k] = F.f4; fx[5 * M2_NFX + k] = F.f5; fx[6 * M2_NFX + k] = F.f6;
+    }
+    // ---- C: y-face fluxes, y faces j0..j0+TY, columns i0-1..i0+TX (M2:728-747) ----
+    for (int k = tid; k < M2_NGY; k += M2_NT) {
+        const int col = k % (M2_TX + 2) - 1, g = k / (M2_TX + 2);
+        const int gj = j0 + g;
+        if (gj > c.ny) continue;
+        const int ci = c.ax.cell(i0 + col);
+        const int kd = (g - 1 + M2_HALO) * M2_RX + (col + M2_HALO);  // lower cell
+        const Prim<T> WL = face_state(kd, M2_RX, true, T(1));
+        const Prim<T> WR = face_state(kd + M2_RX, M2_RX, true, T(-1));
+        const Flux<T> G = hlld_y(c, WL, WR, in.by[(size_t)gj * P + ci]);
+        gy[k] = G.f0; gy[M2_NGY + k] = G.f1; gy[2 * M2_NGY + k] = G.f2; gy[3 * M2_NGY + k] = G.f3;
+        gy[4 * M2_NGY + k] = G.f4; gy[5 * M2_NGY + k] = G.f5; gy[6 * M2_NGY + k] = G.f6;
+    }
+    __syncthreads();
+
+    // ---- E: edge EMFs, edges i0..i0+TX x j0..j0+TY (M2:782-804, 565-575) ----
+    for (int k = tid; k < M2_NE; k += M2_NT) {
+        const int ei = k % (M2_TX + 1), ej = k / (M2_TX + 1);
+        const int ie = i0 + ei, je = j0 + ej;
+        if (ie > c.nx || je > c.ny) continue;
+        const T exm = -fx[5 * M2_NFX + ej * (M2_TX + 1) + ei];        // x face ie, row je-1
+        const T ex0 = -fx[5 * M2_NFX + (ej + 1) * (M2_TX + 1) + ei];  // x face ie, row je
+        const T eym = gy[5 * M2_NGY + ej * (M2_TX + 2) + ei];         // y face je, col ie-1
+        const T ey0 = gy[5 * M2_NGY + ej * (M2_TX + 2) + ei + 1];     // y face je, col ie
+        const T ideal = T(0.25) * (exm + ex0 + eym + ey0);
+        T res = T(0.0);
+        if (c.resistive) {
+            const int ci = c.ax.cell(ie), cim = c.ax.cell(ie - 1);
+            const int cj = c.ay.cell(je), cjm = c.ay.cell(je - 1);
+            const T dBydx = (in.by[(size_t)je * P + ci] - in.by[(size_t)je * P + cim]) / c.dx;
+            const T dBxdy = (in.bx[(size_t)cj * P + ie] - in.bx[(size_t)cjm * P + ie]) / c.dy;
+            res = c.eta * (dBydx - dBxdy);
+        }
+        ez[k] = ideal + res;
+    }
+    __syncthreads();
+
+    // ---- D+F: FV update, floors, CT, gravity kick, store (M2:750-779, 807-832) ----
+    const int tx = tid % M2_TX, ty = tid / M2_TX;
+    const int gi = i0 + tx, gj = j0 + ty;
+    if (gi >= c.nx || gj >= c.ny) return;
+    const size_t q = (size_t)gj * P + gi;
+    const int o = ty * M2_TX + tx;
+    T rho = own[o], mx = own[M2_NT + o], my = own[2 * M2_NT + o];
+    T mz = own[3 * M2_NT + o], E = own[4 * M2_NT + o], Bz = own[5 * M2_NT + o];
+    {
+        const int kxL = (ty + 1) * (M2_TX + 1) + tx;
+        const int kgD = ty * (M2_TX + 2) + tx + 1, kgU = kgD + (M2_TX + 2);
+        T d[7];
+#pragma unroll
+        for (int m = 0; m < 7; m++)
+            d[m] = -(fx[m * M2_NFX + kxL + 1] - fx[m * M2_NFX + kxL]) * c.inv_dx -
+                   (gy[m * M2_NGY + kgU] - gy[m * M2_NGY + kgD]) * c.inv_dy;
+        rho += dt * d[0];
+        mx += dt * d[1];
+        my += dt * d[2];
+        mz += dt * d[3];
+        E += dt * d[4];
+        Bz += dt * d[6];
+        const int kc = (ty + M2_HALO) * M2_RX + tx + M2_HALO;
+        floors(c, rho, mx, my, mz, E, s_bx[kc], s_by[kc], Bz);
+    }
+    // CT (M2:807-830) for this cell's four faces
+    const T dtdy = dt / c.dy, dtdx = dt / c.dx;
+    const T e00 = ez[ty * (M2_TX + 1) + tx], e10 = ez[ty * (M2_TX + 1) + tx + 1];
+    const T e01 = ez[(ty + 1) * (M2_TX + 1) + tx], e11 = ez[(ty + 1) * (M2_TX + 1) + tx + 1];
+    const T bxL = in.bx[q] + -(dtdy) * (e01 - e00);
+    const T bxR = in.bx[q + 1] + -(dtdy) * (e11 - e10);
+    const T byD = in.by[q] + +(dtdx) * (e10 - e00);
+    const T byU = in.by[q + P] + +(dtdx) * (e11 - e01);
+    out.bx[q] = bxL;
+    if (gi == c.nx - 1) out.bx[q + 1] = bxR;
+    out.by[q] = byD;
+    if (gj == c.ny - 1) out.by[q + P] = byU;
+
+    // gravity kick + floors with the post-CT B (add_gravity_sources, M2:602-629)
+    if (GMODE != GRAV_NONE && c.gravity_on) {
+        T gxq, gyq;
+        if (GMODE == GRAV_ARRAYS) {
+            gxq = ga[q]; gyq = gb[q];
+        } else {
+            const T* phi = ga;
+            const int iE = c.ax.cell(gi + 1), iW = c.ax.cell(gi - 1);
+            const int jN = c.ay.cell(gj + 1), jS = c.ay.cell(gj - 1);
+            gxq = -(phi[(size_t)gj * P + iE] - phi[(size_t)gj * P + iW]) / c.two_dx;
+            gyq = -(phi[(size_t)jN * P + gi] - phi[(size_t)jS * P + gi]) / c.two_dy;
+        }
+        const T u = mx / vmax(rho, T(1e-300));
+        const T v = my / vmax(rho, T(1e-300));
+        mx += dt * rho * gxq;
+        my += dt * rho * gyq;
+        E += dt * rho * (u * gxq + v * gyq);
+        floors(c, rho, mx, my, mz, E, T(0.5) * (bxL + bxR), T(0.5) * (byD + byU), Bz);
+    }
+    out.rho[q] = rho; out.mx[q] = mx; out.my[q] = my; out.mz[q] = mz; out.E[q] = E; out.Bz[q] = Bz;
+}
+
+// ---------------------------------------------------------------------------
+// RK average (M2:848-868) fused with the deferred stage-2 Joule sub-step, the
+// CFL speed reduction of the next step (M2:579-598) and the density sum the
+// next Poisson solve needs.  un: U^n, s2: stage-2 output (pre-Joule), out: U^{n+1}.
+// ---------------------------------------------------------------------------
+template <class T, int NT>
+__global__ void __launch_bounds__(NT)
+m2_average_kernel(const M2Const<T> c, const Fields<T> un, const Fields<T> s2, const Fields<T> out,
+                  const double* __restrict__ dtp, const int* __restrict__ active, double* __restrict__ spd_part,
+                  double* __restrict__ rho_part) {
+    // Once t >= t_end the step kernels are no-ops; this kernel then carries
+    // U^n over unchanged so that the host's buffer rotation stays valid.
+    const bool act = (active == nullptr) || (*active != 0);
+    __shared__ double sh[NT / 32];
+    const T dt = (T)(*dtp);
+    const int P = c.pitch;
+    double smax = 0.0, rsum = 0.0;
+    const int ncell = c.nx * c.ny;
+    for (int k = blockIdx.x * NT + threadIdx.x; k < ncell; k += gridDim.x * NT) {
+        const int i = k % c.nx, j = k / c.nx;
+        const size_t q = (size_t)j * P + i;
+        if (!act) {
+            const T rho = un.rho[q], mx = un.mx[q], my = un.my[q], mz = un.mz[q], E = un.E[q], Bz = un.Bz[q];
+            const T bxl = un.bx[q], bxr = un.bx[q + 1], byd = un.by[q], byu = un.by[q + P];
+            out.rho[q] = rho; out.mx[q] = mx; out.my[q] = my; out.mz[q] = mz; out.E[q] = E; out.Bz[q] = Bz;
+            out.bx[q] = bxl;
+            if (i == c.nx - 1) out.bx[q + 1] = bxr;
+            out.by[q] = byd;
+            if (j == c.ny - 1) out.by[q + P] = byu;
+            const Prim<T> W = to_prim(c, rho, mx, my, mz, E, T(0.5) * (bxl + bxr), T(0.5) * (byd + byu), Bz);
+            const double s = (double)vmax(fabs(W.u) + fast_speed(c, W, W.bx), fabs(W.v) + fast_speed(c, W, W.by));
+            if (s > smax) smax = s;
+            rsum += (double)rho;
+            continue;
+        }
+        T rho = s2.rho[q], mx = s2.mx[q], my = s2.my[q], mz = s2.mz[q], E = s2.E[q], Bz = s2.Bz[q];
+        const T bxl2 = s2.bx[q], bxr2 = s2.bx[q + 1], byd2 = s2.by[q], byu2 = s2.by[q + P];
+        joule_cell(c, s2, i, j, dt, rho, mx, my, mz, E, Bz, T(0.5) * (bxl2 + bxr2), T(0.5) * (byd2 + byu2));
+        rho = T(0.5) * (un.rho[q] + rho);
+        mx = T(0.5) * (un.mx[q] + mx);
+        my = T(0.5) * (un.my[q] + my);
+        mz = T(0.5) * (un.mz[q] + mz);
+        E = T(0.5) * (un.E[q] + E);
+        Bz = T(0.5) * (un.Bz[q] + Bz);
+        const T bxl = T(0.5) * (un.bx[q] + bxl2), bxr = T(0.5) * (un.bx[q + 1] + bxr2);
+        const T byd = T(0.5) * (un.by[q] + byd2), byu = T(0.5) * (un.by[q + P] + byu2);
+        const T Bx = T(0.5) * (bxl + bxr), By = T(0.5) * (byd + byu);
+        floors(c, rho, mx, my, mz, E, Bx, By, Bz);
+        out.rho[q] = rho; out.mx[q] = mx; out.my[q] = my; out.mz[q] = mz; out.E[q] = E; out.Bz[q] = Bz;
+        out.bx[q] = bxl;
+        if (i == c.nx - 1) out.bx[q + 1] = bxr;
+        out.by[q] = byd;
+        if (j == c.ny - 1) out.by[q + P] = byu;
+        // CFL speeds of U^{n+1} (compute_dt's loop body, M2:585-587)
+        const Prim<T> W = to_prim(c, rho, mx, my, mz, E, Bx, By, Bz);
+        const T sx = fabs(W.u) + fast_speed(c, W, W.bx);
+        const T sy = fabs(W.v) + fast_speed(c, W, W.by);
+        const double s = (double)vmax(sx, sy);
+        if (s > smax) smax = s;   // NaN never wins, as in std::max(maxs, x)
+        rsum += (double)rho;
+    }
+    const double bm = block_max<NT>(smax, sh);
+    const double bs = block_sum<NT>(rsum, sh);
+    if (threadIdx.x == 0) { spd_part[blockIdx.x] = bm; rho_part[blockIdx.x] = bs; }
+}
+
+// CFL speed reduction and density sum of a state (compute_dt, M2:579-598).
+template <class T, int NT>
+__global__ void __launch_bounds__(NT)
+m2_speed_kernel(const M2Const<T> c, const Fields<T> s, double* __restrict__ spd_part, double* __restrict__ rho_part) {
+    __shared__ double sh[NT / 32];
+    const int P = c.pitch;
+    double smax = 0.0, rsum = 0.0;
+    const int ncell = c.nx * c.ny;
+    for (int k = blockIdx.x * NT + threadIdx.x; k < ncell; k += gridDim.x * NT) {
+        const int i = k % c.nx, j = k / c.nx;
+        const size_t q = (size_t)j * P + i;
+        const T Bx = T(0.5) * (s.bx[q] + s.bx[q + 1]), By = T(0.5) * (s.by[q] + s.by[q + P]);
+        const Prim<T> W = to_prim(c, s.rho[q], s.mx[q], s.my[q], s.mz[q], s.E[q], Bx, By, s.Bz[q]);
+        const T sx = fabs(W.u) + fast_speed(c, W, W.bx);
+        const T sy = fabs(W.v) + fast_speed(c, W, W.by);
+        const double v = (double)vmax(sx, sy);
+        if (v > smax) smax = v;
+        rsum += (double)s.rho[q];
+    }
+    const double bm = block_max<NT>(smax, sh);
+    const double bs = block_sum<NT>(rsum, sh);
+    if (threadIdx.x == 0) { spd_part[blockIdx.x] = bm; rho_part[blockIdx.x] = bs; }
+}
+
+// Sum of the density of a state (for the Poisson mean).
+template <class T, int NT>
+__global__ void __launch_bounds__(NT)
+m2_rho_sum_kernel(const M2Const<T> c, const T* __restrict__ rho, double* __restrict__ rho_part) {
+    __shared__ double sh[NT / 32];
+    double rsum = 0.0;
+    const int ncell = c.nx * c.ny;
+    for (int k = blockIdx.x * NT + threadIdx.x; k < ncell; k += gridDim.x * NT) {
+        const int i = k % c.nx, j = k / c.nx;
+        rsum += (double)rho[(size_t)j * c.pitch + i];
+    }
+    const double bs = block_sum<NT>(rsum, sh);
+    if (threadIdx.x == 0) rho_part[blockIdx.x] = bs;
+}
+
+// Host-visible diagnostics of a state: FP64 sums and max |div B| (M2:873-879).
+template <class T, int NT>
+__global__ void __launch_bounds__(NT)
+m2_diag_kernel(const M2Const<T> c, const Fields<T> s, double* __restrict__ part /* 7 * gridDim.x */) {
+    __shared__ double sh[NT / 32];
+    const int P = c.pitch;
+    double acc[6] = {0, 0, 0, 0, 0, 0};
+    double dmax = 0.0;
+    double nonfinite = 0.0;
+    const int ncell = c.nx * c.ny;
+    for (int k = blockIdx.x * NT + threadIdx.x; k < ncell; k += gridDim.x * NT) {
+        const int i = k % c.nx, j = k / c.nx;
+        const size_t q = (size_t)j * P + i;
+        const double v[6] = {(double)s.rho[q], (double)s.mx[q], (double)s.my[q], (double)s.mz[q], (double)s.E[q],
+                             (double)s.Bz[q]};
+        for (int m = 0; m < 6; m++) {
+            acc[m] += v[m];
+            if (!isfinite(v[m])) nonfinite = 1.0;
+        }
+        // divB_cc with the reference's face lookups (i+1, j+1 never wrap for a cell)
+        const double d = ((double)s.bx[q + 1] - (double)s.bx[q]) / (double)c.dx +
+                         ((double)s.by[q + P] - (double)s.by[q]) / (double)c.dy;
+        dmax = fmax(dmax, fabs(d));
+    }
+    for (int m = 0; m < 5; m++) {
+        const double b = block_sum<NT>(acc[m], sh);
+        if (threadIdx.x == 0) part[m * gridDim.x + blockIdx.x] = b;
+    }
+    const double bm = block_max<NT>(dmax, sh);
+    const double bn = block_max<NT>(nonfinite, sh);
+    if (threadIdx.x == 0) { part[5 * gridDim.x + blockIdx.x] = bm; part[6 * gridDim.x + blockIdx.x] = bn; }
+}
+
+// Combine CFL partials into dt (M2:590-597), clamp to t_end (M2:1114) and set
+// the active flag that makes the step kernels no-ops once t >= t_end.
+struct DtSpec {
+    double cfl, hmin, eta, t_end;
+    int clamp_to_end;
+};
+
+// Host <-> device layout conversion: contiguous FP64 reference layout with row
+// length w and h rows  <->  pitched T field.
+template <class T>
+__global__ void pack_in_kernel(const double* __restrict__ src, T* __restrict__ dst, int w, int h, int pitch) {
+    const size_t n = (size_t)w * h;
+    for (size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += (size_t)gridDim.x * blockDim.x) {
+        const int i = (int)(k % w), j = (int)(k / w);
+        dst[(size_t)j * pitch + i] = (T)src[k];
+    }
+}
+template <class T>
+__global__ void pack_out_kernel(const T* __restrict__ src, double* __restrict__ dst, int w, int h, int pitch) {
+    const size_t n = (size_t)w * h;
+    for (size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += (size_t)gridDim.x * blockDim.x) {
+        const int i = (int)(k % w), j = (int)(k / w);
+        dst[k] = (double)src[(size_t)j * pitch + i];
+    }
+}
+
+}  // namespace ccb

@@ -1,0 +1,48 @@
+// Host-side launchers of the 2D MHD and Poisson kernels.  Defined once per
+// precision in mhd2d_f64.cu (built with -fmad=false: the parity path) and
+// mhd2d_f32.cu (FMA contraction on: the bulk path).
+#pragma once
+#include <cuda_runtime.h>
+
+#include "mhd2d_kernels.cuh"
+#include "poisson_kernels.cuh"
+
+namespace ccb {
+
+constexpr int RED_NT = 256;      // threads of the reduction kernels
+constexpr int RED_BLOCKS = 296;  // 2 x 148 SMs; fixed so reduction order is fixed
+
+template <class T> struct M2Launch {
+    // raise the dynamic shared-memory limits of the kernels (once per device, before any launch or capture)
+    static cudaError_t prepare(int nx, int ny);
+    static cudaError_t stage(const M2Const<T>& c, const Fields<T>& in, const Fields<T>& out, bool defer, int gmode,
+                             const T* ga, const T* gb, const double* dt, const int* active, cudaStream_t s);
+    static cudaError_t average(const M2Const<T>& c, const Fields<T>& un, const Fields<T>& s2, const Fields<T>& out,
+                               const double* dt, const int* active, double* spd_part, double* rho_part,
+                               cudaStream_t s);
+    static cudaError_t speeds(const M2Const<T>& c, const Fields<T>& st, double* spd_part, double* rho_part,
+                              cudaStream_t s);
+    static cudaError_t rho_sum(const M2Const<T>& c, const T* rho, double* rho_part, cudaStream_t s);
+    static cudaError_t diag(const M2Const<T>& c, const Fields<T>& st, double* part, cudaStream_t s);
+    static cudaError_t pack_in(const double* src, T* dst, int w, int h, int pitch, cudaStream_t s);
+    static cudaError_t pack_out(const T* src, double* dst, int w, int h, int pitch, cudaStream_t s);
+    // spectral solve: rho (pitched T) -> phi (pitched T); A: nx*ny complex work
+    static cudaError_t fft_solve(const T* rho, int pitch, const double* rho_part, int nx, int ny, int lognx,
+                                 int logny, const Cplx<T>* twx_f, const Cplx<T>* twx_i, const Cplx<T>* twy_f,
+                                 const Cplx<T>* twy_i, double Lx, double Ly, double G, Cplx<T>* A, T* phi,
+                                 const int* active, cudaStream_t s);
+    static cudaError_t sor_rhs(const T* rho, int nx, int ny, int pitch, const double* rho_part, double fourpiG,
+                               double* rhs, const int* active, cudaStream_t s);
+    static cudaError_t phi_to_field(const double* phi, int nx, int ny, T* out, int pitch, const int* active,
+                                    cudaStream_t s);
+    static cudaError_t gravity_from_phi(const T* phi, int nx, int ny, int pitch, AxisMap ax, AxisMap ay, T two_dx,
+                                        T two_dy, T* gx, T* gy, cudaStream_t s);
+};
+
+cudaError_t launch_dt_finalize(const double* spd_part, DtSpec d, double* dt_out, const double* t_now, int* active,
+                               cudaStream_t s);
+cudaError_t launch_clock(double* t, const double* dt, const int* active, long long* steps, cudaStream_t s);
+// cooperative launch of the red-black SOR; nblocks must all be co-resident
+cudaError_t launch_sor(const SorArgs& a, int* nblocks_out, cudaStream_t s);
+
+}  // namespace ccb

@@ -1,0 +1,297 @@
+// Self-gravity Poisson solves (templated on T; instantiated per precision).
+//
+// Spectral periodic solve (navier_stokes_2d_hllc_poisson.cpp:285-328), three
+// passes over a complex work array A (nx*ny, row-major):
+//   1. rows:    A = FFT_x(rho - mean)                      (fft_rows_fwd)
+//   2. columns: A = IFFT_y( K(k) * FFT_y(A) ),  K = -4 pi G / |k|^2, K(0)=0
+//   3. rows:    phi = Re IFFT_x(A)
+// Every 1D transform is the reference's radix-2 decimation-in-time FFT
+// (NS:152-177): bit-reversed load, log2(n) butterfly passes with twiddles built
+// on the host by the reference's recurrence w *= wlen, inverse scaled by 1/n.
+// The reference runs the inverse as rows-then-columns; here it is
+// columns-then-rows so that the column inverse fuses with the spectral
+// multiply (rounding differs at the 1e-16 level; stated in the tests).
+//
+// Red-black SOR (the GPU ordering of M2:207-223 / EH:335-368): a persistent
+// cooperative kernel, one grid barrier per colour, deterministic FP64 mean
+// removal after each sweep, optional residual test.
+#pragma once
+#include "cc_device.cuh"
+
+namespace ccb {
+
+template <class T> struct Cplx { T re, im; };
+
+// the reference's complex product (x.re*w.re - x.im*w.im, x.re*w.im + x.im*w.re)
+template <class T> __device__ __forceinline__ Cplx<T> cmul(Cplx<T> x, Cplx<T> w) {
+    Cplx<T> r;
+    r.re = x.re * w.re - x.im * w.im;
+    r.im = x.re * w.im + x.im * w.re;
+    return r;
+}
+
+__device__ __forceinline__ int bitrev(int i, int logn) { return (int)(__brev((unsigned)i) >> (32 - logn)); }
+
+// In-place radix-2 passes over `lines` independent transforms of length n held
+// in shared memory (line l at a + l*n, already in bit-reversed order).
+// tw: twiddles of all passes, pass with half-length h at tw[h-1 .. 2h-2].
+template <class T>
+__device__ __forceinline__ void fft_passes(Cplx<T>* a, int n, int lines, const Cplx<T>* __restrict__ tw) {
+    const int nb = lines * (n >> 1);
+    for (int h = 1; h < n; h <<= 1) {
+        for (int b = threadIdx.x; b < nb; b += blockDim.x) {
+            const int l = b / (n >> 1), bb = b % (n >> 1);
+            const int jj = bb & (h - 1);
+            const int i = l * n + ((bb - jj) << 1) + jj;
+            const Cplx<T> u = a[i];
+            const Cplx<T> v = cmul(a[i + h], tw[h - 1 + jj]);
+            a[i].re = u.re + v.re; a[i].im = u.im + v.im;
+            a[i + h].re = u.re - v.re; a[i + h].im = u.im - v.im;
+        }
+        __syncthreads();
+    }
+}
+
+// pass 1: one block per row.  rho is a pitched T field; mean = sum/N.
+template <class T>
+__global__ void fft_rows_fwd_kernel(const T* __restrict__ rho, int pitch, const double* __restrict__ rho_part,
+                                    int nparts, double ncell, Cplx<T>* __restrict__ A, int nx, int logn,
+                                    const Cplx<T>* __restrict__ tw, const int* __restrict__ active) {
+    if (active && *active == 0) return;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    Cplx<T>* a = reinterpret_cast<Cplx<T>*>(smem_raw);
+    __shared__ double s_mean;
+    if (threadIdx.x == 0) {
+        double s = 0.0;
+        for (int b = 0; b < nparts; b++) s += rho_part[b];
+        s_mean = s / ncell;
+    }
+    __syncthreads();
+    const T mean = (T)s_mean;
+    const int j = blockIdx.x;
+    for (int i = threadIdx.x; i < nx; i += blockDim.x) {
+        Cplx<T> z;
+        z.re = rho[(size_t)j * pitch + i] - mean;
+        z.im = T(0);
+        a[bitrev(i, logn)] = z;
+    }
+    __syncthreads();
+    fft_passes(a, nx, 1, tw);
+    for (int i = threadIdx.x; i < nx; i += blockDim.x) A[(size_t)j * nx + i] = a[i];
+}
+
+// pass 2: CW adjacent columns per block: forward FFT along y, spectral
+// multiply, inverse FFT along y.
+template <class T, int CW>
+__global__ void fft_cols_solve_kernel(Cplx<T>* __restrict__ A, int nx, int ny, int logn,
+                                      const Cplx<T>* __restrict__ twf, const Cplx<T>* __restrict__ twi,
+                                      double Lx, double Ly, double G, const int* __restrict__ active) {
+    if (active && *active == 0) return;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    Cplx<T>* a = reinterpret_cast<Cplx<T>*>(smem_raw);   // CW lines of ny
+    const int c0 = blockIdx.x * CW;
+    for (int k = threadIdx.x; k < CW * ny; k += blockDim.x) {
+        const int cc = k % CW, j = k / CW;
+        a[cc * ny + bitrev(j, logn)] = A[(size_t)j * nx + c0 + cc];
+    }
+    __syncthreads();
+    fft_passes(a, ny, CW, twf);
+    // spectral kernel (NS:308-322), continuous |k|^2, zero mode removed
+    const double two_pi = 2.0 * M_PI;
+    for (int k = threadIdx.x; k < CW * ny; k += blockDim.x) {
+        const int cc = k % CW, j = k / CW, i = c0 + cc;
+        const int nj = (j <= ny / 2) ? j : j - ny;
+        const int ni = (i <= nx / 2) ? i : i - nx;
+        const double ky = two_pi * (double)nj / Ly;
+        const double kx = two_pi * (double)ni / Lx;
+        const double k2 = kx * kx + ky * ky;
+        Cplx<T>& z = a[cc * ny + j];
+        if (k2 == 0.0) { z.re = T(0); z.im = T(0); }
+        else {
+            const T s = (T)(-(4.0 * M_PI * G) / k2);
+            z.re = z.re * s; z.im = z.im * s;
+        }
+    }
+    __syncthreads();
+    // bit-reverse permutation of each line for the inverse DIT transform
+    for (int k = threadIdx.x; k < CW * ny; k += blockDim.x) {
+        const int cc = k / ny, j = k % ny, r = bitrev(j, logn);
+        if (j < r) { Cplx<T> t = a[cc * ny + j]; a[cc * ny + j] = a[cc * ny + r]; a[cc * ny + r] = t; }
+    }
+    __syncthreads();
+    fft_passes(a, ny, CW, twi);
+    const T n = (T)ny;
+    for (int k = threadIdx.x; k < CW * ny; k += blockDim.x) {
+        const int cc = k % CW, j = k / CW;
+        Cplx<T> z = a[cc * ny + j];
+        z.re = z.re / n; z.im = z.im / n;
+        A[(size_t)j * nx + c0 + cc] = z;
+    }
+}
+
+// pass 3: inverse FFT along x, real part -> phi (pitched).
+template <class T>
+__global__ void fft_rows_inv_kernel(const Cplx<T>* __restrict__ A, int nx, int logn, const Cplx<T>* __restrict__ tw,
+                                    T* __restrict__ phi, int pitch, const int* __restrict__ active) {
+    if (active && *active == 0) return;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    Cplx<T>* a = reinterpret_cast<Cplx<T>*>(smem_raw);
+    const int j = blockIdx.x;
+    for (int i = threadIdx.x; i < nx; i += blockDim.x) a[bitrev(i, logn)] = A[(size_t)j * nx + i];
+    __syncthreads();
+    fft_passes(a, nx, 1, tw);
+    const T n = (T)nx;
+    for (int i = threadIdx.x; i < nx; i += blockDim.x) phi[(size_t)j * pitch + i] = a[i].re / n;
+}
+
+// ---------------------------------------------------------------------------
+// Red-black SOR, FP64 throughout.
+// ---------------------------------------------------------------------------
+struct SorArgs {
+    int nx, ny;
+    AxisMap ax, ay;
+    double idx2, idy2, denom, omega, tol;
+    int max_iter;
+    const double* rhs;      // nx*ny contiguous
+    double* phi;            // nx*ny contiguous
+    double* part;           // gridDim.x partials
+    double* part2;          // gridDim.x partials (residual)
+    GridBarrier bar;
+    int* iters_out;
+    double* res_out;
+    const int* active;
+};
+
+template <int NT>
+__device__ __forceinline__ double sor_residual_block(const SorArgs& a, double* sh) {
+    double r = 0.0;
+    const int N = a.nx * a.ny;
+    for (int k = blockIdx.x * NT + threadIdx.x; k < N; k += gridDim.x * NT) {
+        const int i = k % a.nx, j = k / a.nx;
+        const double c = a.phi[k];
+        const double lap = (a.phi[(size_t)j * a.nx + a.ax.cell(i + 1)] - 2.0 * c + a.phi[(size_t)j * a.nx + a.ax.cell(i - 1)]) * a.idx2 +
+                           (a.phi[(size_t)a.ay.cell(j + 1) * a.nx + i] - 2.0 * c + a.phi[(size_t)a.ay.cell(j - 1) * a.nx + i]) * a.idy2;
+        r = fmax(r, fabs(lap - a.rhs[k]));
+    }
+    return block_max<NT>(r, sh);
+}
+
+template <int NT>
+__global__ void __launch_bounds__(NT) sor_rb_kernel(SorArgs a) {
+    if (a.active && *a.active == 0) return;
+    __shared__ double sh[NT / 32];
+    __shared__ double s_val;
+    const unsigned nb = gridDim.x;
+    const int N = a.nx * a.ny;
+    const int half = (a.nx + 1) / 2;        // cells of one colour per row (upper bound)
+    for (int k = blockIdx.x * NT + threadIdx.x; k < N; k += nb * NT) a.phi[k] = 0.0;
+    if (!grid_sync(a.bar, nb)) return;
+    int it = 0;
+    double res = 0.0;
+    for (; it < a.max_iter; ++it) {
+        for (int colour = 0; colour < 2; ++colour) {
+            const int M = half * a.ny;
+            for (int k = blockIdx.x * NT + threadIdx.x; k < M; k += nb * NT) {
+                const int j = k / half;
+                const int i = 2 * (k % half) + ((j + colour) & 1);
+                if (i >= a.nx) continue;
+                const size_t q = (size_t)j * a.nx + i;
+                const double pE = a.phi[(size_t)j * a.nx + a.ax.cell(i + 1)];
+                const double pW = a.phi[(size_t)j * a.nx + a.ax.cell(i - 1)];
+                const double pN = a.phi[(size_t)a.ay.cell(j + 1) * a.nx + i];
+                const double pS = a.phi[(size_t)a.ay.cell(j - 1) * a.nx + i];
+                const double pn = ((pE + pW) * a.idx2 + (pN + pS) * a.idy2 - a.rhs[q]) / a.denom;
+                a.phi[q] += a.omega * (pn - a.phi[q]);
+            }
+            if (!grid_sync(a.bar, nb)) return;
+        }
+        // mean removal: block partial sums, then every block adds the partials in block order
+        double s = 0.0;
+        for (int k = blockIdx.x * NT + threadIdx.x; k < N; k += nb * NT) s += a.phi[k];
+        s = block_sum<NT>(s, sh);
+        if (threadIdx.x == 0) a.part[blockIdx.x] = s;
+        if (!grid_sync(a.bar, nb)) return;
+        if (threadIdx.x == 0) {
+            double t = 0.0;
+            for (unsigned b = 0; b < nb; b++) t += a.part[b];
+            s_val = t / (double)N;
+        }
+        __syncthreads();
+        const double mean = s_val;
+        for (int k = blockIdx.x * NT + threadIdx.x; k < N; k += nb * NT) a.phi[k] -= mean;
+        if (!grid_sync(a.bar, nb)) return;
+        if (a.tol > 0.0) {
+            const double r = sor_residual_block<NT>(a, sh);
+            if (threadIdx.x == 0) a.part2[blockIdx.x] = r;
+            if (!grid_sync(a.bar, nb)) return;
+            if (threadIdx.x == 0) {
+                double m = 0.0;
+                for (unsigned b = 0; b < nb; b++) m = fmax(m, a.part2[b]);
+                s_val = m;
+            }
+            __syncthreads();
+            res = s_val;
+            // part2 is next written after three more grid barriers, so no
+            // barrier is needed here before the blocks' reads of it are done
+            if (res < a.tol) { ++it; break; }
+        }
+    }
+    if (!(a.tol > 0.0)) {
+        const double r = sor_residual_block<NT>(a, sh);
+        if (threadIdx.x == 0) a.part2[blockIdx.x] = r;
+        if (!grid_sync(a.bar, nb)) return;
+        if (threadIdx.x == 0) {
+            double m = 0.0;
+            for (unsigned b = 0; b < nb; b++) m = fmax(m, a.part2[b]);
+            res = m;
+        }
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) { *a.iters_out = it; *a.res_out = res; }
+}
+
+// rhs = 4 pi G (rho - mean) (M2:187-194), mean from the density partial sums.
+template <class T>
+__global__ void sor_rhs_kernel(const T* __restrict__ rho, int nx, int ny, int pitch, const double* __restrict__ rho_part,
+                               int nparts, double fourpiG, double* __restrict__ rhs, const int* __restrict__ active) {
+    if (active && *active == 0) return;
+    __shared__ double s_mean;
+    if (threadIdx.x == 0) {
+        double s = 0.0;
+        for (int b = 0; b < nparts; b++) s += rho_part[b];
+        s_mean = s / ((double)nx * (double)ny);
+    }
+    __syncthreads();
+    const double mean = s_mean;
+    const int N = nx * ny;
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < N; k += gridDim.x * blockDim.x) {
+        const int i = k % nx, j = k / nx;
+        rhs[k] = fourpiG * ((double)rho[(size_t)j * pitch + i] - mean);
+    }
+}
+
+// copy the contiguous FP64 phi into the pitched T field the stage kernel reads
+template <class T>
+__global__ void phi_to_field_kernel(const double* __restrict__ phi, int nx, int ny, T* __restrict__ out, int pitch,
+                                    const int* __restrict__ active) {
+    if (active && *active == 0) return;
+    const int N = nx * ny;
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < N; k += gridDim.x * blockDim.x) {
+        const int i = k % nx, j = k / nx;
+        out[(size_t)j * pitch + i] = (T)phi[k];
+    }
+}
+
+// g = -grad(phi) (M2:225-235), written pitched, for the host-facing gravity call
+template <class T>
+__global__ void gravity_from_phi_kernel(const T* __restrict__ phi, int nx, int ny, int pitch, AxisMap ax, AxisMap ay,
+                                        T two_dx, T two_dy, T* __restrict__ gx, T* __restrict__ gy) {
+    const int N = nx * ny;
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < N; k += gridDim.x * blockDim.x) {
+        const int i = k % nx, j = k / nx;
+        const size_t q = (size_t)j * pitch + i;
+        gx[q] = -(phi[(size_t)j * pitch + ax.cell(i + 1)] - phi[(size_t)j * pitch + ax.cell(i - 1)]) / two_dx;
+        gy[q] = -(phi[(size_t)ay.cell(j + 1) * pitch + i] - phi[(size_t)ay.cell(j - 1) * pitch + i]) / two_dy;
+    }
+}
+
+}  // namespace ccb

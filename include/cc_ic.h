@@ -1,0 +1,52 @@
+/*
+ * cc_ic.h -- host-side initial conditions of libcc_b200 (no GPU needed).
+ *
+ * Each function fills FP64 arrays in the reference layouts
+ *   f = {rho, mx, my, mz, E, Bz, Bx_f, By_f}
+ * (sizes Nx*Ny for the six cell fields, (Nx+1)*Ny for Bx_f, Nx*(Ny+1) for By_f)
+ * and returns 0, or -1 on a bad argument.  Cells are set through the
+ * reference's prim_to_cons + enforce_floors
+ * (mhd2d_resistive_hlld_ct_gravity.cpp:137-146, 114-124).
+ */
+#ifndef CC_IC_H
+#define CC_IC_H
+
+#include <stdint.h>
+
+#include "cc_step.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* IC knobs of the reference main() (mhd2d_resistive_hlld_ct_gravity.cpp:74-85, 1011) */
+typedef struct cc_mhd2d_ic_knobs {
+    double rho_bg, rho_core, r_core, r_edge, P0, vin, rot_omega;
+    double B0x, Bshear;
+    double gamma_eff;   /* 1.05, the pressure exponent of M2:1011 */
+} cc_mhd2d_ic_knobs;
+
+void cc_mhd2d_ic_knobs_default(cc_mhd2d_ic_knobs* k);
+
+/* The reference main()'s core-collapse IC (M2:957-1048): corner vector
+ * potential Az -> divergence-free faces, tanh core, infall + rotation. */
+int cc_ic_mhd2d_reference(const cc_mhd2d_params* p, const cc_mhd2d_ic_knobs* k, double* const* f);
+
+/* Gaussian collapse core with multiplicative noise:
+ *   rho = (1 + core_amp exp(-r^2/(2 core_width^2))) (1 + noise U(-1,1)),
+ * one std::mt19937(seed) + uniform_real_distribution<double>(-1,1) draw per
+ * cell, j outer, i inner; v = 0; P = p0 rho^p_exponent; Bx_f = Bx0, By_f = 0, Bz = 0. */
+int cc_ic_mhd2d_collapse(const cc_mhd2d_params* p, double core_amp, double core_width, double noise, uint32_t seed,
+                         double Bx0, double p0, double p_exponent, double* const* f);
+
+/* Orszag-Tang fields plus an additive Gaussian density core:
+ *   rho = 25/(36 pi) + core_amp exp(-r^2/(2 core_width^2)), P = 5/(12 pi),
+ *   v = (-sin 2 pi y, sin 2 pi x), B from Az = B0 (cos(2 pi y)/(2 pi) + cos(4 pi x)/(4 pi)),
+ *   B0 = 1/sqrt(4 pi) on corners (div B = 0 to roundoff). */
+int cc_ic_mhd2d_orszag_tang(const cc_mhd2d_params* p, double core_amp, double core_width, double* const* f);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* CC_IC_H */

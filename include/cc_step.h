@@ -1,0 +1,200 @@
+/*
+ * cc_step.h -- C ABI of the B200 finite-volume step (libcc_b200.so).
+ *
+ * The reference solvers have no FFI: each is one C++ translation unit whose
+ * main() calls a handful of static functions on std::vector<double> state.
+ * Every entry point below replaces one of those calls (cited as file:line in
+ * the reference tree) so that a host main() can swap its CPU step for this
+ * library without changing its initial conditions, time loop or output.
+ *
+ * Conventions
+ *   - Every function returns an int status: CC_OK (0) or a negative CC_ERR_*.
+ *     cc_last_error() gives a message for the last failure on a handle.
+ *   - Host arrays are caller-owned FP64 arrays in the reference layouts:
+ *       2D cells    q = j*Nx + i                       (Nx*Ny)
+ *       2D Bx faces f = j*(Nx+1) + i_face              ((Nx+1)*Ny)
+ *       2D By faces f = j_face*Nx + i                  (Nx*(Ny+1))
+ *       3D cells    q = (k*Ny + j)*Nx + i
+ *       3D faces    Bx (k*Ny+j)*(Nx+1)+i, By (k*(Ny+1)+j)*Nx+i, Bz (k*Ny+j)*Nx+i with k in [0,Nz]
+ *     Device copies are owned by the handle; the state stays resident on the
+ *     GPU between calls.  Host<->device copies happen only in upload/download
+ *     and in calls that take or return host arrays.
+ *   - A handle owns one CUDA stream and is used by one host thread at a time.
+ *   - precision: CC_FP64 runs every kernel in double precision and is the
+ *     parity path; CC_FP32 runs the flux/EMF/update bulk in single precision
+ *     with FP64 reductions (dt minimum, conserved sums, Poisson residual).
+ */
+#ifndef CC_STEP_H
+#define CC_STEP_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ---- */
+#define CC_OK                 0
+#define CC_ERR_ARG           -1   /* bad argument (null pointer, size, enum) */
+#define CC_ERR_CUDA          -2   /* a CUDA runtime call failed */
+#define CC_ERR_STATE         -3   /* call not valid in the handle's state */
+#define CC_ERR_NONFINITE     -4   /* dt not finite or <= 0 (euler2d_gravity_hllc.cpp:699-702) */
+#define CC_ERR_NOT_CONVERGED -5   /* Poisson SOR hit its iteration cap before sor_tol */
+#define CC_ERR_UNSUPPORTED   -6   /* option combination not implemented */
+
+/* ---- enums ---- */
+#define CC_FP64 0
+#define CC_FP32 1
+
+#define CC_POISSON_SOR 0   /* red-black SOR (GPU-parallel ordering of M2's SOR) */
+#define CC_POISSON_FFT 1   /* spectral periodic solve, power-of-two grids */
+
+typedef struct cc_handle cc_handle;
+
+/*
+ * 2D resistive MHD + self-gravity.  Fields mirror Params in
+ * mhd2d_resistive_hlld_ct_gravity.cpp:44-86 (IC knobs omitted: initial
+ * conditions are host-side); the last four fields are additions.
+ */
+typedef struct cc_mhd2d_params {
+    double gamma;
+    double cfl;
+    double x0, x1, y0, y1;
+    int32_t Nx, Ny;
+    double t_end;
+    double dt_store;
+    double floor_rho;
+    double floor_P;
+    int32_t periodic_x;     /* 1: periodic (imod); 0: outflow (clamp)      */
+    int32_t periodic_y;
+    double eta;             /* constant resistivity                         */
+    int32_t gravity_on;
+    double G;
+    double softening;       /* unused by the Poisson path, kept for layout  */
+    int32_t sor_iters;      /* sweep count (sor_tol <= 0) or sweep cap      */
+    double sor_omega;
+    /* additions */
+    double sor_tol;         /* > 0: stop once max|lap(phi)-rhs| < sor_tol   */
+    int32_t poisson_kind;   /* CC_POISSON_SOR or CC_POISSON_FFT             */
+    int32_t precision;      /* CC_FP64 or CC_FP32                           */
+    int32_t reserved;
+} cc_mhd2d_params;
+
+/*
+ * 3D resistive MHD with the hybrid cold+thermal EOS.  Fields mirror Params in
+ * mhd3d_resistive_hlld_ct.cpp:43-89 (IC knobs omitted).
+ */
+typedef struct cc_mhd3d_params {
+    double gamma1, gamma2, K1, rho_nuc, gamma_th;
+    double rho_bounce, gamma_bounce, Kbounce;
+    double gamma_init;
+    double cfl;
+    double x0, x1, y0, y1, z0, z1;
+    int32_t Nx, Ny, Nz;
+    int32_t precision;      /* addition: CC_FP64 or CC_FP32 */
+    double t_end;
+    double dt_store;
+    double floor_rho;
+    double floor_P;
+    int32_t periodic_x, periodic_y, periodic_z;
+    int32_t reserved;
+    double eta;
+} cc_mhd3d_params;
+
+/*
+ * 2D Euler + self-gravity with HLLC.  Fields mirror Params in
+ * euler2d_gravity_hllc.cpp:29-56; the SOR constants that the reference
+ * hard-codes inside its Poisson solve (euler2d_gravity_hllc.cpp:329-331) are
+ * fields here.
+ */
+typedef struct cc_euler2d_params {
+    double gamma;
+    double cfl;
+    double x0, x1, y0, y1;
+    int32_t Nx, Ny;
+    double t_end;
+    double dt_store;
+    double floor_rho;
+    double floor_P;
+    int32_t periodic_x, periodic_y;
+    int32_t gravity_on;
+    int32_t sor_max_iter;   /* 50000 in the reference */
+    double G;
+    double softening;
+    double sor_tol;         /* 1e-10 */
+    double sor_omega;       /* 1.7   */
+    int32_t poisson_kind;   /* addition */
+    int32_t precision;      /* addition */
+} cc_euler2d_params;
+
+/* Diagnostics gathered on the device (FP64 sums over cells). */
+typedef struct cc_diag {
+    double mass;            /* sum rho * dV        */
+    double mom_x, mom_y, mom_z;
+    double energy;          /* sum E * dV          */
+    double max_divB;        /* max |div B| over cells (M2:873-879) */
+    double t;               /* simulated time advanced by cc_*_advance */
+    double dt_last;         /* last dt used        */
+    int64_t steps;          /* steps taken by cc_*_advance */
+    int32_t poisson_iters;  /* sweeps of the last SOR solve (0 for FFT) */
+    int32_t nonfinite;      /* 1 if a non-finite conserved value was seen */
+    double poisson_residual;/* max |lap(phi)-rhs| after the last SOR solve */
+} cc_diag;
+
+/* Fill with the reference defaults (mhd2d_resistive_hlld_ct_gravity.cpp:44-86). */
+void cc_mhd2d_params_default(cc_mhd2d_params* p);
+
+/* ---- handle lifetime (all solvers) ---- */
+int cc_mhd2d_create(const cc_mhd2d_params* p, cc_handle** out);
+int cc_destroy(cc_handle* h);
+const char* cc_last_error(const cc_handle* h);
+/* Make the handle issue its work on a caller stream (cudaStream_t as void*);
+ * NULL restores the handle's own stream. */
+int cc_set_stream(cc_handle* h, void* stream);
+int cc_synchronize(cc_handle* h);
+
+/* ---- 2D MHD state transfer (reference layouts, FP64 host arrays) ---- */
+/* Ucc {rho,mx,my,mz,E,Bz} and Bfaces {Bx_f,By_f}: M2:88-95 */
+int cc_mhd2d_upload(cc_handle* h,
+                    const double* rho, const double* mx, const double* my,
+                    const double* mz, const double* E, const double* Bz,
+                    const double* Bx_f, const double* By_f);
+int cc_mhd2d_download(cc_handle* h,
+                      double* rho, double* mx, double* my,
+                      double* mz, double* E, double* Bz,
+                      double* Bx_f, double* By_f);
+
+/* ---- 2D MHD step pieces (each replaces one reference call) ---- */
+
+/* compute_poisson_gravity_periodic(p, U.rho, dx, dy) -> GravField
+ * (mhd2d_resistive_hlld_ct_gravity.cpp:178-237).  Solves on the resident rho
+ * and keeps g on the device; gx/gy (Nx*Ny each) may be NULL, otherwise g is
+ * also copied to the host.  With gravity_on == 0, g is zero. */
+int cc_mhd2d_compute_gravity(cc_handle* h, double* gx, double* gy);
+
+/* compute_dt(p, U, B, dx, dy) (mhd2d_resistive_hlld_ct_gravity.cpp:579-598).
+ * FP64 max-reduction of |u|+c_f over cells; writes dt to *dt (host). */
+int cc_mhd2d_compute_dt(cc_handle* h, double* dt);
+
+/* rk2_step(p, U, B, g, dx, dy, dt) (mhd2d_resistive_hlld_ct_gravity.cpp:838-869).
+ * gx/gy: host gravity arrays for stage 1, or NULL to use the device-resident g
+ * from the last cc_mhd2d_compute_gravity.  Stage 2 always solves Poisson on the
+ * stage-1 density on the device (M2:843). */
+int cc_mhd2d_rk2_step(cc_handle* h, const double* gx, const double* gy, double dt);
+
+/* The body of the main() time loop (mhd2d_resistive_hlld_ct_gravity.cpp:1111-1117)
+ * run nsteps times on the device: g = Poisson(rho); dt = compute_dt;
+ * dt = min(dt, t_end - t); rk2_step.  Stops early once t >= t_end.  *t is the
+ * current time on entry and the advanced time on return (may be NULL: start at
+ * the handle's clock).  dt never leaves the device. */
+int cc_mhd2d_advance(cc_handle* h, int nsteps, double* t);
+
+/* Diagnostics of the resident state. */
+int cc_mhd2d_diagnostics(cc_handle* h, cc_diag* d);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* CC_STEP_H */

@@ -1,0 +1,211 @@
+// ORACLE / TEST INFRASTRUCTURE ONLY -- never linked into core_collapse_b200.
+//
+// C ABI over the CPU restatements in this directory, for tests/ (through
+// ctypes) and for bench.py's CPU-baseline leg.  Poisson ordering per call:
+//   mode 0  lexicographic SOR, the reference's own ordering (M2:207-223, EH:335-368)
+//   mode 1  red-black SOR, the ordering the GPU kernels use
+//   mode 2  spectral FFT solve (NS:285-328)
+#include <cstring>
+#include <vector>
+
+#include "../include/cc_step.h"
+#include "mhd2d_oracle.hpp"
+#include "poisson_oracle.hpp"
+
+namespace {
+using namespace cco;
+
+M2Par m2par(const cc_mhd2d_params* c) {
+    M2Par p;
+    p.gamma = c->gamma; p.cfl = c->cfl;
+    p.x0 = c->x0; p.x1 = c->x1; p.y0 = c->y0; p.y1 = c->y1;
+    p.nx = c->Nx; p.ny = c->Ny;
+    p.floor_rho = c->floor_rho; p.floor_P = c->floor_P;
+    p.px = c->periodic_x != 0; p.py = c->periodic_y != 0;
+    p.eta = c->eta; p.gravity = c->gravity_on != 0; p.G = c->G;
+    p.sor_iters = c->sor_iters; p.sor_omega = c->sor_omega; p.sor_tol = c->sor_tol;
+    return p;
+}
+
+PoissonSpec m2spec(const cc_mhd2d_params* c) {
+    PoissonSpec s;
+    s.nx = c->Nx; s.ny = c->Ny;
+    s.px = c->periodic_x != 0; s.py = c->periodic_y != 0;
+    s.dx = (c->x1 - c->x0) / c->Nx; s.dy = (c->y1 - c->y0) / c->Ny;
+    s.G = c->G; s.omega = c->sor_omega; s.max_iter = c->sor_iters; s.tol = c->sor_tol;
+    s.floor_density = false; s.floor_rho = c->floor_rho;
+    s.Lx = c->x1 - c->x0; s.Ly = c->y1 - c->y0;
+    return s;
+}
+
+template <class T> void load(const cc_mhd2d_params* c, const double* const* f, M2State<T>& s) {
+    size_t N = (size_t)c->Nx * c->Ny, NX = (size_t)(c->Nx + 1) * c->Ny, NY = (size_t)c->Nx * (c->Ny + 1);
+    std::vector<T>* cell[6] = {&s.rho, &s.mx, &s.my, &s.mz, &s.E, &s.Bz};
+    for (int k = 0; k < 6; k++) cell[k]->assign(f[k], f[k] + N);
+    s.bxf.assign(f[6], f[6] + NX);
+    s.byf.assign(f[7], f[7] + NY);
+}
+
+template <class T> void store(const M2State<T>& s, double* const* f) {
+    const std::vector<T>* v[8] = {&s.rho, &s.mx, &s.my, &s.mz, &s.E, &s.Bz, &s.bxf, &s.byf};
+    for (int k = 0; k < 8; k++)
+        for (size_t q = 0; q < v[k]->size(); q++) f[k][q] = (double)(*v[k])[q];
+}
+
+// Gravity of a density field: phi by the chosen ordering, g by M2:225-235.
+PoissonResult gravity(const cc_mhd2d_params* c, const std::vector<double>& rho, std::vector<double>& gx,
+                      std::vector<double>& gy, int mode) {
+    PoissonSpec s = m2spec(c);
+    PoissonResult r;
+    size_t N = (size_t)c->Nx * c->Ny;
+    if (!c->gravity_on) { gx.assign(N, 0.0); gy.assign(N, 0.0); return r; }
+    std::vector<double> phi;
+    if (mode == 2) {
+        fft_periodic(s, rho, phi);
+    } else {
+        std::vector<double> rhs = poisson_rhs(s, rho);
+        r = mode == 0 ? sor_lexicographic(s, rhs, phi) : sor_red_black(s, rhs, phi);
+    }
+    gravity_from_phi(s, phi, gx, gy);
+    return r;
+}
+
+template <class T> std::vector<T> cast(const std::vector<double>& v) { return std::vector<T>(v.begin(), v.end()); }
+template <class T> std::vector<double> widen(const std::vector<T>& v) { return std::vector<double>(v.begin(), v.end()); }
+
+template <class T>
+void rk2(const cc_mhd2d_params* c, M2State<T>& s, const std::vector<double>& gx, const std::vector<double>& gy,
+         double dt, int mode) {
+    M2<T> m(m2par(c));
+    auto poisson = [&](const std::vector<T>& rho, std::vector<T>& ox, std::vector<T>& oy) {
+        std::vector<double> x, y;
+        gravity(c, widen(rho), x, y, mode);
+        ox = cast<T>(x); oy = cast<T>(y);
+    };
+    m.rk2_step(s, cast<T>(gx), cast<T>(gy), T(dt), poisson);
+}
+
+template <class T> int main_loop(const cc_mhd2d_params* c, double* const* f, int nsteps, double* t, int mode) {
+    M2State<T> s;
+    load(c, f, s);
+    M2<T> m(m2par(c));
+    double tt = t ? *t : 0.0;
+    for (int n = 0; n < nsteps && tt < c->t_end; ++n) {
+        std::vector<double> gx, gy;
+        gravity(c, widen(s.rho), gx, gy, mode);
+        double dt = m.compute_dt(s);
+        if (tt + dt > c->t_end) dt = c->t_end - tt;
+        rk2<T>(c, s, gx, gy, dt, mode);
+        tt += dt;
+    }
+    store(s, f);
+    if (t) *t = tt;
+    return 0;
+}
+}  // namespace
+
+extern "C" {
+
+int or_mhd2d_gravity(const cc_mhd2d_params* c, const double* rho, double* gx, double* gy, int mode,
+                     int* iters, double* residual) {
+    std::vector<double> r(rho, rho + (size_t)c->Nx * c->Ny), x, y;
+    PoissonResult res = gravity(c, r, x, y, mode);
+    std::memcpy(gx, x.data(), x.size() * sizeof(double));
+    std::memcpy(gy, y.data(), y.size() * sizeof(double));
+    if (iters) *iters = res.iters;
+    if (residual) *residual = res.residual;
+    return 0;
+}
+
+int or_mhd2d_phi(const cc_mhd2d_params* c, const double* rho, double* phi_out, int mode, int* iters,
+                 double* residual) {
+    PoissonSpec s = m2spec(c);
+    std::vector<double> r(rho, rho + (size_t)c->Nx * c->Ny), phi;
+    PoissonResult res;
+    if (mode == 2) fft_periodic(s, r, phi);
+    else {
+        std::vector<double> rhs = poisson_rhs(s, r);
+        res = mode == 0 ? sor_lexicographic(s, rhs, phi) : sor_red_black(s, rhs, phi);
+    }
+    std::memcpy(phi_out, phi.data(), phi.size() * sizeof(double));
+    if (iters) *iters = res.iters;
+    if (residual) *residual = res.residual;
+    return 0;
+}
+
+double or_mhd2d_compute_dt(const cc_mhd2d_params* c, const double* const* f) {
+    M2State<double> s;
+    load(c, f, s);
+    return M2<double>(m2par(c)).compute_dt(s);
+}
+
+int or_mhd2d_advance_stage(const cc_mhd2d_params* c, const double* const* fin, double* const* fout,
+                           const double* gx, const double* gy, double dt) {
+    M2State<double> s0, s1;
+    load(c, fin, s0);
+    size_t N = (size_t)c->Nx * c->Ny;
+    std::vector<double> x = gx ? std::vector<double>(gx, gx + N) : std::vector<double>(N, 0.0);
+    std::vector<double> y = gy ? std::vector<double>(gy, gy + N) : std::vector<double>(N, 0.0);
+    M2<double>(m2par(c)).advance_stage(s0, s1, x, y, dt);
+    store(s1, fout);
+    return 0;
+}
+
+int or_mhd2d_rk2_step(const cc_mhd2d_params* c, double* const* f, const double* gx, const double* gy,
+                      double dt, int mode) {
+    M2State<double> s;
+    load(c, f, s);
+    size_t N = (size_t)c->Nx * c->Ny;
+    std::vector<double> x = gx ? std::vector<double>(gx, gx + N) : std::vector<double>(N, 0.0);
+    std::vector<double> y = gy ? std::vector<double>(gy, gy + N) : std::vector<double>(N, 0.0);
+    rk2<double>(c, s, x, y, dt, mode);
+    store(s, f);
+    return 0;
+}
+
+// nsteps of the main() loop body (M2:1111-1117) in double (fp32 == 0) or float.
+int or_mhd2d_main_loop(const cc_mhd2d_params* c, double* const* f, int nsteps, double* t, int mode, int fp32) {
+    return fp32 ? main_loop<float>(c, f, nsteps, t, mode) : main_loop<double>(c, f, nsteps, t, mode);
+}
+
+double or_mhd2d_divB_max(const cc_mhd2d_params* c, const double* const* f) {
+    M2State<double> s;
+    load(c, f, s);
+    return M2<double>(m2par(c)).max_divB(s);
+}
+
+// Gravity of a density field with every Poisson knob explicit (used to pin the
+// restated SOR against both reference variants: M2's fixed sweeps and EH's
+// floored-density, residual-tolerance solve).
+int or_poisson_generic(int nx, int ny, int px, int py, double dx, double dy, double G, double omega, int max_iter,
+                       double tol, int floor_density, double floor_rho, int mode, const double* rho, double* gx,
+                       double* gy, int* iters, double* residual) {
+    PoissonSpec s;
+    s.nx = nx; s.ny = ny; s.px = px != 0; s.py = py != 0; s.dx = dx; s.dy = dy; s.G = G; s.omega = omega;
+    s.max_iter = max_iter; s.tol = tol; s.floor_density = floor_density != 0; s.floor_rho = floor_rho;
+    s.Lx = nx * dx; s.Ly = ny * dy;
+    std::vector<double> r(rho, rho + (size_t)nx * ny), phi, x, y;
+    PoissonResult res;
+    if (mode == 2) fft_periodic(s, r, phi);
+    else {
+        std::vector<double> rhs = poisson_rhs(s, r);
+        res = mode == 0 ? sor_lexicographic(s, rhs, phi) : sor_red_black(s, rhs, phi);
+    }
+    gravity_from_phi(s, phi, x, y);
+    std::memcpy(gx, x.data(), x.size() * sizeof(double));
+    std::memcpy(gy, y.data(), y.size() * sizeof(double));
+    if (iters) *iters = res.iters;
+    if (residual) *residual = res.residual;
+    return 0;
+}
+
+// Standalone FFT pieces for the tests.
+int or_fft1d(int n, double* reim, int inverse) {
+    std::vector<std::complex<double>> a(n);
+    for (int i = 0; i < n; i++) a[i] = {reim[2 * i], reim[2 * i + 1]};
+    fft_1d(a, inverse != 0);
+    for (int i = 0; i < n; i++) { reim[2 * i] = a[i].real(); reim[2 * i + 1] = a[i].imag(); }
+    return 0;
+}
+
+}  // extern "C"

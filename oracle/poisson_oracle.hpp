@@ -1,0 +1,225 @@
+// ORACLE / TEST INFRASTRUCTURE ONLY -- never linked into core_collapse_b200.
+//
+// CPU restatements of the periodic/outflow Poisson solves used for self-gravity:
+//   sor_lexicographic  M2:178-237 (fixed sweeps) and EH:288-386 (residual tolerance)
+//   sor_red_black      the GPU ordering of the same SOR update (red cells (i+j) even,
+//                      then black), mean removed after each full sweep, residual
+//                      max|lap(phi)-rhs| of the current iterate checked after it
+//   fft_periodic       NS:152-195 (radix-2 FFT, twiddles by recurrence) and NS:285-328
+//   gravity_from_phi   M2:225-235 (g = -central difference of phi)
+// All in double, whatever the caller's state type.
+#pragma once
+#include <cmath>
+#include <complex>
+#include <vector>
+
+#include "oracle_common.hpp"
+
+namespace cco {
+
+struct PoissonSpec {
+    int nx, ny;
+    bool px, py;
+    double dx, dy;
+    double G;
+    double omega;
+    int max_iter;
+    double tol;          // <= 0: run exactly max_iter sweeps
+    bool floor_density;  // EH floors rho before the solve (EH:312)
+    double floor_rho;
+    double Lx, Ly;       // box lengths for the spectral wavenumbers
+};
+
+struct PoissonResult {
+    int iters = 0;
+    double residual = 0.0;
+};
+
+inline size_t pidx(const PoissonSpec& s, int i, int j) {
+    Axis ax{s.nx, s.px}, ay{s.ny, s.py};
+    return (size_t)ay.cell(j) * s.nx + ax.cell(i);
+}
+
+// rhs = 4 pi G (rho - mean(rho)), mean by a sequential sum (M2:187-194)
+inline std::vector<double> poisson_rhs(const PoissonSpec& s, const std::vector<double>& rho_in) {
+    const size_t N = (size_t)s.nx * s.ny;
+    std::vector<double> rho(rho_in.begin(), rho_in.begin() + N);
+    if (s.floor_density)
+        for (auto& r : rho) r = vmax(r, s.floor_rho);
+    double mean = 0.0;
+    for (double r : rho) mean += r;
+    mean /= (double)N;
+    std::vector<double> rhs(N);
+    for (size_t q = 0; q < N; q++) rhs[q] = 4.0 * M_PI * s.G * (rho[q] - mean);
+    return rhs;
+}
+
+inline void remove_mean(std::vector<double>& phi) {
+    double m = 0.0;
+    for (double v : phi) m += v;
+    m /= (double)phi.size();
+    for (double& v : phi) v -= m;
+}
+
+inline double residual_max(const PoissonSpec& s, const std::vector<double>& phi, const std::vector<double>& rhs) {
+    const double idx2 = 1.0 / (s.dx * s.dx), idy2 = 1.0 / (s.dy * s.dy);
+    double r = 0.0;
+    for (int j = 0; j < s.ny; j++)
+        for (int i = 0; i < s.nx; i++) {
+            size_t k = (size_t)j * s.nx + i;
+            double c = phi[k];
+            double lap = (phi[pidx(s, i + 1, j)] - 2.0 * c + phi[pidx(s, i - 1, j)]) * idx2 +
+                         (phi[pidx(s, i, j + 1)] - 2.0 * c + phi[pidx(s, i, j - 1)]) * idy2;
+            r = vmax(r, std::abs(lap - rhs[k]));
+        }
+    return r;
+}
+
+// Lexicographic SOR.  tol <= 0: M2:207-223 (fixed sweeps).  tol > 0: EH:335-368,
+// the residual taken inside the sweep from the just-updated value.
+inline PoissonResult sor_lexicographic(const PoissonSpec& s, const std::vector<double>& rhs, std::vector<double>& phi) {
+    const double idx2 = 1.0 / (s.dx * s.dx), idy2 = 1.0 / (s.dy * s.dy);
+    const double denom = 2.0 * (idx2 + idy2);
+    phi.assign((size_t)s.nx * s.ny, 0.0);
+    PoissonResult out;
+    for (int it = 0; it < s.max_iter; ++it) {
+        double max_res = 0.0;
+        for (int j = 0; j < s.ny; j++)
+            for (int i = 0; i < s.nx; i++) {
+                size_t k = (size_t)j * s.nx + i;
+                double pE = phi[pidx(s, i + 1, j)], pW = phi[pidx(s, i - 1, j)];
+                double pN = phi[pidx(s, i, j + 1)], pS = phi[pidx(s, i, j - 1)];
+                double pn = ((pE + pW) * idx2 + (pN + pS) * idy2 - rhs[k]) / denom;
+                phi[k] += s.omega * (pn - phi[k]);
+                if (s.tol > 0.0) {
+                    double lap = (pE - 2.0 * phi[k] + pW) * idx2 + (pN - 2.0 * phi[k] + pS) * idy2;
+                    max_res = vmax(max_res, std::abs(lap - rhs[k]));
+                }
+            }
+        remove_mean(phi);
+        out.iters = it + 1;
+        out.residual = max_res;
+        if (s.tol > 0.0 && max_res < s.tol) break;
+    }
+    return out;
+}
+
+// Red-black SOR: the parallel ordering the GPU uses.  Within one colour no
+// cell reads another cell of the same colour (grids with an even periodic
+// extent, or any outflow extent), so the colour update is order-free.
+inline PoissonResult sor_red_black(const PoissonSpec& s, const std::vector<double>& rhs, std::vector<double>& phi) {
+    const double idx2 = 1.0 / (s.dx * s.dx), idy2 = 1.0 / (s.dy * s.dy);
+    const double denom = 2.0 * (idx2 + idy2);
+    phi.assign((size_t)s.nx * s.ny, 0.0);
+    PoissonResult out;
+    for (int it = 0; it < s.max_iter; ++it) {
+        for (int colour = 0; colour < 2; ++colour)
+            for (int j = 0; j < s.ny; j++)
+                for (int i = (j + colour) & 1; i < s.nx; i += 2) {
+                    size_t k = (size_t)j * s.nx + i;
+                    double pE = phi[pidx(s, i + 1, j)], pW = phi[pidx(s, i - 1, j)];
+                    double pN = phi[pidx(s, i, j + 1)], pS = phi[pidx(s, i, j - 1)];
+                    double pn = ((pE + pW) * idx2 + (pN + pS) * idy2 - rhs[k]) / denom;
+                    phi[k] += s.omega * (pn - phi[k]);
+                }
+        remove_mean(phi);
+        out.iters = it + 1;
+        if (s.tol > 0.0) {
+            out.residual = residual_max(s, phi, rhs);
+            if (out.residual < s.tol) break;
+        }
+    }
+    if (!(s.tol > 0.0)) out.residual = residual_max(s, phi, rhs);
+    return out;
+}
+
+// Twiddles of one radix-2 pass of length len, built by the reference's
+// recurrence w_{j+1} = w_j * wlen (NS:161-171).
+inline std::vector<std::complex<double>> fft_twiddles(int len, bool inverse) {
+    const double ang = 2.0 * M_PI / len * (inverse ? +1.0 : -1.0);
+    std::complex<double> wlen(std::cos(ang), std::sin(ang)), w(1.0, 0.0);
+    std::vector<std::complex<double>> t(len / 2);
+    for (int j = 0; j < len / 2; j++) { t[j] = w; w *= wlen; }
+    return t;
+}
+
+// In-place radix-2 decimation-in-time FFT (NS:152-177).
+inline void fft_1d(std::vector<std::complex<double>>& a, bool inverse) {
+    const int n = (int)a.size();
+    for (int i = 1, j = 0; i < n; i++) {
+        int bit = n >> 1;
+        for (; j & bit; bit >>= 1) j ^= bit;
+        j ^= bit;
+        if (i < j) std::swap(a[i], a[j]);
+    }
+    for (int len = 2; len <= n; len <<= 1) {
+        std::vector<std::complex<double>> tw = fft_twiddles(len, inverse);
+        for (int i = 0; i < n; i += len)
+            for (int j = 0; j < len / 2; j++) {
+                std::complex<double> u = a[i + j], v = a[i + j + len / 2] * tw[j];
+                a[i + j] = u + v;
+                a[i + j + len / 2] = u - v;
+            }
+    }
+    if (inverse)
+        for (auto& z : a) z /= (double)n;
+}
+
+// rows then columns, for both directions (NS:179-195)
+inline void fft_2d(std::vector<std::complex<double>>& A, int nx, int ny, bool inverse) {
+    std::vector<std::complex<double>> line;
+    for (int j = 0; j < ny; j++) {
+        line.assign(A.begin() + (size_t)j * nx, A.begin() + (size_t)(j + 1) * nx);
+        fft_1d(line, inverse);
+        std::copy(line.begin(), line.end(), A.begin() + (size_t)j * nx);
+    }
+    line.resize(ny);
+    for (int i = 0; i < nx; i++) {
+        for (int j = 0; j < ny; j++) line[j] = A[(size_t)j * nx + i];
+        fft_1d(line, inverse);
+        for (int j = 0; j < ny; j++) A[(size_t)j * nx + i] = line[j];
+    }
+}
+
+// Spectral periodic solve phi_k = -4 pi G rho_k / |k|^2 (NS:285-328).
+inline void fft_periodic(const PoissonSpec& s, const std::vector<double>& rho, std::vector<double>& phi) {
+    const int nx = s.nx, ny = s.ny;
+    const size_t N = (size_t)nx * ny;
+    double mean = 0.0;
+    for (size_t q = 0; q < N; q++) mean += rho[q];
+    mean /= (double)N;
+    std::vector<std::complex<double>> A(N);
+    for (size_t q = 0; q < N; q++) A[q] = std::complex<double>(rho[q] - mean, 0.0);
+    fft_2d(A, nx, ny, false);
+    const double two_pi = 2.0 * M_PI;
+    for (int j = 0; j < ny; j++) {
+        int nj = (j <= ny / 2) ? j : j - ny;
+        double ky = two_pi * (double)nj / s.Ly;
+        for (int i = 0; i < nx; i++) {
+            int ni = (i <= nx / 2) ? i : i - nx;
+            double kx = two_pi * (double)ni / s.Lx;
+            double k2 = kx * kx + ky * ky;
+            size_t q = (size_t)j * nx + i;
+            if (k2 == 0.0) A[q] = 0.0;
+            else A[q] *= (-(4.0 * M_PI * s.G) / k2);
+        }
+    }
+    fft_2d(A, nx, ny, true);
+    phi.resize(N);
+    for (size_t q = 0; q < N; q++) phi[q] = A[q].real();
+}
+
+// g = -grad(phi), central differences with the solver's wrap rule (M2:225-235)
+inline void gravity_from_phi(const PoissonSpec& s, const std::vector<double>& phi, std::vector<double>& gx,
+                             std::vector<double>& gy) {
+    gx.assign((size_t)s.nx * s.ny, 0.0);
+    gy.assign((size_t)s.nx * s.ny, 0.0);
+    for (int j = 0; j < s.ny; j++)
+        for (int i = 0; i < s.nx; i++) {
+            size_t k = (size_t)j * s.nx + i;
+            gx[k] = -(phi[pidx(s, i + 1, j)] - phi[pidx(s, i - 1, j)]) / (2.0 * s.dx);
+            gy[k] = -(phi[pidx(s, i, j + 1)] - phi[pidx(s, i, j - 1)]) / (2.0 * s.dy);
+        }
+}
+
+}  // namespace cco

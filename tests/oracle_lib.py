@@ -1,0 +1,162 @@
+"""Test-side access to the CPU checkers under oracle/ (never used by the
+product): liboracle.so (the restatement) and oracle/_ref/libref_*.so (the
+reference solvers compiled in place).  Built by `make -C oracle`."""
+from __future__ import annotations
+
+import ctypes as C
+import subprocess
+from pathlib import Path
+
+import numpy as np
+
+from core_collapse_b200 import _lib as L
+
+ROOT = Path(__file__).resolve().parents[1]
+ORACLE_DIR = ROOT / "oracle"
+REF_DIR = ORACLE_DIR / "_ref"
+REFERENCE_SRC = Path("/root/reference")
+
+_DP = C.POINTER(C.c_double)
+_PP = C.POINTER(_DP)
+
+
+def build_oracle():
+    """(Re)build liboracle.so and, where the reference tree exists, _ref/*.so."""
+    subprocess.run(["make", "-s", "-C", str(ORACLE_DIR)], check=True, capture_output=True)
+
+
+def _load(path: Path) -> C.CDLL | None:
+    return C.CDLL(str(path)) if path.exists() else None
+
+
+_oracle = None
+_refs: dict = {}
+
+
+def oracle() -> C.CDLL:
+    global _oracle
+    if _oracle is None:
+        if not (ORACLE_DIR / "liboracle.so").exists():
+            build_oracle()
+        O = C.CDLL(str(ORACLE_DIR / "liboracle.so"))
+        P2 = C.POINTER(L.CcMhd2dParams)
+        O.or_mhd2d_gravity.argtypes = [P2, _DP, _DP, _DP, C.c_int, C.POINTER(C.c_int), _DP]
+        O.or_mhd2d_phi.argtypes = [P2, _DP, _DP, C.c_int, C.POINTER(C.c_int), _DP]
+        O.or_mhd2d_compute_dt.argtypes = [P2, _PP]
+        O.or_mhd2d_compute_dt.restype = C.c_double
+        O.or_mhd2d_advance_stage.argtypes = [P2, _PP, _PP, _DP, _DP, C.c_double]
+        O.or_mhd2d_rk2_step.argtypes = [P2, _PP, _DP, _DP, C.c_double, C.c_int]
+        O.or_mhd2d_main_loop.argtypes = [P2, _PP, C.c_int, _DP, C.c_int, C.c_int]
+        O.or_mhd2d_divB_max.argtypes = [P2, _PP]
+        O.or_mhd2d_divB_max.restype = C.c_double
+        O.or_fft1d.argtypes = [C.c_int, _DP, C.c_int]
+        O.or_poisson_generic.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, C.c_double, C.c_double, C.c_double,
+                                         C.c_double, C.c_int, C.c_double, C.c_int, C.c_double, C.c_int, _DP, _DP,
+                                         _DP, C.POINTER(C.c_int), _DP]
+        _oracle = O
+    return _oracle
+
+
+def ref(name: str) -> C.CDLL | None:
+    """The reference solver library `name` in {mhd2d, mhd3d, euler2d, fft}, or None."""
+    if name not in _refs:
+        path = REF_DIR / f"libref_{name}.so"
+        if not path.exists() and REFERENCE_SRC.exists():
+            build_oracle()
+        R = _load(path)
+        if R is not None and name == "mhd2d":
+            P2 = C.POINTER(L.CcMhd2dParams)
+            R.ref_mhd2d_rk2_step.argtypes = [P2, _PP, _DP, _DP, C.c_double]
+            R.ref_mhd2d_advance_stage.argtypes = [P2, _PP, _PP, _DP, _DP, C.c_double]
+            R.ref_mhd2d_compute_dt.argtypes = [P2, _PP]
+            R.ref_mhd2d_compute_dt.restype = C.c_double
+            R.ref_mhd2d_poisson.argtypes = [P2, _DP, _DP, _DP]
+            R.ref_mhd2d_main_loop.argtypes = [P2, _PP, C.c_int, _DP]
+            R.ref_mhd2d_divB_max.argtypes = [P2, _PP]
+            R.ref_mhd2d_divB_max.restype = C.c_double
+        if R is not None and name == "euler2d":
+            P2 = C.POINTER(L.CcEuler2dParams)
+            R.ref_euler2d_rk2_step.argtypes = [P2, _PP, C.c_double]
+            R.ref_euler2d_rhs.argtypes = [P2, _PP, _PP]
+            R.ref_euler2d_compute_dt.argtypes = [P2, _PP]
+            R.ref_euler2d_compute_dt.restype = C.c_double
+            R.ref_euler2d_poisson.argtypes = [P2, _PP, _DP, _DP]
+            R.ref_euler2d_init_random_blob.argtypes = [P2, _PP]
+            R.ref_euler2d_main_loop.argtypes = [P2, _PP, C.c_int, _DP]
+        if R is not None and name == "fft":
+            R.ref_fft_poisson.argtypes = [C.c_int, C.c_int, C.c_double, C.c_double, C.c_double, C.c_double,
+                                          C.c_double, _DP, _DP]
+            R.ref_fft_gravity_accel.argtypes = [C.c_int, C.c_int, C.c_double, C.c_double, C.c_double, C.c_double,
+                                                _DP, _DP, _DP]
+            R.ref_fft1d.argtypes = [C.c_int, _DP, C.c_int]
+        _refs[name] = R
+    return _refs[name]
+
+
+def dp(a: np.ndarray):
+    assert a.dtype == np.float64 and a.flags["C_CONTIGUOUS"]
+    return a.ctypes.data_as(_DP)
+
+
+def pp(arrays) -> C.Array:
+    return (_DP * len(arrays))(*[dp(a) for a in arrays])
+
+
+# ---- state helpers: a 2D MHD state is the list [rho, mx, my, mz, E, Bz, Bx_f, By_f] ----
+
+def state_list(U, B) -> list[np.ndarray]:
+    return [a.copy() for a in U.arrays()] + [B.Bx_f.copy(), B.By_f.copy()]
+
+
+def copy_state(S):
+    return [a.copy() for a in S]
+
+
+def m2_rk2_ref(cp, S, gx, gy, dt):
+    out = copy_state(S)
+    ref("mhd2d").ref_mhd2d_rk2_step(C.byref(cp), pp(out), dp(gx), dp(gy), dt)
+    return out
+
+
+def m2_rk2_oracle(cp, S, gx, gy, dt, mode):
+    out = copy_state(S)
+    oracle().or_mhd2d_rk2_step(C.byref(cp), pp(out), dp(gx), dp(gy), dt, mode)
+    return out
+
+
+def m2_stage_ref(cp, S, gx, gy, dt):
+    out = [np.zeros_like(a) for a in S]
+    ref("mhd2d").ref_mhd2d_advance_stage(C.byref(cp), pp(S), pp(out), dp(gx), dp(gy), dt)
+    return out
+
+
+def m2_stage_oracle(cp, S, gx, gy, dt):
+    out = [np.zeros_like(a) for a in S]
+    oracle().or_mhd2d_advance_stage(C.byref(cp), pp(S), pp(out), dp(gx), dp(gy), dt)
+    return out
+
+
+def m2_gravity_oracle(cp, rho, mode):
+    n = cp.Nx * cp.Ny
+    gx, gy = np.zeros(n), np.zeros(n)
+    it = C.c_int()
+    res = C.c_double()
+    oracle().or_mhd2d_gravity(C.byref(cp), dp(np.ascontiguousarray(rho)), dp(gx), dp(gy), mode, C.byref(it),
+                              C.byref(res))
+    return gx, gy, it.value, res.value
+
+
+def m2_main_loop_oracle(cp, S, nsteps, mode, fp32=False, t0=0.0):
+    out = copy_state(S)
+    t = C.c_double(t0)
+    oracle().or_mhd2d_main_loop(C.byref(cp), pp(out), nsteps, C.byref(t), mode, 1 if fp32 else 0)
+    return out, t.value
+
+
+def rel_linf(a: np.ndarray, b: np.ndarray) -> float:
+    """max|a-b| / max|b| (0 when both are identically zero)."""
+    den = float(np.max(np.abs(b))) if b.size else 0.0
+    num = float(np.max(np.abs(a - b))) if a.size else 0.0
+    if den == 0.0:
+        return num
+    return num / den
