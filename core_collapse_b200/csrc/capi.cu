@@ -188,8 +188,9 @@ template <class T> struct Mhd2d : Mhd2dBase {
             if (p.poisson_kind == CC_POISSON_FFT) {
                 if (!p.periodic_x || !p.periodic_y)
                     return fail(h, CC_ERR_UNSUPPORTED, "FFT Poisson needs periodic_x and periodic_y");
-                if (!is_pow2(nx) || !is_pow2(ny) || nx < 2 || ny < 2)
-                    return fail(h, CC_ERR_UNSUPPORTED, "FFT Poisson needs power-of-two Nx, Ny");
+                // power of two >= 4: the column pass works on strips of 2 (FP64) or 4 (FP32) columns
+                if (!is_pow2(nx) || !is_pow2(ny) || nx < 4 || ny < 4)
+                    return fail(h, CC_ERR_UNSUPPORTED, "FFT Poisson needs power-of-two Nx, Ny >= 4");
                 if ((size_t)nx * sizeof(Cplx<T>) > 200 * 1024 || (size_t)ny * sizeof(Cplx<T>) * (sizeof(T) == 8 ? 2 : 4) > 200 * 1024)
                     return fail(h, CC_ERR_UNSUPPORTED, "FFT line does not fit in shared memory");
                 CC_CUDA(cudaMalloc(&fftA, sizeof(Cplx<T>) * (size_t)nx * ny));
