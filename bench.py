@@ -1,0 +1,380 @@
+#!/usr/bin/env python
+"""Benchmark of the 2D resistive-MHD + self-gravity step (the FFT-gravity
+precision-ladder workload: 4096^2 periodic [-1,1]^2, Orszag-Tang fields plus a
+Gaussian density core of amplitude 4 and width 0.1, gamma 5/3, G 1,
+eta 1e-3, CFL 0.4).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+One JSON line on stdout (rank 0).  `value` is FP32 zone-updates/s over all
+ranks (weak scaling: each rank advances its own instance), with the FP64 path
+timed on the same workload beside it and the FP32-vs-FP64 L1 error stated.
+A step is one pass of the reference's main-loop body: Poisson(rho), dt,
+rk2_step (two stages with a second Poisson solve between them).
+
+--impl reference times the CPU implementation of the same path (the oracle
+port of the reference step and its spectral Poisson solve, FP64, one
+independent instance per host thread) on rank 0 and prints the same line with
+"impl": "reference"."""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+sys.path.insert(0, str(ROOT / "tests"))
+
+METRIC = "zone-updates/s FP32 vs FP64 on GPU at stated L1 err; adjoint/forward time ratio"
+UNIT = "zone-updates/s"
+# algorithmic FP words per cell of one stage-kernel launch: state in (6 cell + 2
+# face), the potential, state out (6 cell + 2 face)
+STAGE_WORDS = 17
+# algorithmic FP words per zone-update of a whole RK2 step with gravity
+STEP_WORDS = 42
+
+
+def workload_params(n: int, precision: str):
+    from core_collapse_b200.mhd2d import Params
+    return Params(Nx=n, Ny=n, x0=-1.0, x1=1.0, y0=-1.0, y1=1.0, periodic_x=True, periodic_y=True, gamma=5.0 / 3.0,
+                  G=1.0, eta=1e-3, cfl=0.4, gravity_on=True, poisson="fft", precision=precision, t_end=1e30)
+
+
+def measured_peaks() -> dict:
+    f = ROOT / "MEASURED_PEAKS.json"
+    if f.exists():
+        d = json.loads(f.read_text())
+        return {"hbm_gbs": float(d["hbm_gbs"]), "source": "measured"}
+    return {"hbm_gbs": 6650.0, "source": "fallback"}
+
+
+# ---------------------------------------------------------------- CPU baseline
+
+def cpu_threads() -> int:
+    try:
+        return max(1, len(os.sched_getaffinity(0)))
+    except Exception:
+        return max(1, os.cpu_count() or 1)
+
+
+def cpu_run(sample_n: int, nthreads: int, nsteps: int) -> tuple[float, float]:
+    """Advance `nthreads` independent sample_n^2 instances by nsteps each, one
+    per thread, with the CPU port of the reference step (FP64, spectral
+    gravity).  Returns (wall seconds, zone-updates)."""
+    import ctypes as C
+
+    import oracle_lib as O
+    from core_collapse_b200.mhd2d import ic_orszag_tang
+    p = workload_params(sample_n, "fp64")
+    U, B = ic_orszag_tang(p, core_amp=4.0, core_width=0.1)
+    cp = p.to_c()
+    states = [O.state_list(U, B) for _ in range(nthreads)]
+    ptrs = [O.pp(s) for s in states]
+    orc = O.oracle()
+
+    def work(k):
+        t = C.c_double(0.0)
+        orc.or_mhd2d_main_loop(C.byref(cp), ptrs[k], nsteps, C.byref(t), 2, 0)
+
+    th = [threading.Thread(target=work, args=(k,)) for k in range(nthreads)]
+    t0 = time.perf_counter()
+    for t in th:
+        t.start()
+    for t in th:
+        t.join()
+    wall = time.perf_counter() - t0
+    return wall, float(nthreads) * sample_n * sample_n * nsteps
+
+
+def cpu_baseline(sample_n: int, nsteps: int) -> dict:
+    n = cpu_threads()
+    wall, zu = cpu_run(sample_n, n, nsteps)
+    return {"value": zu / wall, "unit": UNIT, "cores": n, "kind": "port",
+            "sample": f"{nsteps} step(s) of an independent {sample_n}^2 instance of the same workload per thread, "
+                      f"{n} threads, FP64 oracle port (bitwise-pinned to the reference step and spectral solve), "
+                      f"{wall:.1f} s wall"}
+
+
+def run_reference(args) -> None:
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    n = cpu_threads()
+    sample_n = args.cpu_sample_grid
+    for _ in range(args.warmup):
+        cpu_run(sample_n, n, 1)
+    walls = []
+    zus = 0.0
+    for _ in range(args.steps):
+        w, zu = cpu_run(sample_n, n, 1)
+        walls.append(w)
+        zus += zu
+    total = sum(walls)
+    value = zus / total
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * total / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": config_block(args),
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": n, "kind": "port",
+                         "sample": f"each step: one RK2 step of an independent {sample_n}^2 instance of the workload "
+                                   f"per thread on {n} threads (FP64 CPU port of the reference step + spectral "
+                                   f"Poisson; the reference's own M2 step has no spectral solve)"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def config_block(args) -> dict:
+    return {"workload": f"2D resistive MHD HLLD+CT + FFT self-gravity, {args.grid}^2 periodic [-1,1]^2, "
+                        f"Orszag-Tang + Gaussian core (amp 4, width 0.1), gamma 5/3, G 1, eta 1e-3, CFL 0.4",
+            "grid": [args.grid, args.grid], "cells_per_gpu": args.grid * args.grid,
+            "poisson": "fft (2 solves per step)", "precision_headline": "fp32 bulk, fp64 reductions",
+            "l2_policy": "inputs larger than L2 (state buffer >= 537 MB at 4096^2 FP32)",
+            "parallelism": f"{args.gpus} independent instance(s), one per GPU"}
+
+
+# ---------------------------------------------------------------- clocks
+
+class ClockSampler:
+    """NVML samples of the SM clock and throttle reasons during a region."""
+
+    def __init__(self, device_index: int, period_s: float = 0.02):
+        self.idx = device_index
+        self.period = period_s
+        self.samples = []
+        self.reasons = set()
+        self.max_mhz = None
+        self._stop = threading.Event()
+        self._th = None
+        self.ok = False
+
+    def __enter__(self):
+        try:
+            import pynvml as N
+            N.nvmlInit()
+            self._N = N
+            self._h = N.nvmlDeviceGetHandleByIndex(self.idx)
+            self.max_mhz = N.nvmlDeviceGetMaxClockInfo(self._h, N.NVML_CLOCK_SM)
+            self.ok = True
+        except Exception:
+            self.ok = False
+            return self
+        names = {"hw_slowdown": 0x8, "hw_thermal_slowdown": 0x40, "sw_thermal_slowdown": 0x20,
+                 "sw_power_cap": 0x4, "hw_power_brake_slowdown": 0x80}
+
+        def loop():
+            N = self._N
+            while not self._stop.is_set():
+                try:
+                    self.samples.append(N.nvmlDeviceGetClockInfo(self._h, N.NVML_CLOCK_SM))
+                    r = N.nvmlDeviceGetCurrentClocksEventReasons(self._h)
+                    for k, bit in names.items():
+                        if r & bit:
+                            self.reasons.add(k)
+                except Exception:
+                    pass
+                time.sleep(self.period)
+
+        self._th = threading.Thread(target=loop, daemon=True)
+        self._th.start()
+        return self
+
+    def __exit__(self, *exc):
+        self._stop.set()
+        if self._th:
+            self._th.join()
+
+    def summary(self) -> dict:
+        if not self.ok or not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": self.max_mhz, "reasons": sorted(self.reasons), "samples": 0}
+        return {"sm_mhz": statistics.median(self.samples), "sm_max_mhz": self.max_mhz,
+                "reasons": sorted(self.reasons), "samples": len(self.samples)}
+
+
+# ---------------------------------------------------------------- GPU arm
+
+def traffic_per_launch(grid: int):
+    """DRAM bytes per stage-kernel launch from the committed ncu capture,
+    scaled to the benchmark grid by cell count (traffic grows with cells)."""
+    f = ROOT / "profiles" / "stage_kernel_traffic.json"
+    if not f.exists():
+        return None
+    d = json.loads(f.read_text())
+    try:
+        return float(d["dram_bytes_per_launch"]) * (grid * grid) / float(d["cells"])
+    except Exception:
+        return None
+
+
+def run_ours(args) -> None:
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+    from datetime import timedelta
+
+    from core_collapse_b200.mhd2d import Mhd2dSolver, ic_orszag_tang
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=torch.device("cuda", local))
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def max_over_ranks(x: float) -> float:
+        if world == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    n = args.grid
+    cells = n * n
+    # a non-default stream shared by the library and the timing events (the
+    # legacy null stream has handle 0, which the C ABI reads as "own stream")
+    stream = torch.cuda.Stream()
+    p32 = workload_params(n, "fp32")
+    U0, B0 = ic_orszag_tang(p32, core_amp=4.0, core_width=0.1)
+
+    def timed_run(precision: str, profile: bool, clocks: bool):
+        p = workload_params(n, precision)
+        s = Mhd2dSolver(p)
+        s.set_stream(stream.cuda_stream)
+        s.upload(U0, B0)
+        s.advance(args.warmup, 0.0)
+        s.set_profiling(profile)
+        s.reset_perf()
+        barrier()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        sampler = ClockSampler(local) if clocks else None
+        if sampler:
+            sampler.__enter__()
+        e0.record(stream)
+        s.advance(args.steps)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        if sampler:
+            sampler.__exit__()
+        barrier()
+        ms = e0.elapsed_time(e1)
+        perf = s.perf()
+        return s, ms, perf, (sampler.summary() if sampler else None)
+
+    # FP32 headline
+    s32, ms32, perf32, clk = timed_run("fp32", profile=True, clocks=True)
+    ms32_max = max_over_ranks(ms32)
+    value32 = world * cells * args.steps / (ms32_max / 1000.0)
+    stage_avg_ms = perf32["stage_ms"] / max(1, perf32["stage_launches"])
+    stage_bytes = STAGE_WORDS * 4 * cells
+
+    # FP64 on the same workload and step count
+    s64, ms64, perf64, _ = timed_run("fp64", profile=True, clocks=False)
+    ms64_max = max_over_ranks(ms64)
+    value64 = world * cells * args.steps / (ms64_max / 1000.0)
+    stage64_avg_ms = perf64["stage_ms"] / max(1, perf64["stage_launches"])
+
+    # FP32-vs-FP64 L1 error after the same number of steps from the same IC
+    Ua, Ba = s32.download()
+    Ub, Bb = s64.download()
+    names = ["rho", "mx", "my", "mz", "E", "Bz", "Bx_f", "By_f"]
+    l1 = {}
+    for k, (a, b) in enumerate(zip(Ua.arrays() + [Ba.Bx_f, Ba.By_f], Ub.arrays() + [Bb.Bx_f, Bb.By_f])):
+        den = float(np.sum(np.abs(b)))
+        l1[names[k]] = float(np.sum(np.abs(a - b)) / den) if den > 0 else float(np.max(np.abs(a)))
+    d32, d64 = s32.diagnostics(), s64.diagnostics()
+    s64.close()
+
+    # end to end through the C ABI with pinned host buffers, copies timed every step
+    pin = lambda m: torch.empty(m, dtype=torch.float64, pin_memory=True).numpy()
+    from core_collapse_b200.mhd2d import Bfaces, Ucc
+    Uh = Ucc(*[pin(cells) for _ in range(6)])
+    Bh = Bfaces(pin((n + 1) * n), pin(n * (n + 1)))
+    for a, b in zip(Uh.arrays() + [Bh.Bx_f, Bh.By_f], U0.arrays() + [B0.Bx_f, B0.By_f]):
+        a[:] = b
+    h2d = sum(a.nbytes for a in Uh.arrays()) + Bh.Bx_f.nbytes + Bh.By_f.nbytes
+    s32.set_profiling(False)
+    s32.reset_perf()
+    e2e_steps = max(1, min(args.steps, args.e2e_steps))
+    barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(e2e_steps):
+        s32.upload(Uh, Bh)
+        s32.advance(1)
+        s32.download(Uh, Bh)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    barrier()
+    e2e_ms = max_over_ranks(e0.elapsed_time(e1))
+    e2e_value = world * cells * e2e_steps / (e2e_ms / 1000.0)
+    s32.close()
+
+    peaks = measured_peaks()
+    achieved = stage_bytes / (stage_avg_ms / 1000.0) / 1e9
+    line = {
+        "metric": METRIC, "value": value32, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms32_max / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic", "config": config_block(args),
+        "fp64": {"value": value64, "ms_per_step": ms64_max / args.steps, "dtype": "f64",
+                 "stage_kernel_ms": stage64_avg_ms,
+                 "stage_kernel_gbs": STAGE_WORDS * 8 * cells / (stage64_avg_ms / 1000.0) / 1e9},
+        "fp32_over_fp64": value32 / value64,
+        "l1_err_fp32_vs_fp64": {"max": max(l1.values()), "per_field": l1,
+                                "after_steps": args.warmup + args.steps,
+                                "t_fp32": d32["t"], "t_fp64": d64["t"]},
+        "roofline": {"bound": "hbm", "kernel": "m2_stage_kernel<float> (one RK2 stage)",
+                     "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                     "frac": achieved / peaks["hbm_gbs"], "peak_source": peaks["source"],
+                     "traffic": traffic_per_launch(n), "algorithmic_bytes_per_launch": stage_bytes,
+                     "launch_ms": stage_avg_ms,
+                     "step_roofline_frac": STEP_WORDS * 4 * value32 / world / 1e9 / peaks["hbm_gbs"]},
+        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": h2d,
+                "steps": e2e_steps, "api": "cc_mhd2d_upload + cc_mhd2d_advance(1) + cc_mhd2d_download, pinned FP64 host"},
+        "gpu_launches": perf32["kernel_launches"],
+        "clocks": clk,
+        "max_divB_fp32": d32["max_divB"],
+    }
+    if world == 1 and rank == 0 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline(args.cpu_sample_grid, args.cpu_steps)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def main():
+    ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=60)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--grid", type=int, default=4096)
+    ap.add_argument("--e2e-steps", type=int, default=10)
+    ap.add_argument("--cpu-sample-grid", type=int, default=512)
+    ap.add_argument("--cpu-steps", type=int, default=3)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        ap.error("--warmup must be >= 3")
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

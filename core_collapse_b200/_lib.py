@@ -77,6 +77,13 @@ class CcDiag(C.Structure):
     ]
 
 
+class CcPerf(C.Structure):
+    _fields_ = [
+        ("kernel_launches", C.c_int64), ("stage_launches", C.c_int64), ("stage_ms", C.c_double),
+        ("poisson_solves", C.c_int64), ("steps", C.c_int64),
+    ]
+
+
 class CcIcKnobs(C.Structure):
     _fields_ = [
         ("rho_bg", C.c_double), ("rho_core", C.c_double), ("r_core", C.c_double), ("r_edge", C.c_double),
@@ -96,6 +103,9 @@ SIGNATURES = {
     "cc_last_error": (C.c_char_p, [_H]),
     "cc_set_stream": (C.c_int, [_H, C.c_void_p]),
     "cc_synchronize": (C.c_int, [_H]),
+    "cc_set_profiling": (C.c_int, [_H, C.c_int]),
+    "cc_get_perf": (C.c_int, [_H, C.POINTER(CcPerf)]),
+    "cc_reset_perf": (C.c_int, [_H]),
     "cc_mhd2d_upload": (C.c_int, [_H] + [_DP] * 8),
     "cc_mhd2d_download": (C.c_int, [_H] + [_DP] * 8),
     "cc_mhd2d_compute_gravity": (C.c_int, [_H, _DP, _DP]),

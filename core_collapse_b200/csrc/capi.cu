@@ -32,8 +32,26 @@ struct cc_handle {
     std::string err;
     cudaStream_t own = nullptr;
     cudaStream_t stream = nullptr;
+    cc_perf perf{};
+    bool profiling = false;
+    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> timed;  // event pairs around stage launches
     virtual ~cc_handle() {
+        for (auto& e : timed) { cudaEventDestroy(e.first); cudaEventDestroy(e.second); }
         if (own) cudaStreamDestroy(own);
+    }
+    // fold the recorded event pairs into perf.stage_ms (stream must be idle)
+    cudaError_t collect() {
+        for (auto& e : timed) {
+            float ms = 0.f;
+            cudaError_t r = cudaEventElapsedTime(&ms, e.first, e.second);
+            if (r != cudaSuccess) return r;
+            perf.stage_ms += ms;
+            perf.stage_launches += 1;
+            cudaEventDestroy(e.first);
+            cudaEventDestroy(e.second);
+        }
+        timed.clear();
+        return cudaSuccess;
     }
 };
 
@@ -264,6 +282,7 @@ template <class T> struct Mhd2d : Mhd2dBase {
     int ensure_partials() {
         if (rho_part_valid) return CC_OK;
         CC_CUDA(M2Launch<T>::speeds(c, buf[cur], spd_part, rho_part, st()));
+        count(1);
         rho_part_valid = true;
         return CC_OK;
     }
@@ -271,10 +290,12 @@ template <class T> struct Mhd2d : Mhd2dBase {
     // Poisson on a density field; rho_part must hold its sum.  Writes phi.
     int solve(const T* rho) {
         if (!p.gravity_on) return CC_OK;
+        h->perf.poisson_solves += 1;
         const int nx = p.Nx, ny = p.Ny;
         if (p.poisson_kind == CC_POISSON_FFT) {
             CC_CUDA(M2Launch<T>::fft_solve(rho, P, rho_part, nx, ny, ilog2(nx), ilog2(ny), tw[0], tw[1], tw[2], tw[3],
                                            p.x1 - p.x0, p.y1 - p.y0, p.G, fftA, phi, active(), st()));
+            count(3);
         } else {
             CC_CUDA(M2Launch<T>::sor_rhs(rho, nx, ny, P, rho_part, 4.0 * M_PI * p.G, rhs, active(), st()));
             const double dx = (p.x1 - p.x0) / nx, dy = (p.y1 - p.y0) / ny;
@@ -289,6 +310,7 @@ template <class T> struct Mhd2d : Mhd2dBase {
             int nb = 0;
             CC_CUDA(launch_sor(a, &nb, st()));
             CC_CUDA(M2Launch<T>::phi_to_field(sphi, nx, ny, phi, P, active(), st()));
+            count(3);
         }
         return CC_OK;
     }
@@ -346,19 +368,43 @@ template <class T> struct Mhd2d : Mhd2dBase {
         return CC_OK;
     }
 
+    void count(int n) { h->perf.kernel_launches += n; }
+
+    // one stage-kernel launch, bracketed by CUDA events when profiling
+    int stage(const Fields<T>& in, const Fields<T>& out, bool defer, int gmode, const T* ga, const T* gb) {
+        cudaEvent_t e0 = nullptr, e1 = nullptr;
+        if (h->profiling) {
+            CC_CUDA(cudaEventCreate(&e0));
+            CC_CUDA(cudaEventCreate(&e1));
+            CC_CUDA(cudaEventRecord(e0, st()));
+        }
+        CC_CUDA(M2Launch<T>::stage(c, in, out, defer, gmode, ga, gb, dt_dev, active(), st()));
+        count(1);
+        if (h->profiling) {
+            CC_CUDA(cudaEventRecord(e1, st()));
+            h->timed.emplace_back(e0, e1);
+        }
+        return CC_OK;
+    }
+
     // stage 1 (gravity per gmode1), Poisson on S1, stage 2, average; dt in dt_dev
     int step_body(int gmode1) {
         const int a = cur, b = (cur + 1) % 3, d = (cur + 2) % 3;
         const int g2 = p.gravity_on ? GRAV_PHI : GRAV_NONE;
-        CC_CUDA(M2Launch<T>::stage(c, buf[a], buf[b], false, gmode1, gmode1 == GRAV_ARRAYS ? gxa : phi,
-                                   gmode1 == GRAV_ARRAYS ? gya : nullptr, dt_dev, active(), st()));
+        int r = stage(buf[a], buf[b], false, gmode1, gmode1 == GRAV_ARRAYS ? gxa : phi,
+                      gmode1 == GRAV_ARRAYS ? gya : nullptr);
+        if (r) return r;
         if (p.gravity_on) {
             CC_CUDA(M2Launch<T>::rho_sum(c, buf[b].rho, rho_part, st()));
-            int r = solve(buf[b].rho);
+            count(1);
+            r = solve(buf[b].rho);
             if (r) return r;
         }
-        CC_CUDA(M2Launch<T>::stage(c, buf[b], buf[d], true, g2, phi, nullptr, dt_dev, active(), st()));
+        r = stage(buf[b], buf[d], true, g2, phi, nullptr);
+        if (r) return r;
         CC_CUDA(M2Launch<T>::average(c, buf[a], buf[d], buf[b], dt_dev, active(), spd_part, rho_part, st()));
+        count(1);
+        h->perf.steps += 1;
         cur = b;
         rho_part_valid = true;
         phi_valid = false;
@@ -407,13 +453,18 @@ template <class T> struct Mhd2d : Mhd2dBase {
             if (r) return r;
         }
         CC_CUDA(launch_dt_finalize(spd_part, dtspec(true), dt_dev, t_dev, active(), st()));
+        count(1);
         r = step_body(p.gravity_on ? GRAV_PHI : GRAV_NONE);
         if (r) return r;
         CC_CUDA(launch_clock(t_dev, dt_dev, active(), steps_dev, st()));
+        count(1);
         return CC_OK;
     }
 
-    bool graph_ok() const { return !(p.gravity_on && p.poisson_kind == CC_POISSON_SOR); }
+    // SOR uses a cooperative launch and profiling records events per launch:
+    // both run eagerly
+    bool graph_ok() const { return !(p.gravity_on && p.poisson_kind == CC_POISSON_SOR) && !h->profiling; }
+    cc_perf graph_delta{};   // counters added by one replay of graph3
 
     int advance(int nsteps, double* t) override {
         if (!loaded) return fail(h, CC_ERR_STATE, "no state uploaded");
@@ -427,11 +478,16 @@ template <class T> struct Mhd2d : Mhd2dBase {
                 invalidate_graph();
                 const int start = cur;
                 cudaGraph_t g = nullptr;
+                const cc_perf before = h->perf;
                 CC_CUDA(cudaStreamBeginCapture(st(), cudaStreamCaptureModeThreadLocal));
                 int rr = CC_OK;
                 for (int k = 0; k < 3 && rr == CC_OK; k++) rr = device_step();
                 cudaError_t e = cudaStreamEndCapture(st(), &g);
                 cur = start;
+                graph_delta.kernel_launches = h->perf.kernel_launches - before.kernel_launches;
+                graph_delta.poisson_solves = h->perf.poisson_solves - before.poisson_solves;
+                graph_delta.steps = h->perf.steps - before.steps;
+                h->perf = before;   // captured, not run: counted per replay below
                 if (rr) { if (g) cudaGraphDestroy(g); return rr; }
                 if (e != cudaSuccess) return fail(h, CC_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(e));
                 e = cudaGraphInstantiate(&graph3, g, 0);
@@ -442,6 +498,9 @@ template <class T> struct Mhd2d : Mhd2dBase {
             }
             while (nsteps - done >= 3) {
                 CC_CUDA(cudaGraphLaunch(graph3, st()));
+                h->perf.kernel_launches += graph_delta.kernel_launches;
+                h->perf.poisson_solves += graph_delta.poisson_solves;
+                h->perf.steps += graph_delta.steps;
                 done += 3;
             }
             rho_part_valid = true;
@@ -573,6 +632,32 @@ int cc_synchronize(cc_handle* h) {
     if (int r = set_dev(h)) return r;
     cudaError_t e = cudaStreamSynchronize(h->stream);
     if (e != cudaSuccess) return fail(h, CC_ERR_CUDA, cudaGetErrorString(e));
+    return CC_OK;
+}
+
+int cc_set_profiling(cc_handle* h, int on) {
+    if (!h) return CC_ERR_ARG;
+    h->profiling = on != 0;
+    return CC_OK;
+}
+
+int cc_get_perf(cc_handle* h, cc_perf* out) {
+    if (!h || !out) return CC_ERR_ARG;
+    if (int r = set_dev(h)) return r;
+    cudaError_t e = cudaStreamSynchronize(h->stream);
+    if (e == cudaSuccess) e = h->collect();
+    if (e != cudaSuccess) return fail(h, CC_ERR_CUDA, cudaGetErrorString(e));
+    *out = h->perf;
+    return CC_OK;
+}
+
+int cc_reset_perf(cc_handle* h) {
+    if (!h) return CC_ERR_ARG;
+    if (int r = set_dev(h)) return r;
+    cudaError_t e = cudaStreamSynchronize(h->stream);
+    if (e == cudaSuccess) e = h->collect();
+    if (e != cudaSuccess) return fail(h, CC_ERR_CUDA, cudaGetErrorString(e));
+    h->perf = cc_perf{};
     return CC_OK;
 }
 

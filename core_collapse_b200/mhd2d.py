@@ -199,6 +199,24 @@ class Mhd2dSolver:
         self._check(self._lib.cc_mhd2d_advance(self._h, int(nsteps), C.byref(tt)))
         return tt.value
 
+    def set_stream(self, stream_ptr: int | None):
+        """Issue work on a caller's cudaStream_t (e.g. torch's current stream)."""
+        self._check(self._lib.cc_set_stream(self._h, C.c_void_p(stream_ptr) if stream_ptr else None))
+
+    def synchronize(self):
+        self._check(self._lib.cc_synchronize(self._h))
+
+    def set_profiling(self, on: bool):
+        self._check(self._lib.cc_set_profiling(self._h, 1 if on else 0))
+
+    def perf(self) -> dict:
+        q = L.CcPerf()
+        self._check(self._lib.cc_get_perf(self._h, C.byref(q)))
+        return {f: getattr(q, f) for f, _ in L.CcPerf._fields_}
+
+    def reset_perf(self):
+        self._check(self._lib.cc_reset_perf(self._h))
+
     def diagnostics(self) -> dict:
         d = L.CcDiag()
         self._check(self._lib.cc_mhd2d_diagnostics(self._h, C.byref(d)))

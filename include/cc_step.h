@@ -142,6 +142,19 @@ typedef struct cc_diag {
     double poisson_residual;/* max |lap(phi)-rhs| after the last SOR solve */
 } cc_diag;
 
+/* Performance counters of a handle (no reference counterpart: measurement
+ * support).  kernel_launches counts every kernel this library launched on the
+ * handle (graph replays included).  With profiling on, the stage kernels are
+ * bracketed by CUDA events on the handle's stream and time loops run without
+ * graphs; stage_ms is their summed event time. */
+typedef struct cc_perf {
+    int64_t kernel_launches;
+    int64_t stage_launches;     /* stage-kernel launches that were event-timed */
+    double stage_ms;            /* summed event time of those launches */
+    int64_t poisson_solves;
+    int64_t steps;
+} cc_perf;
+
 /* Fill with the reference defaults (mhd2d_resistive_hlld_ct_gravity.cpp:44-86). */
 void cc_mhd2d_params_default(cc_mhd2d_params* p);
 
@@ -153,6 +166,11 @@ const char* cc_last_error(const cc_handle* h);
  * NULL restores the handle's own stream. */
 int cc_set_stream(cc_handle* h, void* stream);
 int cc_synchronize(cc_handle* h);
+
+/* Measurement support (no reference counterpart). */
+int cc_set_profiling(cc_handle* h, int on);
+int cc_get_perf(cc_handle* h, cc_perf* out);   /* synchronizes the handle's stream */
+int cc_reset_perf(cc_handle* h);
 
 /* ---- 2D MHD state transfer (reference layouts, FP64 host arrays) ---- */
 /* Ucc {rho,mx,my,mz,E,Bz} and Bfaces {Bx_f,By_f}: M2:88-95 */

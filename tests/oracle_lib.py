@@ -99,7 +99,12 @@ def dp(a: np.ndarray):
 
 
 def pp(arrays) -> C.Array:
-    return (_DP * len(arrays))(*[dp(a) for a in arrays])
+    """Pointer array over `arrays`; it holds references to them, so a
+    temporary list stays alive for as long as the pointer array does."""
+    arrays = list(arrays)
+    out = (_DP * len(arrays))(*[dp(a) for a in arrays])
+    out._keep = arrays
+    return out
 
 
 # ---- state helpers: a 2D MHD state is the list [rho, mx, my, mz, E, Bz, Bx_f, By_f] ----
