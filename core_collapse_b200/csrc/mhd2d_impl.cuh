@@ -42,10 +42,11 @@ template <class T>
 cudaError_t M2Launch<T>::stage(const M2Const<T>& c, const Fields<T>& in, const Fields<T>& out, bool defer, int gmode,
                                const T* ga, const T* gb, const double* dt, const int* active, cudaStream_t s) {
     const size_t smem = m2_stage_smem<T>();
-    dim3 grid((c.nx + M2_TX - 1) / M2_TX, (c.ny + M2_TY - 1) / M2_TY);
+    using Gm = StageGeom<T>;
+    dim3 grid((c.nx + Gm::TX - 1) / Gm::TX, (c.ny + Gm::TY - 1) / Gm::TY);
 #define CC_STAGE_CASE(D, G)                                                                 \
     if (defer == D && gmode == G) {                                                         \
-        m2_stage_kernel<T, D, G><<<grid, M2_NT, smem, s>>>(c, in, out, ga, gb, dt, active); \
+        m2_stage_kernel<T, D, G><<<grid, Gm::NT, smem, s>>>(c, in, out, ga, gb, dt, active); \
         return cudaGetLastError();                                                          \
     }
     CC_STAGE_CASE(false, GRAV_NONE)

@@ -30,17 +30,25 @@ template <class T> struct Fields {
 
 enum GravMode { GRAV_NONE = 0, GRAV_ARRAYS = 1, GRAV_PHI = 2 };
 
-constexpr int M2_TX = 32, M2_TY = 8, M2_HALO = 2;
-constexpr int M2_RX = M2_TX + 2 * M2_HALO, M2_RY = M2_TY + 2 * M2_HALO;
-constexpr int M2_RR = M2_RX * M2_RY;
-constexpr int M2_NT = M2_TX * M2_TY;
-constexpr int M2_NFX = (M2_TX + 1) * (M2_TY + 2);   // x faces: TX+1 per row, rows -1..TY
-constexpr int M2_NGY = (M2_TX + 2) * (M2_TY + 1);   // y faces: cols -1..TX, TY+1 per col
-constexpr int M2_NE = (M2_TX + 1) * (M2_TY + 1);    // edges
+// Stage tile per precision: TX x TY cells per CTA (one thread per cell), a
+// halo-2 region of primitives, one shared slope buffer reused for x then y.
+template <class T> struct StageTile;
+template <> struct StageTile<double> { static constexpr int TX = 32, TY = 8, MINB = 2; };
+template <> struct StageTile<float> { static constexpr int TX = 32, TY = 16, MINB = 2; };
 
-template <class T> constexpr size_t m2_stage_smem() {
-    return sizeof(T) * (size_t)(8 * M2_RR + 7 * M2_NFX + 7 * M2_NGY + M2_NE + 6 * M2_NT);
-}
+template <class T> struct StageGeom {
+    static constexpr int TX = StageTile<T>::TX, TY = StageTile<T>::TY, HALO = 2;
+    static constexpr int RX = TX + 2 * HALO, RY = TY + 2 * HALO, RR = RX * RY;
+    static constexpr int NT = TX * TY;
+    static constexpr int NFX = (TX + 1) * (TY + 2);  // x faces: TX+1 per row, rows -1..TY
+    static constexpr int NGY = (TX + 2) * (TY + 1);  // y faces: cols -1..TX, TY+1 per col
+    static constexpr int NE = (TX + 1) * (TY + 1);   // edges
+    static constexpr int NSL = (TX + 2) * (TY + 2);  // cells whose slopes a face needs
+    // prims (8 RR) + slopes (7 NSL) + x fluxes (7 NFX) + y fluxes (7 NGY) + Ez + own state (6 NT)
+    static constexpr size_t smem = sizeof(T) * (size_t)(8 * RR + 7 * NSL + 7 * NFX + 7 * NGY + NE + 6 * NT);
+};
+
+template <class T> constexpr size_t m2_stage_smem() { return StageGeom<T>::smem; }
 
 // Joule heating, explicit Bz diffusion and floors of one cell
 // (add_joule_heating_and_Bz_resistive, M2:631-686), applied to the stored
@@ -73,28 +81,32 @@ __device__ __forceinline__ void joule_cell(const M2Const<T>& c, const Fields<T>&
 // Joule sub-step must be applied first.  GMODE selects the gravity source.
 // ---------------------------------------------------------------------------
 template <class T, bool DEFER, int GMODE>
-__global__ void __launch_bounds__(M2_NT, 2)
+__global__ void __launch_bounds__(StageGeom<T>::NT, StageTile<T>::MINB)
 m2_stage_kernel(const M2Const<T> c, const Fields<T> in, const Fields<T> out, const T* __restrict__ ga,
                 const T* __restrict__ gb, const double* __restrict__ dtp, const int* __restrict__ active) {
+    using G = StageGeom<T>;
+    constexpr int TX = G::TX, TY = G::TY, HALO = G::HALO, RX = G::RX, RR = G::RR, NT = G::NT;
+    constexpr int NFX = G::NFX, NGY = G::NGY, NSL = G::NSL;
     if (active && *active == 0) return;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     T* sm = reinterpret_cast<T*>(smem_raw);
-    T* s_r = sm;            T* s_u = s_r + M2_RR;   T* s_v = s_u + M2_RR;   T* s_w = s_v + M2_RR;
-    T* s_P = s_w + M2_RR;   T* s_bx = s_P + M2_RR;  T* s_by = s_bx + M2_RR; T* s_bz = s_by + M2_RR;
-    T* fx = s_bz + M2_RR;       // 7 planes of M2_NFX
-    T* gy = fx + 7 * M2_NFX;    // 7 planes of M2_NGY
-    T* ez = gy + 7 * M2_NGY;    // M2_NE
-    T* own = ez + M2_NE;        // 6 planes of M2_NT
+    T* s_r = sm;          T* s_u = s_r + RR;   T* s_v = s_u + RR;   T* s_w = s_v + RR;
+    T* s_P = s_w + RR;    T* s_bx = s_P + RR;  T* s_by = s_bx + RR; T* s_bz = s_by + RR;
+    T* sl = s_bz + RR;          // 7 planes of NSL: slopes of cells (-1..TX) x (-1..TY), x then y
+    T* fx = sl + 7 * NSL;       // 7 planes of NFX
+    T* gy = fx + 7 * NFX;       // 7 planes of NGY
+    T* ez = gy + 7 * NGY;       // NE
+    T* own = ez + G::NE;        // 6 planes of NT
 
     const int tid = threadIdx.x;
-    const int i0 = blockIdx.x * M2_TX, j0 = blockIdx.y * M2_TY;
+    const int i0 = blockIdx.x * TX, j0 = blockIdx.y * TY;
     const int P = c.pitch;
     const T dt = (T)(*dtp);
 
     // ---- A: primitives on the halo-2 region (get_prim_cc, M2:278-286) ----
-    for (int k = tid; k < M2_RR; k += M2_NT) {
-        const int rx = k % M2_RX, ry = k / M2_RX;
-        const int gi = i0 - M2_HALO + rx, gj = j0 - M2_HALO + ry;
+    for (int k = tid; k < RR; k += NT) {
+        const int rx = k % RX, ry = k / RX;
+        const int gi = i0 - HALO + rx, gj = j0 - HALO + ry;
         const int ci = c.ax.cell(gi), cj = c.ay.cell(gj);
         const size_t q = (size_t)cj * P + ci;
         T rho = in.rho[q], mx = in.mx[q], my = in.my[q], mz = in.mz[q], E = in.E[q], Bz = in.Bz[q];
@@ -104,78 +116,94 @@ m2_stage_kernel(const M2Const<T> c, const Fields<T> in, const Fields<T> out, con
         const Prim<T> W = to_prim(c, rho, mx, my, mz, E, Bx, By, Bz);
         s_r[k] = W.r; s_u[k] = W.u; s_v[k] = W.v; s_w[k] = W.w;
         s_P[k] = W.P; s_bx[k] = W.bx; s_by[k] = W.by; s_bz[k] = W.bz;
-        const int ox = rx - M2_HALO, oy = ry - M2_HALO;
-        if (ox >= 0 && ox < M2_TX && oy >= 0 && oy < M2_TY) {
-            const int o = oy * M2_TX + ox;
-            own[o] = rho; own[M2_NT + o] = mx; own[2 * M2_NT + o] = my;
-            own[3 * M2_NT + o] = mz; own[4 * M2_NT + o] = E; own[5 * M2_NT + o] = Bz;
+        const int ox = rx - HALO, oy = ry - HALO;
+        if (ox >= 0 && ox < TX && oy >= 0 && oy < TY) {
+            const int o = oy * TX + ox;
+            own[o] = rho; own[NT + o] = mx; own[2 * NT + o] = my;
+            own[3 * NT + o] = mz; own[4 * NT + o] = E; own[5 * NT + o] = Bz;
         }
     }
     __syncthreads();
 
-    auto load_prim = [&](int k) {
-        Prim<T> W;
-        W.r = s_r[k]; W.u = s_u[k]; W.v = s_v[k]; W.w = s_w[k];
-        W.P = s_P[k]; W.bx = s_bx[k]; W.by = s_by[k]; W.bz = s_bz[k];
-        return W;
+    // slope-buffer index of the cell at local (lx, ly), lx, ly in [-1, TX] x [-1, TY]
+    auto sidx = [&](int lx, int ly) { return (ly + 1) * (TX + 2) + (lx + 1); };
+    // region index of the same cell
+    auto ridx = [&](int lx, int ly) { return (ly + HALO) * RX + (lx + HALO); };
+    // MC slopes of one cell along stride st (recon_x / recon_y, M2:295-303, 319-327);
+    // component 5 is the transverse in-plane B (By for x, Bx for y)
+    auto slopes = [&](int k, int st, bool ydir, int o) {
+        sl[o] = mc_slope(s_r[k - st], s_r[k], s_r[k + st]);
+        sl[NSL + o] = mc_slope(s_u[k - st], s_u[k], s_u[k + st]);
+        sl[2 * NSL + o] = mc_slope(s_v[k - st], s_v[k], s_v[k + st]);
+        sl[3 * NSL + o] = mc_slope(s_w[k - st], s_w[k], s_w[k + st]);
+        sl[4 * NSL + o] = mc_slope(s_P[k - st], s_P[k], s_P[k + st]);
+        sl[5 * NSL + o] = ydir ? mc_slope(s_bx[k - st], s_bx[k], s_bx[k + st])
+                               : mc_slope(s_by[k - st], s_by[k], s_by[k + st]);
+        sl[6 * NSL + o] = mc_slope(s_bz[k - st], s_bz[k], s_bz[k + st]);
     };
-    // MUSCL-MC face state of the cell at region index k, stencil stride st
-    // (1: x, M2_RX: y); side +1 gives the state at the cell's upper face,
-    // -1 at its lower face (recon_x / recon_y, M2:290-336).
-    auto face_state = [&](int k, int st, bool ydir, T side) {
-        const Prim<T> Wc = load_prim(k);
-        Prim<T> W = Wc;
+    // face state of a cell: centre value + side * 0.5 * slope, then floors (M2:305-311)
+    auto face_state = [&](int k, int o, bool ydir, T side) {
+        Prim<T> W;
         const T h = T(0.5) * side;
-        W.r = Wc.r + h * mc_slope(s_r[k - st], Wc.r, s_r[k + st]);
-        W.u = Wc.u + h * mc_slope(s_u[k - st], Wc.u, s_u[k + st]);
-        W.v = Wc.v + h * mc_slope(s_v[k - st], Wc.v, s_v[k + st]);
-        W.w = Wc.w + h * mc_slope(s_w[k - st], Wc.w, s_w[k + st]);
-        W.P = Wc.P + h * mc_slope(s_P[k - st], Wc.P, s_P[k + st]);
-        if (ydir) W.bx = Wc.bx + h * mc_slope(s_bx[k - st], Wc.bx, s_bx[k + st]);
-        else      W.by = Wc.by + h * mc_slope(s_by[k - st], Wc.by, s_by[k + st]);
-        W.bz = Wc.bz + h * mc_slope(s_bz[k - st], Wc.bz, s_bz[k + st]);
+        W.r = s_r[k] + h * sl[o];
+        W.u = s_u[k] + h * sl[NSL + o];
+        W.v = s_v[k] + h * sl[2 * NSL + o];
+        W.w = s_w[k] + h * sl[3 * NSL + o];
+        W.P = s_P[k] + h * sl[4 * NSL + o];
+        if (ydir) { W.bx = s_bx[k] + h * sl[5 * NSL + o]; W.by = s_by[k]; }
+        else      { W.bx = s_bx[k]; W.by = s_by[k] + h * sl[5 * NSL + o]; }
+        W.bz = s_bz[k] + h * sl[6 * NSL + o];
         W.r = vmax(W.r, c.floor_rho);
         W.P = vmax(W.P, c.floor_P);
         return W;
     };
 
-    // ---- B: x-face fluxes, faces i0..i0+TX, rows j0-1..j0+TY (M2:706-725) ----
-    for (int k = tid; k < M2_NFX; k += M2_NT) {
-        const int f = k % (M2_TX + 1), r = k / (M2_TX + 1) - 1;
+    // ---- B: x slopes, then x-face fluxes: faces i0..i0+TX, rows j0-1..j0+TY (M2:706-725) ----
+    for (int k = tid; k < NSL; k += NT) {
+        const int lx = k % (TX + 2) - 1, ly = k / (TX + 2) - 1;
+        slopes(ridx(lx, ly), 1, false, k);
+    }
+    __syncthreads();
+    for (int k = tid; k < NFX; k += NT) {
+        const int f = k % (TX + 1), r = k / (TX + 1) - 1;
         const int gi = i0 + f;
         if (gi > c.nx) continue;
         const int cj = c.ay.cell(j0 + r);
-        const int kl = (r + M2_HALO) * M2_RX + (f - 1 + M2_HALO);   // left cell
-        const Prim<T> WL = face_state(kl, 1, false, T(1));
-        const Prim<T> WR = face_state(kl + 1, 1, false, T(-1));
+        const Prim<T> WL = face_state(ridx(f - 1, r), sidx(f - 1, r), false, T(1));
+        const Prim<T> WR = face_state(ridx(f, r), sidx(f, r), false, T(-1));
         const Flux<T> F = hlld_x(c, WL, WR, in.bx[(size_t)cj * P + gi]);
-        fx[k] = F.f0; fx[M2_NFX + k] = F.f1; fx[2 * M2_NFX + k] = F.f2; fx[3 * M2_NFX + k] = F.f3;
-        fx[4 * M2_NFX + k] = F.f4; fx[5 * M2_NFX + k] = F.f5; fx[6 * M2_NFX + k] = F.f6;
+        fx[k] = F.f0; fx[NFX + k] = F.f1; fx[2 * NFX + k] = F.f2; fx[3 * NFX + k] = F.f3;
+        fx[4 * NFX + k] = F.f4; fx[5 * NFX + k] = F.f5; fx[6 * NFX + k] = F.f6;
     }
-    // ---- C: y-face fluxes, y faces j0..j0+TY, columns i0-1..i0+TX (M2:728-747) ----
-    for (int k = tid; k < M2_NGY; k += M2_NT) {
-        const int col = k % (M2_TX + 2) - 1, g = k / (M2_TX + 2);
+    __syncthreads();
+    // ---- C: y slopes, then y-face fluxes: y faces j0..j0+TY, columns i0-1..i0+TX (M2:728-747) ----
+    for (int k = tid; k < NSL; k += NT) {
+        const int lx = k % (TX + 2) - 1, ly = k / (TX + 2) - 1;
+        slopes(ridx(lx, ly), RX, true, k);
+    }
+    __syncthreads();
+    for (int k = tid; k < NGY; k += NT) {
+        const int col = k % (TX + 2) - 1, g = k / (TX + 2);
         const int gj = j0 + g;
         if (gj > c.ny) continue;
         const int ci = c.ax.cell(i0 + col);
-        const int kd = (g - 1 + M2_HALO) * M2_RX + (col + M2_HALO);  // lower cell
-        const Prim<T> WL = face_state(kd, M2_RX, true, T(1));
-        const Prim<T> WR = face_state(kd + M2_RX, M2_RX, true, T(-1));
-        const Flux<T> G = hlld_y(c, WL, WR, in.by[(size_t)gj * P + ci]);
-        gy[k] = G.f0; gy[M2_NGY + k] = G.f1; gy[2 * M2_NGY + k] = G.f2; gy[3 * M2_NGY + k] = G.f3;
-        gy[4 * M2_NGY + k] = G.f4; gy[5 * M2_NGY + k] = G.f5; gy[6 * M2_NGY + k] = G.f6;
+        const Prim<T> WL = face_state(ridx(col, g - 1), sidx(col, g - 1), true, T(1));
+        const Prim<T> WR = face_state(ridx(col, g), sidx(col, g), true, T(-1));
+        const Flux<T> Gf = hlld_y(c, WL, WR, in.by[(size_t)gj * P + ci]);
+        gy[k] = Gf.f0; gy[NGY + k] = Gf.f1; gy[2 * NGY + k] = Gf.f2; gy[3 * NGY + k] = Gf.f3;
+        gy[4 * NGY + k] = Gf.f4; gy[5 * NGY + k] = Gf.f5; gy[6 * NGY + k] = Gf.f6;
     }
     __syncthreads();
 
     // ---- E: edge EMFs, edges i0..i0+TX x j0..j0+TY (M2:782-804, 565-575) ----
-    for (int k = tid; k < M2_NE; k += M2_NT) {
-        const int ei = k % (M2_TX + 1), ej = k / (M2_TX + 1);
+    for (int k = tid; k < G::NE; k += NT) {
+        const int ei = k % (TX + 1), ej = k / (TX + 1);
         const int ie = i0 + ei, je = j0 + ej;
         if (ie > c.nx || je > c.ny) continue;
-        const T exm = -fx[5 * M2_NFX + ej * (M2_TX + 1) + ei];        // x face ie, row je-1
-        const T ex0 = -fx[5 * M2_NFX + (ej + 1) * (M2_TX + 1) + ei];  // x face ie, row je
-        const T eym = gy[5 * M2_NGY + ej * (M2_TX + 2) + ei];         // y face je, col ie-1
-        const T ey0 = gy[5 * M2_NGY + ej * (M2_TX + 2) + ei + 1];     // y face je, col ie
+        const T exm = -fx[5 * NFX + ej * (TX + 1) + ei];        // x face ie, row je-1
+        const T ex0 = -fx[5 * NFX + (ej + 1) * (TX + 1) + ei];  // x face ie, row je
+        const T eym = gy[5 * NGY + ej * (TX + 2) + ei];         // y face je, col ie-1
+        const T ey0 = gy[5 * NGY + ej * (TX + 2) + ei + 1];     // y face je, col ie
         const T ideal = T(0.25) * (exm + ex0 + eym + ey0);
         T res = T(0.0);
         if (c.resistive) {
@@ -190,34 +218,34 @@ m2_stage_kernel(const M2Const<T> c, const Fields<T> in, const Fields<T> out, con
     __syncthreads();
 
     // ---- D+F: FV update, floors, CT, gravity kick, store (M2:750-779, 807-832) ----
-    const int tx = tid % M2_TX, ty = tid / M2_TX;
+    const int tx = tid % TX, ty = tid / TX;
     const int gi = i0 + tx, gj = j0 + ty;
     if (gi >= c.nx || gj >= c.ny) return;
     const size_t q = (size_t)gj * P + gi;
-    const int o = ty * M2_TX + tx;
-    T rho = own[o], mx = own[M2_NT + o], my = own[2 * M2_NT + o];
-    T mz = own[3 * M2_NT + o], E = own[4 * M2_NT + o], Bz = own[5 * M2_NT + o];
+    const int o = ty * TX + tx;
+    T rho = own[o], mx = own[NT + o], my = own[2 * NT + o];
+    T mz = own[3 * NT + o], E = own[4 * NT + o], Bz = own[5 * NT + o];
     {
-        const int kxL = (ty + 1) * (M2_TX + 1) + tx;
-        const int kgD = ty * (M2_TX + 2) + tx + 1, kgU = kgD + (M2_TX + 2);
+        const int kxL = (ty + 1) * (TX + 1) + tx;
+        const int kgD = ty * (TX + 2) + tx + 1, kgU = kgD + (TX + 2);
         T d[7];
 #pragma unroll
         for (int m = 0; m < 7; m++)
-            d[m] = -(fx[m * M2_NFX + kxL + 1] - fx[m * M2_NFX + kxL]) * c.inv_dx -
-                   (gy[m * M2_NGY + kgU] - gy[m * M2_NGY + kgD]) * c.inv_dy;
+            d[m] = -(fx[m * NFX + kxL + 1] - fx[m * NFX + kxL]) * c.inv_dx -
+                   (gy[m * NGY + kgU] - gy[m * NGY + kgD]) * c.inv_dy;
         rho += dt * d[0];
         mx += dt * d[1];
         my += dt * d[2];
         mz += dt * d[3];
         E += dt * d[4];
         Bz += dt * d[6];
-        const int kc = (ty + M2_HALO) * M2_RX + tx + M2_HALO;
+        const int kc = ridx(tx, ty);
         floors(c, rho, mx, my, mz, E, s_bx[kc], s_by[kc], Bz);
     }
     // CT (M2:807-830) for this cell's four faces
     const T dtdy = dt / c.dy, dtdx = dt / c.dx;
-    const T e00 = ez[ty * (M2_TX + 1) + tx], e10 = ez[ty * (M2_TX + 1) + tx + 1];
-    const T e01 = ez[(ty + 1) * (M2_TX + 1) + tx], e11 = ez[(ty + 1) * (M2_TX + 1) + tx + 1];
+    const T e00 = ez[ty * (TX + 1) + tx], e10 = ez[ty * (TX + 1) + tx + 1];
+    const T e01 = ez[(ty + 1) * (TX + 1) + tx], e11 = ez[(ty + 1) * (TX + 1) + tx + 1];
     const T bxL = in.bx[q] + -(dtdy) * (e01 - e00);
     const T bxR = in.bx[q + 1] + -(dtdy) * (e11 - e10);
     const T byD = in.by[q] + +(dtdx) * (e10 - e00);
