@@ -14,6 +14,9 @@ CC_ERR_STATE = -3
 CC_ERR_NONFINITE = -4
 CC_ERR_NOT_CONVERGED = -5
 CC_ERR_UNSUPPORTED = -6
+CC_ERR_TOO_LARGE = -7
+CC_NOALLOC_MAX_CELLS = 1 << 18
+CC_NOALLOC_MAX_SIDE = 4096
 
 CC_FP64 = 0
 CC_FP32 = 1
@@ -113,6 +116,8 @@ SIGNATURES = {
     "cc_mhd2d_rk2_step": (C.c_int, [_H, _DP, _DP, C.c_double]),
     "cc_mhd2d_advance": (C.c_int, [_H, C.c_int, _DP]),
     "cc_mhd2d_diagnostics": (C.c_int, [_H, C.POINTER(CcDiag)]),
+    "cc_mhd2d_gravity_fft_noalloc": (C.c_int, [C.POINTER(CcMhd2dParams), C.c_void_p, C.c_void_p, C.c_void_p,
+                                               C.c_void_p]),
     "cc_mhd2d_ic_knobs_default": (None, [C.POINTER(CcIcKnobs)]),
     "cc_ic_mhd2d_reference": (C.c_int, [C.POINTER(CcMhd2dParams), C.POINTER(CcIcKnobs), C.POINTER(_DP)]),
     "cc_ic_mhd2d_collapse": (C.c_int, [C.POINTER(CcMhd2dParams), C.c_double, C.c_double, C.c_double, C.c_uint32,

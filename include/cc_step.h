@@ -211,6 +211,33 @@ int cc_mhd2d_advance(cc_handle* h, int nsteps, double* t);
 /* Diagnostics of the resident state. */
 int cc_mhd2d_diagnostics(cc_handle* h, cc_diag* d);
 
+/* ---- spectral gravity without device allocation ----
+ * No counterpart in the reference: an addition for callers that cannot call
+ * cudaMalloc -- a host application whose memory manager owns the GPU's
+ * memory, or a loop that must not pay cudaMalloc's implicit device
+ * synchronisation.  Same result as cc_mhd2d_compute_gravity with
+ * poisson_kind == CC_POISSON_FFT and precision == CC_FP64, computed from device
+ * arrays: rho (input) and gx, gy (outputs) are caller-owned device pointers,
+ * FP64, Nx*Ny each, q = j*Nx + i.  Work is queued on `stream`
+ * (cudaStream_t, NULL = legacy default stream) and the call returns without
+ * waiting for it.
+ *
+ * Scratch lives in one fixed device array inside the library (about 6.6 MB,
+ * held by every GPU that loads the library until the process exits); nothing
+ * is allocated or freed.  Limits: periodic, Nx and Ny powers of two with
+ * 4 <= Nx, Ny <= CC_NOALLOC_MAX_SIDE and Nx*Ny <= CC_NOALLOC_MAX_CELLS;
+ * larger grids return CC_ERR_TOO_LARGE.
+ * The first call on a device looks up the array's device address and raises
+ * the FFT kernels' shared-memory limits; make that first call before any
+ * stream capture.  Every call reuses the same array, which keeps the last
+ * call's contents (each call overwrites everything it reads, nothing needs to
+ * start at zero): calls that overlap on the GPU -- on two streams, from two
+ * host threads -- race and must be serialised by the caller. */
+#define CC_ERR_TOO_LARGE -7
+#define CC_NOALLOC_MAX_CELLS (1 << 18)
+#define CC_NOALLOC_MAX_SIDE 4096
+int cc_mhd2d_gravity_fft_noalloc(const cc_mhd2d_params* p, const double* rho, double* gx, double* gy, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
