@@ -10,6 +10,7 @@
 
 #include "../include/cc_step.h"
 #include "mhd2d_oracle.hpp"
+#include "mhd3d_oracle.hpp"
 #include "poisson_oracle.hpp"
 
 namespace {
@@ -68,6 +69,49 @@ PoissonResult gravity(const cc_mhd2d_params* c, const std::vector<double>& rho, 
     }
     gravity_from_phi(s, phi, gx, gy);
     return r;
+}
+
+M3Par m3par(const cc_mhd3d_params* c) {
+    M3Par p;
+    p.gamma1 = c->gamma1; p.gamma2 = c->gamma2; p.K1 = c->K1; p.rho_nuc = c->rho_nuc; p.gamma_th = c->gamma_th;
+    p.rho_bounce = c->rho_bounce; p.gamma_bounce = c->gamma_bounce; p.Kbounce = c->Kbounce; p.cfl = c->cfl;
+    p.x0 = c->x0; p.x1 = c->x1; p.y0 = c->y0; p.y1 = c->y1; p.z0 = c->z0; p.z1 = c->z1;
+    p.nx = c->Nx; p.ny = c->Ny; p.nz = c->Nz;
+    p.floor_rho = c->floor_rho; p.floor_P = c->floor_P;
+    p.px = c->periodic_x != 0; p.py = c->periodic_y != 0; p.pz = c->periodic_z != 0;
+    p.eta = c->eta;
+    return p;
+}
+
+template <class T> void load3(const cc_mhd3d_params* c, const double* const* f, M3State<T>& s) {
+    size_t nx = c->Nx, ny = c->Ny, nz = c->Nz, N = nx * ny * nz;
+    std::vector<T>* cell[5] = {&s.rho, &s.mx, &s.my, &s.mz, &s.E};
+    for (int k = 0; k < 5; k++) cell[k]->assign(f[k], f[k] + N);
+    s.bxf.assign(f[5], f[5] + (nx + 1) * ny * nz);
+    s.byf.assign(f[6], f[6] + nx * (ny + 1) * nz);
+    s.bzf.assign(f[7], f[7] + nx * ny * (nz + 1));
+}
+
+template <class T> void store3(const M3State<T>& s, double* const* f) {
+    const std::vector<T>* v[8] = {&s.rho, &s.mx, &s.my, &s.mz, &s.E, &s.bxf, &s.byf, &s.bzf};
+    for (int k = 0; k < 8; k++)
+        for (size_t q = 0; q < v[k]->size(); q++) f[k][q] = (double)(*v[k])[q];
+}
+
+template <class T> int main_loop3(const cc_mhd3d_params* c, double* const* f, int nsteps, double* t) {
+    M3State<T> s;
+    load3(c, f, s);
+    M3<T> m(m3par(c));
+    double tt = t ? *t : 0.0;
+    for (int n = 0; n < nsteps && tt < c->t_end; ++n) {  // M3:1285-1291
+        double dt = m.compute_dt(s);
+        if (tt + dt > c->t_end) dt = c->t_end - tt;
+        m.rk2_step(s, T(dt));
+        tt += dt;
+    }
+    store3(s, f);
+    if (t) *t = tt;
+    return 0;
 }
 
 template <class T> std::vector<T> cast(const std::vector<double>& v) { return std::vector<T>(v.begin(), v.end()); }
@@ -172,6 +216,39 @@ double or_mhd2d_divB_max(const cc_mhd2d_params* c, const double* const* f) {
     M2State<double> s;
     load(c, f, s);
     return M2<double>(m2par(c)).max_divB(s);
+}
+
+// ---- 3D MHD (mhd3d_resistive_hlld_ct.cpp) ----
+int or_mhd3d_advance_stage(const cc_mhd3d_params* c, const double* const* fin, double* const* fout, double dt) {
+    M3State<double> s0, s1;
+    load3(c, fin, s0);
+    M3<double>(m3par(c)).advance_stage(s0, s1, dt);
+    store3(s1, fout);
+    return 0;
+}
+
+int or_mhd3d_rk2_step(const cc_mhd3d_params* c, double* const* f, double dt) {
+    M3State<double> s;
+    load3(c, f, s);
+    M3<double>(m3par(c)).rk2_step(s, dt);
+    store3(s, f);
+    return 0;
+}
+
+double or_mhd3d_compute_dt(const cc_mhd3d_params* c, const double* const* f) {
+    M3State<double> s;
+    load3(c, f, s);
+    return M3<double>(m3par(c)).compute_dt(s);
+}
+
+int or_mhd3d_main_loop(const cc_mhd3d_params* c, double* const* f, int nsteps, double* t, int fp32) {
+    return fp32 ? main_loop3<float>(c, f, nsteps, t) : main_loop3<double>(c, f, nsteps, t);
+}
+
+double or_mhd3d_divB_max(const cc_mhd3d_params* c, const double* const* f) {
+    M3State<double> s;
+    load3(c, f, s);
+    return M3<double>(m3par(c)).max_divB(s);
 }
 
 // Gravity of a density field with every Poisson knob explicit (used to pin the

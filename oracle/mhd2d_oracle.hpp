@@ -33,9 +33,6 @@ template <class T> struct M2State {
     std::vector<T> byf;                     // nx*(ny+1), j_face*nx+i
 };
 
-template <class T> struct Prim8 { T r, u, v, w, P, bx, by, bz; };
-template <class T> struct Flux7 { T f[7]; };  // rho, mx, my, mz, E, B_t1, B_t2
-
 template <class T> class M2 {
 public:
     M2Par p;
@@ -105,102 +102,9 @@ public:
         return std::sqrt(vmax(T(0.0), cf2));
     }
 
-    // x-normal ideal flux (M2:351-370); f[5]=flux of By, f[6]=flux of Bz
-    Flux7<T> flux_x(const Prim8<T>& W) const {
-        T rho = W.r, u = W.u, v = W.v, w = W.w, P = W.P, Bx = W.bx, By = W.by, Bz = W.bz;
-        T v2 = u * u + v * v + w * w;
-        T B2 = Bx * Bx + By * By + Bz * Bz;
-        T pt = P + T(0.5) * B2;
-        T E = P / gm1 + T(0.5) * rho * v2 + T(0.5) * B2;
-        T vdotB = u * Bx + v * By + w * Bz;
-        Flux7<T> F;
-        F.f[0] = rho * u;
-        F.f[1] = rho * u * u + pt - Bx * Bx;
-        F.f[2] = rho * u * v - Bx * By;
-        F.f[3] = rho * u * w - Bx * Bz;
-        F.f[4] = (E + pt) * u - Bx * vdotB;
-        F.f[5] = u * By - v * Bx;
-        F.f[6] = u * Bz - w * Bx;
-        return F;
-    }
-
-    // HLLD with the reference's own star/double-star construction (M2:372-530)
-    Flux7<T> hlld_x(Prim8<T> L, Prim8<T> R, T Bn) const {
-        L.bx = Bn; R.bx = Bn;
-        Flux7<T> FL = flux_x(L), FR = flux_x(R);
-        T cfL = fast(L, L.bx * L.bx), cfR = fast(R, R.bx * R.bx);
-        T SL = vmin(L.u - cfL, R.u - cfR);
-        T SR = vmax(L.u + cfL, R.u + cfR);
-        if (T(0.0) <= SL) return FL;
-        if (T(0.0) >= SR) return FR;
-
-        std::array<T, 7> UL = {L.r, L.r * L.u, L.r * L.v, L.r * L.w, energy(L), L.by, L.bz};
-        std::array<T, 7> UR = {R.r, R.r * R.u, R.r * R.v, R.r * R.w, energy(R), R.by, R.bz};
-        T ptL = L.P + T(0.5) * (L.bx * L.bx + L.by * L.by + L.bz * L.bz);
-        T ptR = R.P + T(0.5) * (R.bx * R.bx + R.by * R.by + R.bz * R.bz);
-
-        T den = L.r * (SL - L.u) - R.r * (SR - R.u);
-        T SM = T(0.0);
-        if (std::abs(den) > T(1e-14)) SM = (ptR - ptL + L.r * L.u * (SL - L.u) - R.r * R.u * (SR - R.u)) / den;
-
-        T rLs = L.r * (SL - L.u) / (SL - SM);
-        T rRs = R.r * (SR - R.u) / (SR - SM);
-        T pts = ptL + L.r * (SL - L.u) * (SM - L.u);
-        T sL = SL - L.u, sR = SR - R.u;
-        T dL = L.r * sL * (SL - SM) - Bn * Bn;
-        T dR = R.r * sR * (SR - SM) - Bn * Bn;
-
-        T ByLs = L.by, BzLs = L.bz, ByRs = R.by, BzRs = R.bz;
-        T vLs = L.v, wLs = L.w, vRs = R.v, wRs = R.w;
-        if (std::abs(dL) > T(1e-14)) {
-            ByLs = L.by * (L.r * sL * (SL - L.u) - Bn * Bn) / dL;
-            BzLs = L.bz * (L.r * sL * (SL - L.u) - Bn * Bn) / dL;
-            vLs = L.v - Bn * (ByLs - L.by) / (L.r * (SL - L.u) * (SL - SM));
-            wLs = L.w - Bn * (BzLs - L.bz) / (L.r * (SL - L.u) * (SL - SM));
-        }
-        if (std::abs(dR) > T(1e-14)) {
-            ByRs = R.by * (R.r * sR * (SR - R.u) - Bn * Bn) / dR;
-            BzRs = R.bz * (R.r * sR * (SR - R.u) - Bn * Bn) / dR;
-            vRs = R.v - Bn * (ByRs - R.by) / (R.r * (SR - R.u) * (SR - SM));
-            wRs = R.w - Bn * (BzRs - R.bz) / (R.r * (SR - R.u) * (SR - SM));
-        }
-        T sqL = std::sqrt(vmax(rLs, T(1e-300)));
-        T sqR = std::sqrt(vmax(rRs, T(1e-300)));
-        T SLL = SM - std::abs(Bn) / sqL;
-        T SRR = SM + std::abs(Bn) / sqR;
-
-        if (std::abs(Bn) < T(1e-12)) {  // HLL fallback (M2:449-467)
-            T inv = T(1.0) / (SR - SL);
-            Flux7<T> F;
-            for (int k = 0; k < 7; k++) F.f[k] = (SR * FL.f[k] - SL * FR.f[k] + SL * SR * (UR[k] - UL[k])) * inv;
-            return F;
-        }
-        T sgn = (Bn >= T(0.0)) ? T(1.0) : T(-1.0);
-        T d2 = sqL + sqR;
-        T vss = (sqL * vLs + sqR * vRs + (ByRs - ByLs) * sgn) / d2;
-        T wss = (sqL * wLs + sqR * wRs + (BzRs - BzLs) * sgn) / d2;
-        T Byss = (sqL * ByRs + sqR * ByLs + sqL * sqR * (vRs - vLs) * sgn) / d2;
-        T Bzss = (sqL * BzRs + sqR * BzLs + sqL * sqR * (wRs - wLs) * sgn) / d2;
-
-        // star state relative to the outer state W (M2:486-505)
-        auto ustar = [&](const Prim8<T>& W, T S, T rs, T vs, T ws, T Bys, T Bzs) {
-            T EW = energy(W);
-            T vBs = SM * Bn + vs * Bys + ws * Bzs;
-            T vBw = W.u * W.bx + W.v * W.by + W.w * W.bz;
-            T ptW = W.P + T(0.5) * (W.bx * W.bx + W.by * W.by + W.bz * W.bz);
-            T E = ((S - W.u) * EW - (ptW * W.u - Bn * vBw) + (pts * SM - Bn * vBs)) / (S - SM);
-            return std::array<T, 7>{rs, rs * SM, rs * vs, rs * ws, E, Bys, Bzs};
-        };
-        auto jump = [&](const std::array<T, 7>& Us, const std::array<T, 7>& U0, const Flux7<T>& F0, T S) {
-            Flux7<T> F;
-            for (int k = 0; k < 7; k++) F.f[k] = F0.f[k] + S * (Us[k] - U0[k]);
-            return F;
-        };
-        if (T(0.0) < SLL) return jump(ustar(L, SL, rLs, vLs, wLs, ByLs, BzLs), UL, FL, SL);
-        if (T(0.0) < SM) return jump(ustar(L, SL, rLs, vss, wss, Byss, Bzss), UL, FL, SL);
-        if (T(0.0) < SRR) return jump(ustar(R, SR, rRs, vss, wss, Byss, Bzss), UR, FR, SR);
-        return jump(ustar(R, SR, rRs, vRs, wRs, ByRs, BzRs), UR, FR, SR);
-    }
+    // x-normal ideal flux (M2:351-370) and HLLD (M2:372-530)
+    Flux7<T> flux_x(const Prim8<T>& W) const { return ideal_flux_x(*this, W); }
+    Flux7<T> hlld_x(Prim8<T> L, Prim8<T> R, T Bn) const { return hlld_x_generic(*this, L, R, Bn); }
 
     // y-normal HLLD by the (u,v)/(Bx,By) swap (M2:540-561); output
     // f[1]=flux of mx, f[2]=flux of my, f[5]=flux of Bx, f[6]=flux of Bz

@@ -50,6 +50,14 @@ def oracle() -> C.CDLL:
         O.or_mhd2d_divB_max.argtypes = [P2, _PP]
         O.or_mhd2d_divB_max.restype = C.c_double
         O.or_fft1d.argtypes = [C.c_int, _DP, C.c_int]
+        P3 = C.POINTER(L.CcMhd3dParams)
+        O.or_mhd3d_advance_stage.argtypes = [P3, _PP, _PP, C.c_double]
+        O.or_mhd3d_rk2_step.argtypes = [P3, _PP, C.c_double]
+        O.or_mhd3d_compute_dt.argtypes = [P3, _PP]
+        O.or_mhd3d_compute_dt.restype = C.c_double
+        O.or_mhd3d_main_loop.argtypes = [P3, _PP, C.c_int, _DP, C.c_int]
+        O.or_mhd3d_divB_max.argtypes = [P3, _PP]
+        O.or_mhd3d_divB_max.restype = C.c_double
         O.or_poisson_generic.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, C.c_double, C.c_double, C.c_double,
                                          C.c_double, C.c_int, C.c_double, C.c_int, C.c_double, C.c_int, _DP, _DP,
                                          _DP, C.POINTER(C.c_int), _DP]
@@ -74,6 +82,15 @@ def ref(name: str) -> C.CDLL | None:
             R.ref_mhd2d_main_loop.argtypes = [P2, _PP, C.c_int, _DP]
             R.ref_mhd2d_divB_max.argtypes = [P2, _PP]
             R.ref_mhd2d_divB_max.restype = C.c_double
+        if R is not None and name == "mhd3d":
+            P3 = C.POINTER(L.CcMhd3dParams)
+            R.ref_mhd3d_rk2_step.argtypes = [P3, _PP, C.c_double]
+            R.ref_mhd3d_advance_stage.argtypes = [P3, _PP, _PP, C.c_double]
+            R.ref_mhd3d_compute_dt.argtypes = [P3, _PP]
+            R.ref_mhd3d_compute_dt.restype = C.c_double
+            R.ref_mhd3d_main_loop.argtypes = [P3, _PP, C.c_int, _DP]
+            R.ref_mhd3d_divB_max.argtypes = [P3, _PP]
+            R.ref_mhd3d_divB_max.restype = C.c_double
         if R is not None and name == "euler2d":
             P2 = C.POINTER(L.CcEuler2dParams)
             R.ref_euler2d_rk2_step.argtypes = [P2, _PP, C.c_double]
@@ -165,3 +182,24 @@ def rel_linf(a: np.ndarray, b: np.ndarray) -> float:
     if den == 0.0:
         return num
     return num / den
+
+
+# ---- 3D state helpers: [rho, mx, my, mz, E, Bx_f, By_f, Bz_f] ----
+
+def m3_rk2_ref(cp, S, dt):
+    out = copy_state(S)
+    ref("mhd3d").ref_mhd3d_rk2_step(C.byref(cp), pp(out), dt)
+    return out
+
+
+def m3_rk2_oracle(cp, S, dt):
+    out = copy_state(S)
+    oracle().or_mhd3d_rk2_step(C.byref(cp), pp(out), dt)
+    return out
+
+
+def m3_main_loop_oracle(cp, S, nsteps, fp32=False, t0=0.0):
+    out = copy_state(S)
+    t = C.c_double(t0)
+    oracle().or_mhd3d_main_loop(C.byref(cp), pp(out), nsteps, C.byref(t), 1 if fp32 else 0)
+    return out, t.value
