@@ -347,6 +347,8 @@ def run_ours(args) -> None:
         "clocks": clk,
         "max_divB_fp32": d32["max_divB"],
     }
+    if world == 1 and not args.skip_3d:
+        line["mhd3d"] = run_3d(args, stream)
     if world == 1 and rank == 0 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(args.cpu_sample_grid, args.cpu_steps)
     if rank == 0:
@@ -354,6 +356,44 @@ def run_ours(args) -> None:
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
+
+
+def run_3d(args, stream) -> dict:
+    """3D resistive HLLD+CT workload: 256^3 periodic unit cube, ideal gas
+    gamma 5/3 (hybrid EOS with K1 = Kbounce = 0), eta 5e-4, rho 1, p 1/gamma,
+    random-phase v and A with 1 <= |k| <= 4 (seed 1), rms v 0.5, rms B 0.3."""
+    import torch
+
+    from core_collapse_b200.mhd3d import Mhd3dSolver, Params3, ic_turbulence3d
+    n = args.grid3d
+    steps = max(1, min(args.steps, args.steps3d))
+    s0 = ic_turbulence3d(Params3.ideal_gas(Nx=n, Ny=n, Nz=n), seed=1)
+    out = {"workload": f"3D resistive MHD HLLD+CT, {n}^3 periodic, random-phase v and A (|k| in [1,4], seed 1), "
+                       f"rms v 0.5, rms B 0.3, eta 5e-4, CFL 0.4", "steps": steps, "warmup": args.warmup}
+    for prec in ("fp32", "fp64"):
+        p = Params3.ideal_gas(Nx=n, Ny=n, Nz=n, eta=5e-4, cfl=0.4, precision=prec, t_end=1e30)
+        with Mhd3dSolver(p) as g:
+            g.set_stream(stream.cuda_stream)
+            g.upload(s0)
+            d0 = g.diagnostics()
+            g.advance(args.warmup, 0.0)
+            g.set_profiling(True)
+            g.reset_perf()
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            g.advance(steps)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            ms = e0.elapsed_time(e1)
+            pf = g.perf()
+            d1 = g.diagnostics()
+        out[prec] = {"value": n ** 3 * steps / (ms / 1000.0), "unit": UNIT, "ms_per_step": ms / steps,
+                     "stage_ms": pf["stage_ms"] / max(1, pf["stage_launches"]),
+                     "max_divB_end": d1["max_divB"], "energy_drift_rel": (d1["energy"] - d0["energy"]) / d0["energy"],
+                     "mass_drift_rel": (d1["mass"] - d0["mass"]) / d0["mass"]}
+    out["fp32_over_fp64"] = out["fp32"]["value"] / out["fp64"]["value"]
+    return out
 
 
 def main():
@@ -367,6 +407,9 @@ def main():
     ap.add_argument("--cpu-sample-grid", type=int, default=512)
     ap.add_argument("--cpu-steps", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--skip-3d", action="store_true")
+    ap.add_argument("--grid3d", type=int, default=256)
+    ap.add_argument("--steps3d", type=int, default=20)
     args = ap.parse_args()
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")

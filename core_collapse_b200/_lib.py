@@ -118,6 +118,14 @@ SIGNATURES = {
     "cc_mhd2d_diagnostics": (C.c_int, [_H, C.POINTER(CcDiag)]),
     "cc_mhd2d_gravity_fft_noalloc": (C.c_int, [C.POINTER(CcMhd2dParams), C.c_void_p, C.c_void_p, C.c_void_p,
                                                C.c_void_p]),
+    "cc_mhd3d_params_default": (None, [C.POINTER(CcMhd3dParams)]),
+    "cc_mhd3d_create": (C.c_int, [C.POINTER(CcMhd3dParams), C.POINTER(_H)]),
+    "cc_mhd3d_upload": (C.c_int, [_H] + [_DP] * 8),
+    "cc_mhd3d_download": (C.c_int, [_H] + [_DP] * 8),
+    "cc_mhd3d_compute_dt": (C.c_int, [_H, _DP]),
+    "cc_mhd3d_rk2_step": (C.c_int, [_H, C.c_double]),
+    "cc_mhd3d_advance": (C.c_int, [_H, C.c_int, _DP]),
+    "cc_mhd3d_diagnostics": (C.c_int, [_H, C.POINTER(CcDiag)]),
     "cc_mhd2d_ic_knobs_default": (None, [C.POINTER(CcIcKnobs)]),
     "cc_ic_mhd2d_reference": (C.c_int, [C.POINTER(CcMhd2dParams), C.POINTER(CcIcKnobs), C.POINTER(_DP)]),
     "cc_ic_mhd2d_collapse": (C.c_int, [C.POINTER(CcMhd2dParams), C.c_double, C.c_double, C.c_double, C.c_uint32,

@@ -19,57 +19,11 @@
 
 #include "../../include/cc_step.h"
 #include "mhd2d_launch.h"
-
-namespace ccb {
-cudaError_t launch_set_scalar(double* p, double v, cudaStream_t s);
-}
+#include "handle.h"
 
 using namespace ccb;
 
-struct cc_handle {
-    int kind = 0;
-    int device = 0;
-    std::string err;
-    cudaStream_t own = nullptr;
-    cudaStream_t stream = nullptr;
-    cc_perf perf{};
-    bool profiling = false;
-    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> timed;  // event pairs around stage launches
-    virtual ~cc_handle() {
-        for (auto& e : timed) { cudaEventDestroy(e.first); cudaEventDestroy(e.second); }
-        if (own) cudaStreamDestroy(own);
-    }
-    // fold the recorded event pairs into perf.stage_ms (stream must be idle)
-    cudaError_t collect() {
-        for (auto& e : timed) {
-            float ms = 0.f;
-            cudaError_t r = cudaEventElapsedTime(&ms, e.first, e.second);
-            if (r != cudaSuccess) return r;
-            perf.stage_ms += ms;
-            perf.stage_launches += 1;
-            cudaEventDestroy(e.first);
-            cudaEventDestroy(e.second);
-        }
-        timed.clear();
-        return cudaSuccess;
-    }
-};
-
 namespace {
-
-constexpr int KIND_MHD2D = 1;
-
-int fail(cc_handle* h, int code, const std::string& msg) {
-    if (h) h->err = msg;
-    return code;
-}
-
-#define CC_CUDA(call)                                                                          \
-    do {                                                                                       \
-        cudaError_t e_ = (call);                                                               \
-        if (e_ != cudaSuccess)                                                                 \
-            return fail(this_handle(), CC_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
-    } while (0)
 
 bool is_pow2(int n) { return n > 0 && (n & (n - 1)) == 0; }
 int ilog2(int n) { int l = 0; while ((1 << l) < n) ++l; return l; }
@@ -558,12 +512,6 @@ struct Mhd2dHandle : cc_handle {
 Mhd2dBase* m2(cc_handle* h) {
     if (!h || h->kind != KIND_MHD2D) return nullptr;
     return static_cast<Mhd2dHandle*>(h)->impl.get();
-}
-
-int set_dev(cc_handle* h) {
-    cudaError_t e = cudaSetDevice(h->device);
-    if (e != cudaSuccess) return fail(h, CC_ERR_CUDA, std::string("cudaSetDevice: ") + cudaGetErrorString(e));
-    return CC_OK;
 }
 
 }  // namespace

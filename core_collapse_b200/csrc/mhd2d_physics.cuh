@@ -75,14 +75,15 @@ __device__ __forceinline__ T fast_speed(const M2Const<T>& c, const Prim<T>& W, T
     return sqrt(vmax(T(0.0), cf2));
 }
 
-// x-normal ideal flux (M2:351-370)
-template <class T>
-__device__ __forceinline__ Flux<T> ideal_flux(const M2Const<T>& c, const Prim<T>& W) {
+// x-normal ideal flux (M2:351-370; M3:396-413 with the hybrid-EOS energy).
+// Cst is the solver's constant block: energy(c, W) and fast_speed(c, W, bn)
+// are overloaded on it.
+template <class T, class Cst>
+__device__ __forceinline__ Flux<T> ideal_flux(const Cst& c, const Prim<T>& W) {
     T rho = W.r, u = W.u, v = W.v, w = W.w, P = W.P, Bx = W.bx, By = W.by, Bz = W.bz;
-    T v2 = u * u + v * v + w * w;
     T B2 = Bx * Bx + By * By + Bz * Bz;
     T pt = P + T(0.5) * B2;
-    T E = P / c.gm1 + T(0.5) * rho * v2 + T(0.5) * B2;
+    T E = energy(c, W);
     T vdotB = u * Bx + v * By + w * Bz;
     Flux<T> F;
     F.f0 = rho * u;
@@ -98,8 +99,8 @@ __device__ __forceinline__ Flux<T> ideal_flux(const M2Const<T>& c, const Prim<T>
 // HLLD (M2:372-530), the reference's own star / double-star construction:
 // degenerate guards at 1e-14, HLL fallback for |Bn| < 1e-12, double-star
 // fluxes jumped from the outer state with the outer speed.
-template <class T>
-__device__ __forceinline__ Flux<T> hlld_x(const M2Const<T>& c, Prim<T> L, Prim<T> R, T Bn) {
+template <class T, class Cst>
+__device__ __forceinline__ Flux<T> hlld_x(const Cst& c, Prim<T> L, Prim<T> R, T Bn) {
     L.bx = Bn; R.bx = Bn;
     const T cfL = fast_speed(c, L, Bn), cfR = fast_speed(c, R, Bn);
     const T SL = vmin(L.u - cfL, R.u - cfR);
@@ -197,13 +198,26 @@ __device__ __forceinline__ Flux<T> hlld_x(const M2Const<T>& c, Prim<T> L, Prim<T
 
 // y-normal HLLD through the (u,v)/(Bx,By) swap (M2:540-561).  Returns
 // f1 = flux of mx, f2 = flux of my, f5 = flux of Bx (= Ez at the y face), f6 = flux of Bz.
-template <class T>
-__device__ __forceinline__ Flux<T> hlld_y(const M2Const<T>& c, const Prim<T>& L, const Prim<T>& R, T Bn) {
+template <class T, class Cst>
+__device__ __forceinline__ Flux<T> hlld_y(const Cst& c, const Prim<T>& L, const Prim<T>& R, T Bn) {
     Prim<T> aL, aR;
     aL.r = L.r; aL.u = L.v; aL.v = L.u; aL.w = L.w; aL.P = L.P; aL.bx = Bn; aL.by = L.bx; aL.bz = L.bz;
     aR.r = R.r; aR.u = R.v; aR.v = R.u; aR.w = R.w; aR.P = R.P; aR.bx = Bn; aR.by = R.bx; aR.bz = R.bz;
     Flux<T> F = hlld_x(c, aL, aR, Bn);
     const T t = F.f1; F.f1 = F.f2; F.f2 = t;
+    return F;
+}
+
+// z-normal HLLD through the cyclic (w,u,v)/(Bz,Bx,By) map (M3:604-622).
+// Returns f1 = F(mx), f2 = F(my), f3 = F(mz), f5 = F(Bx), f6 = F(By).
+template <class T, class Cst>
+__device__ __forceinline__ Flux<T> hlld_z(const Cst& c, const Prim<T>& L, const Prim<T>& R, T Bn) {
+    Prim<T> aL, aR;
+    aL.r = L.r; aL.u = L.w; aL.v = L.u; aL.w = L.v; aL.P = L.P; aL.bx = Bn; aL.by = L.bx; aL.bz = L.by;
+    aR.r = R.r; aR.u = R.w; aR.v = R.u; aR.w = R.v; aR.P = R.P; aR.bx = Bn; aR.by = R.bx; aR.bz = R.by;
+    Flux<T> F = hlld_x(c, aL, aR, Bn);
+    const T fmx = F.f2, fmy = F.f3, fmz = F.f1;
+    F.f1 = fmx; F.f2 = fmy; F.f3 = fmz;
     return F;
 }
 

@@ -1,0 +1,91 @@
+// Definitions of M3Launch<T>; included once per precision TU.
+#pragma once
+#include "mhd3d_launch.h"
+
+namespace ccb {
+
+namespace {
+inline int grid3(long long n) {
+    long long g = (n + 255) / 256;
+    if (g < 1) g = 1;
+    if (g > 148LL * 16) g = 148LL * 16;
+    return (int)g;
+}
+}  // namespace
+
+template <class T>
+cudaError_t M3Launch<T>::prim(const M3Const<T>& c, const Fields3<T>& s, const PrimData<T>& pr, bool defer,
+                              const double* dt, const int* active, cudaStream_t st) {
+    const int g = grid3((long long)c.nx * c.ny * c.nz);
+    if (defer) m3_prim_kernel<T, true><<<g, 256, 0, st>>>(c, s, pr, dt, active);
+    else m3_prim_kernel<T, false><<<g, 256, 0, st>>>(c, s, pr, dt, active);
+    return cudaGetLastError();
+}
+
+template <class T>
+cudaError_t M3Launch<T>::faces(const M3Const<T>& c, const Fields3<T>& s, const PrimData<T>& pr, const FaceData<T>& X,
+                               const FaceData<T>& Y, const FaceData<T>& Z, const int* active, cudaStream_t st) {
+    m3_face_kernel<T, 0><<<grid3((long long)(c.nx + 1) * c.ny * c.nz), 256, 0, st>>>(c, s, pr, X, active);
+    m3_face_kernel<T, 1><<<grid3((long long)c.nx * (c.ny + 1) * c.nz), 256, 0, st>>>(c, s, pr, Y, active);
+    m3_face_kernel<T, 2><<<grid3((long long)c.nx * c.ny * (c.nz + 1)), 256, 0, st>>>(c, s, pr, Z, active);
+    return cudaGetLastError();
+}
+
+template <class T>
+cudaError_t M3Launch<T>::update(const M3Const<T>& c, const Fields3<T>& in, const Fields3<T>& out, const FaceData<T>& X,
+                                const FaceData<T>& Y, const FaceData<T>& Z, const double* dt, const int* active,
+                                cudaStream_t st) {
+    m3_update_kernel<T><<<grid3((long long)c.nx * c.ny * c.nz), 256, 0, st>>>(c, in, out, X, Y, Z, dt, active);
+    return cudaGetLastError();
+}
+
+template <class T>
+cudaError_t M3Launch<T>::edges(const M3Const<T>& c, const Fields3<T>& in, const FaceData<T>& X, const FaceData<T>& Y,
+                               const FaceData<T>& Z, T* Ex, T* Ey, T* Ez, const int* active, cudaStream_t st) {
+    m3_edge_kernel<T><<<grid3((long long)(c.nx + 1) * (c.ny + 1) * (c.nz + 1)), 256, 0, st>>>(c, in, X, Y, Z, Ex, Ey,
+                                                                                               Ez, active);
+    return cudaGetLastError();
+}
+
+template <class T>
+cudaError_t M3Launch<T>::ct(const M3Const<T>& c, const Fields3<T>& in, const Fields3<T>& out, const T* Ex, const T* Ey,
+                            const T* Ez, const double* dt, const int* active, cudaStream_t st) {
+    m3_ct_kernel<T><<<grid3((long long)(c.nx + 1) * (c.ny + 1) * (c.nz + 1)), 256, 0, st>>>(c, in, out, Ex, Ey, Ez,
+                                                                                             dt, active);
+    return cudaGetLastError();
+}
+
+template <class T>
+cudaError_t M3Launch<T>::average(const M3Const<T>& c, const Fields3<T>& un, const Fields3<T>& s2, const Fields3<T>& out,
+                                 const double* dt, const int* active, double* spd_part, double* rho_part,
+                                 cudaStream_t st) {
+    m3_average_kernel<T, RED_NT><<<RED_BLOCKS, RED_NT, 0, st>>>(c, un, s2, out, dt, active, spd_part, rho_part);
+    return cudaGetLastError();
+}
+
+template <class T>
+cudaError_t M3Launch<T>::speeds(const M3Const<T>& c, const Fields3<T>& s, double* spd_part, cudaStream_t st) {
+    m3_speed_kernel<T, RED_NT><<<RED_BLOCKS, RED_NT, 0, st>>>(c, s, spd_part);
+    return cudaGetLastError();
+}
+
+template <class T>
+cudaError_t M3Launch<T>::diag(const M3Const<T>& c, const Fields3<T>& s, double* part, cudaStream_t st) {
+    m3_diag_kernel<T, RED_NT><<<RED_BLOCKS, RED_NT, 0, st>>>(c, s, part);
+    return cudaGetLastError();
+}
+
+template <class T>
+cudaError_t M3Launch<T>::pack_in(const double* src, T* dst, int w, int h, int d, int P, long long PS, cudaStream_t st) {
+    pack3_in_kernel<T><<<grid3((long long)w * h * d), 256, 0, st>>>(src, dst, w, h, d, P, PS);
+    return cudaGetLastError();
+}
+
+template <class T>
+cudaError_t M3Launch<T>::pack_out(const T* src, double* dst, int w, int h, int d, int P, long long PS,
+                                  cudaStream_t st) {
+    pack3_out_kernel<T><<<grid3((long long)w * h * d), 256, 0, st>>>(src, dst, w, h, d, P, PS);
+    return cudaGetLastError();
+}
+
+}  // namespace ccb

@@ -1,0 +1,408 @@
+// 3D resistive-MHD step kernels (mhd3d_resistive_hlld_ct.cpp, cited M3:<line>),
+// templated on T; instantiated per precision in mhd3d_f64.cu / mhd3d_f32.cu.
+//
+// Layout: every field is a pitched 3D array, element (i,j,k) at
+// k*PS + j*P + i with P = round_up(Nx+1, 32), PS = P*(Ny+1) and Nz+1 planes, so
+// cells, the three face arrays (index N along their own axis), the edge
+// arrays and the face-flux arrays all share one indexing.
+//
+// One RK stage (advance_stage, M3:694-1030) is a short pipeline of kernels
+// addressed by actual cell / face / edge indices with the reference's own wrap
+// rules (cells mod N or clamp; faces mod N+1 or clamp; cell-centred B formed
+// from unwrapped indices through the face lookups, as M3:280-296 do):
+//   m3_prim_kernel    primitives of every cell (stage 2: first the deferred
+//                     Joule heating + floors of stage 1, in place)
+//   m3_face_kernel    MUSCL-MC face states + HLLD for x, y or z faces;
+//                     5 flux components and the two face EMFs per face
+//   m3_update_kernel  FV update + floors with the stage-input B
+//   m3_edge_kernel    edge EMFs: average of four face EMFs + eta J (cell-centred B)
+//   m3_ct_kernel      CT update of the three face arrays
+// The Joule sub-step (M3:1017) needs the post-CT faces of neighbouring cells,
+// so it is applied by the next kernel that reads the stage output (the stage-2
+// prim kernel, the RK average).  It changes only E of its own cell, so doing it
+// in place is race-free.
+#pragma once
+#include "mhd3d_physics.cuh"
+
+namespace ccb {
+
+template <class T> struct Fields3 {
+    T* rho; T* mx; T* my; T* mz; T* E; T* bx; T* by; T* bz;
+};
+
+// per-direction face data: 5 flux components + 2 face EMFs, each a full plane set
+template <class T> struct FaceData {
+    T* f[7];
+};
+
+// ---- face and cell-centred B with the reference's index rules (M3:250-296) ----
+template <class T>
+__device__ __forceinline__ T bxf3(const M3Const<T>& c, const T* bx, int i, int j, int k) {
+    return bx[c.idx(c.ax.face(i), c.ay.cell(j), c.az.cell(k))];
+}
+template <class T>
+__device__ __forceinline__ T byf3(const M3Const<T>& c, const T* by, int i, int j, int k) {
+    return by[c.idx(c.ax.cell(i), c.ay.face(j), c.az.cell(k))];
+}
+template <class T>
+__device__ __forceinline__ T bzf3(const M3Const<T>& c, const T* bz, int i, int j, int k) {
+    return bz[c.idx(c.ax.cell(i), c.ay.cell(j), c.az.face(k))];
+}
+template <class T>
+__device__ __forceinline__ T bx_cc3(const M3Const<T>& c, const T* bx, int i, int j, int k) {
+    return T(0.5) * (bxf3(c, bx, i, j, k) + bxf3(c, bx, i + 1, j, k));
+}
+template <class T>
+__device__ __forceinline__ T by_cc3(const M3Const<T>& c, const T* by, int i, int j, int k) {
+    return T(0.5) * (byf3(c, by, i, j, k) + byf3(c, by, i, j + 1, k));
+}
+template <class T>
+__device__ __forceinline__ T bz_cc3(const M3Const<T>& c, const T* bz, int i, int j, int k) {
+    return T(0.5) * (bzf3(c, bz, i, j, k) + bzf3(c, bz, i, j, k + 1));
+}
+
+// Joule heating E += dt eta |J|^2 of cell (i,j,k) (add_joule_heating, M3:652-692)
+template <class T>
+__device__ __forceinline__ T joule3(const M3Const<T>& c, const Fields3<T>& s, int i, int j, int k, T dt) {
+    const T dBzdy = (bz_cc3(c, s.bz, i, j + 1, k) - bz_cc3(c, s.bz, i, j - 1, k)) / c.two_dy;
+    const T dBydz = (by_cc3(c, s.by, i, j, k + 1) - by_cc3(c, s.by, i, j, k - 1)) / c.two_dz;
+    const T dBxdz = (bx_cc3(c, s.bx, i, j, k + 1) - bx_cc3(c, s.bx, i, j, k - 1)) / c.two_dz;
+    const T dBzdx = (bz_cc3(c, s.bz, i + 1, j, k) - bz_cc3(c, s.bz, i - 1, j, k)) / c.two_dx;
+    const T dBydx = (by_cc3(c, s.by, i + 1, j, k) - by_cc3(c, s.by, i - 1, j, k)) / c.two_dx;
+    const T dBxdy = (bx_cc3(c, s.bx, i, j + 1, k) - bx_cc3(c, s.bx, i, j - 1, k)) / c.two_dy;
+    const T Jx = dBzdy - dBydz, Jy = dBxdz - dBzdx, Jz = dBydx - dBxdy;
+    const T J2 = Jx * Jx + Jy * Jy + Jz * Jz;
+    return dt * c.eta * J2;
+}
+
+// grid-stride helper over an (nx, ny, nz) box
+#define CC_FOR3(nx_, ny_, nz_)                                                                          \
+    const long long n3_ = (long long)(nx_) * (ny_) * (nz_);                                             \
+    for (long long t_ = (long long)blockIdx.x * blockDim.x + threadIdx.x; t_ < n3_;                     \
+         t_ += (long long)gridDim.x * blockDim.x)
+
+// ---------------------------------------------------------------------------
+// primitives: 8 planes (rho, u, v, w, P, Bx, By, Bz)
+template <class T> struct PrimData {
+    T* w[8];
+};
+
+template <class T, bool DEFER>
+__global__ void __launch_bounds__(256) m3_prim_kernel(const M3Const<T> c, const Fields3<T> s, const PrimData<T> pr,
+                                                       const double* __restrict__ dtp, const int* __restrict__ active) {
+    if (active && *active == 0) return;
+    const T dt = (T)(*dtp);
+    CC_FOR3(c.nx, c.ny, c.nz) {
+        const int i = (int)(t_ % c.nx), j = (int)((t_ / c.nx) % c.ny), k = (int)(t_ / ((long long)c.nx * c.ny));
+        const size_t q = c.idx(i, j, k);
+        T rho = s.rho[q], mx = s.mx[q], my = s.my[q], mz = s.mz[q], E = s.E[q];
+        const T Bx = bx_cc3(c, s.bx, i, j, k), By = by_cc3(c, s.by, i, j, k), Bz = bz_cc3(c, s.bz, i, j, k);
+        if (DEFER) {
+            if (c.resistive) E += joule3(c, s, i, j, k, dt);
+            floors(c, rho, mx, my, mz, E, Bx, By, Bz);  // M3:1019-1029
+            s.rho[q] = rho;
+            s.E[q] = E;
+        }
+        const Prim<T> W = to_prim(c, rho, mx, my, mz, E, Bx, By, Bz);
+        pr.w[0][q] = W.r; pr.w[1][q] = W.u; pr.w[2][q] = W.v; pr.w[3][q] = W.w;
+        pr.w[4][q] = W.P; pr.w[5][q] = W.bx; pr.w[6][q] = W.by; pr.w[7][q] = W.bz;
+    }
+}
+
+// MUSCL-MC face state of cell q along (stride) with neighbours qm, qp:
+// side +1 -> state at the cell's upper face, -1 -> lower face (M3:312-382).
+// dir selects which B components are reconstructed (the normal one is not).
+template <class T>
+__device__ __forceinline__ Prim<T> face_state3(const PrimData<T>& pr, size_t qm, size_t q, size_t qp, int dir, T side,
+                                               T floor_rho, T floor_P) {
+    Prim<T> W;
+    const T h = T(0.5) * side;
+    auto rec = [&](int m) { return pr.w[m][q] + h * mc_slope(pr.w[m][qm], pr.w[m][q], pr.w[m][qp]); };
+    W.r = rec(0); W.u = rec(1); W.v = rec(2); W.w = rec(3); W.P = rec(4);
+    W.bx = (dir == 0) ? pr.w[5][q] : rec(5);
+    W.by = (dir == 1) ? pr.w[6][q] : rec(6);
+    W.bz = (dir == 2) ? pr.w[7][q] : rec(7);
+    W.r = vmax(W.r, floor_rho);
+    W.P = vmax(W.P, floor_P);
+    return W;
+}
+
+// Faces of direction DIR (0 x, 1 y, 2 z): HLLD flux and face EMFs
+// (M3:728-800).  Output slots: f[0..4] fluxes of rho, mx, my, mz, E;
+// x: f[5] = Ey_x = F(Bz), f[6] = Ez_x = -F(By)
+// y: f[5] = Ez_y = G(Bx), f[6] = Ex_y = -G(Bz)
+// z: f[5] = Ex_z = H(By), f[6] = Ey_z = -H(Bx)
+template <class T, int DIR>
+__global__ void __launch_bounds__(256) m3_face_kernel(const M3Const<T> c, const Fields3<T> s, const PrimData<T> pr,
+                                                      const FaceData<T> out, const int* __restrict__ active) {
+    if (active && *active == 0) return;
+    const int fx = c.nx + (DIR == 0), fy = c.ny + (DIR == 1), fz = c.nz + (DIR == 2);
+    CC_FOR3(fx, fy, fz) {
+        const int i = (int)(t_ % fx), j = (int)((t_ / fx) % fy), k = (int)(t_ / ((long long)fx * fy));
+        int Li = i, Lj = j, Lk = k, Ri = i, Rj = j, Rk = k;
+        if (DIR == 0) { Li = c.ax.cell(i - 1); Ri = c.ax.cell(i); }
+        if (DIR == 1) { Lj = c.ay.cell(j - 1); Rj = c.ay.cell(j); }
+        if (DIR == 2) { Lk = c.az.cell(k - 1); Rk = c.az.cell(k); }
+        // stencil neighbours of each side's cell, wrapped again from the wrapped index
+        auto nb = [&](int a, int b, int d, int o) -> size_t {
+            if (DIR == 0) return c.idx(c.ax.cell(a + o), b, d);
+            if (DIR == 1) return c.idx(a, c.ay.cell(b + o), d);
+            return c.idx(a, b, c.az.cell(d + o));
+        };
+        const Prim<T> WL = face_state3(pr, nb(Li, Lj, Lk, -1), c.idx(Li, Lj, Lk), nb(Li, Lj, Lk, +1), DIR, T(1),
+                                       c.floor_rho, c.floor_P);
+        const Prim<T> WR = face_state3(pr, nb(Ri, Rj, Rk, -1), c.idx(Ri, Rj, Rk), nb(Ri, Rj, Rk, +1), DIR, T(-1),
+                                       c.floor_rho, c.floor_P);
+        const size_t qf = c.idx(i, j, k);
+        Flux<T> F;
+        T e1, e2;
+        if (DIR == 0) {
+            F = hlld_x(c, WL, WR, s.bx[qf]);
+            e1 = F.f6; e2 = -F.f5;
+        } else if (DIR == 1) {
+            F = hlld_y(c, WL, WR, s.by[qf]);
+            e1 = F.f5; e2 = -F.f6;
+        } else {
+            F = hlld_z(c, WL, WR, s.bz[qf]);
+            e1 = F.f6; e2 = -F.f5;
+        }
+        out.f[0][qf] = F.f0; out.f[1][qf] = F.f1; out.f[2][qf] = F.f2; out.f[3][qf] = F.f3; out.f[4][qf] = F.f4;
+        out.f[5][qf] = e1; out.f[6][qf] = e2;
+    }
+}
+
+// FV update + floors with the stage-input B (M3:803-834)
+template <class T>
+__global__ void __launch_bounds__(256) m3_update_kernel(const M3Const<T> c, const Fields3<T> in, const Fields3<T> out,
+                                                        const FaceData<T> X, const FaceData<T> Y, const FaceData<T> Z,
+                                                        const double* __restrict__ dtp, const int* __restrict__ active) {
+    if (active && *active == 0) return;
+    const T dt = (T)(*dtp);
+    CC_FOR3(c.nx, c.ny, c.nz) {
+        const int i = (int)(t_ % c.nx), j = (int)((t_ / c.nx) % c.ny), k = (int)(t_ / ((long long)c.nx * c.ny));
+        const size_t q = c.idx(i, j, k), qx = c.idx(i + 1, j, k), qy = c.idx(i, j + 1, k), qz = c.idx(i, j, k + 1);
+        T d[5];
+#pragma unroll
+        for (int m = 0; m < 5; m++)
+            d[m] = -(X.f[m][qx] - X.f[m][q]) * c.inv_dx - (Y.f[m][qy] - Y.f[m][q]) * c.inv_dy -
+                   (Z.f[m][qz] - Z.f[m][q]) * c.inv_dz;
+        T rho = in.rho[q] + dt * d[0];
+        T mx = in.mx[q] + dt * d[1];
+        T my = in.my[q] + dt * d[2];
+        T mz = in.mz[q] + dt * d[3];
+        T E = in.E[q] + dt * d[4];
+        floors(c, rho, mx, my, mz, E, bx_cc3(c, in.bx, i, j, k), by_cc3(c, in.by, i, j, k), bz_cc3(c, in.bz, i, j, k));
+        out.rho[q] = rho; out.mx[q] = mx; out.my[q] = my; out.mz[q] = mz; out.E[q] = E;
+    }
+}
+
+// Edge EMFs (M3:879-939): Ex at (i, jf, kf), Ey at (if, j, kf), Ez at (if, jf, k)
+template <class T>
+__global__ void __launch_bounds__(256) m3_edge_kernel(const M3Const<T> c, const Fields3<T> in, const FaceData<T> X,
+                                                      const FaceData<T> Y, const FaceData<T> Z, T* __restrict__ Ex,
+                                                      T* __restrict__ Ey, T* __restrict__ Ez,
+                                                      const int* __restrict__ active) {
+    if (active && *active == 0) return;
+    CC_FOR3(c.nx + 1, c.ny + 1, c.nz + 1) {
+        const int i = (int)(t_ % (c.nx + 1)), j = (int)((t_ / (c.nx + 1)) % (c.ny + 1));
+        const int k = (int)(t_ / ((long long)(c.nx + 1) * (c.ny + 1)));
+        const size_t q = c.idx(i, j, k);
+        // x-face EMF planes: X.f[5] = Ey_x, X.f[6] = Ez_x; y: Y.f[5] = Ez_y, Y.f[6] = Ex_y; z: Z.f[5] = Ex_z, Z.f[6] = Ey_z
+        auto exy = [&](int a, int b, int d) { return Y.f[6][c.idx(c.ax.cell(a), c.ay.face(b), c.az.cell(d))]; };
+        auto exz = [&](int a, int b, int d) { return Z.f[5][c.idx(c.ax.cell(a), c.ay.cell(b), c.az.face(d))]; };
+        auto eyx = [&](int a, int b, int d) { return X.f[5][c.idx(c.ax.face(a), c.ay.cell(b), c.az.cell(d))]; };
+        auto eyz = [&](int a, int b, int d) { return Z.f[6][c.idx(c.ax.cell(a), c.ay.cell(b), c.az.face(d))]; };
+        auto ezx = [&](int a, int b, int d) { return X.f[6][c.idx(c.ax.face(a), c.ay.cell(b), c.az.cell(d))]; };
+        auto ezy = [&](int a, int b, int d) { return Y.f[5][c.idx(c.ax.cell(a), c.ay.face(b), c.az.cell(d))]; };
+        if (i < c.nx) {  // Ex
+            const T ideal = T(0.25) * (exy(i, j, k - 1) + exy(i, j, k) + exz(i, j - 1, k) + exz(i, j, k));
+            T res = T(0.0);
+            if (c.resistive) {
+                const T dBzdy = (bz_cc3(c, in.bz, i, j, k) - bz_cc3(c, in.bz, i, j - 1, k)) / c.dy;
+                const T dBydz = (by_cc3(c, in.by, i, j, k) - by_cc3(c, in.by, i, j, k - 1)) / c.dz;
+                res = c.eta * (dBzdy - dBydz);
+            }
+            Ex[q] = ideal + res;
+        }
+        if (j < c.ny) {  // Ey
+            const T ideal = T(0.25) * (eyx(i, j, k - 1) + eyx(i, j, k) + eyz(i - 1, j, k) + eyz(i, j, k));
+            T res = T(0.0);
+            if (c.resistive) {
+                const T dBxdz = (bx_cc3(c, in.bx, i, j, k) - bx_cc3(c, in.bx, i, j, k - 1)) / c.dz;
+                const T dBzdx = (bz_cc3(c, in.bz, i, j, k) - bz_cc3(c, in.bz, i - 1, j, k)) / c.dx;
+                res = c.eta * (dBxdz - dBzdx);
+            }
+            Ey[q] = ideal + res;
+        }
+        if (k < c.nz) {  // Ez
+            const T ideal = T(0.25) * (ezx(i, j - 1, k) + ezx(i, j, k) + ezy(i - 1, j, k) + ezy(i, j, k));
+            T res = T(0.0);
+            if (c.resistive) {
+                const T dBydx = (by_cc3(c, in.by, i, j, k) - by_cc3(c, in.by, i - 1, j, k)) / c.dx;
+                const T dBxdy = (bx_cc3(c, in.bx, i, j, k) - bx_cc3(c, in.bx, i, j - 1, k)) / c.dy;
+                res = c.eta * (dBydx - dBxdy);
+            }
+            Ez[q] = ideal + res;
+        }
+    }
+}
+
+// CT update of the three face arrays (M3:942-1015)
+template <class T>
+__global__ void __launch_bounds__(256) m3_ct_kernel(const M3Const<T> c, const Fields3<T> in, const Fields3<T> out,
+                                                    const T* __restrict__ Ex, const T* __restrict__ Ey,
+                                                    const T* __restrict__ Ez, const double* __restrict__ dtp,
+                                                    const int* __restrict__ active) {
+    if (active && *active == 0) return;
+    const T dt = (T)(*dtp);
+    const T dtdx = dt / c.dx, dtdy = dt / c.dy, dtdz = dt / c.dz;
+    CC_FOR3(c.nx + 1, c.ny + 1, c.nz + 1) {
+        const int i = (int)(t_ % (c.nx + 1)), j = (int)((t_ / (c.nx + 1)) % (c.ny + 1));
+        const int k = (int)(t_ / ((long long)(c.nx + 1) * (c.ny + 1)));
+        const size_t q = c.idx(i, j, k);
+        if (j < c.ny && k < c.nz) {  // Bx face (i, j, k)
+            const T ezU = Ez[c.idx(i, j + 1, k)], ezD = Ez[q];
+            const T eyF = Ey[c.idx(i, j, k + 1)], eyB = Ey[q];
+            out.bx[q] = in.bx[q] + (-(dtdy) * (ezU - ezD) + (dtdz) * (eyF - eyB));
+        }
+        if (i < c.nx && k < c.nz) {  // By face (i, j, k)
+            const T ezR = Ez[c.idx(i + 1, j, k)], ezL = Ez[q];
+            const T exF = Ex[c.idx(i, j, k + 1)], exB = Ex[q];
+            out.by[q] = in.by[q] + (+(dtdx) * (ezR - ezL) - (dtdz) * (exF - exB));
+        }
+        if (i < c.nx && j < c.ny) {  // Bz face (i, j, k)
+            const T eyR = Ey[c.idx(i + 1, j, k)], eyL = Ey[q];
+            const T exU = Ex[c.idx(i, j + 1, k)], exD = Ex[q];
+            out.bz[q] = in.bz[q] + (-(dtdx) * (eyR - eyL) + (dtdy) * (exU - exD));
+        }
+    }
+}
+
+// CFL speeds of a cell in three directions (compute_dt loop body, M3:633-636)
+template <class T>
+__device__ __forceinline__ double speed3(const M3Const<T>& c, const Prim<T>& W) {
+    const T sx = fabs(W.u) + fast_speed(c, W, W.bx);
+    const T sy = fabs(W.v) + fast_speed(c, W, W.by);
+    const T sz = fabs(W.w) + fast_speed(c, W, W.bz);
+    // std::max(maxs, x) ignores NaN x; keep each finite value
+    double m = 0.0;
+    if ((double)sx > m) m = (double)sx;
+    if ((double)sy > m) m = (double)sy;
+    if ((double)sz > m) m = (double)sz;
+    return m;
+}
+
+// RK average (M3:1042-1065) with the deferred stage-2 Joule sub-step; emits the
+// CFL and density partials of U^{n+1}.  Inactive: U^n carried over.
+template <class T, int NT>
+__global__ void __launch_bounds__(NT)
+m3_average_kernel(const M3Const<T> c, const Fields3<T> un, const Fields3<T> s2, const Fields3<T> out,
+                  const double* __restrict__ dtp, const int* __restrict__ active, double* __restrict__ spd_part,
+                  double* __restrict__ rho_part) {
+    const bool act = (active == nullptr) || (*active != 0);
+    __shared__ double sh[NT / 32];
+    const T dt = (T)(*dtp);
+    double smax = 0.0, rsum = 0.0;
+    CC_FOR3(c.nx + 1, c.ny + 1, c.nz + 1) {
+        const int i = (int)(t_ % (c.nx + 1)), j = (int)((t_ / (c.nx + 1)) % (c.ny + 1));
+        const int k = (int)(t_ / ((long long)(c.nx + 1) * (c.ny + 1)));
+        const size_t q = c.idx(i, j, k);
+        auto avx = [&](size_t f) { return act ? T(0.5) * (un.bx[f] + s2.bx[f]) : un.bx[f]; };
+        auto avy = [&](size_t f) { return act ? T(0.5) * (un.by[f] + s2.by[f]) : un.by[f]; };
+        auto avz = [&](size_t f) { return act ? T(0.5) * (un.bz[f] + s2.bz[f]) : un.bz[f]; };
+        if (j < c.ny && k < c.nz) out.bx[q] = avx(q);
+        if (i < c.nx && k < c.nz) out.by[q] = avy(q);
+        if (i < c.nx && j < c.ny) out.bz[q] = avz(q);
+        if (i >= c.nx || j >= c.ny || k >= c.nz) continue;
+        const T Bx = T(0.5) * (avx(q) + avx(c.idx(i + 1, j, k)));
+        const T By = T(0.5) * (avy(q) + avy(c.idx(i, j + 1, k)));
+        const T Bz = T(0.5) * (avz(q) + avz(c.idx(i, j, k + 1)));
+        T rho, mx, my, mz, E;
+        if (act) {
+            T r2 = s2.rho[q], m2x = s2.mx[q], m2y = s2.my[q], m2z = s2.mz[q], E2 = s2.E[q];
+            if (c.resistive) E2 += joule3(c, s2, i, j, k, dt);
+            floors(c, r2, m2x, m2y, m2z, E2, bx_cc3(c, s2.bx, i, j, k), by_cc3(c, s2.by, i, j, k),
+                   bz_cc3(c, s2.bz, i, j, k));
+            rho = T(0.5) * (un.rho[q] + r2);
+            mx = T(0.5) * (un.mx[q] + m2x);
+            my = T(0.5) * (un.my[q] + m2y);
+            mz = T(0.5) * (un.mz[q] + m2z);
+            E = T(0.5) * (un.E[q] + E2);
+            floors(c, rho, mx, my, mz, E, Bx, By, Bz);
+        } else {
+            rho = un.rho[q]; mx = un.mx[q]; my = un.my[q]; mz = un.mz[q]; E = un.E[q];
+        }
+        out.rho[q] = rho; out.mx[q] = mx; out.my[q] = my; out.mz[q] = mz; out.E[q] = E;
+        const Prim<T> W = to_prim(c, rho, mx, my, mz, E, Bx, By, Bz);
+        const double s = speed3(c, W);
+        if (s > smax) smax = s;
+        rsum += (double)rho;
+    }
+    const double bm = block_max<NT>(smax, sh);
+    const double bs = block_sum<NT>(rsum, sh);
+    if (threadIdx.x == 0) { spd_part[blockIdx.x] = bm; rho_part[blockIdx.x] = bs; }
+}
+
+template <class T, int NT>
+__global__ void __launch_bounds__(NT)
+m3_speed_kernel(const M3Const<T> c, const Fields3<T> s, double* __restrict__ spd_part) {
+    __shared__ double sh[NT / 32];
+    double smax = 0.0;
+    CC_FOR3(c.nx, c.ny, c.nz) {
+        const int i = (int)(t_ % c.nx), j = (int)((t_ / c.nx) % c.ny), k = (int)(t_ / ((long long)c.nx * c.ny));
+        const size_t q = c.idx(i, j, k);
+        const Prim<T> W = to_prim(c, s.rho[q], s.mx[q], s.my[q], s.mz[q], s.E[q], bx_cc3(c, s.bx, i, j, k),
+                                  by_cc3(c, s.by, i, j, k), bz_cc3(c, s.bz, i, j, k));
+        const double v = speed3(c, W);
+        if (v > smax) smax = v;
+    }
+    const double bm = block_max<NT>(smax, sh);
+    if (threadIdx.x == 0) spd_part[blockIdx.x] = bm;
+}
+
+// FP64 sums (rho, mx, my, mz, E), max |div B| (M3:1070-1078), non-finite flag
+template <class T, int NT>
+__global__ void __launch_bounds__(NT) m3_diag_kernel(const M3Const<T> c, const Fields3<T> s, double* __restrict__ part) {
+    __shared__ double sh[NT / 32];
+    double acc[5] = {0, 0, 0, 0, 0}, dmax = 0.0, nonf = 0.0;
+    CC_FOR3(c.nx, c.ny, c.nz) {
+        const int i = (int)(t_ % c.nx), j = (int)((t_ / c.nx) % c.ny), k = (int)(t_ / ((long long)c.nx * c.ny));
+        const size_t q = c.idx(i, j, k);
+        const double v[5] = {(double)s.rho[q], (double)s.mx[q], (double)s.my[q], (double)s.mz[q], (double)s.E[q]};
+        for (int m = 0; m < 5; m++) {
+            acc[m] += v[m];
+            if (!isfinite(v[m])) nonf = 1.0;
+        }
+        const double d = ((double)s.bx[c.idx(i + 1, j, k)] - (double)s.bx[q]) / (double)c.dx +
+                         ((double)s.by[c.idx(i, j + 1, k)] - (double)s.by[q]) / (double)c.dy +
+                         ((double)s.bz[c.idx(i, j, k + 1)] - (double)s.bz[q]) / (double)c.dz;
+        dmax = fmax(dmax, fabs(d));
+    }
+    for (int m = 0; m < 5; m++) {
+        const double b = block_sum<NT>(acc[m], sh);
+        if (threadIdx.x == 0) part[m * gridDim.x + blockIdx.x] = b;
+    }
+    const double bm = block_max<NT>(dmax, sh);
+    const double bn = block_max<NT>(nonf, sh);
+    if (threadIdx.x == 0) { part[5 * gridDim.x + blockIdx.x] = bm; part[6 * gridDim.x + blockIdx.x] = bn; }
+}
+
+// host layout (x fastest, w x h x d) <-> pitched 3D field
+template <class T>
+__global__ void pack3_in_kernel(const double* __restrict__ src, T* __restrict__ dst, int w, int h, int d, int P,
+                                long long PS) {
+    CC_FOR3(w, h, d) {
+        const int i = (int)(t_ % w), j = (int)((t_ / w) % h), k = (int)(t_ / ((long long)w * h));
+        dst[(size_t)k * PS + (size_t)j * P + i] = (T)src[t_];
+    }
+}
+template <class T>
+__global__ void pack3_out_kernel(const T* __restrict__ src, double* __restrict__ dst, int w, int h, int d, int P,
+                                 long long PS) {
+    CC_FOR3(w, h, d) {
+        const int i = (int)(t_ % w), j = (int)((t_ / w) % h), k = (int)(t_ / ((long long)w * h));
+        dst[t_] = (double)src[(size_t)k * PS + (size_t)j * P + i];
+    }
+}
+
+}  // namespace ccb

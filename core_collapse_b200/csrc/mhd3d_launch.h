@@ -1,0 +1,32 @@
+// Host-side launchers of the 3D MHD kernels, defined once per precision in
+// mhd3d_f64.cu (-fmad=false, the parity path) and mhd3d_f32.cu.
+#pragma once
+#include <cuda_runtime.h>
+
+#include "mhd2d_launch.h"
+#include "mhd3d_kernels.cuh"
+
+namespace ccb {
+
+template <class T> struct M3Launch {
+    static cudaError_t prim(const M3Const<T>& c, const Fields3<T>& s, const PrimData<T>& pr, bool defer,
+                            const double* dt, const int* active, cudaStream_t st);
+    static cudaError_t faces(const M3Const<T>& c, const Fields3<T>& s, const PrimData<T>& pr, const FaceData<T>& X,
+                             const FaceData<T>& Y, const FaceData<T>& Z, const int* active, cudaStream_t st);
+    static cudaError_t update(const M3Const<T>& c, const Fields3<T>& in, const Fields3<T>& out, const FaceData<T>& X,
+                              const FaceData<T>& Y, const FaceData<T>& Z, const double* dt, const int* active,
+                              cudaStream_t st);
+    static cudaError_t edges(const M3Const<T>& c, const Fields3<T>& in, const FaceData<T>& X, const FaceData<T>& Y,
+                             const FaceData<T>& Z, T* Ex, T* Ey, T* Ez, const int* active, cudaStream_t st);
+    static cudaError_t ct(const M3Const<T>& c, const Fields3<T>& in, const Fields3<T>& out, const T* Ex, const T* Ey,
+                          const T* Ez, const double* dt, const int* active, cudaStream_t st);
+    static cudaError_t average(const M3Const<T>& c, const Fields3<T>& un, const Fields3<T>& s2, const Fields3<T>& out,
+                               const double* dt, const int* active, double* spd_part, double* rho_part,
+                               cudaStream_t st);
+    static cudaError_t speeds(const M3Const<T>& c, const Fields3<T>& s, double* spd_part, cudaStream_t st);
+    static cudaError_t diag(const M3Const<T>& c, const Fields3<T>& s, double* part, cudaStream_t st);
+    static cudaError_t pack_in(const double* src, T* dst, int w, int h, int d, int P, long long PS, cudaStream_t st);
+    static cudaError_t pack_out(const T* src, double* dst, int w, int h, int d, int P, long long PS, cudaStream_t st);
+};
+
+}  // namespace ccb

@@ -106,3 +106,160 @@ class State3:
 
 def empty_state3(p: Params3) -> State3:
     return State3(*[np.zeros(n) for n in p.sizes()])
+
+
+def _dp(a: np.ndarray):
+    assert a.dtype == np.float64 and a.flags["C_CONTIGUOUS"], "state arrays must be contiguous float64"
+    return a.ctypes.data_as(L._DP)
+
+
+class Mhd3dSolver:
+    """A device-resident 3D MHD instance (one libcc_b200 handle)."""
+
+    def __init__(self, p: Params3):
+        from .mhd2d import CcError
+        self._Err = CcError
+        self.p = p
+        self._lib = L.lib()
+        self._cp = p.to_c()
+        self._h = C.c_void_p()
+        r = self._lib.cc_mhd3d_create(C.byref(self._cp), C.byref(self._h))
+        if r != L.CC_OK:
+            msg = self._lib.cc_last_error(self._h).decode() if self._h.value else "create failed"
+            if self._h.value:
+                self._lib.cc_destroy(self._h)
+            self._h = C.c_void_p()
+            raise CcError(r, msg)
+
+    def _check(self, r: int):
+        if r != L.CC_OK:
+            raise self._Err(r, self._lib.cc_last_error(self._h).decode())
+
+    def close(self):
+        if self._h and self._h.value:
+            self._lib.cc_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def upload(self, s: State3):
+        self._check(self._lib.cc_mhd3d_upload(self._h, *[_dp(a) for a in s.arrays()]))
+
+    def download(self, s: State3 | None = None) -> State3:
+        if s is None:
+            s = empty_state3(self.p)
+        self._check(self._lib.cc_mhd3d_download(self._h, *[_dp(a) for a in s.arrays()]))
+        return s
+
+    def compute_dt(self) -> float:
+        dt = C.c_double()
+        self._check(self._lib.cc_mhd3d_compute_dt(self._h, C.byref(dt)))
+        return dt.value
+
+    def rk2_step(self, dt: float):
+        self._check(self._lib.cc_mhd3d_rk2_step(self._h, float(dt)))
+
+    def advance(self, nsteps: int, t: float | None = None) -> float:
+        tt = C.c_double(0.0 if t is None else t)
+        self._check(self._lib.cc_mhd3d_advance(self._h, int(nsteps), C.byref(tt)))
+        return tt.value
+
+    def set_stream(self, stream_ptr: int | None):
+        self._check(self._lib.cc_set_stream(self._h, C.c_void_p(stream_ptr) if stream_ptr else None))
+
+    def set_profiling(self, on: bool):
+        self._check(self._lib.cc_set_profiling(self._h, 1 if on else 0))
+
+    def perf(self) -> dict:
+        q = L.CcPerf()
+        self._check(self._lib.cc_get_perf(self._h, C.byref(q)))
+        return {f: getattr(q, f) for f, _ in L.CcPerf._fields_}
+
+    def reset_perf(self):
+        self._check(self._lib.cc_reset_perf(self._h))
+
+    def diagnostics(self) -> dict:
+        d = L.CcDiag()
+        self._check(self._lib.cc_mhd3d_diagnostics(self._h, C.byref(d)))
+        return {f: getattr(d, f) for f, _ in L.CcDiag._fields_}
+
+
+# ---- drop-in functions with the reference's signatures (M3:626, 1034) ----
+
+def compute_dt(p: Params3, s: State3, dx: float, dy: float, dz: float) -> float:
+    with Mhd3dSolver(p) as g:
+        g.upload(s)
+        return g.compute_dt()
+
+
+def rk2_step(p: Params3, s: State3, dx: float, dy: float, dz: float, dt: float) -> None:
+    """rk2_step on the GPU; the state arrays are updated in place."""
+    with Mhd3dSolver(p) as g:
+        g.upload(s)
+        g.rk2_step(dt)
+        g.download(s)
+
+
+# ---- initial conditions (host side) ----
+
+def _random_phase_field(shape, offset, modes, phases, amp=1.0):
+    """Re sum_n amp e^{i phase_n} e^{2 pi i n.(j + offset)/N} at grid indices j of
+    `shape` = (Nz, Ny, Nx), for integer mode vectors `modes` (m, 3) as (nx, ny, nz)."""
+    nz, ny, nx = shape
+    F = np.zeros(shape, dtype=np.complex128)
+    shift = np.exp(2j * np.pi * (modes[:, 0] * offset[0] / nx + modes[:, 1] * offset[1] / ny +
+                                 modes[:, 2] * offset[2] / nz))
+    np.add.at(F, (modes[:, 2] % nz, modes[:, 1] % ny, modes[:, 0] % nx), amp * np.exp(1j * phases) * shift)
+    return np.real(np.fft.ifftn(F)) * (nx * ny * nz)
+
+
+def ic_turbulence3d(p: Params3, seed: int = 1, v_rms: float = 0.5, b_rms: float = 0.3, kmin: float = 1.0,
+                    kmax: float = 4.0, rho0: float = 1.0, gamma: float = 5.0 / 3.0) -> State3:
+    """Uniform density rho0 and pressure 1/gamma; velocity and edge vector
+    potential A are random-phase Fourier fields over the integer mode vectors
+    with kmin <= |n| <= kmax (one numpy Generator(seed) draws every phase);
+    v is scaled to rms v_rms over cells, B = curl A on faces (div B = 0 to
+    roundoff) scaled so the cell-centred |B| has rms b_rms.  Periodic box."""
+    nx, ny, nz = p.Nx, p.Ny, p.Nz
+    rng = np.random.default_rng(seed)
+    r = int(np.ceil(kmax))
+    g = np.arange(-r, r + 1)
+    M = np.stack(np.meshgrid(g, g, g, indexing="ij"), -1).reshape(-1, 3)
+    kk = np.sqrt((M ** 2).sum(1))
+    modes = M[(kk >= kmin) & (kk <= kmax)]
+    ph = rng.uniform(0.0, 2.0 * np.pi, size=(6, len(modes)))
+    shape = (nz, ny, nx)
+    v = [_random_phase_field(shape, (0.5, 0.5, 0.5), modes, ph[c]) for c in range(3)]
+    vs = v_rms / np.sqrt(np.mean(v[0] ** 2 + v[1] ** 2 + v[2] ** 2))
+    u, vv, w = (a.ravel() * vs for a in v)
+    Ax = _random_phase_field(shape, (0.5, 0.0, 0.0), modes, ph[3])   # x-edges (i+1/2, j, k)
+    Ay = _random_phase_field(shape, (0.0, 0.5, 0.0), modes, ph[4])   # y-edges (i, j+1/2, k)
+    Az = _random_phase_field(shape, (0.0, 0.0, 0.5), modes, ph[5])   # z-edges (i, j, k+1/2)
+    dx, dy, dz = p.dx, p.dy, p.dz
+    roll = lambda a, ax: np.roll(a, -1, axis=ax)   # value at index + 1 (periodic)
+    # cell-indexed faces, then the face at index N repeats face 0
+    bx = (roll(Az, 1) - Az) / dy - (roll(Ay, 0) - Ay) / dz
+    by = (roll(Ax, 0) - Ax) / dz - (roll(Az, 2) - Az) / dx
+    bz = (roll(Ay, 2) - Ay) / dx - (roll(Ax, 1) - Ax) / dy
+    bxc, byc, bzc = 0.5 * (bx + roll(bx, 2)), 0.5 * (by + roll(by, 1)), 0.5 * (bz + roll(bz, 0))
+    bs = b_rms / np.sqrt(np.mean(bxc ** 2 + byc ** 2 + bzc ** 2))
+    bx, by, bz, bxc, byc, bzc = (a * bs for a in (bx, by, bz, bxc, byc, bzc))
+    Bx_f = np.concatenate([bx, bx[:, :, :1]], axis=2)
+    By_f = np.concatenate([by, by[:, :1, :]], axis=1)
+    Bz_f = np.concatenate([bz, bz[:1, :, :]], axis=0)
+    n = nx * ny * nz
+    rho = np.full(n, rho0)
+    P = 1.0 / gamma
+    E = 0.5 * rho * (u * u + vv * vv + w * w) + 0.5 * (bxc.ravel() ** 2 + byc.ravel() ** 2 + bzc.ravel() ** 2) + \
+        P / (gamma - 1.0)
+    return State3(rho, rho * u, rho * vv, rho * w, E, Bx_f.ravel().copy(), By_f.ravel().copy(), Bz_f.ravel().copy())

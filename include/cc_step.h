@@ -211,6 +211,26 @@ int cc_mhd2d_advance(cc_handle* h, int nsteps, double* t);
 /* Diagnostics of the resident state. */
 int cc_mhd2d_diagnostics(cc_handle* h, cc_diag* d);
 
+/* ---- 3D MHD (mhd3d_resistive_hlld_ct.cpp) ---- */
+
+/* Fill with the reference defaults (mhd3d_resistive_hlld_ct.cpp:43-89). */
+void cc_mhd3d_params_default(cc_mhd3d_params* p);
+int cc_mhd3d_create(const cc_mhd3d_params* p, cc_handle** out);
+/* Ucc {rho,mx,my,mz,E} and Bfaces {Bx_f,By_f,Bz_f}: M3:91-99 */
+int cc_mhd3d_upload(cc_handle* h, const double* rho, const double* mx, const double* my, const double* mz,
+                    const double* E, const double* Bx_f, const double* By_f, const double* Bz_f);
+int cc_mhd3d_download(cc_handle* h, double* rho, double* mx, double* my, double* mz, double* E,
+                      double* Bx_f, double* By_f, double* Bz_f);
+/* compute_dt(p, U, B, dx, dy, dz) (mhd3d_resistive_hlld_ct.cpp:626-648) */
+int cc_mhd3d_compute_dt(cc_handle* h, double* dt);
+/* rk2_step(p, U, B, dx, dy, dz, dt) (mhd3d_resistive_hlld_ct.cpp:1034-1066) */
+int cc_mhd3d_rk2_step(cc_handle* h, double dt);
+/* nsteps of the main() loop body (mhd3d_resistive_hlld_ct.cpp:1285-1291) on the
+ * device: dt = compute_dt, clamped to t_end; rk2_step.  Stops once t >= t_end. */
+int cc_mhd3d_advance(cc_handle* h, int nsteps, double* t);
+/* FP64 sums and max |div B| (mhd3d_resistive_hlld_ct.cpp:1070-1078) */
+int cc_mhd3d_diagnostics(cc_handle* h, cc_diag* d);
+
 /* ---- spectral gravity without device allocation ----
  * No counterpart in the reference: an addition for callers that cannot call
  * cudaMalloc -- a host application whose memory manager owns the GPU's
