@@ -126,11 +126,21 @@ SIGNATURES = {
     "cc_mhd3d_rk2_step": (C.c_int, [_H, C.c_double]),
     "cc_mhd3d_advance": (C.c_int, [_H, C.c_int, _DP]),
     "cc_mhd3d_diagnostics": (C.c_int, [_H, C.POINTER(CcDiag)]),
+    "cc_euler2d_params_default": (None, [C.POINTER(CcEuler2dParams)]),
+    "cc_euler2d_create": (C.c_int, [C.POINTER(CcEuler2dParams), C.POINTER(_H)]),
+    "cc_euler2d_upload": (C.c_int, [_H] + [_DP] * 4),
+    "cc_euler2d_download": (C.c_int, [_H] + [_DP] * 4),
+    "cc_euler2d_compute_dt": (C.c_int, [_H, _DP]),
+    "cc_euler2d_compute_gravity": (C.c_int, [_H, _DP, _DP]),
+    "cc_euler2d_rk2_step": (C.c_int, [_H, C.c_double]),
+    "cc_euler2d_advance": (C.c_int, [_H, C.c_int, _DP]),
+    "cc_euler2d_diagnostics": (C.c_int, [_H, C.POINTER(CcDiag)]),
     "cc_mhd2d_ic_knobs_default": (None, [C.POINTER(CcIcKnobs)]),
     "cc_ic_mhd2d_reference": (C.c_int, [C.POINTER(CcMhd2dParams), C.POINTER(CcIcKnobs), C.POINTER(_DP)]),
     "cc_ic_mhd2d_collapse": (C.c_int, [C.POINTER(CcMhd2dParams), C.c_double, C.c_double, C.c_double, C.c_uint32,
                                        C.c_double, C.c_double, C.c_double, C.POINTER(_DP)]),
     "cc_ic_mhd2d_orszag_tang": (C.c_int, [C.POINTER(CcMhd2dParams), C.c_double, C.c_double, C.POINTER(_DP)]),
+    "cc_ic_euler2d_random_blob": (C.c_int, [C.POINTER(CcEuler2dParams), C.POINTER(_DP)]),
 }
 
 _lib = None

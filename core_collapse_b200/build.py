@@ -3,10 +3,12 @@
     python -m core_collapse_b200.build [-v]
 
 Translation units and their floating-point contract:
-  mhd2d_f64.cu, mhd3d_f64.cu, common_kernels.cu,
+  mhd2d_f64.cu, mhd3d_f64.cu, euler2d_f64.cu,
+  common_kernels.cu,
   noalloc.cu                         -fmad=false: FP64 kernels round exactly like
                                      the reference's x86-64 build (no FMA)
-  mhd2d_f32.cu, mhd3d_f32.cu         FMA contraction on, approximate FP32 division
+  mhd2d_f32.cu, mhd3d_f32.cu,
+  euler2d_f32.cu                     FMA contraction on, approximate FP32 division
                                      and square root, flush-to-zero (the FP32 bulk path)
   capi.cu, ic.cpp                    host code
 """
@@ -31,13 +33,16 @@ COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-I", str(INC
 UNITS = [
     ("mhd2d_f64.cu", ["-fmad=false"]),
     ("mhd3d_f64.cu", ["-fmad=false"]),
+    ("euler2d_f64.cu", ["-fmad=false"]),
     ("common_kernels.cu", ["-fmad=false"]),
     ("noalloc.cu", ["-fmad=false"]),
     # FP32 bulk path: approximate division/sqrt (<= 2 ulp), denormals flushed
     ("mhd2d_f32.cu", ["-prec-div=false", "-prec-sqrt=false", "-ftz=true"]),
     ("mhd3d_f32.cu", ["-prec-div=false", "-prec-sqrt=false", "-ftz=true"]),
+    ("euler2d_f32.cu", ["-prec-div=false", "-prec-sqrt=false", "-ftz=true"]),
     ("capi.cu", []),
     ("capi_mhd3d.cu", []),
+    ("capi_euler2d.cu", []),
     ("ic.cpp", []),
 ]
 

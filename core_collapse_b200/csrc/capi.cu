@@ -251,7 +251,7 @@ template <class T> struct Mhd2d : Mhd2dBase {
                                            p.x1 - p.x0, p.y1 - p.y0, p.G, fftA, phi, active(), st()));
             count(3);
         } else {
-            CC_CUDA(M2Launch<T>::sor_rhs(rho, nx, ny, P, rho_part, 4.0 * M_PI * p.G, rhs, active(), st()));
+            CC_CUDA(M2Launch<T>::sor_rhs(rho, nx, ny, P, rho_part, 4.0 * M_PI * p.G, -1.0, rhs, active(), st()));
             const double dx = (p.x1 - p.x0) / nx, dy = (p.y1 - p.y0) / ny;
             SorArgs a;
             a.nx = nx; a.ny = ny; a.ax = c.ax; a.ay = c.ay;
@@ -309,6 +309,7 @@ template <class T> struct Mhd2d : Mhd2dBase {
         const double dx = (p.x1 - p.x0) / p.Nx, dy = (p.y1 - p.y0) / p.Ny;
         DtSpec d;
         d.cfl = p.cfl; d.hmin = vmin(dx, dy); d.eta = p.eta; d.t_end = p.t_end; d.clamp_to_end = clamp ? 1 : 0;
+        d.seed = 1e-14; d.end_eps = 0.0; d.check = 0; d.cap = 1;
         return d;
     }
 

@@ -1,0 +1,435 @@
+// C ABI of the 2D Euler + self-gravity HLLC step (euler2d_gravity_hllc.cpp).
+//
+// Per step (EH:697-706, 529-550): CFL partials and floored-density sums of U;
+// dt = cfl min(dx,dy) / max speed, a non-finite or non-positive dt stops the
+// loop with CC_ERR_NONFINITE (EH:699-702), clamp to t_end;
+// Poisson(U) -> phi; stage 1: U1 = floors(U + dt rhs(U));
+// Poisson(U1) -> phi; stage 2: U = floors(0.5 U + 0.5 (U1 + dt rhs(U1)));
+// t += dt.  The Poisson solve floors the density and always wraps (EH:300-317).
+#include <cmath>
+#include <cstring>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "euler2d_launch.h"
+#include "handle.h"
+
+using namespace ccb;
+
+namespace {
+
+struct Euler2dBase {
+    virtual ~Euler2dBase() {}
+    virtual int init() = 0;
+    virtual int upload(const double* const* f) = 0;
+    virtual int download(double* const* f) = 0;
+    virtual int compute_dt(double* dt) = 0;
+    virtual int gravity(double* gx, double* gy) = 0;
+    virtual int rk2_step(double dt) = 0;
+    virtual int advance(int nsteps, double* t) = 0;
+    virtual int diagnostics(cc_diag* d) = 0;
+};
+
+template <class T> struct Euler2d : Euler2dBase {
+    cc_handle* h;
+    cc_euler2d_params p;
+    EHConst<T> c{};
+    int P = 0;
+    size_t plane = 0;
+    void* block = nullptr;
+    EHFields<T> U{}, U1{};
+    T* phi = nullptr;
+    T* g2[2] = {nullptr, nullptr};
+    double *rhs = nullptr, *sphi = nullptr, *sor_part = nullptr, *sor_part2 = nullptr;
+    double *staging = nullptr, *spd_part = nullptr, *rho_part = nullptr, *diag_part = nullptr, *scal = nullptr;
+    unsigned int* bar = nullptr;
+    long long* steps_dev = nullptr;
+    int* iflags = nullptr;   // active, barrier error, SOR sweeps, bad dt
+    bool loaded = false;
+    cudaGraphExec_t graph1 = nullptr;
+    cudaStream_t graph_stream = nullptr;
+    cc_perf graph_delta{};
+
+    Euler2d(cc_handle* hh, const cc_euler2d_params& pp) : h(hh), p(pp) {}
+    cc_handle* this_handle() { return h; }
+    cudaStream_t st() const { return h->stream; }
+    double* dt_dev() { return scal; }
+    double* t_dev() { return scal + 1; }
+    double* res_dev() { return scal + 2; }
+    int* active() { return iflags; }
+    void count(int n) { h->perf.kernel_launches += n; }
+
+    ~Euler2d() override {
+        if (graph1) cudaGraphExecDestroy(graph1);
+        void* ptrs[] = {block, phi, g2[0], g2[1], rhs, sphi, sor_part, sor_part2, staging, spd_part, rho_part,
+                        diag_part, scal, bar, steps_dev, iflags};
+        for (void* q : ptrs)
+            if (q) cudaFree(q);
+    }
+
+    int init() override {
+        const int nx = p.Nx, ny = p.Ny;
+        const double dx = (p.x1 - p.x0) / nx, dy = (p.y1 - p.y0) / ny;
+        c.gamma = (T)p.gamma; c.gm1 = (T)p.gamma - (T)1.0;
+        c.floor_rho = (T)p.floor_rho; c.floor_P = (T)p.floor_P;
+        c.dx = (T)dx; c.dy = (T)dy; c.two_dx = (T)(2.0 * dx); c.two_dy = (T)(2.0 * dy);
+        c.nx = nx; c.ny = ny;
+        P = ((nx + 1 + 31) / 32) * 32;
+        c.pitch = P;
+        c.ax = AxisMap{nx, p.periodic_x ? 1 : 0};
+        c.ay = AxisMap{ny, p.periodic_y ? 1 : 0};
+        c.pax = AxisMap{nx, 1};
+        c.pay = AxisMap{ny, 1};
+        c.gravity_on = p.gravity_on ? 1 : 0;
+        plane = (size_t)P * (ny + 1);
+        if (p.gravity_on) {
+            if (p.poisson_kind != CC_POISSON_SOR)
+                return fail(h, CC_ERR_UNSUPPORTED, "the Euler/HLLC solver supports the SOR Poisson solve only");
+            if ((nx & 1) || (ny & 1)) return fail(h, CC_ERR_UNSUPPORTED, "red-black SOR needs even Nx and Ny (periodic)");
+        }
+        CC_CUDA(EHLaunch<T>::prepare());
+        CC_CUDA(cudaMalloc(&block, sizeof(T) * plane * 8));
+        CC_CUDA(cudaMemsetAsync(block, 0, sizeof(T) * plane * 8, st()));
+        T* b = reinterpret_cast<T*>(block);
+        U = EHFields<T>{b, b + plane, b + 2 * plane, b + 3 * plane};
+        U1 = EHFields<T>{b + 4 * plane, b + 5 * plane, b + 6 * plane, b + 7 * plane};
+        CC_CUDA(cudaMalloc(&phi, sizeof(T) * plane));
+        CC_CUDA(cudaMemsetAsync(phi, 0, sizeof(T) * plane, st()));
+        CC_CUDA(cudaMalloc(&staging, sizeof(double) * (size_t)(nx + 1) * (ny + 1)));
+        CC_CUDA(cudaMalloc(&spd_part, sizeof(double) * RED_BLOCKS));
+        CC_CUDA(cudaMalloc(&rho_part, sizeof(double) * RED_BLOCKS));
+        CC_CUDA(cudaMalloc(&diag_part, sizeof(double) * RED_BLOCKS * 5));
+        CC_CUDA(cudaMalloc(&scal, sizeof(double) * 4));
+        CC_CUDA(cudaMemsetAsync(scal, 0, sizeof(double) * 4, st()));
+        CC_CUDA(cudaMalloc(&steps_dev, sizeof(long long)));
+        CC_CUDA(cudaMemsetAsync(steps_dev, 0, sizeof(long long), st()));
+        CC_CUDA(cudaMalloc(&iflags, sizeof(int) * 4));
+        int init_flags[4] = {1, 0, 0, 0};
+        CC_CUDA(cudaMemcpyAsync(iflags, init_flags, sizeof(init_flags), cudaMemcpyHostToDevice, st()));
+        if (p.gravity_on) {
+            CC_CUDA(cudaMalloc(&rhs, sizeof(double) * (size_t)nx * ny));
+            CC_CUDA(cudaMalloc(&sphi, sizeof(double) * (size_t)nx * ny));
+            CC_CUDA(cudaMalloc(&sor_part, sizeof(double) * 4096));
+            CC_CUDA(cudaMalloc(&sor_part2, sizeof(double) * 4096));
+            CC_CUDA(cudaMalloc(&bar, sizeof(unsigned int) * 2));
+            CC_CUDA(cudaMemsetAsync(bar, 0, sizeof(unsigned int) * 2, st()));
+        }
+        CC_CUDA(cudaStreamSynchronize(st()));
+        return CC_OK;
+    }
+
+    T* field(const EHFields<T>& f, int k) const {
+        T* a[4] = {f.rho, f.mx, f.my, f.E};
+        return a[k];
+    }
+
+    int upload(const double* const* f) override {
+        for (int k = 0; k < 4; k++) {
+            if (!f[k]) return fail(h, CC_ERR_ARG, "null state array");
+            CC_CUDA(cudaMemcpyAsync(staging, f[k], sizeof(double) * (size_t)p.Nx * p.Ny, cudaMemcpyHostToDevice, st()));
+            CC_CUDA(M2Launch<T>::pack_in(staging, field(U, k), p.Nx, p.Ny, P, st()));
+            count(1);
+        }
+        loaded = true;
+        return CC_OK;
+    }
+
+    int download(double* const* f) override {
+        if (!loaded) return fail(h, CC_ERR_STATE, "no state uploaded");
+        for (int k = 0; k < 4; k++) {
+            if (!f[k]) continue;
+            CC_CUDA(M2Launch<T>::pack_out(field(U, k), staging, p.Nx, p.Ny, P, st()));
+            count(1);
+            CC_CUDA(cudaMemcpyAsync(f[k], staging, sizeof(double) * (size_t)p.Nx * p.Ny, cudaMemcpyDeviceToHost, st()));
+        }
+        CC_CUDA(cudaStreamSynchronize(st()));
+        return CC_OK;
+    }
+
+    // Poisson on a density field whose floored sum is in rho_part -> phi
+    int solve(const T* rho) {
+        if (!p.gravity_on) return CC_OK;
+        h->perf.poisson_solves += 1;
+        const int nx = p.Nx, ny = p.Ny;
+        CC_CUDA(M2Launch<T>::sor_rhs(rho, nx, ny, P, rho_part, 4.0 * M_PI * p.G, p.floor_rho, rhs, active(), st()));
+        const double dx = (p.x1 - p.x0) / nx, dy = (p.y1 - p.y0) / ny;
+        SorArgs a;
+        a.nx = nx; a.ny = ny; a.ax = c.pax; a.ay = c.pay;
+        a.idx2 = 1.0 / (dx * dx); a.idy2 = 1.0 / (dy * dy);
+        a.denom = 2.0 * (a.idx2 + a.idy2);
+        a.omega = p.sor_omega; a.tol = p.sor_tol; a.max_iter = p.sor_max_iter;
+        a.rhs = rhs; a.phi = sphi; a.part = sor_part; a.part2 = sor_part2;
+        a.bar = GridBarrier{bar, bar + 1, iflags + 1};
+        a.iters_out = iflags + 2; a.res_out = res_dev(); a.active = active();
+        int nb = 0;
+        CC_CUDA(launch_sor(a, &nb, st()));
+        CC_CUDA(M2Launch<T>::phi_to_field(sphi, nx, ny, phi, P, active(), st()));
+        count(3);
+        return CC_OK;
+    }
+
+    DtSpec dtspec(bool clamp) const {
+        const double dx = (p.x1 - p.x0) / p.Nx, dy = (p.y1 - p.y0) / p.Ny;
+        DtSpec d;
+        d.cfl = p.cfl; d.hmin = vmin(dx, dy); d.eta = 0.0; d.t_end = p.t_end; d.clamp_to_end = clamp ? 1 : 0;
+        d.seed = 1e-30; d.end_eps = 1e-14; d.check = 1; d.cap = 0;   // EH:395, 697, 699-702
+        return d;
+    }
+
+    int compute_dt(double* dt) override {
+        if (!loaded) return fail(h, CC_ERR_STATE, "no state uploaded");
+        CC_CUDA(EHLaunch<T>::speeds(c, U, spd_part, rho_part, st()));
+        CC_CUDA(launch_dt_finalize(spd_part, dtspec(false), dt_dev(), t_dev(), active(), st()));
+        count(2);
+        CC_CUDA(cudaMemcpyAsync(dt, dt_dev(), sizeof(double), cudaMemcpyDeviceToHost, st()));
+        CC_CUDA(cudaStreamSynchronize(st()));
+        return CC_OK;
+    }
+
+    int gravity(double* gx, double* gy) override {
+        if (!loaded) return fail(h, CC_ERR_STATE, "no state uploaded");
+        const int nx = p.Nx, ny = p.Ny;
+        int one = 1;
+        CC_CUDA(cudaMemcpyAsync(iflags, &one, sizeof(int), cudaMemcpyHostToDevice, st()));
+        if (p.gravity_on) {
+            CC_CUDA(EHLaunch<T>::rho_sum(c, U.rho, rho_part, st()));
+            count(1);
+            if (int r = solve(U.rho)) return r;
+        }
+        if (!g2[0]) {
+            CC_CUDA(cudaMalloc(&g2[0], sizeof(T) * plane));
+            CC_CUDA(cudaMalloc(&g2[1], sizeof(T) * plane));
+        }
+        if (p.gravity_on) {
+            CC_CUDA(M2Launch<T>::gravity_from_phi(phi, nx, ny, P, c.pax, c.pay, c.two_dx, c.two_dy, g2[0], g2[1], st()));
+            count(1);
+        } else {
+            CC_CUDA(cudaMemsetAsync(g2[0], 0, sizeof(T) * plane, st()));
+            CC_CUDA(cudaMemsetAsync(g2[1], 0, sizeof(T) * plane, st()));
+        }
+        double* dst[2] = {gx, gy};
+        for (int k = 0; k < 2; k++) {
+            if (!dst[k]) continue;
+            CC_CUDA(M2Launch<T>::pack_out(g2[k], staging, nx, ny, P, st()));
+            count(1);
+            CC_CUDA(cudaMemcpyAsync(dst[k], staging, sizeof(double) * (size_t)nx * ny, cudaMemcpyDeviceToHost, st()));
+        }
+        CC_CUDA(cudaStreamSynchronize(st()));
+        return check_flags();
+    }
+
+    int check_flags() {
+        int fl[4];
+        CC_CUDA(cudaMemcpy(fl, iflags, sizeof(fl), cudaMemcpyDeviceToHost));
+        if (fl[1]) return fail(h, CC_ERR_CUDA, "SOR grid barrier timed out");
+        if (fl[3]) return fail(h, CC_ERR_NONFINITE, "dt not finite or not positive (the reference aborts here)");
+        return CC_OK;
+    }
+
+    // rk2_step (EH:529-550) with dt in dt_dev; the RHS solves Poisson itself (EH:411)
+    int step_body() {
+        if (p.gravity_on) {
+            CC_CUDA(EHLaunch<T>::rho_sum(c, U.rho, rho_part, st()));
+            count(1);
+            if (int r = solve(U.rho)) return r;
+        }
+        CC_CUDA(EHLaunch<T>::stage(c, U, U, U1, false, phi, dt_dev(), active(), st()));
+        count(1);
+        if (p.gravity_on) {
+            CC_CUDA(EHLaunch<T>::rho_sum(c, U1.rho, rho_part, st()));
+            count(1);
+            if (int r = solve(U1.rho)) return r;
+        }
+        CC_CUDA(EHLaunch<T>::stage(c, U, U1, U, true, phi, dt_dev(), active(), st()));
+        count(1);
+        h->perf.steps += 1;
+        return CC_OK;
+    }
+
+    int rk2_step(double dt) override {
+        if (!loaded) return fail(h, CC_ERR_STATE, "no state uploaded");
+        int one = 1;
+        CC_CUDA(cudaMemcpyAsync(iflags, &one, sizeof(int), cudaMemcpyHostToDevice, st()));
+        CC_CUDA(launch_set_scalar(dt_dev(), dt, st()));
+        count(1);
+        if (int r = step_body()) return r;
+        CC_CUDA(cudaStreamSynchronize(st()));
+        return check_flags();
+    }
+
+    int device_step() {
+        CC_CUDA(EHLaunch<T>::speeds(c, U, spd_part, rho_part, st()));
+        CC_CUDA(launch_dt_finalize(spd_part, dtspec(true), dt_dev(), t_dev(), active(), st()));
+        count(2);
+        if (int r = step_body()) return r;
+        CC_CUDA(launch_clock(t_dev(), dt_dev(), active(), steps_dev, st()));
+        count(1);
+        return CC_OK;
+    }
+
+    int advance(int nsteps, double* t) override {
+        if (!loaded) return fail(h, CC_ERR_STATE, "no state uploaded");
+        if (nsteps < 0) return fail(h, CC_ERR_ARG, "nsteps < 0");
+        if (t) {
+            CC_CUDA(launch_set_scalar(t_dev(), *t, st()));
+            count(1);
+        }
+        const bool graphable = !p.gravity_on && !h->profiling;
+        if (graphable && nsteps >= 1) {
+            if (!graph1 || graph_stream != st()) {
+                if (graph1) { cudaGraphExecDestroy(graph1); graph1 = nullptr; }
+                const cc_perf before = h->perf;
+                cudaGraph_t g = nullptr;
+                CC_CUDA(cudaStreamBeginCapture(st(), cudaStreamCaptureModeThreadLocal));
+                int rr = device_step();
+                cudaError_t e = cudaStreamEndCapture(st(), &g);
+                graph_delta.kernel_launches = h->perf.kernel_launches - before.kernel_launches;
+                graph_delta.steps = h->perf.steps - before.steps;
+                h->perf = before;
+                if (rr) { if (g) cudaGraphDestroy(g); return rr; }
+                if (e != cudaSuccess) return fail(h, CC_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(e));
+                e = cudaGraphInstantiate(&graph1, g, 0);
+                cudaGraphDestroy(g);
+                if (e != cudaSuccess) return fail(h, CC_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(e));
+                graph_stream = st();
+            }
+            for (int k = 0; k < nsteps; k++) {
+                CC_CUDA(cudaGraphLaunch(graph1, st()));
+                h->perf.kernel_launches += graph_delta.kernel_launches;
+                h->perf.steps += graph_delta.steps;
+            }
+        } else {
+            for (int k = 0; k < nsteps; k++)
+                if (int r = device_step()) return r;
+        }
+        if (t) CC_CUDA(cudaMemcpyAsync(t, t_dev(), sizeof(double), cudaMemcpyDeviceToHost, st()));
+        CC_CUDA(cudaStreamSynchronize(st()));
+        return check_flags();
+    }
+
+    int diagnostics(cc_diag* d) override {
+        if (!loaded) return fail(h, CC_ERR_STATE, "no state uploaded");
+        CC_CUDA(EHLaunch<T>::diag(c, U, diag_part, st()));
+        count(1);
+        std::vector<double> part(RED_BLOCKS * 5);
+        CC_CUDA(cudaMemcpyAsync(part.data(), diag_part, sizeof(double) * part.size(), cudaMemcpyDeviceToHost, st()));
+        double sc[4];
+        CC_CUDA(cudaMemcpyAsync(sc, scal, sizeof(sc), cudaMemcpyDeviceToHost, st()));
+        long long steps = 0;
+        CC_CUDA(cudaMemcpyAsync(&steps, steps_dev, sizeof(steps), cudaMemcpyDeviceToHost, st()));
+        int fl[4];
+        CC_CUDA(cudaMemcpyAsync(fl, iflags, sizeof(fl), cudaMemcpyDeviceToHost, st()));
+        CC_CUDA(cudaStreamSynchronize(st()));
+        double s[4] = {0, 0, 0, 0}, nonf = 0.0;
+        for (int m = 0; m < 4; m++)
+            for (int b = 0; b < RED_BLOCKS; b++) s[m] += part[m * RED_BLOCKS + b];
+        for (int b = 0; b < RED_BLOCKS; b++) nonf = std::fmax(nonf, part[4 * RED_BLOCKS + b]);
+        const double dV = ((p.x1 - p.x0) / p.Nx) * ((p.y1 - p.y0) / p.Ny);
+        std::memset(d, 0, sizeof(*d));
+        d->mass = s[0] * dV; d->mom_x = s[1] * dV; d->mom_y = s[2] * dV; d->energy = s[3] * dV;
+        d->t = sc[1]; d->dt_last = sc[0]; d->steps = steps;
+        d->poisson_iters = fl[2]; d->poisson_residual = sc[2];
+        d->nonfinite = nonf > 0.0 ? 1 : 0;
+        return CC_OK;
+    }
+};
+
+struct Euler2dHandle : cc_handle {
+    std::unique_ptr<Euler2dBase> impl;
+};
+
+Euler2dBase* eh(cc_handle* h) {
+    if (!h || h->kind != KIND_EULER2D) return nullptr;
+    return static_cast<Euler2dHandle*>(h)->impl.get();
+}
+
+}  // namespace
+
+extern "C" {
+
+void cc_euler2d_params_default(cc_euler2d_params* p) {
+    if (!p) return;
+    std::memset(p, 0, sizeof(*p));
+    p->gamma = 1.2; p->cfl = 0.45;
+    p->x0 = 0.0; p->x1 = 1.0; p->y0 = 0.0; p->y1 = 1.0;
+    p->Nx = 50; p->Ny = 50;
+    p->t_end = 5.0; p->dt_store = 1e-3;
+    p->floor_rho = 1e-12; p->floor_P = 1e-12;
+    p->periodic_x = 1; p->periodic_y = 1;
+    p->gravity_on = 1; p->sor_max_iter = 50000;
+    p->G = 1.0; p->softening = 1e-4;
+    p->sor_tol = 1e-10; p->sor_omega = 1.7;
+    p->poisson_kind = CC_POISSON_SOR; p->precision = CC_FP64;
+}
+
+int cc_euler2d_create(const cc_euler2d_params* p, cc_handle** out) {
+    if (!p || !out) return CC_ERR_ARG;
+    *out = nullptr;
+    if (p->Nx < 2 || p->Ny < 2 || !(p->x1 > p->x0) || !(p->y1 > p->y0)) return CC_ERR_ARG;
+    if (p->precision != CC_FP64 && p->precision != CC_FP32) return CC_ERR_ARG;
+    auto h = std::make_unique<Euler2dHandle>();
+    h->kind = KIND_EULER2D;
+    if (cudaGetDevice(&h->device) != cudaSuccess) return CC_ERR_CUDA;
+    if (cudaStreamCreateWithFlags(&h->own, cudaStreamNonBlocking) != cudaSuccess) return CC_ERR_CUDA;
+    h->stream = h->own;
+    if (p->precision == CC_FP64) h->impl = std::make_unique<Euler2d<double>>(h.get(), *p);
+    else h->impl = std::make_unique<Euler2d<float>>(h.get(), *p);
+    int r = h->impl->init();
+    *out = h.release();
+    return r;
+}
+
+int cc_euler2d_upload(cc_handle* h, const double* rho, const double* mx, const double* my, const double* E) {
+    Euler2dBase* m = eh(h);
+    if (!m) return CC_ERR_ARG;
+    if (int r = set_dev(h)) return r;
+    const double* f[4] = {rho, mx, my, E};
+    return m->upload(f);
+}
+
+int cc_euler2d_download(cc_handle* h, double* rho, double* mx, double* my, double* E) {
+    Euler2dBase* m = eh(h);
+    if (!m) return CC_ERR_ARG;
+    if (int r = set_dev(h)) return r;
+    double* f[4] = {rho, mx, my, E};
+    return m->download(f);
+}
+
+int cc_euler2d_compute_dt(cc_handle* h, double* dt) {
+    Euler2dBase* m = eh(h);
+    if (!m || !dt) return CC_ERR_ARG;
+    if (int r = set_dev(h)) return r;
+    return m->compute_dt(dt);
+}
+
+int cc_euler2d_compute_gravity(cc_handle* h, double* gx, double* gy) {
+    Euler2dBase* m = eh(h);
+    if (!m) return CC_ERR_ARG;
+    if (int r = set_dev(h)) return r;
+    return m->gravity(gx, gy);
+}
+
+int cc_euler2d_rk2_step(cc_handle* h, double dt) {
+    Euler2dBase* m = eh(h);
+    if (!m) return CC_ERR_ARG;
+    if (!std::isfinite(dt) || dt <= 0.0) return fail(h, CC_ERR_NONFINITE, "dt not finite or not positive");
+    if (int r = set_dev(h)) return r;
+    return m->rk2_step(dt);
+}
+
+int cc_euler2d_advance(cc_handle* h, int nsteps, double* t) {
+    Euler2dBase* m = eh(h);
+    if (!m) return CC_ERR_ARG;
+    if (int r = set_dev(h)) return r;
+    return m->advance(nsteps, t);
+}
+
+int cc_euler2d_diagnostics(cc_handle* h, cc_diag* d) {
+    Euler2dBase* m = eh(h);
+    if (!m || !d) return CC_ERR_ARG;
+    if (int r = set_dev(h)) return r;
+    return m->diagnostics(d);
+}
+
+}  // extern "C"

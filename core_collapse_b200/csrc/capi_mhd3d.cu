@@ -180,6 +180,7 @@ template <class T> struct Mhd3d : Mhd3dBase {
         d.eta = p.eta;
         d.t_end = p.t_end;
         d.clamp_to_end = clamp ? 1 : 0;
+        d.seed = 1e-14; d.end_eps = 0.0; d.check = 0; d.cap = 1;
         return d;
     }
 

@@ -9,18 +9,22 @@ __global__ void m2_dt_finalize_kernel(const double* __restrict__ spd_part, int n
                                       double* __restrict__ dt_out, const double* __restrict__ t_now,
                                       int* __restrict__ active) {
     if (threadIdx.x != 0 || blockIdx.x != 0) return;
-    double maxs = 1e-14;
+    double maxs = d.seed;
     for (int b = 0; b < nparts; b++) maxs = vmax(maxs, spd_part[b]);
     const double dt_h = d.cfl * d.hmin / maxs;
-    double dt_r = 1e100;
-    if (d.eta > 0.0) dt_r = 0.25 * d.hmin * d.hmin / d.eta;
-    double dt = vmin(dt_h, dt_r);
+    double dt = dt_h;
+    if (d.cap) {
+        double dt_r = 1e100;
+        if (d.eta > 0.0) dt_r = 0.25 * d.hmin * d.hmin / d.eta;
+        dt = vmin(dt_h, dt_r);
+    }
     if (d.clamp_to_end) {
         const double t = *t_now;
-        if (!(t < d.t_end)) { *active = 0; *dt_out = 0.0; return; }
+        if (!(t < d.t_end - d.end_eps)) { active[0] = 0; *dt_out = 0.0; return; }
+        if (d.check && !(isfinite(dt) && dt > 0.0)) { active[0] = 0; active[3] = 1; *dt_out = 0.0; return; }
         if (t + dt > d.t_end) dt = d.t_end - t;
     }
-    *active = 1;
+    active[0] = 1;
     *dt_out = dt;
 }
 

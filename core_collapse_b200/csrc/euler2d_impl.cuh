@@ -1,0 +1,45 @@
+// Definitions of EHLaunch<T>; included once per precision TU.
+#pragma once
+#include "euler2d_launch.h"
+
+namespace ccb {
+
+template <class T>
+cudaError_t EHLaunch<T>::prepare() {
+    const int smem = (int)EHGeom<T>::smem;
+    cudaError_t e = cudaFuncSetAttribute(eh_stage_kernel<T, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    if (e != cudaSuccess) return e;
+    return cudaFuncSetAttribute(eh_stage_kernel<T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+}
+
+template <class T>
+cudaError_t EHLaunch<T>::stage(const EHConst<T>& c, const EHFields<T>& un, const EHFields<T>& in,
+                               const EHFields<T>& out, bool stage2, const T* phi, const double* dt, const int* active,
+                               cudaStream_t s) {
+    using G = EHGeom<T>;
+    dim3 grid((c.nx + G::TX - 1) / G::TX, (c.ny + G::TY - 1) / G::TY);
+    if (stage2) eh_stage_kernel<T, true><<<grid, G::NT, G::smem, s>>>(c, un, in, out, phi, dt, active);
+    else eh_stage_kernel<T, false><<<grid, G::NT, G::smem, s>>>(c, un, in, out, phi, dt, active);
+    return cudaGetLastError();
+}
+
+template <class T>
+cudaError_t EHLaunch<T>::speeds(const EHConst<T>& c, const EHFields<T>& st, double* spd_part, double* rho_part,
+                                cudaStream_t s) {
+    eh_speed_kernel<T, RED_NT><<<RED_BLOCKS, RED_NT, 0, s>>>(c, st, spd_part, rho_part);
+    return cudaGetLastError();
+}
+
+template <class T>
+cudaError_t EHLaunch<T>::rho_sum(const EHConst<T>& c, const T* rho, double* rho_part, cudaStream_t s) {
+    eh_rho_sum_kernel<T, RED_NT><<<RED_BLOCKS, RED_NT, 0, s>>>(c, rho, rho_part);
+    return cudaGetLastError();
+}
+
+template <class T>
+cudaError_t EHLaunch<T>::diag(const EHConst<T>& c, const EHFields<T>& st, double* part, cudaStream_t s) {
+    eh_diag_kernel<T, RED_NT><<<RED_BLOCKS, RED_NT, 0, s>>>(c, st, part);
+    return cudaGetLastError();
+}
+
+}  // namespace ccb

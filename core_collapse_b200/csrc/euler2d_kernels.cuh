@@ -1,0 +1,265 @@
+// 2D Euler + self-gravity with HLLC (euler2d_gravity_hllc.cpp, cited EH:<line>),
+// templated on T; instantiated per precision in euler2d_f64.cu / euler2d_f32.cu.
+//
+// One RK stage is one kernel.  A CTA owns a TX x TY tile of cells, builds the
+// primitives of a halo-2 region in shared memory (each from a floored copy of
+// the conserved state, EH:420-425), computes the x and y faces of its cells
+// with the reference's 4-point MUSCL-MC stencil and HLLC, and applies
+//   stage 1:  U1 = floors(U + dt rhs(U))                      (EH:530-540)
+//   stage 2:  U  = floors(0.5 U + 0.5 (U1 + dt rhs(U1)))       (EH:542-549)
+// where rhs includes the gravity source with g from the potential of the
+// stage input (EH:411, 516-523).  Stage 2 writes U in place (it reads U only
+// at its own cell).  Same pitched layout as the 2D MHD solver.
+#pragma once
+#include "mhd2d_physics.cuh"
+
+namespace ccb {
+
+template <class T> struct EHConst {
+    T gamma, gm1, floor_rho, floor_P;
+    T dx, dy, two_dx, two_dy;
+    int nx, ny, pitch;
+    AxisMap ax, ay;     // boundary rule of the fluxes
+    AxisMap pax, pay;   // the Poisson solve always wraps (EH:300-304)
+    int gravity_on;
+};
+
+template <class T> struct EHFields { T* rho; T* mx; T* my; T* E; };
+template <class T> struct EPrim { T r, u, v, P; };
+
+// enforce_floors (EH:62-72)
+template <class T>
+__device__ __forceinline__ void eh_floors(const EHConst<T>& c, T& rho, T mx, T my, T& E) {
+    rho = vmax(rho, c.floor_rho);
+    const T u = mx / rho, v = my / rho;
+    const T kin = T(0.5) * rho * (u * u + v * v);
+    const T P = c.gm1 * (E - kin);
+    if (P < c.floor_P) {
+        const T eint = c.floor_P / c.gm1;
+        E = kin + eint;
+    }
+}
+
+// cons_to_prim_full / cons_to_prim (EH:74-100); *a = sqrt(gamma P / rho)
+template <class T>
+__device__ __forceinline__ EPrim<T> eh_prim(const EHConst<T>& c, T rho, T mx, T my, T E, T* a = nullptr) {
+    const T r = vmax(rho, c.floor_rho);
+    const T u = mx / r, v = my / r;
+    const T kin = T(0.5) * r * (u * u + v * v);
+    T P = c.gm1 * (E - kin);
+    if (P < c.floor_P) P = c.floor_P;
+    if (a) *a = sqrt(c.gamma * P / r);
+    EPrim<T> W;
+    W.r = r; W.u = u; W.v = v; W.P = P;
+    return W;
+}
+
+// HLLC (EH:125-219).  DIR 0: x faces (normal u), 1: y faces (normal v).
+// Star energy uses P, not P* (EH:154, 202); SM = 0 when |den| <= 1e-14.
+template <class T, int DIR>
+__device__ __forceinline__ void eh_hllc(const EHConst<T>& c, const EPrim<T>& L, const EPrim<T>& R, T F[4]) {
+    const T aL = sqrt(c.gamma * L.P / vmax(L.r, c.floor_rho));
+    const T aR = sqrt(c.gamma * R.P / vmax(R.r, c.floor_rho));
+    const T nL = DIR == 0 ? L.u : L.v, nR = DIR == 0 ? R.u : R.v;
+    const T SL = vmin(nL - aL, nR - aR);
+    const T SR = vmax(nL + aL, nR + aR);
+    // prim_to_cons (EH:102-109)
+    const T rL = vmax(L.r, c.floor_rho), rR = vmax(R.r, c.floor_rho);
+    const T mLx = rL * L.u, mLy = rL * L.v, mRx = rR * R.u, mRy = rR * R.v;
+    const T EL = T(0.5) * rL * (L.u * L.u + L.v * L.v) + L.P / c.gm1;
+    const T ER = T(0.5) * rR * (R.u * R.u + R.v * R.v) + R.P / c.gm1;
+    const T num = (R.P - L.P) + rL * nL * (SL - nL) - rR * nR * (SR - nR);
+    const T den = rL * (SL - nL) - rR * (SR - nR);
+    const T SM = (fabs(den) > T(1e-14)) ? (num / den) : T(0.0);
+    // euler_flux_x / euler_flux_y (EH:113-123) of the chosen side
+    const bool upL = (T(0.0) <= SL), upR = !(T(0.0) <= SL) && (T(0.0) >= SR);
+    const bool left = upL || (!upR && (T(0.0) < SM));
+    const EPrim<T>& W = left ? L : R;
+    const T Ef = W.P / c.gm1 + T(0.5) * W.r * (W.u * W.u + W.v * W.v);
+    if (DIR == 0) {
+        F[0] = W.r * W.u; F[1] = W.r * W.u * W.u + W.P; F[2] = W.r * W.u * W.v; F[3] = (Ef + W.P) * W.u;
+    } else {
+        F[0] = W.r * W.v; F[1] = W.r * W.u * W.v; F[2] = W.r * W.v * W.v + W.P; F[3] = (Ef + W.P) * W.v;
+    }
+    if (upL || upR) return;
+    // star state of the chosen side (EH:147-156, 195-204)
+    const T S = left ? SL : SR;
+    const T r = left ? rL : rR, E = left ? EL : ER;
+    const T mx = left ? mLx : mRx, my = left ? mLy : mRy;
+    const T n = DIR == 0 ? W.u : W.v, t = DIR == 0 ? W.v : W.u;
+    const T rS = r * (S - n) / (S - SM);
+    const T mn = rS * SM, mt = rS * t;
+    const T ES = ((S - n) * E - W.P * n + W.P * SM) / (S - SM);
+    const T mxS = DIR == 0 ? mn : mt, myS = DIR == 0 ? mt : mn;
+    F[0] = F[0] + S * (rS - r);
+    F[1] = F[1] + S * (mxS - mx);
+    F[2] = F[2] + S * (myS - my);
+    F[3] = F[3] + S * (ES - E);
+}
+
+template <class T> struct EHTile;
+template <> struct EHTile<double> { static constexpr int TX = 32, TY = 8; };
+template <> struct EHTile<float> { static constexpr int TX = 32, TY = 16; };
+
+template <class T> struct EHGeom {
+    static constexpr int TX = EHTile<T>::TX, TY = EHTile<T>::TY, HALO = 2;
+    static constexpr int RX = TX + 2 * HALO, RY = TY + 2 * HALO, RR = RX * RY, NT = TX * TY;
+    static constexpr int NFX = (TX + 1) * TY, NGY = TX * (TY + 1);
+    static constexpr size_t smem = sizeof(T) * (size_t)(4 * RR + 4 * NFX + 4 * NGY);
+};
+
+template <class T, bool STAGE2>
+__global__ void __launch_bounds__(EHGeom<T>::NT, 2)
+eh_stage_kernel(const EHConst<T> c, const EHFields<T> un, const EHFields<T> in, const EHFields<T> out,
+                const T* __restrict__ phi, const double* __restrict__ dtp, const int* __restrict__ active) {
+    using G = EHGeom<T>;
+    constexpr int TX = G::TX, TY = G::TY, HALO = G::HALO, RX = G::RX, RR = G::RR, NT = G::NT;
+    constexpr int NFX = G::NFX, NGY = G::NGY;
+    if (active && *active == 0) return;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    T* sm = reinterpret_cast<T*>(smem_raw);
+    T* s_r = sm; T* s_u = s_r + RR; T* s_v = s_u + RR; T* s_P = s_v + RR;
+    T* fx = s_P + RR;        // 4 planes of NFX
+    T* gy = fx + 4 * NFX;    // 4 planes of NGY
+    const int tid = threadIdx.x;
+    const int i0 = blockIdx.x * TX, j0 = blockIdx.y * TY;
+    const int P = c.pitch;
+    const T dt = (T)(*dtp);
+
+    // primitives of floored copies over the halo-2 region (EH:420-425)
+    for (int k = tid; k < RR; k += NT) {
+        const int rx = k % RX, ry = k / RX;
+        const size_t q = (size_t)c.ay.cell(j0 - HALO + ry) * P + c.ax.cell(i0 - HALO + rx);
+        T rho = in.rho[q], mx = in.mx[q], my = in.my[q], E = in.E[q];
+        eh_floors(c, rho, mx, my, E);
+        const EPrim<T> W = eh_prim(c, rho, mx, my, E);
+        s_r[k] = W.r; s_u[k] = W.u; s_v[k] = W.v; s_P[k] = W.P;
+    }
+    __syncthreads();
+
+    // 4-point MUSCL-MC face states (EH:437-459): left = w0 + sL/2, right = wp - sR/2
+    auto face = [&](int km, int k0, int kp, int kpp, EPrim<T>& L, EPrim<T>& R) {
+        auto lr = [&](const T* s, T& l, T& r) {
+            const T sL = mc_slope(s[km], s[k0], s[kp]);    // mc_limiter(w0 - wm, wp - w0)
+            const T sR = mc_slope(s[k0], s[kp], s[kpp]);   // mc_limiter(wp - w0, wpp - wp)
+            l = s[k0] + T(0.5) * sL;
+            r = s[kp] - T(0.5) * sR;
+        };
+        lr(s_r, L.r, R.r); lr(s_u, L.u, R.u); lr(s_v, L.v, R.v); lr(s_P, L.P, R.P);
+        L.r = vmax(L.r, c.floor_rho); R.r = vmax(R.r, c.floor_rho);
+        L.P = vmax(L.P, c.floor_P); R.P = vmax(R.P, c.floor_P);
+    };
+    auto ridx = [&](int lx, int ly) { return (ly + HALO) * RX + (lx + HALO); };
+
+    for (int k = tid; k < NFX; k += NT) {  // x faces i0..i0+TX of rows j0..j0+TY-1
+        const int f = k % (TX + 1), r = k / (TX + 1);
+        if (i0 + f > c.nx || j0 + r >= c.ny) continue;
+        EPrim<T> L, R;
+        face(ridx(f - 2, r), ridx(f - 1, r), ridx(f, r), ridx(f + 1, r), L, R);
+        T F[4];
+        eh_hllc<T, 0>(c, L, R, F);
+        fx[k] = F[0]; fx[NFX + k] = F[1]; fx[2 * NFX + k] = F[2]; fx[3 * NFX + k] = F[3];
+    }
+    for (int k = tid; k < NGY; k += NT) {  // y faces j0..j0+TY of columns i0..i0+TX-1
+        const int col = k % TX, g = k / TX;
+        if (j0 + g > c.ny || i0 + col >= c.nx) continue;
+        EPrim<T> L, R;
+        face(ridx(col, g - 2), ridx(col, g - 1), ridx(col, g), ridx(col, g + 1), L, R);
+        T F[4];
+        eh_hllc<T, 1>(c, L, R, F);
+        gy[k] = F[0]; gy[NGY + k] = F[1]; gy[2 * NGY + k] = F[2]; gy[3 * NGY + k] = F[3];
+    }
+    __syncthreads();
+
+    const int tx = tid % TX, ty = tid / TX;
+    const int gi = i0 + tx, gj = j0 + ty;
+    if (gi >= c.nx || gj >= c.ny) return;
+    const size_t q = (size_t)gj * P + gi;
+    // rhs (EH:503-524): flux divergence, then the gravity source with the raw state
+    const int kx = ty * (TX + 1) + tx, ky = ty * TX + tx;
+    T d[4];
+#pragma unroll
+    for (int m = 0; m < 4; m++)
+        d[m] = -(fx[m * NFX + kx + 1] - fx[m * NFX + kx]) / c.dx - (gy[m * NGY + ky + TX] - gy[m * NGY + ky]) / c.dy;
+    const T r0 = in.rho[q], mx0 = in.mx[q], my0 = in.my[q], E0 = in.E[q];
+    if (c.gravity_on) {
+        const int iE = c.pax.cell(gi + 1), iW = c.pax.cell(gi - 1);
+        const int jN = c.pay.cell(gj + 1), jS = c.pay.cell(gj - 1);
+        const T gxq = -(phi[(size_t)gj * P + iE] - phi[(size_t)gj * P + iW]) / c.two_dx;
+        const T gyq = -(phi[(size_t)jN * P + gi] - phi[(size_t)jS * P + gi]) / c.two_dy;
+        const T rho = vmax(r0, c.floor_rho);
+        const T u = mx0 / rho, v = my0 / rho;
+        d[1] += rho * gxq;
+        d[2] += rho * gyq;
+        d[3] += rho * (u * gxq + v * gyq);
+    }
+    T rho, mx, my, E;
+    if (!STAGE2) {
+        rho = r0 + dt * d[0]; mx = mx0 + dt * d[1]; my = my0 + dt * d[2]; E = E0 + dt * d[3];
+    } else {
+        rho = T(0.5) * un.rho[q] + T(0.5) * (r0 + dt * d[0]);
+        mx = T(0.5) * un.mx[q] + T(0.5) * (mx0 + dt * d[1]);
+        my = T(0.5) * un.my[q] + T(0.5) * (my0 + dt * d[2]);
+        E = T(0.5) * un.E[q] + T(0.5) * (E0 + dt * d[3]);
+    }
+    eh_floors(c, rho, mx, my, E);
+    out.rho[q] = rho; out.mx[q] = mx; out.my[q] = my; out.E[q] = E;
+}
+
+// CFL speeds (EH:396-402) and the floored-density sum the Poisson mean needs
+// (EH:309-317), FP64 block partials.
+template <class T, int NT>
+__global__ void __launch_bounds__(NT)
+eh_speed_kernel(const EHConst<T> c, const EHFields<T> s, double* __restrict__ spd_part, double* __restrict__ rho_part) {
+    __shared__ double sh[NT / 32];
+    double smax = 0.0, rsum = 0.0;
+    const int ncell = c.nx * c.ny;
+    for (int k = blockIdx.x * NT + threadIdx.x; k < ncell; k += gridDim.x * NT) {
+        const int i = k % c.nx, j = k / c.nx;
+        const size_t q = (size_t)j * c.pitch + i;
+        T a;
+        const EPrim<T> W = eh_prim(c, s.rho[q], s.mx[q], s.my[q], s.E[q], &a);
+        const double sx = (double)(fabs(W.u) + a), sy = (double)(fabs(W.v) + a);
+        if (sx > smax) smax = sx;   // std::max(maxs, x) never keeps a NaN
+        if (sy > smax) smax = sy;
+        rsum += (double)vmax(s.rho[q], c.floor_rho);
+    }
+    const double bm = block_max<NT>(smax, sh);
+    const double bs = block_sum<NT>(rsum, sh);
+    if (threadIdx.x == 0) { spd_part[blockIdx.x] = bm; rho_part[blockIdx.x] = bs; }
+}
+
+template <class T, int NT>
+__global__ void __launch_bounds__(NT)
+eh_rho_sum_kernel(const EHConst<T> c, const T* __restrict__ rho, double* __restrict__ rho_part) {
+    __shared__ double sh[NT / 32];
+    double rsum = 0.0;
+    const int ncell = c.nx * c.ny;
+    for (int k = blockIdx.x * NT + threadIdx.x; k < ncell; k += gridDim.x * NT)
+        rsum += (double)vmax(rho[(size_t)(k / c.nx) * c.pitch + (k % c.nx)], c.floor_rho);
+    const double bs = block_sum<NT>(rsum, sh);
+    if (threadIdx.x == 0) rho_part[blockIdx.x] = bs;
+}
+
+template <class T, int NT>
+__global__ void __launch_bounds__(NT) eh_diag_kernel(const EHConst<T> c, const EHFields<T> s, double* __restrict__ part) {
+    __shared__ double sh[NT / 32];
+    double acc[4] = {0, 0, 0, 0}, nonf = 0.0;
+    const int ncell = c.nx * c.ny;
+    for (int k = blockIdx.x * NT + threadIdx.x; k < ncell; k += gridDim.x * NT) {
+        const size_t q = (size_t)(k / c.nx) * c.pitch + (k % c.nx);
+        const double v[4] = {(double)s.rho[q], (double)s.mx[q], (double)s.my[q], (double)s.E[q]};
+        for (int m = 0; m < 4; m++) {
+            acc[m] += v[m];
+            if (!isfinite(v[m])) nonf = 1.0;
+        }
+    }
+    for (int m = 0; m < 4; m++) {
+        const double b = block_sum<NT>(acc[m], sh);
+        if (threadIdx.x == 0) part[m * gridDim.x + blockIdx.x] = b;
+    }
+    const double bn = block_max<NT>(nonf, sh);
+    if (threadIdx.x == 0) part[4 * gridDim.x + blockIdx.x] = bn;
+}
+
+}  // namespace ccb

@@ -1,0 +1,23 @@
+// Host-side launchers of the 2D Euler/HLLC kernels, defined once per precision
+// in euler2d_f64.cu (-fmad=false, the parity path) and euler2d_f32.cu.
+#pragma once
+#include <cuda_runtime.h>
+
+#include "euler2d_kernels.cuh"
+#include "mhd2d_launch.h"
+
+namespace ccb {
+
+template <class T> struct EHLaunch {
+    static cudaError_t prepare();
+    // stage 1: out = floors(in + dt rhs(in)); stage 2: out = floors(0.5 un + 0.5 (in + dt rhs(in)))
+    static cudaError_t stage(const EHConst<T>& c, const EHFields<T>& un, const EHFields<T>& in,
+                             const EHFields<T>& out, bool stage2, const T* phi, const double* dt, const int* active,
+                             cudaStream_t s);
+    static cudaError_t speeds(const EHConst<T>& c, const EHFields<T>& st, double* spd_part, double* rho_part,
+                              cudaStream_t s);
+    static cudaError_t rho_sum(const EHConst<T>& c, const T* rho, double* rho_part, cudaStream_t s);
+    static cudaError_t diag(const EHConst<T>& c, const EHFields<T>& st, double* part, cudaStream_t s);
+};
+
+}  // namespace ccb

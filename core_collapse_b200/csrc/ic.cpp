@@ -176,4 +176,41 @@ int cc_ic_mhd2d_orszag_tang(const cc_mhd2d_params* p, double core_amp, double co
     return 0;
 }
 
+int cc_ic_euler2d_random_blob(const cc_euler2d_params* p, double* const* f) {
+    if (!p || !f || p->Nx < 1 || p->Ny < 1 || !f[0] || !f[1] || !f[2] || !f[3]) return -1;
+    const int nx = p->Nx, ny = p->Ny;
+    const double dx = (p->x1 - p->x0) / nx, dy = (p->y1 - p->y0) / ny;
+    std::mt19937 rng(42);
+    std::uniform_real_distribution<double> uni01(0.0, 1.0);
+    std::uniform_real_distribution<double> uniV(-1.0, 1.0);
+    const double rho0 = 1.0, P0 = 1.0, amp_rho = 0.10, amp_P = 0.10, vmax = 0.05;
+    const double xc = 0.5 * (p->x0 + p->x1), yc = 0.5 * (p->y0 + p->y1);
+    const double sigma = 0.08, bump_amp = 0.5;
+    const double gm1 = p->gamma - 1.0;
+    for (int j = 0; j < ny; ++j) {
+        const double y = p->y0 + (j + 0.5) * dy;
+        for (int i = 0; i < nx; ++i) {
+            const double x = p->x0 + (i + 0.5) * dx;
+            const size_t k = (size_t)j * nx + i;
+            const double fr = 2.0 * uni01(rng) - 1.0;
+            const double fp = 2.0 * uni01(rng) - 1.0;
+            double rho = rho0 * (1.0 + amp_rho * fr);
+            double P = P0 * (1.0 + amp_P * fp);
+            const double rx = x - xc, ry = y - yc, r2 = rx * rx + ry * ry;
+            rho += bump_amp * rho0 * std::exp(-r2 / (2.0 * sigma * sigma));
+            const double u = vmax * uniV(rng);
+            const double v = vmax * uniV(rng);
+            rho = vmaxd(rho, p->floor_rho);
+            P = vmaxd(P, p->floor_P);
+            double r = rho, mx = rho * u, my = rho * v, E = P / gm1 + 0.5 * rho * (u * u + v * v);
+            // enforce_floors (EH:62-72)
+            r = vmaxd(r, p->floor_rho);
+            const double uu = mx / r, vv = my / r, kin = 0.5 * r * (uu * uu + vv * vv);
+            if (gm1 * (E - kin) < p->floor_P) E = kin + p->floor_P / gm1;
+            f[0][k] = r; f[1][k] = mx; f[2][k] = my; f[3][k] = E;
+        }
+    }
+    return 0;
+}
+
 }  // extern "C"

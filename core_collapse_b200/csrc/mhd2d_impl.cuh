@@ -120,9 +120,9 @@ cudaError_t M2Launch<T>::fft_solve(const T* rho, int pitch, const double* rho_pa
 
 template <class T>
 cudaError_t M2Launch<T>::sor_rhs(const T* rho, int nx, int ny, int pitch, const double* rho_part, double fourpiG,
-                                 double* rhs, const int* active, cudaStream_t s) {
+                                 double floor_rho, double* rhs, const int* active, cudaStream_t s) {
     sor_rhs_kernel<T><<<grid_for((size_t)nx * ny, 256, 2048), 256, 0, s>>>(rho, nx, ny, pitch, rho_part, RED_BLOCKS,
-                                                                          fourpiG, rhs, active);
+                                                                          fourpiG, floor_rho, rhs, active);
     return cudaGetLastError();
 }
 

@@ -420,6 +420,10 @@ m2_diag_kernel(const M2Const<T> c, const Fields<T> s, double* __restrict__ part 
 struct DtSpec {
     double cfl, hmin, eta, t_end;
     int clamp_to_end;
+    double seed;      // initial value of the speed maximum (M2/M3: 1e-14, EH: 1e-30)
+    double end_eps;   // loop runs while t < t_end - end_eps (M2/M3: 0, EH: 1e-14)
+    int check;        // 1: flag a non-finite or non-positive dt (EH:699-702)
+    int cap;          // 1: dt = min(dt_h, dt_r), dt_r = 1e100 or the resistive limit (M2:592-597, M3:643-647)
 };
 
 // Host <-> device layout conversion: contiguous FP64 reference layout with row

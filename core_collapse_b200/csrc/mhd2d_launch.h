@@ -32,7 +32,7 @@ template <class T> struct M2Launch {
                                  const Cplx<T>* twy_i, double Lx, double Ly, double G, Cplx<T>* A, T* phi,
                                  const int* active, cudaStream_t s);
     static cudaError_t sor_rhs(const T* rho, int nx, int ny, int pitch, const double* rho_part, double fourpiG,
-                               double* rhs, const int* active, cudaStream_t s);
+                               double floor_rho, double* rhs, const int* active, cudaStream_t s);
     static cudaError_t phi_to_field(const double* phi, int nx, int ny, T* out, int pitch, const int* active,
                                     cudaStream_t s);
     static cudaError_t gravity_from_phi(const T* phi, int nx, int ny, int pitch, AxisMap ax, AxisMap ay, T two_dx,

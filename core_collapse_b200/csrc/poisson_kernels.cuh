@@ -250,9 +250,12 @@ __global__ void __launch_bounds__(NT) sor_rb_kernel(SorArgs a) {
 }
 
 // rhs = 4 pi G (rho - mean) (M2:187-194), mean from the density partial sums.
+// floor_rho >= 0: the density is floored first (EH:312), and the partial sums
+// must then be sums of the floored density.
 template <class T>
 __global__ void sor_rhs_kernel(const T* __restrict__ rho, int nx, int ny, int pitch, const double* __restrict__ rho_part,
-                               int nparts, double fourpiG, double* __restrict__ rhs, const int* __restrict__ active) {
+                               int nparts, double fourpiG, double floor_rho, double* __restrict__ rhs,
+                               const int* __restrict__ active) {
     if (active && *active == 0) return;
     __shared__ double s_mean;
     if (threadIdx.x == 0) {
@@ -265,7 +268,9 @@ __global__ void sor_rhs_kernel(const T* __restrict__ rho, int nx, int ny, int pi
     const int N = nx * ny;
     for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < N; k += gridDim.x * blockDim.x) {
         const int i = k % nx, j = k / nx;
-        rhs[k] = fourpiG * ((double)rho[(size_t)j * pitch + i] - mean);
+        double r = (double)rho[(size_t)j * pitch + i];
+        if (floor_rho >= 0.0) r = vmax(r, floor_rho);
+        rhs[k] = fourpiG * (r - mean);
     }
 }
 

@@ -45,6 +45,12 @@ int cc_ic_mhd2d_collapse(const cc_mhd2d_params* p, double core_amp, double core_
  *   B0 = 1/sqrt(4 pi) on corners (div B = 0 to roundoff). */
 int cc_ic_mhd2d_orszag_tang(const cc_mhd2d_params* p, double core_amp, double core_width, double* const* f);
 
+/* The Euler/HLLC main()'s IC, init_random_blob (euler2d_gravity_hllc.cpp:574-642):
+ * std::mt19937(42), per cell two uniform(0,1) draws (density and pressure
+ * noise) then two uniform(-1,1) draws (velocity); Gaussian density bump.
+ * f = {rho, mx, my, E}. */
+int cc_ic_euler2d_random_blob(const cc_euler2d_params* p, double* const* f);
+
 #ifdef __cplusplus
 }
 #endif

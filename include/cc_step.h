@@ -231,6 +231,28 @@ int cc_mhd3d_advance(cc_handle* h, int nsteps, double* t);
 /* FP64 sums and max |div B| (mhd3d_resistive_hlld_ct.cpp:1070-1078) */
 int cc_mhd3d_diagnostics(cc_handle* h, cc_diag* d);
 
+/* ---- 2D Euler + self-gravity, HLLC (euler2d_gravity_hllc.cpp) ---- */
+
+/* Fill with the reference defaults (euler2d_gravity_hllc.cpp:29-56, 329-331). */
+void cc_euler2d_params_default(cc_euler2d_params* p);
+int cc_euler2d_create(const cc_euler2d_params* p, cc_handle** out);
+/* State {rho,mx,my,E}: EH:58-60 */
+int cc_euler2d_upload(cc_handle* h, const double* rho, const double* mx, const double* my, const double* E);
+int cc_euler2d_download(cc_handle* h, double* rho, double* mx, double* my, double* E);
+/* compute_dt(p, U) (euler2d_gravity_hllc.cpp:390-404) */
+int cc_euler2d_compute_dt(cc_handle* h, double* dt);
+/* compute_poisson_gravity_periodic(p, U) (euler2d_gravity_hllc.cpp:288-386) on the
+ * resident state; gx/gy (Nx*Ny) may be NULL. */
+int cc_euler2d_compute_gravity(cc_handle* h, double* gx, double* gy);
+/* rk2_step(p, U, dt) (euler2d_gravity_hllc.cpp:529-550); the right-hand side
+ * solves Poisson itself, on U and on the stage-1 state (EH:411). */
+int cc_euler2d_rk2_step(cc_handle* h, double dt);
+/* nsteps of the main() loop body (euler2d_gravity_hllc.cpp:697-706) on the
+ * device; returns CC_ERR_NONFINITE if dt is not finite or not positive (where
+ * the reference aborts, EH:699-702), the state then being the last good one. */
+int cc_euler2d_advance(cc_handle* h, int nsteps, double* t);
+int cc_euler2d_diagnostics(cc_handle* h, cc_diag* d);
+
 /* ---- spectral gravity without device allocation ----
  * No counterpart in the reference: an addition for callers that cannot call
  * cudaMalloc -- a host application whose memory manager owns the GPU's

@@ -11,6 +11,7 @@
 #include "../include/cc_step.h"
 #include "mhd2d_oracle.hpp"
 #include "mhd3d_oracle.hpp"
+#include "euler2d_oracle.hpp"
 #include "poisson_oracle.hpp"
 
 namespace {
@@ -112,6 +113,57 @@ template <class T> int main_loop3(const cc_mhd3d_params* c, double* const* f, in
     store3(s, f);
     if (t) *t = tt;
     return 0;
+}
+
+EHPar ehpar(const cc_euler2d_params* c) {
+    EHPar p;
+    p.gamma = c->gamma; p.cfl = c->cfl;
+    p.x0 = c->x0; p.x1 = c->x1; p.y0 = c->y0; p.y1 = c->y1;
+    p.nx = c->Nx; p.ny = c->Ny;
+    p.floor_rho = c->floor_rho; p.floor_P = c->floor_P;
+    p.px = c->periodic_x != 0; p.py = c->periodic_y != 0;
+    p.gravity = c->gravity_on != 0;
+    return p;
+}
+
+// EH's Poisson: floored density, always periodic (EH:300-323)
+PoissonSpec ehspec(const cc_euler2d_params* c) {
+    PoissonSpec s;
+    s.nx = c->Nx; s.ny = c->Ny; s.px = true; s.py = true;
+    s.dx = (c->x1 - c->x0) / c->Nx; s.dy = (c->y1 - c->y0) / c->Ny;
+    s.G = c->G; s.omega = c->sor_omega; s.max_iter = c->sor_max_iter; s.tol = c->sor_tol;
+    s.floor_density = true; s.floor_rho = c->floor_rho;
+    s.Lx = c->x1 - c->x0; s.Ly = c->y1 - c->y0;
+    return s;
+}
+
+PoissonResult eh_gravity(const cc_euler2d_params* c, const std::vector<double>& rho, std::vector<double>& gx,
+                         std::vector<double>& gy, int mode) {
+    PoissonSpec s = ehspec(c);
+    PoissonResult r;
+    size_t N = (size_t)c->Nx * c->Ny;
+    if (!c->gravity_on) { gx.assign(N, 0.0); gy.assign(N, 0.0); return r; }
+    std::vector<double> phi;
+    if (mode == 2) {
+        std::vector<double> fr(rho.begin(), rho.end());
+        for (auto& v : fr) v = vmax(v, c->floor_rho);
+        fft_periodic(s, fr, phi);
+    } else {
+        std::vector<double> rhs = poisson_rhs(s, rho);
+        r = mode == 0 ? sor_lexicographic(s, rhs, phi) : sor_red_black(s, rhs, phi);
+    }
+    gravity_from_phi(s, phi, gx, gy);
+    return r;
+}
+
+template <class T> void loadE(const cc_euler2d_params* c, const double* const* f, EHState<T>& s) {
+    size_t N = (size_t)c->Nx * c->Ny;
+    s.rho.assign(f[0], f[0] + N); s.mx.assign(f[1], f[1] + N); s.my.assign(f[2], f[2] + N); s.E.assign(f[3], f[3] + N);
+}
+template <class T> void storeE(const EHState<T>& s, double* const* f) {
+    const std::vector<T>* v[4] = {&s.rho, &s.mx, &s.my, &s.E};
+    for (int k = 0; k < 4; k++)
+        for (size_t q = 0; q < v[k]->size(); q++) f[k][q] = (double)(*v[k])[q];
 }
 
 template <class T> std::vector<T> cast(const std::vector<double>& v) { return std::vector<T>(v.begin(), v.end()); }
@@ -249,6 +301,74 @@ double or_mhd3d_divB_max(const cc_mhd3d_params* c, const double* const* f) {
     M3State<double> s;
     load3(c, f, s);
     return M3<double>(m3par(c)).max_divB(s);
+}
+
+// ---- 2D Euler + gravity, HLLC (euler2d_gravity_hllc.cpp) ----
+int or_euler2d_gravity(const cc_euler2d_params* c, const double* rho, double* gx, double* gy, int mode, int* iters,
+                       double* residual) {
+    std::vector<double> r(rho, rho + (size_t)c->Nx * c->Ny), x, y;
+    PoissonResult res = eh_gravity(c, r, x, y, mode);
+    std::memcpy(gx, x.data(), x.size() * sizeof(double));
+    std::memcpy(gy, y.data(), y.size() * sizeof(double));
+    if (iters) *iters = res.iters;
+    if (residual) *residual = res.residual;
+    return 0;
+}
+
+int or_euler2d_rhs(const cc_euler2d_params* c, const double* const* f, double* const* dU, int mode) {
+    EHState<double> s;
+    loadE(c, f, s);
+    std::vector<double> gx, gy;
+    eh_gravity(c, s.rho, gx, gy, mode);
+    EHState<double> d = EH<double>(ehpar(c)).rhs(s, gx, gy);
+    storeE(d, dU);
+    return 0;
+}
+
+double or_euler2d_compute_dt(const cc_euler2d_params* c, const double* const* f) {
+    EHState<double> s;
+    loadE(c, f, s);
+    return EH<double>(ehpar(c)).compute_dt(s);
+}
+
+int or_euler2d_rk2_step(const cc_euler2d_params* c, double* const* f, double dt, int mode) {
+    EHState<double> s;
+    loadE(c, f, s);
+    auto grav = [&](const EHState<double>& U, std::vector<double>& gx, std::vector<double>& gy) {
+        eh_gravity(c, U.rho, gx, gy, mode);
+    };
+    EH<double>(ehpar(c)).rk2_step(s, dt, grav);
+    storeE(s, f);
+    return 0;
+}
+
+// main() loop body (EH:697-706) in double (fp32 == 0) or float; returns
+// CC_ERR_NONFINITE on a bad dt like the reference's abort (EH:699-702)
+int or_euler2d_main_loop(const cc_euler2d_params* c, double* const* f, int nsteps, double* t, int mode, int fp32) {
+    auto run = [&](auto tag) -> int {
+        using T = decltype(tag);
+        EHState<T> s;
+        loadE(c, f, s);
+        EH<T> m(ehpar(c));
+        auto grav = [&](const EHState<T>& U, std::vector<T>& gx, std::vector<T>& gy) {
+            std::vector<double> x, y;
+            eh_gravity(c, widen(U.rho), x, y, mode);
+            gx = cast<T>(x); gy = cast<T>(y);
+        };
+        double tt = t ? *t : 0.0;
+        int rc = 0;
+        for (int n = 0; n < nsteps && tt < c->t_end - 1e-14; ++n) {
+            double dt = m.compute_dt(s);
+            if (!std::isfinite(dt) || dt <= 0.0) { rc = CC_ERR_NONFINITE; break; }
+            if (tt + dt > c->t_end) dt = c->t_end - tt;
+            m.rk2_step(s, T(dt), grav);
+            tt += dt;
+        }
+        storeE(s, f);
+        if (t) *t = tt;
+        return rc;
+    };
+    return fp32 ? run(0.0f) : run(0.0);
 }
 
 // Gravity of a density field with every Poisson knob explicit (used to pin the

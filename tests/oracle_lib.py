@@ -50,6 +50,13 @@ def oracle() -> C.CDLL:
         O.or_mhd2d_divB_max.argtypes = [P2, _PP]
         O.or_mhd2d_divB_max.restype = C.c_double
         O.or_fft1d.argtypes = [C.c_int, _DP, C.c_int]
+        PE = C.POINTER(L.CcEuler2dParams)
+        O.or_euler2d_gravity.argtypes = [PE, _DP, _DP, _DP, C.c_int, C.POINTER(C.c_int), _DP]
+        O.or_euler2d_rhs.argtypes = [PE, _PP, _PP, C.c_int]
+        O.or_euler2d_compute_dt.argtypes = [PE, _PP]
+        O.or_euler2d_compute_dt.restype = C.c_double
+        O.or_euler2d_rk2_step.argtypes = [PE, _PP, C.c_double, C.c_int]
+        O.or_euler2d_main_loop.argtypes = [PE, _PP, C.c_int, _DP, C.c_int, C.c_int]
         P3 = C.POINTER(L.CcMhd3dParams)
         O.or_mhd3d_advance_stage.argtypes = [P3, _PP, _PP, C.c_double]
         O.or_mhd3d_rk2_step.argtypes = [P3, _PP, C.c_double]
@@ -203,3 +210,12 @@ def m3_main_loop_oracle(cp, S, nsteps, fp32=False, t0=0.0):
     t = C.c_double(t0)
     oracle().or_mhd3d_main_loop(C.byref(cp), pp(out), nsteps, C.byref(t), 1 if fp32 else 0)
     return out, t.value
+
+
+# ---- 2D Euler helpers: [rho, mx, my, E] ----
+
+def eh_main_loop_oracle(cp, S, nsteps, mode, fp32=False, t0=0.0):
+    out = copy_state(S)
+    t = C.c_double(t0)
+    rc = oracle().or_euler2d_main_loop(C.byref(cp), pp(out), nsteps, C.byref(t), mode, 1 if fp32 else 0)
+    return out, t.value, rc

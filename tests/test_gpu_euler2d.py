@@ -1,0 +1,140 @@
+"""GPU parity of the 2D Euler/HLLC step (libcc_b200 through its C ABI)
+against the CPU oracle (pinned bit-for-bit to euler2d_gravity_hllc.cpp).
+
+Without gravity the FP64 step is bit-identical.  With gravity the GPU runs
+red-black SOR (the oracle's red-black restatement is the reference): with a
+fixed sweep count the only difference is the FP64 mean-reduction order
+(relative L-inf <= 1e-12); with the residual tolerance the stopping sweep may
+differ by one or two, bounded by the tolerance (<= 1e-8)."""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+import oracle_lib as O
+from cases_euler2d import CASES_EH, make_case_eh
+from core_collapse_b200 import _lib as L
+from core_collapse_b200.euler2d import Euler2dSolver, ParamsEH, ic_random_blob
+from core_collapse_b200.mhd2d import CcError
+
+pytestmark = pytest.mark.gpu
+
+
+def _fixed_sweeps(p: ParamsEH, n=150):
+    p.sor_tol = 0.0
+    p.sor_max_iter = n
+    return p
+
+
+def _close(got, want, tol):
+    for k, (a, b) in enumerate(zip(got, want)):
+        r = O.rel_linf(a, b)
+        assert r <= tol, f"field {k}: rel L-inf {r:.3e} > {tol:.1e}"
+
+
+@pytest.mark.parametrize("name", sorted(CASES_EH))
+def test_roundtrip_and_dt_bitwise(name):
+    p, s = make_case_eh(name)
+    cp = p.to_c()
+    S = [a.copy() for a in s.arrays()]
+    want = O.oracle().or_euler2d_compute_dt(C.byref(cp), O.pp(S))
+    with Euler2dSolver(p) as g:
+        g.upload(s)
+        got = g.download()
+        assert g.compute_dt() == want
+    for a, b in zip(got.arrays(), S):
+        assert np.array_equal(a, b)
+
+
+@pytest.mark.parametrize("name", sorted(CASES_EH))
+def test_rk2_step_parity(name):
+    p, s = make_case_eh(name)
+    _fixed_sweeps(p)
+    cp = p.to_c()
+    S = [a.copy() for a in s.arrays()]
+    dt = O.oracle().or_euler2d_compute_dt(C.byref(cp), O.pp(S))
+    want = O.copy_state(S)
+    O.oracle().or_euler2d_rk2_step(C.byref(cp), O.pp(want), dt, 1)
+    with Euler2dSolver(p) as g:
+        g.upload(s)
+        g.rk2_step(dt)
+        got = g.download().arrays()
+    if not p.gravity_on:
+        for a, b in zip(got, want):
+            assert np.array_equal(a, b)
+    _close(got, want, 1e-12)
+
+
+def test_gravity_with_tolerance_matches_red_black_oracle():
+    p, s = make_case_eh("periodic_grav")
+    cp = p.to_c()
+    n = p.Nx * p.Ny
+    gx, gy = np.zeros(n), np.zeros(n)
+    it, res = C.c_int(), C.c_double()
+    O.oracle().or_euler2d_gravity(C.byref(cp), O.dp(s.rho), O.dp(gx), O.dp(gy), 1, C.byref(it), C.byref(res))
+    with Euler2dSolver(p) as g:
+        g.upload(s)
+        x, y = g.compute_gravity()
+        d = g.diagnostics()
+    assert abs(d["poisson_iters"] - it.value) <= 2 and d["poisson_residual"] < p.sor_tol
+    assert O.rel_linf(x, gx) <= 1e-8 and O.rel_linf(y, gy) <= 1e-8
+
+
+@pytest.mark.parametrize("name", sorted(CASES_EH))
+def test_advance_matches_main_loop(name):
+    p, s = make_case_eh(name)
+    _fixed_sweeps(p)
+    p.t_end = 10.0
+    cp = p.to_c()
+    want, t_want, rc = O.eh_main_loop_oracle(cp, [a.copy() for a in s.arrays()], 4, mode=1)
+    assert rc == 0
+    with Euler2dSolver(p) as g:
+        g.upload(s)
+        t = g.advance(4, 0.0)
+        got = g.download().arrays()
+        d = g.diagnostics()
+    assert d["steps"] == 4
+    if not p.gravity_on:
+        assert t == t_want
+        for a, b in zip(got, want):
+            assert np.array_equal(a, b)
+    else:
+        assert abs(t - t_want) <= 1e-12 * t_want
+        _close(got, want, 1e-12)
+
+
+def test_reference_ic_loop_and_mass():
+    """The reference's own main(): random-blob IC, SOR to 1e-10, 3 steps;
+    mass (periodic, floors idle) conserved to roundoff."""
+    p = ParamsEH(Nx=32, Ny=32, t_end=10.0)
+    U = ic_random_blob(p)
+    cp = p.to_c()
+    want, t_want, rc = O.eh_main_loop_oracle(cp, [a.copy() for a in U.arrays()], 3, mode=1)
+    with Euler2dSolver(p) as g:
+        g.upload(U)
+        d0 = g.diagnostics()
+        t = g.advance(3, 0.0)
+        d1 = g.diagnostics()
+        got = g.download().arrays()
+    assert abs(t - t_want) <= 1e-9 * t_want
+    _close(got, want, 1e-8)
+    assert abs(d1["mass"] - d0["mass"]) <= 1e-13 * d0["mass"]
+
+
+def test_bad_dt_stops_the_loop():
+    """An infinite momentum makes dt = 0: the reference aborts (EH:699-702),
+    the device loop stops with CC_ERR_NONFINITE and keeps the last good state."""
+    p, s = make_case_eh("mixed_nograv")
+    s.mx[5] = np.inf
+    p.t_end = 10.0
+    rc_or = O.eh_main_loop_oracle(p.to_c(), [a.copy() for a in s.arrays()], 3, mode=1)[2]
+    assert rc_or == L.CC_ERR_NONFINITE
+    with Euler2dSolver(p) as g:
+        g.upload(s)
+        with pytest.raises(CcError) as e:
+            g.advance(3, 0.0)
+        assert e.value.code == L.CC_ERR_NONFINITE
+        d = g.diagnostics()
+        assert d["steps"] == 0
+        back = g.download()
+    assert np.array_equal(back.rho, s.rho)
