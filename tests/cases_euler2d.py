@@ -10,8 +10,9 @@ from core_collapse_b200.euler2d import ParamsEH, StateEH
 
 CASES_EH = {
     "periodic_grav": (dict(Nx=12, Ny=10, periodic_x=True, periodic_y=True, gravity_on=True, G=1.0), 1),
-    "outflow_grav": (dict(Nx=9, Ny=8, periodic_x=False, periodic_y=False, gravity_on=True, G=2.0), 2),
+    "outflow_grav": (dict(Nx=10, Ny=8, periodic_x=False, periodic_y=False, gravity_on=True, G=2.0), 2),
     "mixed_nograv": (dict(Nx=8, Ny=12, periodic_x=True, periodic_y=False, gravity_on=False), 3),
+    "outflow_odd_nograv": (dict(Nx=9, Ny=7, periodic_x=False, periodic_y=False, gravity_on=False), 4),
 }
 
 

@@ -138,3 +138,13 @@ def test_bad_dt_stops_the_loop():
         assert d["steps"] == 0
         back = g.download()
     assert np.array_equal(back.rho, s.rho)
+
+
+def test_odd_extent_with_gravity_is_rejected():
+    """The red-black SOR colouring needs even extents on its (always periodic)
+    axes; an odd grid with gravity is refused at create time, not mis-solved."""
+    p, _ = make_case_eh("outflow_odd_nograv")
+    p.gravity_on = True
+    with pytest.raises(CcError) as e:
+        Euler2dSolver(p)
+    assert e.value.code == L.CC_ERR_UNSUPPORTED
