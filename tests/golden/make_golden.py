@@ -1,0 +1,148 @@
+"""Generate the golden fixtures of tests/golden/ from the compiled reference.
+
+The reference solvers (mhd2d_resistive_hlld_ct_gravity.cpp,
+mhd3d_resistive_hlld_ct.cpp, euler2d_gravity_hllc.cpp and the FFT Poisson of
+navier_stokes_2d_hllc_poisson.cpp) are compiled in place into oracle/_ref/ by
+oracle/Makefile.  This script runs them on the seeded cases of
+tests/cases_*.py and stores inputs and reference outputs as .npz files, so
+that tests/test_golden.py can pin the CPU oracle to the reference on a
+machine without the reference tree.  Every stored output is the reference's
+own result; nothing here is computed by the oracle or the library.
+
+    python tests/golden/make_golden.py          (from the repository root)
+"""
+from __future__ import annotations
+
+import ctypes as C
+import dataclasses
+import json
+import sys
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+sys.path[:0] = [str(HERE.parent.parent), str(HERE.parent)]
+
+import oracle_lib as O  # noqa: E402
+from cases_euler2d import CASES_EH, make_case_eh  # noqa: E402
+from cases_mhd2d import CASES, make_case  # noqa: E402
+from cases_mhd3d import CASES3, make_case3  # noqa: E402
+
+MAIN_LOOP_STEPS = 3
+
+
+def _params_json(kind: str, p) -> np.ndarray:
+    return np.array(json.dumps({"kind": kind, "fields": dataclasses.asdict(p)}))
+
+
+def _save(name: str, **arrays):
+    np.savez_compressed(HERE / f"{name}.npz", **arrays)
+
+
+def _state(prefix: str, S) -> dict:
+    return {f"{prefix}{k}": np.asarray(a).copy() for k, a in enumerate(S)}
+
+
+def mhd2d():
+    R = O.ref("mhd2d")
+    for name in sorted(CASES):
+        p, U, B = make_case(name)
+        cp = p.to_c()
+        S = O.state_list(U, B)
+        n = p.Nx * p.Ny
+        gx, gy = np.zeros(n), np.zeros(n)
+        if p.gravity_on:
+            R.ref_mhd2d_poisson(C.byref(cp), O.dp(S[0]), O.dp(gx), O.dp(gy))
+        dt = R.ref_mhd2d_compute_dt(C.byref(cp), O.pp(S))
+        stage = O.m2_stage_ref(cp, S, gx, gy, dt)
+        step = O.m2_rk2_ref(cp, S, gx, gy, dt)
+        loop = O.copy_state(S)
+        cp.t_end = 10.0
+        t = C.c_double(0.0)
+        R.ref_mhd2d_main_loop(C.byref(cp), O.pp(loop), MAIN_LOOP_STEPS, C.byref(t))
+        divb = R.ref_mhd2d_divB_max(C.byref(cp), O.pp(loop))
+        _save(f"mhd2d_{name}", params=_params_json("mhd2d", p), gx=gx, gy=gy, dt=np.float64(dt),
+              loop_t=np.float64(t.value), loop_divb=np.float64(divb),
+              **_state("in", S), **_state("stage", stage), **_state("step", step), **_state("loop", loop))
+
+
+def mhd3d():
+    R = O.ref("mhd3d")
+    for name in sorted(CASES3):
+        p, s = make_case3(name)
+        cp = p.to_c()
+        S = [a.copy() for a in s.arrays()]
+        dt = R.ref_mhd3d_compute_dt(C.byref(cp), O.pp(S))
+        stage = O.copy_state(S)
+        R.ref_mhd3d_advance_stage(C.byref(cp), O.pp(S), O.pp(stage), dt)
+        step = O.m3_rk2_ref(cp, S, dt)
+        loop = O.copy_state(S)
+        cp.t_end = 10.0
+        t = C.c_double(0.0)
+        R.ref_mhd3d_main_loop(C.byref(cp), O.pp(loop), MAIN_LOOP_STEPS, C.byref(t))
+        divb = R.ref_mhd3d_divB_max(C.byref(cp), O.pp(loop))
+        _save(f"mhd3d_{name}", params=_params_json("mhd3d", p), dt=np.float64(dt), loop_t=np.float64(t.value),
+              loop_divb=np.float64(divb),
+              **_state("in", S), **_state("stage", stage), **_state("step", step), **_state("loop", loop))
+
+
+def euler2d():
+    from core_collapse_b200.euler2d import ParamsEH
+    R = O.ref("euler2d")
+    for name in sorted(CASES_EH):
+        p, s = make_case_eh(name)   # the reference's SOR is fixed at omega 1.7, tol 1e-10 (EH:328-330)
+        cp = p.to_c()
+        S = [a.copy() for a in s.arrays()]
+        dt = R.ref_euler2d_compute_dt(C.byref(cp), O.pp(S))
+        rhs = [np.zeros_like(a) for a in S]
+        R.ref_euler2d_rhs(C.byref(cp), O.pp(S), O.pp(rhs))
+        step = O.copy_state(S)
+        R.ref_euler2d_rk2_step(C.byref(cp), O.pp(step), dt)
+        _save(f"euler2d_{name}", params=_params_json("euler2d", p), dt=np.float64(dt),
+              **_state("in", S), **_state("rhs", rhs), **_state("step", step))
+    # the reference's own main(): random-blob IC, tolerance SOR, 3 steps
+    p = ParamsEH(Nx=16, Ny=12)
+    cp = p.to_c()
+    n = p.Nx * p.Ny
+    S = [np.zeros(n) for _ in range(4)]
+    R.ref_euler2d_init_random_blob(C.byref(cp), O.pp(S))
+    loop = O.copy_state(S)
+    t = C.c_double(0.0)
+    rc = R.ref_euler2d_main_loop(C.byref(cp), O.pp(loop), MAIN_LOOP_STEPS, C.byref(t))
+    assert rc == 0
+    _save("euler2d_random_blob", params=_params_json("euler2d", p), loop_t=np.float64(t.value),
+          **_state("ic", S), **_state("loop", loop))
+
+
+def fft():
+    R = O.ref("fft")
+    rng = np.random.default_rng(11)
+    out = {}
+    for n in (8, 64):
+        for inv in (0, 1):
+            z = rng.normal(size=2 * n)
+            a = z.copy()
+            R.ref_fft1d(n, O.dp(a), inv)
+            out[f"fft1d_{n}_{inv}_in"], out[f"fft1d_{n}_{inv}_out"] = z, a
+    for nx, ny in ((16, 16), (32, 8)):
+        rho = 1.0 + rng.random(nx * ny)
+        phi = np.zeros(nx * ny)
+        R.ref_fft_poisson(nx, ny, -1.0, 1.0, -1.0, 1.0, 1.0, O.dp(rho), O.dp(phi))
+        out[f"poisson_{nx}x{ny}_rho"], out[f"poisson_{nx}x{ny}_phi"] = rho, phi
+    _save("fft", **out)
+
+
+def main():
+    for name in ("mhd2d", "mhd3d", "euler2d", "fft"):
+        if O.ref(name) is None:
+            raise SystemExit(f"compiled reference libref_{name}.so is missing: run make -C oracle")
+    mhd2d()
+    mhd3d()
+    euler2d()
+    fft()
+    print("wrote", sorted(p.name for p in HERE.glob("*.npz")))
+
+
+if __name__ == "__main__":
+    main()
