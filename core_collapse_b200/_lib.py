@@ -1,5 +1,5 @@
-"""ctypes binding of libcc_b200.so (the C ABI declared in include/cc_step.h and
-include/cc_ic.h).  Loading fails loudly: there is no CPU fallback."""
+"""ctypes binding of libcc_b200.so (the C ABI declared in include/cc_step.h,
+include/cc_ic.h and include/cc_batch.h).  Loading fails loudly: there is no CPU fallback."""
 from __future__ import annotations
 
 import ctypes as C
@@ -22,6 +22,8 @@ CC_FP64 = 0
 CC_FP32 = 1
 CC_POISSON_SOR = 0
 CC_POISSON_FFT = 1
+CC_POISSON_DIRECT = 2
+CC_BATCH_MAX_DIRECT_SIDE = 2048
 
 
 class CcMhd2dParams(C.Structure):
@@ -99,6 +101,15 @@ _DP = C.POINTER(C.c_double)
 _H = C.c_void_p
 
 # name -> (restype, argtypes); every symbol declared in include/*.h
+class CcBatchInfo(C.Structure):
+    _fields_ = [
+        ("n", C.c_int32), ("precision", C.c_int32), ("cells", C.c_int64),
+        ("shape", C.c_int32), ("n_shapes", C.c_int32), ("tile_x", C.c_int32), ("tile_y", C.c_int32),
+        ("stage_tiles", C.c_int32), ("stage_ctas", C.c_int32), ("reduce_tiles", C.c_int32),
+        ("poisson_tiles", C.c_int32), ("device_bytes", C.c_int64),
+    ]
+
+
 SIGNATURES = {
     "cc_mhd2d_params_default": (None, [C.POINTER(CcMhd2dParams)]),
     "cc_mhd2d_create": (C.c_int, [C.POINTER(CcMhd2dParams), C.POINTER(_H)]),
@@ -141,6 +152,15 @@ SIGNATURES = {
                                        C.c_double, C.c_double, C.c_double, C.POINTER(_DP)]),
     "cc_ic_mhd2d_orszag_tang": (C.c_int, [C.POINTER(CcMhd2dParams), C.c_double, C.c_double, C.POINTER(_DP)]),
     "cc_ic_euler2d_random_blob": (C.c_int, [C.POINTER(CcEuler2dParams), C.POINTER(_DP)]),
+    "cc_batch_create": (C.c_int, [C.POINTER(CcMhd2dParams), C.c_int, C.POINTER(_H)]),
+    "cc_batch_upload": (C.c_int, [_H, C.c_int, C.POINTER(_DP)]),
+    "cc_batch_download": (C.c_int, [_H, C.c_int, C.POINTER(_DP)]),
+    "cc_batch_compute_dt": (C.c_int, [_H, _DP]),
+    "cc_batch_advance": (C.c_int, [_H, C.c_int, _DP]),
+    "cc_batch_diagnostics": (C.c_int, [_H, C.c_int, C.POINTER(CcDiag)]),
+    "cc_batch_autotune": (C.c_int, [_H, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_double)]),
+    "cc_batch_set_shape": (C.c_int, [_H, C.c_int]),
+    "cc_batch_get_info": (C.c_int, [_H, C.POINTER(CcBatchInfo)]),
 }
 
 _lib = None

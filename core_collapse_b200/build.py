@@ -4,13 +4,15 @@
 
 Translation units and their floating-point contract:
   mhd2d_f64.cu, mhd3d_f64.cu, euler2d_f64.cu,
-  common_kernels.cu,
-  noalloc.cu                         -fmad=false: FP64 kernels round exactly like
+  common_kernels.cu, batch_f64.cu,
+  batch_common.cu, noalloc.cu        -fmad=false: FP64 kernels round exactly like
                                      the reference's x86-64 build (no FMA)
+  dpoisson.cu                        -fmad=false, explicit fma() only: the batched
+                                     direct Poisson solve, reproducible on the CPU
   mhd2d_f32.cu, mhd3d_f32.cu,
-  euler2d_f32.cu                     FMA contraction on, approximate FP32 division
+  euler2d_f32.cu, batch_f32.cu       FMA contraction on, approximate FP32 division
                                      and square root, flush-to-zero (the FP32 bulk path)
-  capi.cu, ic.cpp                    host code
+  capi*.cu, ic.cpp                   host code
 """
 from __future__ import annotations
 
@@ -36,13 +38,18 @@ UNITS = [
     ("euler2d_f64.cu", ["-fmad=false"]),
     ("common_kernels.cu", ["-fmad=false"]),
     ("noalloc.cu", ["-fmad=false"]),
+    ("batch_f64.cu", ["-fmad=false"]),
+    ("batch_common.cu", ["-fmad=false"]),
+    ("dpoisson.cu", ["-fmad=false"]),
     # FP32 bulk path: approximate division/sqrt (<= 2 ulp), denormals flushed
     ("mhd2d_f32.cu", ["-prec-div=false", "-prec-sqrt=false", "-ftz=true"]),
     ("mhd3d_f32.cu", ["-prec-div=false", "-prec-sqrt=false", "-ftz=true"]),
     ("euler2d_f32.cu", ["-prec-div=false", "-prec-sqrt=false", "-ftz=true"]),
+    ("batch_f32.cu", ["-prec-div=false", "-prec-sqrt=false", "-ftz=true"]),
     ("capi.cu", []),
     ("capi_mhd3d.cu", []),
     ("capi_euler2d.cu", []),
+    ("capi_batch.cu", []),
     ("ic.cpp", []),
 ]
 

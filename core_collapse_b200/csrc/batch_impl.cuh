@@ -1,0 +1,129 @@
+// Definitions of BatchLaunch<T>; included once per precision TU.
+//
+// Stage tile candidates (TX, TY, CTAs per SM the launch bounds ask for):
+//   FP64: 32x8 (2), 16x16 (2)
+//   FP32: 32x16 (2), 32x8 (4), 64x8 (2)
+// The autotuner of the batch handle times each on the actual work-list.
+#pragma once
+#include "batch_launch.h"
+
+namespace ccb {
+
+template <class T> struct BatchShapes;
+template <> struct BatchShapes<double> {
+    static constexpr int N = 2;
+    template <int K> struct S;
+};
+template <> template <> struct BatchShapes<double>::S<0> { static constexpr int TX = 32, TY = 8, MINB = 2; };
+template <> template <> struct BatchShapes<double>::S<1> { static constexpr int TX = 16, TY = 16, MINB = 2; };
+template <> struct BatchShapes<float> {
+    static constexpr int N = 3;
+    template <int K> struct S;
+};
+template <> template <> struct BatchShapes<float>::S<0> { static constexpr int TX = 32, TY = 16, MINB = 2; };
+template <> template <> struct BatchShapes<float>::S<1> { static constexpr int TX = 32, TY = 8, MINB = 4; };
+template <> template <> struct BatchShapes<float>::S<2> { static constexpr int TX = 64, TY = 8, MINB = 2; };
+
+namespace {
+
+template <class T, int K> struct ShapeOps {
+    using S = typename BatchShapes<T>::template S<K>;
+    static constexpr size_t smem() { return StageGeomT<T, S::TX, S::TY>::smem; }
+    template <bool D, int G> static auto kern() { return m2b_stage_kernel<T, S::TX, S::TY, S::MINB, D, G>; }
+    static cudaError_t prepare() {
+        cudaError_t e;
+        const int b = (int)smem();
+        if ((e = cudaFuncSetAttribute(kern<false, GRAV_NONE>(), cudaFuncAttributeMaxDynamicSharedMemorySize, b))) return e;
+        if ((e = cudaFuncSetAttribute(kern<false, GRAV_PHI>(), cudaFuncAttributeMaxDynamicSharedMemorySize, b))) return e;
+        if ((e = cudaFuncSetAttribute(kern<true, GRAV_NONE>(), cudaFuncAttributeMaxDynamicSharedMemorySize, b))) return e;
+        return cudaFuncSetAttribute(kern<true, GRAV_PHI>(), cudaFuncAttributeMaxDynamicSharedMemorySize, b);
+    }
+    static cudaError_t resident(int* per_sm) {
+        return cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm, kern<false, GRAV_PHI>(), S::TX * S::TY, smem());
+    }
+    static cudaError_t stage(int grid, const BatchInst<T>* inst, const int2* work, int nwork, int src, int dst,
+                             bool defer, bool grav, const double* dt, const int* active, cudaStream_t s) {
+        const dim3 b(S::TX * S::TY);
+        if (defer && grav) kern<true, GRAV_PHI>()<<<grid, b, smem(), s>>>(inst, work, nwork, src, dst, dt, active);
+        else if (defer) kern<true, GRAV_NONE>()<<<grid, b, smem(), s>>>(inst, work, nwork, src, dst, dt, active);
+        else if (grav) kern<false, GRAV_PHI>()<<<grid, b, smem(), s>>>(inst, work, nwork, src, dst, dt, active);
+        else kern<false, GRAV_NONE>()<<<grid, b, smem(), s>>>(inst, work, nwork, src, dst, dt, active);
+        return cudaGetLastError();
+    }
+};
+
+template <class T, int K = 0> struct ShapeLoop {
+    static cudaError_t prepare() {
+        if constexpr (K < BatchShapes<T>::N) {
+            cudaError_t e = ShapeOps<T, K>::prepare();
+            if (e != cudaSuccess) return e;
+            return ShapeLoop<T, K + 1>::prepare();
+        }
+        return cudaSuccess;
+    }
+    static TileShape shape(int k) {
+        if constexpr (K < BatchShapes<T>::N) {
+            if (k == K) return TileShape{ShapeOps<T, K>::S::TX, ShapeOps<T, K>::S::TY};
+            return ShapeLoop<T, K + 1>::shape(k);
+        }
+        return TileShape{0, 0};
+    }
+    static cudaError_t resident(int k, int* per_sm) {
+        if constexpr (K < BatchShapes<T>::N) {
+            if (k == K) return ShapeOps<T, K>::resident(per_sm);
+            return ShapeLoop<T, K + 1>::resident(k, per_sm);
+        }
+        return cudaErrorInvalidValue;
+    }
+    static cudaError_t stage(int k, int grid, const BatchInst<T>* inst, const int2* work, int nwork, int src, int dst,
+                             bool defer, bool grav, const double* dt, const int* active, cudaStream_t s) {
+        if constexpr (K < BatchShapes<T>::N) {
+            if (k == K) return ShapeOps<T, K>::stage(grid, inst, work, nwork, src, dst, defer, grav, dt, active, s);
+            return ShapeLoop<T, K + 1>::stage(k, grid, inst, work, nwork, src, dst, defer, grav, dt, active, s);
+        }
+        return cudaErrorInvalidValue;
+    }
+};
+
+inline int rgrid(int nrwork) {
+    const int g = nrwork < 8192 ? nrwork : 8192;
+    return g < 1 ? 1 : g;
+}
+
+}  // namespace
+
+template <class T> int BatchLaunch<T>::n_shapes() { return BatchShapes<T>::N; }
+template <class T> TileShape BatchLaunch<T>::shape(int k) { return ShapeLoop<T>::shape(k); }
+template <class T> cudaError_t BatchLaunch<T>::prepare() { return ShapeLoop<T>::prepare(); }
+template <class T> cudaError_t BatchLaunch<T>::resident(int k, int* per_sm) { return ShapeLoop<T>::resident(k, per_sm); }
+
+template <class T>
+cudaError_t BatchLaunch<T>::stage(int k, int grid, const BatchInst<T>* inst, const int2* work, int nwork, int src,
+                                  int dst, bool defer, bool grav, const double* dt, const int* active,
+                                  cudaStream_t s) {
+    return ShapeLoop<T>::stage(k, grid, inst, work, nwork, src, dst, defer, grav, dt, active, s);
+}
+
+template <class T>
+cudaError_t BatchLaunch<T>::average(const BatchInst<T>* inst, const int2* rwork, int nrwork, int a, int d, int b,
+                                    const double* dt, const int* active, double* spd_part, double* rho_part,
+                                    cudaStream_t s) {
+    m2b_average_kernel<T><<<rgrid(nrwork), RNT, 0, s>>>(inst, rwork, nrwork, a, d, b, dt, active, spd_part, rho_part);
+    return cudaGetLastError();
+}
+
+template <class T>
+cudaError_t BatchLaunch<T>::speeds(const BatchInst<T>* inst, const int2* rwork, int nrwork, int src,
+                                   double* spd_part, double* rho_part, cudaStream_t s) {
+    m2b_speed_kernel<T><<<rgrid(nrwork), RNT, 0, s>>>(inst, rwork, nrwork, src, spd_part, rho_part);
+    return cudaGetLastError();
+}
+
+template <class T>
+cudaError_t BatchLaunch<T>::rho_sum(const BatchInst<T>* inst, const int2* rwork, int nrwork, int src,
+                                    const int* active, double* rho_part, cudaStream_t s) {
+    m2b_rho_sum_kernel<T><<<rgrid(nrwork), RNT, 0, s>>>(inst, rwork, nrwork, src, active, rho_part);
+    return cudaGetLastError();
+}
+
+}  // namespace ccb

@@ -1,0 +1,193 @@
+// Direct Poisson solve for the batched ensemble (FP64 arithmetic, T only at the
+// density load and the potential store).
+//
+// It solves the discrete problem the reference's SOR iterates towards
+// (mhd2d_resistive_hlld_ct_gravity.cpp:207-223: 5-point Laplacian, clamp or
+// wrap neighbours, zero-mean potential) exactly instead of iterating:
+//   1. U = R * Tx^T     R = 4 pi G (rho - mean), Tx rows = orthonormal
+//                       eigenvectors of the x second difference (DCT-II for
+//                       clamp, Hartley for periodic)        -- dp_gemm, MODE 0
+//   2. per x wavenumber k: (Dyy + lam_x[k]) u_k = U[:, k] along y: Thomas,
+//      cyclic Thomas (Sherman-Morrison), or for k = 0 the cumulative-flux
+//      solution with its mean removed                        -- dp_ysolve
+//   3. phi = U * Tx                                          -- dp_gemm, MODE 1
+// The translation unit is compiled with -fmad=false and every multiply-add is
+// an explicit fma() in a fixed order, so the CPU restatement (std::fma in the
+// same order) reproduces the result bit for bit.
+//
+// Work-lists: GEMM tiles {instance, (tm << 16) | tn} of DPM x DPN outputs;
+// y-solve blocks {instance, column block} of DPC columns, one thread per column.
+#pragma once
+#include "batch_kernels.cuh"
+
+namespace ccb {
+
+constexpr int DPM = 64, DPN = 64, DPK = 16, DPNT = 256;   // GEMM tile, 4 x 4 outputs per thread
+constexpr int DPC = 32;                                    // y-solve columns per block
+
+template <class T, int MODE>
+__global__ void __launch_bounds__(DPNT)
+dp_gemm_kernel(const BatchInst<T>* __restrict__ inst, const int2* __restrict__ gwork, int ngwork, int src,
+               const double* __restrict__ rho_mean, const int* __restrict__ active) {
+    __shared__ double As[DPK][DPM + 1];   // k-major A tile
+    __shared__ double Bs[DPK][DPN];
+    const int tr = threadIdx.x / 16, tc = threadIdx.x % 16;
+    for (int w = blockIdx.x; w < ngwork; w += gridDim.x) {
+        const int2 it = gwork[w];
+        if (active[it.x] == 0) continue;   // uniform over the block
+        const BatchInst<T>& I = inst[it.x];
+        const int nx = I.c.nx, ny = I.c.ny, P = I.c.pitch;
+        const int m0 = (it.y >> 16) * DPM, n0 = (it.y & 0xffff) * DPN;
+        const double* __restrict__ B = (MODE == 0) ? I.txt : I.tx;   // K x N row-major, K = N = nx
+        const T* __restrict__ rho = I.buf[src].rho;
+        const double mean = (MODE == 0) ? rho_mean[it.x] : 0.0;
+        const double fpg = I.fourpiG;
+        double acc[4][4];
+#pragma unroll
+        for (int r = 0; r < 4; r++)
+#pragma unroll
+            for (int c = 0; c < 4; c++) acc[r][c] = 0.0;
+        for (int k0 = 0; k0 < nx; k0 += DPK) {
+#pragma unroll
+            for (int q = 0; q < 4; q++) {
+                const int e = threadIdx.x + q * DPNT;
+                const int m = e / DPK, kk = e % DPK;
+                const int gm = m0 + m, gk = k0 + kk;
+                double v = 0.0;
+                if (gm < ny && gk < nx) {
+                    if (MODE == 0) v = fpg * ((double)rho[(size_t)gm * P + gk] - mean);
+                    else v = I.ah[(size_t)gm * nx + gk];
+                }
+                As[kk][m] = v;
+                const int kb = e / DPN, nb = e % DPN;
+                const int gkb = k0 + kb, gn = n0 + nb;
+                Bs[kb][nb] = (gkb < nx && gn < nx) ? B[(size_t)gkb * nx + gn] : 0.0;
+            }
+            __syncthreads();
+            const int kend = min(DPK, nx - k0);
+            for (int kk = 0; kk < kend; kk++) {
+                double a[4], b[4];
+#pragma unroll
+                for (int r = 0; r < 4; r++) a[r] = As[kk][tr + 16 * r];
+#pragma unroll
+                for (int c = 0; c < 4; c++) b[c] = Bs[kk][tc + 16 * c];
+#pragma unroll
+                for (int r = 0; r < 4; r++)
+#pragma unroll
+                    for (int c = 0; c < 4; c++) acc[r][c] = fma(a[r], b[c], acc[r][c]);
+            }
+            __syncthreads();
+        }
+#pragma unroll
+        for (int r = 0; r < 4; r++) {
+            const int gm = m0 + tr + 16 * r;
+            if (gm >= ny) continue;
+#pragma unroll
+            for (int c = 0; c < 4; c++) {
+                const int gn = n0 + tc + 16 * c;
+                if (gn >= nx) continue;
+                if (MODE == 0) I.ah[(size_t)gm * nx + gn] = acc[r][c];
+                else I.phi[(size_t)gm * P + gn] = (T)acc[r][c];
+            }
+        }
+    }
+}
+
+// One thread per x wavenumber (column of ah), sequential along y.
+template <class T>
+__global__ void __launch_bounds__(DPC)
+dp_ysolve_kernel(const BatchInst<T>* __restrict__ inst, const int2* __restrict__ ywork, int nywork,
+                 const int* __restrict__ active) {
+    for (int w = blockIdx.x; w < nywork; w += gridDim.x) {
+        const int2 it = ywork[w];
+        if (active[it.x] == 0) continue;
+        const BatchInst<T>& I = inst[it.x];
+        const int nx = I.c.nx, n = I.c.ny;
+        const int col = it.y * DPC + threadIdx.x;
+        if (col >= nx) continue;
+        double* __restrict__ u = I.ah + col;
+        double* __restrict__ cp = I.w1 + col;
+        double* __restrict__ z = I.w2 + col;
+        const size_t S = (size_t)nx;
+        const bool py = I.c.ay.periodic != 0;
+        const double a = I.ay;
+        if (col == 0) {
+            // singular k = 0: flux G_j = a (u_{j+1} - u_j) = G_{j-1} + r_j
+            double g0 = 0.0;
+            if (py) {
+                double Sr = 0.0, SS = 0.0;
+                for (int j = 0; j < n; j++) { Sr = Sr + u[j * S]; SS = SS + Sr; }
+                g0 = -(SS / (double)n);
+            }
+            double G = g0, prev = 0.0;
+            cp[0] = 0.0;   // the solution is built in cp, then moved to u
+            for (int j = 0; j + 1 < n; j++) {
+                G = G + u[j * S];
+                prev = fma(I.dy2, G, prev);
+                cp[(j + 1) * S] = prev;
+            }
+            double m = 0.0;
+            for (int j = 0; j < n; j++) m = m + cp[j * S];
+            m = m / (double)n;
+            for (int j = 0; j < n; j++) u[j * S] = cp[j * S] - m;
+            continue;
+        }
+        const double lam = I.lamx[col];
+        const double b = fma(-2.0, a, lam);
+        if (!py) {
+            const double bE = lam - a;
+            double m = bE;
+            double cprev = a / m;
+            cp[0] = cprev;
+            double dprev = u[0] / m;
+            u[0] = dprev;
+            for (int j = 1; j < n; j++) {
+                const double bj = (j == n - 1) ? bE : b;
+                m = fma(-a, cprev, bj);
+                cprev = a / m;
+                cp[j * S] = cprev;
+                dprev = fma(-a, dprev, u[j * S]) / m;
+                u[j * S] = dprev;
+            }
+            double x = dprev;
+            for (int j = n - 2; j >= 0; j--) {
+                x = fma(-cp[j * S], x, u[j * S]);
+                u[j * S] = x;
+            }
+            continue;
+        }
+        const double gam = -b;
+        const double b0 = b - gam, bn = b - a * a / gam;
+        double m = b0;
+        double cprev = a / m;
+        cp[0] = cprev;
+        double dprev = u[0] / m, zprev = gam / m;
+        u[0] = dprev;
+        z[0] = zprev;
+        for (int j = 1; j < n; j++) {
+            const double bj = (j == n - 1) ? bn : b;
+            m = fma(-a, cprev, bj);
+            cprev = a / m;
+            cp[j * S] = cprev;
+            const double zr = (j == n - 1) ? a : 0.0;
+            dprev = fma(-a, dprev, u[j * S]) / m;
+            zprev = fma(-a, zprev, zr) / m;
+            u[j * S] = dprev;
+            z[j * S] = zprev;
+        }
+        double x = dprev, zz = zprev;
+        for (int j = n - 2; j >= 0; j--) {
+            const double c = cp[j * S];
+            x = fma(-c, x, u[j * S]);
+            zz = fma(-c, zz, z[j * S]);
+            u[j * S] = x;
+            z[j * S] = zz;
+        }
+        // x, zz hold the j = 0 entries; v^T x = x_0 + (a / gamma) x_{n-1}
+        const double xl = u[(n - 1) * S], zl = z[(n - 1) * S];
+        const double fac = fma(a / gam, xl, x) / (1.0 + fma(a / gam, zl, zz));
+        for (int j = 0; j < n; j++) u[j * S] = fma(-fac, z[j * S], u[j * S]);
+    }
+}
+
+}  // namespace ccb

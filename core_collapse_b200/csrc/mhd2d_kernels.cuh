@@ -36,8 +36,8 @@ template <class T> struct StageTile;
 template <> struct StageTile<double> { static constexpr int TX = 32, TY = 8, MINB = 2; };
 template <> struct StageTile<float> { static constexpr int TX = 32, TY = 16, MINB = 2; };
 
-template <class T> struct StageGeom {
-    static constexpr int TX = StageTile<T>::TX, TY = StageTile<T>::TY, HALO = 2;
+template <class T, int TX_, int TY_> struct StageGeomT {
+    static constexpr int TX = TX_, TY = TY_, HALO = 2;
     static constexpr int RX = TX + 2 * HALO, RY = TY + 2 * HALO, RR = RX * RY;
     static constexpr int NT = TX * TY;
     static constexpr int NFX = (TX + 1) * (TY + 2);  // x faces: TX+1 per row, rows -1..TY
@@ -48,6 +48,7 @@ template <class T> struct StageGeom {
     static constexpr size_t smem = sizeof(T) * (size_t)(8 * RR + 7 * NSL + 7 * NFX + 7 * NGY + NE + 6 * NT);
 };
 
+template <class T> using StageGeom = StageGeomT<T, StageTile<T>::TX, StageTile<T>::TY>;
 template <class T> constexpr size_t m2_stage_smem() { return StageGeom<T>::smem; }
 
 // Joule heating, explicit Bz diffusion and floors of one cell
@@ -77,19 +78,19 @@ __device__ __forceinline__ void joule_cell(const M2Const<T>& c, const Fields<T>&
 }
 
 // ---------------------------------------------------------------------------
-// One RK stage.  DEFER: the input is a stored pre-Joule stage output whose
-// Joule sub-step must be applied first.  GMODE selects the gravity source.
+// One RK stage on one TX x TY tile whose first cell is (i0, j0).  DEFER: the
+// input is a stored pre-Joule stage output whose Joule sub-step must be
+// applied first.  GMODE selects the gravity source.  sm: StageGeomT::smem
+// bytes of shared memory.  Called by the single-grid kernel (one tile per
+// CTA) and by the batched persistent kernel (a run of tiles per CTA).
 // ---------------------------------------------------------------------------
-template <class T, bool DEFER, int GMODE>
-__global__ void __launch_bounds__(StageGeom<T>::NT, StageTile<T>::MINB)
-m2_stage_kernel(const M2Const<T> c, const Fields<T> in, const Fields<T> out, const T* __restrict__ ga,
-                const T* __restrict__ gb, const double* __restrict__ dtp, const int* __restrict__ active) {
-    using G = StageGeom<T>;
+template <class T, int TX_, int TY_, bool DEFER, int GMODE>
+__device__ __forceinline__ void m2_stage_tile(const M2Const<T>& c, const Fields<T>& in, const Fields<T>& out,
+                                              const T* __restrict__ ga, const T* __restrict__ gb, const T dt,
+                                              const int i0, const int j0, T* sm) {
+    using G = StageGeomT<T, TX_, TY_>;
     constexpr int TX = G::TX, TY = G::TY, HALO = G::HALO, RX = G::RX, RR = G::RR, NT = G::NT;
     constexpr int NFX = G::NFX, NGY = G::NGY, NSL = G::NSL;
-    if (active && *active == 0) return;
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    T* sm = reinterpret_cast<T*>(smem_raw);
     T* s_r = sm;          T* s_u = s_r + RR;   T* s_v = s_u + RR;   T* s_w = s_v + RR;
     T* s_P = s_w + RR;    T* s_bx = s_P + RR;  T* s_by = s_bx + RR; T* s_bz = s_by + RR;
     T* sl = s_bz + RR;          // 7 planes of NSL: slopes of cells (-1..TX) x (-1..TY), x then y
@@ -99,9 +100,7 @@ m2_stage_kernel(const M2Const<T> c, const Fields<T> in, const Fields<T> out, con
     T* own = ez + G::NE;        // 6 planes of NT
 
     const int tid = threadIdx.x;
-    const int i0 = blockIdx.x * TX, j0 = blockIdx.y * TY;
     const int P = c.pitch;
-    const T dt = (T)(*dtp);
 
     // ---- A: primitives on the halo-2 region (get_prim_cc, M2:278-286) ----
     for (int k = tid; k < RR; k += NT) {
@@ -277,66 +276,92 @@ m2_stage_kernel(const M2Const<T> c, const Fields<T> in, const Fields<T> out, con
     out.rho[q] = rho; out.mx[q] = mx; out.my[q] = my; out.mz[q] = mz; out.E[q] = E; out.Bz[q] = Bz;
 }
 
+template <class T, bool DEFER, int GMODE>
+__global__ void __launch_bounds__(StageGeom<T>::NT, StageTile<T>::MINB)
+m2_stage_kernel(const M2Const<T> c, const Fields<T> in, const Fields<T> out, const T* __restrict__ ga,
+                const T* __restrict__ gb, const double* __restrict__ dtp, const int* __restrict__ active) {
+    constexpr int TX = StageTile<T>::TX, TY = StageTile<T>::TY;
+    if (active && *active == 0) return;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    m2_stage_tile<T, TX, TY, DEFER, GMODE>(c, in, out, ga, gb, (T)(*dtp), blockIdx.x * TX, blockIdx.y * TY,
+                                           reinterpret_cast<T*>(smem_raw));
+}
+
 // ---------------------------------------------------------------------------
-// RK average (M2:848-868) fused with the deferred stage-2 Joule sub-step, the
-// CFL speed reduction of the next step (M2:579-598) and the density sum the
-// next Poisson solve needs.  un: U^n, s2: stage-2 output (pre-Joule), out: U^{n+1}.
+// RK average (M2:848-868) of one cell, fused with the deferred stage-2 Joule
+// sub-step; returns the CFL speed of the result (compute_dt's loop body,
+// M2:585-587) and adds its density to rsum.  Inactive (t >= t_end): U^n is
+// carried over unchanged so that the buffer rotation stays valid.
 // ---------------------------------------------------------------------------
-template <class T, int NT>
-__global__ void __launch_bounds__(NT)
-m2_average_kernel(const M2Const<T> c, const Fields<T> un, const Fields<T> s2, const Fields<T> out,
-                  const double* __restrict__ dtp, const int* __restrict__ active, double* __restrict__ spd_part,
-                  double* __restrict__ rho_part) {
-    // Once t >= t_end the step kernels are no-ops; this kernel then carries
-    // U^n over unchanged so that the host's buffer rotation stays valid.
-    const bool act = (active == nullptr) || (*active != 0);
-    __shared__ double sh[NT / 32];
-    const T dt = (T)(*dtp);
+template <class T>
+__device__ __forceinline__ double average_cell(const M2Const<T>& c, const Fields<T>& un, const Fields<T>& s2,
+                                               const Fields<T>& out, const T dt, const bool act, const int i,
+                                               const int j, double& rsum) {
     const int P = c.pitch;
-    double smax = 0.0, rsum = 0.0;
-    const int ncell = c.nx * c.ny;
-    for (int k = blockIdx.x * NT + threadIdx.x; k < ncell; k += gridDim.x * NT) {
-        const int i = k % c.nx, j = k / c.nx;
-        const size_t q = (size_t)j * P + i;
-        if (!act) {
-            const T rho = un.rho[q], mx = un.mx[q], my = un.my[q], mz = un.mz[q], E = un.E[q], Bz = un.Bz[q];
-            const T bxl = un.bx[q], bxr = un.bx[q + 1], byd = un.by[q], byu = un.by[q + P];
-            out.rho[q] = rho; out.mx[q] = mx; out.my[q] = my; out.mz[q] = mz; out.E[q] = E; out.Bz[q] = Bz;
-            out.bx[q] = bxl;
-            if (i == c.nx - 1) out.bx[q + 1] = bxr;
-            out.by[q] = byd;
-            if (j == c.ny - 1) out.by[q + P] = byu;
-            const Prim<T> W = to_prim(c, rho, mx, my, mz, E, T(0.5) * (bxl + bxr), T(0.5) * (byd + byu), Bz);
-            const double s = (double)vmax(fabs(W.u) + fast_speed(c, W, W.bx), fabs(W.v) + fast_speed(c, W, W.by));
-            if (s > smax) smax = s;
-            rsum += (double)rho;
-            continue;
-        }
-        T rho = s2.rho[q], mx = s2.mx[q], my = s2.my[q], mz = s2.mz[q], E = s2.E[q], Bz = s2.Bz[q];
-        const T bxl2 = s2.bx[q], bxr2 = s2.bx[q + 1], byd2 = s2.by[q], byu2 = s2.by[q + P];
-        joule_cell(c, s2, i, j, dt, rho, mx, my, mz, E, Bz, T(0.5) * (bxl2 + bxr2), T(0.5) * (byd2 + byu2));
-        rho = T(0.5) * (un.rho[q] + rho);
-        mx = T(0.5) * (un.mx[q] + mx);
-        my = T(0.5) * (un.my[q] + my);
-        mz = T(0.5) * (un.mz[q] + mz);
-        E = T(0.5) * (un.E[q] + E);
-        Bz = T(0.5) * (un.Bz[q] + Bz);
-        const T bxl = T(0.5) * (un.bx[q] + bxl2), bxr = T(0.5) * (un.bx[q + 1] + bxr2);
-        const T byd = T(0.5) * (un.by[q] + byd2), byu = T(0.5) * (un.by[q + P] + byu2);
-        const T Bx = T(0.5) * (bxl + bxr), By = T(0.5) * (byd + byu);
-        floors(c, rho, mx, my, mz, E, Bx, By, Bz);
+    const size_t q = (size_t)j * P + i;
+    if (!act) {
+        const T rho = un.rho[q], mx = un.mx[q], my = un.my[q], mz = un.mz[q], E = un.E[q], Bz = un.Bz[q];
+        const T bxl = un.bx[q], bxr = un.bx[q + 1], byd = un.by[q], byu = un.by[q + P];
         out.rho[q] = rho; out.mx[q] = mx; out.my[q] = my; out.mz[q] = mz; out.E[q] = E; out.Bz[q] = Bz;
         out.bx[q] = bxl;
         if (i == c.nx - 1) out.bx[q + 1] = bxr;
         out.by[q] = byd;
         if (j == c.ny - 1) out.by[q + P] = byu;
-        // CFL speeds of U^{n+1} (compute_dt's loop body, M2:585-587)
-        const Prim<T> W = to_prim(c, rho, mx, my, mz, E, Bx, By, Bz);
-        const T sx = fabs(W.u) + fast_speed(c, W, W.bx);
-        const T sy = fabs(W.v) + fast_speed(c, W, W.by);
-        const double s = (double)vmax(sx, sy);
-        if (s > smax) smax = s;   // NaN never wins, as in std::max(maxs, x)
+        const Prim<T> W = to_prim(c, rho, mx, my, mz, E, T(0.5) * (bxl + bxr), T(0.5) * (byd + byu), Bz);
         rsum += (double)rho;
+        return (double)vmax(fabs(W.u) + fast_speed(c, W, W.bx), fabs(W.v) + fast_speed(c, W, W.by));
+    }
+    T rho = s2.rho[q], mx = s2.mx[q], my = s2.my[q], mz = s2.mz[q], E = s2.E[q], Bz = s2.Bz[q];
+    const T bxl2 = s2.bx[q], bxr2 = s2.bx[q + 1], byd2 = s2.by[q], byu2 = s2.by[q + P];
+    joule_cell(c, s2, i, j, dt, rho, mx, my, mz, E, Bz, T(0.5) * (bxl2 + bxr2), T(0.5) * (byd2 + byu2));
+    rho = T(0.5) * (un.rho[q] + rho);
+    mx = T(0.5) * (un.mx[q] + mx);
+    my = T(0.5) * (un.my[q] + my);
+    mz = T(0.5) * (un.mz[q] + mz);
+    E = T(0.5) * (un.E[q] + E);
+    Bz = T(0.5) * (un.Bz[q] + Bz);
+    const T bxl = T(0.5) * (un.bx[q] + bxl2), bxr = T(0.5) * (un.bx[q + 1] + bxr2);
+    const T byd = T(0.5) * (un.by[q] + byd2), byu = T(0.5) * (un.by[q + P] + byu2);
+    const T Bx = T(0.5) * (bxl + bxr), By = T(0.5) * (byd + byu);
+    floors(c, rho, mx, my, mz, E, Bx, By, Bz);
+    out.rho[q] = rho; out.mx[q] = mx; out.my[q] = my; out.mz[q] = mz; out.E[q] = E; out.Bz[q] = Bz;
+    out.bx[q] = bxl;
+    if (i == c.nx - 1) out.bx[q + 1] = bxr;
+    out.by[q] = byd;
+    if (j == c.ny - 1) out.by[q + P] = byu;
+    const Prim<T> W = to_prim(c, rho, mx, my, mz, E, Bx, By, Bz);
+    const T sx = fabs(W.u) + fast_speed(c, W, W.bx);
+    const T sy = fabs(W.v) + fast_speed(c, W, W.by);
+    rsum += (double)rho;
+    return (double)vmax(sx, sy);
+}
+
+// CFL speed of one cell of a state (compute_dt's loop body, M2:585-587)
+template <class T>
+__device__ __forceinline__ double speed_cell(const M2Const<T>& c, const Fields<T>& s, const int i, const int j) {
+    const size_t q = (size_t)j * c.pitch + i;
+    const T Bx = T(0.5) * (s.bx[q] + s.bx[q + 1]), By = T(0.5) * (s.by[q] + s.by[q + c.pitch]);
+    const Prim<T> W = to_prim(c, s.rho[q], s.mx[q], s.my[q], s.mz[q], s.E[q], Bx, By, s.Bz[q]);
+    const T sx = fabs(W.u) + fast_speed(c, W, W.bx);
+    const T sy = fabs(W.v) + fast_speed(c, W, W.by);
+    return (double)vmax(sx, sy);
+}
+
+// RK average over the whole grid; emits the CFL and density partials of
+// U^{n+1} for the next step.  un: U^n, s2: stage-2 output (pre-Joule), out: U^{n+1}.
+template <class T, int NT>
+__global__ void __launch_bounds__(NT)
+m2_average_kernel(const M2Const<T> c, const Fields<T> un, const Fields<T> s2, const Fields<T> out,
+                  const double* __restrict__ dtp, const int* __restrict__ active, double* __restrict__ spd_part,
+                  double* __restrict__ rho_part) {
+    const bool act = (active == nullptr) || (*active != 0);
+    __shared__ double sh[NT / 32];
+    const T dt = (T)(*dtp);
+    double smax = 0.0, rsum = 0.0;
+    const int ncell = c.nx * c.ny;
+    for (int k = blockIdx.x * NT + threadIdx.x; k < ncell; k += gridDim.x * NT) {
+        const double s = average_cell(c, un, s2, out, dt, act, k % c.nx, k / c.nx, rsum);
+        if (s > smax) smax = s;   // NaN never wins, as in std::max(maxs, x)
     }
     const double bm = block_max<NT>(smax, sh);
     const double bs = block_sum<NT>(rsum, sh);
@@ -353,14 +378,9 @@ m2_speed_kernel(const M2Const<T> c, const Fields<T> s, double* __restrict__ spd_
     const int ncell = c.nx * c.ny;
     for (int k = blockIdx.x * NT + threadIdx.x; k < ncell; k += gridDim.x * NT) {
         const int i = k % c.nx, j = k / c.nx;
-        const size_t q = (size_t)j * P + i;
-        const T Bx = T(0.5) * (s.bx[q] + s.bx[q + 1]), By = T(0.5) * (s.by[q] + s.by[q + P]);
-        const Prim<T> W = to_prim(c, s.rho[q], s.mx[q], s.my[q], s.mz[q], s.E[q], Bx, By, s.Bz[q]);
-        const T sx = fabs(W.u) + fast_speed(c, W, W.bx);
-        const T sy = fabs(W.v) + fast_speed(c, W, W.by);
-        const double v = (double)vmax(sx, sy);
+        const double v = speed_cell(c, s, i, j);
         if (v > smax) smax = v;
-        rsum += (double)s.rho[q];
+        rsum += (double)s.rho[(size_t)j * P + i];
     }
     const double bm = block_max<NT>(smax, sh);
     const double bs = block_sum<NT>(rsum, sh);

@@ -45,7 +45,7 @@ class Params:
     sor_omega: float = 1.8
     # additions
     sor_tol: float = 0.0            # > 0: stop SOR once max|lap(phi)-rhs| < sor_tol
-    poisson: str = "sor"            # "sor" (red-black) or "fft"
+    poisson: str = "sor"            # "sor" (red-black), "fft", or "direct" (batched ensemble only)
     precision: str = "fp64"         # "fp64" or "fp32"
 
     def to_c(self) -> L.CcMhd2dParams:
@@ -55,7 +55,7 @@ class Params:
                 continue
             v = getattr(self, f.name)
             setattr(c, f.name, int(v) if isinstance(v, bool) else v)
-        c.poisson_kind = {"sor": L.CC_POISSON_SOR, "fft": L.CC_POISSON_FFT}[self.poisson]
+        c.poisson_kind = {"sor": L.CC_POISSON_SOR, "fft": L.CC_POISSON_FFT, "direct": L.CC_POISSON_DIRECT}[self.poisson]
         c.precision = {"fp64": L.CC_FP64, "fp32": L.CC_FP32}[self.precision]
         return c
 

@@ -49,6 +49,7 @@ extern "C" {
 
 #define CC_POISSON_SOR 0   /* red-black SOR (GPU-parallel ordering of M2's SOR) */
 #define CC_POISSON_FFT 1   /* spectral periodic solve, power-of-two grids */
+#define CC_POISSON_DIRECT 2 /* exact solve of the SOR's discrete problem (batched ensemble, cc_batch.h) */
 
 typedef struct cc_handle cc_handle;
 

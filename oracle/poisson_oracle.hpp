@@ -209,6 +209,178 @@ inline void fft_periodic(const PoissonSpec& s, const std::vector<double>& rho, s
     for (size_t q = 0; q < N; q++) phi[q] = A[q].real();
 }
 
+// ---------------------------------------------------------------------------
+// Direct solve of the discrete problem the SOR iterates towards (the
+// library's batched-ensemble Poisson): 5-point Laplacian with the solver's
+// boundary rule (clamp = mirrored ghost, periodic = wrap), zero-mean solution.
+//   1. x transform by a dense orthonormal eigenbasis of the x second
+//      difference: DCT-II for clamp, discrete Hartley (cas) for periodic;
+//   2. per x wavenumber k, the y system (Dyy + lam_x[k]) u = r: Thomas
+//      (clamp y), Sherman-Morrison cyclic Thomas (periodic y), and for k = 0
+//      (singular) the cumulative-flux solution with its mean removed;
+//   3. inverse x transform.
+// Every multiply-add the library fuses is written as std::fma here, in the
+// same order, so that the double result matches the library bit for bit.
+// ---------------------------------------------------------------------------
+
+// Row k of `basis` (n x n) is the k-th orthonormal eigenvector; lam[k] its
+// eigenvalue of (u[i+1] - 2u[i] + u[i-1]) / d^2 under the boundary rule.
+inline void direct_basis(int n, bool periodic, double d, std::vector<double>& basis, std::vector<double>& lam) {
+    basis.assign((size_t)n * n, 0.0);
+    lam.assign(n, 0.0);
+    for (int k = 0; k < n; k++) {
+        double sn;
+        if (periodic) {
+            const double sc = 1.0 / std::sqrt((double)n);
+            for (int i = 0; i < n; i++) {
+                const double arg = 2.0 * M_PI * (double)(((long long)k * i) % n) / (double)n;
+                basis[(size_t)k * n + i] = (std::cos(arg) + std::sin(arg)) * sc;
+            }
+            sn = std::sin(M_PI * (double)k / (double)n);
+        } else {
+            const double sc = std::sqrt((k == 0 ? 1.0 : 2.0) / (double)n);
+            for (int i = 0; i < n; i++) {
+                const double arg = M_PI * (double)((long long)k * (2 * i + 1)) / (double)(2 * n);
+                basis[(size_t)k * n + i] = sc * std::cos(arg);
+            }
+            sn = std::sin(M_PI * (double)k / (double)(2 * n));
+        }
+        lam[k] = -4.0 * sn * sn / (d * d);
+    }
+}
+
+// Density mean in the batched reduction order: 32 x 8 cell tiles in row-major
+// tile order; inside a tile a warp holds one row of 32 cells, the lanes are
+// summed by a shuffle-down tree (offsets 16..1), then the 8 warp sums by the
+// same tree (absent lanes 0.0); tile sums are added sequentially.
+inline double batch_tile_mean(int nx, int ny, const std::vector<double>& rho) {
+    const int tx_n = (nx + 31) / 32, ty_n = (ny + 7) / 8;
+    double total = 0.0;
+    for (int ty = 0; ty < ty_n; ty++)
+        for (int tx = 0; tx < tx_n; tx++) {
+            double w[32];
+            for (int r = 0; r < 32; r++) w[r] = 0.0;
+            for (int r = 0; r < 8; r++) {
+                double v[32];
+                for (int l = 0; l < 32; l++) {
+                    const int i = tx * 32 + l, j = ty * 8 + r;
+                    v[l] = (i < nx && j < ny) ? rho[(size_t)j * nx + i] : 0.0;
+                }
+                for (int o = 16; o > 0; o >>= 1)
+                    for (int l = 0; l < o; l++) v[l] = v[l] + v[l + o];
+                w[r] = v[0];
+            }
+            for (int o = 16; o > 0; o >>= 1)
+                for (int l = 0; l < o; l++) w[l] = w[l] + w[l + o];
+            total += w[0];
+        }
+    return total / ((double)nx * (double)ny);
+}
+
+// One y system for x wavenumber k (column col of the ny x nx array u, solved in place).
+inline void direct_ysolve(int nx, int ny, bool py, double ay, double dy2, double lam, bool singular, int col,
+                          std::vector<double>& u) {
+    auto at = [&](int j) -> double& { return u[(size_t)j * nx + col]; };
+    const int n = ny;
+    if (singular) {
+        // flux G_j = a (u_{j+1} - u_j) = G_{j-1} + r_j; clamp: G_{-1} = 0;
+        // periodic: G_{-1} = -(1/n) sum_j S_j with S_j the running sum of r
+        double g0 = 0.0;
+        if (py) {
+            double S = 0.0, SS = 0.0;
+            for (int j = 0; j < n; j++) { S = S + at(j); SS = SS + S; }
+            g0 = -(SS / (double)n);
+        }
+        double G = g0, prev = 0.0;
+        std::vector<double> out(n);
+        out[0] = 0.0;
+        for (int j = 0; j + 1 < n; j++) {
+            G = G + at(j);
+            prev = std::fma(dy2, G, prev);
+            out[j + 1] = prev;
+        }
+        double m = 0.0;
+        for (int j = 0; j < n; j++) m = m + out[j];
+        m = m / (double)n;
+        for (int j = 0; j < n; j++) at(j) = out[j] - m;
+        return;
+    }
+    const double a = ay;
+    const double b = std::fma(-2.0, a, lam);   // interior diagonal
+    std::vector<double> cp(n), z(n);
+    if (!py) {
+        const double bE = lam - a;              // mirrored-ghost end rows
+        // Thomas: c'_j = a / m_j, d'_j = (r_j - a d'_{j-1}) / m_j, m_j = b_j - a c'_{j-1}
+        double m = bE;
+        cp[0] = a / m;
+        at(0) = at(0) / m;
+        for (int j = 1; j < n; j++) {
+            const double bj = (j == n - 1) ? bE : b;
+            m = std::fma(-a, cp[j - 1], bj);
+            cp[j] = a / m;
+            at(j) = std::fma(-a, at(j - 1), at(j)) / m;
+        }
+        for (int j = n - 2; j >= 0; j--) at(j) = std::fma(-cp[j], at(j + 1), at(j));
+        return;
+    }
+    // cyclic: A = T' + u v^T with gamma = -b, u = (gamma, 0.., a), v = (1, 0.., a/gamma);
+    // T' has diagonal b - gamma at 0 and b - a*a/gamma at n-1
+    const double gam = -b;
+    const double b0 = b - gam, bn = b - a * a / gam;
+    double m = b0;
+    cp[0] = a / m;
+    at(0) = at(0) / m;
+    z[0] = gam / m;
+    for (int j = 1; j < n; j++) {
+        const double bj = (j == n - 1) ? bn : b;
+        m = std::fma(-a, cp[j - 1], bj);
+        cp[j] = a / m;
+        const double zr = (j == n - 1) ? a : 0.0;
+        at(j) = std::fma(-a, at(j - 1), at(j)) / m;
+        z[j] = std::fma(-a, z[j - 1], zr) / m;
+    }
+    for (int j = n - 2; j >= 0; j--) {
+        at(j) = std::fma(-cp[j], at(j + 1), at(j));
+        z[j] = std::fma(-cp[j], z[j + 1], z[j]);
+    }
+    const double fac = std::fma(a / gam, at(n - 1), at(0)) / (1.0 + std::fma(a / gam, z[n - 1], z[0]));
+    for (int j = 0; j < n; j++) at(j) = std::fma(-fac, z[j], at(j));
+}
+
+// phi solving lap(phi) = rhs (ny x nx row-major), zero mean.
+inline void direct_solve(const PoissonSpec& s, const std::vector<double>& rhs, std::vector<double>& phi) {
+    const int nx = s.nx, ny = s.ny;
+    std::vector<double> tx, lam;
+    direct_basis(nx, s.px, s.dx, tx, lam);
+    std::vector<double> u((size_t)nx * ny);
+    // u[j][k] = sum_i rhs[j][i] tx[k][i], i ascending
+    for (int j = 0; j < ny; j++)
+        for (int k = 0; k < nx; k++) {
+            double acc = 0.0;
+            for (int i = 0; i < nx; i++) acc = std::fma(rhs[(size_t)j * nx + i], tx[(size_t)k * nx + i], acc);
+            u[(size_t)j * nx + k] = acc;
+        }
+    const double ay = 1.0 / (s.dy * s.dy), dy2 = s.dy * s.dy;
+    for (int k = 0; k < nx; k++) direct_ysolve(nx, ny, s.py, ay, dy2, lam[k], k == 0, k, u);
+    phi.assign((size_t)nx * ny, 0.0);
+    for (int j = 0; j < ny; j++)
+        for (int i = 0; i < nx; i++) {
+            double acc = 0.0;
+            for (int k = 0; k < nx; k++) acc = std::fma(u[(size_t)j * nx + k], tx[(size_t)k * nx + i], acc);
+            phi[(size_t)j * nx + i] = acc;
+        }
+}
+
+// rhs of the direct solve: 4 pi G (rho - mean), mean in the batched order
+inline std::vector<double> direct_rhs(const PoissonSpec& s, const std::vector<double>& rho) {
+    const size_t N = (size_t)s.nx * s.ny;
+    const double mean = batch_tile_mean(s.nx, s.ny, rho);
+    const double fourpiG = 4.0 * M_PI * s.G;
+    std::vector<double> rhs(N);
+    for (size_t q = 0; q < N; q++) rhs[q] = fourpiG * (rho[q] - mean);
+    return rhs;
+}
+
 // g = -grad(phi), central differences with the solver's wrap rule (M2:225-235)
 inline void gravity_from_phi(const PoissonSpec& s, const std::vector<double>& phi, std::vector<double>& gx,
                              std::vector<double>& gy) {

@@ -52,6 +52,28 @@ def test_create_rejects_bad_arguments_without_gpu_work():
     assert lib.cc_last_error(None) == b"null handle"
 
 
+def test_batch_create_validates_instances_before_gpu_work():
+    """cc_batch_create checks every instance before touching the device; the
+    message names the instance."""
+    lib = L.lib()
+    ok = Params(Nx=16, Ny=16, gravity_on=True, poisson="direct")
+    cases = [
+        ([ok, Params(Nx=16, Ny=16, gravity_on=True, poisson="sor")], L.CC_ERR_UNSUPPORTED, b"instance 1"),
+        ([ok, Params(Nx=3, Ny=16, gravity_on=False)], L.CC_ERR_ARG, b"instance 1"),
+        ([Params(Nx=16, Ny=16, precision="fp32", gravity_on=False), ok], L.CC_ERR_ARG, b"one precision"),
+        ([Params(Nx=4096, Ny=16, gravity_on=True, poisson="direct")], L.CC_ERR_UNSUPPORTED, b"instance 0"),
+    ]
+    for plist, code, msg in cases:
+        arr = (L.CcMhd2dParams * len(plist))(*[q.to_c() for q in plist])
+        h = C.c_void_p()
+        assert lib.cc_batch_create(arr, len(plist), C.byref(h)) == code
+        assert msg in lib.cc_last_error(h)
+        assert lib.cc_destroy(h) == L.CC_OK
+    h = C.c_void_p()
+    assert lib.cc_batch_create(None, 1, C.byref(h)) == L.CC_ERR_ARG
+    assert lib.cc_batch_advance(None, 1, None) == L.CC_ERR_ARG
+
+
 def test_ic_collapse_is_seeded_and_divergence_free():
     p = Params(Nx=32, Ny=24, x0=-1, x1=1, y0=-1, y1=1, periodic_x=False, periodic_y=False)
     U1, B1 = ic_collapse(p, seed=0)
