@@ -349,6 +349,8 @@ def run_ours(args) -> None:
     }
     if world == 1 and not args.skip_3d:
         line["mhd3d"] = run_3d(args, stream)
+    if not args.skip_ensemble:
+        line["ensemble"] = run_ensemble(args, stream, rank, world, barrier, max_over_ranks, value32 / world)
     if world == 1 and rank == 0 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(args.cpu_sample_grid, args.cpu_steps)
     if rank == 0:
@@ -396,6 +398,68 @@ def run_3d(args, stream) -> dict:
     return out
 
 
+def run_ensemble(args, stream, rank: int, world: int, barrier, max_over_ranks, single_fp32: float) -> dict:
+    """Batched ensemble: 512 independent 2D collapse instances on [-1,1]^2
+    with outflow boundaries, side drawn uniformly from {64,96,128,192,256}
+    (seed 2), core amplitude U(2,20), width U(0.05,0.2), Bx U(0,0.2), eta
+    log-uniform [1e-4,1e-2]; gamma 5/3, G 1, CFL 0.4, direct Poisson; FP32
+    state with FP64 reductions and FP64 Poisson.  Instances are split over
+    the ranks by cell count (no collective inside a step)."""
+    import numpy as np
+    import torch
+
+    from core_collapse_b200.batch import BatchSolver, collapse_ensemble, partition_by_cells
+    params, states = collapse_ensemble(args.ensemble, seed=2, precision="fp32")
+    mine = partition_by_cells(params, world)[rank]
+    total_cells = sum(p.Nx * p.Ny for p in params)
+    steps = max(1, args.ensemble_steps)
+    out = {"workload": f"{args.ensemble} independent 2D collapse instances, sides from {{64,96,128,192,256}} (seed 2), "
+                       "outflow [-1,1]^2, per-instance core amplitude/width, Bx, eta; direct Poisson",
+           "instances": args.ensemble, "cells": total_cells, "steps": steps, "warmup": args.warmup,
+           "dtype": "f32", "reductions": "f64", "poisson": "direct (FP64)", "scaling": "strong"}
+    b = BatchSolver([params[i] for i in mine])
+    b.set_stream(stream.cuda_stream)
+    for k, i in enumerate(mine):
+        b.upload(k, *states[i])
+    shape, tune_ms = b.autotune(reps=3)
+    b.advance(args.warmup, np.zeros(len(mine)))
+    barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    b.advance(steps)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    barrier()
+    ms = max_over_ranks(e0.elapsed_time(e1))
+    info = b.info()
+    nonfinite = sum(b.diagnostics(k)["nonfinite"] for k in range(len(mine)))
+    # share of the stage kernels in a step, from profiled stage events (eager, no graph)
+    b.set_profiling(True)
+    b.reset_perf()
+    e0.record(stream)
+    b.advance(3)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    prof_ms = e0.elapsed_time(e1)
+    pf = b.perf()
+    b.close()
+    value = total_cells * steps / (ms / 1000.0)
+    out.update({"value": value, "unit": UNIT, "ms_per_step": ms / steps,
+                "ensemble_over_single_grid": value / world / single_fp32 if single_fp32 else None,
+                "tile": [info["tile_x"], info["tile_y"]], "autotune_choice": shape, "autotune_stage_ms": tune_ms,
+                "stage_ctas": info["stage_ctas"], "stage_tiles": info["stage_tiles"],
+                "stage_share_of_step": pf["stage_ms"] / prof_ms if prof_ms > 0 else None,
+                "nonfinite_instances": nonfinite, "device_bytes_rank0": info["device_bytes"]})
+    return out
+
+
+def run_ensemble_only(args) -> None:
+    import torch
+    torch.cuda.set_device(0)
+    stream = torch.cuda.Stream()
+    print(json.dumps(run_ensemble(args, stream, 0, 1, torch.cuda.synchronize, lambda x: x, 0.0)), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
     ap.add_argument("--gpus", type=int, default=1)
@@ -410,9 +474,17 @@ def main():
     ap.add_argument("--skip-3d", action="store_true")
     ap.add_argument("--grid3d", type=int, default=256)
     ap.add_argument("--steps3d", type=int, default=20)
+    ap.add_argument("--skip-ensemble", action="store_true")
+    ap.add_argument("--ensemble", type=int, default=512)
+    ap.add_argument("--ensemble-steps", type=int, default=60)
+    ap.add_argument("--ensemble-only", action="store_true",
+                    help="time only the batched ensemble (a profiling aid; prints the ensemble block)")
     args = ap.parse_args()
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")
+    if args.ensemble_only:
+        run_ensemble_only(args)
+        return
     if args.impl == "reference":
         run_reference(args)
     else:

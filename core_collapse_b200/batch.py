@@ -113,6 +113,13 @@ class BatchSolver:
         self._check(self._lib.cc_batch_get_info(self._h, C.byref(o)))
         return {f: getattr(o, f) for f, _ in L.CcBatchInfo._fields_}
 
+    def set_profiling(self, on: bool):
+        """Bracket stage launches with CUDA events (time loops then run without graphs)."""
+        self._check(self._lib.cc_set_profiling(self._h, 1 if on else 0))
+
+    def reset_perf(self):
+        self._check(self._lib.cc_reset_perf(self._h))
+
     def perf(self) -> dict:
         pf = L.CcPerf()
         self._check(self._lib.cc_get_perf(self._h, C.byref(pf)))
@@ -142,3 +149,34 @@ def collapse_ensemble(n: int, seed: int = 2, sides=(64, 96, 128, 192, 256), prec
         params.append(p)
         states.append((U, B))
     return params, states
+
+
+def partition_by_cells(params: list[Params], world: int) -> list[list[int]]:
+    """Split instance indices over `world` GPUs, balancing cells: largest
+    instance first onto the least-loaded GPU (ties to the lower rank), each
+    GPU's list kept in instance order.  The ensemble needs no collective
+    inside a step; ranks only gather results at the end."""
+    if world < 1:
+        raise ValueError("world must be >= 1")
+    order = sorted(range(len(params)), key=lambda i: (-params[i].Nx * params[i].Ny, i))
+    load = [0] * world
+    parts: list[list[int]] = [[] for _ in range(world)]
+    for i in order:
+        r = min(range(world), key=lambda k: (load[k], k))
+        parts[r].append(i)
+        load[r] += params[i].Nx * params[i].Ny
+    return [sorted(pl) for pl in parts]
+
+
+def gather_by_instance(local: dict[int, object], world: int) -> dict[int, object]:
+    """All-gather per-instance results {instance: value} from every rank
+    (torch.distributed, any backend) into one dict on every rank."""
+    if world == 1:
+        return dict(local)
+    import torch.distributed as dist
+    out: list = [None] * world
+    dist.all_gather_object(out, local)
+    merged: dict[int, object] = {}
+    for d in out:
+        merged.update(d)
+    return merged

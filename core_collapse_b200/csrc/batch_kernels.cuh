@@ -35,8 +35,11 @@ template <class T> struct BatchInst {
     const double* txt;    // its transpose
     const double* lamx;   // nx eigenvalues of the x second difference (1/dx^2 units included)
     double* ah;           // ny*nx: transformed rhs, then transformed phi (in place)
-    double* w1;           // ny*nx scratch (Thomas coefficients)
-    double* w2;           // ny*nx scratch (cyclic correction vector)
+    // factors of the y systems, [j*nx + k] (set up once per grid shape):
+    const double* ycp;    // Thomas cp_j
+    const double* yinv;   // 1 / m_j
+    const double* yz;     // cyclic correction vector (periodic y only)
+    const double* yfden;  // nx: 1 / (1 + v.z) (periodic y only)
     double fourpiG;
     double ay;            // 1/dy^2
     double dy2;           // dy^2

@@ -58,6 +58,45 @@ void x_basis(int n, bool periodic, double d, std::vector<double>& tx, std::vecto
     }
 }
 
+// Factors of the y systems (Dyy + lam_k) u = r of every x wavenumber k >= 1
+// of a grid, stored [j*nx + k]: m_j = b_j - a cp_{j-1} (fma), inv_j = 1/m_j,
+// cp_j = a inv_j, clamp end rows b = lam - a; periodic y: Sherman-Morrison
+// with gamma = -b (rows 0 and n-1 of T' modified), z = T'^-1 (gamma, 0.., a)
+// and fden = 1 / (1 + v.z).  The CPU oracle sets up the same values the same way.
+void y_factors(int nx, int ny, bool py, double a, const std::vector<double>& lam, std::vector<double>& cp,
+               std::vector<double>& inv, std::vector<double>& z, std::vector<double>& fden) {
+    cp.assign((size_t)nx * ny, 0.0);
+    inv.assign((size_t)nx * ny, 0.0);
+    z.assign(py ? (size_t)nx * ny : 0, 0.0);
+    fden.assign(nx, 0.0);
+    for (int k = 1; k < nx; k++) {
+        const double lk = lam[k];
+        const double b = std::fma(-2.0, a, lk);
+        const double gam = -b;
+        const double bE = py ? b - gam : lk - a;
+        const double bL = py ? b - a * a / gam : lk - a;
+        double cprev = 0.0;
+        for (int j = 0; j < ny; j++) {
+            const double bj = (j == 0) ? bE : (j == ny - 1 ? bL : b);
+            const double m = (j == 0) ? bj : std::fma(-a, cprev, bj);
+            const double iv = 1.0 / m;
+            inv[(size_t)j * nx + k] = iv;
+            cprev = a * iv;
+            cp[(size_t)j * nx + k] = cprev;
+        }
+        if (py) {
+            for (int j = 0; j < ny; j++) {
+                const double zr = (j == 0) ? gam : (j == ny - 1 ? a : 0.0);
+                const double iv = inv[(size_t)j * nx + k];
+                z[(size_t)j * nx + k] = (j == 0) ? zr * iv : std::fma(-a, z[(size_t)(j - 1) * nx + k], zr) * iv;
+            }
+            for (int j = ny - 2; j >= 0; j--)
+                z[(size_t)j * nx + k] = std::fma(-cp[(size_t)j * nx + k], z[(size_t)(j + 1) * nx + k], z[(size_t)j * nx + k]);
+            fden[k] = 1.0 / (1.0 + std::fma(a / gam, z[(size_t)(ny - 1) * nx + k], z[k]));
+        }
+    }
+}
+
 struct BatchBase {
     virtual ~BatchBase() {}
     virtual int init() = 0;
@@ -83,9 +122,12 @@ template <class T> struct Batch : BatchBase {
     std::vector<void*> allocs;
     size_t bytes = 0;
     // work-lists
+    // stage candidates: tile shape k = c % NS, launched persistent (c < NS:
+    // one CTA per resident slot, each walking a contiguous run of the
+    // work-list) or flat (c >= NS: one CTA per tile, scheduled by hardware)
     std::vector<int2*> swork;        // per stage shape
     std::vector<int> nswork;
-    std::vector<int> sgrid;          // persistent CTAs per shape
+    std::vector<int> sgrid;          // CTAs per candidate
     int2* rwork = nullptr; int nrwork = 0;
     int2* gwork = nullptr; int ngwork = 0;
     int2* ywork = nullptr; int nywork = 0;
@@ -154,8 +196,9 @@ template <class T> struct Batch : BatchBase {
         T* pool = nullptr;
         if (int r = dalloc(&pool, total)) return r;
         CC_CUDA(cudaMemsetAsync(pool, 0, sizeof(T) * total, st()));
-        // ---- direct Poisson: bases per (nx, periodic, dx), work arrays per instance ----
+        // ---- direct Poisson: x bases per (nx, periodic, dx), y factors per grid shape ----
         std::map<std::tuple<int, int, double>, std::tuple<double*, double*, double*>> bases;
+        std::map<std::tuple<int, int, double, int, int, double>, std::tuple<double*, double*, double*, double*>> yfac;
         for (int i = 0; i < n; i++) {
             const cc_mhd2d_params& q = p[i];
             const int nx = q.Nx, ny = q.Ny, P = pitch[i];
@@ -206,11 +249,25 @@ template <class T> struct Batch : BatchBase {
                 I.tx = std::get<0>(it->second);
                 I.txt = std::get<1>(it->second);
                 I.lamx = std::get<2>(it->second);
-                double* wk = nullptr;
-                if (int r = dalloc(&wk, (size_t)nx * ny * 3)) return r;
-                I.ah = wk;
-                I.w1 = wk + (size_t)nx * ny;
-                I.w2 = wk + 2 * (size_t)nx * ny;
+                auto ykey = std::make_tuple(nx, q.periodic_x ? 1 : 0, dx, ny, q.periodic_y ? 1 : 0, dy);
+                auto yt = yfac.find(ykey);
+                if (yt == yfac.end()) {
+                    std::vector<double> tx, lam, cp, inv, z, fden;
+                    x_basis(nx, q.periodic_x != 0, dx, tx, lam);
+                    y_factors(nx, ny, q.periodic_y != 0, 1.0 / (dy * dy), lam, cp, inv, z, fden);
+                    double *d_cp, *d_inv, *d_z = nullptr, *d_fden;
+                    if (int r = upload_vec(&d_cp, cp)) return r;
+                    if (int r = upload_vec(&d_inv, inv)) return r;
+                    if (q.periodic_y)
+                        if (int r = upload_vec(&d_z, z)) return r;
+                    if (int r = upload_vec(&d_fden, fden)) return r;
+                    yt = yfac.emplace(ykey, std::make_tuple(d_cp, d_inv, d_z, d_fden)).first;
+                }
+                I.ycp = std::get<0>(yt->second);
+                I.yinv = std::get<1>(yt->second);
+                I.yz = std::get<2>(yt->second);
+                I.yfden = std::get<3>(yt->second);
+                if (int r = dalloc(&I.ah, (size_t)nx * ny)) return r;
             }
             BatchRed& R = hred[i];
             R.ncell = (double)nx * (double)ny;
@@ -242,7 +299,7 @@ template <class T> struct Batch : BatchBase {
         const int NS = BatchLaunch<T>::n_shapes();
         swork.assign(NS, nullptr);
         nswork.assign(NS, 0);
-        sgrid.assign(NS, 1);
+        sgrid.assign(2 * NS, 1);
         for (int k = 0; k < NS; k++) {
             const TileShape sh = BatchLaunch<T>::shape(k);
             std::vector<int2> sw;
@@ -257,6 +314,7 @@ template <class T> struct Batch : BatchBase {
             CC_CUDA(BatchLaunch<T>::resident(k, &per_sm));
             if (per_sm < 1) per_sm = 1;
             sgrid[k] = std::max(1, std::min(nswork[k], per_sm * nsm));
+            sgrid[NS + k] = std::max(1, nswork[k]);
         }
         if (int r = upload_vec(&dinst, hinst)) return r;
         if (int r = upload_vec(&dred, hred)) return r;
@@ -365,8 +423,9 @@ template <class T> struct Batch : BatchBase {
             CC_CUDA(cudaEventCreate(&e1));
             CC_CUDA(cudaEventRecord(e0, st()));
         }
-        CC_CUDA(BatchLaunch<T>::stage(shape, sgrid[shape], dinst, swork[shape], nswork[shape], src, dst_, defer,
-                                      any_grav, dt, active, st()));
+        const int k = shape % BatchLaunch<T>::n_shapes();
+        CC_CUDA(BatchLaunch<T>::stage(k, sgrid[shape], dinst, swork[k], nswork[k], src, dst_, defer, any_grav, dt,
+                                      active, st()));
         count(1);
         if (h->profiling) {
             CC_CUDA(cudaEventRecord(e1, st()));
@@ -488,12 +547,14 @@ template <class T> struct Batch : BatchBase {
         CC_CUDA(cudaEventCreate(&e1));
         int best = shape;
         double best_ms = 1e300;
-        for (int k = 0; k < BatchLaunch<T>::n_shapes(); k++) {
-            CC_CUDA(BatchLaunch<T>::stage(k, sgrid[k], dinst, swork[k], nswork[k], cur, b, false, any_grav, dt,
+        const int NS = BatchLaunch<T>::n_shapes();
+        for (int c = 0; c < 2 * NS; c++) {
+            const int k = c % NS;
+            CC_CUDA(BatchLaunch<T>::stage(k, sgrid[c], dinst, swork[k], nswork[k], cur, b, false, any_grav, dt,
                                           active, st()));
             CC_CUDA(cudaEventRecord(e0, st()));
             for (int r = 0; r < reps; r++)
-                CC_CUDA(BatchLaunch<T>::stage(k, sgrid[k], dinst, swork[k], nswork[k], cur, b, false, any_grav, dt,
+                CC_CUDA(BatchLaunch<T>::stage(k, sgrid[c], dinst, swork[k], nswork[k], cur, b, false, any_grav, dt,
                                               active, st()));
             CC_CUDA(cudaEventRecord(e1, st()));
             CC_CUDA(cudaEventSynchronize(e1));
@@ -501,7 +562,7 @@ template <class T> struct Batch : BatchBase {
             CC_CUDA(cudaEventElapsedTime(&ms, e0, e1));
             count(reps + 1);
             const double per = (double)ms / reps;
-            if (per < best_ms) { best_ms = per; best = k; }
+            if (per < best_ms) { best_ms = per; best = c; }
         }
         cudaEventDestroy(e0);
         cudaEventDestroy(e1);
@@ -513,7 +574,7 @@ template <class T> struct Batch : BatchBase {
     }
 
     int set_shape(int k) override {
-        if (k < 0 || k >= BatchLaunch<T>::n_shapes()) return fail(h, CC_ERR_ARG, "no such stage tile candidate");
+        if (k < 0 || k >= 2 * BatchLaunch<T>::n_shapes()) return fail(h, CC_ERR_ARG, "no such stage candidate");
         if (k != shape) invalidate_graph();
         shape = k;
         return CC_OK;
@@ -525,10 +586,11 @@ template <class T> struct Batch : BatchBase {
         o->precision = sizeof(T) == 8 ? CC_FP64 : CC_FP32;
         for (int i = 0; i < n; i++) o->cells += (long long)p[i].Nx * p[i].Ny;
         o->shape = shape;
-        o->n_shapes = BatchLaunch<T>::n_shapes();
-        const TileShape sh = BatchLaunch<T>::shape(shape);
+        const int NS = BatchLaunch<T>::n_shapes();
+        o->n_shapes = 2 * NS;
+        const TileShape sh = BatchLaunch<T>::shape(shape % NS);
         o->tile_x = sh.tx; o->tile_y = sh.ty;
-        o->stage_tiles = nswork[shape];
+        o->stage_tiles = nswork[shape % NS];
         o->stage_ctas = sgrid[shape];
         o->reduce_tiles = nrwork;
         o->poisson_tiles = ngwork;

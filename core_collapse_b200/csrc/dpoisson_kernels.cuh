@@ -18,6 +18,8 @@
 // Work-lists: GEMM tiles {instance, (tm << 16) | tn} of DPM x DPN outputs;
 // y-solve blocks {instance, column block} of DPC columns, one thread per column.
 #pragma once
+#include <type_traits>
+
 #include "batch_kernels.cuh"
 
 namespace ccb {
@@ -25,10 +27,15 @@ namespace ccb {
 constexpr int DPM = 64, DPN = 64, DPK = 16, DPNT = 256;   // GEMM tile, 4 x 4 outputs per thread
 constexpr int DPC = 32;                                    // y-solve columns per block
 
+// Software-pipelined tile loop: the next K chunk is loaded into registers
+// while the current one is multiplied from shared memory; raw values are
+// converted (MODE 0: 4 pi G (rho - mean)) only when they are stored, so no
+// instruction waits on a load in flight during the multiply.
 template <class T, int MODE>
 __global__ void __launch_bounds__(DPNT)
 dp_gemm_kernel(const BatchInst<T>* __restrict__ inst, const int2* __restrict__ gwork, int ngwork, int src,
                const double* __restrict__ rho_mean, const int* __restrict__ active) {
+    using AT = typename std::conditional<MODE == 0, T, double>::type;
     __shared__ double As[DPK][DPM + 1];   // k-major A tile
     __shared__ double Bs[DPK][DPN];
     const int tr = threadIdx.x / 16, tc = threadIdx.x % 16;
@@ -40,30 +47,43 @@ dp_gemm_kernel(const BatchInst<T>* __restrict__ inst, const int2* __restrict__ g
         const int m0 = (it.y >> 16) * DPM, n0 = (it.y & 0xffff) * DPN;
         const double* __restrict__ B = (MODE == 0) ? I.txt : I.tx;   // K x N row-major, K = N = nx
         const T* __restrict__ rho = I.buf[src].rho;
+        const double* __restrict__ ah = I.ah;
         const double mean = (MODE == 0) ? rho_mean[it.x] : 0.0;
         const double fpg = I.fourpiG;
+        AT ra[4];
+        double rb[4];
+        auto gload = [&](int k0) {
+#pragma unroll
+            for (int q = 0; q < 4; q++) {
+                const int e = threadIdx.x + q * DPNT;
+                const int gm = m0 + e / DPK, gk = k0 + e % DPK;
+                ra[q] = AT(0);
+                if (gm < ny && gk < nx) {
+                    if (MODE == 0) ra[q] = (AT)rho[(size_t)gm * P + gk];
+                    else ra[q] = (AT)ah[(size_t)gm * nx + gk];
+                }
+                const int gkb = k0 + e / DPN, gn = n0 + e % DPN;
+                rb[q] = (gkb < nx && gn < nx) ? B[(size_t)gkb * nx + gn] : 0.0;
+            }
+        };
         double acc[4][4];
 #pragma unroll
         for (int r = 0; r < 4; r++)
 #pragma unroll
             for (int c = 0; c < 4; c++) acc[r][c] = 0.0;
+        gload(0);
         for (int k0 = 0; k0 < nx; k0 += DPK) {
 #pragma unroll
             for (int q = 0; q < 4; q++) {
                 const int e = threadIdx.x + q * DPNT;
                 const int m = e / DPK, kk = e % DPK;
-                const int gm = m0 + m, gk = k0 + kk;
-                double v = 0.0;
-                if (gm < ny && gk < nx) {
-                    if (MODE == 0) v = fpg * ((double)rho[(size_t)gm * P + gk] - mean);
-                    else v = I.ah[(size_t)gm * nx + gk];
-                }
+                double v = (double)ra[q];
+                if (MODE == 0) v = (m0 + m < ny && k0 + kk < nx) ? fpg * (v - mean) : 0.0;
                 As[kk][m] = v;
-                const int kb = e / DPN, nb = e % DPN;
-                const int gkb = k0 + kb, gn = n0 + nb;
-                Bs[kb][nb] = (gkb < nx && gn < nx) ? B[(size_t)gkb * nx + gn] : 0.0;
+                Bs[e / DPN][e % DPN] = rb[q];
             }
             __syncthreads();
+            if (k0 + DPK < nx) gload(k0 + DPK);
             const int kend = min(DPK, nx - k0);
             for (int kk = 0; kk < kend; kk++) {
                 double a[4], b[4];
@@ -93,7 +113,9 @@ dp_gemm_kernel(const BatchInst<T>* __restrict__ inst, const int2* __restrict__ g
     }
 }
 
-// One thread per x wavenumber (column of ah), sequential along y.
+// One thread per x wavenumber (column of ah), sequential along y, with the
+// factors set up at handle creation: each sweep is a chain of fma's (no
+// division), and the loads of the factors do not depend on the chain.
 template <class T>
 __global__ void __launch_bounds__(DPC)
 dp_ysolve_kernel(const BatchInst<T>* __restrict__ inst, const int2* __restrict__ ywork, int nywork,
@@ -106,13 +128,11 @@ dp_ysolve_kernel(const BatchInst<T>* __restrict__ inst, const int2* __restrict__
         const int col = it.y * DPC + threadIdx.x;
         if (col >= nx) continue;
         double* __restrict__ u = I.ah + col;
-        double* __restrict__ cp = I.w1 + col;
-        double* __restrict__ z = I.w2 + col;
         const size_t S = (size_t)nx;
         const bool py = I.c.ay.periodic != 0;
         const double a = I.ay;
         if (col == 0) {
-            // singular k = 0: flux G_j = a (u_{j+1} - u_j) = G_{j-1} + r_j
+            // singular k = 0: flux G_j = a (u_{j+1} - u_j) = G_{j-1} + r_j, then mean removal
             double g0 = 0.0;
             if (py) {
                 double Sr = 0.0, SS = 0.0;
@@ -120,72 +140,37 @@ dp_ysolve_kernel(const BatchInst<T>* __restrict__ inst, const int2* __restrict__
                 g0 = -(SS / (double)n);
             }
             double G = g0, prev = 0.0;
-            cp[0] = 0.0;   // the solution is built in cp, then moved to u
+            double r = u[0];
+            u[0] = 0.0;
             for (int j = 0; j + 1 < n; j++) {
-                G = G + u[j * S];
+                G = G + r;
+                r = u[(j + 1) * S];
                 prev = fma(I.dy2, G, prev);
-                cp[(j + 1) * S] = prev;
+                u[(j + 1) * S] = prev;
             }
             double m = 0.0;
-            for (int j = 0; j < n; j++) m = m + cp[j * S];
+            for (int j = 0; j < n; j++) m = m + u[j * S];
             m = m / (double)n;
-            for (int j = 0; j < n; j++) u[j * S] = cp[j * S] - m;
+            for (int j = 0; j < n; j++) u[j * S] = u[j * S] - m;
             continue;
         }
-        const double lam = I.lamx[col];
-        const double b = fma(-2.0, a, lam);
-        if (!py) {
-            const double bE = lam - a;
-            double m = bE;
-            double cprev = a / m;
-            cp[0] = cprev;
-            double dprev = u[0] / m;
-            u[0] = dprev;
-            for (int j = 1; j < n; j++) {
-                const double bj = (j == n - 1) ? bE : b;
-                m = fma(-a, cprev, bj);
-                cprev = a / m;
-                cp[j * S] = cprev;
-                dprev = fma(-a, dprev, u[j * S]) / m;
-                u[j * S] = dprev;
-            }
-            double x = dprev;
-            for (int j = n - 2; j >= 0; j--) {
-                x = fma(-cp[j * S], x, u[j * S]);
-                u[j * S] = x;
-            }
-            continue;
-        }
-        const double gam = -b;
-        const double b0 = b - gam, bn = b - a * a / gam;
-        double m = b0;
-        double cprev = a / m;
-        cp[0] = cprev;
-        double dprev = u[0] / m, zprev = gam / m;
-        u[0] = dprev;
-        z[0] = zprev;
+        const double* __restrict__ cp = I.ycp + col;
+        const double* __restrict__ inv = I.yinv + col;
+        double d = u[0] * inv[0];
+        u[0] = d;
         for (int j = 1; j < n; j++) {
-            const double bj = (j == n - 1) ? bn : b;
-            m = fma(-a, cprev, bj);
-            cprev = a / m;
-            cp[j * S] = cprev;
-            const double zr = (j == n - 1) ? a : 0.0;
-            dprev = fma(-a, dprev, u[j * S]) / m;
-            zprev = fma(-a, zprev, zr) / m;
-            u[j * S] = dprev;
-            z[j * S] = zprev;
+            d = fma(-a, d, u[j * S]) * inv[j * S];
+            u[j * S] = d;
         }
-        double x = dprev, zz = zprev;
+        double x = d;
         for (int j = n - 2; j >= 0; j--) {
-            const double c = cp[j * S];
-            x = fma(-c, x, u[j * S]);
-            zz = fma(-c, zz, z[j * S]);
+            x = fma(-cp[j * S], x, u[j * S]);
             u[j * S] = x;
-            z[j * S] = zz;
         }
-        // x, zz hold the j = 0 entries; v^T x = x_0 + (a / gamma) x_{n-1}
-        const double xl = u[(n - 1) * S], zl = z[(n - 1) * S];
-        const double fac = fma(a / gam, xl, x) / (1.0 + fma(a / gam, zl, zz));
+        if (!py) continue;
+        const double* __restrict__ z = I.yz + col;
+        const double gam = -fma(-2.0, a, I.lamx[col]);
+        const double fac = fma(a / gam, d, x) * I.yfden[col];   // d = x_{n-1}, x = x_0
         for (int j = 0; j < n; j++) u[j * S] = fma(-fac, z[j * S], u[j * S]);
     }
 }

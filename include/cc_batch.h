@@ -37,8 +37,8 @@ typedef struct cc_batch_info {
     int32_t n;               /* instances                                  */
     int32_t precision;       /* CC_FP64 or CC_FP32                         */
     int64_t cells;           /* sum of Nx*Ny over instances                */
-    int32_t shape;           /* stage tile candidate in use                */
-    int32_t n_shapes;
+    int32_t shape;           /* stage candidate in use                     */
+    int32_t n_shapes;        /* candidates: tile shapes x {persistent, one CTA per tile} */
     int32_t tile_x, tile_y;  /* its tile                                   */
     int32_t stage_tiles;     /* work-list length of the stage kernel       */
     int32_t stage_ctas;      /* persistent CTAs of the stage kernel        */
@@ -65,9 +65,11 @@ int cc_batch_advance(cc_handle* h, int nsteps, double* t);
 
 int cc_batch_diagnostics(cc_handle* h, int inst, cc_diag* d);
 
-/* Time every stage-tile candidate on the resident state (reps launches
- * each) and keep the fastest; shape / ms (may be NULL) receive the choice and
- * its mean stage time. */
+/* Time every stage candidate on the resident state (reps launches each) and
+ * keep the fastest; shape / ms (may be NULL) receive the choice and its mean
+ * stage time.  Candidate c uses tile shape c % S of the S compiled shapes,
+ * launched persistent (c < S: one CTA per resident slot walking a contiguous
+ * run of the tile work-list) or flat (c >= S: one CTA per tile). */
 int cc_batch_autotune(cc_handle* h, int reps, int* shape, double* ms);
 /* Use candidate `shape` (0 <= shape < n_shapes). */
 int cc_batch_set_shape(cc_handle* h, int shape);

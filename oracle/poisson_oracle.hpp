@@ -277,6 +277,45 @@ inline double batch_tile_mean(int nx, int ny, const std::vector<double>& rho) {
     return total / ((double)nx * (double)ny);
 }
 
+// Factors of the y system (Dyy + lam) u = r for one x wavenumber, set up
+// once per grid: m_j = b_j - a cp_{j-1} (fma), inv_j = 1/m_j, cp_j = a inv_j;
+// the clamp rule's end rows have b = lam - a.  Periodic y (cyclic system):
+// Sherman-Morrison with gamma = -b, u = (gamma, 0.., a), v = (1, 0.., a/gamma);
+// T' has b - gamma at row 0 and b - a*a/gamma at row n-1; z = T'^-1 u and
+// fden = 1 / (1 + v.z) are part of the factors.
+struct YFactors {
+    std::vector<double> cp, inv, z;
+    double fden = 0.0;
+};
+
+inline YFactors direct_yfactors(int n, bool py, double a, double lam) {
+    YFactors f;
+    f.cp.assign(n, 0.0);
+    f.inv.assign(n, 0.0);
+    const double b = std::fma(-2.0, a, lam);
+    const double gam = -b;
+    const double bE = py ? b - gam : lam - a;           // row 0
+    const double bL = py ? b - a * a / gam : lam - a;   // row n-1
+    double cprev = 0.0;
+    for (int j = 0; j < n; j++) {
+        const double bj = (j == 0) ? bE : (j == n - 1 ? bL : b);
+        const double m = (j == 0) ? bj : std::fma(-a, cprev, bj);
+        f.inv[j] = 1.0 / m;
+        cprev = a * f.inv[j];
+        f.cp[j] = cprev;
+    }
+    if (py) {
+        f.z.assign(n, 0.0);
+        for (int j = 0; j < n; j++) {
+            const double zr = (j == 0) ? gam : (j == n - 1 ? a : 0.0);
+            f.z[j] = (j == 0) ? zr * f.inv[0] : std::fma(-a, f.z[j - 1], zr) * f.inv[j];
+        }
+        for (int j = n - 2; j >= 0; j--) f.z[j] = std::fma(-f.cp[j], f.z[j + 1], f.z[j]);
+        f.fden = 1.0 / (1.0 + std::fma(a / gam, f.z[n - 1], f.z[0]));
+    }
+    return f;
+}
+
 // One y system for x wavenumber k (column col of the ny x nx array u, solved in place).
 inline void direct_ysolve(int nx, int ny, bool py, double ay, double dy2, double lam, bool singular, int col,
                           std::vector<double>& u) {
@@ -306,45 +345,14 @@ inline void direct_ysolve(int nx, int ny, bool py, double ay, double dy2, double
         return;
     }
     const double a = ay;
-    const double b = std::fma(-2.0, a, lam);   // interior diagonal
-    std::vector<double> cp(n), z(n);
-    if (!py) {
-        const double bE = lam - a;              // mirrored-ghost end rows
-        // Thomas: c'_j = a / m_j, d'_j = (r_j - a d'_{j-1}) / m_j, m_j = b_j - a c'_{j-1}
-        double m = bE;
-        cp[0] = a / m;
-        at(0) = at(0) / m;
-        for (int j = 1; j < n; j++) {
-            const double bj = (j == n - 1) ? bE : b;
-            m = std::fma(-a, cp[j - 1], bj);
-            cp[j] = a / m;
-            at(j) = std::fma(-a, at(j - 1), at(j)) / m;
-        }
-        for (int j = n - 2; j >= 0; j--) at(j) = std::fma(-cp[j], at(j + 1), at(j));
-        return;
-    }
-    // cyclic: A = T' + u v^T with gamma = -b, u = (gamma, 0.., a), v = (1, 0.., a/gamma);
-    // T' has diagonal b - gamma at 0 and b - a*a/gamma at n-1
-    const double gam = -b;
-    const double b0 = b - gam, bn = b - a * a / gam;
-    double m = b0;
-    cp[0] = a / m;
-    at(0) = at(0) / m;
-    z[0] = gam / m;
-    for (int j = 1; j < n; j++) {
-        const double bj = (j == n - 1) ? bn : b;
-        m = std::fma(-a, cp[j - 1], bj);
-        cp[j] = a / m;
-        const double zr = (j == n - 1) ? a : 0.0;
-        at(j) = std::fma(-a, at(j - 1), at(j)) / m;
-        z[j] = std::fma(-a, z[j - 1], zr) / m;
-    }
-    for (int j = n - 2; j >= 0; j--) {
-        at(j) = std::fma(-cp[j], at(j + 1), at(j));
-        z[j] = std::fma(-cp[j], z[j + 1], z[j]);
-    }
-    const double fac = std::fma(a / gam, at(n - 1), at(0)) / (1.0 + std::fma(a / gam, z[n - 1], z[0]));
-    for (int j = 0; j < n; j++) at(j) = std::fma(-fac, z[j], at(j));
+    const YFactors f = direct_yfactors(n, py, a, lam);
+    at(0) = at(0) * f.inv[0];
+    for (int j = 1; j < n; j++) at(j) = std::fma(-a, at(j - 1), at(j)) * f.inv[j];
+    for (int j = n - 2; j >= 0; j--) at(j) = std::fma(-f.cp[j], at(j + 1), at(j));
+    if (!py) return;
+    const double gam = -std::fma(-2.0, a, lam);
+    const double fac = std::fma(a / gam, at(n - 1), at(0)) * f.fden;
+    for (int j = 0; j < n; j++) at(j) = std::fma(-fac, f.z[j], at(j));
 }
 
 // phi solving lap(phi) = rhs (ny x nx row-major), zero mean.
