@@ -28,7 +28,7 @@ template <class T> struct Flux { T f0, f1, f2, f3, f4, f5, f6; };  // rho,mx,my,
 
 // enforce_floors (M2:114-124)
 template <class T>
-__device__ __forceinline__ void floors(const M2Const<T>& c, T& rho, T mx, T my, T mz, T& E, T Bx, T By, T Bz) {
+__host__ __device__ __forceinline__ void floors(const M2Const<T>& c, T& rho, T mx, T my, T mz, T& E, T Bx, T By, T Bz) {
     rho = vmax(rho, c.floor_rho);
     T u = mx / rho, v = my / rho, w = mz / rho;
     T kin = T(0.5) * rho * (u * u + v * v + w * w);
@@ -42,7 +42,7 @@ __device__ __forceinline__ void floors(const M2Const<T>& c, T& rho, T mx, T my, 
 
 // cons_to_prim (M2:126-135)
 template <class T>
-__device__ __forceinline__ Prim<T> to_prim(const M2Const<T>& c, T rho, T mx, T my, T mz, T E, T Bx, T By, T Bz) {
+__host__ __device__ __forceinline__ Prim<T> to_prim(const M2Const<T>& c, T rho, T mx, T my, T mz, T E, T Bx, T By, T Bz) {
     rho = vmax(rho, c.floor_rho);
     T u = mx / rho, v = my / rho, w = mz / rho;
     T kin = T(0.5) * rho * (u * u + v * v + w * w);
@@ -56,14 +56,14 @@ __device__ __forceinline__ Prim<T> to_prim(const M2Const<T>& c, T rho, T mx, T m
 
 // total energy of a primitive state, ideal gas (M2:357, 397, 482, 495)
 template <class T>
-__device__ __forceinline__ T energy(const M2Const<T>& c, const Prim<T>& W) {
+__host__ __device__ __forceinline__ T energy(const M2Const<T>& c, const Prim<T>& W) {
     T B2 = W.bx * W.bx + W.by * W.by + W.bz * W.bz;
     return W.P / c.gm1 + T(0.5) * W.r * (W.u * W.u + W.v * W.v + W.w * W.w) + T(0.5) * B2;
 }
 
 // fast magnetosonic speed with normal component bn (M2:148-174)
 template <class T>
-__device__ __forceinline__ T fast_speed(const M2Const<T>& c, const Prim<T>& W, T bn) {
+__host__ __device__ __forceinline__ T fast_speed(const M2Const<T>& c, const Prim<T>& W, T bn) {
     T a2 = c.gamma * W.P / vmax(W.r, c.floor_rho);
     T b2 = W.bx * W.bx + W.by * W.by + W.bz * W.bz;
     T rho = vmax(W.r, T(1e-300));
@@ -79,7 +79,7 @@ __device__ __forceinline__ T fast_speed(const M2Const<T>& c, const Prim<T>& W, T
 // Cst is the solver's constant block: energy(c, W) and fast_speed(c, W, bn)
 // are overloaded on it.
 template <class T, class Cst>
-__device__ __forceinline__ Flux<T> ideal_flux(const Cst& c, const Prim<T>& W) {
+__host__ __device__ __forceinline__ Flux<T> ideal_flux(const Cst& c, const Prim<T>& W) {
     T rho = W.r, u = W.u, v = W.v, w = W.w, P = W.P, Bx = W.bx, By = W.by, Bz = W.bz;
     T B2 = Bx * Bx + By * By + Bz * Bz;
     T pt = P + T(0.5) * B2;
@@ -100,7 +100,7 @@ __device__ __forceinline__ Flux<T> ideal_flux(const Cst& c, const Prim<T>& W) {
 // degenerate guards at 1e-14, HLL fallback for |Bn| < 1e-12, double-star
 // fluxes jumped from the outer state with the outer speed.
 template <class T, class Cst>
-__device__ __forceinline__ Flux<T> hlld_x(const Cst& c, Prim<T> L, Prim<T> R, T Bn) {
+__host__ __device__ __forceinline__ Flux<T> hlld_x(const Cst& c, Prim<T> L, Prim<T> R, T Bn) {
     L.bx = Bn; R.bx = Bn;
     const T cfL = fast_speed(c, L, Bn), cfR = fast_speed(c, R, Bn);
     const T SL = vmin(L.u - cfL, R.u - cfR);
@@ -199,7 +199,7 @@ __device__ __forceinline__ Flux<T> hlld_x(const Cst& c, Prim<T> L, Prim<T> R, T 
 // y-normal HLLD through the (u,v)/(Bx,By) swap (M2:540-561).  Returns
 // f1 = flux of mx, f2 = flux of my, f5 = flux of Bx (= Ez at the y face), f6 = flux of Bz.
 template <class T, class Cst>
-__device__ __forceinline__ Flux<T> hlld_y(const Cst& c, const Prim<T>& L, const Prim<T>& R, T Bn) {
+__host__ __device__ __forceinline__ Flux<T> hlld_y(const Cst& c, const Prim<T>& L, const Prim<T>& R, T Bn) {
     Prim<T> aL, aR;
     aL.r = L.r; aL.u = L.v; aL.v = L.u; aL.w = L.w; aL.P = L.P; aL.bx = Bn; aL.by = L.bx; aL.bz = L.bz;
     aR.r = R.r; aR.u = R.v; aR.v = R.u; aR.w = R.w; aR.P = R.P; aR.bx = Bn; aR.by = R.bx; aR.bz = R.bz;
@@ -211,7 +211,7 @@ __device__ __forceinline__ Flux<T> hlld_y(const Cst& c, const Prim<T>& L, const 
 // z-normal HLLD through the cyclic (w,u,v)/(Bz,Bx,By) map (M3:604-622).
 // Returns f1 = F(mx), f2 = F(my), f3 = F(mz), f5 = F(Bx), f6 = F(By).
 template <class T, class Cst>
-__device__ __forceinline__ Flux<T> hlld_z(const Cst& c, const Prim<T>& L, const Prim<T>& R, T Bn) {
+__host__ __device__ __forceinline__ Flux<T> hlld_z(const Cst& c, const Prim<T>& L, const Prim<T>& R, T Bn) {
     Prim<T> aL, aR;
     aL.r = L.r; aL.u = L.w; aL.v = L.u; aL.w = L.v; aL.P = L.P; aL.bx = Bn; aL.by = L.bx; aL.bz = L.by;
     aR.r = R.r; aR.u = R.w; aR.v = R.u; aR.w = R.v; aR.P = R.P; aR.bx = Bn; aR.by = R.bx; aR.bz = R.by;
@@ -222,11 +222,11 @@ __device__ __forceinline__ Flux<T> hlld_z(const Cst& c, const Prim<T>& L, const 
 }
 
 // MC-limited slope (M2:106-112, 295)
-template <class T> __device__ __forceinline__ T minmod(T a, T b) {
+template <class T> __host__ __device__ __forceinline__ T minmod(T a, T b) {
     if (a * b <= T(0.0)) return T(0.0);
     return (fabs(a) < fabs(b)) ? a : b;
 }
-template <class T> __device__ __forceinline__ T mc_slope(T wm, T wc, T wp) {
+template <class T> __host__ __device__ __forceinline__ T mc_slope(T wm, T wc, T wp) {
     const T dm = wc - wm, dp = wp - wc;
     return minmod(T(0.5) * (dm + dp), minmod(T(2.0) * dm, T(2.0) * dp));
 }
