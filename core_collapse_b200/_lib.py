@@ -1,5 +1,5 @@
 """ctypes binding of libcc_b200.so (the C ABI declared in include/cc_step.h,
-include/cc_ic.h and include/cc_batch.h).  Loading fails loudly: there is no CPU fallback."""
+include/cc_ic.h, include/cc_batch.h and include/cc_adjoint.h).  Loading fails loudly: there is no CPU fallback."""
 from __future__ import annotations
 
 import ctypes as C
@@ -161,6 +161,12 @@ SIGNATURES = {
     "cc_batch_autotune": (C.c_int, [_H, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_double)]),
     "cc_batch_set_shape": (C.c_int, [_H, C.c_int]),
     "cc_batch_get_info": (C.c_int, [_H, C.POINTER(CcBatchInfo)]),
+    "cc_adjoint_create": (C.c_int, [C.POINTER(CcMhd2dParams), C.c_int, C.c_int, C.POINTER(_H)]),
+    "cc_adjoint_upload": (C.c_int, [_H, C.POINTER(_DP)]),
+    "cc_adjoint_forward": (C.c_int, [_H, C.c_int, C.c_double, C.c_int, _DP]),
+    "cc_adjoint_download": (C.c_int, [_H, C.POINTER(_DP)]),
+    "cc_adjoint_get_dts": (C.c_int, [_H, _DP, C.c_int]),
+    "cc_adjoint_vjp": (C.c_int, [_H, C.POINTER(_DP), C.POINTER(_DP), _DP]),
 }
 
 _lib = None

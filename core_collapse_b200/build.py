@@ -9,6 +9,8 @@ Translation units and their floating-point contract:
                                      the reference's x86-64 build (no FMA)
   dpoisson.cu                        -fmad=false, explicit fma() only: the batched
                                      direct Poisson solve, reproducible on the CPU
+  capi_adjoint.cu                    -fmad=false: the adjoint kernels recompute FP64
+                                     forward intermediates and must round like them
   mhd2d_f32.cu, mhd3d_f32.cu,
   euler2d_f32.cu, batch_f32.cu       FMA contraction on, approximate FP32 division
                                      and square root, flush-to-zero (the FP32 bulk path)
@@ -41,6 +43,7 @@ UNITS = [
     ("batch_f64.cu", ["-fmad=false"]),
     ("batch_common.cu", ["-fmad=false"]),
     ("dpoisson.cu", ["-fmad=false"]),
+    ("capi_adjoint.cu", ["-fmad=false"]),
     # FP32 bulk path: approximate division/sqrt (<= 2 ulp), denormals flushed
     ("mhd2d_f32.cu", ["-prec-div=false", "-prec-sqrt=false", "-ftz=true"]),
     ("mhd3d_f32.cu", ["-prec-div=false", "-prec-sqrt=false", "-ftz=true"]),

@@ -29,7 +29,26 @@ namespace {
 template <class T, int K> struct ShapeOps {
     using S = typename BatchShapes<T>::template S<K>;
     static constexpr size_t smem() { return StageGeomT<T, S::TX, S::TY>::smem; }
-    template <bool D, int G> static auto kern() { return m2b_stage_kernel<T, S::TX, S::TY, S::MINB, D, G>; }
+    template <bool D, int G, bool R = false> static auto kern() {
+        return m2b_stage_kernel<T, S::TX, S::TY, S::MINB, D, G, R>;
+    }
+    static cudaError_t prepare_rec() {
+        cudaError_t e;
+        const int b = (int)smem();
+        if ((e = cudaFuncSetAttribute(kern<false, GRAV_NONE, true>(), cudaFuncAttributeMaxDynamicSharedMemorySize, b))) return e;
+        if ((e = cudaFuncSetAttribute(kern<false, GRAV_PHI, true>(), cudaFuncAttributeMaxDynamicSharedMemorySize, b))) return e;
+        if ((e = cudaFuncSetAttribute(kern<true, GRAV_NONE, true>(), cudaFuncAttributeMaxDynamicSharedMemorySize, b))) return e;
+        return cudaFuncSetAttribute(kern<true, GRAV_PHI, true>(), cudaFuncAttributeMaxDynamicSharedMemorySize, b);
+    }
+    static cudaError_t stage_rec(int grid, const BatchInst<T>* inst, const int2* work, int nwork, int src, int dst,
+                                 bool defer, bool grav, const double* dt, const int* active, cudaStream_t s) {
+        const dim3 b(S::TX * S::TY);
+        if (defer && grav) kern<true, GRAV_PHI, true>()<<<grid, b, smem(), s>>>(inst, work, nwork, src, dst, dt, active);
+        else if (defer) kern<true, GRAV_NONE, true>()<<<grid, b, smem(), s>>>(inst, work, nwork, src, dst, dt, active);
+        else if (grav) kern<false, GRAV_PHI, true>()<<<grid, b, smem(), s>>>(inst, work, nwork, src, dst, dt, active);
+        else kern<false, GRAV_NONE, true>()<<<grid, b, smem(), s>>>(inst, work, nwork, src, dst, dt, active);
+        return cudaGetLastError();
+    }
     static cudaError_t prepare() {
         cudaError_t e;
         const int b = (int)smem();
@@ -91,6 +110,18 @@ inline int rgrid(int nrwork) {
 }
 
 }  // namespace
+
+template <class T>
+cudaError_t BatchLaunch<T>::stage_rec(const BatchInst<T>* inst, const int2* work, int nwork, int src, int dst,
+                                      bool defer, bool grav, const double* dt, const int* active, cudaStream_t s) {
+    static bool prepared = false;
+    if (!prepared) {
+        cudaError_t e = ShapeOps<T, 0>::prepare_rec();
+        if (e != cudaSuccess) return e;
+        prepared = true;
+    }
+    return ShapeOps<T, 0>::stage_rec(nwork < 1 ? 1 : nwork, inst, work, nwork, src, dst, defer, grav, dt, active, s);
+}
 
 template <class T> int BatchLaunch<T>::n_shapes() { return BatchShapes<T>::N; }
 template <class T> TileShape BatchLaunch<T>::shape(int k) { return ShapeLoop<T>::shape(k); }

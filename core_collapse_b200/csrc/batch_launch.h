@@ -23,6 +23,9 @@ template <class T> struct BatchLaunch {
     static cudaError_t resident(int k, int* per_sm);
     static cudaError_t stage(int k, int grid, const BatchInst<T>* inst, const int2* work, int nwork, int src, int dst,
                              bool defer, bool grav, const double* dt, const int* active, cudaStream_t s);
+    // stage with the record of the pre-floor update (inst->rec), tile candidate 0, one CTA per tile
+    static cudaError_t stage_rec(const BatchInst<T>* inst, const int2* work, int nwork, int src, int dst, bool defer,
+                                 bool grav, const double* dt, const int* active, cudaStream_t s);
     static cudaError_t average(const BatchInst<T>* inst, const int2* rwork, int nrwork, int a, int d, int b,
                                const double* dt, const int* active, double* spd_part, double* rho_part,
                                cudaStream_t s);

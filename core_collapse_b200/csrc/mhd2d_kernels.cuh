@@ -84,10 +84,13 @@ __device__ __forceinline__ void joule_cell(const M2Const<T>& c, const Fields<T>&
 // bytes of shared memory.  Called by the single-grid kernel (one tile per
 // CTA) and by the batched persistent kernel (a run of tiles per CTA).
 // ---------------------------------------------------------------------------
-template <class T, int TX_, int TY_, bool DEFER, int GMODE>
+// REC: also store the updated cell state before its floors (rho, mx, my, mz,
+// E, Bz into rec[0..5], pitched like the state): the record the discrete
+// adjoint replays the floor and gravity-kick branches from.
+template <class T, int TX_, int TY_, bool DEFER, int GMODE, bool REC = false>
 __device__ __forceinline__ void m2_stage_tile(const M2Const<T>& c, const Fields<T>& in, const Fields<T>& out,
                                               const T* __restrict__ ga, const T* __restrict__ gb, const T dt,
-                                              const int i0, const int j0, T* sm) {
+                                              const int i0, const int j0, T* sm, T* const* rec = nullptr) {
     using G = StageGeomT<T, TX_, TY_>;
     constexpr int TX = G::TX, TY = G::TY, HALO = G::HALO, RX = G::RX, RR = G::RR, NT = G::NT;
     constexpr int NFX = G::NFX, NGY = G::NGY, NSL = G::NSL;
@@ -238,6 +241,9 @@ __device__ __forceinline__ void m2_stage_tile(const M2Const<T>& c, const Fields<
         mz += dt * d[3];
         E += dt * d[4];
         Bz += dt * d[6];
+        if (REC) {
+            rec[0][q] = rho; rec[1][q] = mx; rec[2][q] = my; rec[3][q] = mz; rec[4][q] = E; rec[5][q] = Bz;
+        }
         const int kc = ridx(tx, ty);
         floors(c, rho, mx, my, mz, E, s_bx[kc], s_by[kc], Bz);
     }

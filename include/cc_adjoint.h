@@ -1,0 +1,52 @@
+/*
+ * cc_adjoint.h -- discrete adjoint (vector-Jacobian product) of n steps of the
+ * 2D resistive-MHD step (mhd2d_resistive_hlld_ct_gravity.cpp, rk2_step
+ * M2:838-869 with compute_dt M2:579-598), FP64, one grid.
+ *
+ * No reference counterpart: the reference has no derivatives.  The forward
+ * map is the step of cc_batch.h / cc_step.h: RK2 stages of MUSCL-MC + HLLD +
+ * CT + resistive EMF + gravity kick + Joule/Bz diffusion, floors, RK
+ * average; with gravity on, the Poisson solve is the direct solve
+ * (CC_POISSON_DIRECT).  Each step's dt is computed by the CFL rule in the
+ * recorded forward run and then treated as a constant (replayed in the
+ * recomputation and in any finite-difference check); the derivative of a
+ * floor, limiter or Riemann-solver branch is that of the branch taken.
+ *
+ * Use: cc_adjoint_upload(U0) ; cc_adjoint_forward(n, t0, 0, &t) records dt and
+ * keeps a checkpoint every `checkpoint_every` steps ; cc_adjoint_download
+ * gives U_n ; cc_adjoint_vjp(lambda_n) returns lambda_0 = (dU_n/dU_0)^T
+ * lambda_n and d(lambda_n . U_n)/d eta.  cc_adjoint_forward(n, t0, 1, ...)
+ * reruns the forward with the recorded dt (for finite differences).
+ * State and adjoint arrays: f = {rho, mx, my, mz, E, Bz, Bx_f, By_f} in the
+ * reference layouts (cc_step.h).
+ */
+#ifndef CC_ADJOINT_H
+#define CC_ADJOINT_H
+
+#include "cc_step.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* p: FP64; gravity_on requires poisson_kind == CC_POISSON_DIRECT.  Device
+ * memory: about 40 planes of (Nx+1)*(Ny+1) doubles per step of a checkpoint
+ * block, plus 8 planes per checkpoint of max_steps. */
+int cc_adjoint_create(const cc_mhd2d_params* p, int checkpoint_every, int max_steps, cc_handle** out);
+int cc_adjoint_upload(cc_handle* h, const double* const* f);
+/* replay = 0: dt from the CFL rule, recorded; 1: the recorded dt of a previous run. */
+int cc_adjoint_forward(cc_handle* h, int nsteps, double t0, int replay, double* t_out);
+/* state after the last forward run */
+int cc_adjoint_download(cc_handle* h, double* const* f);
+/* the first n recorded dt values */
+int cc_adjoint_get_dts(cc_handle* h, double* dts, int n);
+/* lam_final: adjoint of the final state (8 arrays); lam_initial (8 arrays, may
+ * be NULL) and lam_eta (may be NULL) receive the adjoints of the initial state
+ * and of eta, for the steps of the last recorded forward run. */
+int cc_adjoint_vjp(cc_handle* h, const double* const* lam_final, double* const* lam_initial, double* lam_eta);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* CC_ADJOINT_H */
