@@ -166,6 +166,7 @@ SIGNATURES = {
     "cc_adjoint_forward": (C.c_int, [_H, C.c_int, C.c_double, C.c_int, _DP]),
     "cc_adjoint_download": (C.c_int, [_H, C.POINTER(_DP)]),
     "cc_adjoint_get_dts": (C.c_int, [_H, _DP, C.c_int]),
+    "cc_adjoint_set_dts": (C.c_int, [_H, _DP, C.c_int]),
     "cc_adjoint_vjp": (C.c_int, [_H, C.POINTER(_DP), C.POINTER(_DP), _DP]),
 }
 

@@ -192,8 +192,7 @@ struct Adjoint : Batch<double> {
 
     int upload0(const double* const* f) {
         if (int r = xfer(St[0], f, nullptr)) return r;
-        loaded0 = true;
-        nrec = 0;
+        loaded0 = true;   // the recorded dt sequence is kept: a replayed run may follow
         return CC_OK;
     }
 
@@ -270,6 +269,17 @@ struct Adjoint : Batch<double> {
         CC_CUDA(cudaMemcpyAsync(&t, tclk, sizeof(double), cudaMemcpyDeviceToHost, st()));
         CC_CUDA(cudaStreamSynchronize(st()));
         if (tout) *tout = t;
+        return CC_OK;
+    }
+
+    int set_dts(const double* v, int n) {
+        if (n < 1 || n > max_steps) return fail(h, CC_ERR_ARG, "n outside [1, max_steps]");
+        for (int i = 0; i < n; i++)
+            if (!(v[i] >= 0.0) || !std::isfinite(v[i])) return fail(h, CC_ERR_NONFINITE, "dt not finite or negative");
+        dts.assign(v, v + n);
+        CC_CUDA(cudaMemcpyAsync(dtrec, dts.data(), sizeof(double) * n, cudaMemcpyHostToDevice, st()));
+        CC_CUDA(cudaStreamSynchronize(st()));
+        nrec = n;
         return CC_OK;
     }
 
@@ -453,6 +463,13 @@ int cc_adjoint_get_dts(cc_handle* h, double* dts, int n) {
     if (n > a->nrec) return fail(h, CC_ERR_ARG, "fewer recorded steps than requested");
     for (int i = 0; i < n; i++) dts[i] = a->dts[i];
     return CC_OK;
+}
+
+int cc_adjoint_set_dts(cc_handle* h, const double* dts, int n) {
+    Adjoint* a = aj(h);
+    if (!a || !dts) return CC_ERR_ARG;
+    if (int r = set_dev(h)) return r;
+    return a->set_dts(dts, n);
 }
 
 int cc_adjoint_vjp(cc_handle* h, const double* const* lam_final, double* const* lam_initial, double* lam_eta) {

@@ -40,9 +40,13 @@ int cc_adjoint_forward(cc_handle* h, int nsteps, double t0, int replay, double* 
 int cc_adjoint_download(cc_handle* h, double* const* f);
 /* the first n recorded dt values */
 int cc_adjoint_get_dts(cc_handle* h, double* dts, int n);
+/* make dts[0..n) the recorded sequence (a replayed forward run and the next
+ * vjp use it), e.g. to rerun another handle's run with a perturbed parameter */
+int cc_adjoint_set_dts(cc_handle* h, const double* dts, int n);
 /* lam_final: adjoint of the final state (8 arrays); lam_initial (8 arrays, may
  * be NULL) and lam_eta (may be NULL) receive the adjoints of the initial state
- * and of eta, for the steps of the last recorded forward run. */
+ * and of eta along the trajectory of the last forward run (recorded or
+ * replayed), with the recorded dt sequence. */
 int cc_adjoint_vjp(cc_handle* h, const double* const* lam_final, double* const* lam_initial, double* lam_eta);
 
 #ifdef __cplusplus
