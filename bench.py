@@ -351,6 +351,8 @@ def run_ours(args) -> None:
         line["mhd3d"] = run_3d(args, stream)
     if not args.skip_ensemble:
         line["ensemble"] = run_ensemble(args, stream, rank, world, barrier, max_over_ranks, value32 / world)
+    if world == 1 and not args.skip_adjoint:
+        line["adjoint"] = run_adjoint(args, stream)
     if world == 1 and rank == 0 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(args.cpu_sample_grid, args.cpu_steps)
     if rank == 0:
@@ -453,6 +455,72 @@ def run_ensemble(args, stream, rank: int, world: int, barrier, max_over_ranks, s
     return out
 
 
+def run_adjoint(args, stream) -> dict:
+    """Discrete adjoint of the 2D step: 512^2 collapse on [-1,1]^2 with
+    outflow boundaries (gamma 5/3, G 1, eta 1e-3, CFL 0.4, direct Poisson),
+    core amplitude 9, width 0.1, 1% density noise (seed 0), Bx 0.05; 100
+    steps, a checkpoint every 10.  Loss 0.5 sum (rho_T - rho_target)^2, the
+    target from the same run with core amplitude 12 (seed 3).  FP64.
+    Reported: recorded-forward and VJP times (CUDA events on the handle's
+    stream), their ratio, and central finite differences (h 1e-6, recorded
+    dt replayed) of the loss along --adjoint-fd random cell directions."""
+    import numpy as np
+    import torch
+
+    from core_collapse_b200.adjoint import AdjointSolver, density_loss_adjoint
+    from core_collapse_b200.mhd2d import Params, ic_collapse
+    n, nsteps, k = args.adjoint_grid, args.adjoint_steps, 10
+    p = Params(Nx=n, Ny=n, x0=-1.0, x1=1.0, y0=-1.0, y1=1.0, periodic_x=False, periodic_y=False, gamma=5.0 / 3.0,
+               G=1.0, eta=1e-3, cfl=0.4, gravity_on=True, poisson="direct", precision="fp64", t_end=1e30)
+    U, B = ic_collapse(p, core_amp=9.0, core_width=0.1, noise=0.01, seed=0, Bx0=0.05)
+    Ut, Bt = ic_collapse(p, core_amp=12.0, core_width=0.1, noise=0.01, seed=3, Bx0=0.05)
+    out = {"workload": f"{n}^2 collapse, outflow [-1,1]^2, gamma 5/3, G 1, eta 1e-3, CFL 0.4, direct Poisson, "
+                       f"{nsteps} steps, checkpoint every {k}; loss 0.5 |rho_T - rho_target|^2 (target: core 12, seed 3)",
+           "dtype": "f64"}
+    with AdjointSolver(p, k, nsteps) as s:
+        s.set_stream(stream.cuda_stream)
+        s.upload(Ut, Bt)
+        s.forward(nsteps)
+        target = s.download()[0].rho.copy()
+        s.upload(U, B)
+        s.forward(nsteps)                       # warm-up (and the recorded dt)
+        e0, e1, e2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+        torch.cuda.synchronize()
+        e0.record(stream)
+        s.forward(nsteps)
+        e1.record(stream)
+        UT, _ = s.download()
+        loss, lamU, lamB = density_loss_adjoint(p, UT.rho, target)
+        torch.cuda.synchronize()
+        e1.synchronize()
+        e2.record(stream)
+        g, _, geta = s.vjp(lamU, lamB)
+        e3 = torch.cuda.Event(enable_timing=True)
+        e3.record(stream)
+        torch.cuda.synchronize()
+        fwd_ms, adj_ms = e0.elapsed_time(e1), e2.elapsed_time(e3)
+        rng = np.random.default_rng(3)
+        cells = rng.choice(n * n, size=args.adjoint_fd, replace=False)
+        worst = 0.0
+        gscale = float(np.max(np.abs(g.rho)))
+        for c in cells:
+            vals = []
+            for sgn in (1.0, -1.0):
+                V = U.copy()
+                V.rho[c] += sgn * 1e-6
+                s.upload(V, B)
+                s.forward(nsteps, replay=True)
+                vals.append(density_loss_adjoint(p, s.download()[0].rho, target)[0])
+            fd = (vals[0] - vals[1]) / 2e-6
+            worst = max(worst, abs(g.rho[c] - fd) / gscale)
+    out.update({"forward_ms": fwd_ms, "adjoint_ms": adj_ms, "adjoint_over_forward": adj_ms / fwd_ms,
+                "zone_updates_per_s_forward": n * n * nsteps / (fwd_ms / 1000.0),
+                "loss": loss, "dloss_deta": geta,
+                "fd_check": {"cells": int(args.adjoint_fd), "h": 1e-6,
+                             "max_abs_err_over_max_grad": worst}})
+    return out
+
+
 def run_ensemble_only(args) -> None:
     import torch
     torch.cuda.set_device(0)
@@ -477,6 +545,11 @@ def main():
     ap.add_argument("--skip-ensemble", action="store_true")
     ap.add_argument("--ensemble", type=int, default=512)
     ap.add_argument("--ensemble-steps", type=int, default=60)
+    ap.add_argument("--skip-adjoint", action="store_true")
+    ap.add_argument("--adjoint-grid", type=int, default=512)
+    ap.add_argument("--adjoint-steps", type=int, default=100)
+    ap.add_argument("--adjoint-fd", type=int, default=4)
+    ap.add_argument("--adjoint-only", action="store_true", help="time only the adjoint block (a profiling aid)")
     ap.add_argument("--ensemble-only", action="store_true",
                     help="time only the batched ensemble (a profiling aid; prints the ensemble block)")
     args = ap.parse_args()
@@ -484,6 +557,11 @@ def main():
         ap.error("--warmup must be >= 3")
     if args.ensemble_only:
         run_ensemble_only(args)
+        return
+    if args.adjoint_only:
+        import torch
+        torch.cuda.set_device(0)
+        print(json.dumps(run_adjoint(args, torch.cuda.Stream())), flush=True)
         return
     if args.impl == "reference":
         run_reference(args)

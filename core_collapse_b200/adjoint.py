@@ -68,6 +68,14 @@ class AdjointSolver:
     def __exit__(self, *exc):
         self.close()
 
+    def set_stream(self, stream: int):
+        self._check(self._lib.cc_set_stream(self._h, C.c_void_p(stream)))
+
+    def perf(self) -> dict:
+        pf = L.CcPerf()
+        self._check(self._lib.cc_get_perf(self._h, C.byref(pf)))
+        return {f: getattr(pf, f) for f, _ in L.CcPerf._fields_}
+
     def upload(self, U: Ucc, B: Bfaces):
         self._check(self._lib.cc_adjoint_upload(self._h, _ptrs(U, B)))
 
