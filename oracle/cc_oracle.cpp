@@ -187,6 +187,25 @@ void rk2(const cc_mhd2d_params* c, M2State<T>& s, const std::vector<double>& gx,
     m.rk2_step(s, cast<T>(gx), cast<T>(gy), T(dt), poisson);
 }
 
+// Gravity of a dual density field: the value by the chosen solve, the
+// tangent by the same (linear) direct solve applied to the density tangent
+// (direct mode or gravity off only).
+void gravity_dual(const cc_mhd2d_params* c, const std::vector<Dual>& rho, std::vector<Dual>& gx,
+                  std::vector<Dual>& gy, int mode) {
+    const size_t N = rho.size();
+    std::vector<double> rv(N), rd(N), x, y, xd(N, 0.0), yd(N, 0.0);
+    for (size_t q = 0; q < N; q++) { rv[q] = rho[q].v; rd[q] = rho[q].d; }
+    gravity(c, rv, x, y, mode);
+    if (c->gravity_on) {
+        PoissonSpec sp = m2spec(c);
+        std::vector<double> phi;
+        direct_solve(sp, direct_rhs(sp, rd), phi);
+        gravity_from_phi(sp, phi, xd, yd);
+    }
+    gx.resize(N); gy.resize(N);
+    for (size_t q = 0; q < N; q++) { gx[q] = Dual(x[q], xd[q]); gy[q] = Dual(y[q], yd[q]); }
+}
+
 template <class T> int main_loop(const cc_mhd2d_params* c, double* const* f, int nsteps, double* t, int mode) {
     M2State<T> s;
     load(c, f, s);
@@ -270,6 +289,33 @@ int or_mhd2d_rk2_step(const cc_mhd2d_params* c, double* const* f, const double* 
 }
 
 // nsteps of the main() loop body (M2:1111-1117) in double (fp32 == 0) or float.
+// Tangent-linear model of nsteps of the main-loop body with the dt sequence
+// dts (dt held constant): f = values (updated in place, bitwise the double
+// run), fd = tangents (updated to J fd).  Gravity: direct solve (mode 3) or off.
+int or_mhd2d_tlm(const cc_mhd2d_params* c, double* const* f, double* const* fd, int nsteps, const double* dts) {
+    if (c->gravity_on && c->poisson_kind != 2) return -1;
+    M2State<Dual> s;
+    const size_t N = (size_t)c->Nx * c->Ny, NX = (size_t)(c->Nx + 1) * c->Ny, NY = (size_t)c->Nx * (c->Ny + 1);
+    std::vector<Dual>* v[8] = {&s.rho, &s.mx, &s.my, &s.mz, &s.E, &s.Bz, &s.bxf, &s.byf};
+    const size_t sz[8] = {N, N, N, N, N, N, NX, NY};
+    for (int k = 0; k < 8; k++) {
+        v[k]->resize(sz[k]);
+        for (size_t q = 0; q < sz[k]; q++) (*v[k])[q] = Dual(f[k][q], fd[k][q]);
+    }
+    M2<Dual> m(m2par(c));
+    auto poisson = [&](const std::vector<Dual>& rho, std::vector<Dual>& ox, std::vector<Dual>& oy) {
+        gravity_dual(c, rho, ox, oy, 3);
+    };
+    for (int n = 0; n < nsteps; ++n) {
+        std::vector<Dual> gx, gy;
+        gravity_dual(c, s.rho, gx, gy, 3);
+        m.rk2_step(s, gx, gy, Dual(dts[n]), poisson);
+    }
+    for (int k = 0; k < 8; k++)
+        for (size_t q = 0; q < sz[k]; q++) { f[k][q] = (*v[k])[q].v; fd[k][q] = (*v[k])[q].d; }
+    return 0;
+}
+
 int or_mhd2d_main_loop(const cc_mhd2d_params* c, double* const* f, int nsteps, double* t, int mode, int fp32) {
     return fp32 ? main_loop<float>(c, f, nsteps, t, mode) : main_loop<double>(c, f, nsteps, t, mode);
 }

@@ -98,8 +98,8 @@ public:
         T vn2 = bn2 / rho;
         T disc = (a2 + vA2) * (a2 + vA2) - T(4.0) * a2 * vn2;
         disc = vmax(T(0.0), disc);
-        T cf2 = T(0.5) * ((a2 + vA2) + std::sqrt(disc));
-        return std::sqrt(vmax(T(0.0), cf2));
+        T cf2 = T(0.5) * ((a2 + vA2) + osqrt(disc));
+        return osqrt(vmax(T(0.0), cf2));
     }
 
     // x-normal ideal flux (M2:351-370) and HLLD (M2:372-530)

@@ -23,6 +23,45 @@ namespace cco {
 template <class T> inline T vmax(T a, T b) { return (a < b) ? b : a; }
 template <class T> inline T vmin(T a, T b) { return (b < a) ? b : a; }
 
+// |a| and sqrt(a) found by argument-dependent lookup: std:: for double and
+// float (unchanged results), the Dual overloads below for the tangent build.
+template <class T> inline T oabs(T a) { using std::abs; return abs(a); }
+template <class T> inline T osqrt(T a) { using std::sqrt; return sqrt(a); }
+
+// Forward-mode dual number for the tangent-linear build of the restatement:
+// v carries exactly the double operations of the value computation (so the
+// value trajectory is bitwise the T = double one), d the directional
+// derivative along the branch the value took.
+struct Dual {
+    double v, d;
+    Dual(double x = 0.0) : v(x), d(0.0) {}
+    Dual(double x, double dx) : v(x), d(dx) {}
+};
+inline Dual operator+(Dual a, Dual b) { return Dual(a.v + b.v, a.d + b.d); }
+inline Dual operator-(Dual a, Dual b) { return Dual(a.v - b.v, a.d - b.d); }
+inline Dual operator*(Dual a, Dual b) { return Dual(a.v * b.v, a.d * b.v + a.v * b.d); }
+inline Dual operator/(Dual a, Dual b) {
+    const double q = a.v / b.v;
+    return Dual(q, (a.d - q * b.d) / b.v);
+}
+inline Dual operator-(Dual a) { return Dual(-a.v, -a.d); }
+inline Dual operator+(Dual a) { return a; }
+inline Dual& operator+=(Dual& a, Dual b) { return a = a + b; }
+inline Dual& operator-=(Dual& a, Dual b) { return a = a - b; }
+inline Dual& operator*=(Dual& a, Dual b) { return a = a * b; }
+inline Dual& operator/=(Dual& a, Dual b) { return a = a / b; }
+inline bool operator<(Dual a, Dual b) { return a.v < b.v; }
+inline bool operator<=(Dual a, Dual b) { return a.v <= b.v; }
+inline bool operator>(Dual a, Dual b) { return a.v > b.v; }
+inline bool operator>=(Dual a, Dual b) { return a.v >= b.v; }
+inline bool operator==(Dual a, Dual b) { return a.v == b.v; }
+inline bool operator!=(Dual a, Dual b) { return a.v != b.v; }
+inline Dual abs(Dual a) { return a.v < 0.0 ? -a : a; }
+inline Dual sqrt(Dual a) {
+    const double r = std::sqrt(a.v);
+    return Dual(r, r > 0.0 ? a.d / (2.0 * r) : 0.0);
+}
+
 inline int wrap_idx(int i, int n) { int r = i % n; return (r < 0) ? r + n : r; }
 inline int clamp_idx(int i, int lo, int hi) { return i < lo ? lo : (i > hi ? hi : i); }
 
@@ -39,7 +78,7 @@ struct Axis {
 // minmod / MC limiter (M2:106-112, M3:106-112, EH:85-92).
 template <class T> inline T minmod(T a, T b) {
     if (a * b <= T(0)) return T(0);
-    return (std::abs(a) < std::abs(b)) ? a : b;
+    return (oabs(a) < oabs(b)) ? a : b;
 }
 template <class T> inline T mc_slope(T dm, T dp) {
     return minmod(T(0.5) * (dm + dp), minmod(T(2.0) * dm, T(2.0) * dp));
@@ -89,7 +128,7 @@ template <class T, class Phys> Flux7<T> hlld_x_generic(const Phys& ph, Prim8<T> 
 
     T den = L.r * (SL - L.u) - R.r * (SR - R.u);
     T SM = T(0.0);
-    if (std::abs(den) > T(1e-14)) SM = (ptR - ptL + L.r * L.u * (SL - L.u) - R.r * R.u * (SR - R.u)) / den;
+    if (oabs(den) > T(1e-14)) SM = (ptR - ptL + L.r * L.u * (SL - L.u) - R.r * R.u * (SR - R.u)) / den;
 
     T rLs = L.r * (SL - L.u) / (SL - SM);
     T rRs = R.r * (SR - R.u) / (SR - SM);
@@ -100,24 +139,24 @@ template <class T, class Phys> Flux7<T> hlld_x_generic(const Phys& ph, Prim8<T> 
 
     T ByLs = L.by, BzLs = L.bz, ByRs = R.by, BzRs = R.bz;
     T vLs = L.v, wLs = L.w, vRs = R.v, wRs = R.w;
-    if (std::abs(dL) > T(1e-14)) {
+    if (oabs(dL) > T(1e-14)) {
         ByLs = L.by * (L.r * sL * (SL - L.u) - Bn * Bn) / dL;
         BzLs = L.bz * (L.r * sL * (SL - L.u) - Bn * Bn) / dL;
         vLs = L.v - Bn * (ByLs - L.by) / (L.r * (SL - L.u) * (SL - SM));
         wLs = L.w - Bn * (BzLs - L.bz) / (L.r * (SL - L.u) * (SL - SM));
     }
-    if (std::abs(dR) > T(1e-14)) {
+    if (oabs(dR) > T(1e-14)) {
         ByRs = R.by * (R.r * sR * (SR - R.u) - Bn * Bn) / dR;
         BzRs = R.bz * (R.r * sR * (SR - R.u) - Bn * Bn) / dR;
         vRs = R.v - Bn * (ByRs - R.by) / (R.r * (SR - R.u) * (SR - SM));
         wRs = R.w - Bn * (BzRs - R.bz) / (R.r * (SR - R.u) * (SR - SM));
     }
-    T sqL = std::sqrt(vmax(rLs, T(1e-300)));
-    T sqR = std::sqrt(vmax(rRs, T(1e-300)));
-    T SLL = SM - std::abs(Bn) / sqL;
-    T SRR = SM + std::abs(Bn) / sqR;
+    T sqL = osqrt(vmax(rLs, T(1e-300)));
+    T sqR = osqrt(vmax(rRs, T(1e-300)));
+    T SLL = SM - oabs(Bn) / sqL;
+    T SRR = SM + oabs(Bn) / sqR;
 
-    if (std::abs(Bn) < T(1e-12)) {  // HLL fallback (M2:449-467)
+    if (oabs(Bn) < T(1e-12)) {  // HLL fallback (M2:449-467)
         T inv = T(1.0) / (SR - SL);
         Flux7<T> F;
         for (int k = 0; k < 7; k++) F.f[k] = (SR * FL.f[k] - SL * FR.f[k] + SL * SR * (UR[k] - UL[k])) * inv;

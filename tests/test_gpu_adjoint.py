@@ -8,38 +8,20 @@ the density misfit loss, and the eta gradient through a second handle that
 replays the recorded dt.  Tolerance: 1e-6 relative.  Test states keep every
 face off the HLL branch (Bn != 0) and every MC slope off its zero kink, so a
 finite-difference step measures a derivative, not a branch jump."""
+import ctypes as C
+
 import numpy as np
 import pytest
 
+import oracle_lib as O
+
 from core_collapse_b200.adjoint import AdjointSolver, Mhd2dRollout, RolloutSetup, density_loss_adjoint
-from core_collapse_b200.mhd2d import Params, empty_state, ic_collapse
+from cases_adjoint import make_case_adj as _case
+from core_collapse_b200.mhd2d import empty_state
 
 pytestmark = pytest.mark.gpu
 
 FIELDS = ["rho", "mx", "my", "mz", "E", "Bz", "Bx_f", "By_f"]
-
-
-def _case(periodic: bool, grav: bool, nx=24, ny=20, eta=2e-3, seed=3):
-    p = Params(Nx=nx, Ny=ny, x0=-1.0, x1=1.0, y0=-1.0, y1=1.0, periodic_x=periodic, periodic_y=not periodic,
-               gamma=5.0 / 3.0, G=1.0, eta=eta, cfl=0.4, gravity_on=grav, poisson="direct", t_end=1e30)
-    U, B = ic_collapse(p, core_amp=6.0, core_width=0.3, noise=0.02, seed=seed, Bx0=0.1)
-    rng = np.random.default_rng(seed)
-    n = nx * ny
-    U.mx += U.rho * rng.normal(0.0, 0.3, n)
-    U.my += U.rho * rng.normal(0.0, 0.3, n)
-    U.mz += U.rho * rng.normal(0.0, 0.1, n)
-    U.Bz += rng.normal(0.0, 0.05, n)
-    # In-plane B = uniform (0.1, 0.07) + curl of a random corner potential
-    # Az (div B = 0 to roundoff).  A finite-difference step must not sit on a
-    # branch point of the discrete map: Bn = 0 selects HLL (|Bn| < 1e-12,
-    # M2:449) and a uniform field gives zero MC slopes, the limiter's kink.
-    Az = rng.normal(0.0, 0.004, (ny + 1, nx + 1))
-    B.Bx_f[:] = (0.1 + (Az[1:, :] - Az[:-1, :]) / p.dy).ravel()
-    B.By_f[:] = (0.07 - (Az[:, 1:] - Az[:, :-1]) / p.dx).ravel()
-    Bx = 0.5 * (B.Bx_f.reshape(ny, nx + 1)[:, 1:] + B.Bx_f.reshape(ny, nx + 1)[:, :-1]).ravel()
-    By = 0.5 * (B.By_f.reshape(ny + 1, nx)[1:, :] + B.By_f.reshape(ny + 1, nx)[:-1, :]).ravel()
-    U.E += 0.5 * (U.mx ** 2 + U.my ** 2 + U.mz ** 2) / U.rho + 0.5 * (U.Bz ** 2 + Bx ** 2 + By ** 2) - 0.5 * 0.01
-    return p, U, B
 
 
 def _arrays(U, B):
@@ -149,3 +131,30 @@ def test_autograd_function_matches_the_c_abi():
         g, _, ge = s.vjp(lamU, lamB)
     assert np.allclose(rho0.grad.numpy(), g.rho, rtol=1e-12, atol=1e-14 * np.abs(g.rho).max())
     assert abs(eta.grad.item() - ge) <= 1e-12 * abs(ge)
+
+
+@pytest.mark.parametrize("periodic,grav", [(False, True), (True, True), (True, False)])
+def test_adjoint_is_the_transpose_of_the_dual_number_tangent(periodic, grav):
+    """<lambda_T, J v> from the oracle's dual-number tangent-linear build
+    (same recorded dt) equals <J^T lambda_T, v> from the GPU adjoint, and the
+    GPU forward equals the oracle's value trajectory bit for bit."""
+    p, U, B = _case(periodic, grav)
+    nsteps = 5
+    rng = np.random.default_rng(21)
+    with AdjointSolver(p, checkpoint_every=2, max_steps=nsteps) as s:
+        UT, BT = _run(s, U, B, nsteps, replay=False)
+        dts = s.dts()
+        lamU, lamB = empty_state(p)
+        for a in _arrays(lamU, lamB):
+            a[:] = rng.normal(size=a.size)
+        l0U, l0B, _ = s.vjp(lamU, lamB)
+    V = [rng.normal(size=a.size) * (np.abs(a).mean() + 1e-3) for a in _arrays(U, B)]
+    vals = O.copy_state(_arrays(U, B))
+    tans = O.copy_state(V)
+    cp = p.to_c()
+    assert O.oracle().or_mhd2d_tlm(C.byref(cp), O.pp(vals), O.pp(tans), nsteps, O.dp(dts)) == 0
+    for a, b in zip(vals, _arrays(UT, BT)):
+        assert np.array_equal(a, b)
+    lhs = sum(float(l @ t) for l, t in zip(_arrays(lamU, lamB), tans))
+    rhs = sum(float(l @ v) for l, v in zip(_arrays(l0U, l0B), V))
+    assert abs(lhs - rhs) <= 1e-10 * abs(lhs), f"<lam, Jv> {lhs} vs <J^T lam, v> {rhs}"
