@@ -18,12 +18,14 @@ __global__ void batch_finalize_kernel(const BatchRed* __restrict__ red, int n, c
     const BatchRed r = red[id];
     if (flags & BF_MEAN) {
         double s = 0.0;
+#pragma unroll 16
         for (int k = 0; k < r.count; k++) s += rho_part[r.base + k];
         rho_mean[id] = s / r.ncell;
     }
     if (flags & BF_DT) {
         const DtSpec d = r.dts;
         double maxs = d.seed;
+#pragma unroll 16
         for (int k = 0; k < r.count; k++) maxs = vmax(maxs, spd_part[r.base + k]);
         const double dt_h = d.cfl * d.hmin / maxs;
         double v = dt_h;

@@ -280,7 +280,10 @@ template <class T> struct Batch : BatchBase {
             if (p[i].gravity_on) {
                 for (int tm = 0; tm < (ny + 63) / 64; tm++)
                     for (int tn = 0; tn < (nx + 63) / 64; tn++) gw.push_back(make_int2(i, (tm << 16) | tn));
-                for (int cb = 0; cb < (nx + 31) / 32; cb++) yw.push_back(make_int2(i, cb));
+                // item -1: the singular x wavenumber 0 on its own; items cb >= 0:
+                // wavenumbers 1 + 32 cb + lane
+                yw.push_back(make_int2(i, -1));
+                for (int cb = 0; cb < (nx - 1 + 31) / 32; cb++) yw.push_back(make_int2(i, cb));
             }
         }
         nrwork = (int)rw.size(); ngwork = (int)gw.size(); nywork = (int)yw.size();

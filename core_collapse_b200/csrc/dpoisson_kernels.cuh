@@ -16,7 +16,8 @@
 // same order) reproduces the result bit for bit.
 //
 // Work-lists: GEMM tiles {instance, (tm << 16) | tn} of DPM x DPN outputs;
-// y-solve blocks {instance, column block} of DPC columns, one thread per column.
+// y-solve items {instance, -1} (the singular wavenumber 0) and {instance,
+// column block} of DPC wavenumbers 1 + DPC cb + lane, one thread per column.
 #pragma once
 #include <type_traits>
 
@@ -113,9 +114,84 @@ dp_gemm_kernel(const BatchInst<T>* __restrict__ inst, const int2* __restrict__ g
     }
 }
 
-// One thread per x wavenumber (column of ah), sequential along y, with the
-// factors set up at handle creation: each sweep is a chain of fma's (no
-// division), and the loads of the factors do not depend on the chain.
+// y solves: one thread per x wavenumber k >= 1 (a warp covers 32 adjacent
+// wavenumbers, so every row access is one coalesced 256-byte line), the
+// singular k = 0 on a CTA of its own.  Each sweep is a chain of fma's whose
+// loads do not depend on the chain: rows are fetched YB at a time into
+// registers one block ahead of the block being computed, which overlaps the
+// L2 latency with the chain.  The arithmetic and its order are those of the
+// CPU restatement (bitwise).
+constexpr int YB = 16;
+
+// forward sweep: d_0 = u_0 inv_0, d_j = (u_j - a d_{j-1}) inv_j, u_j <- d_j; returns d_{n-1}
+// (the prefetch of the block after the last one reads clamped, in-range rows)
+__device__ __forceinline__ double ysweep_fwd(double* __restrict__ u, const double* __restrict__ inv, size_t S,
+                                             int n, double a) {
+    double d = u[0] * inv[0];
+    u[0] = d;
+    int j = 1;
+    const int nb = (n - 1) / YB;
+    double cu[YB], ci[YB];
+#pragma unroll
+    for (int t = 0; t < YB; t++) {
+        const int r = min(j + t, n - 1);
+        cu[t] = u[r * S]; ci[t] = inv[r * S];
+    }
+    for (int b = 0; b < nb; b++, j += YB) {
+        double nu[YB], ni[YB];
+#pragma unroll
+        for (int t = 0; t < YB; t++) {
+            const int r = min(j + YB + t, n - 1);
+            nu[t] = u[r * S]; ni[t] = inv[r * S];
+        }
+#pragma unroll
+        for (int t = 0; t < YB; t++) {
+            d = fma(-a, d, cu[t]) * ci[t];
+            u[(j + t) * S] = d;
+        }
+#pragma unroll
+        for (int t = 0; t < YB; t++) { cu[t] = nu[t]; ci[t] = ni[t]; }
+    }
+    for (; j < n; j++) {
+        d = fma(-a, d, u[j * S]) * inv[j * S];
+        u[j * S] = d;
+    }
+    return d;
+}
+
+// backward sweep: x_{n-1} = d_{n-1}, x_j = d_j - cp_j x_{j+1}, u_j <- x_j; returns x_0
+__device__ __forceinline__ double ysweep_bwd(double* __restrict__ u, const double* __restrict__ cp, size_t S,
+                                             int n, double x) {
+    int j = n - 2;
+    const int nb = (n - 1) / YB;
+    double cu[YB], cc[YB];
+#pragma unroll
+    for (int t = 0; t < YB; t++) {
+        const int r = max(j - t, 0);
+        cu[t] = u[r * S]; cc[t] = cp[r * S];
+    }
+    for (int b = 0; b < nb; b++, j -= YB) {
+        double nu[YB], nc[YB];
+#pragma unroll
+        for (int t = 0; t < YB; t++) {
+            const int r = max(j - YB - t, 0);
+            nu[t] = u[r * S]; nc[t] = cp[r * S];
+        }
+#pragma unroll
+        for (int t = 0; t < YB; t++) {
+            x = fma(-cc[t], x, cu[t]);
+            u[(j - t) * S] = x;
+        }
+#pragma unroll
+        for (int t = 0; t < YB; t++) { cu[t] = nu[t]; cc[t] = nc[t]; }
+    }
+    for (; j >= 0; j--) {
+        x = fma(-cp[j * S], x, u[j * S]);
+        u[j * S] = x;
+    }
+    return x;
+}
+
 template <class T>
 __global__ void __launch_bounds__(DPC)
 dp_ysolve_kernel(const BatchInst<T>* __restrict__ inst, const int2* __restrict__ ywork, int nywork,
@@ -125,23 +201,24 @@ dp_ysolve_kernel(const BatchInst<T>* __restrict__ inst, const int2* __restrict__
         if (active[it.x] == 0) continue;
         const BatchInst<T>& I = inst[it.x];
         const int nx = I.c.nx, n = I.c.ny;
-        const int col = it.y * DPC + threadIdx.x;
-        if (col >= nx) continue;
-        double* __restrict__ u = I.ah + col;
         const size_t S = (size_t)nx;
         const bool py = I.c.ay.periodic != 0;
         const double a = I.ay;
-        if (col == 0) {
+        if (it.y < 0) {
             // singular k = 0: flux G_j = a (u_{j+1} - u_j) = G_{j-1} + r_j, then mean removal
+            if (threadIdx.x != 0) continue;
+            double* __restrict__ u = I.ah;
             double g0 = 0.0;
             if (py) {
                 double Sr = 0.0, SS = 0.0;
+#pragma unroll 16
                 for (int j = 0; j < n; j++) { Sr = Sr + u[j * S]; SS = SS + Sr; }
                 g0 = -(SS / (double)n);
             }
             double G = g0, prev = 0.0;
             double r = u[0];
             u[0] = 0.0;
+#pragma unroll 16
             for (int j = 0; j + 1 < n; j++) {
                 G = G + r;
                 r = u[(j + 1) * S];
@@ -149,28 +226,23 @@ dp_ysolve_kernel(const BatchInst<T>* __restrict__ inst, const int2* __restrict__
                 u[(j + 1) * S] = prev;
             }
             double m = 0.0;
+#pragma unroll 16
             for (int j = 0; j < n; j++) m = m + u[j * S];
             m = m / (double)n;
+#pragma unroll 16
             for (int j = 0; j < n; j++) u[j * S] = u[j * S] - m;
             continue;
         }
-        const double* __restrict__ cp = I.ycp + col;
-        const double* __restrict__ inv = I.yinv + col;
-        double d = u[0] * inv[0];
-        u[0] = d;
-        for (int j = 1; j < n; j++) {
-            d = fma(-a, d, u[j * S]) * inv[j * S];
-            u[j * S] = d;
-        }
-        double x = d;
-        for (int j = n - 2; j >= 0; j--) {
-            x = fma(-cp[j * S], x, u[j * S]);
-            u[j * S] = x;
-        }
+        const int col = 1 + it.y * DPC + threadIdx.x;
+        if (col >= nx) continue;
+        double* __restrict__ u = I.ah + col;
+        const double d = ysweep_fwd(u, I.yinv + col, S, n, a);
+        const double x = ysweep_bwd(u, I.ycp + col, S, n, d);
         if (!py) continue;
         const double* __restrict__ z = I.yz + col;
         const double gam = -fma(-2.0, a, I.lamx[col]);
         const double fac = fma(a / gam, d, x) * I.yfden[col];   // d = x_{n-1}, x = x_0
+#pragma unroll 8
         for (int j = 0; j < n; j++) u[j * S] = fma(-fac, z[j * S], u[j * S]);
     }
 }
