@@ -123,7 +123,7 @@ template <class T> struct Batch : BatchBase {
     std::vector<int> nswork;
     std::vector<int> sgrid;          // CTAs per candidate
     int2* rwork = nullptr; int nrwork = 0;
-    int2* gwork = nullptr; int ngwork = 0;
+    int2* gwork = nullptr; int ngwork = 0; int gtile = 64;
     int2* ywork = nullptr; int nywork = 0;
     // per-instance device scalars and partials
     double* spd_part = nullptr;
@@ -270,7 +270,7 @@ template <class T> struct Batch : BatchBase {
             R.dts.clamp_to_end = 1; R.dts.seed = 1e-14; R.dts.end_eps = 0.0; R.dts.check = 0; R.dts.cap = 1;
         }
         // ---- work-lists ----
-        std::vector<int2> rw, gw, yw;
+        std::vector<int2> rw, gw, gw32, yw;
         for (int i = 0; i < n; i++) {
             const int nx = p[i].Nx, ny = p[i].Ny;
             hred[i].base = (int)rw.size();
@@ -280,12 +280,16 @@ template <class T> struct Batch : BatchBase {
             if (p[i].gravity_on) {
                 for (int tm = 0; tm < (ny + 63) / 64; tm++)
                     for (int tn = 0; tn < (nx + 63) / 64; tn++) gw.push_back(make_int2(i, (tm << 16) | tn));
+                for (int tm = 0; tm < (ny + 31) / 32; tm++)
+                    for (int tn = 0; tn < (nx + 31) / 32; tn++) gw32.push_back(make_int2(i, (tm << 16) | tn));
                 // item -1: the singular x wavenumber 0 on its own; items cb >= 0:
                 // wavenumbers 1 + 32 cb + lane
                 yw.push_back(make_int2(i, -1));
                 for (int cb = 0; cb < (nx - 1 + 31) / 32; cb++) yw.push_back(make_int2(i, cb));
             }
         }
+        // 64 x 64 GEMM tiles unless they would leave most SMs idle (small batches)
+        if (gw.size() < 296) { gw.swap(gw32); gtile = 32; }
         nrwork = (int)rw.size(); ngwork = (int)gw.size(); nywork = (int)yw.size();
         if (int r = upload_vec(&rwork, rw)) return r;
         if (int r = upload_vec(&gwork, gw)) return r;
@@ -407,7 +411,7 @@ template <class T> struct Batch : BatchBase {
     // density means from rho_part, then the direct solve on buffer src
     int poisson(int src) {
         CC_CUDA(launch_batch_finalize(dred, n, spd_part, rho_part, BF_MEAN, dt, tclk, active, rho_mean, st()));
-        CC_CUDA(DPoissonLaunch<T>::solve(dinst, gwork, ngwork, ywork, nywork, src, rho_mean, active, st()));
+        CC_CUDA(DPoissonLaunch<T>::solve(dinst, gwork, ngwork, gtile, ywork, nywork, src, rho_mean, active, st()));
         count(4);
         h->perf.poisson_solves += 1;
         return CC_OK;

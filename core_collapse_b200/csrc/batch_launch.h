@@ -37,8 +37,9 @@ template <class T> struct BatchLaunch {
 
 template <class T> struct DPoissonLaunch {
     // rho of buffer src -> phi, for every active instance
-    static cudaError_t solve(const BatchInst<T>* inst, const int2* gwork, int ngwork, const int2* ywork, int nywork,
-                             int src, const double* rho_mean, const int* active, cudaStream_t s);
+    // gwork: GEMM tiles of gtile x gtile outputs (64 or 32)
+    static cudaError_t solve(const BatchInst<T>* inst, const int2* gwork, int ngwork, int gtile, const int2* ywork,
+                             int nywork, int src, const double* rho_mean, const int* active, cudaStream_t s);
 };
 
 // flags of the finaliser

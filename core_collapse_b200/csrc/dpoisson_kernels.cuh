@@ -15,7 +15,8 @@
 // an explicit fma() in a fixed order, so the CPU restatement (std::fma in the
 // same order) reproduces the result bit for bit.
 //
-// Work-lists: GEMM tiles {instance, (tm << 16) | tn} of DPM x DPN outputs;
+// Work-lists: GEMM tiles {instance, (tm << 16) | tn} of TM x TM outputs (TM 64,
+// or 32 when 64-tiles would leave SMs idle: same per-output k order, same bits);
 // y-solve items {instance, -1} (the singular wavenumber 0) and {instance,
 // column block} of DPC wavenumbers 1 + DPC cb + lane, one thread per column.
 #pragma once
@@ -25,37 +26,39 @@
 
 namespace ccb {
 
-constexpr int DPM = 64, DPN = 64, DPK = 16, DPNT = 256;   // GEMM tile, 4 x 4 outputs per thread
+constexpr int DPK = 16, DPNT = 256;   // GEMM K chunk and threads; tiles TM x TM, TM/16 x TM/16 outputs per thread
 constexpr int DPC = 32;                                    // y-solve columns per block
 
 // Software-pipelined tile loop: the next K chunk is loaded into registers
 // while the current one is multiplied from shared memory; raw values are
 // converted (MODE 0: 4 pi G (rho - mean)) only when they are stored, so no
 // instruction waits on a load in flight during the multiply.
-template <class T, int MODE>
+template <class T, int MODE, int TM>
 __global__ void __launch_bounds__(DPNT)
 dp_gemm_kernel(const BatchInst<T>* __restrict__ inst, const int2* __restrict__ gwork, int ngwork, int src,
                const double* __restrict__ rho_mean, const int* __restrict__ active) {
     using AT = typename std::conditional<MODE == 0, T, double>::type;
-    __shared__ double As[DPK][DPM + 1];   // k-major A tile
-    __shared__ double Bs[DPK][DPN];
+    constexpr int RPT = TM / 16;            // outputs per thread per dimension
+    constexpr int LQ = TM * DPK / DPNT;     // tile elements each thread loads per K chunk
+    __shared__ double As[DPK][TM + 1];      // k-major A tile
+    __shared__ double Bs[DPK][TM];
     const int tr = threadIdx.x / 16, tc = threadIdx.x % 16;
     for (int w = blockIdx.x; w < ngwork; w += gridDim.x) {
         const int2 it = gwork[w];
         if (active[it.x] == 0) continue;   // uniform over the block
         const BatchInst<T>& I = inst[it.x];
         const int nx = I.c.nx, ny = I.c.ny, P = I.c.pitch;
-        const int m0 = (it.y >> 16) * DPM, n0 = (it.y & 0xffff) * DPN;
+        const int m0 = (it.y >> 16) * TM, n0 = (it.y & 0xffff) * TM;
         const double* __restrict__ B = (MODE == 0) ? I.txt : I.tx;   // K x N row-major, K = N = nx
         const T* __restrict__ rho = I.buf[src].rho;
         const double* __restrict__ ah = I.ah;
         const double mean = (MODE == 0) ? rho_mean[it.x] : 0.0;
         const double fpg = I.fourpiG;
-        AT ra[4];
-        double rb[4];
+        AT ra[LQ];
+        double rb[LQ];
         auto gload = [&](int k0) {
 #pragma unroll
-            for (int q = 0; q < 4; q++) {
+            for (int q = 0; q < LQ; q++) {
                 const int e = threadIdx.x + q * DPNT;
                 const int gm = m0 + e / DPK, gk = k0 + e % DPK;
                 ra[q] = AT(0);
@@ -63,48 +66,48 @@ dp_gemm_kernel(const BatchInst<T>* __restrict__ inst, const int2* __restrict__ g
                     if (MODE == 0) ra[q] = (AT)rho[(size_t)gm * P + gk];
                     else ra[q] = (AT)ah[(size_t)gm * nx + gk];
                 }
-                const int gkb = k0 + e / DPN, gn = n0 + e % DPN;
+                const int gkb = k0 + e / TM, gn = n0 + e % TM;
                 rb[q] = (gkb < nx && gn < nx) ? B[(size_t)gkb * nx + gn] : 0.0;
             }
         };
-        double acc[4][4];
+        double acc[RPT][RPT];
 #pragma unroll
-        for (int r = 0; r < 4; r++)
+        for (int r = 0; r < RPT; r++)
 #pragma unroll
-            for (int c = 0; c < 4; c++) acc[r][c] = 0.0;
+            for (int c = 0; c < RPT; c++) acc[r][c] = 0.0;
         gload(0);
         for (int k0 = 0; k0 < nx; k0 += DPK) {
 #pragma unroll
-            for (int q = 0; q < 4; q++) {
+            for (int q = 0; q < LQ; q++) {
                 const int e = threadIdx.x + q * DPNT;
                 const int m = e / DPK, kk = e % DPK;
                 double v = (double)ra[q];
                 if (MODE == 0) v = (m0 + m < ny && k0 + kk < nx) ? fpg * (v - mean) : 0.0;
                 As[kk][m] = v;
-                Bs[e / DPN][e % DPN] = rb[q];
+                Bs[e / TM][e % TM] = rb[q];
             }
             __syncthreads();
             if (k0 + DPK < nx) gload(k0 + DPK);
             const int kend = min(DPK, nx - k0);
             for (int kk = 0; kk < kend; kk++) {
-                double a[4], b[4];
+                double a[RPT], b[RPT];
 #pragma unroll
-                for (int r = 0; r < 4; r++) a[r] = As[kk][tr + 16 * r];
+                for (int r = 0; r < RPT; r++) a[r] = As[kk][tr + 16 * r];
 #pragma unroll
-                for (int c = 0; c < 4; c++) b[c] = Bs[kk][tc + 16 * c];
+                for (int c = 0; c < RPT; c++) b[c] = Bs[kk][tc + 16 * c];
 #pragma unroll
-                for (int r = 0; r < 4; r++)
+                for (int r = 0; r < RPT; r++)
 #pragma unroll
-                    for (int c = 0; c < 4; c++) acc[r][c] = fma(a[r], b[c], acc[r][c]);
+                    for (int c = 0; c < RPT; c++) acc[r][c] = fma(a[r], b[c], acc[r][c]);
             }
             __syncthreads();
         }
 #pragma unroll
-        for (int r = 0; r < 4; r++) {
+        for (int r = 0; r < RPT; r++) {
             const int gm = m0 + tr + 16 * r;
             if (gm >= ny) continue;
 #pragma unroll
-            for (int c = 0; c < 4; c++) {
+            for (int c = 0; c < RPT; c++) {
                 const int gn = n0 + tc + 16 * c;
                 if (gn >= nx) continue;
                 if (MODE == 0) I.ah[(size_t)gm * nx + gn] = acc[r][c];

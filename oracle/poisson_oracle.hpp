@@ -252,12 +252,15 @@ inline void direct_basis(int n, bool periodic, double d, std::vector<double>& ba
 // Density mean in the batched reduction order: 32 x 8 cell tiles in row-major
 // tile order; inside a tile a warp holds one row of 32 cells, the lanes are
 // summed by a shuffle-down tree (offsets 16..1), then the 8 warp sums by the
-// same tree (absent lanes 0.0); tile sums are added sequentially.
+// same tree (absent lanes 0.0).  The tile sums are folded by 32 lanes (lane
+// l: tiles l, l+32, ... in order) and the lane values by the same tree.
 inline double batch_tile_mean(int nx, int ny, const std::vector<double>& rho) {
     const int tx_n = (nx + 31) / 32, ty_n = (ny + 7) / 8;
-    double total = 0.0;
+    double lane[32];
+    for (int l = 0; l < 32; l++) lane[l] = 0.0;
+    int t = 0;
     for (int ty = 0; ty < ty_n; ty++)
-        for (int tx = 0; tx < tx_n; tx++) {
+        for (int tx = 0; tx < tx_n; tx++, t++) {
             double w[32];
             for (int r = 0; r < 32; r++) w[r] = 0.0;
             for (int r = 0; r < 8; r++) {
@@ -272,9 +275,11 @@ inline double batch_tile_mean(int nx, int ny, const std::vector<double>& rho) {
             }
             for (int o = 16; o > 0; o >>= 1)
                 for (int l = 0; l < o; l++) w[l] = w[l] + w[l + o];
-            total += w[0];
+            lane[t % 32] = lane[t % 32] + w[0];
         }
-    return total / ((double)nx * (double)ny);
+    for (int o = 16; o > 0; o >>= 1)
+        for (int l = 0; l < o; l++) lane[l] = lane[l] + lane[l + o];
+    return lane[0] / ((double)nx * (double)ny);
 }
 
 // Factors of the y system (Dyy + lam) u = r for one x wavenumber, set up
