@@ -416,6 +416,16 @@ __global__ void adj_add_state_kernel(const M2Const<double> c, const Fields<doubl
     }
 }
 
+// zero nplanes planes of `plane` doubles each (one launch for a whole set)
+__global__ void adj_zero_kernel(double* const* planes, int nplanes, size_t plane) {
+    const size_t n2 = plane / 2;   // planes hold an even number of doubles (pitch is a multiple of 32)
+    for (int k = 0; k < nplanes; k++) {
+        double2* q = reinterpret_cast<double2*>(planes[k]);
+        for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n2; i += (size_t)gridDim.x * blockDim.x)
+            q[i] = make_double2(0.0, 0.0);
+    }
+}
+
 // dst[q] += src[q] over the cells of a pitched plane
 __global__ void adj_add_plane_kernel(int nx, int ny, int P, double* __restrict__ dst, const double* __restrict__ src) {
     for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < nx * ny; k += gridDim.x * blockDim.x) {

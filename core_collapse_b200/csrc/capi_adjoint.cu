@@ -62,6 +62,9 @@ struct Adjoint : Batch<double> {
     BatchInst<double>* recB = nullptr;   // same buffers, phi Phi1[l], rec Rec2[l]
     BatchInst<double>* recC = nullptr;   // buf {St[l], St[l+1], S2[l]} for the average
     BatchInst<double>* recP = nullptr;   // Poisson adjoint: density <- LamPhi, phi -> PoisOut
+    double** zAvg = nullptr;             // planes zeroed before the average reverse (LamS2, LamBav)
+    double** zStage = nullptr;           // before a stage reverse (LamIn, LamW, LamF5x, LamG5y, LamPhi)
+    double** zS1 = nullptr;              // LamS1
     bool loaded0 = false;
 
     Adjoint(cc_handle* hh, const cc_mhd2d_params& pp, int k, int mx)
@@ -124,6 +127,19 @@ struct Adjoint : Batch<double> {
         for (int l = 0; l < K; l++) {
             if (int r = upload_vec(&dRec1[l], Rec1[l])) return r;
             if (int r = upload_vec(&dRec2[l], Rec2[l])) return r;
+        }
+        {
+            auto st8 = [](const Fields<double>& f, std::vector<double*>& v) {
+                for (double* q : {f.rho, f.mx, f.my, f.mz, f.E, f.Bz, f.bx, f.by}) v.push_back(q);
+            };
+            std::vector<double*> za, zs, z1;
+            st8(LamS2, za); za.push_back(LamBavx); za.push_back(LamBavy);
+            st8(LamIn, zs); for (int m = 0; m < 8; m++) zs.push_back(LamW[m]);
+            zs.push_back(LamF5x); zs.push_back(LamG5y); zs.push_back(LamPhi);
+            st8(LamS1, z1);
+            if (int r = upload_vec(&zAvg, za)) return r;
+            if (int r = upload_vec(&zStage, zs)) return r;
+            if (int r = upload_vec(&zS1, z1)) return r;
         }
         if (int r = dalloc(&dtrec, (size_t)max_steps)) return r;
         if (int r = dalloc(&lam_eta, 1)) return r;
@@ -302,11 +318,8 @@ struct Adjoint : Batch<double> {
         const M2Const<double>& c = hinst[0].c;
         const int ncell = c.nx * c.ny;
         const int nedge = (c.nx + 1) * (c.ny + 1);
-        if (int r = zero_state(LamIn)) return r;
-        for (int m = 0; m < 8; m++)
-            if (int r = zero(LamW[m])) return r;
-        for (double* q : {LamF5x, LamG5y, LamPhi})
-            if (int r = zero(q)) return r;
+        adj_zero_kernel<<<adj_grid((int)(plane / 2)), ADJ_NT, 0, st()>>>(zStage, 19, plane);
+        CC_CUDA(cudaGetLastError());
         CC_CUDA(cudaMemcpyAsync(LamB1x, lout.bx, sizeof(double) * plane, cudaMemcpyDeviceToDevice, st()));
         CC_CUDA(cudaMemcpyAsync(LamB1y, lout.by, sizeof(double) * plane, cudaMemcpyDeviceToDevice, st()));
         adj_prep_kernel<<<adj_grid(ncell), ADJ_NT, 0, st()>>>(c, sin, defer, dtv, dUt, dWp);
@@ -336,9 +349,8 @@ struct Adjoint : Batch<double> {
         const M2Const<double>& c = hinst[0].c;
         const int ncell = c.nx * c.ny, nedge = (c.nx + 1) * (c.ny + 1);
         // RK average
-        if (int r = zero_state(LamS2)) return r;
-        if (int r = zero(LamBavx)) return r;
-        if (int r = zero(LamBavy)) return r;
+        adj_zero_kernel<<<adj_grid((int)(plane / 2)), ADJ_NT, 0, st()>>>(zAvg, 10, plane);
+        CC_CUDA(cudaGetLastError());
         adj_average_kernel<<<adj_grid(ncell), ADJ_NT, 0, st()>>>(c, St[l], S2[l], dtv, lnext, lun, LamS2, LamBavx,
                                                                  LamBavy, lam_eta);
         CC_CUDA(cudaGetLastError());
@@ -346,7 +358,8 @@ struct Adjoint : Batch<double> {
         CC_CUDA(cudaGetLastError());
         // stage 2: Joule(S1') -> S2'
         if (int r = stage_reverse(S1[l], S2[l], Phi1[l], dRec2[l], true, dtv, LamS2)) return r;
-        if (int r = zero_state(LamS1)) return r;
+        adj_zero_kernel<<<adj_grid((int)(plane / 2)), ADJ_NT, 0, st()>>>(zS1, 8, plane);
+        CC_CUDA(cudaGetLastError());
         adj_joule_kernel<<<adj_grid(ncell), ADJ_NT, 0, st()>>>(c, S1[l], dtv, LamIn, LamS1, lam_eta);
         CC_CUDA(cudaGetLastError());
         adj_add_state_kernel<<<adj_grid(nedge), ADJ_NT, 0, st()>>>(c, LamS1, LamIn, false);
