@@ -265,6 +265,7 @@ adj_edge_kernel(const M2Const<double> c, const Fields<double> sin, double dt, co
 __device__ __forceinline__ void face_state_scatter(const M2Const<double>& c, double* const* wp, double* const* lw,
                                                    const int comp[7], size_t qm, size_t q0, size_t qp, double h,
                                                    const double lf[7]) {
+#pragma unroll
     for (int k = 0; k < 7; k++) {
         const int m = comp[k];
         const double wm = wp[m][qm], wc = wp[m][q0], wq = wp[m][qp];
@@ -285,8 +286,10 @@ __device__ __forceinline__ Prim<double> face_state_fwd(const M2Const<double>& c,
                                                        size_t q0, size_t qp, double h, bool ydir) {
     Prim<double> W;
     double v[8];
+#pragma unroll
     for (int m = 0; m < 8; m++) v[m] = wp[m][q0];
     const int rc[7] = {0, 1, 2, 3, 4, ydir ? 5 : 6, 7};
+#pragma unroll
     for (int k = 0; k < 7; k++) {
         const int m = rc[k];
         v[m] = wp[m][q0] + h * mc_slope(wp[m][qm], wp[m][q0], wp[m][qp]);
@@ -325,6 +328,7 @@ adj_face_kernel(const M2Const<double> c, const Fields<double> sin, double* const
         const double ih = YDIR ? c.inv_dy : c.inv_dx;
         double lF[7];
         const int dmap[7] = {0, 1, 2, 3, 4, -1, 5};
+#pragma unroll
         for (int m = 0; m < 7; m++) {
             if (dmap[m] < 0) { lF[m] = lf5[qface]; continue; }
             double v = 0.0;
@@ -333,6 +337,7 @@ adj_face_kernel(const M2Const<double> c, const Fields<double> sin, double* const
             lF[m] = ih * v;
         }
         bool any = false;
+#pragma unroll
         for (int m = 0; m < 7; m++) any = any || (lF[m] != 0.0);
         if (!any) continue;
         Flux<double> g;
@@ -348,6 +353,7 @@ adj_face_kernel(const M2Const<double> c, const Fields<double> sin, double* const
         const double aL[8] = {lL.r, lL.u, lL.v, lL.w, lL.P, lL.bx, lL.by, lL.bz};
         const double aR[8] = {lR.r, lR.u, lR.v, lR.w, lR.P, lR.bx, lR.by, lR.bz};
         double fl[7], fr[7];
+#pragma unroll
         for (int m = 0; m < 7; m++) { fl[m] = aL[rc[m]]; fr[m] = aR[rc[m]]; }
         face_state_scatter(c, wp, lw, rc, qLm, qL, qR, 0.5, fl);
         face_state_scatter(c, wp, lw, rc, qL, qR, qRp, -0.5, fr);

@@ -74,7 +74,8 @@ __device__ __forceinline__ void eh_hllc(const EHConst<T>& c, const EPrim<T>& L, 
     // euler_flux_x / euler_flux_y (EH:113-123) of the chosen side
     const bool upL = (T(0.0) <= SL), upR = !(T(0.0) <= SL) && (T(0.0) >= SR);
     const bool left = upL || (!upR && (T(0.0) < SM));
-    const EPrim<T>& W = left ? L : R;
+    EPrim<T> W;   // by value: a reference chosen at run time would put L and R in local memory
+    W.r = left ? L.r : R.r; W.u = left ? L.u : R.u; W.v = left ? L.v : R.v; W.P = left ? L.P : R.P;
     const T Ef = W.P / c.gm1 + T(0.5) * W.r * (W.u * W.u + W.v * W.v);
     if (DIR == 0) {
         F[0] = W.r * W.u; F[1] = W.r * W.u * W.u + W.P; F[2] = W.r * W.u * W.v; F[3] = (Ef + W.P) * W.u;

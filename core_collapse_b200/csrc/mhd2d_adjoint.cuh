@@ -23,10 +23,14 @@ template <class T> CC_HD Prim<T> prim_zero() {
     return p;
 }
 
+template <class T> CC_HD void prim_acc(Prim<T>& a, const Prim<T>& b) {
+    a.r += b.r; a.u += b.u; a.v += b.v; a.w += b.w; a.P += b.P; a.bx += b.bx; a.by += b.by; a.bz += b.bz;
+}
+
 // energy (M2:357): P/gm1 + 0.5 r |v|^2 + 0.5 |B|^2
 template <class T>
 CC_HD void energy_vjp(const M2Const<T>& c, const Prim<T>& W, T lE, Prim<T>& lW) {
-    lW.P += lE / c.gm1;
+    lW.P += lE * (T(1) / c.gm1);
     lW.r += T(0.5) * (W.u * W.u + W.v * W.v + W.w * W.w) * lE;
     lW.u += W.r * W.u * lE;
     lW.v += W.r * W.v * lE;
@@ -61,12 +65,13 @@ CC_HD void fast_speed_vjp(const M2Const<T>& c, const Prim<T>& W, T bn, T lcf, Pr
     const T lvn2 = -T(4.0) * a2 * ldisc;
     la2 += ls;
     const T lvA2 = ls;
-    const T lb2 = lvA2 / rr;
-    const T lrr = -lvA2 * vA2 / rr - lvn2 * vn2 / rr;
-    lbn += T(2) * bn * lvn2 / rr;
+    const T i_rr = T(1) / rr, i_rf = T(1) / rf;
+    const T lb2 = lvA2 * i_rr;
+    const T lrr = -(lvA2 * vA2 + lvn2 * vn2) * i_rr;
+    lbn += T(2) * bn * lvn2 * i_rr;
     if (!(W.r < T(1e-300))) lW.r += lrr;
-    lW.P += c.gamma * la2 / rf;
-    const T lrf = -la2 * a2 / rf;
+    lW.P += c.gamma * la2 * i_rf;
+    const T lrf = -la2 * a2 * i_rf;
     if (!(W.r < c.floor_rho)) lW.r += lrf;
     lW.bx += T(2) * W.bx * lb2;
     lW.by += T(2) * W.by * lb2;
@@ -116,330 +121,329 @@ CC_HD void hlld_x_vjp(const M2Const<T>& c, Prim<T> L, Prim<T> R, const T Bn, con
     const T SL = vmin(uLm, uRm);
     const T SR = vmax(uLp, uRp);
 
-    auto finish = [&]() {
-        T lcfL = T(0), lcfR = T(0);
-        if (uRm < uLm) { aR.u += lSL; lcfR -= lSL; } else { aL.u += lSL; lcfL -= lSL; }
-        if (uLp < uRp) { aR.u += lSR; lcfR += lSR; } else { aL.u += lSR; lcfL += lSR; }
-        fast_speed_vjp(c, L, Bn, lcfL, aL, aBn);
-        fast_speed_vjp(c, R, Bn, lcfR, aR, aBn);
-        aBn += aL.bx + aR.bx;
-        lL.r += aL.r; lL.u += aL.u; lL.v += aL.v; lL.w += aL.w; lL.P += aL.P; lL.by += aL.by; lL.bz += aL.bz;
-        lR.r += aR.r; lR.u += aR.u; lR.v += aR.v; lR.w += aR.w; lR.P += aR.P; lR.by += aR.by; lR.bz += aR.bz;
-        lBn += aBn;
-    };
+    do {   // one exit: the common tail below runs once, whatever the region
+        if (T(0.0) <= SL) { ideal_flux_vjp(c, L, lF, aL); break; }
+        if (T(0.0) >= SR) { ideal_flux_vjp(c, R, lF, aR); break; }
 
-    if (T(0.0) <= SL) { ideal_flux_vjp(c, L, lF, aL); finish(); return; }
-    if (T(0.0) >= SR) { ideal_flux_vjp(c, R, lF, aR); finish(); return; }
+        const T EL = energy(c, L), ER = energy(c, R);
+        const T ptL = L.P + T(0.5) * (L.bx * L.bx + L.by * L.by + L.bz * L.bz);
+        const T ptR = R.P + T(0.5) * (R.bx * R.bx + R.by * R.by + R.bz * R.bz);
+        T lEL = T(0), lER = T(0), lptL = T(0), lptR = T(0);
 
-    const T EL = energy(c, L), ER = energy(c, R);
-    const T ptL = L.P + T(0.5) * (L.bx * L.bx + L.by * L.by + L.bz * L.bz);
-    const T ptR = R.P + T(0.5) * (R.bx * R.bx + R.by * R.by + R.bz * R.bz);
-    T lEL = T(0), lER = T(0), lptL = T(0), lptR = T(0);
+        if (fabs(Bn) < T(1e-12)) {  // HLL (M2:449-467)
+            const Flux<T> FL = ideal_flux(c, L), FR = ideal_flux(c, R);
+            const T inv = T(1.0) / (SR - SL);
+            const T s2 = SL * SR;
+            const T fl[7] = {FL.f0, FL.f1, FL.f2, FL.f3, FL.f4, FL.f5, FL.f6};
+            const T fr[7] = {FR.f0, FR.f1, FR.f2, FR.f3, FR.f4, FR.f5, FR.f6};
+            const T ul[7] = {L.r, L.r * L.u, L.r * L.v, L.r * L.w, EL, L.by, L.bz};
+            const T ur[7] = {R.r, R.r * R.u, R.r * R.v, R.r * R.w, ER, R.by, R.bz};
+            const T lf[7] = {lF.f0, lF.f1, lF.f2, lF.f3, lF.f4, lF.f5, lF.f6};
+            T lfl[7], lfr[7], lul[7], lur[7];
+            T linv = T(0), ls2 = T(0);
+    #pragma unroll
+            for (int k = 0; k < 7; k++) {
+                const T num = SR * fl[k] - SL * fr[k] + s2 * (ur[k] - ul[k]);
+                const T lnum = lf[k] * inv;
+                linv += lf[k] * num;
+                lSR += lnum * fl[k];
+                lfl[k] = lnum * SR;
+                lSL -= lnum * fr[k];
+                lfr[k] = -lnum * SL;
+                ls2 += lnum * (ur[k] - ul[k]);
+                lur[k] = lnum * s2;
+                lul[k] = -lnum * s2;
+            }
+            const T ld = -linv * inv * inv;
+            lSR += ld;
+            lSL -= ld;
+            lSL += ls2 * SR;
+            lSR += ls2 * SL;
+            Flux<T> g;
+            g.f0 = lfl[0]; g.f1 = lfl[1]; g.f2 = lfl[2]; g.f3 = lfl[3]; g.f4 = lfl[4]; g.f5 = lfl[5]; g.f6 = lfl[6];
+            ideal_flux_vjp(c, L, g, aL);
+            g.f0 = lfr[0]; g.f1 = lfr[1]; g.f2 = lfr[2]; g.f3 = lfr[3]; g.f4 = lfr[4]; g.f5 = lfr[5]; g.f6 = lfr[6];
+            ideal_flux_vjp(c, R, g, aR);
+            aL.r += lul[0] + lul[1] * L.u + lul[2] * L.v + lul[3] * L.w;
+            aL.u += lul[1] * L.r; aL.v += lul[2] * L.r; aL.w += lul[3] * L.r;
+            lEL += lul[4]; aL.by += lul[5]; aL.bz += lul[6];
+            aR.r += lur[0] + lur[1] * R.u + lur[2] * R.v + lur[3] * R.w;
+            aR.u += lur[1] * R.r; aR.v += lur[2] * R.r; aR.w += lur[3] * R.r;
+            lER += lur[4]; aR.by += lur[5]; aR.bz += lur[6];
+        } else {
+            // ---- forward recompute of the star construction (M2:470-529) ----
+            const T den = L.r * (SL - L.u) - R.r * (SR - R.u);
+            const bool sm_ok = fabs(den) > T(1e-14);
+            T SM = T(0.0);
+            if (sm_ok) SM = (ptR - ptL + L.r * L.u * (SL - L.u) - R.r * R.u * (SR - R.u)) / den;
+            const T rLs = L.r * (SL - L.u) / (SL - SM);
+            const T rRs = R.r * (SR - R.u) / (SR - SM);
+            const T pts = ptL + L.r * (SL - L.u) * (SM - L.u);
+            const T sL = SL - L.u, sR = SR - R.u;
+            const T bn2 = Bn * Bn;
+            const T dL = L.r * sL * (SL - SM) - bn2;
+            const T dR = R.r * sR * (SR - SM) - bn2;
+            const bool starL = fabs(dL) > T(1e-14), starR = fabs(dR) > T(1e-14);
+            T ByLs = L.by, BzLs = L.bz, ByRs = R.by, BzRs = R.bz;
+            T vLs = L.v, wLs = L.w, vRs = R.v, wRs = R.w;
+            T numL = T(0), ddL = T(1), numR = T(0), ddR = T(1);
+            if (starL) {
+                numL = L.r * sL * (SL - L.u) - bn2;
+                ByLs = L.by * numL / dL;
+                BzLs = L.bz * numL / dL;
+                ddL = L.r * (SL - L.u) * (SL - SM);
+                vLs = L.v - Bn * (ByLs - L.by) / ddL;
+                wLs = L.w - Bn * (BzLs - L.bz) / ddL;
+            }
+            if (starR) {
+                numR = R.r * sR * (SR - R.u) - bn2;
+                ByRs = R.by * numR / dR;
+                BzRs = R.bz * numR / dR;
+                ddR = R.r * (SR - R.u) * (SR - SM);
+                vRs = R.v - Bn * (ByRs - R.by) / ddR;
+                wRs = R.w - Bn * (BzRs - R.bz) / ddR;
+            }
+            const T sqL = sqrt(vmax(rLs, T(1e-300)));
+            const T sqR = sqrt(vmax(rRs, T(1e-300)));
+            const T SLL = SM - fabs(Bn) / sqL;
+            const T SRR = SM + fabs(Bn) / sqR;
+            const bool left = (T(0.0) < SM);
+            const bool outer = left ? (T(0.0) < SLL) : !(T(0.0) < SRR);
+            // the upwind side by value; its adjoint is folded into aL or aR after the last use
+            const Prim<T> W = prim_select(left, L, R);
+            Prim<T> aW = prim_zero<T>();
+            const T S = left ? SL : SR;
+            const T EW = left ? EL : ER;
+            const T ptW = left ? ptL : ptR;
+            const T rs = left ? rLs : rRs;
+            const T sgn = (Bn >= T(0.0)) ? T(1.0) : T(-1.0);
+            const T d2 = sqL + sqR;
+            T vs, ws, Bys, Bzs;
+            if (outer) {
+                vs = left ? vLs : vRs; ws = left ? wLs : wRs;
+                Bys = left ? ByLs : ByRs; Bzs = left ? BzLs : BzRs;
+            } else {
+                vs = (sqL * vLs + sqR * vRs + (ByRs - ByLs) * sgn) / d2;
+                ws = (sqL * wLs + sqR * wRs + (BzRs - BzLs) * sgn) / d2;
+                Bys = (sqL * ByRs + sqR * ByLs + sqL * sqR * (vRs - vLs) * sgn) / d2;
+                Bzs = (sqL * BzRs + sqR * BzLs + sqL * sqR * (wRs - wLs) * sgn) / d2;
+            }
+            const T vBs = SM * Bn + vs * Bys + ws * Bzs;
+            const T vBw = W.u * W.bx + W.v * W.by + W.w * W.bz;
+            const T numE = (S - W.u) * EW - (ptW * W.u - Bn * vBw) + (pts * SM - Bn * vBs);
+            const T dE = S - SM;
+            const T Es = numE / dE;
 
-    auto energies_and_pt = [&]() {
+            // ---- reverse (reciprocals of the recurring denominators computed once) ----
+            const T i_d2 = T(1) / d2, i_dE = T(1) / dE;
+            const T i_ddL = T(1) / ddL, i_ddR = T(1) / ddR;
+            const T i_dL = starL ? T(1) / dL : T(0), i_dR = starR ? T(1) / dR : T(0);
+            const T i_sLm = T(1) / (SL - SM), i_sRm = T(1) / (SR - SM);
+            ideal_flux_vjp(c, W, lF, aW);
+            T lS = lF.f0 * (rs - W.r) + lF.f1 * (rs * SM - W.r * W.u) + lF.f2 * (rs * vs - W.r * W.v) +
+                   lF.f3 * (rs * ws - W.r * W.w) + lF.f4 * (Es - EW) + lF.f5 * (Bys - W.by) + lF.f6 * (Bzs - W.bz);
+            const T lrs = S * (lF.f0 + lF.f1 * SM + lF.f2 * vs + lF.f3 * ws);
+            T lSM = S * lF.f1 * rs;
+            T lvs = S * lF.f2 * rs, lws = S * lF.f3 * rs;
+            const T lEs = S * lF.f4;
+            T lEW = -S * lF.f4;
+            T lBys = S * lF.f5, lBzs = S * lF.f6;
+            aW.r -= S * (lF.f0 + lF.f1 * W.u + lF.f2 * W.v + lF.f3 * W.w);
+            aW.u -= S * lF.f1 * W.r;
+            aW.v -= S * lF.f2 * W.r;
+            aW.w -= S * lF.f3 * W.r;
+            aW.by -= S * lF.f5;
+            aW.bz -= S * lF.f6;
+            // Es = numE / dE
+            const T lnumE = lEs * i_dE;
+            const T ldE = -lEs * Es * i_dE;
+            lS += ldE;
+            lSM -= ldE;
+            lS += lnumE * EW;
+            aW.u -= lnumE * EW;
+            lEW += lnumE * (S - W.u);
+            T lptW = -lnumE * W.u;
+            aW.u -= lnumE * ptW;
+            aBn += lnumE * vBw;
+            const T lvBw = lnumE * Bn;
+            T lpts = lnumE * SM;
+            lSM += lnumE * pts;
+            aBn -= lnumE * vBs;
+            const T lvBs = -lnumE * Bn;
+            // vBw = W.u W.bx + W.v W.by + W.w W.bz   (W.bx = Bn)
+            aW.u += lvBw * W.bx; aW.bx += lvBw * W.u;
+            aW.v += lvBw * W.by; aW.by += lvBw * W.v;
+            aW.w += lvBw * W.bz; aW.bz += lvBw * W.w;
+            if (left) prim_acc(aL, aW); else prim_acc(aR, aW);
+            // vBs = SM Bn + vs Bys + ws Bzs
+            lSM += lvBs * Bn; aBn += lvBs * SM;
+            lvs += lvBs * Bys; lBys += lvBs * vs;
+            lws += lvBs * Bzs; lBzs += lvBs * ws;
+            // side quantities
+            if (left) { lEL += lEW; lptL += lptW; lSL += lS; } else { lER += lEW; lptR += lptW; lSR += lS; }
+            T lrLs = left ? lrs : T(0), lrRs = left ? T(0) : lrs;
+            T lvLs = T(0), lwLs = T(0), lByLs = T(0), lBzLs = T(0), lvRs = T(0), lwRs = T(0), lByRs = T(0), lBzRs = T(0);
+            T lsqL = T(0), lsqR = T(0);
+            if (outer) {
+                if (left) { lvLs += lvs; lwLs += lws; lByLs += lBys; lBzLs += lBzs; }
+                else { lvRs += lvs; lwRs += lws; lByRs += lBys; lBzRs += lBzs; }
+            } else {
+                T ld2 = T(0);
+                const T lnv = lvs * i_d2;
+                ld2 -= lvs * vs * i_d2;
+                lsqL += lnv * vLs; lvLs += lnv * sqL; lsqR += lnv * vRs; lvRs += lnv * sqR;
+                lByRs += lnv * sgn; lByLs -= lnv * sgn;
+                const T lnw = lws * i_d2;
+                ld2 -= lws * ws * i_d2;
+                lsqL += lnw * wLs; lwLs += lnw * sqL; lsqR += lnw * wRs; lwRs += lnw * sqR;
+                lBzRs += lnw * sgn; lBzLs -= lnw * sgn;
+                const T lnby = lBys * i_d2;
+                ld2 -= lBys * Bys * i_d2;
+                lsqL += lnby * (ByRs + sqR * (vRs - vLs) * sgn);
+                lByRs += lnby * sqL;
+                lsqR += lnby * (ByLs + sqL * (vRs - vLs) * sgn);
+                lByLs += lnby * sqR;
+                lvRs += lnby * sqL * sqR * sgn;
+                lvLs -= lnby * sqL * sqR * sgn;
+                const T lnbz = lBzs * i_d2;
+                ld2 -= lBzs * Bzs * i_d2;
+                lsqL += lnbz * (BzRs + sqR * (wRs - wLs) * sgn);
+                lBzRs += lnbz * sqL;
+                lsqR += lnbz * (BzLs + sqL * (wRs - wLs) * sgn);
+                lBzLs += lnbz * sqR;
+                lwRs += lnbz * sqL * sqR * sgn;
+                lwLs -= lnbz * sqL * sqR * sgn;
+                lsqL += ld2;
+                lsqR += ld2;
+            }
+            if (!(rLs < T(1e-300)) && sqL > T(0)) lrLs += lsqL / (T(2) * sqL);
+            if (!(rRs < T(1e-300)) && sqR > T(0)) lrRs += lsqR / (T(2) * sqR);
+            // star states of each side (M2:424-442)
+            T ldL = T(0), ldR = T(0), lbn2 = T(0), lsL = T(0), lsR = T(0);
+            if (starL) {
+                const T tB = (ByLs - L.by), tZ = (BzLs - L.bz);
+                aL.v += lvLs;
+                aBn -= lvLs * tB * i_ddL;
+                lByLs -= lvLs * Bn * i_ddL;
+                aL.by += lvLs * Bn * i_ddL;
+                T lddL = lvLs * Bn * tB * i_ddL * i_ddL;
+                aL.w += lwLs;
+                aBn -= lwLs * tZ * i_ddL;
+                lBzLs -= lwLs * Bn * i_ddL;
+                aL.bz += lwLs * Bn * i_ddL;
+                lddL += lwLs * Bn * tZ * i_ddL * i_ddL;
+                // ddL = L.r (SL - L.u)(SL - SM)
+                aL.r += lddL * sL * (SL - SM);
+                lsL += lddL * L.r * (SL - SM);
+                lSL += lddL * L.r * sL;
+                lSM -= lddL * L.r * sL;
+                // ByLs = L.by numL / dL, BzLs = L.bz numL / dL
+                const T lnumL = (lByLs * L.by + lBzLs * L.bz) * i_dL;
+                aL.by += lByLs * numL * i_dL;
+                aL.bz += lBzLs * numL * i_dL;
+                ldL -= (lByLs * ByLs + lBzLs * BzLs) * i_dL;
+                // numL = L.r sL (SL - L.u) - bn2
+                aL.r += lnumL * sL * sL;
+                lsL += T(2) * lnumL * L.r * sL;
+                lbn2 -= lnumL;
+            } else {
+                aL.by += lByLs; aL.bz += lBzLs; aL.v += lvLs; aL.w += lwLs;
+            }
+            if (starR) {
+                const T tB = (ByRs - R.by), tZ = (BzRs - R.bz);
+                aR.v += lvRs;
+                aBn -= lvRs * tB * i_ddR;
+                lByRs -= lvRs * Bn * i_ddR;
+                aR.by += lvRs * Bn * i_ddR;
+                T lddR = lvRs * Bn * tB * i_ddR * i_ddR;
+                aR.w += lwRs;
+                aBn -= lwRs * tZ * i_ddR;
+                lBzRs -= lwRs * Bn * i_ddR;
+                aR.bz += lwRs * Bn * i_ddR;
+                lddR += lwRs * Bn * tZ * i_ddR * i_ddR;
+                aR.r += lddR * sR * (SR - SM);
+                lsR += lddR * R.r * (SR - SM);
+                lSR += lddR * R.r * sR;
+                lSM -= lddR * R.r * sR;
+                const T lnumR = (lByRs * R.by + lBzRs * R.bz) * i_dR;
+                aR.by += lByRs * numR * i_dR;
+                aR.bz += lBzRs * numR * i_dR;
+                ldR -= (lByRs * ByRs + lBzRs * BzRs) * i_dR;
+                aR.r += lnumR * sR * sR;
+                lsR += T(2) * lnumR * R.r * sR;
+                lbn2 -= lnumR;
+            } else {
+                aR.by += lByRs; aR.bz += lBzRs; aR.v += lvRs; aR.w += lwRs;
+            }
+            // dL = L.r sL (SL - SM) - bn2 (only differentiated where it was used)
+            if (starL) {
+                aL.r += ldL * sL * (SL - SM);
+                lsL += ldL * L.r * (SL - SM);
+                lSL += ldL * L.r * sL;
+                lSM -= ldL * L.r * sL;
+                lbn2 -= ldL;
+            }
+            if (starR) {
+                aR.r += ldR * sR * (SR - SM);
+                lsR += ldR * R.r * (SR - SM);
+                lSR += ldR * R.r * sR;
+                lSM -= ldR * R.r * sR;
+                lbn2 -= ldR;
+            }
+            aBn += T(2) * Bn * lbn2;
+            // pts = ptL + L.r (SL - L.u)(SM - L.u)
+            lptL += lpts;
+            aL.r += lpts * sL * (SM - L.u);
+            lSL += lpts * L.r * (SM - L.u);
+            lSM += lpts * L.r * sL;
+            aL.u -= lpts * L.r * ((SM - L.u) + sL);
+            // rLs = L.r (SL - L.u) / (SL - SM), rRs likewise
+            {
+                const T lq = lrLs * i_sLm;
+                const T lden = -lrLs * rLs * i_sLm;
+                lSL += lden; lSM -= lden;
+                aL.r += lq * sL; lSL += lq * L.r; aL.u -= lq * L.r;
+            }
+            {
+                const T lq = lrRs * i_sRm;
+                const T lden = -lrRs * rRs * i_sRm;
+                lSR += lden; lSM -= lden;
+                aR.r += lq * sR; lSR += lq * R.r; aR.u -= lq * R.r;
+            }
+            // sL = SL - L.u, sR = SR - R.u
+            lSL += lsL; aL.u -= lsL;
+            lSR += lsR; aR.u -= lsR;
+            // SM = numSM / den
+            if (sm_ok) {
+                const T i_den = T(1) / den;
+                const T lnum = lSM * i_den;
+                const T lden = -lSM * SM * i_den;
+                lptR += lnum;
+                lptL -= lnum;
+                aL.r += lnum * L.u * sL;
+                aL.u += lnum * L.r * (sL - L.u);
+                lSL += lnum * L.r * L.u;
+                aR.r -= lnum * R.u * sR;
+                aR.u -= lnum * R.r * (sR - R.u);
+                lSR -= lnum * R.r * R.u;
+                aL.r += lden * sL; lSL += lden * L.r; aL.u -= lden * L.r;
+                aR.r -= lden * sR; lSR -= lden * R.r; aR.u += lden * R.r;
+            }
+        }
         energy_vjp(c, L, lEL, aL);
         energy_vjp(c, R, lER, aR);
         aL.P += lptL; aL.bx += lptL * L.bx; aL.by += lptL * L.by; aL.bz += lptL * L.bz;
         aR.P += lptR; aR.bx += lptR * R.bx; aR.by += lptR * R.by; aR.bz += lptR * R.bz;
-    };
-
-    if (fabs(Bn) < T(1e-12)) {  // HLL (M2:449-467)
-        const Flux<T> FL = ideal_flux(c, L), FR = ideal_flux(c, R);
-        const T inv = T(1.0) / (SR - SL);
-        const T s2 = SL * SR;
-        const T fl[7] = {FL.f0, FL.f1, FL.f2, FL.f3, FL.f4, FL.f5, FL.f6};
-        const T fr[7] = {FR.f0, FR.f1, FR.f2, FR.f3, FR.f4, FR.f5, FR.f6};
-        const T ul[7] = {L.r, L.r * L.u, L.r * L.v, L.r * L.w, EL, L.by, L.bz};
-        const T ur[7] = {R.r, R.r * R.u, R.r * R.v, R.r * R.w, ER, R.by, R.bz};
-        const T lf[7] = {lF.f0, lF.f1, lF.f2, lF.f3, lF.f4, lF.f5, lF.f6};
-        T lfl[7], lfr[7], lul[7], lur[7];
-        T linv = T(0), ls2 = T(0);
-        for (int k = 0; k < 7; k++) {
-            const T num = SR * fl[k] - SL * fr[k] + s2 * (ur[k] - ul[k]);
-            const T lnum = lf[k] * inv;
-            linv += lf[k] * num;
-            lSR += lnum * fl[k];
-            lfl[k] = lnum * SR;
-            lSL -= lnum * fr[k];
-            lfr[k] = -lnum * SL;
-            ls2 += lnum * (ur[k] - ul[k]);
-            lur[k] = lnum * s2;
-            lul[k] = -lnum * s2;
-        }
-        const T ld = -linv * inv * inv;
-        lSR += ld;
-        lSL -= ld;
-        lSL += ls2 * SR;
-        lSR += ls2 * SL;
-        Flux<T> g;
-        g.f0 = lfl[0]; g.f1 = lfl[1]; g.f2 = lfl[2]; g.f3 = lfl[3]; g.f4 = lfl[4]; g.f5 = lfl[5]; g.f6 = lfl[6];
-        ideal_flux_vjp(c, L, g, aL);
-        g.f0 = lfr[0]; g.f1 = lfr[1]; g.f2 = lfr[2]; g.f3 = lfr[3]; g.f4 = lfr[4]; g.f5 = lfr[5]; g.f6 = lfr[6];
-        ideal_flux_vjp(c, R, g, aR);
-        aL.r += lul[0] + lul[1] * L.u + lul[2] * L.v + lul[3] * L.w;
-        aL.u += lul[1] * L.r; aL.v += lul[2] * L.r; aL.w += lul[3] * L.r;
-        lEL += lul[4]; aL.by += lul[5]; aL.bz += lul[6];
-        aR.r += lur[0] + lur[1] * R.u + lur[2] * R.v + lur[3] * R.w;
-        aR.u += lur[1] * R.r; aR.v += lur[2] * R.r; aR.w += lur[3] * R.r;
-        lER += lur[4]; aR.by += lur[5]; aR.bz += lur[6];
-        energies_and_pt();
-        finish();
-        return;
-    }
-
-    // ---- forward recompute of the star construction (M2:470-529) ----
-    const T den = L.r * (SL - L.u) - R.r * (SR - R.u);
-    const bool sm_ok = fabs(den) > T(1e-14);
-    T SM = T(0.0);
-    if (sm_ok) SM = (ptR - ptL + L.r * L.u * (SL - L.u) - R.r * R.u * (SR - R.u)) / den;
-    const T rLs = L.r * (SL - L.u) / (SL - SM);
-    const T rRs = R.r * (SR - R.u) / (SR - SM);
-    const T pts = ptL + L.r * (SL - L.u) * (SM - L.u);
-    const T sL = SL - L.u, sR = SR - R.u;
-    const T bn2 = Bn * Bn;
-    const T dL = L.r * sL * (SL - SM) - bn2;
-    const T dR = R.r * sR * (SR - SM) - bn2;
-    const bool starL = fabs(dL) > T(1e-14), starR = fabs(dR) > T(1e-14);
-    T ByLs = L.by, BzLs = L.bz, ByRs = R.by, BzRs = R.bz;
-    T vLs = L.v, wLs = L.w, vRs = R.v, wRs = R.w;
-    T numL = T(0), ddL = T(1), numR = T(0), ddR = T(1);
-    if (starL) {
-        numL = L.r * sL * (SL - L.u) - bn2;
-        ByLs = L.by * numL / dL;
-        BzLs = L.bz * numL / dL;
-        ddL = L.r * (SL - L.u) * (SL - SM);
-        vLs = L.v - Bn * (ByLs - L.by) / ddL;
-        wLs = L.w - Bn * (BzLs - L.bz) / ddL;
-    }
-    if (starR) {
-        numR = R.r * sR * (SR - R.u) - bn2;
-        ByRs = R.by * numR / dR;
-        BzRs = R.bz * numR / dR;
-        ddR = R.r * (SR - R.u) * (SR - SM);
-        vRs = R.v - Bn * (ByRs - R.by) / ddR;
-        wRs = R.w - Bn * (BzRs - R.bz) / ddR;
-    }
-    const T sqL = sqrt(vmax(rLs, T(1e-300)));
-    const T sqR = sqrt(vmax(rRs, T(1e-300)));
-    const T SLL = SM - fabs(Bn) / sqL;
-    const T SRR = SM + fabs(Bn) / sqR;
-    const bool left = (T(0.0) < SM);
-    const bool outer = left ? (T(0.0) < SLL) : !(T(0.0) < SRR);
-    const Prim<T>& W = left ? L : R;
-    Prim<T>& aW = left ? aL : aR;
-    const T S = left ? SL : SR;
-    const T EW = left ? EL : ER;
-    const T ptW = left ? ptL : ptR;
-    const T rs = left ? rLs : rRs;
-    const T sgn = (Bn >= T(0.0)) ? T(1.0) : T(-1.0);
-    const T d2 = sqL + sqR;
-    T vs, ws, Bys, Bzs;
-    if (outer) {
-        vs = left ? vLs : vRs; ws = left ? wLs : wRs;
-        Bys = left ? ByLs : ByRs; Bzs = left ? BzLs : BzRs;
-    } else {
-        vs = (sqL * vLs + sqR * vRs + (ByRs - ByLs) * sgn) / d2;
-        ws = (sqL * wLs + sqR * wRs + (BzRs - BzLs) * sgn) / d2;
-        Bys = (sqL * ByRs + sqR * ByLs + sqL * sqR * (vRs - vLs) * sgn) / d2;
-        Bzs = (sqL * BzRs + sqR * BzLs + sqL * sqR * (wRs - wLs) * sgn) / d2;
-    }
-    const T vBs = SM * Bn + vs * Bys + ws * Bzs;
-    const T vBw = W.u * W.bx + W.v * W.by + W.w * W.bz;
-    const T numE = (S - W.u) * EW - (ptW * W.u - Bn * vBw) + (pts * SM - Bn * vBs);
-    const T dE = S - SM;
-    const T Es = numE / dE;
-
-    // ---- reverse ----
-    ideal_flux_vjp(c, W, lF, aW);
-    T lS = lF.f0 * (rs - W.r) + lF.f1 * (rs * SM - W.r * W.u) + lF.f2 * (rs * vs - W.r * W.v) +
-           lF.f3 * (rs * ws - W.r * W.w) + lF.f4 * (Es - EW) + lF.f5 * (Bys - W.by) + lF.f6 * (Bzs - W.bz);
-    const T lrs = S * (lF.f0 + lF.f1 * SM + lF.f2 * vs + lF.f3 * ws);
-    T lSM = S * lF.f1 * rs;
-    T lvs = S * lF.f2 * rs, lws = S * lF.f3 * rs;
-    const T lEs = S * lF.f4;
-    T lEW = -S * lF.f4;
-    T lBys = S * lF.f5, lBzs = S * lF.f6;
-    aW.r -= S * (lF.f0 + lF.f1 * W.u + lF.f2 * W.v + lF.f3 * W.w);
-    aW.u -= S * lF.f1 * W.r;
-    aW.v -= S * lF.f2 * W.r;
-    aW.w -= S * lF.f3 * W.r;
-    aW.by -= S * lF.f5;
-    aW.bz -= S * lF.f6;
-    // Es = numE / dE
-    const T lnumE = lEs / dE;
-    const T ldE = -lEs * Es / dE;
-    lS += ldE;
-    lSM -= ldE;
-    lS += lnumE * EW;
-    aW.u -= lnumE * EW;
-    lEW += lnumE * (S - W.u);
-    T lptW = -lnumE * W.u;
-    aW.u -= lnumE * ptW;
-    aBn += lnumE * vBw;
-    const T lvBw = lnumE * Bn;
-    T lpts = lnumE * SM;
-    lSM += lnumE * pts;
-    aBn -= lnumE * vBs;
-    const T lvBs = -lnumE * Bn;
-    // vBw = W.u W.bx + W.v W.by + W.w W.bz   (W.bx = Bn)
-    aW.u += lvBw * W.bx; aW.bx += lvBw * W.u;
-    aW.v += lvBw * W.by; aW.by += lvBw * W.v;
-    aW.w += lvBw * W.bz; aW.bz += lvBw * W.w;
-    // vBs = SM Bn + vs Bys + ws Bzs
-    lSM += lvBs * Bn; aBn += lvBs * SM;
-    lvs += lvBs * Bys; lBys += lvBs * vs;
-    lws += lvBs * Bzs; lBzs += lvBs * ws;
-    // side quantities
-    if (left) { lEL += lEW; lptL += lptW; lSL += lS; } else { lER += lEW; lptR += lptW; lSR += lS; }
-    T lrLs = left ? lrs : T(0), lrRs = left ? T(0) : lrs;
-    T lvLs = T(0), lwLs = T(0), lByLs = T(0), lBzLs = T(0), lvRs = T(0), lwRs = T(0), lByRs = T(0), lBzRs = T(0);
-    T lsqL = T(0), lsqR = T(0);
-    if (outer) {
-        if (left) { lvLs += lvs; lwLs += lws; lByLs += lBys; lBzLs += lBzs; }
-        else { lvRs += lvs; lwRs += lws; lByRs += lBys; lBzRs += lBzs; }
-    } else {
-        T ld2 = T(0);
-        const T lnv = lvs / d2;
-        ld2 -= lvs * vs / d2;
-        lsqL += lnv * vLs; lvLs += lnv * sqL; lsqR += lnv * vRs; lvRs += lnv * sqR;
-        lByRs += lnv * sgn; lByLs -= lnv * sgn;
-        const T lnw = lws / d2;
-        ld2 -= lws * ws / d2;
-        lsqL += lnw * wLs; lwLs += lnw * sqL; lsqR += lnw * wRs; lwRs += lnw * sqR;
-        lBzRs += lnw * sgn; lBzLs -= lnw * sgn;
-        const T lnby = lBys / d2;
-        ld2 -= lBys * Bys / d2;
-        lsqL += lnby * (ByRs + sqR * (vRs - vLs) * sgn);
-        lByRs += lnby * sqL;
-        lsqR += lnby * (ByLs + sqL * (vRs - vLs) * sgn);
-        lByLs += lnby * sqR;
-        lvRs += lnby * sqL * sqR * sgn;
-        lvLs -= lnby * sqL * sqR * sgn;
-        const T lnbz = lBzs / d2;
-        ld2 -= lBzs * Bzs / d2;
-        lsqL += lnbz * (BzRs + sqR * (wRs - wLs) * sgn);
-        lBzRs += lnbz * sqL;
-        lsqR += lnbz * (BzLs + sqL * (wRs - wLs) * sgn);
-        lBzLs += lnbz * sqR;
-        lwRs += lnbz * sqL * sqR * sgn;
-        lwLs -= lnbz * sqL * sqR * sgn;
-        lsqL += ld2;
-        lsqR += ld2;
-    }
-    if (!(rLs < T(1e-300)) && sqL > T(0)) lrLs += lsqL / (T(2) * sqL);
-    if (!(rRs < T(1e-300)) && sqR > T(0)) lrRs += lsqR / (T(2) * sqR);
-    // star states of each side (M2:424-442)
-    T ldL = T(0), ldR = T(0), lbn2 = T(0), lsL = T(0), lsR = T(0);
-    if (starL) {
-        const T tB = (ByLs - L.by), tZ = (BzLs - L.bz);
-        aL.v += lvLs;
-        aBn -= lvLs * tB / ddL;
-        lByLs -= lvLs * Bn / ddL;
-        aL.by += lvLs * Bn / ddL;
-        T lddL = lvLs * Bn * tB / (ddL * ddL);
-        aL.w += lwLs;
-        aBn -= lwLs * tZ / ddL;
-        lBzLs -= lwLs * Bn / ddL;
-        aL.bz += lwLs * Bn / ddL;
-        lddL += lwLs * Bn * tZ / (ddL * ddL);
-        // ddL = L.r (SL - L.u)(SL - SM)
-        aL.r += lddL * sL * (SL - SM);
-        lsL += lddL * L.r * (SL - SM);
-        lSL += lddL * L.r * sL;
-        lSM -= lddL * L.r * sL;
-        // ByLs = L.by numL / dL, BzLs = L.bz numL / dL
-        const T lnumL = lByLs * L.by / dL + lBzLs * L.bz / dL;
-        aL.by += lByLs * numL / dL;
-        aL.bz += lBzLs * numL / dL;
-        ldL -= lByLs * ByLs / dL + lBzLs * BzLs / dL;
-        // numL = L.r sL (SL - L.u) - bn2
-        aL.r += lnumL * sL * sL;
-        lsL += T(2) * lnumL * L.r * sL;
-        lbn2 -= lnumL;
-    } else {
-        aL.by += lByLs; aL.bz += lBzLs; aL.v += lvLs; aL.w += lwLs;
-    }
-    if (starR) {
-        const T tB = (ByRs - R.by), tZ = (BzRs - R.bz);
-        aR.v += lvRs;
-        aBn -= lvRs * tB / ddR;
-        lByRs -= lvRs * Bn / ddR;
-        aR.by += lvRs * Bn / ddR;
-        T lddR = lvRs * Bn * tB / (ddR * ddR);
-        aR.w += lwRs;
-        aBn -= lwRs * tZ / ddR;
-        lBzRs -= lwRs * Bn / ddR;
-        aR.bz += lwRs * Bn / ddR;
-        lddR += lwRs * Bn * tZ / (ddR * ddR);
-        aR.r += lddR * sR * (SR - SM);
-        lsR += lddR * R.r * (SR - SM);
-        lSR += lddR * R.r * sR;
-        lSM -= lddR * R.r * sR;
-        const T lnumR = lByRs * R.by / dR + lBzRs * R.bz / dR;
-        aR.by += lByRs * numR / dR;
-        aR.bz += lBzRs * numR / dR;
-        ldR -= lByRs * ByRs / dR + lBzRs * BzRs / dR;
-        aR.r += lnumR * sR * sR;
-        lsR += T(2) * lnumR * R.r * sR;
-        lbn2 -= lnumR;
-    } else {
-        aR.by += lByRs; aR.bz += lBzRs; aR.v += lvRs; aR.w += lwRs;
-    }
-    // dL = L.r sL (SL - SM) - bn2 (only differentiated where it was used)
-    if (starL) {
-        aL.r += ldL * sL * (SL - SM);
-        lsL += ldL * L.r * (SL - SM);
-        lSL += ldL * L.r * sL;
-        lSM -= ldL * L.r * sL;
-        lbn2 -= ldL;
-    }
-    if (starR) {
-        aR.r += ldR * sR * (SR - SM);
-        lsR += ldR * R.r * (SR - SM);
-        lSR += ldR * R.r * sR;
-        lSM -= ldR * R.r * sR;
-        lbn2 -= ldR;
-    }
-    aBn += T(2) * Bn * lbn2;
-    // pts = ptL + L.r (SL - L.u)(SM - L.u)
-    lptL += lpts;
-    aL.r += lpts * sL * (SM - L.u);
-    lSL += lpts * L.r * (SM - L.u);
-    lSM += lpts * L.r * sL;
-    aL.u -= lpts * L.r * ((SM - L.u) + sL);
-    // rLs = L.r (SL - L.u) / (SL - SM), rRs likewise
-    {
-        const T lq = lrLs / (SL - SM);
-        const T lden = -lrLs * rLs / (SL - SM);
-        lSL += lden; lSM -= lden;
-        aL.r += lq * sL; lSL += lq * L.r; aL.u -= lq * L.r;
-    }
-    {
-        const T lq = lrRs / (SR - SM);
-        const T lden = -lrRs * rRs / (SR - SM);
-        lSR += lden; lSM -= lden;
-        aR.r += lq * sR; lSR += lq * R.r; aR.u -= lq * R.r;
-    }
-    // sL = SL - L.u, sR = SR - R.u
-    lSL += lsL; aL.u -= lsL;
-    lSR += lsR; aR.u -= lsR;
-    // SM = numSM / den
-    if (sm_ok) {
-        const T lnum = lSM / den;
-        const T lden = -lSM * SM / den;
-        lptR += lnum;
-        lptL -= lnum;
-        aL.r += lnum * L.u * sL;
-        aL.u += lnum * L.r * (sL - L.u);
-        lSL += lnum * L.r * L.u;
-        aR.r -= lnum * R.u * sR;
-        aR.u -= lnum * R.r * (sR - R.u);
-        lSR -= lnum * R.r * R.u;
-        aL.r += lden * sL; lSL += lden * L.r; aL.u -= lden * L.r;
-        aR.r -= lden * sR; lSR -= lden * R.r; aR.u += lden * R.r;
-    }
-    energies_and_pt();
-    finish();
+    } while (false);
+    T lcfL = T(0), lcfR = T(0);
+    if (uRm < uLm) { aR.u += lSL; lcfR -= lSL; } else { aL.u += lSL; lcfL -= lSL; }
+    if (uLp < uRp) { aR.u += lSR; lcfR += lSR; } else { aL.u += lSR; lcfL += lSR; }
+    fast_speed_vjp(c, L, Bn, lcfL, aL, aBn);
+    fast_speed_vjp(c, R, Bn, lcfR, aR, aBn);
+    aBn += aL.bx + aR.bx;
+    lL.r += aL.r; lL.u += aL.u; lL.v += aL.v; lL.w += aL.w; lL.P += aL.P; lL.by += aL.by; lL.bz += aL.bz;
+    lR.r += aR.r; lR.u += aR.u; lR.v += aR.v; lR.w += aR.w; lR.P += aR.P; lR.by += aR.by; lR.bz += aR.bz;
+    lBn += aBn;
 }
 
 // y-normal HLLD through the (u,v)/(Bx,By) swap (M2:540-561), reverse

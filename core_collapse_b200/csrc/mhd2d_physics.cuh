@@ -26,6 +26,16 @@ template <class T> struct M2Const {
 template <class T> struct Prim { T r, u, v, w, P, bx, by, bz; };
 template <class T> struct Flux { T f0, f1, f2, f3, f4, f5, f6; };  // rho,mx,my,mz,E,Bt1,Bt2
 
+// One of two states by value, component-wise (a reference chosen at run time
+// would force both states into local memory).
+template <class T>
+__host__ __device__ __forceinline__ Prim<T> prim_select(bool left, const Prim<T>& L, const Prim<T>& R) {
+    Prim<T> W;
+    W.r = left ? L.r : R.r; W.u = left ? L.u : R.u; W.v = left ? L.v : R.v; W.w = left ? L.w : R.w;
+    W.P = left ? L.P : R.P; W.bx = left ? L.bx : R.bx; W.by = left ? L.by : R.by; W.bz = left ? L.bz : R.bz;
+    return W;
+}
+
 // enforce_floors (M2:114-124)
 template <class T>
 __host__ __device__ __forceinline__ void floors(const M2Const<T>& c, T& rho, T mx, T my, T mz, T& E, T Bx, T By, T Bz) {
@@ -165,7 +175,7 @@ __host__ __device__ __forceinline__ Flux<T> hlld_x(const Cst& c, Prim<T> L, Prim
     // pick the region first, then build only the state it needs
     const bool left = (T(0.0) < SM);
     const bool outer = left ? (T(0.0) < SLL) : !(T(0.0) < SRR);
-    const Prim<T>& W = left ? L : R;
+    const Prim<T> W = prim_select(left, L, R);
     const T S = left ? SL : SR;
     const T EW = left ? EL : ER;
     const T ptW = left ? ptL : ptR;
