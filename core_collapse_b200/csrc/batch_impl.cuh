@@ -1,8 +1,9 @@
 // Definitions of BatchLaunch<T>; included once per precision TU.
 //
-// Stage tile candidates (TX, TY, CTAs per SM the launch bounds ask for):
-//   FP64: 32x8 (2), 16x16 (2)
-//   FP32: 32x16 (2), 32x8 (4), 64x8 (2)
+// Stage tile candidates (TX, TY, threads, CTAs per SM the launch bounds ask
+// for, split x/y slope buffers):
+//   FP64: 32x8/256 (2), 16x16/256 (2)
+//   FP32: 32x16/512 (2, split), 32x8/256 (4), 64x8/512 (2), 32x14/544 (2, split)
 // The autotuner of the batch handle times each on the actual work-list.
 #pragma once
 #include "batch_launch.h"
@@ -14,23 +15,36 @@ template <> struct BatchShapes<double> {
     static constexpr int N = 2;
     template <int K> struct S;
 };
-template <> template <> struct BatchShapes<double>::S<0> { static constexpr int TX = 32, TY = 8, MINB = 2; };
-template <> template <> struct BatchShapes<double>::S<1> { static constexpr int TX = 16, TY = 16, MINB = 2; };
+template <> template <> struct BatchShapes<double>::S<0> {
+    static constexpr int TX = 32, TY = 8, NT = 256, MINB = 2; static constexpr bool SPLIT = false;
+};
+template <> template <> struct BatchShapes<double>::S<1> {
+    static constexpr int TX = 16, TY = 16, NT = 256, MINB = 2; static constexpr bool SPLIT = false;
+};
 template <> struct BatchShapes<float> {
-    static constexpr int N = 3;
+    static constexpr int N = 4;
     template <int K> struct S;
 };
-template <> template <> struct BatchShapes<float>::S<0> { static constexpr int TX = 32, TY = 16, MINB = 2; };
-template <> template <> struct BatchShapes<float>::S<1> { static constexpr int TX = 32, TY = 8, MINB = 4; };
-template <> template <> struct BatchShapes<float>::S<2> { static constexpr int TX = 64, TY = 8, MINB = 2; };
+template <> template <> struct BatchShapes<float>::S<0> {
+    static constexpr int TX = 32, TY = 16, NT = 512, MINB = 2; static constexpr bool SPLIT = true;
+};
+template <> template <> struct BatchShapes<float>::S<1> {
+    static constexpr int TX = 32, TY = 8, NT = 256, MINB = 4; static constexpr bool SPLIT = false;
+};
+template <> template <> struct BatchShapes<float>::S<2> {
+    static constexpr int TX = 64, TY = 8, NT = 512, MINB = 2; static constexpr bool SPLIT = false;
+};
+template <> template <> struct BatchShapes<float>::S<3> {
+    static constexpr int TX = 32, TY = 14, NT = 544, MINB = 2; static constexpr bool SPLIT = true;
+};
 
 namespace {
 
 template <class T, int K> struct ShapeOps {
     using S = typename BatchShapes<T>::template S<K>;
-    static constexpr size_t smem() { return StageGeomT<T, S::TX, S::TY>::smem; }
+    static constexpr size_t smem() { return StageGeomT<T, S::TX, S::TY, S::NT, S::SPLIT>::smem; }
     template <bool D, int G, bool R = false> static auto kern() {
-        return m2b_stage_kernel<T, S::TX, S::TY, S::MINB, D, G, R>;
+        return m2b_stage_kernel<T, S::TX, S::TY, S::NT, S::MINB, S::SPLIT, D, G, R>;
     }
     static cudaError_t prepare_rec() {
         cudaError_t e;
@@ -42,7 +56,7 @@ template <class T, int K> struct ShapeOps {
     }
     static cudaError_t stage_rec(int grid, const BatchInst<T>* inst, const int2* work, int nwork, int src, int dst,
                                  bool defer, bool grav, const double* dt, const int* active, cudaStream_t s) {
-        const dim3 b(S::TX * S::TY);
+        const dim3 b(S::NT);
         if (defer && grav) kern<true, GRAV_PHI, true>()<<<grid, b, smem(), s>>>(inst, work, nwork, src, dst, dt, active);
         else if (defer) kern<true, GRAV_NONE, true>()<<<grid, b, smem(), s>>>(inst, work, nwork, src, dst, dt, active);
         else if (grav) kern<false, GRAV_PHI, true>()<<<grid, b, smem(), s>>>(inst, work, nwork, src, dst, dt, active);
@@ -58,11 +72,11 @@ template <class T, int K> struct ShapeOps {
         return cudaFuncSetAttribute(kern<true, GRAV_PHI>(), cudaFuncAttributeMaxDynamicSharedMemorySize, b);
     }
     static cudaError_t resident(int* per_sm) {
-        return cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm, kern<false, GRAV_PHI>(), S::TX * S::TY, smem());
+        return cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm, kern<false, GRAV_PHI>(), S::NT, smem());
     }
     static cudaError_t stage(int grid, const BatchInst<T>* inst, const int2* work, int nwork, int src, int dst,
                              bool defer, bool grav, const double* dt, const int* active, cudaStream_t s) {
-        const dim3 b(S::TX * S::TY);
+        const dim3 b(S::NT);
         if (defer && grav) kern<true, GRAV_PHI>()<<<grid, b, smem(), s>>>(inst, work, nwork, src, dst, dt, active);
         else if (defer) kern<true, GRAV_NONE>()<<<grid, b, smem(), s>>>(inst, work, nwork, src, dst, dt, active);
         else if (grav) kern<false, GRAV_PHI>()<<<grid, b, smem(), s>>>(inst, work, nwork, src, dst, dt, active);

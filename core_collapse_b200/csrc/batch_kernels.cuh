@@ -71,8 +71,8 @@ __device__ __forceinline__ void load_inst(BatchInst<T>* dst, const BatchInst<T>*
 // src/dst index the instance's rotating buffers; gravity from phi (GRAV_PHI)
 // or none.
 // ---------------------------------------------------------------------------
-template <class T, int TX, int TY, int MINB, bool DEFER, int GMODE, bool REC = false>
-__global__ void __launch_bounds__(TX * TY, MINB)
+template <class T, int TX, int TY, int NT, int MINB, bool SPLIT, bool DEFER, int GMODE, bool REC = false>
+__global__ void __launch_bounds__(NT, MINB)
 m2b_stage_kernel(const BatchInst<T>* __restrict__ inst, const int2* __restrict__ work, int nwork, int src, int dst,
                  const double* __restrict__ dt, const int* __restrict__ active) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -92,8 +92,8 @@ m2b_stage_kernel(const BatchInst<T>* __restrict__ inst, const int2* __restrict__
         }
         int tx, ty;
         unpack_tile(it, tx, ty);
-        m2_stage_tile<T, TX, TY, DEFER, GMODE, REC>(s_inst.c, s_inst.buf[src], s_inst.buf[dst], s_inst.phi, nullptr,
-                                                    (T)dt[it.x], tx * TX, ty * TY, sm, s_inst.rec);
+        m2_stage_tile<T, TX, TY, DEFER, GMODE, REC, NT, SPLIT>(s_inst.c, s_inst.buf[src], s_inst.buf[dst], s_inst.phi,
+                                                        nullptr, (T)dt[it.x], tx * TX, ty * TY, sm, s_inst.rec);
         __syncthreads();                            // shared tile buffers reused by the next tile
     }
 }

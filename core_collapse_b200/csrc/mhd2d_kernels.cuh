@@ -30,25 +30,46 @@ template <class T> struct Fields {
 
 enum GravMode { GRAV_NONE = 0, GRAV_ARRAYS = 1, GRAV_PHI = 2 };
 
-// Stage tile per precision: TX x TY cells per CTA (one thread per cell), a
-// halo-2 region of primitives, one shared slope buffer reused for x then y.
+// Stage tile per precision: TX x TY cells per CTA, NT threads, a halo-2
+// region of primitives, one shared slope buffer reused for x then y.  Every
+// phase is a loop of its items over the NT threads between two barriers, so
+// a phase whose item count is just above NT costs a second, nearly empty
+// round while the CTA's other warps wait at the barrier.  The FP32 tile is
+// sized so that slopes, x faces, y faces, edges and cells each fit one round:
+// 32 x 14 cells, 544 threads = 34 x 16 slope cells, 33 x 16 x faces,
+// 34 x 15 y faces.
+// SPLIT: separate x and y slope buffers (7 NSL more shared memory), so that
+// the x and y slopes form one phase and the x and y face fluxes another
+// (4 barriers per tile instead of 6; each item range padded to whole warps so
+// no warp mixes x and y work).
 template <class T> struct StageTile;
-template <> struct StageTile<double> { static constexpr int TX = 32, TY = 8, MINB = 2; };
-template <> struct StageTile<float> { static constexpr int TX = 32, TY = 16, MINB = 2; };
+template <> struct StageTile<double> {
+    static constexpr int TX = 32, TY = 8, NT = 256, MINB = 2;
+    static constexpr bool SPLIT = false;
+};
+template <> struct StageTile<float> {
+    static constexpr int TX = 32, TY = 14, NT = 544, MINB = 2;
+    static constexpr bool SPLIT = false;
+};
 
-template <class T, int TX_, int TY_> struct StageGeomT {
+template <class T, int TX_, int TY_, int NT_ = TX_ * TY_, bool SPLIT_ = false> struct StageGeomT {
     static constexpr int TX = TX_, TY = TY_, HALO = 2;
     static constexpr int RX = TX + 2 * HALO, RY = TY + 2 * HALO, RR = RX * RY;
-    static constexpr int NT = TX * TY;
+    static constexpr int NT = NT_;        // threads
+    static constexpr int NC = TX * TY;    // cells
+    static constexpr bool SPLIT = SPLIT_;
+    static_assert(NT >= NC && NT % 32 == 0, "one thread per cell in the update phase, whole warps");
     static constexpr int NFX = (TX + 1) * (TY + 2);  // x faces: TX+1 per row, rows -1..TY
     static constexpr int NGY = (TX + 2) * (TY + 1);  // y faces: cols -1..TX, TY+1 per col
     static constexpr int NE = (TX + 1) * (TY + 1);   // edges
     static constexpr int NSL = (TX + 2) * (TY + 2);  // cells whose slopes a face needs
-    // prims (8 RR) + slopes (7 NSL) + x fluxes (7 NFX) + y fluxes (7 NGY) + Ez + own state (6 NT)
-    static constexpr size_t smem = sizeof(T) * (size_t)(8 * RR + 7 * NSL + 7 * NFX + 7 * NGY + NE + 6 * NT);
+    static constexpr int NSB = SPLIT ? 2 : 1;         // slope buffers
+    // prims (8 RR) + slopes (7 NSL each) + x fluxes (7 NFX) + y fluxes (7 NGY) + Ez + own state (6 NC)
+    static constexpr size_t smem = sizeof(T) * (size_t)(8 * RR + 7 * NSB * NSL + 7 * NFX + 7 * NGY + NE + 6 * NC);
 };
 
-template <class T> using StageGeom = StageGeomT<T, StageTile<T>::TX, StageTile<T>::TY>;
+template <class T>
+using StageGeom = StageGeomT<T, StageTile<T>::TX, StageTile<T>::TY, StageTile<T>::NT, StageTile<T>::SPLIT>;
 template <class T> constexpr size_t m2_stage_smem() { return StageGeom<T>::smem; }
 
 // Joule heating, explicit Bz diffusion and floors of one cell
@@ -86,21 +107,24 @@ __device__ __forceinline__ void joule_cell(const M2Const<T>& c, const Fields<T>&
 // ---------------------------------------------------------------------------
 // REC: also store the updated cell state before its floors (rho, mx, my, mz,
 // E, Bz into rec[0..5], pitched like the state): the record the discrete
-// adjoint replays the floor and gravity-kick branches from.
-template <class T, int TX_, int TY_, bool DEFER, int GMODE, bool REC = false>
+// adjoint replays the floor and gravity-kick branches from.  NT_: threads of
+// the CTA (at least TX * TY); SPLIT_ as in StageGeomT.
+template <class T, int TX_, int TY_, bool DEFER, int GMODE, bool REC = false, int NT_ = TX_ * TY_,
+          bool SPLIT_ = false>
 __device__ __forceinline__ void m2_stage_tile(const M2Const<T>& c, const Fields<T>& in, const Fields<T>& out,
                                               const T* __restrict__ ga, const T* __restrict__ gb, const T dt,
                                               const int i0, const int j0, T* sm, T* const* rec = nullptr) {
-    using G = StageGeomT<T, TX_, TY_>;
-    constexpr int TX = G::TX, TY = G::TY, HALO = G::HALO, RX = G::RX, RR = G::RR, NT = G::NT;
+    using G = StageGeomT<T, TX_, TY_, NT_, SPLIT_>;
+    constexpr int TX = G::TX, TY = G::TY, HALO = G::HALO, RX = G::RX, RR = G::RR, NT = G::NT, NC = G::NC;
     constexpr int NFX = G::NFX, NGY = G::NGY, NSL = G::NSL;
     T* s_r = sm;          T* s_u = s_r + RR;   T* s_v = s_u + RR;   T* s_w = s_v + RR;
     T* s_P = s_w + RR;    T* s_bx = s_P + RR;  T* s_by = s_bx + RR; T* s_bz = s_by + RR;
-    T* sl = s_bz + RR;          // 7 planes of NSL: slopes of cells (-1..TX) x (-1..TY), x then y
-    T* fx = sl + 7 * NSL;       // 7 planes of NFX
+    T* slx = s_bz + RR;         // 7 planes of NSL: slopes of cells (-1..TX) x (-1..TY), x direction
+    T* sly = slx + 7 * (G::NSB - 1) * NSL;   // y direction (the same buffer, reused, unless SPLIT)
+    T* fx = sly + 7 * NSL;      // 7 planes of NFX
     T* gy = fx + 7 * NFX;       // 7 planes of NGY
     T* ez = gy + 7 * NGY;       // NE
-    T* own = ez + G::NE;        // 6 planes of NT
+    T* own = ez + G::NE;        // 6 planes of NC
 
     const int tid = threadIdx.x;
     const int P = c.pitch;
@@ -121,8 +145,8 @@ __device__ __forceinline__ void m2_stage_tile(const M2Const<T>& c, const Fields<
         const int ox = rx - HALO, oy = ry - HALO;
         if (ox >= 0 && ox < TX && oy >= 0 && oy < TY) {
             const int o = oy * TX + ox;
-            own[o] = rho; own[NT + o] = mx; own[2 * NT + o] = my;
-            own[3 * NT + o] = mz; own[4 * NT + o] = E; own[5 * NT + o] = Bz;
+            own[o] = rho; own[NC + o] = mx; own[2 * NC + o] = my;
+            own[3 * NC + o] = mz; own[4 * NC + o] = E; own[5 * NC + o] = Bz;
         }
     }
     __syncthreads();
@@ -134,6 +158,7 @@ __device__ __forceinline__ void m2_stage_tile(const M2Const<T>& c, const Fields<
     // MC slopes of one cell along stride st (recon_x / recon_y, M2:295-303, 319-327);
     // component 5 is the transverse in-plane B (By for x, Bx for y)
     auto slopes = [&](int k, int st, bool ydir, int o) {
+        T* sl = ydir ? sly : slx;
         sl[o] = mc_slope(s_r[k - st], s_r[k], s_r[k + st]);
         sl[NSL + o] = mc_slope(s_u[k - st], s_u[k], s_u[k + st]);
         sl[2 * NSL + o] = mc_slope(s_v[k - st], s_v[k], s_v[k + st]);
@@ -145,6 +170,7 @@ __device__ __forceinline__ void m2_stage_tile(const M2Const<T>& c, const Fields<
     };
     // face state of a cell: centre value + side * 0.5 * slope, then floors (M2:305-311)
     auto face_state = [&](int k, int o, bool ydir, T side) {
+        const T* sl = ydir ? sly : slx;
         Prim<T> W;
         const T h = T(0.5) * side;
         W.r = s_r[k] + h * sl[o];
@@ -160,42 +186,62 @@ __device__ __forceinline__ void m2_stage_tile(const M2Const<T>& c, const Fields<
         return W;
     };
 
-    // ---- B: x slopes, then x-face fluxes: faces i0..i0+TX, rows j0-1..j0+TY (M2:706-725) ----
-    for (int k = tid; k < NSL; k += NT) {
+    auto x_slopes = [&](int k) {
         const int lx = k % (TX + 2) - 1, ly = k / (TX + 2) - 1;
         slopes(ridx(lx, ly), 1, false, k);
-    }
-    __syncthreads();
-    for (int k = tid; k < NFX; k += NT) {
+    };
+    auto y_slopes = [&](int k) {
+        const int lx = k % (TX + 2) - 1, ly = k / (TX + 2) - 1;
+        slopes(ridx(lx, ly), RX, true, k);
+    };
+    // x faces i0..i0+TX, rows j0-1..j0+TY (M2:706-725)
+    auto x_face = [&](int k) {
         const int f = k % (TX + 1), r = k / (TX + 1) - 1;
         const int gi = i0 + f;
-        if (gi > c.nx) continue;
+        if (gi > c.nx) return;
         const int cj = c.ay.cell(j0 + r);
         const Prim<T> WL = face_state(ridx(f - 1, r), sidx(f - 1, r), false, T(1));
         const Prim<T> WR = face_state(ridx(f, r), sidx(f, r), false, T(-1));
         const Flux<T> F = hlld_x(c, WL, WR, in.bx[(size_t)cj * P + gi]);
         fx[k] = F.f0; fx[NFX + k] = F.f1; fx[2 * NFX + k] = F.f2; fx[3 * NFX + k] = F.f3;
         fx[4 * NFX + k] = F.f4; fx[5 * NFX + k] = F.f5; fx[6 * NFX + k] = F.f6;
-    }
-    __syncthreads();
-    // ---- C: y slopes, then y-face fluxes: y faces j0..j0+TY, columns i0-1..i0+TX (M2:728-747) ----
-    for (int k = tid; k < NSL; k += NT) {
-        const int lx = k % (TX + 2) - 1, ly = k / (TX + 2) - 1;
-        slopes(ridx(lx, ly), RX, true, k);
-    }
-    __syncthreads();
-    for (int k = tid; k < NGY; k += NT) {
+    };
+    // y faces j0..j0+TY, columns i0-1..i0+TX (M2:728-747)
+    auto y_face = [&](int k) {
         const int col = k % (TX + 2) - 1, g = k / (TX + 2);
         const int gj = j0 + g;
-        if (gj > c.ny) continue;
+        if (gj > c.ny) return;
         const int ci = c.ax.cell(i0 + col);
         const Prim<T> WL = face_state(ridx(col, g - 1), sidx(col, g - 1), true, T(1));
         const Prim<T> WR = face_state(ridx(col, g), sidx(col, g), true, T(-1));
         const Flux<T> Gf = hlld_y(c, WL, WR, in.by[(size_t)gj * P + ci]);
         gy[k] = Gf.f0; gy[NGY + k] = Gf.f1; gy[2 * NGY + k] = Gf.f2; gy[3 * NGY + k] = Gf.f3;
         gy[4 * NGY + k] = Gf.f4; gy[5 * NGY + k] = Gf.f5; gy[6 * NGY + k] = Gf.f6;
+    };
+    if constexpr (G::SPLIT) {
+        // ---- B: x and y slopes; C: x and y face fluxes (ranges padded to whole warps) ----
+        constexpr int NSLP = (NSL + 31) / 32 * 32, NFXP = (NFX + 31) / 32 * 32;
+        for (int k = tid; k < NSLP + NSL; k += NT) {
+            if (k < NSL) x_slopes(k);
+            else if (k >= NSLP) y_slopes(k - NSLP);
+        }
+        __syncthreads();
+        for (int k = tid; k < NFXP + NGY; k += NT) {
+            if (k < NFX) x_face(k);
+            else if (k >= NFXP) y_face(k - NFXP);
+        }
+        __syncthreads();
+    } else {
+        // ---- B: x slopes, then x faces; C: y slopes (same buffer), then y faces ----
+        for (int k = tid; k < NSL; k += NT) x_slopes(k);
+        __syncthreads();
+        for (int k = tid; k < NFX; k += NT) x_face(k);
+        __syncthreads();
+        for (int k = tid; k < NSL; k += NT) y_slopes(k);
+        __syncthreads();
+        for (int k = tid; k < NGY; k += NT) y_face(k);
+        __syncthreads();
     }
-    __syncthreads();
 
     // ---- E: edge EMFs, edges i0..i0+TX x j0..j0+TY (M2:782-804, 565-575) ----
     for (int k = tid; k < G::NE; k += NT) {
@@ -220,13 +266,14 @@ __device__ __forceinline__ void m2_stage_tile(const M2Const<T>& c, const Fields<
     __syncthreads();
 
     // ---- D+F: FV update, floors, CT, gravity kick, store (M2:750-779, 807-832) ----
+    if (tid >= NC) return;
     const int tx = tid % TX, ty = tid / TX;
     const int gi = i0 + tx, gj = j0 + ty;
     if (gi >= c.nx || gj >= c.ny) return;
     const size_t q = (size_t)gj * P + gi;
     const int o = ty * TX + tx;
-    T rho = own[o], mx = own[NT + o], my = own[2 * NT + o];
-    T mz = own[3 * NT + o], E = own[4 * NT + o], Bz = own[5 * NT + o];
+    T rho = own[o], mx = own[NC + o], my = own[2 * NC + o];
+    T mz = own[3 * NC + o], E = own[4 * NC + o], Bz = own[5 * NC + o];
     {
         const int kxL = (ty + 1) * (TX + 1) + tx;
         const int kgD = ty * (TX + 2) + tx + 1, kgU = kgD + (TX + 2);
@@ -289,8 +336,8 @@ m2_stage_kernel(const M2Const<T> c, const Fields<T> in, const Fields<T> out, con
     constexpr int TX = StageTile<T>::TX, TY = StageTile<T>::TY;
     if (active && *active == 0) return;
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    m2_stage_tile<T, TX, TY, DEFER, GMODE>(c, in, out, ga, gb, (T)(*dtp), blockIdx.x * TX, blockIdx.y * TY,
-                                           reinterpret_cast<T*>(smem_raw));
+    m2_stage_tile<T, TX, TY, DEFER, GMODE, false, StageTile<T>::NT, StageTile<T>::SPLIT>(
+        c, in, out, ga, gb, (T)(*dtp), blockIdx.x * TX, blockIdx.y * TY, reinterpret_cast<T*>(smem_raw));
 }
 
 // ---------------------------------------------------------------------------
