@@ -10,6 +10,7 @@
 // Three pitched state buffers rotate (U^n, S1, S2); dt, t and the "active"
 // flag (t < t_end) live on the device, so a run of steps needs no host sync
 // and is captured as a CUDA graph (three steps = one buffer rotation).
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -31,6 +32,18 @@ int ilog2(int n) { int l = 0; while ((1 << l) < n) ++l; return l; }
 // Twiddles of every radix-2 pass of an n-point transform by the reference's
 // recurrence w_{j+1} = w_j * wlen (navier_stokes_2d_hllc_poisson.cpp:160-171),
 // pass with half-length h stored at [h-1, 2h-1).
+// n-th roots of unity W^e = (cos 2 pi e / n, -sin 2 pi e / n), e < n, for the
+// FP32 spectral solve (evaluated in FP64, then rounded)
+std::vector<float> fft32_roots(int n) {
+    std::vector<float> t(2 * (size_t)n);
+    for (int e = 0; e < n; e++) {
+        const double ang = 2.0 * M_PI * (double)e / (double)n;
+        t[2 * (size_t)e] = (float)std::cos(ang);
+        t[2 * (size_t)e + 1] = (float)-std::sin(ang);
+    }
+    return t;
+}
+
 std::vector<double> twiddle_table(int n, bool inverse) {
     std::vector<double> t(2 * (size_t)(n > 1 ? n - 1 : 1), 0.0);
     for (int len = 2; len <= n; len <<= 1) {
@@ -76,7 +89,8 @@ template <class T> struct Mhd2d : Mhd2dBase {
     T* gxa = nullptr;
     T* gya = nullptr;
     Cplx<T>* fftA = nullptr;
-    Cplx<T>* tw[4] = {nullptr, nullptr, nullptr, nullptr};  // x fwd, x inv, y fwd, y inv
+    // FP64: twiddles x fwd, x inv, y fwd, y inv; FP32: roots of nx in tw[0], of ny in tw[2]
+    Cplx<T>* tw[4] = {nullptr, nullptr, nullptr, nullptr};
     double* rhs = nullptr;
     double* sphi = nullptr;
     double* scal = nullptr;   // small device scalars
@@ -165,13 +179,27 @@ template <class T> struct Mhd2d : Mhd2dBase {
                     return fail(h, CC_ERR_UNSUPPORTED, "FFT Poisson needs power-of-two Nx, Ny >= 4");
                 if ((size_t)nx * sizeof(Cplx<T>) > 200 * 1024 || (size_t)ny * sizeof(Cplx<T>) * (sizeof(T) == 8 ? 2 : 4) > 200 * 1024)
                     return fail(h, CC_ERR_UNSUPPORTED, "FFT line does not fit in shared memory");
-                CC_CUDA(cudaMalloc(&fftA, sizeof(Cplx<T>) * (size_t)nx * ny));
-                const int ns[4] = {nx, nx, ny, ny};
-                for (int k = 0; k < 4; k++) {
-                    std::vector<double> t = twiddle_table(ns[k], k & 1);
-                    std::vector<T> tt(t.begin(), t.end());
-                    CC_CUDA(cudaMalloc(&tw[k], sizeof(T) * tt.size()));
-                    CC_CUDA(cudaMemcpyAsync(tw[k], tt.data(), sizeof(T) * tt.size(), cudaMemcpyHostToDevice, st()));
+                if (sizeof(T) == 4 && (nx > FFT32_MAXN || ny > FFT32_MAXN))
+                    return fail(h, CC_ERR_UNSUPPORTED, "FP32 FFT Poisson supports Nx, Ny <= 8192");
+                if constexpr (sizeof(T) == 4) {
+                    // FP32: half-spectrum work array, root tables of nx and ny in tw[0], tw[2]
+                    const size_t w = (size_t)std::max(nx, fft32_half_pitch(nx));
+                    CC_CUDA(cudaMalloc(&fftA, sizeof(Cplx<T>) * w * ny));
+                    const int ns[2] = {nx, ny};
+                    for (int k = 0; k < 2; k++) {
+                        const std::vector<float> t = fft32_roots(ns[k]);
+                        CC_CUDA(cudaMalloc(&tw[2 * k], sizeof(float) * t.size()));
+                        CC_CUDA(cudaMemcpyAsync(tw[2 * k], t.data(), sizeof(float) * t.size(), cudaMemcpyHostToDevice, st()));
+                    }
+                } else {
+                    CC_CUDA(cudaMalloc(&fftA, sizeof(Cplx<T>) * (size_t)nx * ny));
+                    const int ns[4] = {nx, nx, ny, ny};
+                    for (int k = 0; k < 4; k++) {
+                        std::vector<double> t = twiddle_table(ns[k], k & 1);
+                        std::vector<T> tt(t.begin(), t.end());
+                        CC_CUDA(cudaMalloc(&tw[k], sizeof(T) * tt.size()));
+                        CC_CUDA(cudaMemcpyAsync(tw[k], tt.data(), sizeof(T) * tt.size(), cudaMemcpyHostToDevice, st()));
+                    }
                 }
             } else if (p.poisson_kind == CC_POISSON_SOR) {
                 if ((p.periodic_x && (nx & 1)) || (p.periodic_y && (ny & 1)))
@@ -247,8 +275,13 @@ template <class T> struct Mhd2d : Mhd2dBase {
         h->perf.poisson_solves += 1;
         const int nx = p.Nx, ny = p.Ny;
         if (p.poisson_kind == CC_POISSON_FFT) {
-            CC_CUDA(M2Launch<T>::fft_solve(rho, P, rho_part, nx, ny, ilog2(nx), ilog2(ny), tw[0], tw[1], tw[2], tw[3],
-                                           p.x1 - p.x0, p.y1 - p.y0, p.G, fftA, phi, active(), st()));
+            if constexpr (sizeof(T) == 4)
+                CC_CUDA(M2Launch<T>::fft32_solve(rho, P, rho_part, nx, ny, reinterpret_cast<const float2*>(tw[0]),
+                                                 reinterpret_cast<const float2*>(tw[2]), p.x1 - p.x0, p.y1 - p.y0,
+                                                 p.G, reinterpret_cast<float2*>(fftA), phi, active(), st()));
+            else
+                CC_CUDA(M2Launch<T>::fft_solve(rho, P, rho_part, nx, ny, ilog2(nx), ilog2(ny), tw[0], tw[1], tw[2],
+                                               tw[3], p.x1 - p.x0, p.y1 - p.y0, p.G, fftA, phi, active(), st()));
             count(3);
         } else {
             CC_CUDA(M2Launch<T>::sor_rhs(rho, nx, ny, P, rho_part, 4.0 * M_PI * p.G, -1.0, rhs, active(), st()));

@@ -1,0 +1,249 @@
+// FP32 spectral Poisson solve (the bulk path of the periodic FFT gravity).
+//
+// Same three passes and the same spectral kernel as the FP64 solve in
+// poisson_kernels.cuh (navier_stokes_2d_hllc_poisson.cpp:285-328), arranged
+// for throughput; the differences change only the rounding:
+//   * real-to-complex: rows are real, so two rows ride in one complex
+//     transform (z = row_a + i row_b) and only the half spectrum kx = 0..nx/2
+//     is stored (row pitch nhp = fft32_half_pitch(nx)); the column pass works
+//     on nx/2 + 1 columns, the inverse row pass rebuilds the other half from
+//     Hermitian symmetry.  Half the transforms and half the work-array traffic.
+//   * Stockham autosort transforms: radix-16 passes (then one radix 8, 4 or 2
+//     pass), 16 values per thread in registers, in-place in shared memory with
+//     a barrier between the reads and the writes of a pass, so no bit-reversal
+//     pass; log16(n) passes instead of log2(n).  Twiddles from a table of the
+//     n-th roots W_n^e = exp(-2 pi i e / n) evaluated in FP64 on the host.
+//   * shared-memory lines padded by one element per 16 so that the stride-16
+//     writes of the first pass hit distinct banks.
+#pragma once
+#include <cuda_runtime.h>
+
+namespace ccb {
+
+// threads per CTA at most (n / 16 per line): lines of up to 8192 points
+constexpr int FFT32_MAXT = 512;
+constexpr int FFT32_MAXN = 16 * FFT32_MAXT;
+
+// row pitch (complex elements) of the half-spectrum work array
+__host__ __device__ constexpr int fft32_half_pitch(int nx) { return ((nx / 2 + 1) + 15) / 16 * 16; }
+__host__ __device__ constexpr int fft32_pad(int i) { return i + (i >> 4); }
+__host__ __device__ constexpr int fft32_line(int n) { return fft32_pad(n - 1) + 1; }   // padded line length
+// values per thread (16, or n below 16) and threads per line
+__host__ __device__ constexpr int fft32_vals(int n) { return n < 16 ? n : 16; }
+__host__ __device__ constexpr int fft32_tpl(int n) { return n / fft32_vals(n); }
+
+__device__ __forceinline__ float2 f2add(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ float2 f2sub(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
+// x * w (forward) or x * conj(w) (inverse)
+template <bool INV> __device__ __forceinline__ float2 f2twiddle(float2 x, float2 w) {
+    if (INV) return make_float2(x.x * w.x + x.y * w.y, x.y * w.x - x.x * w.y);
+    return make_float2(x.x * w.x - x.y * w.y, x.x * w.y + x.y * w.x);
+}
+
+// x * W_16^e (forward, W_16 = exp(-2 pi i / 16)) or x * W_16^-e (inverse), e in [0, 8)
+template <bool INV> __device__ __forceinline__ float2 f2w16(float2 x, int e) {
+    constexpr float C[8] = {1.0f, 0.92387953251128674f, 0.70710678118654752f, 0.38268343236508977f,
+                            0.0f, -0.38268343236508977f, -0.70710678118654752f, -0.92387953251128674f};
+    constexpr float S[8] = {0.0f, 0.38268343236508977f, 0.70710678118654752f, 0.92387953251128674f,
+                            1.0f, 0.92387953251128674f, 0.70710678118654752f, 0.38268343236508977f};
+    if (e == 0) return x;
+    if (e == 4) return INV ? make_float2(-x.y, x.x) : make_float2(x.y, -x.x);   // * (+i) or * (-i)
+    return f2twiddle<INV>(x, make_float2(C[e], -S[e]));
+}
+
+// R-point DFT (R = 2, 4, 8, 16) of v[0..R) in registers, natural order in and
+// out: bit-reversal permutation, then radix-2 butterflies (every index is a
+// compile-time constant once the loops are unrolled).
+template <int R, bool INV> __device__ __forceinline__ void f32_dft(float2* v) {
+    constexpr int LR = R == 2 ? 1 : R == 4 ? 2 : R == 8 ? 3 : 4;
+#pragma unroll
+    for (int i = 0; i < R; i++) {
+        int j = 0;
+#pragma unroll
+        for (int b = 0; b < LR; b++) j |= ((i >> b) & 1) << (LR - 1 - b);
+        if (i < j) { const float2 t = v[i]; v[i] = v[j]; v[j] = t; }
+    }
+#pragma unroll
+    for (int h = 1; h < R; h <<= 1) {
+#pragma unroll
+        for (int i = 0; i < R; i += 2 * h) {
+#pragma unroll
+            for (int k = 0; k < h; k++) {
+                const float2 a = v[i + k];
+                const float2 b = f2w16<INV>(v[i + k + h], k * (8 / h));
+                v[i + k] = f2add(a, b);
+                v[i + k + h] = f2sub(a, b);
+            }
+        }
+    }
+}
+
+// One radix-R Stockham pass over a line of n values (padded layout), sub-
+// transform length Ns before the pass.  tl threads per line (lt its thread,
+// act false for the idle threads of a rounded-up block), each with V / R
+// butterflies.  Contains two barriers: every thread of the CTA calls it.
+template <int R, int V, bool INV>
+__device__ __forceinline__ void f32_pass(float2* a, int n, int Ns, const float2* __restrict__ roots, int lt, int tl,
+                                         bool act) {
+    constexpr int G = V / R;
+    const int nb = n / R;
+    float2 v[V];
+    if (act) {
+#pragma unroll
+        for (int g = 0; g < G; g++) {
+            const int j = lt + g * tl;
+#pragma unroll
+            for (int r = 0; r < R; r++) v[g * R + r] = a[fft32_pad(j + r * nb)];
+        }
+    }
+    __syncthreads();
+    if (act) {
+        const int span = n / (Ns * R);
+#pragma unroll
+        for (int g = 0; g < G; g++) {
+            const int j = lt + g * tl;
+            const int k = j & (Ns - 1);
+            if (Ns > 1) {
+#pragma unroll
+                for (int r = 1; r < R; r++) v[g * R + r] = f2twiddle<INV>(v[g * R + r], __ldg(&roots[r * k * span]));
+            }
+            f32_dft<R, INV>(&v[g * R]);
+            const int base = (j - k) * R + k;
+#pragma unroll
+            for (int s = 0; s < R; s++) a[fft32_pad(base + s * Ns)] = v[g * R + s];
+        }
+    }
+    __syncthreads();
+}
+
+// Whole transform of one line (unnormalised); uniform over the CTA.
+template <bool INV>
+__device__ __forceinline__ void f32_fft_line(float2* a, int n, const float2* __restrict__ roots, int lt, bool act) {
+    const int tl = fft32_tpl(n);
+    if (n >= 16) {
+        int Ns = 1;
+        while (n / Ns >= 16) {
+            f32_pass<16, 16, INV>(a, n, Ns, roots, lt, tl, act);
+            Ns *= 16;
+        }
+        const int rem = n / Ns;
+        if (rem == 8) f32_pass<8, 16, INV>(a, n, Ns, roots, lt, tl, act);
+        else if (rem == 4) f32_pass<4, 16, INV>(a, n, Ns, roots, lt, tl, act);
+        else if (rem == 2) f32_pass<2, 16, INV>(a, n, Ns, roots, lt, tl, act);
+    } else if (n == 8) {
+        f32_pass<8, 8, INV>(a, n, 1, roots, lt, tl, act);
+    } else if (n == 4) {
+        f32_pass<4, 4, INV>(a, n, 1, roots, lt, tl, act);
+    } else if (n == 2) {
+        f32_pass<2, 2, INV>(a, n, 1, roots, lt, tl, act);
+    }
+}
+
+// pass 1: rows 2b and 2b+1 -> half spectra.  rho pitched; mean = sum/N.
+template <class F>   // F = float (a template so that only the FP32 unit instantiates it)
+__global__ void __launch_bounds__(FFT32_MAXT)
+f32_rows_fwd_kernel(const F* __restrict__ rho, int pitch, const double* __restrict__ rho_part, int nparts,
+                    double ncell, float2* __restrict__ A, int nx, int nhp, const float2* __restrict__ roots,
+                    const int* __restrict__ active) {
+    if (active && *active == 0) return;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    float2* a = reinterpret_cast<float2*>(smem_raw);
+    __shared__ double s_mean;
+    if (threadIdx.x == 0) {
+        double s = 0.0;
+        for (int b = 0; b < nparts; b++) s += rho_part[b];
+        s_mean = s / ncell;
+    }
+    __syncthreads();
+    const float mean = (float)s_mean;
+    const int ja = 2 * blockIdx.x, jb = ja + 1;
+    for (int i = threadIdx.x; i < nx; i += blockDim.x)
+        a[fft32_pad(i)] = make_float2(rho[(size_t)ja * pitch + i] - mean, rho[(size_t)jb * pitch + i] - mean);
+    __syncthreads();
+    const int tl = fft32_tpl(nx);
+    f32_fft_line<false>(a, nx, roots, (int)threadIdx.x, (int)threadIdx.x < tl);
+    // Z = FFT(x_a + i x_b):  X_a[k] = (Z[k] + conj Z[-k]) / 2,  X_b[k] = (Z[k] - conj Z[-k]) / (2 i)
+    for (int k = threadIdx.x; k <= nx / 2; k += blockDim.x) {
+        const float2 z = a[fft32_pad(k)], m = a[fft32_pad((nx - k) & (nx - 1))];
+        A[(size_t)ja * nhp + k] = make_float2(0.5f * (z.x + m.x), 0.5f * (z.y - m.y));
+        A[(size_t)jb * nhp + k] = make_float2(0.5f * (z.y + m.y), 0.5f * (m.x - z.x));
+    }
+}
+
+// pass 2: CW columns kx = c0 .. c0+CW-1 (those <= nx/2): forward FFT along y,
+// spectral kernel, inverse FFT along y, 1/ny.
+template <int CW>
+__global__ void __launch_bounds__(FFT32_MAXT)
+f32_cols_solve_kernel(float2* __restrict__ A, int nx, int ny, int nhp, const float2* __restrict__ roots, double Lx,
+                      double Ly, double G, const int* __restrict__ active) {
+    if (active && *active == 0) return;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    float2* a = reinterpret_cast<float2*>(smem_raw);
+    const int LP = fft32_line(ny);
+    const int c0 = blockIdx.x * CW;
+    const int ncol = nx / 2 + 1;
+    for (int k = threadIdx.x; k < CW * ny; k += blockDim.x) {
+        const int cc = k % CW, j = k / CW;
+        a[cc * LP + fft32_pad(j)] = (c0 + cc < ncol) ? A[(size_t)j * nhp + c0 + cc] : make_float2(0.0f, 0.0f);
+    }
+    __syncthreads();
+    const int tl = fft32_tpl(ny);
+    const int l = (int)threadIdx.x / tl, lt = (int)threadIdx.x % tl;
+    const bool act = l < CW;
+    float2* line = a + (act ? l : 0) * LP;
+    f32_fft_line<false>(line, ny, roots, lt, act);
+    // spectral kernel (NS:308-322), continuous |k|^2, zero mode removed
+    const double two_pi = 2.0 * M_PI;
+    for (int k = threadIdx.x; k < CW * ny; k += blockDim.x) {
+        const int cc = k / ny, j = k % ny, i = c0 + cc;
+        const int nj = (j <= ny / 2) ? j : j - ny;
+        const double ky = two_pi * (double)nj / Ly;
+        const double kx = two_pi * (double)i / Lx;
+        const double k2 = kx * kx + ky * ky;
+        float2& z = a[cc * LP + fft32_pad(j)];
+        if (k2 == 0.0) {
+            z = make_float2(0.0f, 0.0f);
+        } else {
+            const float s = (float)(-(4.0 * M_PI * G) / k2);
+            z.x = z.x * s;
+            z.y = z.y * s;
+        }
+    }
+    __syncthreads();
+    f32_fft_line<true>(line, ny, roots, lt, act);
+    const float n = (float)ny;
+    for (int k = threadIdx.x; k < CW * ny; k += blockDim.x) {
+        const int cc = k % CW, j = k / CW;
+        if (c0 + cc >= ncol) continue;
+        const float2 z = a[cc * LP + fft32_pad(j)];
+        A[(size_t)j * nhp + c0 + cc] = make_float2(z.x / n, z.y / n);
+    }
+}
+
+// pass 3: half spectra of rows 2b, 2b+1 -> Z = X_a + i X_b over all kx
+// (Hermitian completion), inverse FFT, phi_a = Re / nx, phi_b = Im / nx.
+template <class F>   // F = float (a template so that only the FP32 unit instantiates it)
+__global__ void __launch_bounds__(FFT32_MAXT)
+f32_rows_inv_kernel(const float2* __restrict__ A, int nx, int nhp, const float2* __restrict__ roots,
+                    F* __restrict__ phi, int pitch, const int* __restrict__ active) {
+    if (active && *active == 0) return;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    float2* a = reinterpret_cast<float2*>(smem_raw);
+    const int ja = 2 * blockIdx.x, jb = ja + 1;
+    for (int k = threadIdx.x; k <= nx / 2; k += blockDim.x) {
+        const float2 xa = A[(size_t)ja * nhp + k], xb = A[(size_t)jb * nhp + k];
+        a[fft32_pad(k)] = make_float2(xa.x - xb.y, xa.y + xb.x);
+        if (k > 0 && k < nx / 2) a[fft32_pad(nx - k)] = make_float2(xa.x + xb.y, xb.x - xa.y);
+    }
+    __syncthreads();
+    const int tl = fft32_tpl(nx);
+    f32_fft_line<true>(a, nx, roots, (int)threadIdx.x, (int)threadIdx.x < tl);
+    const float n = (float)nx;
+    for (int i = threadIdx.x; i < nx; i += blockDim.x) {
+        const float2 z = a[fft32_pad(i)];
+        phi[(size_t)ja * pitch + i] = z.x / n;
+        phi[(size_t)jb * pitch + i] = z.y / n;
+    }
+}
+
+}  // namespace ccb

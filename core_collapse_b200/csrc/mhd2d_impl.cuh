@@ -5,6 +5,17 @@
 namespace ccb {
 
 namespace {
+// columns per CTA of the FP32 column pass: at most FFT32_MAXT threads and
+// 72 KB of lines (three CTAs per SM)
+inline int fft32_cw(int ny) {
+    const int tl = fft32_tpl(ny);
+    const size_t line = sizeof(float2) * (size_t)fft32_line(ny);
+    int cw = 16;
+    while (cw > 1 && (cw * tl > FFT32_MAXT || cw * line > 72 * 1024)) cw >>= 1;
+    return cw;
+}
+inline int round32(int t) { return (t + 31) / 32 * 32; }
+
 inline int grid_for(size_t n, int nt, int cap) {
     size_t g = (n + nt - 1) / nt;
     if (g < 1) g = 1;
@@ -26,6 +37,21 @@ cudaError_t M2Launch<T>::prepare(int nx, int ny) {
     CC_ATTR((m2_stage_kernel<T, true, GRAV_NONE>), smem)
     CC_ATTR((m2_stage_kernel<T, true, GRAV_ARRAYS>), smem)
     CC_ATTR((m2_stage_kernel<T, true, GRAV_PHI>), smem)
+    if constexpr (sizeof(T) == 4) {
+        if (nx >= 2 && ny >= 2) {
+            const int row = (int)(sizeof(float2) * (size_t)fft32_line(nx));
+            const int col = (int)(sizeof(float2) * (size_t)fft32_line(ny)) * fft32_cw(ny);
+            if (row <= 227 * 1024 && col <= 227 * 1024) {
+                CC_ATTR(f32_rows_fwd_kernel<T>, row)
+                CC_ATTR(f32_rows_inv_kernel<T>, row)
+                CC_ATTR(f32_cols_solve_kernel<1>, col)
+                CC_ATTR(f32_cols_solve_kernel<2>, col)
+                CC_ATTR(f32_cols_solve_kernel<4>, col)
+                CC_ATTR(f32_cols_solve_kernel<8>, col)
+                CC_ATTR(f32_cols_solve_kernel<16>, col)
+            }
+        }
+    }
     constexpr int CW = (sizeof(T) == 8) ? 2 : 4;
     const int smem_row = (int)(sizeof(Cplx<T>) * (size_t)nx);
     const int smem_col = (int)(sizeof(Cplx<T>) * (size_t)ny * CW);
@@ -116,6 +142,37 @@ cudaError_t M2Launch<T>::fft_solve(const T* rho, int pitch, const double* rho_pa
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
     fft_rows_inv_kernel<T><<<ny, nt_row, smem_row, s>>>(A, nx, lognx, twx_i, phi, pitch, active);
     return cudaGetLastError();
+}
+
+template <class T>
+cudaError_t M2Launch<T>::fft32_solve(const T* rho, int pitch, const double* rho_part, int nx, int ny,
+                                     const float2* rootx, const float2* rooty, double Lx, double Ly, double G,
+                                     float2* A, T* phi, const int* active, cudaStream_t s) {
+    if constexpr (sizeof(T) != 4) {
+        return cudaErrorNotSupported;
+    } else {
+        if (nx > FFT32_MAXN || ny > FFT32_MAXN || nx < 2 || ny < 2) return cudaErrorInvalidValue;
+        const int nhp = fft32_half_pitch(nx);
+        const size_t row = sizeof(float2) * (size_t)fft32_line(nx);
+        const int cw = fft32_cw(ny);
+        const size_t col = sizeof(float2) * (size_t)fft32_line(ny) * cw;
+        cudaError_t e;
+        f32_rows_fwd_kernel<T><<<ny / 2, round32(fft32_tpl(nx)), row, s>>>(rho, pitch, rho_part, RED_BLOCKS,
+                                                                        (double)nx * (double)ny, A, nx, nhp,
+                                                                        rootx, active);
+        if ((e = cudaGetLastError()) != cudaSuccess) return e;
+        const int nt = round32(cw * fft32_tpl(ny)), nb = nhp / cw;
+        switch (cw) {
+            case 16: f32_cols_solve_kernel<16><<<nb, nt, col, s>>>(A, nx, ny, nhp, rooty, Lx, Ly, G, active); break;
+            case 8: f32_cols_solve_kernel<8><<<nb, nt, col, s>>>(A, nx, ny, nhp, rooty, Lx, Ly, G, active); break;
+            case 4: f32_cols_solve_kernel<4><<<nb, nt, col, s>>>(A, nx, ny, nhp, rooty, Lx, Ly, G, active); break;
+            case 2: f32_cols_solve_kernel<2><<<nb, nt, col, s>>>(A, nx, ny, nhp, rooty, Lx, Ly, G, active); break;
+            default: f32_cols_solve_kernel<1><<<nb, nt, col, s>>>(A, nx, ny, nhp, rooty, Lx, Ly, G, active); break;
+        }
+        if ((e = cudaGetLastError()) != cudaSuccess) return e;
+        f32_rows_inv_kernel<T><<<ny / 2, round32(fft32_tpl(nx)), row, s>>>(A, nx, nhp, rootx, phi, pitch, active);
+        return cudaGetLastError();
+    }
 }
 
 template <class T>

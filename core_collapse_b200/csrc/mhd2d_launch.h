@@ -4,6 +4,7 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include "fft32_kernels.cuh"
 #include "mhd2d_kernels.cuh"
 #include "poisson_kernels.cuh"
 
@@ -31,6 +32,12 @@ template <class T> struct M2Launch {
                                  int logny, const Cplx<T>* twx_f, const Cplx<T>* twx_i, const Cplx<T>* twy_f,
                                  const Cplx<T>* twy_i, double Lx, double Ly, double G, Cplx<T>* A, T* phi,
                                  const int* active, cudaStream_t s);
+    // FP32 spectral solve (fft32_kernels.cuh), T = float only: rootx / rooty
+    // the nx-th / ny-th roots of unity W^e = (cos 2 pi e/n, -sin 2 pi e/n),
+    // A: ny x fft32_half_pitch(nx) complex work array; needs nx, ny powers of two.
+    static cudaError_t fft32_solve(const T* rho, int pitch, const double* rho_part, int nx, int ny,
+                                   const float2* rootx, const float2* rooty, double Lx, double Ly, double G,
+                                   float2* A, T* phi, const int* active, cudaStream_t s);
     static cudaError_t sor_rhs(const T* rho, int nx, int ny, int pitch, const double* rho_part, double fourpiG,
                                double floor_rho, double* rhs, const int* active, cudaStream_t s);
     static cudaError_t phi_to_field(const double* phi, int nx, int ny, T* out, int pitch, const int* active,
