@@ -10,7 +10,6 @@
 // Three pitched state buffers rotate (U^n, S1, S2); dt, t and the "active"
 // flag (t < t_end) live on the device, so a run of steps needs no host sync
 // and is captured as a CUDA graph (three steps = one buffer rotation).
-#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -182,8 +181,8 @@ template <class T> struct Mhd2d : Mhd2dBase {
                 if (sizeof(T) == 4 && (nx > FFT32_MAXN || ny > FFT32_MAXN))
                     return fail(h, CC_ERR_UNSUPPORTED, "FP32 FFT Poisson supports Nx, Ny <= 8192");
                 if constexpr (sizeof(T) == 4) {
-                    // FP32: half-spectrum work array, root tables of nx and ny in tw[0], tw[2]
-                    const size_t w = (size_t)std::max(nx, fft32_half_pitch(nx));
+                    // FP32: half-spectrum work array (kx-major), root tables of nx and ny in tw[0], tw[2]
+                    const size_t w = (size_t)fft32_half_lines(nx);
                     CC_CUDA(cudaMalloc(&fftA, sizeof(Cplx<T>) * w * ny));
                     const int ns[2] = {nx, ny};
                     for (int k = 0; k < 2; k++) {

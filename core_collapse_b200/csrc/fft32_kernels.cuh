@@ -5,9 +5,12 @@
 // for throughput; the differences change only the rounding:
 //   * real-to-complex: rows are real, so two rows ride in one complex
 //     transform (z = row_a + i row_b) and only the half spectrum kx = 0..nx/2
-//     is stored (row pitch nhp = fft32_half_pitch(nx)); the column pass works
-//     on nx/2 + 1 columns, the inverse row pass rebuilds the other half from
-//     Hermitian symmetry.  Half the transforms and half the work-array traffic.
+//     is stored; the column pass works on nx/2 + 1 columns, the inverse row
+//     pass rebuilds the other half from Hermitian symmetry.  Half the
+//     transforms and half the work-array traffic.
+//   * the work array is kx-major, A[kx * ny + y] (nhl = fft32_half_lines(nx)
+//     lines of ny), so the column pass reads and writes contiguous lines; a row
+//     pair writes / reads 16 contiguous bytes per kx.
 //   * Stockham autosort transforms: radix-16 passes (then one radix 8, 4 or 2
 //     pass), 16 values per thread in registers, in-place in shared memory with
 //     a barrier between the reads and the writes of a pass, so no bit-reversal
@@ -20,12 +23,15 @@
 
 namespace ccb {
 
-// threads per CTA at most (n / 16 per line): lines of up to 8192 points
+// threads per CTA at most (n / 16 per line): lines of up to 8192 points.  The
+// column pass asks for two such CTAs per SM (at most 64 registers), so that
+// four 256-thread CTAs (4096-point lines) are resident per SM; the row passes
+// keep their registers (fewer spills, they have the other latencies to hide).
 constexpr int FFT32_MAXT = 512;
 constexpr int FFT32_MAXN = 16 * FFT32_MAXT;
 
-// row pitch (complex elements) of the half-spectrum work array
-__host__ __device__ constexpr int fft32_half_pitch(int nx) { return ((nx / 2 + 1) + 15) / 16 * 16; }
+// kx lines of the half-spectrum work array (nx/2 + 1, rounded up to 16)
+__host__ __device__ constexpr int fft32_half_lines(int nx) { return ((nx / 2 + 1) + 15) / 16 * 16; }
 __host__ __device__ constexpr int fft32_pad(int i) { return i + (i >> 4); }
 __host__ __device__ constexpr int fft32_line(int n) { return fft32_pad(n - 1) + 1; }   // padded line length
 // values per thread (16, or n below 16) and threads per line
@@ -143,7 +149,7 @@ __device__ __forceinline__ void f32_fft_line(float2* a, int n, const float2* __r
 template <class F>   // F = float (a template so that only the FP32 unit instantiates it)
 __global__ void __launch_bounds__(FFT32_MAXT)
 f32_rows_fwd_kernel(const F* __restrict__ rho, int pitch, const double* __restrict__ rho_part, int nparts,
-                    double ncell, float2* __restrict__ A, int nx, int nhp, const float2* __restrict__ roots,
+                    double ncell, float2* __restrict__ A, int nx, int ny, const float2* __restrict__ roots,
                     const int* __restrict__ active) {
     if (active && *active == 0) return;
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -165,17 +171,17 @@ f32_rows_fwd_kernel(const F* __restrict__ rho, int pitch, const double* __restri
     // Z = FFT(x_a + i x_b):  X_a[k] = (Z[k] + conj Z[-k]) / 2,  X_b[k] = (Z[k] - conj Z[-k]) / (2 i)
     for (int k = threadIdx.x; k <= nx / 2; k += blockDim.x) {
         const float2 z = a[fft32_pad(k)], m = a[fft32_pad((nx - k) & (nx - 1))];
-        A[(size_t)ja * nhp + k] = make_float2(0.5f * (z.x + m.x), 0.5f * (z.y - m.y));
-        A[(size_t)jb * nhp + k] = make_float2(0.5f * (z.y + m.y), 0.5f * (m.x - z.x));
+        *reinterpret_cast<float4*>(A + (size_t)k * ny + ja) =
+            make_float4(0.5f * (z.x + m.x), 0.5f * (z.y - m.y), 0.5f * (z.y + m.y), 0.5f * (m.x - z.x));
     }
 }
 
 // pass 2: CW columns kx = c0 .. c0+CW-1 (those <= nx/2): forward FFT along y,
 // spectral kernel, inverse FFT along y, 1/ny.
 template <int CW>
-__global__ void __launch_bounds__(FFT32_MAXT)
-f32_cols_solve_kernel(float2* __restrict__ A, int nx, int ny, int nhp, const float2* __restrict__ roots, double Lx,
-                      double Ly, double G, const int* __restrict__ active) {
+__global__ void __launch_bounds__(FFT32_MAXT, 2)
+f32_cols_solve_kernel(float2* __restrict__ A, int nx, int ny, const float2* __restrict__ roots, double Lx, double Ly,
+                      double G, const int* __restrict__ active) {
     if (active && *active == 0) return;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     float2* a = reinterpret_cast<float2*>(smem_raw);
@@ -183,8 +189,8 @@ f32_cols_solve_kernel(float2* __restrict__ A, int nx, int ny, int nhp, const flo
     const int c0 = blockIdx.x * CW;
     const int ncol = nx / 2 + 1;
     for (int k = threadIdx.x; k < CW * ny; k += blockDim.x) {
-        const int cc = k % CW, j = k / CW;
-        a[cc * LP + fft32_pad(j)] = (c0 + cc < ncol) ? A[(size_t)j * nhp + c0 + cc] : make_float2(0.0f, 0.0f);
+        const int cc = k / ny, j = k % ny;
+        a[cc * LP + fft32_pad(j)] = (c0 + cc < ncol) ? A[(size_t)(c0 + cc) * ny + j] : make_float2(0.0f, 0.0f);
     }
     __syncthreads();
     const int tl = fft32_tpl(ny);
@@ -192,19 +198,19 @@ f32_cols_solve_kernel(float2* __restrict__ A, int nx, int ny, int nhp, const flo
     const bool act = l < CW;
     float2* line = a + (act ? l : 0) * LP;
     f32_fft_line<false>(line, ny, roots, lt, act);
-    // spectral kernel (NS:308-322), continuous |k|^2, zero mode removed
-    const double two_pi = 2.0 * M_PI;
+    // spectral kernel (NS:308-322), continuous |k|^2, zero mode removed; in
+    // FP32 here (the factor carries the FP32 solve's rounding anyway)
+    const float fy = (float)(2.0 * M_PI / Ly), fx = (float)(2.0 * M_PI / Lx), g4 = (float)(4.0 * M_PI * G);
     for (int k = threadIdx.x; k < CW * ny; k += blockDim.x) {
         const int cc = k / ny, j = k % ny, i = c0 + cc;
         const int nj = (j <= ny / 2) ? j : j - ny;
-        const double ky = two_pi * (double)nj / Ly;
-        const double kx = two_pi * (double)i / Lx;
-        const double k2 = kx * kx + ky * ky;
+        const float ky = fy * (float)nj, kx = fx * (float)i;
+        const float k2 = kx * kx + ky * ky;
         float2& z = a[cc * LP + fft32_pad(j)];
-        if (k2 == 0.0) {
+        if (k2 == 0.0f) {
             z = make_float2(0.0f, 0.0f);
         } else {
-            const float s = (float)(-(4.0 * M_PI * G) / k2);
+            const float s = -g4 / k2;
             z.x = z.x * s;
             z.y = z.y * s;
         }
@@ -213,10 +219,10 @@ f32_cols_solve_kernel(float2* __restrict__ A, int nx, int ny, int nhp, const flo
     f32_fft_line<true>(line, ny, roots, lt, act);
     const float n = (float)ny;
     for (int k = threadIdx.x; k < CW * ny; k += blockDim.x) {
-        const int cc = k % CW, j = k / CW;
+        const int cc = k / ny, j = k % ny;
         if (c0 + cc >= ncol) continue;
         const float2 z = a[cc * LP + fft32_pad(j)];
-        A[(size_t)j * nhp + c0 + cc] = make_float2(z.x / n, z.y / n);
+        A[(size_t)(c0 + cc) * ny + j] = make_float2(z.x / n, z.y / n);
     }
 }
 
@@ -224,14 +230,15 @@ f32_cols_solve_kernel(float2* __restrict__ A, int nx, int ny, int nhp, const flo
 // (Hermitian completion), inverse FFT, phi_a = Re / nx, phi_b = Im / nx.
 template <class F>   // F = float (a template so that only the FP32 unit instantiates it)
 __global__ void __launch_bounds__(FFT32_MAXT)
-f32_rows_inv_kernel(const float2* __restrict__ A, int nx, int nhp, const float2* __restrict__ roots,
+f32_rows_inv_kernel(const float2* __restrict__ A, int nx, int ny, const float2* __restrict__ roots,
                     F* __restrict__ phi, int pitch, const int* __restrict__ active) {
     if (active && *active == 0) return;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     float2* a = reinterpret_cast<float2*>(smem_raw);
     const int ja = 2 * blockIdx.x, jb = ja + 1;
     for (int k = threadIdx.x; k <= nx / 2; k += blockDim.x) {
-        const float2 xa = A[(size_t)ja * nhp + k], xb = A[(size_t)jb * nhp + k];
+        const float4 x = *reinterpret_cast<const float4*>(A + (size_t)k * ny + ja);
+        const float2 xa = make_float2(x.x, x.y), xb = make_float2(x.z, x.w);
         a[fft32_pad(k)] = make_float2(xa.x - xb.y, xa.y + xb.x);
         if (k > 0 && k < nx / 2) a[fft32_pad(nx - k)] = make_float2(xa.x + xb.y, xb.x - xa.y);
     }

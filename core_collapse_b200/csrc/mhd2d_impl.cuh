@@ -5,13 +5,13 @@
 namespace ccb {
 
 namespace {
-// columns per CTA of the FP32 column pass: at most FFT32_MAXT threads and
-// 72 KB of lines (three CTAs per SM)
+// columns per CTA of the FP32 column pass: at most 256 threads and 48 KB of
+// lines (four CTAs per SM)
 inline int fft32_cw(int ny) {
     const int tl = fft32_tpl(ny);
     const size_t line = sizeof(float2) * (size_t)fft32_line(ny);
     int cw = 16;
-    while (cw > 1 && (cw * tl > FFT32_MAXT || cw * line > 72 * 1024)) cw >>= 1;
+    while (cw > 1 && (cw * tl > 256 || cw * line > 48 * 1024)) cw >>= 1;
     return cw;
 }
 inline int round32(int t) { return (t + 31) / 32 * 32; }
@@ -152,25 +152,25 @@ cudaError_t M2Launch<T>::fft32_solve(const T* rho, int pitch, const double* rho_
         return cudaErrorNotSupported;
     } else {
         if (nx > FFT32_MAXN || ny > FFT32_MAXN || nx < 2 || ny < 2) return cudaErrorInvalidValue;
-        const int nhp = fft32_half_pitch(nx);
+        const int nhl = fft32_half_lines(nx);
         const size_t row = sizeof(float2) * (size_t)fft32_line(nx);
         const int cw = fft32_cw(ny);
         const size_t col = sizeof(float2) * (size_t)fft32_line(ny) * cw;
         cudaError_t e;
         f32_rows_fwd_kernel<T><<<ny / 2, round32(fft32_tpl(nx)), row, s>>>(rho, pitch, rho_part, RED_BLOCKS,
-                                                                        (double)nx * (double)ny, A, nx, nhp,
+                                                                        (double)nx * (double)ny, A, nx, ny,
                                                                         rootx, active);
         if ((e = cudaGetLastError()) != cudaSuccess) return e;
-        const int nt = round32(cw * fft32_tpl(ny)), nb = nhp / cw;
+        const int nt = round32(cw * fft32_tpl(ny)), nb = nhl / cw;
         switch (cw) {
-            case 16: f32_cols_solve_kernel<16><<<nb, nt, col, s>>>(A, nx, ny, nhp, rooty, Lx, Ly, G, active); break;
-            case 8: f32_cols_solve_kernel<8><<<nb, nt, col, s>>>(A, nx, ny, nhp, rooty, Lx, Ly, G, active); break;
-            case 4: f32_cols_solve_kernel<4><<<nb, nt, col, s>>>(A, nx, ny, nhp, rooty, Lx, Ly, G, active); break;
-            case 2: f32_cols_solve_kernel<2><<<nb, nt, col, s>>>(A, nx, ny, nhp, rooty, Lx, Ly, G, active); break;
-            default: f32_cols_solve_kernel<1><<<nb, nt, col, s>>>(A, nx, ny, nhp, rooty, Lx, Ly, G, active); break;
+            case 16: f32_cols_solve_kernel<16><<<nb, nt, col, s>>>(A, nx, ny, rooty, Lx, Ly, G, active); break;
+            case 8: f32_cols_solve_kernel<8><<<nb, nt, col, s>>>(A, nx, ny, rooty, Lx, Ly, G, active); break;
+            case 4: f32_cols_solve_kernel<4><<<nb, nt, col, s>>>(A, nx, ny, rooty, Lx, Ly, G, active); break;
+            case 2: f32_cols_solve_kernel<2><<<nb, nt, col, s>>>(A, nx, ny, rooty, Lx, Ly, G, active); break;
+            default: f32_cols_solve_kernel<1><<<nb, nt, col, s>>>(A, nx, ny, rooty, Lx, Ly, G, active); break;
         }
         if ((e = cudaGetLastError()) != cudaSuccess) return e;
-        f32_rows_inv_kernel<T><<<ny / 2, round32(fft32_tpl(nx)), row, s>>>(A, nx, nhp, rootx, phi, pitch, active);
+        f32_rows_inv_kernel<T><<<ny / 2, round32(fft32_tpl(nx)), row, s>>>(A, nx, ny, rootx, phi, pitch, active);
         return cudaGetLastError();
     }
 }

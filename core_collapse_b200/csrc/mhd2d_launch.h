@@ -34,7 +34,7 @@ template <class T> struct M2Launch {
                                  const int* active, cudaStream_t s);
     // FP32 spectral solve (fft32_kernels.cuh), T = float only: rootx / rooty
     // the nx-th / ny-th roots of unity W^e = (cos 2 pi e/n, -sin 2 pi e/n),
-    // A: ny x fft32_half_pitch(nx) complex work array; needs nx, ny powers of two.
+    // A: fft32_half_lines(nx) x ny complex work array; needs nx, ny powers of two.
     static cudaError_t fft32_solve(const T* rho, int pitch, const double* rho_part, int nx, int ny,
                                    const float2* rootx, const float2* rooty, double Lx, double Ly, double G,
                                    float2* A, T* phi, const int* active, cudaStream_t s);
