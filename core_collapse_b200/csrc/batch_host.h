@@ -191,8 +191,10 @@ template <class T> struct Batch : BatchBase {
         if (int r = dalloc(&pool, total)) return r;
         CC_CUDA(cudaMemsetAsync(pool, 0, sizeof(T) * total, st()));
         // ---- direct Poisson: x bases per (nx, periodic, dx), y factors per grid shape ----
-        std::map<std::tuple<int, int, double>, std::tuple<double*, double*, double*>> bases;
-        std::map<std::tuple<int, int, double, int, int, double>, std::tuple<double*, double*, double*, double*>> yfac;
+        // (built in FP64, stored in the state precision T)
+        std::map<std::tuple<int, int, double>, std::tuple<T*, T*, T*>> bases;
+        std::map<std::tuple<int, int, double, int, int, double>, std::tuple<T*, T*, T*, T*>> yfac;
+        auto to_t = [](const std::vector<double>& v) { return std::vector<T>(v.begin(), v.end()); };
         for (int i = 0; i < n; i++) {
             const cc_mhd2d_params& q = p[i];
             const int nx = q.Nx, ny = q.Ny, P = pitch[i];
@@ -234,10 +236,10 @@ template <class T> struct Batch : BatchBase {
                     std::vector<double> txt((size_t)nx * nx);
                     for (int a = 0; a < nx; a++)
                         for (int b = 0; b < nx; b++) txt[(size_t)b * nx + a] = tx[(size_t)a * nx + b];
-                    double *d_tx, *d_txt, *d_lam;
-                    if (int r = upload_vec(&d_tx, tx)) return r;
-                    if (int r = upload_vec(&d_txt, txt)) return r;
-                    if (int r = upload_vec(&d_lam, lam)) return r;
+                    T *d_tx, *d_txt, *d_lam;
+                    if (int r = upload_vec(&d_tx, to_t(tx))) return r;
+                    if (int r = upload_vec(&d_txt, to_t(txt))) return r;
+                    if (int r = upload_vec(&d_lam, to_t(lam))) return r;
                     it = bases.emplace(key, std::make_tuple(d_tx, d_txt, d_lam)).first;
                 }
                 I.tx = std::get<0>(it->second);
@@ -249,12 +251,12 @@ template <class T> struct Batch : BatchBase {
                     std::vector<double> tx, lam, cp, inv, z, fden;
                     x_basis(nx, q.periodic_x != 0, dx, tx, lam);
                     y_factors(nx, ny, q.periodic_y != 0, 1.0 / (dy * dy), lam, cp, inv, z, fden);
-                    double *d_cp, *d_inv, *d_z = nullptr, *d_fden;
-                    if (int r = upload_vec(&d_cp, cp)) return r;
-                    if (int r = upload_vec(&d_inv, inv)) return r;
+                    T *d_cp, *d_inv, *d_z = nullptr, *d_fden;
+                    if (int r = upload_vec(&d_cp, to_t(cp))) return r;
+                    if (int r = upload_vec(&d_inv, to_t(inv))) return r;
                     if (q.periodic_y)
-                        if (int r = upload_vec(&d_z, z)) return r;
-                    if (int r = upload_vec(&d_fden, fden)) return r;
+                        if (int r = upload_vec(&d_z, to_t(z))) return r;
+                    if (int r = upload_vec(&d_fden, to_t(fden))) return r;
                     yt = yfac.emplace(ykey, std::make_tuple(d_cp, d_inv, d_z, d_fden)).first;
                 }
                 I.ycp = std::get<0>(yt->second);

@@ -29,17 +29,19 @@ template <class T> struct BatchInst {
     M2Const<T> c;
     Fields<T> buf[3];
     T* phi;               // pitched gravitational potential (stage gravity source)
-    // direct Poisson solve (FP64): x transform by a dense orthonormal basis,
-    // then one tridiagonal (or cyclic) solve per x wavenumber along y
-    const double* tx;     // nx*nx: row k = k-th basis vector of the x second difference
-    const double* txt;    // its transpose
-    const double* lamx;   // nx eigenvalues of the x second difference (1/dx^2 units included)
-    double* ah;           // ny*nx: transformed rhs, then transformed phi (in place)
+    // direct Poisson solve in the state precision T (FP64 instances: the
+    // bitwise-reproducible path; FP32 instances: FP32 bases, factors and
+    // work array): x transform by a dense orthonormal basis, then one
+    // tridiagonal (or cyclic) solve per x wavenumber along y
+    const T* tx;          // nx*nx: row k = k-th basis vector of the x second difference
+    const T* txt;         // its transpose
+    const T* lamx;        // nx eigenvalues of the x second difference (1/dx^2 units included)
+    T* ah;                // ny*nx: transformed rhs, then transformed phi (in place)
     // factors of the y systems, [j*nx + k] (set up once per grid shape):
-    const double* ycp;    // Thomas cp_j
-    const double* yinv;   // 1 / m_j
-    const double* yz;     // cyclic correction vector (periodic y only)
-    const double* yfden;  // nx: 1 / (1 + v.z) (periodic y only)
+    const T* ycp;         // Thomas cp_j
+    const T* yinv;        // 1 / m_j
+    const T* yz;          // cyclic correction vector (periodic y only)
+    const T* yfden;       // nx: 1 / (1 + v.z) (periodic y only)
     double fourpiG;
     double ay;            // 1/dy^2
     double dy2;           // dy^2

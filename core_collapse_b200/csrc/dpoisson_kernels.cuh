@@ -1,5 +1,6 @@
-// Direct Poisson solve for the batched ensemble (FP64 arithmetic, T only at the
-// density load and the potential store).
+// Direct Poisson solve for the batched ensemble, in the state precision T
+// (FP64 instances: FP64 throughout, bitwise reproducible on the CPU; FP32
+// instances: the same operations in FP32).
 //
 // It solves the discrete problem the reference's SOR iterates towards
 // (mhd2d_resistive_hlld_ct_gravity.cpp:207-223: 5-point Laplacian, clamp or
@@ -37,11 +38,10 @@ template <class T, int MODE, int TM>
 __global__ void __launch_bounds__(DPNT)
 dp_gemm_kernel(const BatchInst<T>* __restrict__ inst, const int2* __restrict__ gwork, int ngwork, int src,
                const double* __restrict__ rho_mean, const int* __restrict__ active) {
-    using AT = typename std::conditional<MODE == 0, T, double>::type;
     constexpr int RPT = TM / 16;            // outputs per thread per dimension
     constexpr int LQ = TM * DPK / DPNT;     // tile elements each thread loads per K chunk
-    __shared__ double As[DPK][TM + 1];      // k-major A tile
-    __shared__ double Bs[DPK][TM];
+    __shared__ T As[DPK][TM + 1];           // k-major A tile
+    __shared__ T Bs[DPK][TM];
     const int tr = threadIdx.x / 16, tc = threadIdx.x % 16;
     for (int w = blockIdx.x; w < ngwork; w += gridDim.x) {
         const int2 it = gwork[w];
@@ -49,40 +49,40 @@ dp_gemm_kernel(const BatchInst<T>* __restrict__ inst, const int2* __restrict__ g
         const BatchInst<T>& I = inst[it.x];
         const int nx = I.c.nx, ny = I.c.ny, P = I.c.pitch;
         const int m0 = (it.y >> 16) * TM, n0 = (it.y & 0xffff) * TM;
-        const double* __restrict__ B = (MODE == 0) ? I.txt : I.tx;   // K x N row-major, K = N = nx
+        const T* __restrict__ B = (MODE == 0) ? I.txt : I.tx;   // K x N row-major, K = N = nx
         const T* __restrict__ rho = I.buf[src].rho;
-        const double* __restrict__ ah = I.ah;
-        const double mean = (MODE == 0) ? rho_mean[it.x] : 0.0;
-        const double fpg = I.fourpiG;
-        AT ra[LQ];
-        double rb[LQ];
+        const T* __restrict__ ah = I.ah;
+        const T mean = (MODE == 0) ? (T)rho_mean[it.x] : T(0);
+        const T fpg = (T)I.fourpiG;
+        T ra[LQ];
+        T rb[LQ];
         auto gload = [&](int k0) {
 #pragma unroll
             for (int q = 0; q < LQ; q++) {
                 const int e = threadIdx.x + q * DPNT;
                 const int gm = m0 + e / DPK, gk = k0 + e % DPK;
-                ra[q] = AT(0);
+                ra[q] = T(0);
                 if (gm < ny && gk < nx) {
-                    if (MODE == 0) ra[q] = (AT)rho[(size_t)gm * P + gk];
-                    else ra[q] = (AT)ah[(size_t)gm * nx + gk];
+                    if (MODE == 0) ra[q] = rho[(size_t)gm * P + gk];
+                    else ra[q] = ah[(size_t)gm * nx + gk];
                 }
                 const int gkb = k0 + e / TM, gn = n0 + e % TM;
-                rb[q] = (gkb < nx && gn < nx) ? B[(size_t)gkb * nx + gn] : 0.0;
+                rb[q] = (gkb < nx && gn < nx) ? B[(size_t)gkb * nx + gn] : T(0);
             }
         };
-        double acc[RPT][RPT];
+        T acc[RPT][RPT];
 #pragma unroll
         for (int r = 0; r < RPT; r++)
 #pragma unroll
-            for (int c = 0; c < RPT; c++) acc[r][c] = 0.0;
+            for (int c = 0; c < RPT; c++) acc[r][c] = T(0);
         gload(0);
         for (int k0 = 0; k0 < nx; k0 += DPK) {
 #pragma unroll
             for (int q = 0; q < LQ; q++) {
                 const int e = threadIdx.x + q * DPNT;
                 const int m = e / DPK, kk = e % DPK;
-                double v = (double)ra[q];
-                if (MODE == 0) v = (m0 + m < ny && k0 + kk < nx) ? fpg * (v - mean) : 0.0;
+                T v = ra[q];
+                if (MODE == 0) v = (m0 + m < ny && k0 + kk < nx) ? fpg * (v - mean) : T(0);
                 As[kk][m] = v;
                 Bs[e / TM][e % TM] = rb[q];
             }
@@ -90,7 +90,7 @@ dp_gemm_kernel(const BatchInst<T>* __restrict__ inst, const int2* __restrict__ g
             if (k0 + DPK < nx) gload(k0 + DPK);
             const int kend = min(DPK, nx - k0);
             for (int kk = 0; kk < kend; kk++) {
-                double a[RPT], b[RPT];
+                T a[RPT], b[RPT];
 #pragma unroll
                 for (int r = 0; r < RPT; r++) a[r] = As[kk][tr + 16 * r];
 #pragma unroll
@@ -111,7 +111,7 @@ dp_gemm_kernel(const BatchInst<T>* __restrict__ inst, const int2* __restrict__ g
                 const int gn = n0 + tc + 16 * c;
                 if (gn >= nx) continue;
                 if (MODE == 0) I.ah[(size_t)gm * nx + gn] = acc[r][c];
-                else I.phi[(size_t)gm * P + gn] = (T)acc[r][c];
+                else I.phi[(size_t)gm * P + gn] = acc[r][c];
             }
         }
     }
@@ -128,20 +128,20 @@ constexpr int YB = 16;
 
 // forward sweep: d_0 = u_0 inv_0, d_j = (u_j - a d_{j-1}) inv_j, u_j <- d_j; returns d_{n-1}
 // (the prefetch of the block after the last one reads clamped, in-range rows)
-__device__ __forceinline__ double ysweep_fwd(double* __restrict__ u, const double* __restrict__ inv, size_t S,
-                                             int n, double a) {
-    double d = u[0] * inv[0];
+template <class S_>
+__device__ __forceinline__ S_ ysweep_fwd(S_* __restrict__ u, const S_* __restrict__ inv, size_t S, int n, S_ a) {
+    S_ d = u[0] * inv[0];
     u[0] = d;
     int j = 1;
     const int nb = (n - 1) / YB;
-    double cu[YB], ci[YB];
+    S_ cu[YB], ci[YB];
 #pragma unroll
     for (int t = 0; t < YB; t++) {
         const int r = min(j + t, n - 1);
         cu[t] = u[r * S]; ci[t] = inv[r * S];
     }
     for (int b = 0; b < nb; b++, j += YB) {
-        double nu[YB], ni[YB];
+        S_ nu[YB], ni[YB];
 #pragma unroll
         for (int t = 0; t < YB; t++) {
             const int r = min(j + YB + t, n - 1);
@@ -163,18 +163,18 @@ __device__ __forceinline__ double ysweep_fwd(double* __restrict__ u, const doubl
 }
 
 // backward sweep: x_{n-1} = d_{n-1}, x_j = d_j - cp_j x_{j+1}, u_j <- x_j; returns x_0
-__device__ __forceinline__ double ysweep_bwd(double* __restrict__ u, const double* __restrict__ cp, size_t S,
-                                             int n, double x) {
+template <class S_>
+__device__ __forceinline__ S_ ysweep_bwd(S_* __restrict__ u, const S_* __restrict__ cp, size_t S, int n, S_ x) {
     int j = n - 2;
     const int nb = (n - 1) / YB;
-    double cu[YB], cc[YB];
+    S_ cu[YB], cc[YB];
 #pragma unroll
     for (int t = 0; t < YB; t++) {
         const int r = max(j - t, 0);
         cu[t] = u[r * S]; cc[t] = cp[r * S];
     }
     for (int b = 0; b < nb; b++, j -= YB) {
-        double nu[YB], nc[YB];
+        S_ nu[YB], nc[YB];
 #pragma unroll
         for (int t = 0; t < YB; t++) {
             const int r = max(j - YB - t, 0);
@@ -206,45 +206,46 @@ dp_ysolve_kernel(const BatchInst<T>* __restrict__ inst, const int2* __restrict__
         const int nx = I.c.nx, n = I.c.ny;
         const size_t S = (size_t)nx;
         const bool py = I.c.ay.periodic != 0;
-        const double a = I.ay;
+        const T a = (T)I.ay;
         if (it.y < 0) {
             // singular k = 0: flux G_j = a (u_{j+1} - u_j) = G_{j-1} + r_j, then mean removal
             if (threadIdx.x != 0) continue;
-            double* __restrict__ u = I.ah;
-            double g0 = 0.0;
+            T* __restrict__ u = I.ah;
+            T g0 = T(0);
             if (py) {
-                double Sr = 0.0, SS = 0.0;
+                T Sr = T(0), SS = T(0);
 #pragma unroll 16
                 for (int j = 0; j < n; j++) { Sr = Sr + u[j * S]; SS = SS + Sr; }
-                g0 = -(SS / (double)n);
+                g0 = -(SS / (T)n);
             }
-            double G = g0, prev = 0.0;
-            double r = u[0];
-            u[0] = 0.0;
+            const T dy2 = (T)I.dy2;
+            T G = g0, prev = T(0);
+            T r = u[0];
+            u[0] = T(0);
 #pragma unroll 16
             for (int j = 0; j + 1 < n; j++) {
                 G = G + r;
                 r = u[(j + 1) * S];
-                prev = fma(I.dy2, G, prev);
+                prev = fma(dy2, G, prev);
                 u[(j + 1) * S] = prev;
             }
-            double m = 0.0;
+            T m = T(0);
 #pragma unroll 16
             for (int j = 0; j < n; j++) m = m + u[j * S];
-            m = m / (double)n;
+            m = m / (T)n;
 #pragma unroll 16
             for (int j = 0; j < n; j++) u[j * S] = u[j * S] - m;
             continue;
         }
         const int col = 1 + it.y * DPC + threadIdx.x;
         if (col >= nx) continue;
-        double* __restrict__ u = I.ah + col;
-        const double d = ysweep_fwd(u, I.yinv + col, S, n, a);
-        const double x = ysweep_bwd(u, I.ycp + col, S, n, d);
+        T* __restrict__ u = I.ah + col;
+        const T d = ysweep_fwd<T>(u, I.yinv + col, S, n, a);
+        const T x = ysweep_bwd<T>(u, I.ycp + col, S, n, d);
         if (!py) continue;
-        const double* __restrict__ z = I.yz + col;
-        const double gam = -fma(-2.0, a, I.lamx[col]);
-        const double fac = fma(a / gam, d, x) * I.yfden[col];   // d = x_{n-1}, x = x_0
+        const T* __restrict__ z = I.yz + col;
+        const T gam = -fma(T(-2), a, I.lamx[col]);
+        const T fac = fma(a / gam, d, x) * I.yfden[col];   // d = x_{n-1}, x = x_0
 #pragma unroll 8
         for (int j = 0; j < n; j++) u[j * S] = fma(-fac, z[j * S], u[j * S]);
     }
