@@ -418,7 +418,7 @@ def run_ensemble(args, stream, rank: int, world: int, barrier, max_over_ranks, s
     out = {"workload": f"{args.ensemble} independent 2D collapse instances, sides from {{64,96,128,192,256}} (seed 2), "
                        "outflow [-1,1]^2, per-instance core amplitude/width, Bx, eta; direct Poisson",
            "instances": args.ensemble, "cells": total_cells, "steps": steps, "warmup": args.warmup,
-           "dtype": "f32", "reductions": "f64", "poisson": "direct (FP64)", "scaling": "strong"}
+           "dtype": "f32", "reductions": "f64", "poisson": "direct (FP32, the instances' precision)", "scaling": "strong"}
     b = BatchSolver([params[i] for i in mine])
     b.set_stream(stream.cuda_stream)
     for k, i in enumerate(mine):

@@ -106,7 +106,8 @@ class CcBatchInfo(C.Structure):
         ("n", C.c_int32), ("precision", C.c_int32), ("cells", C.c_int64),
         ("shape", C.c_int32), ("n_shapes", C.c_int32), ("tile_x", C.c_int32), ("tile_y", C.c_int32),
         ("stage_tiles", C.c_int32), ("stage_ctas", C.c_int32), ("reduce_tiles", C.c_int32),
-        ("poisson_tiles", C.c_int32), ("device_bytes", C.c_int64),
+        ("poisson_tiles", C.c_int32), ("device_bytes", C.c_int64), ("poisson_tile", C.c_int32),
+        ("reserved", C.c_int32),
     ]
 
 

@@ -124,6 +124,8 @@ template <class T> struct Batch : BatchBase {
     std::vector<int> sgrid;          // CTAs per candidate
     int2* rwork = nullptr; int nrwork = 0;
     int2* gwork = nullptr; int ngwork = 0; int gtile = 64;
+    int2* tcwork = nullptr; int ntcwork = 0;   // FP32 instances with 16-byte rows: tcgen05 transforms
+    int* tcerr = nullptr;            // timed-out waits of the tensor-core transforms
     int2* ywork = nullptr; int nywork = 0;
     // per-instance device scalars and partials
     double* spd_part = nullptr;
@@ -172,6 +174,7 @@ template <class T> struct Batch : BatchBase {
 
     int init() override {
         CC_CUDA(BatchLaunch<T>::prepare());
+        CC_CUDA(DPoissonLaunch<T>::prepare());
         hinst.resize(n);
         hred.resize(n);
         pitch.resize(n);
@@ -272,7 +275,7 @@ template <class T> struct Batch : BatchBase {
             R.dts.clamp_to_end = 1; R.dts.seed = 1e-14; R.dts.end_eps = 0.0; R.dts.check = 0; R.dts.cap = 1;
         }
         // ---- work-lists ----
-        std::vector<int2> rw, gw, gw32, yw;
+        std::vector<int2> rw, gw, gw32, gw128, yw;
         for (int i = 0; i < n; i++) {
             const int nx = p[i].Nx, ny = p[i].Ny;
             hred[i].base = (int)rw.size();
@@ -280,18 +283,30 @@ template <class T> struct Batch : BatchBase {
                 for (int tx = 0; tx < (nx + RTX - 1) / RTX; tx++) rw.push_back(make_int2(i, (ty << 16) | tx));
             hred[i].count = (int)rw.size() - hred[i].base;
             if (p[i].gravity_on) {
-                for (int tm = 0; tm < (ny + 63) / 64; tm++)
-                    for (int tn = 0; tn < (nx + 63) / 64; tn++) gw.push_back(make_int2(i, (tm << 16) | tn));
-                for (int tm = 0; tm < (ny + 31) / 32; tm++)
-                    for (int tn = 0; tn < (nx + 31) / 32; tn++) gw32.push_back(make_int2(i, (tm << 16) | tn));
+                // per instance (so that its result does not depend on the batch):
+                // FP32 with 16-byte rows on the tensor cores, else CUDA cores
+                if (sizeof(T) == 4 && nx % 4 == 0) {
+                    for (int tm = 0; tm < (ny + 127) / 128; tm++)
+                        for (int tn = 0; tn < (nx + 127) / 128; tn++) gw128.push_back(make_int2(i, (tm << 16) | tn));
+                } else {
+                    for (int tm = 0; tm < (ny + 63) / 64; tm++)
+                        for (int tn = 0; tn < (nx + 63) / 64; tn++) gw.push_back(make_int2(i, (tm << 16) | tn));
+                    for (int tm = 0; tm < (ny + 31) / 32; tm++)
+                        for (int tn = 0; tn < (nx + 31) / 32; tn++) gw32.push_back(make_int2(i, (tm << 16) | tn));
+                }
                 // item -1: the singular x wavenumber 0 on its own; items cb >= 0:
                 // wavenumbers 1 + 32 cb + lane
                 yw.push_back(make_int2(i, -1));
                 for (int cb = 0; cb < (nx - 1 + 31) / 32; cb++) yw.push_back(make_int2(i, cb));
             }
         }
-        // 64 x 64 GEMM tiles unless they would leave most SMs idle (small batches)
+        // CUDA-core GEMMs on 64 x 64 tiles unless they would leave most SMs
+        // idle (small batches); same per-output k order, same bits
         if (gw.size() < 296) { gw.swap(gw32); gtile = 32; }
+        ntcwork = (int)gw128.size();
+        if (int r = upload_vec(&tcwork, gw128)) return r;
+        if (int r = dalloc(&tcerr, 1)) return r;
+        CC_CUDA(cudaMemsetAsync(tcerr, 0, sizeof(int), st()));
         nrwork = (int)rw.size(); ngwork = (int)gw.size(); nywork = (int)yw.size();
         if (int r = upload_vec(&rwork, rw)) return r;
         if (int r = upload_vec(&gwork, gw)) return r;
@@ -413,7 +428,8 @@ template <class T> struct Batch : BatchBase {
     // density means from rho_part, then the direct solve on buffer src
     int poisson(int src) {
         CC_CUDA(launch_batch_finalize(dred, n, spd_part, rho_part, BF_MEAN, dt, tclk, active, rho_mean, st()));
-        CC_CUDA(DPoissonLaunch<T>::solve(dinst, gwork, ngwork, gtile, ywork, nywork, src, rho_mean, active, st()));
+        CC_CUDA(DPoissonLaunch<T>::solve(dinst, gwork, ngwork, gtile, tcwork, ntcwork, ywork, nywork, src, rho_mean,
+                                         active, tcerr, st()));
         count(4);
         h->perf.poisson_solves += 1;
         return CC_OK;
@@ -502,7 +518,10 @@ template <class T> struct Batch : BatchBase {
         for (; done < nsteps; ++done)
             if (int r = device_step()) return r;
         if (t) CC_CUDA(cudaMemcpyAsync(t, tclk, sizeof(double) * n, cudaMemcpyDeviceToHost, st()));
+        int terr = 0;
+        CC_CUDA(cudaMemcpyAsync(&terr, tcerr, sizeof(int), cudaMemcpyDeviceToHost, st()));
         CC_CUDA(cudaStreamSynchronize(st()));
+        if (terr) return fail(h, CC_ERR_CUDA, "tensor-core Poisson transform: an mbarrier wait timed out");
         return CC_OK;
     }
 
@@ -596,7 +615,8 @@ template <class T> struct Batch : BatchBase {
         o->stage_tiles = nswork[shape % NS];
         o->stage_ctas = sgrid[shape];
         o->reduce_tiles = nrwork;
-        o->poisson_tiles = ngwork;
+        o->poisson_tiles = ngwork + ntcwork;
+        o->poisson_tile = ntcwork > 0 ? (ngwork > 0 ? -128 : 128) : gtile;
         o->device_bytes = (int64_t)bytes;
         return CC_OK;
     }

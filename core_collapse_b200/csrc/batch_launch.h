@@ -36,10 +36,16 @@ template <class T> struct BatchLaunch {
 };
 
 template <class T> struct DPoissonLaunch {
+    // shared-memory limit of the tensor-core transforms (FP32; before any launch or capture)
+    static cudaError_t prepare();
     // rho of buffer src -> phi, for every active instance
-    // gwork: GEMM tiles of gtile x gtile outputs (64 or 32)
-    static cudaError_t solve(const BatchInst<T>* inst, const int2* gwork, int ngwork, int gtile, const int2* ywork,
-                             int nywork, int src, const double* rho_mean, const int* active, cudaStream_t s);
+    // gwork: CUDA-core GEMM tiles of gtile x gtile outputs (64 or 32);
+    // tcwork: 128 x 128 tiles of the instances solved on the tcgen05 tensor
+    // cores (FP32 instances with nx a multiple of 4; a timed-out wait inside
+    // them sets *err).  An instance is in one of the two lists.
+    static cudaError_t solve(const BatchInst<T>* inst, const int2* gwork, int ngwork, int gtile, const int2* tcwork,
+                             int ntcwork, const int2* ywork, int nywork, int src, const double* rho_mean,
+                             const int* active, int* err, cudaStream_t s);
 };
 
 // flags of the finaliser

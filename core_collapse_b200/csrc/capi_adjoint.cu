@@ -219,7 +219,8 @@ struct Adjoint : Batch<double> {
         const BatchInst<double>* Cc = recC + l;
         if (grav) {
             CC_CUDA(launch_batch_finalize(dred, 1, spd_part, rho_part, BF_MEAN, dt, tclk, active, rho_mean, st()));
-            CC_CUDA(DPoissonLaunch<double>::solve(A, gwork, ngwork, gtile, ywork, nywork, 0, rho_mean, active, st()));
+            CC_CUDA(DPoissonLaunch<double>::solve(A, gwork, ngwork, gtile, nullptr, 0, ywork, nywork, 0, rho_mean,
+                                                  active, tcerr, st()));
         }
         if (mode == 0) {
             CC_CUDA(launch_batch_finalize(dred, 1, spd_part, rho_part, BF_DT | BF_CLAMP, dt, tclk, active, rho_mean,
@@ -240,7 +241,8 @@ struct Adjoint : Batch<double> {
         if (grav) {
             CC_CUDA(BatchLaunch<double>::rho_sum(B, rwork, nrwork, 1, active, rho_part, st()));
             CC_CUDA(launch_batch_finalize(dred, 1, spd_part, rho_part, BF_MEAN, dt, tclk, active, rho_mean, st()));
-            CC_CUDA(DPoissonLaunch<double>::solve(B, gwork, ngwork, gtile, ywork, nywork, 1, rho_mean, active, st()));
+            CC_CUDA(DPoissonLaunch<double>::solve(B, gwork, ngwork, gtile, nullptr, 0, ywork, nywork, 1, rho_mean,
+                                                  active, tcerr, st()));
         }
         if (int r = stage(B, 1, 2, true)) return r;
         CC_CUDA(BatchLaunch<double>::average(Cc, rwork, nrwork, 0, 2, 1, dt, active, spd_part, rho_part, st()));
@@ -304,7 +306,8 @@ struct Adjoint : Batch<double> {
     int poisson_adjoint(const Fields<double>& ltarget) {
         CC_CUDA(BatchLaunch<double>::rho_sum(recP, rwork, nrwork, 0, active, rho_part, st()));
         CC_CUDA(launch_batch_finalize(dred, 1, spd_part, rho_part, BF_MEAN, dt, tclk, active, rho_mean, st()));
-        CC_CUDA(DPoissonLaunch<double>::solve(recP, gwork, ngwork, gtile, ywork, nywork, 0, rho_mean, active, st()));
+        CC_CUDA(DPoissonLaunch<double>::solve(recP, gwork, ngwork, gtile, nullptr, 0, ywork, nywork, 0, rho_mean,
+                                              active, tcerr, st()));
         adj_add_plane_kernel<<<adj_grid(p[0].Nx * p[0].Ny), ADJ_NT, 0, st()>>>(p[0].Nx, p[0].Ny, P, ltarget.rho,
                                                                                 PoisOut);
         CC_CUDA(cudaGetLastError());

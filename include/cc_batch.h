@@ -43,8 +43,11 @@ typedef struct cc_batch_info {
     int32_t stage_tiles;     /* work-list length of the stage kernel       */
     int32_t stage_ctas;      /* persistent CTAs of the stage kernel        */
     int32_t reduce_tiles;    /* 32x8 reduce tiles (one partial each)       */
-    int32_t poisson_tiles;   /* 64x64 GEMM tiles of the direct solve       */
+    int32_t poisson_tiles;   /* GEMM tiles of the direct solve             */
     int64_t device_bytes;    /* device memory held by the handle           */
+    int32_t poisson_tile;    /* their edge: 32 or 64 (CUDA cores), 128 (every solved instance on the
+                                tcgen05 tensor cores: FP32 with Nx % 4 == 0), -128 (some of them) */
+    int32_t reserved;
 } cc_batch_info;
 
 /* params: n instance descriptions (Nx, Ny >= 4; same precision). */

@@ -142,6 +142,38 @@ def test_fp32_batch_error_vs_fp64_oracle():
             assert l1 <= 1e-5, f"instance {i} field {k}: rel L1 {l1:.2e}"
 
 
+def test_fp32_tensor_core_poisson_vs_fp64_oracle():
+    """FP32 instances whose Nx are multiples of 4 solve the direct Poisson
+    transforms on the tcgen05 tensor cores (3xTF32, 128 x 128 tiles): sizes
+    with one and several tiles and partial tiles, both boundary kinds; per-field
+    relative L1 error against the FP64 oracle after 10 steps below 1e-5 (the
+    face fields relative to the mean in-plane field |Bx_f| + |By_f|: By_f
+    starts at zero and stays small, so its own mean is no scale)."""
+    base = Params(x0=-1.0, x1=1.0, y0=-1.0, y1=1.0, gamma=5.0 / 3.0, cfl=0.4, G=1.0, poisson="direct",
+                  precision="fp32", t_end=10.0, gravity_on=True)
+    specs = [dict(Nx=40, Ny=24, periodic_x=False, periodic_y=False, eta=1e-3),
+             dict(Nx=136, Ny=200, periodic_x=True, periodic_y=True, eta=5e-4),
+             dict(Nx=260, Ny=132, periodic_x=False, periodic_y=True, eta=2e-3),
+             dict(Nx=128, Ny=128, periodic_x=True, periodic_y=False, eta=1e-3)]
+    params, states = [], []
+    for k, kw in enumerate(specs):
+        p = replace(base, **kw)
+        U, B = ic_collapse(p, core_amp=6.0 + 2 * k, core_width=0.25, noise=0.02, seed=11 + k, Bx0=0.05)
+        params.append(p)
+        states.append((U, B))
+    with BatchSolver(params) as b:
+        assert b.info()["poisson_tile"] == 128
+    out, tt, _ = _run_batch(params, states, 10)
+    for i, p in enumerate(params):
+        want, tw = O.m2_main_loop_oracle(replace(p, precision="fp64").to_c(), O.state_list(*states[i]), 10, mode=3)
+        assert abs(tt[i] - tw) <= 1e-5 * tw
+        bscale = np.mean(np.abs(want[6])) + np.mean(np.abs(want[7]))
+        for k, (a, w) in enumerate(zip(_flat(*out[i]), want)):
+            scale = (bscale if k >= 6 else np.mean(np.abs(w))) + 1e-30
+            l1 = np.mean(np.abs(a - w)) / scale
+            assert l1 <= 1e-5, f"instance {i} field {k}: rel L1 {l1:.2e}"
+
+
 def test_mass_conserved_periodic_instance():
     params, states = _mixed("fp64")
     out, tt, diags = _run_batch(params, states, 6)
