@@ -118,10 +118,8 @@ template <class T, int K = 0> struct ShapeLoop {
     }
 };
 
-inline int rgrid(int nrwork) {
-    const int g = nrwork < 8192 ? nrwork : 8192;
-    return g < 1 ? 1 : g;
-}
+// one CTA per reduce tile: the hardware keeps SMs fed while tiles wait on memory
+inline int rgrid(int nrwork) { return nrwork < 1 ? 1 : nrwork; }
 
 }  // namespace
 

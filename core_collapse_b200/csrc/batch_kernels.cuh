@@ -109,7 +109,7 @@ __global__ void __launch_bounds__(RNT)
 m2b_average_kernel(const BatchInst<T>* __restrict__ inst, const int2* __restrict__ rwork, int nrwork, int a, int d,
                    int b, const double* __restrict__ dt, const int* __restrict__ active,
                    double* __restrict__ spd_part, double* __restrict__ rho_part) {
-    __shared__ double sh[RNT / 32];
+    __shared__ double sh[2 * RNT / 32];
     for (int w = blockIdx.x; w < nrwork; w += gridDim.x) {
         const int2 it = rwork[w];
         const BatchInst<T>& I = inst[it.x];
@@ -122,9 +122,8 @@ m2b_average_kernel(const BatchInst<T>* __restrict__ inst, const int2* __restrict
                                           rsum);
             if (s > smax) smax = s;
         }
-        const double bm = block_max<RNT>(smax, sh);
-        const double bs = block_sum<RNT>(rsum, sh);
-        if (threadIdx.x == 0) { spd_part[w] = bm; rho_part[w] = bs; }
+        block_max_sum<RNT>(smax, rsum, sh);
+        if (threadIdx.x == 0) { spd_part[w] = smax; rho_part[w] = rsum; }
     }
 }
 
@@ -133,7 +132,7 @@ template <class T>
 __global__ void __launch_bounds__(RNT)
 m2b_speed_kernel(const BatchInst<T>* __restrict__ inst, const int2* __restrict__ rwork, int nrwork, int src,
                  double* __restrict__ spd_part, double* __restrict__ rho_part) {
-    __shared__ double sh[RNT / 32];
+    __shared__ double sh[2 * RNT / 32];
     for (int w = blockIdx.x; w < nrwork; w += gridDim.x) {
         const int2 it = rwork[w];
         const BatchInst<T>& I = inst[it.x];
@@ -146,9 +145,8 @@ m2b_speed_kernel(const BatchInst<T>* __restrict__ inst, const int2* __restrict__
             if (v > smax) smax = v;
             rsum = (double)I.buf[src].rho[(size_t)j * I.c.pitch + i];
         }
-        const double bm = block_max<RNT>(smax, sh);
-        const double bs = block_sum<RNT>(rsum, sh);
-        if (threadIdx.x == 0) { spd_part[w] = bm; rho_part[w] = bs; }
+        block_max_sum<RNT>(smax, rsum, sh);
+        if (threadIdx.x == 0) { spd_part[w] = smax; rho_part[w] = rsum; }
     }
 }
 

@@ -65,6 +65,29 @@ __device__ __forceinline__ double block_max(double v, double* sh) {
     return r;
 }
 
+// block_max and block_sum of two values at once, with the same orders (so
+// the same bits) and one barrier pair instead of two.  Results in thread 0.
+template <int NT>
+__device__ __forceinline__ void block_max_sum(double& vmax_, double& vsum, double* sh /* >= 2 NT/32 */) {
+    for (int o = 16; o > 0; o >>= 1) {
+        vmax_ = fmax(vmax_, __shfl_down_sync(0xffffffffu, vmax_, o));
+        vsum += __shfl_down_sync(0xffffffffu, vsum, o);
+    }
+    const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+    if (l == 0) { sh[w] = vmax_; sh[NT / 32 + w] = vsum; }
+    __syncthreads();
+    if (w == 0) {
+        double m = (l < NT / 32) ? sh[l] : 0.0, r = (l < NT / 32) ? sh[NT / 32 + l] : 0.0;
+        for (int o = 16; o > 0; o >>= 1) {
+            m = fmax(m, __shfl_down_sync(0xffffffffu, m, o));
+            r += __shfl_down_sync(0xffffffffu, r, o);
+        }
+        vmax_ = m;
+        vsum = r;
+    }
+    __syncthreads();
+}
+
 // Grid-wide barrier for kernels launched cooperatively (all blocks resident).
 // Sense is a generation counter.  The wait is bounded: after max_spins polls the
 // block records an error in *err and leaves; callers test the return value and

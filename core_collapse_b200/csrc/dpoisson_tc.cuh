@@ -12,15 +12,17 @@
 //
 // Per CTA (256 threads, one output tile):
 //   * warp 0 allocates 128 TMEM columns (the 128 x 128 FP32 accumulator);
-//   * K runs in chunks of 32: all threads load the A and B chunks from global
+//   * K runs in chunks of 16: all threads load the A and B chunks from global
 //     memory (B = rows of Tx or Tx^T, i.e. both operands K-major), split them
 //     and store hi and lo parts to shared memory in the canonical K-major
 //     no-swizzle layout -- 16-byte core-matrix rows, unit (kc, row) at byte
 //     (kc * 128 + row) * 16, so 8-row groups are 128 B apart (SBO) and the two
-//     16-byte K halves of one MMA are 2048 B apart (LBO);
-//   * one thread issues the 4 K-steps x 3 products of the chunk
+//     16-byte K halves of one MMA are 2048 B apart (LBO); the global loads of
+//     chunk c+1 are issued into registers before chunk c is handed to the
+//     tensor core, so their latency overlaps the barrier and the MMAs;
+//   * one thread issues the 2 K-steps x 3 products of the chunk
 //     (tcgen05.mma.cta_group::1.kind::tf32, M = N = 128, K = 8) and commits
-//     them to the chunk's mbarrier; two shared-memory stages, so the loads of
+//     them to the chunk's mbarrier; two shared-memory stages, so the stores of
 //     chunk c+1 overlap the MMAs of chunk c;
 //   * epilogue: each warp reads 32 accumulator lanes (rows) x 64 columns with
 //     tcgen05.ld and stores them (float4) to ah or phi.
@@ -33,10 +35,12 @@
 
 namespace ccb {
 
-constexpr int TCM = 128, TCN = 128, TCK = 32, TCNT = 256;
+constexpr int TCM = 128, TCN = 128, TCK = 16, TCNT = 256;
+constexpr int TCU = TCM * (TCK / 4) / TCNT;              // 16-byte units per thread and operand per chunk
 constexpr int TC_PART = TCM * TCK * 4;                   // bytes of one operand part (A or B, hi or lo)
 constexpr int TC_STAGE = 4 * TC_PART;                    // A hi, A lo, B hi, B lo
 constexpr int TC_SMEM = 2 * TC_STAGE + 64;               // two stages, two mbarriers, the TMEM address
+                                                         // (64 KB: three CTAs per SM, 384 TMEM columns)
 constexpr unsigned TC_WAIT_POLLS = 1u << 24;             // x >= 64 ns sleep: > 1 s before giving up
 
 // instruction descriptor: D FP32 (bits 4-5 = 1), A and B TF32 (bits 7-9, 10-12 = 2),
@@ -119,7 +123,7 @@ __device__ __forceinline__ float4 tc_lo(float4 v, float4 h) {
 // gwork items {instance, (tm << 16) | tn} of 128 x 128 tiles; instances with
 // nx a multiple of 4 (16-byte rows).
 template <int MODE>
-__global__ void __launch_bounds__(TCNT, 1)
+__global__ void __launch_bounds__(TCNT, 3)
 dp_gemm_tc_kernel(const BatchInst<float>* __restrict__ inst, const int2* __restrict__ gwork, int src,
                   const double* __restrict__ rho_mean, const int* __restrict__ active, int* __restrict__ err) {
     const int2 it = gwork[blockIdx.x];
@@ -156,6 +160,24 @@ dp_gemm_tc_kernel(const BatchInst<float>* __restrict__ inst, const int2* __restr
     bool ok = true;
     int issued = 0;   // chunks whose MMAs were committed
 
+    // chunk c's operands in registers: A and B, TCU 16-byte units each
+    float4 ra[TCU], rb[TCU];
+    auto gload = [&](int c) {
+        const int k0 = c * TCK;
+#pragma unroll
+        for (int i = 0; i < TCU; i++) {
+            const int u = tid + i * TCNT, kc = u >> 7, row = u & 127;
+            const int gk = k0 + 4 * kc, gm = m0 + row, gn = n0 + row;
+            ra[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+            rb[i] = ra[i];
+            if (gm < ny && gk < nx) {
+                if (MODE == 0) ra[i] = *reinterpret_cast<const float4*>(I.buf[src].rho + (size_t)gm * P + gk);
+                else ra[i] = *reinterpret_cast<const float4*>(I.ah + (size_t)gm * nx + gk);
+            }
+            if (gn < nx && gk < nx) rb[i] = *reinterpret_cast<const float4*>(Bsrc + (size_t)gn * nx + gk);
+        }
+    };
+    gload(0);
     for (int c = 0; c < nk; c++) {
         const int s = c & 1;
         unsigned char* stage = tc_smem + s * TC_STAGE;
@@ -165,23 +187,18 @@ dp_gemm_tc_kernel(const BatchInst<float>* __restrict__ inst, const int2* __restr
             ok = *sok != 0;
             if (!ok) break;   // uniform
         }
-        const int k0 = c * TCK;
-        // 128 rows x 8 sixteen-byte units per operand; unit u -> (kc = u / 128, row = u % 128)
+        // 128 rows x TCK/4 sixteen-byte units per operand; unit u -> (kc = u / 128, row = u % 128)
 #pragma unroll
-        for (int i = 0; i < 4; i++) {
+        for (int i = 0; i < TCU; i++) {
             const int u = tid + i * TCNT, kc = u >> 7, row = u & 127;
-            const int gk = k0 + 4 * kc;
-            float4 a = make_float4(0.f, 0.f, 0.f, 0.f), b = a;
-            const int gm = m0 + row, gn = n0 + row;
-            if (gm < ny && gk < nx) {
-                if (MODE == 0) {
-                    const float4 r = *reinterpret_cast<const float4*>(I.buf[src].rho + (size_t)gm * P + gk);
-                    a = make_float4(fpg * (r.x - mean), fpg * (r.y - mean), fpg * (r.z - mean), fpg * (r.w - mean));
-                } else {
-                    a = *reinterpret_cast<const float4*>(I.ah + (size_t)gm * nx + gk);
-                }
+            const int gk = c * TCK + 4 * kc, gm = m0 + row;
+            float4 a = ra[i];
+            if (MODE == 0) {   // 4 pi G (rho - mean) inside the instance, 0 in the padding
+                const bool in = gm < ny && gk < nx;
+                a = in ? make_float4(fpg * (a.x - mean), fpg * (a.y - mean), fpg * (a.z - mean), fpg * (a.w - mean))
+                       : make_float4(0.f, 0.f, 0.f, 0.f);
             }
-            if (gn < nx && gk < nx) b = *reinterpret_cast<const float4*>(Bsrc + (size_t)gn * nx + gk);
+            const float4 b = rb[i];
             const float4 ah = tc_tf32(a), bh = tc_tf32(b);
             const int off = (kc * 128 + row) * 16;
             *reinterpret_cast<float4*>(stage + off) = ah;
@@ -189,6 +206,7 @@ dp_gemm_tc_kernel(const BatchInst<float>* __restrict__ inst, const int2* __restr
             *reinterpret_cast<float4*>(stage + 2 * TC_PART + off) = bh;
             *reinterpret_cast<float4*>(stage + 3 * TC_PART + off) = tc_lo(b, bh);
         }
+        if (c + 1 < nk) gload(c + 1);
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
         __syncthreads();
         if (tid == 0) {
