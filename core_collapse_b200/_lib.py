@@ -15,6 +15,7 @@ CC_ERR_NONFINITE = -4
 CC_ERR_NOT_CONVERGED = -5
 CC_ERR_UNSUPPORTED = -6
 CC_ERR_TOO_LARGE = -7
+CC_ERR_IO = -8
 CC_NOALLOC_MAX_CELLS = 1 << 18
 CC_NOALLOC_MAX_SIDE = 4096
 
@@ -128,6 +129,9 @@ SIGNATURES = {
     "cc_mhd2d_rk2_step": (C.c_int, [_H, _DP, _DP, C.c_double]),
     "cc_mhd2d_advance": (C.c_int, [_H, C.c_int, _DP]),
     "cc_mhd2d_diagnostics": (C.c_int, [_H, C.POINTER(CcDiag)]),
+    "cc_mhd2d_derived": (C.c_int, [_H, C.POINTER(C.POINTER(C.c_double))]),
+    "cc_mhd2d_checkpoint_save": (C.c_int, [_H, C.c_char_p]),
+    "cc_mhd2d_checkpoint_load": (C.c_int, [_H, C.c_char_p]),
     "cc_mhd2d_gravity_fft_noalloc": (C.c_int, [C.POINTER(CcMhd2dParams), C.c_void_p, C.c_void_p, C.c_void_p,
                                                C.c_void_p]),
     "cc_mhd3d_params_default": (None, [C.POINTER(CcMhd3dParams)]),

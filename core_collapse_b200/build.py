@@ -15,6 +15,8 @@ Translation units and their floating-point contract:
   euler2d_f32.cu, batch_f32.cu       FMA contraction on, approximate FP32 division
                                      and square root, flush-to-zero (the FP32 bulk path)
   capi*.cu, ic.cpp                   host code
+and the host programs of MAINS (g++, linked against the library):
+  main_mhd2d.cpp -> cc_mhd2d_main    drop-in for the reference's 2D driver
 """
 from __future__ import annotations
 
@@ -107,7 +109,31 @@ def build(verbose: bool = False, force: bool = False) -> Path:
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError(f"link failed:\n{r.stdout}\n{r.stderr}")
+    build_mains(verbose)
     return LIB
+
+
+# host programs linked against the library (rpath $ORIGIN: they sit beside it)
+MAINS = [("main_mhd2d.cpp", "cc_mhd2d_main")]
+
+
+def build_mains(verbose: bool = False) -> list[Path]:
+    cxx = shutil.which("g++") or shutil.which("c++")
+    if cxx is None:
+        raise RuntimeError("g++ not found (needed for the drop-in main programs)")
+    outs = []
+    for src_name, exe_name in MAINS:
+        src, exe = CSRC / src_name, PKG / exe_name
+        if not exe.exists() or exe.stat().st_mtime < max(LIB.stat().st_mtime, *(d.stat().st_mtime for d in _deps(src))):
+            cmd = [cxx, "-O2", "-std=c++17", "-I", str(INCLUDE), str(src), "-L", str(PKG), "-lcc_b200",
+                   "-Wl,-rpath,$ORIGIN", "-o", str(exe)]
+            r = subprocess.run(cmd, capture_output=True, text=True)
+            if r.returncode != 0:
+                raise RuntimeError(f"building {exe_name} failed:\n{r.stdout}\n{r.stderr}")
+            if verbose and r.stderr:
+                print(r.stderr, file=sys.stderr)
+        outs.append(exe)
+    return outs
 
 
 if __name__ == "__main__":

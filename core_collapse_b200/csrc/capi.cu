@@ -11,6 +11,7 @@
 // flag (t < t_end) live on the device, so a run of steps needs no host sync
 // and is captured as a CUDA graph (three steps = one buffer rotation).
 #include <cmath>
+#include <cstdint>
 #include <cstdio>
 #include <cstring>
 #include <memory>
@@ -73,6 +74,10 @@ struct Mhd2dBase {
     virtual int rk2_step(const double* gx, const double* gy, double dt) = 0;
     virtual int advance(int nsteps, double* t) = 0;
     virtual int diagnostics(cc_diag* d) = 0;
+    virtual int derived(double* const* out) = 0;
+    virtual int get_clock(double* t, long long* steps) = 0;
+    virtual int set_clock(double t, long long steps) = 0;
+    virtual const cc_mhd2d_params& params() const = 0;
 };
 
 template <class T> struct Mhd2d : Mhd2dBase {
@@ -105,6 +110,7 @@ template <class T> struct Mhd2d : Mhd2dBase {
     double* t_dev = nullptr;
     double* sor_res = nullptr;
     long long* steps_dev = nullptr;
+    double* derived_dev = nullptr;   // 10 planes of Nx*Ny, allocated at the first cc_mhd2d_derived
     bool loaded = false;
     bool rho_part_valid = false;   // rho_part / spd_part describe buf[cur]
     bool phi_valid = false;        // phi is the Poisson solution of buf[cur].rho
@@ -120,7 +126,7 @@ template <class T> struct Mhd2d : Mhd2dBase {
     ~Mhd2d() override {
         if (graph3) cudaGraphExecDestroy(graph3);
         void* ptrs[] = {block, phi, gxa, gya, fftA, tw[0], tw[1], tw[2], tw[3], rhs, sphi, scal, spd_part, rho_part,
-                        diag_part, sor_part, sor_part2, staging, bar, iflags, steps_dev};
+                        diag_part, sor_part, sor_part2, staging, bar, iflags, steps_dev, derived_dev};
         for (void* q : ptrs)
             if (q) cudaFree(q);
     }
@@ -504,6 +510,34 @@ template <class T> struct Mhd2d : Mhd2dBase {
         return check_flags();
     }
 
+    const cc_mhd2d_params& params() const override { return p; }
+
+    int derived(double* const* out) override {
+        if (!loaded) return fail(h, CC_ERR_STATE, "no state uploaded");
+        const size_t n = (size_t)p.Nx * p.Ny;
+        if (!derived_dev) CC_CUDA(cudaMalloc(&derived_dev, sizeof(double) * n * 10));
+        CC_CUDA(M2Launch<T>::derived(c, buf[cur], derived_dev, st()));
+        for (int k = 0; k < 10; k++)
+            if (out[k])
+                CC_CUDA(cudaMemcpyAsync(out[k], derived_dev + k * n, sizeof(double) * n, cudaMemcpyDeviceToHost, st()));
+        CC_CUDA(cudaStreamSynchronize(st()));
+        return check_flags();
+    }
+
+    int get_clock(double* t, long long* steps) override {
+        CC_CUDA(cudaMemcpyAsync(t, t_dev, sizeof(double), cudaMemcpyDeviceToHost, st()));
+        CC_CUDA(cudaMemcpyAsync(steps, steps_dev, sizeof(long long), cudaMemcpyDeviceToHost, st()));
+        CC_CUDA(cudaStreamSynchronize(st()));
+        return CC_OK;
+    }
+
+    int set_clock(double t, long long steps) override {
+        CC_CUDA(launch_set_scalar(t_dev, t, st()));
+        CC_CUDA(cudaMemcpyAsync(steps_dev, &steps, sizeof(long long), cudaMemcpyHostToDevice, st()));
+        CC_CUDA(cudaStreamSynchronize(st()));
+        return CC_OK;
+    }
+
     int diagnostics(cc_diag* d) override {
         if (!loaded) return fail(h, CC_ERR_STATE, "no state uploaded");
         CC_CUDA(M2Launch<T>::diag(c, buf[cur], diag_part, st()));
@@ -541,6 +575,35 @@ template <class T> struct Mhd2d : Mhd2dBase {
 struct Mhd2dHandle : cc_handle {
     std::unique_ptr<Mhd2dBase> impl;
 };
+
+// checkpoint file helpers
+constexpr char CK_MAGIC[9] = "CCB2DCK1";
+constexpr uint32_t CK_VERSION = 1;
+
+std::vector<size_t> ck_sizes(const cc_mhd2d_params& p) {
+    const size_t nx = (size_t)p.Nx, ny = (size_t)p.Ny, n = nx * ny;
+    return {n, n, n, n, n, n, (nx + 1) * ny, nx * (ny + 1)};
+}
+
+void ck_put(std::vector<unsigned char>& b, const void* src, size_t n) {
+    const unsigned char* c = static_cast<const unsigned char*>(src);
+    b.insert(b.end(), c, c + n);
+}
+
+void ck_get(const std::vector<unsigned char>& b, size_t& off, void* dst, size_t n) {
+    std::memcpy(dst, b.data() + off, n);
+    off += n;
+}
+
+// FNV-1a, 64-bit
+uint64_t ck_fnv1a(const unsigned char* d, size_t n) {
+    uint64_t hsh = 1469598103934665603ull;
+    for (size_t i = 0; i < n; i++) {
+        hsh ^= d[i];
+        hsh *= 1099511628211ull;
+    }
+    return hsh;
+}
 
 Mhd2dBase* m2(cc_handle* h) {
     if (!h || h->kind != KIND_MHD2D) return nullptr;
@@ -694,6 +757,95 @@ int cc_mhd2d_diagnostics(cc_handle* h, cc_diag* d) {
     if (!m || !d) return CC_ERR_ARG;
     if (int r = set_dev(h)) return r;
     return m->diagnostics(d);
+}
+
+int cc_mhd2d_derived(cc_handle* h, double* const* out) {
+    Mhd2dBase* m = m2(h);
+    if (!m || !out) return CC_ERR_ARG;
+    if (int r = set_dev(h)) return r;
+    return m->derived(out);
+}
+
+int cc_mhd2d_checkpoint_save(cc_handle* h, const char* path) {
+    Mhd2dBase* m = m2(h);
+    if (!m || !path) return CC_ERR_ARG;
+    if (int r = set_dev(h)) return r;
+    const cc_mhd2d_params& p = m->params();
+    std::vector<std::vector<double>> f;
+    for (size_t n : ck_sizes(p)) f.emplace_back(n);
+    double* fp[8];
+    for (int k = 0; k < 8; k++) fp[k] = f[k].data();
+    if (int r = m->download(fp)) return r;
+    double t = 0.0;
+    long long steps = 0;
+    if (int r = m->get_clock(&t, &steps)) return r;
+    std::vector<unsigned char> b;
+    ck_put(b, CK_MAGIC, 8);
+    const uint32_t ver = CK_VERSION, prec = (uint32_t)p.precision;
+    const int32_t nx = p.Nx, ny = p.Ny;
+    const uint64_t pb = sizeof(cc_mhd2d_params);
+    ck_put(b, &ver, 4); ck_put(b, &prec, 4); ck_put(b, &nx, 4); ck_put(b, &ny, 4);
+    ck_put(b, &pb, 8); ck_put(b, &p, sizeof(p));
+    ck_put(b, &t, 8); ck_put(b, &steps, 8);
+    for (int k = 0; k < 8; k++) ck_put(b, f[k].data(), sizeof(double) * f[k].size());
+    const uint64_t sum = ck_fnv1a(b.data(), b.size());
+    ck_put(b, &sum, 8);
+    FILE* fo = std::fopen(path, "wb");
+    if (!fo) return fail(h, CC_ERR_IO, std::string("cannot open for writing: ") + path);
+    const size_t w = std::fwrite(b.data(), 1, b.size(), fo);
+    const int cl = std::fclose(fo);
+    if (w != b.size() || cl != 0) return fail(h, CC_ERR_IO, std::string("short write: ") + path);
+    return CC_OK;
+}
+
+int cc_mhd2d_checkpoint_load(cc_handle* h, const char* path) {
+    Mhd2dBase* m = m2(h);
+    if (!m || !path) return CC_ERR_ARG;
+    if (int r = set_dev(h)) return r;
+    const cc_mhd2d_params& p = m->params();
+    FILE* fi = std::fopen(path, "rb");
+    if (!fi) return fail(h, CC_ERR_IO, std::string("cannot open for reading: ") + path);
+    std::vector<unsigned char> b;
+    unsigned char chunk[1 << 16];
+    size_t got;
+    while ((got = std::fread(chunk, 1, sizeof(chunk), fi)) > 0) b.insert(b.end(), chunk, chunk + got);
+    const bool rerr = std::ferror(fi) != 0;
+    std::fclose(fi);
+    if (rerr) return fail(h, CC_ERR_IO, std::string("read error: ") + path);
+    const size_t head = 8 + 4 * 4 + 8;
+    if (b.size() < head + 8 || std::memcmp(b.data(), CK_MAGIC, 8) != 0)
+        return fail(h, CC_ERR_ARG, "not a 2D MHD checkpoint (magic)");
+    uint64_t sum = 0;
+    std::memcpy(&sum, b.data() + b.size() - 8, 8);
+    if (sum != ck_fnv1a(b.data(), b.size() - 8)) return fail(h, CC_ERR_ARG, "checkpoint checksum mismatch");
+    size_t off = 8;
+    uint32_t ver = 0, prec = 0;
+    int32_t nx = 0, ny = 0;
+    uint64_t pb = 0;
+    ck_get(b, off, &ver, 4); ck_get(b, off, &prec, 4); ck_get(b, off, &nx, 4); ck_get(b, off, &ny, 4);
+    ck_get(b, off, &pb, 8);
+    if (ver != CK_VERSION || pb != sizeof(cc_mhd2d_params)) return fail(h, CC_ERR_ARG, "checkpoint version mismatch");
+    cc_mhd2d_params q;
+    ck_get(b, off, &q, sizeof(q));
+    if (nx != p.Nx || ny != p.Ny || (int)prec != p.precision || q.x0 != p.x0 || q.x1 != p.x1 || q.y0 != p.y0 ||
+        q.y1 != p.y1 || q.periodic_x != p.periodic_x || q.periodic_y != p.periodic_y)
+        return fail(h, CC_ERR_ARG, "checkpoint grid, domain, boundaries or precision differ from the handle's");
+    double t = 0.0;
+    long long steps = 0;
+    ck_get(b, off, &t, 8); ck_get(b, off, &steps, 8);
+    const std::vector<size_t> sz = ck_sizes(p);
+    size_t need = off + 8;
+    for (size_t n : sz) need += sizeof(double) * n;
+    if (need != b.size()) return fail(h, CC_ERR_ARG, "checkpoint size does not match its grid");
+    std::vector<std::vector<double>> f;
+    for (size_t n : sz) {
+        f.emplace_back(n);
+        ck_get(b, off, f.back().data(), sizeof(double) * n);
+    }
+    const double* fp[8];
+    for (int k = 0; k < 8; k++) fp[k] = f[k].data();
+    if (int r = m->upload(fp)) return r;
+    return m->set_clock(t, steps);
 }
 
 }  // extern "C"

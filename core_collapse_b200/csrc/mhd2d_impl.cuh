@@ -113,6 +113,12 @@ cudaError_t M2Launch<T>::diag(const M2Const<T>& c, const Fields<T>& st, double* 
 }
 
 template <class T>
+cudaError_t M2Launch<T>::derived(const M2Const<T>& c, const Fields<T>& st, double* out, cudaStream_t s) {
+    m2_derived_kernel<T><<<grid_for((size_t)c.nx * c.ny, 256, 4096), 256, 0, s>>>(c, st, out);
+    return cudaGetLastError();
+}
+
+template <class T>
 cudaError_t M2Launch<T>::pack_in(const double* src, T* dst, int w, int h, int pitch, cudaStream_t s) {
     pack_in_kernel<T><<<grid_for((size_t)w * h, 256, 4096), 256, 0, s>>>(src, dst, w, h, pitch);
     return cudaGetLastError();

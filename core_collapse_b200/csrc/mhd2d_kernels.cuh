@@ -488,6 +488,40 @@ m2_diag_kernel(const M2Const<T> c, const Fields<T> s, double* __restrict__ part 
     if (threadIdx.x == 0) { part[5 * gridDim.x + blockIdx.x] = bm; part[6 * gridDim.x + blockIdx.x] = bn; }
 }
 
+// Derived snapshot fields of the reference main()'s store (M2:1065-1106), in
+// its output order: rho, P, Mach, u, v, vabs, Bx, By, Bz (cell-centred, from
+// the faces) and div B; out holds 10 planes of nx*ny doubles, row-major.
+// Primitives through cons_to_prim, cs = sqrt(max(0, gamma P / max(rho,
+// floor_rho))), Mach = |v| / max(cs, 1e-14); in the state precision, the
+// divergence in FP64 as in the diagnostics.
+template <class T>
+__global__ void m2_derived_kernel(const M2Const<T> c, const Fields<T> s, double* __restrict__ out) {
+    const int P = c.pitch;
+    const size_t n = (size_t)c.nx * c.ny;
+    for (size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += (size_t)gridDim.x * blockDim.x) {
+        const int i = (int)(k % c.nx), j = (int)(k / c.nx);
+        const size_t q = (size_t)j * P + i;
+        const T Bx = T(0.5) * (s.bx[q] + s.bx[q + 1]);
+        const T By = T(0.5) * (s.by[q] + s.by[q + P]);
+        const Prim<T> W = to_prim(c, s.rho[q], s.mx[q], s.my[q], s.mz[q], s.E[q], Bx, By, s.Bz[q]);
+        const T cs = sqrt(vmax(T(0.0), c.gamma * W.P / vmax(W.r, c.floor_rho)));
+        const T vabs = sqrt(W.u * W.u + W.v * W.v + W.w * W.w);
+        const T mach = vabs / vmax(cs, T(1e-14));
+        const double div = ((double)s.bx[q + 1] - (double)s.bx[q]) / (double)c.dx +
+                           ((double)s.by[q + P] - (double)s.by[q]) / (double)c.dy;
+        out[k] = W.r;
+        out[n + k] = W.P;
+        out[2 * n + k] = mach;
+        out[3 * n + k] = W.u;
+        out[4 * n + k] = W.v;
+        out[5 * n + k] = vabs;
+        out[6 * n + k] = Bx;
+        out[7 * n + k] = By;
+        out[8 * n + k] = W.bz;
+        out[9 * n + k] = div;
+    }
+}
+
 // Combine CFL partials into dt (M2:590-597), clamp to t_end (M2:1114) and set
 // the active flag that makes the step kernels no-ops once t >= t_end.
 struct DtSpec {

@@ -25,6 +25,8 @@ template <class T> struct M2Launch {
                               cudaStream_t s);
     static cudaError_t rho_sum(const M2Const<T>& c, const T* rho, double* rho_part, cudaStream_t s);
     static cudaError_t diag(const M2Const<T>& c, const Fields<T>& st, double* part, cudaStream_t s);
+    // the 10 derived snapshot fields of the reference's store, out: 10 planes of nx*ny doubles
+    static cudaError_t derived(const M2Const<T>& c, const Fields<T>& st, double* out, cudaStream_t s);
     static cudaError_t pack_in(const double* src, T* dst, int w, int h, int pitch, cudaStream_t s);
     static cudaError_t pack_out(const T* src, double* dst, int w, int h, int pitch, cudaStream_t s);
     // spectral solve: rho (pitched T) -> phi (pitched T); A: nx*ny complex work

@@ -124,6 +124,10 @@ class CcError(RuntimeError):
         self.code = code
 
 
+# output order of the reference's snapshot store (M2:1090-1104, written by write_h5)
+DERIVED_FIELDS = ("rho", "P", "Mach", "u", "v", "vabs", "Bx", "By", "Bz", "divB")
+
+
 class Mhd2dSolver:
     """A device-resident 2D MHD instance (one libcc_b200 handle)."""
 
@@ -221,6 +225,23 @@ class Mhd2dSolver:
         d = L.CcDiag()
         self._check(self._lib.cc_mhd2d_diagnostics(self._h, C.byref(d)))
         return {f: getattr(d, f) for f, _ in L.CcDiag._fields_}
+
+    def derived(self) -> dict:
+        """The reference main()'s snapshot fields (M2:1065-1106) of the resident
+        state: {rho, P, Mach, u, v, vabs, Bx, By, Bz, divB}, each (Ny, Nx)."""
+        n = self.p.Nx * self.p.Ny
+        out = [np.empty(n) for _ in DERIVED_FIELDS]
+        arr = (C.POINTER(C.c_double) * 10)(*[_dp(a) for a in out])
+        self._check(self._lib.cc_mhd2d_derived(self._h, arr))
+        return {k: a.reshape(self.p.Ny, self.p.Nx) for k, a in zip(DERIVED_FIELDS, out)}
+
+    def save_checkpoint(self, path: str):
+        """State, clock and parameters to one file (cc_mhd2d_checkpoint_save)."""
+        self._check(self._lib.cc_mhd2d_checkpoint_save(self._h, str(path).encode()))
+
+    def load_checkpoint(self, path: str):
+        """Restore state and clock from a checkpoint of the same grid (cc_mhd2d_checkpoint_load)."""
+        self._check(self._lib.cc_mhd2d_checkpoint_load(self._h, str(path).encode()))
 
 
 # ---- drop-in functions with the reference's signatures ----

@@ -212,6 +212,28 @@ int cc_mhd2d_advance(cc_handle* h, int nsteps, double* t);
 /* Diagnostics of the resident state. */
 int cc_mhd2d_diagnostics(cc_handle* h, cc_diag* d);
 
+/* The derived fields the reference main() stores at each snapshot
+ * (mhd2d_resistive_hlld_ct_gravity.cpp:1065-1106) from the resident state:
+ * out[0..9] = rho, P, Mach, u, v, vabs, Bx, By, Bz, divB, each Nx*Ny doubles
+ * (row-major, x fastest); a NULL entry is skipped.  Bx, By are the cell-centred
+ * averages of the faces; FP64 handles give the reference's values bit for bit.
+ * The first call allocates 10*Nx*Ny doubles of device scratch for the handle. */
+int cc_mhd2d_derived(cc_handle* h, double* const* out);
+
+/* Checkpoint / restart (no counterpart in the reference, which keeps no
+ * restart file).  save: the resident state in the reference layouts as FP64,
+ * the clock (t, steps) and the parameters, into one file at path: magic
+ * "CCB2DCK1", version, precision, Nx, Ny, the cc_mhd2d_params bytes, t, steps,
+ * the 8 arrays, then an FNV-1a 64-bit checksum of all preceding bytes.  load:
+ * into a handle whose grid, domain, boundaries and precision equal the file's
+ * (other parameters, e.g. t_end, may differ); restores state and clock, so a
+ * run continued from a checkpoint matches the uninterrupted run bit for bit.
+ * Errors: CC_ERR_IO (open, read, write), CC_ERR_ARG (bad magic, version,
+ * checksum or a grid mismatch). */
+#define CC_ERR_IO -8
+int cc_mhd2d_checkpoint_save(cc_handle* h, const char* path);
+int cc_mhd2d_checkpoint_load(cc_handle* h, const char* path);
+
 /* ---- 3D MHD (mhd3d_resistive_hlld_ct.cpp) ---- */
 
 /* Fill with the reference defaults (mhd3d_resistive_hlld_ct.cpp:43-89). */

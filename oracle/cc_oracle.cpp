@@ -326,6 +326,12 @@ double or_mhd2d_divB_max(const cc_mhd2d_params* c, const double* const* f) {
     return M2<double>(m2par(c)).max_divB(s);
 }
 
+void or_mhd2d_derived(const cc_mhd2d_params* c, const double* const* f, double* const* out) {
+    M2State<double> s;
+    load(c, f, s);
+    M2<double>(m2par(c)).derived(s, out);
+}
+
 // ---- 3D MHD (mhd3d_resistive_hlld_ct.cpp) ----
 int or_mhd3d_advance_stage(const cc_mhd3d_params* c, const double* const* fin, double* const* fout, double dt) {
     M3State<double> s0, s1;

@@ -314,6 +314,26 @@ public:
         return vmin(dt_h, dt_r);
     }
 
+    // the main()'s snapshot store (M2:1065-1106): out[0..9] = rho, P, Mach,
+    // u, v, vabs, Bx_cc, By_cc, Bz, divB per cell
+    void derived(const M2State<T>& s, double* const* out) const {
+        const double dx = p.dx(), dy = p.dy();
+        for (int j = 0; j < p.ny; j++)
+            for (int i = 0; i < p.nx; i++) {
+                const size_t q = (size_t)j * p.nx + i;
+                const T Bx = bx_cc(s, i, j), By = by_cc(s, i, j);
+                const Prim8<T> W = to_prim(s.rho[q], s.mx[q], s.my[q], s.mz[q], s.E[q], Bx, By, s.Bz[q]);
+                const T cs = osqrt(vmax(T(0.0), T(p.gamma) * W.P / vmax(W.r, T(p.floor_rho))));
+                const T vabs = osqrt(W.u * W.u + W.v * W.v + W.w * W.w);
+                const T mach = vabs / vmax(cs, T(1e-14));
+                const double d = ((double)bx_face(s, i + 1, j) - (double)bx_face(s, i, j)) / dx +
+                                 ((double)by_face(s, i, j + 1) - (double)by_face(s, i, j)) / dy;
+                const double v[10] = {(double)W.r, (double)W.P, (double)mach, (double)W.u, (double)W.v,
+                                      (double)vabs, (double)Bx, (double)By, (double)W.bz, d};
+                for (int k = 0; k < 10; k++) out[k][q] = v[k];
+            }
+    }
+
     // max |div B| per cell (M2:873-879)
     double max_divB(const M2State<T>& s) const {
         double m = 0.0, dx = p.dx(), dy = p.dy();

@@ -49,6 +49,8 @@ def oracle() -> C.CDLL:
         O.or_mhd2d_main_loop.argtypes = [P2, _PP, C.c_int, _DP, C.c_int, C.c_int]
         O.or_mhd2d_divB_max.argtypes = [P2, _PP]
         O.or_mhd2d_divB_max.restype = C.c_double
+        O.or_mhd2d_derived.argtypes = [P2, _PP, _PP]
+        O.or_mhd2d_derived.restype = None
         O.or_fft1d.argtypes = [C.c_int, _DP, C.c_int]
         PE = C.POINTER(L.CcEuler2dParams)
         O.or_euler2d_gravity.argtypes = [PE, _DP, _DP, _DP, C.c_int, C.POINTER(C.c_int), _DP]
@@ -181,6 +183,15 @@ def m2_main_loop_oracle(cp, S, nsteps, mode, fp32=False, t0=0.0):
     t = C.c_double(t0)
     oracle().or_mhd2d_main_loop(C.byref(cp), pp(out), nsteps, C.byref(t), mode, 1 if fp32 else 0)
     return out, t.value
+
+
+def m2_derived_oracle(cp, S) -> list[np.ndarray]:
+    """The reference main()'s snapshot fields (rho, P, Mach, u, v, vabs, Bx,
+    By, Bz, divB) of state S, restated on the CPU."""
+    n = cp.Nx * cp.Ny
+    out = [np.empty(n) for _ in range(10)]
+    oracle().or_mhd2d_derived(C.byref(cp), pp(S), pp(out))
+    return out
 
 
 def rel_linf(a: np.ndarray, b: np.ndarray) -> float:

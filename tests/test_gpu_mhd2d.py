@@ -253,3 +253,84 @@ def test_errors_are_reported():
         with pytest.raises(CcError) as e:
             s.rk2_step(None, float("nan"))
         assert e.value.code == L.CC_ERR_NONFINITE
+
+
+@pytest.mark.parametrize("name", sorted(CASES))
+def test_derived_fields_match_oracle(name):
+    """cc_mhd2d_derived == the reference main()'s snapshot store (M2:1065-1106)
+    bit for bit in FP64, after 3 steps so that every field is non-trivial."""
+    p, U, B = make_case(name)
+    p.t_end = 10.0
+    with Mhd2dSolver(p) as s:
+        s.upload(U, B)
+        s.advance(3, 0.0)
+        got = s.derived()
+        S = _gpu_state(s)
+    want = O.m2_derived_oracle(p.to_c(), S)
+    from core_collapse_b200.mhd2d import DERIVED_FIELDS
+    for k, name_k in enumerate(DERIVED_FIELDS):
+        assert np.array_equal(got[name_k].ravel(), want[k]), f"{name} field {name_k}"
+
+
+def test_derived_fields_fp32_close():
+    p, U, B = make_case("periodic_grav_eta", precision="fp32")
+    with Mhd2dSolver(p) as s:
+        s.upload(U, B)
+        got = s.derived()
+        S = _gpu_state(s)
+    want = O.m2_derived_oracle(p.to_c(), S)
+    from core_collapse_b200.mhd2d import DERIVED_FIELDS
+    for k, name_k in enumerate(DERIVED_FIELDS[:9]):
+        scale = np.max(np.abs(want[k])) + 1e-30
+        assert np.max(np.abs(got[name_k].ravel() - want[k])) <= 1e-5 * scale, name_k
+    assert np.max(np.abs(got["divB"])) < 1e-4
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+def test_checkpoint_restart_continues_bitwise(tmp_path, precision):
+    """6 steps in one go == 3 steps, checkpoint, load into a fresh handle, 3
+    more steps: state, time and step count identical."""
+    p, U, B = make_case("periodic_grav_eta", precision=precision)
+    p.t_end = 10.0
+    with Mhd2dSolver(p) as s:
+        s.upload(U, B)
+        t_full = s.advance(6, 0.0)
+        want = _gpu_state(s)
+        steps_full = s.diagnostics()["steps"]
+    path = tmp_path / "ck.bin"
+    with Mhd2dSolver(p) as s:
+        s.upload(U, B)
+        s.advance(3, 0.0)
+        s.save_checkpoint(path)
+    with Mhd2dSolver(p) as s:
+        s.load_checkpoint(path)
+        t = s.advance(3)
+        got = _gpu_state(s)
+        d = s.diagnostics()
+    assert t == t_full and d["steps"] == steps_full
+    for a, w in zip(got, want):
+        assert np.array_equal(a, w)
+
+
+def test_checkpoint_rejects_bad_files(tmp_path):
+    p, U, B = make_case("periodic_grav_eta")
+    path = tmp_path / "ck.bin"
+    with Mhd2dSolver(p) as s:
+        s.upload(U, B)
+        s.save_checkpoint(path)
+    raw = bytearray(path.read_bytes())
+    raw[100] ^= 0xFF
+    bad = tmp_path / "bad.bin"
+    bad.write_bytes(bytes(raw))
+    q, U2, B2 = make_case("outflow_grav_eta")
+    with Mhd2dSolver(p) as s:
+        with pytest.raises(CcError) as e:
+            s.load_checkpoint(bad)
+        assert e.value.code == L.CC_ERR_ARG
+        with pytest.raises(CcError) as e:
+            s.load_checkpoint(tmp_path / "missing.bin")
+        assert e.value.code == L.CC_ERR_IO
+    with Mhd2dSolver(q) as s:
+        with pytest.raises(CcError) as e:
+            s.load_checkpoint(path)
+        assert e.value.code == L.CC_ERR_ARG
