@@ -171,6 +171,7 @@ class Mhd2dSolver:
 
     def upload(self, U: Ucc, B: Bfaces):
         self._check(self._lib.cc_mhd2d_upload(self._h, *_state_ptrs(U, B)))
+        self._t = 0.0
 
     def download(self, U: Ucc | None = None, B: Bfaces | None = None) -> tuple[Ucc, Bfaces]:
         if U is None or B is None:
@@ -199,8 +200,11 @@ class Mhd2dSolver:
             self._check(self._lib.cc_mhd2d_rk2_step(self._h, _dp(g.gx), _dp(g.gy), float(dt)))
 
     def advance(self, nsteps: int, t: float | None = None) -> float:
-        tt = C.c_double(0.0 if t is None else t)
+        """nsteps of the main loop from time t (None: where the last advance,
+        upload (t = 0) or checkpoint load left the clock); returns the time."""
+        tt = C.c_double(getattr(self, "_t", 0.0) if t is None else t)
         self._check(self._lib.cc_mhd2d_advance(self._h, int(nsteps), C.byref(tt)))
+        self._t = tt.value
         return tt.value
 
     def set_stream(self, stream_ptr: int | None):
@@ -242,6 +246,7 @@ class Mhd2dSolver:
     def load_checkpoint(self, path: str):
         """Restore state and clock from a checkpoint of the same grid (cc_mhd2d_checkpoint_load)."""
         self._check(self._lib.cc_mhd2d_checkpoint_load(self._h, str(path).encode()))
+        self._t = self.diagnostics()["t"]
 
 
 # ---- drop-in functions with the reference's signatures ----
