@@ -447,7 +447,8 @@ m2_rho_sum_kernel(const M2Const<T> c, const T* __restrict__ rho, double* __restr
     __shared__ double sh[NT / 32];
     double rsum = 0.0;
     const int ncell = c.nx * c.ny;
-    for (int k = blockIdx.x * NT + threadIdx.x; k < ncell; k += gridDim.x * NT) {
+#pragma unroll 8
+    for (int k = blockIdx.x * NT + threadIdx.x; k < ncell; k += gridDim.x * NT) {   // loads issued ahead, sum in order
         const int i = k % c.nx, j = k / c.nx;
         rsum += (double)rho[(size_t)j * c.pitch + i];
     }

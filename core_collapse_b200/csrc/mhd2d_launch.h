@@ -10,7 +10,7 @@
 
 namespace ccb {
 
-constexpr int RED_NT = 256;      // threads of the reduction kernels
+constexpr int RED_NT = 512;      // threads of the reduction kernels (two blocks per SM at <= 64 registers)
 constexpr int RED_BLOCKS = 296;  // 2 x 148 SMs; fixed so reduction order is fixed
 
 template <class T> struct M2Launch {
