@@ -147,7 +147,7 @@ __device__ __forceinline__ void f32_fft_line(float2* a, int n, const float2* __r
 
 // pass 1: rows 2b and 2b+1 -> half spectra.  rho pitched; mean = sum/N.
 template <class F>   // F = float (a template so that only the FP32 unit instantiates it)
-__global__ void __launch_bounds__(FFT32_MAXT)
+__global__ void __maxnreg__(80)   // three 256-thread CTAs per SM; blocks of up to FFT32_MAXT threads
 f32_rows_fwd_kernel(const F* __restrict__ rho, int pitch, const double* __restrict__ rho_part, int nparts,
                     double ncell, float2* __restrict__ A, int nx, int ny, const float2* __restrict__ roots,
                     const int* __restrict__ active) {
@@ -155,16 +155,29 @@ f32_rows_fwd_kernel(const F* __restrict__ rho, int pitch, const double* __restri
     extern __shared__ __align__(16) unsigned char smem_raw[];
     float2* a = reinterpret_cast<float2*>(smem_raw);
     __shared__ double s_mean;
-    if (threadIdx.x == 0) {
+    const int ja = 2 * blockIdx.x, jb = ja + 1;
+    // the two rows into registers first (at most 16 values per thread:
+    // blockDim >= nx / 16), so their loads are in flight while warp 0 forms
+    // the mean from the density partials (lane-strided sums, shuffle tree)
+    float ra[16], rb[16];
+#pragma unroll
+    for (int q = 0; q < 16; q++) {
+        const int i = threadIdx.x + q * blockDim.x;
+        if (i < nx) { ra[q] = rho[(size_t)ja * pitch + i]; rb[q] = rho[(size_t)jb * pitch + i]; }
+    }
+    if (threadIdx.x < 32) {
         double s = 0.0;
-        for (int b = 0; b < nparts; b++) s += rho_part[b];
-        s_mean = s / ncell;
+        for (int b = threadIdx.x; b < nparts; b += 32) s += rho_part[b];
+        for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+        if (threadIdx.x == 0) s_mean = s / ncell;
     }
     __syncthreads();
     const float mean = (float)s_mean;
-    const int ja = 2 * blockIdx.x, jb = ja + 1;
-    for (int i = threadIdx.x; i < nx; i += blockDim.x)
-        a[fft32_pad(i)] = make_float2(rho[(size_t)ja * pitch + i] - mean, rho[(size_t)jb * pitch + i] - mean);
+#pragma unroll
+    for (int q = 0; q < 16; q++) {
+        const int i = threadIdx.x + q * blockDim.x;
+        if (i < nx) a[fft32_pad(i)] = make_float2(ra[q] - mean, rb[q] - mean);
+    }
     __syncthreads();
     const int tl = fft32_tpl(nx);
     f32_fft_line<false>(a, nx, roots, (int)threadIdx.x, (int)threadIdx.x < tl);
