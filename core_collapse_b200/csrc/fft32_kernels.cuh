@@ -201,9 +201,19 @@ f32_cols_solve_kernel(float2* __restrict__ A, int nx, int ny, const float2* __re
     const int LP = fft32_line(ny);
     const int c0 = blockIdx.x * CW;
     const int ncol = nx / 2 + 1;
-    for (int k = threadIdx.x; k < CW * ny; k += blockDim.x) {
-        const int cc = k / ny, j = k % ny;
-        a[cc * LP + fft32_pad(j)] = (c0 + cc < ncol) ? A[(size_t)(c0 + cc) * ny + j] : make_float2(0.0f, 0.0f);
+    // all of this thread's values in flight before any is stored (at most 16
+    // per thread: blockDim >= CW ny / 16); ny is a power of two
+    const int lgy = __ffs(ny) - 1;
+    float2 xr[16];
+#pragma unroll
+    for (int q = 0; q < 16; q++) {
+        const int k = threadIdx.x + q * blockDim.x, cc = k >> lgy;
+        xr[q] = (k < CW * ny && c0 + cc < ncol) ? A[(size_t)c0 * ny + k] : make_float2(0.0f, 0.0f);
+    }
+#pragma unroll
+    for (int q = 0; q < 16; q++) {
+        const int k = threadIdx.x + q * blockDim.x;
+        if (k < CW * ny) a[(k >> lgy) * LP + fft32_pad(k & (ny - 1))] = xr[q];
     }
     __syncthreads();
     const int tl = fft32_tpl(ny);
@@ -249,9 +259,19 @@ f32_rows_inv_kernel(const float2* __restrict__ A, int nx, int ny, const float2* 
     extern __shared__ __align__(16) unsigned char smem_raw[];
     float2* a = reinterpret_cast<float2*>(smem_raw);
     const int ja = 2 * blockIdx.x, jb = ja + 1;
-    for (int k = threadIdx.x; k <= nx / 2; k += blockDim.x) {
-        const float4 x = *reinterpret_cast<const float4*>(A + (size_t)k * ny + ja);
-        const float2 xa = make_float2(x.x, x.y), xb = make_float2(x.z, x.w);
+    // all of this thread's half-spectrum values in flight before any is used
+    // (at most 9 per thread: blockDim >= nx / 16)
+    float4 xr[9];
+#pragma unroll
+    for (int q = 0; q < 9; q++) {
+        const int k = threadIdx.x + q * blockDim.x;
+        if (k <= nx / 2) xr[q] = *reinterpret_cast<const float4*>(A + (size_t)k * ny + ja);
+    }
+#pragma unroll
+    for (int q = 0; q < 9; q++) {
+        const int k = threadIdx.x + q * blockDim.x;
+        if (k > nx / 2) break;
+        const float2 xa = make_float2(xr[q].x, xr[q].y), xb = make_float2(xr[q].z, xr[q].w);
         a[fft32_pad(k)] = make_float2(xa.x - xb.y, xa.y + xb.x);
         if (k > 0 && k < nx / 2) a[fft32_pad(nx - k)] = make_float2(xa.x + xb.y, xb.x - xa.y);
     }
