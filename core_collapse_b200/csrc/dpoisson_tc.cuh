@@ -18,8 +18,8 @@
 //     no-swizzle layout -- 16-byte core-matrix rows, unit (kc, row) at byte
 //     (kc * 128 + row) * 16, so 8-row groups are 128 B apart (SBO) and the two
 //     16-byte K halves of one MMA are 2048 B apart (LBO); the global loads of
-//     chunk c+1 are issued into registers before chunk c is handed to the
-//     tensor core, so their latency overlaps the barrier and the MMAs;
+//     chunk c+2 are issued into registers right after chunk c is stored, so
+//     their latency overlaps two iterations (barriers and MMAs);
 //   * one thread issues the 2 K-steps x 3 products of the chunk
 //     (tcgen05.mma.cta_group::1.kind::tf32, M = N = 128, K = 8) and commits
 //     them to the chunk's mbarrier; two shared-memory stages, so the stores of
@@ -160,45 +160,47 @@ dp_gemm_tc_kernel(const BatchInst<float>* __restrict__ inst, const int2* __restr
     bool ok = true;
     int issued = 0;   // chunks whose MMAs were committed
 
-    // chunk c's operands in registers: A and B, TCU 16-byte units each
-    float4 ra[TCU], rb[TCU];
-    auto gload = [&](int c) {
+    // operands of two chunks in registers (slot = chunk parity): the loads of
+    // chunk c+2 are issued as soon as chunk c is in shared memory, two
+    // iterations ahead of their use
+    float4 ra[2][TCU], rb[2][TCU];
+    auto gload = [&](int c, float4* xa, float4* xb) {
         const int k0 = c * TCK;
 #pragma unroll
         for (int i = 0; i < TCU; i++) {
             const int u = tid + i * TCNT, kc = u >> 7, row = u & 127;
             const int gk = k0 + 4 * kc, gm = m0 + row, gn = n0 + row;
-            ra[i] = make_float4(0.f, 0.f, 0.f, 0.f);
-            rb[i] = ra[i];
+            xa[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+            xb[i] = xa[i];
             if (gm < ny && gk < nx) {
-                if (MODE == 0) ra[i] = *reinterpret_cast<const float4*>(I.buf[src].rho + (size_t)gm * P + gk);
-                else ra[i] = *reinterpret_cast<const float4*>(I.ah + (size_t)gm * nx + gk);
+                if (MODE == 0) xa[i] = *reinterpret_cast<const float4*>(I.buf[src].rho + (size_t)gm * P + gk);
+                else xa[i] = *reinterpret_cast<const float4*>(I.ah + (size_t)gm * nx + gk);
             }
-            if (gn < nx && gk < nx) rb[i] = *reinterpret_cast<const float4*>(Bsrc + (size_t)gn * nx + gk);
+            if (gn < nx && gk < nx) xb[i] = *reinterpret_cast<const float4*>(Bsrc + (size_t)gn * nx + gk);
         }
     };
-    gload(0);
-    for (int c = 0; c < nk; c++) {
+    // one K chunk: wait until its stage is free, split and store, prefetch
+    // chunk c+2, hand the stage to the tensor core; false after a timed-out wait
+    auto chunk = [&](int c, float4* xa, float4* xb) -> bool {
         const int s = c & 1;
         unsigned char* stage = tc_smem + s * TC_STAGE;
         if (c >= 2) {   // the MMAs of chunk c-2 read this stage: thread 0 waits, the CTA follows
             if (tid == 0) *sok = tc_mbar_wait(s ? mb1 : mb0, (uint32_t)(((c - 2) >> 1) & 1)) ? 1 : 0;
             __syncthreads();
-            ok = *sok != 0;
-            if (!ok) break;   // uniform
+            if (*sok == 0) return false;   // uniform
         }
         // 128 rows x TCK/4 sixteen-byte units per operand; unit u -> (kc = u / 128, row = u % 128)
 #pragma unroll
         for (int i = 0; i < TCU; i++) {
             const int u = tid + i * TCNT, kc = u >> 7, row = u & 127;
             const int gk = c * TCK + 4 * kc, gm = m0 + row;
-            float4 a = ra[i];
+            float4 a = xa[i];
             if (MODE == 0) {   // 4 pi G (rho - mean) inside the instance, 0 in the padding
                 const bool in = gm < ny && gk < nx;
                 a = in ? make_float4(fpg * (a.x - mean), fpg * (a.y - mean), fpg * (a.z - mean), fpg * (a.w - mean))
                        : make_float4(0.f, 0.f, 0.f, 0.f);
             }
-            const float4 b = rb[i];
+            const float4 b = xb[i];
             const float4 ah = tc_tf32(a), bh = tc_tf32(b);
             const int off = (kc * 128 + row) * 16;
             *reinterpret_cast<float4*>(stage + off) = ah;
@@ -206,7 +208,7 @@ dp_gemm_tc_kernel(const BatchInst<float>* __restrict__ inst, const int2* __restr
             *reinterpret_cast<float4*>(stage + 2 * TC_PART + off) = bh;
             *reinterpret_cast<float4*>(stage + 3 * TC_PART + off) = tc_lo(b, bh);
         }
-        if (c + 1 < nk) gload(c + 1);
+        if (c + 2 < nk) gload(c + 2, xa, xb);
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
         __syncthreads();
         if (tid == 0) {
@@ -226,6 +228,13 @@ dp_gemm_tc_kernel(const BatchInst<float>* __restrict__ inst, const int2* __restr
             tc_commit(s ? mb1 : mb0);
         }
         issued = c + 1;
+        return true;
+    };
+    gload(0, ra[0], rb[0]);
+    if (nk > 1) gload(1, ra[1], rb[1]);
+    for (int c = 0; c < nk; c += 2) {
+        if (!chunk(c, ra[0], rb[0])) { ok = false; break; }
+        if (c + 1 < nk && !chunk(c + 1, ra[1], rb[1])) { ok = false; break; }
     }
     // wait for the last committed chunk (a commit tracks all earlier MMAs of the thread)
     if (tid == 0) {
