@@ -151,6 +151,7 @@ SIGNATURES = {
     "cc_euler2d_rk2_step": (C.c_int, [_H, C.c_double]),
     "cc_euler2d_advance": (C.c_int, [_H, C.c_int, _DP]),
     "cc_euler2d_diagnostics": (C.c_int, [_H, C.POINTER(CcDiag)]),
+    "cc_euler2d_derived": (C.c_int, [_H, C.POINTER(C.POINTER(C.c_double))]),
     "cc_mhd2d_ic_knobs_default": (None, [C.POINTER(CcIcKnobs)]),
     "cc_ic_mhd2d_reference": (C.c_int, [C.POINTER(CcMhd2dParams), C.POINTER(CcIcKnobs), C.POINTER(_DP)]),
     "cc_ic_mhd2d_collapse": (C.c_int, [C.POINTER(CcMhd2dParams), C.c_double, C.c_double, C.c_double, C.c_uint32,

@@ -16,7 +16,8 @@ Translation units and their floating-point contract:
                                      and square root, flush-to-zero (the FP32 bulk path)
   capi*.cu, ic.cpp                   host code
 and the host programs of MAINS (g++, linked against the library):
-  main_mhd2d.cpp -> cc_mhd2d_main    drop-in for the reference's 2D driver
+  main_mhd2d.cpp -> cc_mhd2d_main    drop-in for the reference's 2D MHD driver
+  main_euler2d.cpp -> cc_euler2d_main  drop-in for the Euler/HLLC driver
 """
 from __future__ import annotations
 
@@ -114,7 +115,7 @@ def build(verbose: bool = False, force: bool = False) -> Path:
 
 
 # host programs linked against the library (rpath $ORIGIN: they sit beside it)
-MAINS = [("main_mhd2d.cpp", "cc_mhd2d_main")]
+MAINS = [("main_mhd2d.cpp", "cc_mhd2d_main"), ("main_euler2d.cpp", "cc_euler2d_main")]
 
 
 def build_mains(verbose: bool = False) -> list[Path]:

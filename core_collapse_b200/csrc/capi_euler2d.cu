@@ -29,6 +29,7 @@ struct Euler2dBase {
     virtual int rk2_step(double dt) = 0;
     virtual int advance(int nsteps, double* t) = 0;
     virtual int diagnostics(cc_diag* d) = 0;
+    virtual int derived(double* const* out) = 0;
 };
 
 template <class T> struct Euler2d : Euler2dBase {
@@ -46,6 +47,7 @@ template <class T> struct Euler2d : Euler2dBase {
     unsigned int* bar = nullptr;
     long long* steps_dev = nullptr;
     int* iflags = nullptr;   // active, barrier error, SOR sweeps, bad dt
+    double* derived_dev = nullptr;   // 3 planes of Nx*Ny, allocated at the first cc_euler2d_derived
     bool loaded = false;
     cudaGraphExec_t graph1 = nullptr;
     cudaStream_t graph_stream = nullptr;
@@ -63,7 +65,7 @@ template <class T> struct Euler2d : Euler2dBase {
     ~Euler2d() override {
         if (graph1) cudaGraphExecDestroy(graph1);
         void* ptrs[] = {block, phi, g2[0], g2[1], rhs, sphi, sor_part, sor_part2, staging, spd_part, rho_part,
-                        diag_part, scal, bar, steps_dev, iflags};
+                        diag_part, scal, bar, steps_dev, iflags, derived_dev};
         for (void* q : ptrs)
             if (q) cudaFree(q);
     }
@@ -308,6 +310,19 @@ template <class T> struct Euler2d : Euler2dBase {
         return check_flags();
     }
 
+    int derived(double* const* out) override {
+        if (!loaded) return fail(h, CC_ERR_STATE, "no state uploaded");
+        const size_t n = (size_t)p.Nx * p.Ny;
+        if (!derived_dev) CC_CUDA(cudaMalloc(&derived_dev, sizeof(double) * n * 3));
+        CC_CUDA(EHLaunch<T>::derived(c, U, derived_dev, st()));
+        count(1);
+        for (int k = 0; k < 3; k++)
+            if (out[k])
+                CC_CUDA(cudaMemcpyAsync(out[k], derived_dev + k * n, sizeof(double) * n, cudaMemcpyDeviceToHost, st()));
+        CC_CUDA(cudaStreamSynchronize(st()));
+        return CC_OK;
+    }
+
     int diagnostics(cc_diag* d) override {
         if (!loaded) return fail(h, CC_ERR_STATE, "no state uploaded");
         CC_CUDA(EHLaunch<T>::diag(c, U, diag_part, st()));
@@ -430,6 +445,13 @@ int cc_euler2d_diagnostics(cc_handle* h, cc_diag* d) {
     if (!m || !d) return CC_ERR_ARG;
     if (int r = set_dev(h)) return r;
     return m->diagnostics(d);
+}
+
+int cc_euler2d_derived(cc_handle* h, double* const* out) {
+    Euler2dBase* m = eh(h);
+    if (!m || !out) return CC_ERR_ARG;
+    if (int r = set_dev(h)) return r;
+    return m->derived(out);
 }
 
 }  // extern "C"

@@ -42,4 +42,12 @@ cudaError_t EHLaunch<T>::diag(const EHConst<T>& c, const EHFields<T>& st, double
     return cudaGetLastError();
 }
 
+template <class T>
+cudaError_t EHLaunch<T>::derived(const EHConst<T>& c, const EHFields<T>& st, double* out, cudaStream_t s) {
+    size_t g = ((size_t)c.nx * c.ny + 255) / 256;
+    if (g > 4096) g = 4096;
+    eh_derived_kernel<T><<<(int)g, 256, 0, s>>>(c, st, out);
+    return cudaGetLastError();
+}
+
 }  // namespace ccb

@@ -242,6 +242,26 @@ eh_rho_sum_kernel(const EHConst<T> c, const T* __restrict__ rho, double* __restr
     if (threadIdx.x == 0) rho_part[blockIdx.x] = bs;
 }
 
+// Snapshot fields of the reference main()'s store (EH:661-689): out[0..2] =
+// rho, P, Mach per cell (3 planes of nx*ny doubles): floors on a copy of the
+// cell, cons_to_prim_full, Mach = |v| / a (0 where a <= 0).
+template <class T>
+__global__ void eh_derived_kernel(const EHConst<T> c, const EHFields<T> s, double* __restrict__ out) {
+    const size_t n = (size_t)c.nx * c.ny;
+    for (size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += (size_t)gridDim.x * blockDim.x) {
+        const size_t q = (k / c.nx) * c.pitch + (k % c.nx);
+        T rho = s.rho[q], E = s.E[q];
+        const T mx = s.mx[q], my = s.my[q];
+        eh_floors(c, rho, mx, my, E);
+        T a;
+        const EPrim<T> W = eh_prim(c, rho, mx, my, E, &a);
+        const T vmag = sqrt(W.u * W.u + W.v * W.v);
+        out[k] = rho;
+        out[n + k] = W.P;
+        out[2 * n + k] = (a > T(0.0)) ? (vmag / a) : T(0.0);
+    }
+}
+
 template <class T, int NT>
 __global__ void __launch_bounds__(NT) eh_diag_kernel(const EHConst<T> c, const EHFields<T> s, double* __restrict__ part) {
     __shared__ double sh[NT / 32];

@@ -18,6 +18,8 @@ template <class T> struct EHLaunch {
                               cudaStream_t s);
     static cudaError_t rho_sum(const EHConst<T>& c, const T* rho, double* rho_part, cudaStream_t s);
     static cudaError_t diag(const EHConst<T>& c, const EHFields<T>& st, double* part, cudaStream_t s);
+    // rho, P, Mach of the reference's snapshot store, out: 3 planes of nx*ny doubles
+    static cudaError_t derived(const EHConst<T>& c, const EHFields<T>& st, double* out, cudaStream_t s);
 };
 
 }  // namespace ccb

@@ -31,67 +31,13 @@
 
 #include "../../include/cc_ic.h"
 #include "../../include/cc_step.h"
+#include "npy_out.h"
 
 namespace {
 
+using namespace ccmain;
+
 const char* const FIELD_NAMES[10] = {"rho", "P", "Mach", "u", "v", "vabs", "Bx", "By", "Bz", "divB"};
-
-// NumPy .npy v1.0 header for little-endian float64 of the given shape, padded
-// with spaces to 128 bytes so that it can be rewritten in place.
-std::string npy_header(const std::vector<long long>& shape) {
-    std::string dict = "{'descr': '<f8', 'fortran_order': False, 'shape': (";
-    for (size_t k = 0; k < shape.size(); k++) {
-        dict += std::to_string(shape[k]);
-        dict += (shape.size() == 1) ? "," : (k + 1 < shape.size() ? ", " : "");
-    }
-    dict += "), }";
-    const size_t total = 128, pre = 10;
-    while (pre + dict.size() + 1 < total) dict += ' ';
-    dict += '\n';
-    std::string h = "\x93NUMPY";
-    h += (char)1;
-    h += (char)0;
-    const uint16_t len = (uint16_t)dict.size();
-    h += (char)(len & 0xff);
-    h += (char)(len >> 8);
-    return h + dict;
-}
-
-bool write_npy(const std::string& path, const std::vector<long long>& shape, const double* data, size_t n) {
-    FILE* f = std::fopen(path.c_str(), "wb");
-    if (!f) return false;
-    const std::string h = npy_header(shape);
-    bool ok = std::fwrite(h.data(), 1, h.size(), f) == h.size();
-    ok = ok && std::fwrite(data, sizeof(double), n, f) == n;
-    return std::fclose(f) == 0 && ok;
-}
-
-// A (Nt, Ny, Nx) field file appended one snapshot at a time.
-struct SeriesFile {
-    FILE* f = nullptr;
-    long long nt = 0, ny = 0, nx = 0;
-    bool open(const std::string& path, int ny_, int nx_) {
-        ny = ny_;
-        nx = nx_;
-        f = std::fopen(path.c_str(), "wb");
-        if (!f) return false;
-        const std::string h = npy_header({0, ny, nx});
-        return std::fwrite(h.data(), 1, h.size(), f) == h.size();
-    }
-    bool append(const double* d) {
-        const size_t n = (size_t)(ny * nx);
-        if (std::fwrite(d, sizeof(double), n, f) != n) return false;
-        nt++;
-        return true;
-    }
-    bool finish() {
-        const std::string h = npy_header({nt, ny, nx});
-        bool ok = std::fseek(f, 0, SEEK_SET) == 0 && std::fwrite(h.data(), 1, h.size(), f) == h.size();
-        ok = (std::fclose(f) == 0) && ok;
-        f = nullptr;
-        return ok;
-    }
-};
 
 int check(cc_handle* h, int r, const char* what) {
     if (r != CC_OK) std::fprintf(stderr, "%s failed (%d): %s\n", what, r, h ? cc_last_error(h) : "");
@@ -167,7 +113,7 @@ int main(int argc, char** argv) {
     mkdir(out.c_str(), 0755);   // an existing directory is fine
     SeriesFile series[10];
     for (int k = 0; k < 10; k++)
-        if (!series[k].open(out + "/" + FIELD_NAMES[k] + ".npy", Ny, Nx)) {
+        if (!series[k].open(out + "/" + FIELD_NAMES[k] + ".npy", {Ny, Nx})) {
             std::fprintf(stderr, "cannot write %s/%s.npy\n", out.c_str(), FIELD_NAMES[k]);
             return 1;
         }

@@ -129,6 +129,7 @@ class Euler2dSolver:
 
     def upload(self, s: StateEH):
         self._check(self._lib.cc_euler2d_upload(self._h, *[_dp(a) for a in s.arrays()]))
+        self._t = 0.0
 
     def download(self, s: StateEH | None = None) -> StateEH:
         if s is None:
@@ -151,14 +152,25 @@ class Euler2dSolver:
         self._check(self._lib.cc_euler2d_rk2_step(self._h, float(dt)))
 
     def advance(self, nsteps: int, t: float | None = None) -> float:
-        tt = C.c_double(0.0 if t is None else t)
+        """nsteps of the main loop from time t (None: where the last advance or
+        upload (t = 0) left the clock); returns the time."""
+        tt = C.c_double(getattr(self, "_t", 0.0) if t is None else t)
         self._check(self._lib.cc_euler2d_advance(self._h, int(nsteps), C.byref(tt)))
+        self._t = tt.value
         return tt.value
 
     def diagnostics(self) -> dict:
         d = L.CcDiag()
         self._check(self._lib.cc_euler2d_diagnostics(self._h, C.byref(d)))
         return {f: getattr(d, f) for f, _ in L.CcDiag._fields_}
+
+    def derived(self) -> dict:
+        """The reference main()'s snapshot fields (EH:661-689): {rho, P, Mach}, each (Ny, Nx)."""
+        n = self.p.Nx * self.p.Ny
+        out = [np.empty(n) for _ in range(3)]
+        arr = (C.POINTER(C.c_double) * 3)(*[a.ctypes.data_as(L._DP) for a in out])
+        self._check(self._lib.cc_euler2d_derived(self._h, arr))
+        return {k: a.reshape(self.p.Ny, self.p.Nx) for k, a in zip(("rho", "P", "Mach"), out)}
 
 
 def compute_dt(p: ParamsEH, U: StateEH) -> float:

@@ -275,6 +275,11 @@ int cc_euler2d_rk2_step(cc_handle* h, double dt);
  * the reference aborts, EH:699-702), the state then being the last good one. */
 int cc_euler2d_advance(cc_handle* h, int nsteps, double* t);
 int cc_euler2d_diagnostics(cc_handle* h, cc_diag* d);
+/* The fields the reference main() stores per snapshot (euler2d_gravity_hllc.cpp:661-689):
+ * out[0..2] = rho, P, Mach (Nx*Ny doubles each; NULL entries skipped), from a
+ * floored copy of each cell; Mach = |v| / a, 0 where a <= 0.  The first call
+ * allocates 3*Nx*Ny doubles of device scratch for the handle. */
+int cc_euler2d_derived(cc_handle* h, double* const* out);
 
 /* ---- spectral gravity without device allocation ----
  * No counterpart in the reference: an addition for callers that cannot call

@@ -387,6 +387,12 @@ int or_euler2d_rhs(const cc_euler2d_params* c, const double* const* f, double* c
     return 0;
 }
 
+void or_euler2d_derived(const cc_euler2d_params* c, const double* const* f, double* const* out) {
+    EHState<double> s;
+    loadE(c, f, s);
+    EH<double>(ehpar(c)).derived(s, out);
+}
+
 double or_euler2d_compute_dt(const cc_euler2d_params* c, const double* const* f) {
     EHState<double> s;
     loadE(c, f, s);

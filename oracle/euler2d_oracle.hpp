@@ -54,6 +54,20 @@ public:
         if (a_out) *a_out = std::sqrt(T(p.gamma) * P / r);
         return {vmax(rho, T(p.floor_rho)), u, v, P};
     }
+    // the main()'s snapshot store (EH:661-689): out = rho, P, Mach per cell
+    void derived(const EHState<T>& s, double* const* out) const {
+        const size_t n = (size_t)p.nx * p.ny;
+        for (size_t q = 0; q < n; q++) {
+            T rho = s.rho[q], mx = s.mx[q], my = s.my[q], E = s.E[q];
+            floors(rho, mx, my, E);
+            T a;
+            const EPrim<T> W = to_prim(rho, mx, my, E, &a);
+            const T vmag = std::sqrt(W.u * W.u + W.v * W.v);
+            out[0][q] = (double)rho;
+            out[1][q] = (double)W.P;
+            out[2][q] = (a > T(0.0)) ? (double)(vmag / a) : 0.0;
+        }
+    }
     // prim_to_cons (EH:102-109)
     void to_cons(const EPrim<T>& W, T& r, T& mx, T& my, T& E) const {
         r = vmax(W.r, T(p.floor_rho));

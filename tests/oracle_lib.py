@@ -57,6 +57,8 @@ def oracle() -> C.CDLL:
         O.or_euler2d_rhs.argtypes = [PE, _PP, _PP, C.c_int]
         O.or_euler2d_compute_dt.argtypes = [PE, _PP]
         O.or_euler2d_compute_dt.restype = C.c_double
+        O.or_euler2d_derived.argtypes = [PE, _PP, _PP]
+        O.or_euler2d_derived.restype = None
         O.or_euler2d_rk2_step.argtypes = [PE, _PP, C.c_double, C.c_int]
         O.or_euler2d_main_loop.argtypes = [PE, _PP, C.c_int, _DP, C.c_int, C.c_int]
         P3 = C.POINTER(L.CcMhd3dParams)

@@ -148,3 +148,20 @@ def test_odd_extent_with_gravity_is_rejected():
     with pytest.raises(CcError) as e:
         Euler2dSolver(p)
     assert e.value.code == L.CC_ERR_UNSUPPORTED
+
+
+@pytest.mark.parametrize("name", sorted(CASES_EH))
+def test_derived_fields_match_oracle(name):
+    """cc_euler2d_derived == the reference main()'s snapshot store (EH:661-689)
+    bit for bit in FP64; the cases hold cold cells, so the floors act."""
+    p, s = make_case_eh(name)
+    cp = p.to_c()
+    S = [a.copy() for a in s.arrays()]
+    n = p.Nx * p.Ny
+    want = [np.empty(n) for _ in range(3)]
+    O.oracle().or_euler2d_derived(C.byref(cp), O.pp(S), O.pp(want))
+    with Euler2dSolver(p) as g:
+        g.upload(s)
+        got = g.derived()
+    for k, name_k in enumerate(("rho", "P", "Mach")):
+        assert np.array_equal(got[name_k].ravel(), want[k]), f"{name} {name_k}"

@@ -73,3 +73,35 @@ def test_main_restart_continues_from_checkpoint(tmp_path):
     assert B["t"][-1] <= 2 * T_END and len(B["t"]) >= 2
     for k in DERIVED_FIELDS:
         assert np.array_equal(B[k][0], want[k]), k
+
+
+EXE_EH = EXE.parent / "cc_euler2d_main"
+
+
+def test_euler_main_matches_wrapper_loop(tmp_path):
+    """cc_euler2d_main (the reference main() of euler2d_gravity_hllc.cpp,
+    EH:645-737): its snapshots equal the same loop driven through the Python
+    wrapper, bit for bit."""
+    from core_collapse_b200.euler2d import Euler2dSolver, ParamsEH, ic_random_blob
+    out = tmp_path / "eh"
+    r = subprocess.run([str(EXE_EH), "--Nx", "32", "--Ny", "32", "--t_end", "0.01", "--dt_store", "0.004",
+                        "--out", str(out)], capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr
+    got = {k: np.load(out / f"{k}.npy") for k in ("x", "y", "t", "rho", "P", "Mach")}
+    p = ParamsEH(Nx=32, Ny=32, t_end=0.01, dt_store=0.004)
+    ts, snaps = [0.0], []
+    with Euler2dSolver(p) as s:
+        s.upload(ic_random_blob(p))
+        snaps.append(s.derived())
+        t, next_store = 0.0, p.dt_store
+        while t < p.t_end - 1e-14:
+            t = s.advance(1)
+            if t + 1e-14 >= next_store or t >= p.t_end - 1e-14:
+                ts.append(t)
+                snaps.append(s.derived())
+                next_store += p.dt_store
+    assert np.array_equal(got["t"], np.array(ts)) and got["x"].shape == (32,)
+    for k in ("rho", "P", "Mach"):
+        assert got[k].shape == (len(ts), 32, 32)
+        for n, snap in enumerate(snaps):
+            assert np.array_equal(got[k][n], snap[k]), f"{k} snapshot {n}"
