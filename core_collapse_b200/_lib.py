@@ -90,6 +90,14 @@ class CcPerf(C.Structure):
     ]
 
 
+class CcIc3Knobs(C.Structure):
+    _fields_ = [
+        ("rho_bg", C.c_double), ("rho_core", C.c_double), ("r_core", C.c_double), ("r_edge", C.c_double),
+        ("P0", C.c_double), ("vin", C.c_double), ("rot_omega", C.c_double),
+        ("B0x", C.c_double), ("B0z", C.c_double), ("Bshear", C.c_double),
+    ]
+
+
 class CcIcKnobs(C.Structure):
     _fields_ = [
         ("rho_bg", C.c_double), ("rho_core", C.c_double), ("r_core", C.c_double), ("r_edge", C.c_double),
@@ -142,6 +150,7 @@ SIGNATURES = {
     "cc_mhd3d_rk2_step": (C.c_int, [_H, C.c_double]),
     "cc_mhd3d_advance": (C.c_int, [_H, C.c_int, _DP]),
     "cc_mhd3d_diagnostics": (C.c_int, [_H, C.POINTER(CcDiag)]),
+    "cc_mhd3d_derived": (C.c_int, [_H, C.POINTER(C.POINTER(C.c_double))]),
     "cc_euler2d_params_default": (None, [C.POINTER(CcEuler2dParams)]),
     "cc_euler2d_create": (C.c_int, [C.POINTER(CcEuler2dParams), C.POINTER(_H)]),
     "cc_euler2d_upload": (C.c_int, [_H] + [_DP] * 4),
@@ -154,6 +163,8 @@ SIGNATURES = {
     "cc_euler2d_derived": (C.c_int, [_H, C.POINTER(C.POINTER(C.c_double))]),
     "cc_mhd2d_ic_knobs_default": (None, [C.POINTER(CcIcKnobs)]),
     "cc_ic_mhd2d_reference": (C.c_int, [C.POINTER(CcMhd2dParams), C.POINTER(CcIcKnobs), C.POINTER(_DP)]),
+    "cc_mhd3d_ic_knobs_default": (None, [C.POINTER(CcIc3Knobs)]),
+    "cc_ic_mhd3d_reference": (C.c_int, [C.POINTER(CcMhd3dParams), C.POINTER(CcIc3Knobs), C.POINTER(_DP)]),
     "cc_ic_mhd2d_collapse": (C.c_int, [C.POINTER(CcMhd2dParams), C.c_double, C.c_double, C.c_double, C.c_uint32,
                                        C.c_double, C.c_double, C.c_double, C.POINTER(_DP)]),
     "cc_ic_mhd2d_orszag_tang": (C.c_int, [C.POINTER(CcMhd2dParams), C.c_double, C.c_double, C.POINTER(_DP)]),

@@ -11,6 +11,8 @@ Translation units and their floating-point contract:
                                      direct Poisson solve, reproducible on the CPU
   capi_adjoint.cu                    -fmad=false: the adjoint kernels recompute FP64
                                      forward intermediates and must round like them
+  ic3d.cu                            -fmad=false: host IC of the 3D driver through the
+                                     solver's EOS functions
   mhd2d_f32.cu, mhd3d_f32.cu,
   euler2d_f32.cu, batch_f32.cu       FMA contraction on, approximate FP32 division
                                      and square root, flush-to-zero (the FP32 bulk path)
@@ -18,6 +20,7 @@ Translation units and their floating-point contract:
 and the host programs of MAINS (g++, linked against the library):
   main_mhd2d.cpp -> cc_mhd2d_main    drop-in for the reference's 2D MHD driver
   main_euler2d.cpp -> cc_euler2d_main  drop-in for the Euler/HLLC driver
+  main_mhd3d.cpp -> cc_mhd3d_main    drop-in for the 3D MHD driver
 """
 from __future__ import annotations
 
@@ -47,6 +50,7 @@ UNITS = [
     ("batch_common.cu", ["-fmad=false"]),
     ("dpoisson.cu", ["-fmad=false"]),
     ("capi_adjoint.cu", ["-fmad=false"]),
+    ("ic3d.cu", ["-fmad=false"]),
     # FP32 bulk path: approximate division/sqrt (<= 2 ulp), denormals flushed
     ("mhd2d_f32.cu", ["-prec-div=false", "-prec-sqrt=false", "-ftz=true"]),
     ("mhd3d_f32.cu", ["-prec-div=false", "-prec-sqrt=false", "-ftz=true"]),
@@ -115,7 +119,8 @@ def build(verbose: bool = False, force: bool = False) -> Path:
 
 
 # host programs linked against the library (rpath $ORIGIN: they sit beside it)
-MAINS = [("main_mhd2d.cpp", "cc_mhd2d_main"), ("main_euler2d.cpp", "cc_euler2d_main")]
+MAINS = [("main_mhd2d.cpp", "cc_mhd2d_main"), ("main_euler2d.cpp", "cc_euler2d_main"),
+         ("main_mhd3d.cpp", "cc_mhd3d_main")]
 
 
 def build_mains(verbose: bool = False) -> list[Path]:

@@ -13,6 +13,7 @@
 #include <vector>
 
 #include "handle.h"
+#include "mhd3d_const.h"
 #include "mhd3d_launch.h"
 
 using namespace ccb;
@@ -28,6 +29,7 @@ struct Mhd3dBase {
     virtual int rk2_step(double dt) = 0;
     virtual int advance(int nsteps, double* t) = 0;
     virtual int diagnostics(cc_diag* d) = 0;
+    virtual int derived(double* const* out) = 0;
 };
 
 template <class T> struct Mhd3d : Mhd3dBase {
@@ -47,6 +49,7 @@ template <class T> struct Mhd3d : Mhd3dBase {
     double* scal = nullptr;   // dt, t
     long long* steps_dev = nullptr;
     int* iflags = nullptr;    // active
+    double* derived_dev = nullptr;   // 11 planes of Nx*Ny*Nz, allocated at the first cc_mhd3d_derived
     int cur = 0;
     bool loaded = false;
     bool partials_valid = false;
@@ -65,37 +68,14 @@ template <class T> struct Mhd3d : Mhd3dBase {
 
     ~Mhd3d() override {
         if (graph3) cudaGraphExecDestroy(graph3);
-        void* ptrs[] = {block, staging, spd_part, rho_part, diag_part, scal, steps_dev, iflags};
+        void* ptrs[] = {block, staging, spd_part, rho_part, diag_part, scal, steps_dev, iflags, derived_dev};
         for (void* q : ptrs)
             if (q) cudaFree(q);
     }
 
     int init() override {
         const int nx = p.Nx, ny = p.Ny, nz = p.Nz;
-        const double dx = (p.x1 - p.x0) / nx, dy = (p.y1 - p.y0) / ny, dz = (p.z1 - p.z0) / nz;
-        // EOS constants; the powers at rho_nuc / rho_bounce use the host's std::pow,
-        // as the reference evaluates them on every call (M3:120, 129-130, 135-137)
-        const double K2 = p.K1 * std::pow(p.rho_nuc, p.gamma1 - p.gamma2);
-        c.g1 = (T)p.gamma1; c.g2 = (T)p.gamma2; c.K1 = (T)p.K1; c.K2 = (T)K2; c.rn = (T)p.rho_nuc;
-        c.gth = (T)p.gamma_th; c.rb = (T)p.rho_bounce; c.gb = (T)p.gamma_bounce; c.Kb = (T)p.Kbounce;
-        c.g1m1 = (T)(p.gamma1 - 1.0); c.g2m1 = (T)(p.gamma2 - 1.0); c.gbm1 = (T)(p.gamma_bounce - 1.0);
-        c.gthm1 = (T)(p.gamma_th - 1.0);
-        c.e1n = (T)(p.K1 * std::pow(p.rho_nuc, p.gamma1 - 1.0) / (p.gamma1 - 1.0));
-        c.e2n = (T)(K2 * std::pow(p.rho_nuc, p.gamma2 - 1.0) / (p.gamma2 - 1.0));
-        c.pbb = (T)std::pow(p.rho_bounce, p.gamma_bounce);
-        c.ebb = (T)std::pow(p.rho_bounce, p.gamma_bounce - 1.0);
-        c.cold_off = (p.K1 == 0.0 && p.Kbounce == 0.0) ? 1 : 0;
-        c.floor_rho = (T)p.floor_rho; c.floor_P = (T)p.floor_P; c.eta = (T)p.eta;
-        c.dx = (T)dx; c.dy = (T)dy; c.dz = (T)dz;
-        c.inv_dx = (T)(1.0 / dx); c.inv_dy = (T)(1.0 / dy); c.inv_dz = (T)(1.0 / dz);
-        c.two_dx = (T)(2.0 * dx); c.two_dy = (T)(2.0 * dy); c.two_dz = (T)(2.0 * dz);
-        c.nx = nx; c.ny = ny; c.nz = nz;
-        c.P = ((nx + 1 + 31) / 32) * 32;
-        c.PS = (long long)c.P * (ny + 1);
-        c.ax = AxisMap{nx, p.periodic_x ? 1 : 0};
-        c.ay = AxisMap{ny, p.periodic_y ? 1 : 0};
-        c.az = AxisMap{nz, p.periodic_z ? 1 : 0};
-        c.resistive = (p.eta > 0.0) ? 1 : 0;
+        c = m3_make_const<T>(p);
         vol = (size_t)c.PS * (nz + 1);
 
         // 3 states x 8 + primitives 8 + 3 x 7 face data + 3 edge arrays = 56 fields
@@ -295,6 +275,18 @@ template <class T> struct Mhd3d : Mhd3dBase {
         return CC_OK;
     }
 
+    int derived(double* const* out) override {
+        if (!loaded) return fail(h, CC_ERR_STATE, "no state uploaded");
+        const size_t n = (size_t)p.Nx * p.Ny * p.Nz;
+        if (!derived_dev) CC_CUDA(cudaMalloc(&derived_dev, sizeof(double) * n * 11));
+        CC_CUDA(M3Launch<T>::derived(c, buf[cur], derived_dev, st()));
+        for (int k = 0; k < 11; k++)
+            if (out[k])
+                CC_CUDA(cudaMemcpyAsync(out[k], derived_dev + k * n, sizeof(double) * n, cudaMemcpyDeviceToHost, st()));
+        CC_CUDA(cudaStreamSynchronize(st()));
+        return CC_OK;
+    }
+
     int diagnostics(cc_diag* d) override {
         if (!loaded) return fail(h, CC_ERR_STATE, "no state uploaded");
         CC_CUDA(M3Launch<T>::diag(c, buf[cur], diag_part, st()));
@@ -416,6 +408,13 @@ int cc_mhd3d_diagnostics(cc_handle* h, cc_diag* d) {
     if (!m || !d) return CC_ERR_ARG;
     if (int r = set_dev(h)) return r;
     return m->diagnostics(d);
+}
+
+int cc_mhd3d_derived(cc_handle* h, double* const* out) {
+    Mhd3dBase* m = m3(h);
+    if (!m || !out) return CC_ERR_ARG;
+    if (int r = set_dev(h)) return r;
+    return m->derived(out);
 }
 
 }  // extern "C"

@@ -76,6 +76,14 @@ cudaError_t M3Launch<T>::diag(const M3Const<T>& c, const Fields3<T>& s, double* 
 }
 
 template <class T>
+cudaError_t M3Launch<T>::derived(const M3Const<T>& c, const Fields3<T>& s, double* out, cudaStream_t st) {
+    size_t g = ((size_t)c.nx * c.ny * c.nz + 255) / 256;
+    if (g > 8192) g = 8192;
+    m3_derived_kernel<T><<<(int)g, 256, 0, st>>>(c, s, out);
+    return cudaGetLastError();
+}
+
+template <class T>
 cudaError_t M3Launch<T>::pack_in(const double* src, T* dst, int w, int h, int d, int P, long long PS, cudaStream_t st) {
     pack3_in_kernel<T><<<grid3((long long)w * h * d), 256, 0, st>>>(src, dst, w, h, d, P, PS);
     return cudaGetLastError();

@@ -387,6 +387,33 @@ __global__ void __launch_bounds__(NT) m3_diag_kernel(const M3Const<T> c, const F
     if (threadIdx.x == 0) { part[5 * gridDim.x + blockIdx.x] = bm; part[6 * gridDim.x + blockIdx.x] = bn; }
 }
 
+// Snapshot fields of the reference main()'s store (M3:1293-1321), in its
+// order: rho, P, Mach, u, v, w, vabs, Bx, By, Bz (cell-centred, from the
+// faces), div B; out: 11 planes of nx*ny*nz doubles, x fastest.
+// cs = sqrt(sound_speed2) (hybrid EOS), Mach = |v| / max(cs, 1e-12); div B in FP64.
+template <class T>
+__global__ void m3_derived_kernel(const M3Const<T> c, const Fields3<T> s, double* __restrict__ out) {
+    const size_t n = (size_t)c.nx * c.ny * c.nz;
+    CC_FOR3(c.nx, c.ny, c.nz) {
+        const int i = (int)(t_ % c.nx), j = (int)((t_ / c.nx) % c.ny), k = (int)(t_ / ((long long)c.nx * c.ny));
+        const size_t q = c.idx(i, j, k), o = (size_t)t_;
+        const T Bx = T(0.5) * (s.bx[q] + s.bx[c.idx(i + 1, j, k)]);
+        const T By = T(0.5) * (s.by[q] + s.by[c.idx(i, j + 1, k)]);
+        const T Bz = T(0.5) * (s.bz[q] + s.bz[c.idx(i, j, k + 1)]);
+        const Prim<T> W = to_prim(c, s.rho[q], s.mx[q], s.my[q], s.mz[q], s.E[q], Bx, By, Bz);
+        const T cs = sqrt(sound_speed2(c, W));
+        const T vabs = sqrt(W.u * W.u + W.v * W.v + W.w * W.w);
+        const T mach = vabs / vmax(cs, T(1e-12));
+        const double div = ((double)s.bx[c.idx(i + 1, j, k)] - (double)s.bx[q]) / (double)c.dx +
+                           ((double)s.by[c.idx(i, j + 1, k)] - (double)s.by[q]) / (double)c.dy +
+                           ((double)s.bz[c.idx(i, j, k + 1)] - (double)s.bz[q]) / (double)c.dz;
+        const double v[11] = {(double)W.r, (double)W.P, (double)mach, (double)W.u, (double)W.v, (double)W.w,
+                              (double)vabs, (double)W.bx, (double)W.by, (double)W.bz, div};
+#pragma unroll
+        for (int m = 0; m < 11; m++) out[m * n + o] = v[m];
+    }
+}
+
 // host layout (x fastest, w x h x d) <-> pitched 3D field
 template <class T>
 __global__ void pack3_in_kernel(const double* __restrict__ src, T* __restrict__ dst, int w, int h, int d, int P,

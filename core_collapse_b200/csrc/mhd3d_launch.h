@@ -25,6 +25,8 @@ template <class T> struct M3Launch {
                                cudaStream_t st);
     static cudaError_t speeds(const M3Const<T>& c, const Fields3<T>& s, double* spd_part, cudaStream_t st);
     static cudaError_t diag(const M3Const<T>& c, const Fields3<T>& s, double* part, cudaStream_t st);
+    // the 11 snapshot fields of the reference's store, out: 11 planes of nx*ny*nz doubles
+    static cudaError_t derived(const M3Const<T>& c, const Fields3<T>& s, double* out, cudaStream_t st);
     static cudaError_t pack_in(const double* src, T* dst, int w, int h, int d, int P, long long PS, cudaStream_t st);
     static cudaError_t pack_out(const T* src, double* dst, int w, int h, int d, int P, long long PS, cudaStream_t st);
 };

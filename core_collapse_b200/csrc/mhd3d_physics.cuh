@@ -32,7 +32,7 @@ template <class T> struct ColdEos { T P, e, g; };
 // finite power, i.e. exactly 0, and the adiabatic index is gamma1, gamma2, or
 // 0 above rho_bounce (0 / floor_P); the shortcut returns those bits directly.
 template <class T>
-__device__ __forceinline__ ColdEos<T> eos_cold(const M3Const<T>& c, T rho) {
+__host__ __device__ __forceinline__ ColdEos<T> eos_cold(const M3Const<T>& c, T rho) {
     rho = vmax(rho, c.floor_rho);
     ColdEos<T> r;
     if (c.cold_off) {
@@ -64,7 +64,7 @@ __device__ __forceinline__ ColdEos<T> eos_cold(const M3Const<T>& c, T rho) {
 
 // pressure_from_rho_espec (M3:146-152)
 template <class T>
-__device__ __forceinline__ T eos_pressure(const M3Const<T>& c, T rho, T e_spec) {
+__host__ __device__ __forceinline__ T eos_pressure(const M3Const<T>& c, T rho, T e_spec) {
     rho = vmax(rho, c.floor_rho);
     const ColdEos<T> cd = eos_cold(c, rho);
     const T eth = vmax(T(0.0), e_spec - cd.e);
@@ -74,7 +74,7 @@ __device__ __forceinline__ T eos_pressure(const M3Const<T>& c, T rho, T e_spec) 
 
 // total_energy_from_prim (M3:154-163)
 template <class T>
-__device__ __forceinline__ T energy(const M3Const<T>& c, const Prim<T>& W) {
+__host__ __device__ __forceinline__ T energy(const M3Const<T>& c, const Prim<T>& W) {
     const T rho = vmax(W.r, c.floor_rho);
     const T kin = T(0.5) * rho * (W.u * W.u + W.v * W.v + W.w * W.w);
     const T mag = T(0.5) * (W.bx * W.bx + W.by * W.by + W.bz * W.bz);
@@ -87,7 +87,7 @@ __device__ __forceinline__ T energy(const M3Const<T>& c, const Prim<T>& W) {
 
 // enforce_floors (M3:165-183): always re-projects E through the EOS
 template <class T>
-__device__ __forceinline__ void floors(const M3Const<T>& c, T& rho, T mx, T my, T mz, T& E, T Bx, T By, T Bz) {
+__host__ __device__ __forceinline__ void floors(const M3Const<T>& c, T& rho, T mx, T my, T mz, T& E, T Bx, T By, T Bz) {
     rho = vmax(rho, c.floor_rho);
     const T u = mx / rho, v = my / rho, w = mz / rho;
     const T kin = T(0.5) * rho * (u * u + v * v + w * w);
@@ -106,7 +106,7 @@ __device__ __forceinline__ void floors(const M3Const<T>& c, T& rho, T mx, T my, 
 
 // cons_to_prim (M3:185-197)
 template <class T>
-__device__ __forceinline__ Prim<T> to_prim(const M3Const<T>& c, T rho, T mx, T my, T mz, T E, T Bx, T By, T Bz) {
+__host__ __device__ __forceinline__ Prim<T> to_prim(const M3Const<T>& c, T rho, T mx, T my, T mz, T E, T Bx, T By, T Bz) {
     rho = vmax(rho, c.floor_rho);
     const T u = mx / rho, v = my / rho, w = mz / rho;
     const T kin = T(0.5) * rho * (u * u + v * v + w * w);
@@ -119,6 +119,16 @@ __device__ __forceinline__ Prim<T> to_prim(const M3Const<T>& c, T rho, T mx, T m
     Prim<T> W;
     W.r = rho; W.u = u; W.v = v; W.w = w; W.P = P; W.bx = Bx; W.by = By; W.bz = Bz;
     return W;
+}
+
+// sound_speed2 (M3:206-212): (gamma_cold Pcold + gamma_th Pth) / rho, >= 0
+template <class T>
+__host__ __device__ __forceinline__ T sound_speed2(const M3Const<T>& c, const Prim<T>& W) {
+    const T rhof = vmax(W.r, c.floor_rho);
+    const ColdEos<T> cd = eos_cold(c, rhof);
+    const T Pth = vmax(T(0.0), W.P - cd.P);
+    const T num = cd.g * cd.P + c.gth * Pth;
+    return vmax(T(0.0), num / rhof);
 }
 
 // fast magnetosonic speed with the hybrid sound speed (M3:206-248)

@@ -113,6 +113,26 @@ def _dp(a: np.ndarray):
     return a.ctypes.data_as(L._DP)
 
 
+# output order of the reference's snapshot store (M3:1309-1319)
+DERIVED3_FIELDS = ("rho", "P", "Mach", "u", "v", "w", "vabs", "Bx", "By", "Bz", "divB")
+
+
+def ic_reference3(p: Params3, **knobs) -> State3:
+    """The 3D reference main()'s core-collapse IC (M3:1159-1272); knobs
+    override cc_mhd3d_ic_knobs_default (rho_bg, rho_core, r_core, r_edge, P0,
+    vin, rot_omega, B0x, B0z, Bshear)."""
+    s = empty_state3(p)
+    k = L.CcIc3Knobs()
+    L.lib().cc_mhd3d_ic_knobs_default(C.byref(k))
+    for name, v in knobs.items():
+        setattr(k, name, float(v))
+    arr = (C.POINTER(C.c_double) * 8)(*[_dp(a) for a in s.arrays()])
+    cp = p.to_c()
+    if L.lib().cc_ic_mhd3d_reference(C.byref(cp), C.byref(k), arr) != 0:
+        raise ValueError("cc_ic_mhd3d_reference rejected its arguments")
+    return s
+
+
 class Mhd3dSolver:
     """A device-resident 3D MHD instance (one libcc_b200 handle)."""
 
@@ -154,6 +174,7 @@ class Mhd3dSolver:
 
     def upload(self, s: State3):
         self._check(self._lib.cc_mhd3d_upload(self._h, *[_dp(a) for a in s.arrays()]))
+        self._t = 0.0
 
     def download(self, s: State3 | None = None) -> State3:
         if s is None:
@@ -170,8 +191,11 @@ class Mhd3dSolver:
         self._check(self._lib.cc_mhd3d_rk2_step(self._h, float(dt)))
 
     def advance(self, nsteps: int, t: float | None = None) -> float:
-        tt = C.c_double(0.0 if t is None else t)
+        """nsteps of the main loop from time t (None: where the last advance or
+        upload (t = 0) left the clock); returns the time."""
+        tt = C.c_double(getattr(self, "_t", 0.0) if t is None else t)
         self._check(self._lib.cc_mhd3d_advance(self._h, int(nsteps), C.byref(tt)))
+        self._t = tt.value
         return tt.value
 
     def set_stream(self, stream_ptr: int | None):
@@ -192,6 +216,14 @@ class Mhd3dSolver:
         d = L.CcDiag()
         self._check(self._lib.cc_mhd3d_diagnostics(self._h, C.byref(d)))
         return {f: getattr(d, f) for f, _ in L.CcDiag._fields_}
+
+    def derived(self) -> dict:
+        """The reference main()'s snapshot fields (M3:1293-1321), each (Nz, Ny, Nx)."""
+        n = self.p.Nx * self.p.Ny * self.p.Nz
+        out = [np.empty(n) for _ in DERIVED3_FIELDS]
+        arr = (C.POINTER(C.c_double) * 11)(*[_dp(a) for a in out])
+        self._check(self._lib.cc_mhd3d_derived(self._h, arr))
+        return {k: a.reshape(self.p.Nz, self.p.Ny, self.p.Nx) for k, a in zip(DERIVED3_FIELDS, out)}
 
 
 # ---- drop-in functions with the reference's signatures (M3:626, 1034) ----

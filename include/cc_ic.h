@@ -45,6 +45,23 @@ int cc_ic_mhd2d_collapse(const cc_mhd2d_params* p, double core_amp, double core_
  *   B0 = 1/sqrt(4 pi) on corners (div B = 0 to roundoff). */
 int cc_ic_mhd2d_orszag_tang(const cc_mhd2d_params* p, double core_amp, double core_width, double* const* f);
 
+/* IC knobs of the 3D reference main() (mhd3d_resistive_hlld_ct.cpp:77-88) */
+typedef struct cc_mhd3d_ic_knobs {
+    double rho_bg, rho_core, r_core, r_edge, P0, vin, rot_omega;
+    double B0x, B0z, Bshear;
+} cc_mhd3d_ic_knobs;
+
+void cc_mhd3d_ic_knobs_default(cc_mhd3d_ic_knobs* k);
+
+/* The 3D reference main()'s core-collapse IC (M3:1159-1272): corner vector
+ * potential Az = Bshear core(r) sin(2 pi X) sin(2 pi Y) -> Bx_f = dAz/dy + B0x,
+ * By_f = -dAz/dx, Bz_f = B0z; tanh core, P = P0 (rho/rho_bg)^gamma_init,
+ * infall + rotation; cells through the hybrid-EOS prim_to_cons and
+ * enforce_floors.  f = {rho, mx, my, mz, E, Bx_f, By_f, Bz_f} in the 3D
+ * reference layouts (cells Nx*Ny*Nz, Bx_f (Nx+1)*Ny*Nz, By_f Nx*(Ny+1)*Nz,
+ * Bz_f Nx*Ny*(Nz+1), x fastest). */
+int cc_ic_mhd3d_reference(const cc_mhd3d_params* p, const cc_mhd3d_ic_knobs* k, double* const* f);
+
 /* The Euler/HLLC main()'s IC, init_random_blob (euler2d_gravity_hllc.cpp:574-642):
  * std::mt19937(42), per cell two uniform(0,1) draws (density and pressure
  * noise) then two uniform(-1,1) draws (velocity); Gaussian density bump.

@@ -253,6 +253,12 @@ int cc_mhd3d_rk2_step(cc_handle* h, double dt);
 int cc_mhd3d_advance(cc_handle* h, int nsteps, double* t);
 /* FP64 sums and max |div B| (mhd3d_resistive_hlld_ct.cpp:1070-1078) */
 int cc_mhd3d_diagnostics(cc_handle* h, cc_diag* d);
+/* The fields the reference main() stores per snapshot (mhd3d_resistive_hlld_ct.cpp:1293-1321):
+ * out[0..10] = rho, P, Mach, u, v, w, vabs, Bx, By, Bz, divB (Nx*Ny*Nz doubles
+ * each, x fastest; NULL entries skipped); B cell-centred from the faces,
+ * Mach with the hybrid-EOS sound speed.  The first call allocates
+ * 11*Nx*Ny*Nz doubles of device scratch for the handle. */
+int cc_mhd3d_derived(cc_handle* h, double* const* out);
 
 /* ---- 2D Euler + self-gravity, HLLC (euler2d_gravity_hllc.cpp) ---- */
 

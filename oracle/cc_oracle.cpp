@@ -359,6 +359,12 @@ int or_mhd3d_main_loop(const cc_mhd3d_params* c, double* const* f, int nsteps, d
     return fp32 ? main_loop3<float>(c, f, nsteps, t) : main_loop3<double>(c, f, nsteps, t);
 }
 
+void or_mhd3d_derived(const cc_mhd3d_params* c, const double* const* f, double* const* out) {
+    M3State<double> s;
+    load3(c, f, s);
+    M3<double>(m3par(c)).derived(s, out);
+}
+
 double or_mhd3d_divB_max(const cc_mhd3d_params* c, const double* const* f) {
     M3State<double> s;
     load3(c, f, s);

@@ -385,6 +385,27 @@ public:
         return vmin(dt_h, dt_r);
     }
 
+    // the main()'s snapshot store (M3:1293-1321): out[0..10] = rho, P, Mach,
+    // u, v, w, vabs, Bx, By, Bz, divB per cell
+    void derived(const M3State<T>& s, double* const* out) const {
+        for (int k = 0; k < p.nz; k++)
+            for (int j = 0; j < p.ny; j++)
+                for (int i = 0; i < p.nx; i++) {
+                    const size_t q = cid(i, j, k);
+                    const Prim8<T> W = to_prim(s.rho[q], s.mx[q], s.my[q], s.mz[q], s.E[q], bx_cc(s, i, j, k),
+                                               by_cc(s, i, j, k), bz_cc(s, i, j, k));
+                    const T cs = osqrt(a2(W));
+                    const T vabs = osqrt(W.u * W.u + W.v * W.v + W.w * W.w);
+                    const T mach = vabs / vmax(cs, T(1e-12));
+                    const double d = ((double)bxf(s, i + 1, j, k) - (double)bxf(s, i, j, k)) / p.dx() +
+                                     ((double)byf(s, i, j + 1, k) - (double)byf(s, i, j, k)) / p.dy() +
+                                     ((double)bzf(s, i, j, k + 1) - (double)bzf(s, i, j, k)) / p.dz();
+                    const double v[11] = {(double)W.r, (double)W.P, (double)mach, (double)W.u, (double)W.v,
+                                          (double)W.w, (double)vabs, (double)W.bx, (double)W.by, (double)W.bz, d};
+                    for (int m = 0; m < 11; m++) out[m][q] = v[m];
+                }
+    }
+
     double max_divB(const M3State<T>& s) const {  // M3:1070-1078
         double m = 0.0;
         for (int k = 0; k < p.nz; k++)

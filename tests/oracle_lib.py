@@ -69,6 +69,8 @@ def oracle() -> C.CDLL:
         O.or_mhd3d_main_loop.argtypes = [P3, _PP, C.c_int, _DP, C.c_int]
         O.or_mhd3d_divB_max.argtypes = [P3, _PP]
         O.or_mhd3d_divB_max.restype = C.c_double
+        O.or_mhd3d_derived.argtypes = [P3, _PP, _PP]
+        O.or_mhd3d_derived.restype = None
         O.or_mhd2d_tlm.argtypes = [C.POINTER(L.CcMhd2dParams), _PP, _PP, C.c_int, _DP]
         O.or_poisson_generic.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, C.c_double, C.c_double, C.c_double,
                                          C.c_double, C.c_int, C.c_double, C.c_int, C.c_double, C.c_int, _DP, _DP,

@@ -105,3 +105,35 @@ def test_euler_main_matches_wrapper_loop(tmp_path):
         assert got[k].shape == (len(ts), 32, 32)
         for n, snap in enumerate(snaps):
             assert np.array_equal(got[k][n], snap[k]), f"{k} snapshot {n}"
+
+
+EXE_3D = EXE.parent / "cc_mhd3d_main"
+
+
+def test_mhd3d_main_matches_wrapper_loop(tmp_path):
+    """cc_mhd3d_main (the reference main() of mhd3d_resistive_hlld_ct.cpp): the
+    reference IC, the loop and its store rule (no frame at t = 0); snapshots equal
+    the same loop driven through the Python wrapper, bit for bit."""
+    from core_collapse_b200.mhd3d import DERIVED3_FIELDS, Mhd3dSolver, Params3, ic_reference3
+    out = tmp_path / "m3"
+    n, t_end, dts = 16, 0.004, 0.0015
+    r = subprocess.run([str(EXE_3D), "--Nx", str(n), "--Ny", str(n), "--Nz", str(n), "--t_end", str(t_end),
+                        "--dt_store", str(dts), "--out", str(out)], capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr
+    got = {k: np.load(out / f"{k}.npy") for k in ("x", "y", "z", "t", *DERIVED3_FIELDS)}
+    p = Params3(Nx=n, Ny=n, Nz=n, t_end=t_end, dt_store=dts)
+    ts, snaps = [], []
+    with Mhd3dSolver(p) as s:
+        s.upload(ic_reference3(p))
+        t, tnext = 0.0, 0.0
+        while t < p.t_end:
+            t = s.advance(1)
+            if t >= tnext - 1e-12:
+                ts.append(t)
+                snaps.append(s.derived())
+                tnext += p.dt_store
+    assert np.array_equal(got["t"], np.array(ts)) and got["z"].shape == (n,)
+    for k in DERIVED3_FIELDS:
+        assert got[k].shape == (len(ts), n, n, n)
+        for m, snap in enumerate(snaps):
+            assert np.array_equal(got[k][m], snap[k]), f"{k} snapshot {m}"

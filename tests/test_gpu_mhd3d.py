@@ -112,3 +112,27 @@ def test_divB_roundoff_and_fp32():
     for k, (a, b) in enumerate(zip(got, ref64)):
         l1 = np.sum(np.abs(a - b)) / np.sum(np.abs(b))
         assert l1 < 1e-5, f"FP32 {FIELDS[k]} L1 {l1:.2e}"
+
+
+@pytest.mark.parametrize("name", sorted(CASES3))
+def test_derived_fields_match_oracle(name):
+    """cc_mhd3d_derived == the reference main()'s snapshot store (M3:1293-1321):
+    bit for bit on the ideal-gas cases, 1e-12 where the hybrid EOS's pow runs on
+    the device."""
+    from core_collapse_b200.mhd3d import DERIVED3_FIELDS
+    p, s = make_case3(name)
+    cp = p.to_c()
+    S = [a.copy() for a in s.arrays()]
+    n = p.Nx * p.Ny * p.Nz
+    want = [np.empty(n) for _ in range(11)]
+    O.oracle().or_mhd3d_derived(C.byref(cp), O.pp(S), O.pp(want))
+    with Mhd3dSolver(p) as g:
+        g.upload(s)
+        got = g.derived()
+    for k, fname in enumerate(DERIVED3_FIELDS):
+        a = got[fname].ravel()
+        if _ideal(name):
+            assert np.array_equal(a, want[k]), f"{name} {fname}"
+        else:
+            scale = np.max(np.abs(want[k])) + 1e-300
+            assert np.max(np.abs(a - want[k])) <= 1e-12 * scale, f"{name} {fname}"
