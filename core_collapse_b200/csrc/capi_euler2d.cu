@@ -6,6 +6,8 @@
 // Poisson(U) -> phi; stage 1: U1 = floors(U + dt rhs(U));
 // Poisson(U1) -> phi; stage 2: U = floors(0.5 U + 0.5 (U1 + dt rhs(U1)));
 // t += dt.  The Poisson solve floors the density and always wraps (EH:300-317).
+#include <algorithm>
+#include <utility>
 #include <cmath>
 #include <cstring>
 #include <memory>
@@ -48,6 +50,12 @@ template <class T> struct Euler2d : Euler2dBase {
     long long* steps_dev = nullptr;
     int* iflags = nullptr;   // active, barrier error, SOR sweeps, bad dt
     double* derived_dev = nullptr;   // 3 planes of Nx*Ny, allocated at the first cc_euler2d_derived
+    // enclosed-mass gravity: cells in radius order, each one's group end, scan scratch
+    int* enc_order = nullptr;
+    int* enc_gend = nullptr;
+    double* enc_cum = nullptr;
+    double* enc_blk = nullptr;
+    bool enclosed() const { return p.gravity_on && p.poisson_kind == CC_GRAVITY_ENCLOSED; }
     bool loaded = false;
     cudaGraphExec_t graph1 = nullptr;
     cudaStream_t graph_stream = nullptr;
@@ -65,7 +73,8 @@ template <class T> struct Euler2d : Euler2dBase {
     ~Euler2d() override {
         if (graph1) cudaGraphExecDestroy(graph1);
         void* ptrs[] = {block, phi, g2[0], g2[1], rhs, sphi, sor_part, sor_part2, staging, spd_part, rho_part,
-                        diag_part, scal, bar, steps_dev, iflags, derived_dev};
+                        diag_part, scal, bar, steps_dev, iflags, derived_dev, enc_order, enc_gend, enc_cum,
+                        enc_blk};
         for (void* q : ptrs)
             if (q) cudaFree(q);
     }
@@ -86,9 +95,10 @@ template <class T> struct Euler2d : Euler2dBase {
         c.gravity_on = p.gravity_on ? 1 : 0;
         plane = (size_t)P * (ny + 1);
         if (p.gravity_on) {
-            if (p.poisson_kind != CC_POISSON_SOR)
-                return fail(h, CC_ERR_UNSUPPORTED, "the Euler/HLLC solver supports the SOR Poisson solve only");
-            if ((nx & 1) || (ny & 1)) return fail(h, CC_ERR_UNSUPPORTED, "red-black SOR needs even Nx and Ny (periodic)");
+            if (p.poisson_kind != CC_POISSON_SOR && p.poisson_kind != CC_GRAVITY_ENCLOSED)
+                return fail(h, CC_ERR_UNSUPPORTED, "the Euler/HLLC solver supports SOR or enclosed-mass gravity");
+            if (p.poisson_kind == CC_POISSON_SOR && ((nx & 1) || (ny & 1)))
+                return fail(h, CC_ERR_UNSUPPORTED, "red-black SOR needs even Nx and Ny (periodic)");
         }
         CC_CUDA(EHLaunch<T>::prepare());
         CC_CUDA(cudaMalloc(&block, sizeof(T) * plane * 8));
@@ -98,6 +108,13 @@ template <class T> struct Euler2d : Euler2dBase {
         U1 = EHFields<T>{b + 4 * plane, b + 5 * plane, b + 6 * plane, b + 7 * plane};
         CC_CUDA(cudaMalloc(&phi, sizeof(T) * plane));
         CC_CUDA(cudaMemsetAsync(phi, 0, sizeof(T) * plane, st()));
+        if (enclosed()) {   // gravity arrays written by every solve, the radius order built once
+            CC_CUDA(cudaMalloc(&g2[0], sizeof(T) * plane));
+            CC_CUDA(cudaMalloc(&g2[1], sizeof(T) * plane));
+            CC_CUDA(cudaMemsetAsync(g2[0], 0, sizeof(T) * plane, st()));
+            CC_CUDA(cudaMemsetAsync(g2[1], 0, sizeof(T) * plane, st()));
+            if (int r = enclosed_setup()) return r;
+        }
         CC_CUDA(cudaMalloc(&staging, sizeof(double) * (size_t)(nx + 1) * (ny + 1)));
         CC_CUDA(cudaMalloc(&spd_part, sizeof(double) * RED_BLOCKS));
         CC_CUDA(cudaMalloc(&rho_part, sizeof(double) * RED_BLOCKS));
@@ -149,9 +166,62 @@ template <class T> struct Euler2d : Euler2dBase {
         return CC_OK;
     }
 
-    // Poisson on a density field whose floored sum is in rho_part -> phi
+    // radius order of the cells and each one's group end (compute_enclosed_mass_gravity,
+    // EH:241-269): the radii depend only on the grid, so they are sorted once
+    int enclosed_setup() {
+        const int nx = p.Nx, ny = p.Ny, n = nx * ny;
+        const double dx = (p.x1 - p.x0) / nx, dy = (p.y1 - p.y0) / ny;
+        const double cx = 0.5 * (p.x0 + p.x1), cy = 0.5 * (p.y0 + p.y1);
+        std::vector<std::pair<double, int>> cells;
+        cells.reserve(n);
+        for (int j = 0; j < ny; ++j) {
+            const double y = p.y0 + (j + 0.5) * dy;
+            for (int i = 0; i < nx; ++i) {
+                const double x = p.x0 + (i + 0.5) * dx;
+                const double rx = x - cx, ry = y - cy;
+                cells.emplace_back(std::sqrt(rx * rx + ry * ry), j * nx + i);
+            }
+        }
+        std::sort(cells.begin(), cells.end(),
+                  [](const std::pair<double, int>& a, const std::pair<double, int>& b) { return a.first < b.first; });
+        std::vector<int> order(n), gend(n);
+        int s = 0;
+        while (s < n) {
+            const double r0 = cells[s].first;
+            int e = s + 1;
+            while (e < n && cells[e].first <= r0 + 1e-12) ++e;
+            for (int t = s; t < e; ++t) { order[t] = cells[t].second; gend[t] = e; }
+            s = e;
+        }
+        const int nb = (n + ENC_NT - 1) / ENC_NT;
+        CC_CUDA(cudaMalloc(&enc_order, sizeof(int) * n));
+        CC_CUDA(cudaMalloc(&enc_gend, sizeof(int) * n));
+        CC_CUDA(cudaMalloc(&enc_cum, sizeof(double) * n));
+        CC_CUDA(cudaMalloc(&enc_blk, sizeof(double) * nb));
+        CC_CUDA(cudaMemcpyAsync(enc_order, order.data(), sizeof(int) * n, cudaMemcpyHostToDevice, st()));
+        CC_CUDA(cudaMemcpyAsync(enc_gend, gend.data(), sizeof(int) * n, cudaMemcpyHostToDevice, st()));
+        CC_CUDA(cudaStreamSynchronize(st()));   // the host vectors go out of scope
+        return CC_OK;
+    }
+
+    // gravity arrays of the stage kernel: g2 in the enclosed-mass mode, none for SOR (phi)
+    const T* gxa() const { return enclosed() ? g2[0] : nullptr; }
+    const T* gya() const { return enclosed() ? g2[1] : nullptr; }
+
+    // Poisson on a density field whose floored sum is in rho_part -> phi;
+    // in the enclosed-mass mode the gravity itself -> g2
     int solve(const T* rho) {
         if (!p.gravity_on) return CC_OK;
+        if (enclosed()) {
+            h->perf.poisson_solves += 1;
+            const int nx = p.Nx, ny = p.Ny;
+            const double dx = (p.x1 - p.x0) / nx, dy = (p.y1 - p.y0) / ny;
+            CC_CUDA(EHLaunch<T>::enclosed(c, rho, enc_order, enc_gend, nx * ny, enc_cum, enc_blk, p.x0, p.y0, dx,
+                                          dy, 0.5 * (p.x0 + p.x1), 0.5 * (p.y0 + p.y1), p.G,
+                                          p.softening * p.softening, p.floor_rho, g2[0], g2[1], active(), st()));
+            count(3);
+            return CC_OK;
+        }
         h->perf.poisson_solves += 1;
         const int nx = p.Nx, ny = p.Ny;
         CC_CUDA(M2Launch<T>::sor_rhs(rho, nx, ny, P, rho_part, 4.0 * M_PI * p.G, p.floor_rho, rhs, active(), st()));
@@ -195,15 +265,19 @@ template <class T> struct Euler2d : Euler2dBase {
         int one = 1;
         CC_CUDA(cudaMemcpyAsync(iflags, &one, sizeof(int), cudaMemcpyHostToDevice, st()));
         if (p.gravity_on) {
-            CC_CUDA(EHLaunch<T>::rho_sum(c, U.rho, rho_part, st()));
-            count(1);
+            if (!enclosed()) {
+                CC_CUDA(EHLaunch<T>::rho_sum(c, U.rho, rho_part, st()));
+                count(1);
+            }
             if (int r = solve(U.rho)) return r;
         }
         if (!g2[0]) {
             CC_CUDA(cudaMalloc(&g2[0], sizeof(T) * plane));
             CC_CUDA(cudaMalloc(&g2[1], sizeof(T) * plane));
         }
-        if (p.gravity_on) {
+        if (enclosed()) {
+            // g2 holds the enclosed-mass gravity from solve()
+        } else if (p.gravity_on) {
             CC_CUDA(M2Launch<T>::gravity_from_phi(phi, nx, ny, P, c.pax, c.pay, c.two_dx, c.two_dy, g2[0], g2[1], st()));
             count(1);
         } else {
@@ -232,18 +306,22 @@ template <class T> struct Euler2d : Euler2dBase {
     // rk2_step (EH:529-550) with dt in dt_dev; the RHS solves Poisson itself (EH:411)
     int step_body() {
         if (p.gravity_on) {
-            CC_CUDA(EHLaunch<T>::rho_sum(c, U.rho, rho_part, st()));
-            count(1);
+            if (!enclosed()) {   // the SOR's density mean
+                CC_CUDA(EHLaunch<T>::rho_sum(c, U.rho, rho_part, st()));
+                count(1);
+            }
             if (int r = solve(U.rho)) return r;
         }
-        CC_CUDA(EHLaunch<T>::stage(c, U, U, U1, false, phi, dt_dev(), active(), st()));
+        CC_CUDA(EHLaunch<T>::stage(c, U, U, U1, false, phi, gxa(), gya(), dt_dev(), active(), st()));
         count(1);
         if (p.gravity_on) {
-            CC_CUDA(EHLaunch<T>::rho_sum(c, U1.rho, rho_part, st()));
-            count(1);
+            if (!enclosed()) {
+                CC_CUDA(EHLaunch<T>::rho_sum(c, U1.rho, rho_part, st()));
+                count(1);
+            }
             if (int r = solve(U1.rho)) return r;
         }
-        CC_CUDA(EHLaunch<T>::stage(c, U, U1, U, true, phi, dt_dev(), active(), st()));
+        CC_CUDA(EHLaunch<T>::stage(c, U, U1, U, true, phi, gxa(), gya(), dt_dev(), active(), st()));
         count(1);
         h->perf.steps += 1;
         return CC_OK;

@@ -14,12 +14,29 @@ cudaError_t EHLaunch<T>::prepare() {
 
 template <class T>
 cudaError_t EHLaunch<T>::stage(const EHConst<T>& c, const EHFields<T>& un, const EHFields<T>& in,
-                               const EHFields<T>& out, bool stage2, const T* phi, const double* dt, const int* active,
-                               cudaStream_t s) {
+                               const EHFields<T>& out, bool stage2, const T* phi, const T* gxa, const T* gya,
+                               const double* dt, const int* active, cudaStream_t s) {
     using G = EHGeom<T>;
     dim3 grid((c.nx + G::TX - 1) / G::TX, (c.ny + G::TY - 1) / G::TY);
-    if (stage2) eh_stage_kernel<T, true><<<grid, G::NT, G::smem, s>>>(c, un, in, out, phi, dt, active);
-    else eh_stage_kernel<T, false><<<grid, G::NT, G::smem, s>>>(c, un, in, out, phi, dt, active);
+    if (stage2) eh_stage_kernel<T, true><<<grid, G::NT, G::smem, s>>>(c, un, in, out, phi, gxa, gya, dt, active);
+    else eh_stage_kernel<T, false><<<grid, G::NT, G::smem, s>>>(c, un, in, out, phi, gxa, gya, dt, active);
+    return cudaGetLastError();
+}
+
+template <class T>
+cudaError_t EHLaunch<T>::enclosed(const EHConst<T>& c, const T* rho, const int* order, const int* gend, int n,
+                                  double* cum, double* blk, double x0, double y0, double dx, double dy, double cx,
+                                  double cy, double G, double soft2, double floor_rho, T* gx, T* gy,
+                                  const int* active, cudaStream_t s) {
+    const int nb = (n + ENC_NT - 1) / ENC_NT;
+    enc_scan_kernel<T><<<nb, ENC_NT, 0, s>>>(rho, c.pitch, c.nx, order, n, floor_rho, dx * dy, cum, blk, active);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    enc_blocks_kernel<<<1, ENC_NT, 0, s>>>(blk, nb, active);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    const int g = nb < 4096 ? nb : 4096;
+    enc_gravity_kernel<T><<<g, ENC_NT, 0, s>>>(order, gend, cum, blk, n, c.nx, c.pitch, x0, y0, dx, dy, cx, cy, G,
+                                               soft2, gx, gy, active);
     return cudaGetLastError();
 }
 

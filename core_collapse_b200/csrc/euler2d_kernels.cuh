@@ -112,7 +112,8 @@ template <class T> struct EHGeom {
 template <class T, bool STAGE2>
 __global__ void __launch_bounds__(EHGeom<T>::NT, 2)
 eh_stage_kernel(const EHConst<T> c, const EHFields<T> un, const EHFields<T> in, const EHFields<T> out,
-                const T* __restrict__ phi, const double* __restrict__ dtp, const int* __restrict__ active) {
+                const T* __restrict__ phi, const T* __restrict__ gxa, const T* __restrict__ gya,
+                const double* __restrict__ dtp, const int* __restrict__ active) {
     using G = EHGeom<T>;
     constexpr int TX = G::TX, TY = G::TY, HALO = G::HALO, RX = G::RX, RR = G::RR, NT = G::NT;
     constexpr int NFX = G::NFX, NGY = G::NGY;
@@ -184,10 +185,16 @@ eh_stage_kernel(const EHConst<T> c, const EHFields<T> un, const EHFields<T> in, 
         d[m] = -(fx[m * NFX + kx + 1] - fx[m * NFX + kx]) / c.dx - (gy[m * NGY + ky + TX] - gy[m * NGY + ky]) / c.dy;
     const T r0 = in.rho[q], mx0 = in.mx[q], my0 = in.my[q], E0 = in.E[q];
     if (c.gravity_on) {
-        const int iE = c.pax.cell(gi + 1), iW = c.pax.cell(gi - 1);
-        const int jN = c.pay.cell(gj + 1), jS = c.pay.cell(gj - 1);
-        const T gxq = -(phi[(size_t)gj * P + iE] - phi[(size_t)gj * P + iW]) / c.two_dx;
-        const T gyq = -(phi[(size_t)jN * P + gi] - phi[(size_t)jS * P + gi]) / c.two_dy;
+        T gxq, gyq;
+        if (gxa) {   // gravity given as arrays (enclosed-mass gravity)
+            gxq = gxa[q];
+            gyq = gya[q];
+        } else {
+            const int iE = c.pax.cell(gi + 1), iW = c.pax.cell(gi - 1);
+            const int jN = c.pay.cell(gj + 1), jS = c.pay.cell(gj - 1);
+            gxq = -(phi[(size_t)gj * P + iE] - phi[(size_t)gj * P + iW]) / c.two_dx;
+            gyq = -(phi[(size_t)jN * P + gi] - phi[(size_t)jS * P + gi]) / c.two_dy;
+        }
         const T rho = vmax(r0, c.floor_rho);
         const T u = mx0 / rho, v = my0 / rho;
         d[1] += rho * gxq;

@@ -3,6 +3,7 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include "enclosed_kernels.cuh"
 #include "euler2d_kernels.cuh"
 #include "mhd2d_launch.h"
 
@@ -11,9 +12,17 @@ namespace ccb {
 template <class T> struct EHLaunch {
     static cudaError_t prepare();
     // stage 1: out = floors(in + dt rhs(in)); stage 2: out = floors(0.5 un + 0.5 (in + dt rhs(in)))
+    // gravity: gxa/gya (pitched arrays) when non-null, else the centred gradient of phi
     static cudaError_t stage(const EHConst<T>& c, const EHFields<T>& un, const EHFields<T>& in,
-                             const EHFields<T>& out, bool stage2, const T* phi, const double* dt, const int* active,
-                             cudaStream_t s);
+                             const EHFields<T>& out, bool stage2, const T* phi, const T* gxa, const T* gya,
+                             const double* dt, const int* active, cudaStream_t s);
+    // enclosed-mass gravity (enclosed_kernels.cuh) of rho into gx, gy; order / gend: the
+    // cells in radius order and each one's group end (host set-up), cum n doubles,
+    // blk ceil(n / ENC_NT) doubles of scratch
+    static cudaError_t enclosed(const EHConst<T>& c, const T* rho, const int* order, const int* gend, int n,
+                                double* cum, double* blk, double x0, double y0, double dx, double dy, double cx,
+                                double cy, double G, double soft2, double floor_rho, T* gx, T* gy, const int* active,
+                                cudaStream_t s);
     static cudaError_t speeds(const EHConst<T>& c, const EHFields<T>& st, double* spd_part, double* rho_part,
                               cudaStream_t s);
     static cudaError_t rho_sum(const EHConst<T>& c, const T* rho, double* rho_part, cudaStream_t s);

@@ -41,7 +41,7 @@ class ParamsEH:
     softening: float = 1e-4
     sor_tol: float = 1e-10
     sor_omega: float = 1.7
-    poisson: str = "sor"
+    poisson: str = "sor"       # or "enclosed": enclosed-mass radial gravity (EH:226-286)
     precision: str = "fp64"
 
     def to_c(self) -> L.CcEuler2dParams:
@@ -51,7 +51,8 @@ class ParamsEH:
                 continue
             v = getattr(self, f.name)
             setattr(c, f.name, int(v) if isinstance(v, bool) else v)
-        c.poisson_kind = {"sor": L.CC_POISSON_SOR, "fft": L.CC_POISSON_FFT}[self.poisson]
+        c.poisson_kind = {"sor": L.CC_POISSON_SOR, "fft": L.CC_POISSON_FFT,
+                          "enclosed": L.CC_GRAVITY_ENCLOSED}[self.poisson]
         c.precision = {"fp64": L.CC_FP64, "fp32": L.CC_FP32}[self.precision]
         return c
 

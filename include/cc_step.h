@@ -50,6 +50,8 @@ extern "C" {
 #define CC_POISSON_SOR 0   /* red-black SOR (GPU-parallel ordering of M2's SOR) */
 #define CC_POISSON_FFT 1   /* spectral periodic solve, power-of-two grids */
 #define CC_POISSON_DIRECT 2 /* exact solve of the SOR's discrete problem (batched ensemble, cc_batch.h) */
+#define CC_GRAVITY_ENCLOSED 3 /* Euler/HLLC only: enclosed-mass radial gravity, compute_enclosed_mass_gravity
+                                 (euler2d_gravity_hllc.cpp:226-286, the rhs's commented-out alternative, EH:411) */
 
 typedef struct cc_handle cc_handle;
 

@@ -8,6 +8,7 @@
 //   mode 3  direct solve of the SOR's discrete problem, density mean in the
 //           batched reduction order (the library's ensemble Poisson)
 #include <cstring>
+#include <algorithm>
 #include <vector>
 
 #include "../include/cc_step.h"
@@ -143,12 +144,58 @@ PoissonSpec ehspec(const cc_euler2d_params* c) {
     return s;
 }
 
+// compute_enclosed_mass_gravity (EH:226-286): cells sorted by distance from
+// the domain centre, ties within 1e-12 of a group's first radius grouped,
+// enclosed mass summed in sorted order up to the end of each group,
+// g = -G M_enc / (r^2 + softening^2) along r-hat.
+void enclosed_mass_gravity(const cc_euler2d_params* c, const std::vector<double>& rho, std::vector<double>& gx,
+                           std::vector<double>& gy) {
+    const int nx = c->Nx, ny = c->Ny;
+    gx.assign((size_t)nx * ny, 0.0);
+    gy.assign((size_t)nx * ny, 0.0);
+    const double dx = (c->x1 - c->x0) / nx, dy = (c->y1 - c->y0) / ny;
+    const double cx = 0.5 * (c->x0 + c->x1), cy = 0.5 * (c->y0 + c->y1);
+    struct Cell { double r; size_t k; double m, x, y; };
+    std::vector<Cell> cells;
+    cells.reserve((size_t)nx * ny);
+    for (int j = 0; j < ny; ++j) {
+        const double y = c->y0 + (j + 0.5) * dy;
+        for (int i = 0; i < nx; ++i) {
+            const double x = c->x0 + (i + 0.5) * dx;
+            const size_t k = (size_t)j * nx + i;
+            const double rx = x - cx, ry = y - cy;
+            cells.push_back({std::sqrt(rx * rx + ry * ry), k, std::max(rho[k], c->floor_rho) * dx * dy, x, y});
+        }
+    }
+    std::sort(cells.begin(), cells.end(), [](const Cell& a, const Cell& b) { return a.r < b.r; });
+    double menc = 0.0;
+    size_t s = 0;
+    while (s < cells.size()) {
+        const double r0 = cells[s].r;
+        size_t e = s + 1;
+        while (e < cells.size() && cells[e].r <= r0 + 1e-12) ++e;
+        for (size_t t = s; t < e; ++t) menc += cells[t].m;
+        for (size_t t = s; t < e; ++t) {
+            const double rx = cells[t].x - cx, ry = cells[t].y - cy;
+            const double r2 = rx * rx + ry * ry + c->softening * c->softening;
+            const double r = std::sqrt(r2);
+            if (r > 0.0) {
+                const double gmag = -c->G * menc / r2;
+                gx[cells[t].k] = gmag * (rx / r);
+                gy[cells[t].k] = gmag * (ry / r);
+            }
+        }
+        s = e;
+    }
+}
+
 PoissonResult eh_gravity(const cc_euler2d_params* c, const std::vector<double>& rho, std::vector<double>& gx,
                          std::vector<double>& gy, int mode) {
     PoissonSpec s = ehspec(c);
     PoissonResult r;
     size_t N = (size_t)c->Nx * c->Ny;
     if (!c->gravity_on) { gx.assign(N, 0.0); gy.assign(N, 0.0); return r; }
+    if (c->poisson_kind == CC_GRAVITY_ENCLOSED) { enclosed_mass_gravity(c, rho, gx, gy); return r; }
     std::vector<double> phi;
     if (mode == 2) {
         std::vector<double> fr(rho.begin(), rho.end());

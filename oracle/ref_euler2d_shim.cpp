@@ -5,6 +5,7 @@
 //   rhs                               EH:406-527
 //   compute_dt                        EH:390-404
 //   compute_poisson_gravity_periodic  EH:288-386 (hard-coded omega 1.7, tol 1e-10, 50000 sweeps)
+//   compute_enclosed_mass_gravity     EH:226-286 (the rhs's commented-out alternative, EH:411)
 #include <algorithm>
 #include <array>
 #include <cmath>
@@ -80,6 +81,15 @@ int ref_euler2d_poisson(const cc_euler2d_params* c, const double* const* f, doub
     Params p = to_params(c);
     State U; load(p, f, U);
     GravField g = compute_poisson_gravity_periodic(p, U);
+    std::copy(g.gx.begin(), g.gx.end(), gx);
+    std::copy(g.gy.begin(), g.gy.end(), gy);
+    return 0;
+}
+
+int ref_euler2d_enclosed_gravity(const cc_euler2d_params* c, const double* const* f, double* gx, double* gy) {
+    Params p = to_params(c);
+    State U; load(p, f, U);
+    GravField g = compute_enclosed_mass_gravity(p, U);
     std::copy(g.gx.begin(), g.gx.end(), gx);
     std::copy(g.gy.begin(), g.gy.end(), gy);
     return 0;

@@ -112,6 +112,7 @@ def ref(name: str) -> C.CDLL | None:
             R.ref_euler2d_compute_dt.argtypes = [P2, _PP]
             R.ref_euler2d_compute_dt.restype = C.c_double
             R.ref_euler2d_poisson.argtypes = [P2, _PP, _DP, _DP]
+            R.ref_euler2d_enclosed_gravity.argtypes = [P2, _PP, _DP, _DP]
             R.ref_euler2d_init_random_blob.argtypes = [P2, _PP]
             R.ref_euler2d_main_loop.argtypes = [P2, _PP, C.c_int, _DP]
         if R is not None and name == "fft":
