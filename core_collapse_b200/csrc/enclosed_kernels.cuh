@@ -61,9 +61,11 @@ enc_scan_kernel(const T* __restrict__ rho, int pitch, int nx, const int* __restr
 
 // exclusive prefix of the nb block totals, in place (one CTA of ENC_NT threads):
 // each thread sums a contiguous run in order, the runs are scanned, each
-// thread writes its run's prefixes
+// thread writes its run's prefixes.  D = double (a template: the header is
+// included by several units)
+template <class D>
 __global__ void __launch_bounds__(ENC_NT)
-enc_blocks_kernel(double* __restrict__ blk, int nb, const int* __restrict__ active) {
+enc_blocks_kernel(D* __restrict__ blk, int nb, const int* __restrict__ active) {
     if (active && *active == 0) return;
     __shared__ double sh[ENC_NT / 32];
     const int per = (nb + ENC_NT - 1) / ENC_NT;

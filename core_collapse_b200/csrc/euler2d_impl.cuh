@@ -32,7 +32,7 @@ cudaError_t EHLaunch<T>::enclosed(const EHConst<T>& c, const T* rho, const int* 
     enc_scan_kernel<T><<<nb, ENC_NT, 0, s>>>(rho, c.pitch, c.nx, order, n, floor_rho, dx * dy, cum, blk, active);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
-    enc_blocks_kernel<<<1, ENC_NT, 0, s>>>(blk, nb, active);
+    enc_blocks_kernel<double><<<1, ENC_NT, 0, s>>>(blk, nb, active);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
     const int g = nb < 4096 ? nb : 4096;
     enc_gravity_kernel<T><<<g, ENC_NT, 0, s>>>(order, gend, cum, blk, n, c.nx, c.pitch, x0, y0, dx, dy, cx, cy, G,
