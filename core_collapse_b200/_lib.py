@@ -75,6 +75,20 @@ class CcEuler2dParams(C.Structure):
     ]
 
 
+class CcNs2dParams(C.Structure):
+    _fields_ = [
+        ("gamma", C.c_double), ("cfl", C.c_double),
+        ("x0", C.c_double), ("x1", C.c_double), ("y0", C.c_double), ("y1", C.c_double),
+        ("Nx", C.c_int32), ("Ny", C.c_int32),
+        ("t_end", C.c_double), ("dt_store", C.c_double),
+        ("seed", C.c_uint32), ("viscosity_on", C.c_int32),
+        ("floor_rho", C.c_double), ("floor_P", C.c_double),
+        ("mu", C.c_double), ("cfl_visc", C.c_double),
+        ("gravity_on", C.c_int32), ("precision", C.c_int32),
+        ("G", C.c_double),
+    ]
+
+
 class CcDiag(C.Structure):
     _fields_ = [
         ("mass", C.c_double), ("mom_x", C.c_double), ("mom_y", C.c_double), ("mom_z", C.c_double),
@@ -162,6 +176,18 @@ SIGNATURES = {
     "cc_euler2d_advance": (C.c_int, [_H, C.c_int, _DP]),
     "cc_euler2d_diagnostics": (C.c_int, [_H, C.POINTER(CcDiag)]),
     "cc_euler2d_derived": (C.c_int, [_H, C.POINTER(C.POINTER(C.c_double))]),
+    "cc_ns2d_params_default": (None, [C.POINTER(CcNs2dParams)]),
+    "cc_ns2d_create": (C.c_int, [C.POINTER(CcNs2dParams), C.POINTER(_H)]),
+    "cc_ns2d_upload": (C.c_int, [_H] + [_DP] * 4),
+    "cc_ns2d_download": (C.c_int, [_H] + [_DP] * 4),
+    "cc_ns2d_compute_dt": (C.c_int, [_H, _DP]),
+    "cc_ns2d_compute_gravity": (C.c_int, [_H, _DP, _DP, _DP]),
+    "cc_ns2d_compute_rhs": (C.c_int, [_H, C.POINTER(_DP)]),
+    "cc_ns2d_rk2_step": (C.c_int, [_H, C.c_double]),
+    "cc_ns2d_advance": (C.c_int, [_H, C.c_int, _DP]),
+    "cc_ns2d_diagnostics": (C.c_int, [_H, C.POINTER(CcDiag)]),
+    "cc_ns2d_derived": (C.c_int, [_H, C.POINTER(_DP)]),
+    "cc_ic_ns2d_collapse": (C.c_int, [C.POINTER(CcNs2dParams), C.POINTER(_DP)]),
     "cc_mhd2d_ic_knobs_default": (None, [C.POINTER(CcIcKnobs)]),
     "cc_ic_mhd2d_reference": (C.c_int, [C.POINTER(CcMhd2dParams), C.POINTER(CcIcKnobs), C.POINTER(_DP)]),
     "cc_mhd3d_ic_knobs_default": (None, [C.POINTER(CcIc3Knobs)]),

@@ -4,7 +4,7 @@
 
 Translation units and their floating-point contract:
   mhd2d_f64.cu, mhd3d_f64.cu, euler2d_f64.cu,
-  common_kernels.cu, batch_f64.cu,
+  ns2d_f64.cu, common_kernels.cu, batch_f64.cu,
   batch_common.cu, noalloc.cu        -fmad=false: FP64 kernels round exactly like
                                      the reference's x86-64 build (no FMA)
   dpoisson.cu                        -fmad=false, explicit fma() only: the batched
@@ -13,7 +13,7 @@ Translation units and their floating-point contract:
                                      forward intermediates and must round like them
   ic3d.cu                            -fmad=false: host IC of the 3D driver through the
                                      solver's EOS functions
-  mhd2d_f32.cu, mhd3d_f32.cu,
+  mhd2d_f32.cu, mhd3d_f32.cu, ns2d_f32.cu,
   euler2d_f32.cu, batch_f32.cu       FMA contraction on, approximate FP32 division
                                      and square root, flush-to-zero (the FP32 bulk path)
   capi*.cu, ic.cpp                   host code
@@ -21,6 +21,7 @@ and the host programs of MAINS (g++, linked against the library):
   main_mhd2d.cpp -> cc_mhd2d_main    drop-in for the reference's 2D MHD driver
   main_euler2d.cpp -> cc_euler2d_main  drop-in for the Euler/HLLC driver
   main_mhd3d.cpp -> cc_mhd3d_main    drop-in for the 3D MHD driver
+  main_ns2d.cpp -> cc_ns2d_main      drop-in for the Navier-Stokes driver
 """
 from __future__ import annotations
 
@@ -44,6 +45,7 @@ UNITS = [
     ("mhd2d_f64.cu", ["-fmad=false"]),
     ("mhd3d_f64.cu", ["-fmad=false"]),
     ("euler2d_f64.cu", ["-fmad=false"]),
+    ("ns2d_f64.cu", ["-fmad=false"]),
     ("common_kernels.cu", ["-fmad=false"]),
     ("noalloc.cu", ["-fmad=false"]),
     ("batch_f64.cu", ["-fmad=false"]),
@@ -55,10 +57,12 @@ UNITS = [
     ("mhd2d_f32.cu", ["-prec-div=false", "-prec-sqrt=false", "-ftz=true"]),
     ("mhd3d_f32.cu", ["-prec-div=false", "-prec-sqrt=false", "-ftz=true"]),
     ("euler2d_f32.cu", ["-prec-div=false", "-prec-sqrt=false", "-ftz=true"]),
+    ("ns2d_f32.cu", ["-prec-div=false", "-prec-sqrt=false", "-ftz=true"]),
     ("batch_f32.cu", ["-prec-div=false", "-prec-sqrt=false", "-ftz=true"]),
     ("capi.cu", []),
     ("capi_mhd3d.cu", []),
     ("capi_euler2d.cu", []),
+    ("capi_ns2d.cu", []),
     ("capi_batch.cu", []),
     ("ic.cpp", []),
 ]
@@ -120,7 +124,7 @@ def build(verbose: bool = False, force: bool = False) -> Path:
 
 # host programs linked against the library (rpath $ORIGIN: they sit beside it)
 MAINS = [("main_mhd2d.cpp", "cc_mhd2d_main"), ("main_euler2d.cpp", "cc_euler2d_main"),
-         ("main_mhd3d.cpp", "cc_mhd3d_main")]
+         ("main_mhd3d.cpp", "cc_mhd3d_main"), ("main_ns2d.cpp", "cc_ns2d_main")]
 
 
 def build_mains(verbose: bool = False) -> list[Path]:

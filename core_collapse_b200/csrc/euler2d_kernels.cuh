@@ -74,8 +74,12 @@ __device__ __forceinline__ void eh_hllc(const EHConst<T>& c, const EPrim<T>& L, 
     // euler_flux_x / euler_flux_y (EH:113-123) of the chosen side
     const bool upL = (T(0.0) <= SL), upR = !(T(0.0) <= SL) && (T(0.0) >= SR);
     const bool left = upL || (!upR && (T(0.0) < SM));
-    EPrim<T> W;   // by value: a reference chosen at run time would put L and R in local memory
+    // the chosen side's state and wave speed, by value (a reference chosen at
+    // run time would put L and R in local memory), selected before the early
+    // return (see ns_hllc in ns2d_kernels.cuh)
+    EPrim<T> W;
     W.r = left ? L.r : R.r; W.u = left ? L.u : R.u; W.v = left ? L.v : R.v; W.P = left ? L.P : R.P;
+    const T S = left ? SL : SR;
     const T Ef = W.P / c.gm1 + T(0.5) * W.r * (W.u * W.u + W.v * W.v);
     if (DIR == 0) {
         F[0] = W.r * W.u; F[1] = W.r * W.u * W.u + W.P; F[2] = W.r * W.u * W.v; F[3] = (Ef + W.P) * W.u;
@@ -84,7 +88,6 @@ __device__ __forceinline__ void eh_hllc(const EHConst<T>& c, const EPrim<T>& L, 
     }
     if (upL || upR) return;
     // star state of the chosen side (EH:147-156, 195-204)
-    const T S = left ? SL : SR;
     const T r = left ? rL : rR, E = left ? EL : ER;
     const T mx = left ? mLx : mRx, my = left ? mLy : mRy;
     const T n = DIR == 0 ? W.u : W.v, t = DIR == 0 ? W.v : W.u;

@@ -58,6 +58,7 @@ inline int fail(cc_handle* h, int code, const std::string& msg) {
 constexpr int KIND_MHD2D = 1;
 constexpr int KIND_MHD3D = 2;
 constexpr int KIND_EULER2D = 3;
+constexpr int KIND_NS2D = 4;
 
 inline int set_dev(cc_handle* h) {
     cudaError_t e = cudaSetDevice(h->device);

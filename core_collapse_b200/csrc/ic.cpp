@@ -213,4 +213,38 @@ int cc_ic_euler2d_random_blob(const cc_euler2d_params* p, double* const* f) {
     return 0;
 }
 
+int cc_ic_ns2d_collapse(const cc_ns2d_params* p, double* const* f) {
+    if (!p || !f || p->Nx < 1 || p->Ny < 1 || !f[0] || !f[1] || !f[2] || !f[3]) return -1;
+    const int nx = p->Nx, ny = p->Ny;
+    const double Lx = p->x1 - p->x0, Ly = p->y1 - p->y0;
+    const double dx = Lx / nx, dy = Ly / ny;
+    std::mt19937 rng(p->seed);
+    std::normal_distribution<double> gauss(0.0, 1.0);
+    // background, Gaussian overdensity, 1% density noise, Mach-0.05 velocity noise (NS:638-659)
+    const double rho0 = 1.0, P0 = 0.05, A = 1, sigma = 0.10 * vmind(Lx, Ly), Arho = 0.01;
+    const double a0 = std::sqrt(p->gamma * P0 / rho0), Mach0 = 0.05, vamp = Mach0 * a0;
+    const double xc = 0.5 * (p->x0 + p->x1), yc = 0.5 * (p->y0 + p->y1);
+    for (int j = 0; j < ny; ++j) {
+        const double y = p->y0 + (j + 0.5) * dy;
+        for (int i = 0; i < nx; ++i) {
+            const double x = p->x0 + (i + 0.5) * dx;
+            const double rx = x - xc, ry = y - yc, r2 = rx * rx + ry * ry;
+            const double bump = A * std::exp(-0.5 * r2 / (sigma * sigma));
+            const double noise = Arho * gauss(rng);
+            const double d0 = vmaxd(rho0 * (1.0 + bump + noise), p->floor_rho);
+            const double P = vmaxd(P0, p->floor_P);
+            const double u = vamp * gauss(rng);
+            const double v = vamp * gauss(rng);
+            // prim_to_cons (NS:134-145)
+            const double d = vmaxd(d0, p->floor_rho), Pc = vmaxd(P, p->floor_P);
+            const size_t k = (size_t)j * nx + i;
+            f[0][k] = d;
+            f[1][k] = d * u;
+            f[2][k] = d * v;
+            f[3][k] = Pc / (p->gamma - 1.0) + 0.5 * d * (u * u + v * v);
+        }
+    }
+    return 0;
+}
+
 }  // extern "C"

@@ -68,6 +68,14 @@ int cc_ic_mhd3d_reference(const cc_mhd3d_params* p, const cc_mhd3d_ic_knobs* k, 
  * f = {rho, mx, my, E}. */
 int cc_ic_euler2d_random_blob(const cc_euler2d_params* p, double* const* f);
 
+/* The Navier-Stokes main()'s collapse IC (navier_stokes_2d_hllc_poisson.cpp:627-700):
+ * std::mt19937(p->seed) + std::normal_distribution<double>(0, 1), per cell
+ * (j outer, i inner) one draw of density noise then two of velocity;
+ * rho = 1 + exp(-r^2 / (2 sigma^2)) + 0.01 N, sigma = 0.1 min(Lx, Ly),
+ * P = 0.05, u, v = 0.05 sqrt(gamma P0) N; cells through prim_to_cons
+ * (NS:134-145).  f = {rho, mx, my, E}, Nx*Ny doubles each. */
+int cc_ic_ns2d_collapse(const cc_ns2d_params* p, double* const* f);
+
 #ifdef __cplusplus
 }
 #endif

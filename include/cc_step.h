@@ -131,6 +131,31 @@ typedef struct cc_euler2d_params {
     int32_t precision;      /* addition */
 } cc_euler2d_params;
 
+/*
+ * 2D compressible Navier-Stokes (explicit viscosity) + periodic spectral
+ * self-gravity with first-order HLLC.  Fields mirror Params in
+ * navier_stokes_2d_hllc_poisson.cpp:53-85 (the HDF5 file name excepted);
+ * periodic in both directions (NS:32), Nx and Ny powers of two when
+ * gravity_on (NS:614-617).
+ */
+typedef struct cc_ns2d_params {
+    double gamma;
+    double cfl;
+    double x0, x1, y0, y1;
+    int32_t Nx, Ny;
+    double t_end;
+    double dt_store;
+    uint32_t seed;          /* 42: std::mt19937 seed of the reference IC */
+    int32_t viscosity_on;
+    double floor_rho;
+    double floor_P;
+    double mu;              /* dynamic viscosity, 1e-6 */
+    double cfl_visc;        /* explicit-diffusion CFL, 0.05 */
+    int32_t gravity_on;
+    int32_t precision;      /* addition */
+    double G;
+} cc_ns2d_params;
+
 /* Diagnostics gathered on the device (FP64 sums over cells). */
 typedef struct cc_diag {
     double mass;            /* sum rho * dV        */
@@ -288,6 +313,38 @@ int cc_euler2d_diagnostics(cc_handle* h, cc_diag* d);
  * floored copy of each cell; Mach = |v| / a, 0 where a <= 0.  The first call
  * allocates 3*Nx*Ny doubles of device scratch for the handle. */
 int cc_euler2d_derived(cc_handle* h, double* const* out);
+
+/* ---- 2D Navier-Stokes + FFT self-gravity, HLLC (navier_stokes_2d_hllc_poisson.cpp) ---- */
+
+/* Fill with the reference defaults (navier_stokes_2d_hllc_poisson.cpp:53-85). */
+void cc_ns2d_params_default(cc_ns2d_params* p);
+int cc_ns2d_create(const cc_ns2d_params* p, cc_handle** out);
+/* State {rho, rho u, rho v, E} (U4, NS:88-90): Nx*Ny doubles each, q = i + Nx*j */
+int cc_ns2d_upload(cc_handle* h, const double* rho, const double* mx, const double* my, const double* E);
+int cc_ns2d_download(cc_handle* h, double* rho, double* mx, double* my, double* E);
+/* compute_dt(U) (NS:521-546), without the loop's clamp to t_end */
+int cc_ns2d_compute_dt(cc_handle* h, double* dt);
+/* solve_poisson_periodic_fft + compute_gravity_accel (NS:285-360) on the
+ * density of cons_to_prim of the resident state (NS:372-383); phi, gx, gy
+ * (Nx*Ny each) may be NULL.  Zero fields with gravity off. */
+int cc_ns2d_compute_gravity(cc_handle* h, double* phi, double* gx, double* gy);
+/* compute_rhs(U) (NS:363-518) of the resident state: dU[0..3] = the rates of
+ * rho, rho u, rho v, E (Nx*Ny doubles each; NULL entries skipped). */
+int cc_ns2d_compute_rhs(cc_handle* h, double* const* dU);
+/* One SSP-RK2 (Heun) step of the main() loop body (NS:762-781) with this dt. */
+int cc_ns2d_rk2_step(cc_handle* h, double dt);
+/* nsteps of the main() loop body (NS:758-791) on the device: dt from
+ * compute_dt, clamped so that t does not pass t_end; once t >= t_end - 1e-14
+ * the remaining steps do nothing.  *t (if not NULL) sets the clock first and
+ * receives it after. */
+int cc_ns2d_advance(cc_handle* h, int nsteps, double* t);
+int cc_ns2d_diagnostics(cc_handle* h, cc_diag* d);
+/* The fields the reference main() stores per snapshot (NS:698-746):
+ * out[0..7] = rho, P, Mach, u, v, momx, momy, Phi (Nx*Ny doubles each; NULL
+ * entries skipped), from cons_to_prim of each cell; Mach = |v| / a, 0 where
+ * a <= 0; Phi the spectral potential of the state's density (0 with gravity
+ * off).  The first call allocates 8*Nx*Ny doubles of device scratch. */
+int cc_ns2d_derived(cc_handle* h, double* const* out);
 
 /* ---- spectral gravity without device allocation ----
  * No counterpart in the reference: an addition for callers that cannot call

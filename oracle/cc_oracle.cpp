@@ -15,6 +15,7 @@
 #include "mhd2d_oracle.hpp"
 #include "mhd3d_oracle.hpp"
 #include "euler2d_oracle.hpp"
+#include "ns2d_oracle.hpp"
 #include "poisson_oracle.hpp"
 
 namespace {
@@ -270,6 +271,43 @@ template <class T> int main_loop(const cc_mhd2d_params* c, double* const* f, int
     if (t) *t = tt;
     return 0;
 }
+// ---- 2D Navier-Stokes helpers + FFT gravity, HLLC (navier_stokes_2d_hllc_poisson.cpp) ----
+NSPar nspar(const cc_ns2d_params* c) {
+    NSPar p;
+    p.gamma = c->gamma; p.cfl = c->cfl;
+    p.x0 = c->x0; p.x1 = c->x1; p.y0 = c->y0; p.y1 = c->y1;
+    p.nx = c->Nx; p.ny = c->Ny;
+    p.floor_rho = c->floor_rho; p.floor_P = c->floor_P;
+    p.viscosity = c->viscosity_on != 0; p.mu = c->mu; p.cfl_visc = c->cfl_visc;
+    p.gravity = c->gravity_on != 0; p.G = c->G;
+    return p;
+}
+
+// the spectral potential (NS:285-328) of a density in T, solved in double
+template <class T> typename NS<T>::Potential ns_potential(const cc_ns2d_params* c) {
+    return [c](const std::vector<T>& rho, std::vector<T>& phi) {
+        PoissonSpec s{};
+        s.nx = c->Nx; s.ny = c->Ny; s.px = s.py = true;
+        s.dx = (c->x1 - c->x0) / c->Nx; s.dy = (c->y1 - c->y0) / c->Ny;
+        s.G = c->G; s.Lx = c->x1 - c->x0; s.Ly = c->y1 - c->y0;
+        std::vector<double> r(rho.begin(), rho.end()), ph;
+        fft_periodic(s, r, ph);
+        phi.assign(ph.begin(), ph.end());
+    };
+}
+
+template <class T> void loadN(const cc_ns2d_params* c, const double* const* f, NSState<T>& s) {
+    const size_t n = (size_t)c->Nx * c->Ny;
+    std::vector<T>* d[4] = {&s.d, &s.mx, &s.my, &s.E};
+    for (int k = 0; k < 4; k++) d[k]->assign(f[k], f[k] + n);
+}
+template <class T> void storeN(const NSState<T>& s, double* const* f) {
+    const std::vector<T>* d[4] = {&s.d, &s.mx, &s.my, &s.E};
+    for (int k = 0; k < 4; k++)
+        if (f[k])
+            for (size_t q = 0; q < d[k]->size(); q++) f[k][q] = (double)(*d[k])[q];
+}
+
 }  // namespace
 
 extern "C" {
@@ -488,6 +526,78 @@ int or_euler2d_main_loop(const cc_euler2d_params* c, double* const* f, int nstep
         storeE(s, f);
         if (t) *t = tt;
         return rc;
+    };
+    return fp32 ? run(0.0f) : run(0.0);
+}
+
+// ---- 2D Navier-Stokes + FFT gravity, HLLC (navier_stokes_2d_hllc_poisson.cpp) ----
+int or_ns2d_ic(const cc_ns2d_params* c, double* const* f) {
+    NSState<double> s;
+    ns_ic_collapse(nspar(c), c->seed, s);
+    storeN(s, f);
+    return 0;
+}
+
+// phi of the state's cons_to_prim density and g = -grad phi (NS:372-383)
+int or_ns2d_gravity(const cc_ns2d_params* c, const double* const* f, double* phi, double* gx, double* gy) {
+    NSState<double> s;
+    loadN(c, f, s);
+    NS<double> m(nspar(c));
+    std::vector<double> rho(s.d.size()), ph, x, y;
+    for (size_t q = 0; q < rho.size(); q++) rho[q] = m.prim(s.d[q], s.mx[q], s.my[q], s.E[q]).d;
+    ns_potential<double>(c)(rho, ph);
+    m.gravity_accel(ph, x, y);
+    if (phi) std::memcpy(phi, ph.data(), ph.size() * sizeof(double));
+    if (gx) std::memcpy(gx, x.data(), x.size() * sizeof(double));
+    if (gy) std::memcpy(gy, y.data(), y.size() * sizeof(double));
+    return 0;
+}
+
+int or_ns2d_rhs(const cc_ns2d_params* c, const double* const* f, double* const* dU) {
+    NSState<double> s;
+    loadN(c, f, s);
+    storeN(NS<double>(nspar(c)).rhs(s, ns_potential<double>(c)), dU);
+    return 0;
+}
+
+double or_ns2d_compute_dt(const cc_ns2d_params* c, const double* const* f) {
+    NSState<double> s;
+    loadN(c, f, s);
+    return NS<double>(nspar(c)).compute_dt(s);
+}
+
+int or_ns2d_rk2_step(const cc_ns2d_params* c, double* const* f, double dt) {
+    NSState<double> s;
+    loadN(c, f, s);
+    NS<double>(nspar(c)).heun(s, dt, ns_potential<double>(c));
+    storeN(s, f);
+    return 0;
+}
+
+void or_ns2d_derived(const cc_ns2d_params* c, const double* const* f, double* const* out) {
+    NSState<double> s;
+    loadN(c, f, s);
+    NS<double>(nspar(c)).derived(s, ns_potential<double>(c), out);
+}
+
+// main() loop body (NS:758-791) in double (fp32 == 0) or float
+int or_ns2d_main_loop(const cc_ns2d_params* c, double* const* f, int nsteps, double* t, int fp32) {
+    auto run = [&](auto tag) -> int {
+        using T = decltype(tag);
+        NSState<T> s;
+        loadN(c, f, s);
+        NS<T> m(nspar(c));
+        const auto pot = ns_potential<T>(c);
+        double tt = t ? *t : 0.0;
+        for (int n = 0; n < nsteps && tt < c->t_end - 1e-14; ++n) {
+            double dt = m.compute_dt(s);
+            if (tt + dt > c->t_end) dt = c->t_end - tt;
+            m.heun(s, T(dt), pot);
+            tt += dt;
+        }
+        storeN(s, f);
+        if (t) *t = tt;
+        return 0;
     };
     return fp32 ? run(0.0f) : run(0.0);
 }

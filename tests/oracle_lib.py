@@ -61,6 +61,16 @@ def oracle() -> C.CDLL:
         O.or_euler2d_derived.restype = None
         O.or_euler2d_rk2_step.argtypes = [PE, _PP, C.c_double, C.c_int]
         O.or_euler2d_main_loop.argtypes = [PE, _PP, C.c_int, _DP, C.c_int, C.c_int]
+        PN = C.POINTER(L.CcNs2dParams)
+        O.or_ns2d_ic.argtypes = [PN, _PP]
+        O.or_ns2d_gravity.argtypes = [PN, _PP, _DP, _DP, _DP]
+        O.or_ns2d_rhs.argtypes = [PN, _PP, _PP]
+        O.or_ns2d_compute_dt.argtypes = [PN, _PP]
+        O.or_ns2d_compute_dt.restype = C.c_double
+        O.or_ns2d_rk2_step.argtypes = [PN, _PP, C.c_double]
+        O.or_ns2d_derived.argtypes = [PN, _PP, _PP]
+        O.or_ns2d_derived.restype = None
+        O.or_ns2d_main_loop.argtypes = [PN, _PP, C.c_int, _DP, C.c_int]
         P3 = C.POINTER(L.CcMhd3dParams)
         O.or_mhd3d_advance_stage.argtypes = [P3, _PP, _PP, C.c_double]
         O.or_mhd3d_rk2_step.argtypes = [P3, _PP, C.c_double]
@@ -121,6 +131,10 @@ def ref(name: str) -> C.CDLL | None:
             R.ref_fft_gravity_accel.argtypes = [C.c_int, C.c_int, C.c_double, C.c_double, C.c_double, C.c_double,
                                                 _DP, _DP, _DP]
             R.ref_fft1d.argtypes = [C.c_int, _DP, C.c_int]
+            R.ref_ns_rhs.argtypes = [C.c_int, C.c_int] + [C.c_double] * 7 + [C.c_int, C.c_double, C.c_int,
+                                                                             C.c_double, _PP, _PP]
+            R.ref_ns_dt.argtypes = [C.c_int, C.c_int] + [C.c_double] * 8 + [C.c_int, C.c_double, C.c_double, _PP]
+            R.ref_ns_dt.restype = C.c_double
         _refs[name] = R
     return _refs[name]
 
@@ -236,3 +250,37 @@ def eh_main_loop_oracle(cp, S, nsteps, mode, fp32=False, t0=0.0):
     t = C.c_double(t0)
     rc = oracle().or_euler2d_main_loop(C.byref(cp), pp(out), nsteps, C.byref(t), mode, 1 if fp32 else 0)
     return out, t.value, rc
+
+
+# ---- 2D Navier-Stokes helpers: [rho, mx, my, E] ----
+
+def ns_main_loop_oracle(cp, S, nsteps, fp32=False, t0=0.0):
+    out = copy_state(S)
+    t = C.c_double(t0)
+    oracle().or_ns2d_main_loop(C.byref(cp), pp(out), nsteps, C.byref(t), 1 if fp32 else 0)
+    return out, t.value
+
+
+def ns_rhs_oracle(cp, S):
+    out = [np.zeros_like(a) for a in S]
+    oracle().or_ns2d_rhs(C.byref(cp), pp(S), pp(out))
+    return out
+
+
+def ns_ref_rhs(cp, S):
+    """compute_rhs of the compiled reference (None without it)."""
+    R = ref("fft")
+    if R is None:
+        return None
+    out = [np.zeros_like(a) for a in S]
+    R.ref_ns_rhs(cp.Nx, cp.Ny, cp.x0, cp.x1, cp.y0, cp.y1, cp.gamma, cp.floor_rho, cp.floor_P, cp.viscosity_on,
+                 cp.mu, cp.gravity_on, cp.G, pp(S), pp(out))
+    return out
+
+
+def ns_ref_dt(cp, S):
+    R = ref("fft")
+    if R is None:
+        return None
+    return R.ref_ns_dt(cp.Nx, cp.Ny, cp.x0, cp.x1, cp.y0, cp.y1, cp.gamma, cp.cfl, cp.floor_rho, cp.floor_P,
+                       cp.viscosity_on, cp.mu, cp.cfl_visc, pp(S))

@@ -137,3 +137,36 @@ def test_mhd3d_main_matches_wrapper_loop(tmp_path):
         assert got[k].shape == (len(ts), n, n, n)
         for m, snap in enumerate(snaps):
             assert np.array_equal(got[k][m], snap[k]), f"{k} snapshot {m}"
+
+
+EXE_NS = EXE.parent / "cc_ns2d_main"
+
+
+def test_ns2d_main_matches_wrapper_loop(tmp_path):
+    """cc_ns2d_main (the reference main() of navier_stokes_2d_hllc_poisson.cpp,
+    NS:611-803): the reference IC, loop and store rule (frame at t = 0);
+    snapshots equal the same loop driven through the Python wrapper, bit for bit."""
+    from core_collapse_b200.ns2d import DERIVED_NS_FIELDS, Ns2dSolver, ParamsNS, ic_collapse
+    out = tmp_path / "ns"
+    n, t_end, dts = 32, 0.05, 0.02
+    r = subprocess.run([str(EXE_NS), "--Nx", str(n), "--Ny", str(n), "--t_end", str(t_end), "--dt_store", str(dts),
+                        "--out", str(out)], capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr
+    got = {k: np.load(out / f"{k}.npy") for k in ("x", "y", "t", *DERIVED_NS_FIELDS)}
+    p = ParamsNS(Nx=n, Ny=n, t_end=t_end, dt_store=dts)
+    ts, snaps = [0.0], []
+    with Ns2dSolver(p) as s:
+        s.upload(ic_collapse(p))
+        snaps.append(s.derived())
+        t, next_store = 0.0, p.dt_store
+        while t < p.t_end - 1e-14:
+            t = s.advance(1)
+            if t + 1e-14 >= next_store or t >= p.t_end - 1e-14:
+                ts.append(t)
+                snaps.append(s.derived())
+                next_store += p.dt_store
+    assert len(ts) >= 3 and np.array_equal(got["t"], np.array(ts)) and got["x"].shape == (n,)
+    for k in DERIVED_NS_FIELDS:
+        assert got[k].shape == (len(ts), n, n)
+        for m, snap in enumerate(snaps):
+            assert np.array_equal(got[k][m], snap[k]), f"{k} snapshot {m}"
