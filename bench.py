@@ -349,6 +349,8 @@ def run_ours(args) -> None:
     }
     if world == 1 and not args.skip_3d:
         line["mhd3d"] = run_3d(args, stream)
+    if world == 1 and not args.skip_ns:
+        line["ns2d"] = run_ns2d(args, stream, peaks)
     if not args.skip_ensemble:
         line["ensemble"] = run_ensemble(args, stream, rank, world, barrier, max_over_ranks, value32 / world)
     if world == 1 and not args.skip_adjoint:
@@ -396,6 +398,53 @@ def run_3d(args, stream) -> dict:
                      "stage_ms": pf["stage_ms"] / max(1, pf["stage_launches"]),
                      "max_divB_end": d1["max_divB"], "energy_drift_rel": (d1["energy"] - d0["energy"]) / d0["energy"],
                      "mass_drift_rel": (d1["mass"] - d0["mass"]) / d0["mass"]}
+    out["fp32_over_fp64"] = out["fp32"]["value"] / out["fp64"]["value"]
+    return out
+
+
+# words of FP32/FP64 state moved per cell and Navier-Stokes step: stage 1 reads U,
+# phi and writes U1, k1 (13); stage 2 reads U1, U, k1, phi and writes U (17);
+# the CFL/density reduction reads U (4) and the stage-2 density sum U1.rho (1);
+# each of the two spectral solves reads rho, writes phi and moves the complex
+# work array through rows, columns and inverse rows (2 x 10)
+NS_STEP_WORDS = 13 + 17 + 4 + 1 + 2 * 10
+
+
+def run_ns2d(args, stream, peaks) -> dict:
+    """2D Navier-Stokes + FFT gravity: the reference's collapse IC (central
+    Gaussian overdensity, 1% density noise, Mach-0.05 velocity noise, seed 42)
+    and parameters (gamma 1.4, CFL 0.35, mu 1e-6, G 10), periodic unit square."""
+    import torch
+
+    from core_collapse_b200.ns2d import Ns2dSolver, ParamsNS, ic_collapse
+    n = args.grid_ns
+    steps = max(1, min(args.steps, args.steps_ns))
+    s0 = ic_collapse(ParamsNS(Nx=n, Ny=n))
+    out = {"workload": f"2D Navier-Stokes + spectral gravity, {n}^2 periodic, reference collapse IC and parameters",
+           "steps": steps, "warmup": args.warmup, "step_words_per_cell": NS_STEP_WORDS}
+    for prec in ("fp32", "fp64"):
+        p = ParamsNS(Nx=n, Ny=n, precision=prec, t_end=1e30)
+        with Ns2dSolver(p) as g:
+            g.set_stream(stream.cuda_stream)
+            g.upload(s0)
+            d0 = g.diagnostics()
+            g.advance(args.warmup, 0.0)
+            g.reset_perf()
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            g.advance(steps)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            ms = e0.elapsed_time(e1)
+            pf = g.perf()
+            d1 = g.diagnostics()
+        word = 4 if prec == "fp32" else 8
+        gbs = NS_STEP_WORDS * word * n * n / (ms / steps / 1000.0) / 1e9
+        out[prec] = {"value": n * n * steps / (ms / 1000.0), "unit": UNIT, "ms_per_step": ms / steps,
+                     "gpu_launches": pf["kernel_launches"], "step_gbs": gbs,
+                     "step_roofline_frac": gbs / peaks["hbm_gbs"],
+                     "mass_drift_rel": (d1["mass"] - d0["mass"]) / d0["mass"], "nonfinite": d1["nonfinite"]}
     out["fp32_over_fp64"] = out["fp32"]["value"] / out["fp64"]["value"]
     return out
 
@@ -542,6 +591,9 @@ def main():
     ap.add_argument("--skip-3d", action="store_true")
     ap.add_argument("--grid3d", type=int, default=256)
     ap.add_argument("--steps3d", type=int, default=20)
+    ap.add_argument("--skip-ns", action="store_true")
+    ap.add_argument("--grid-ns", type=int, default=4096)
+    ap.add_argument("--steps-ns", type=int, default=20)
     ap.add_argument("--skip-ensemble", action="store_true")
     ap.add_argument("--ensemble", type=int, default=512)
     ap.add_argument("--ensemble-steps", type=int, default=60)
@@ -550,6 +602,8 @@ def main():
     ap.add_argument("--adjoint-steps", type=int, default=100)
     ap.add_argument("--adjoint-fd", type=int, default=4)
     ap.add_argument("--adjoint-only", action="store_true", help="time only the adjoint block (a profiling aid)")
+    ap.add_argument("--ns-only", action="store_true",
+                    help="time only the Navier-Stokes block (a profiling aid; prints the ns2d block)")
     ap.add_argument("--ensemble-only", action="store_true",
                     help="time only the batched ensemble (a profiling aid; prints the ensemble block)")
     args = ap.parse_args()
@@ -557,6 +611,11 @@ def main():
         ap.error("--warmup must be >= 3")
     if args.ensemble_only:
         run_ensemble_only(args)
+        return
+    if args.ns_only:
+        import torch
+        torch.cuda.set_device(0)
+        print(json.dumps(run_ns2d(args, torch.cuda.Stream(), measured_peaks())), flush=True)
         return
     if args.adjoint_only:
         import torch
