@@ -176,6 +176,12 @@ SIGNATURES = {
     "cc_euler2d_advance": (C.c_int, [_H, C.c_int, _DP]),
     "cc_euler2d_diagnostics": (C.c_int, [_H, C.POINTER(CcDiag)]),
     "cc_euler2d_derived": (C.c_int, [_H, C.POINTER(C.POINTER(C.c_double))]),
+    "cc_euler2d_checkpoint_save": (C.c_int, [_H, C.c_char_p]),
+    "cc_euler2d_checkpoint_load": (C.c_int, [_H, C.c_char_p]),
+    "cc_ns2d_checkpoint_save": (C.c_int, [_H, C.c_char_p]),
+    "cc_ns2d_checkpoint_load": (C.c_int, [_H, C.c_char_p]),
+    "cc_mhd3d_checkpoint_save": (C.c_int, [_H, C.c_char_p]),
+    "cc_mhd3d_checkpoint_load": (C.c_int, [_H, C.c_char_p]),
     "cc_ns2d_params_default": (None, [C.POINTER(CcNs2dParams)]),
     "cc_ns2d_create": (C.c_int, [C.POINTER(CcNs2dParams), C.POINTER(_H)]),
     "cc_ns2d_upload": (C.c_int, [_H] + [_DP] * 4),

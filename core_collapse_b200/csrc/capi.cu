@@ -19,6 +19,7 @@
 #include <vector>
 
 #include "../../include/cc_step.h"
+#include "checkpoint.h"
 #include "fft_tables.h"
 #include "mhd2d_launch.h"
 #include "handle.h"
@@ -552,26 +553,6 @@ constexpr uint32_t CK_VERSION = 1;
 std::vector<size_t> ck_sizes(const cc_mhd2d_params& p) {
     const size_t nx = (size_t)p.Nx, ny = (size_t)p.Ny, n = nx * ny;
     return {n, n, n, n, n, n, (nx + 1) * ny, nx * (ny + 1)};
-}
-
-void ck_put(std::vector<unsigned char>& b, const void* src, size_t n) {
-    const unsigned char* c = static_cast<const unsigned char*>(src);
-    b.insert(b.end(), c, c + n);
-}
-
-void ck_get(const std::vector<unsigned char>& b, size_t& off, void* dst, size_t n) {
-    std::memcpy(dst, b.data() + off, n);
-    off += n;
-}
-
-// FNV-1a, 64-bit
-uint64_t ck_fnv1a(const unsigned char* d, size_t n) {
-    uint64_t hsh = 1469598103934665603ull;
-    for (size_t i = 0; i < n; i++) {
-        hsh ^= d[i];
-        hsh *= 1099511628211ull;
-    }
-    return hsh;
 }
 
 Mhd2dBase* m2(cc_handle* h) {

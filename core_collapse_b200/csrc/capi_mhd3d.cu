@@ -12,6 +12,7 @@
 #include <string>
 #include <vector>
 
+#include "checkpoint.h"
 #include "handle.h"
 #include "mhd3d_const.h"
 #include "mhd3d_launch.h"
@@ -30,6 +31,9 @@ struct Mhd3dBase {
     virtual int advance(int nsteps, double* t) = 0;
     virtual int diagnostics(cc_diag* d) = 0;
     virtual int derived(double* const* out) = 0;
+    virtual int get_clock(double* t, long long* steps) = 0;
+    virtual int set_clock(double t, long long steps) = 0;
+    virtual const cc_mhd3d_params& params() const = 0;
 };
 
 template <class T> struct Mhd3d : Mhd3dBase {
@@ -287,6 +291,22 @@ template <class T> struct Mhd3d : Mhd3dBase {
         return CC_OK;
     }
 
+    int get_clock(double* t, long long* steps) override {
+        CC_CUDA(cudaMemcpyAsync(t, t_dev(), sizeof(double), cudaMemcpyDeviceToHost, st()));
+        CC_CUDA(cudaMemcpyAsync(steps, steps_dev, sizeof(long long), cudaMemcpyDeviceToHost, st()));
+        CC_CUDA(cudaStreamSynchronize(st()));
+        return CC_OK;
+    }
+
+    int set_clock(double t, long long steps) override {
+        CC_CUDA(launch_set_scalar(t_dev(), t, st()));
+        CC_CUDA(cudaMemcpyAsync(steps_dev, &steps, sizeof(long long), cudaMemcpyHostToDevice, st()));
+        CC_CUDA(cudaStreamSynchronize(st()));
+        return CC_OK;
+    }
+
+    const cc_mhd3d_params& params() const override { return p; }
+
     int diagnostics(cc_diag* d) override {
         if (!loaded) return fail(h, CC_ERR_STATE, "no state uploaded");
         CC_CUDA(M3Launch<T>::diag(c, buf[cur], diag_part, st()));
@@ -415,6 +435,51 @@ int cc_mhd3d_derived(cc_handle* h, double* const* out) {
     if (!m || !out) return CC_ERR_ARG;
     if (int r = set_dev(h)) return r;
     return m->derived(out);
+}
+
+// restart files (checkpoint.h): state {rho, mx, my, mz, E, Bx_f, By_f, Bz_f} and the clock
+static std::vector<size_t> ck3_sizes_m3(const int32_t* n) {
+    const size_t nx = (size_t)n[0], ny = (size_t)n[1], nz = (size_t)n[2], c = nx * ny * nz;
+    return {c, c, c, c, c, (nx + 1) * ny * nz, nx * (ny + 1) * nz, nx * ny * (nz + 1)};
+}
+
+int cc_mhd3d_checkpoint_save(cc_handle* h, const char* path) {
+    Mhd3dBase* m = m3(h);
+    if (!m || !path) return CC_ERR_ARG;
+    if (int r = set_dev(h)) return r;
+    const cc_mhd3d_params& p = m->params();
+    CkMeta meta;
+    meta.precision = (uint32_t)p.precision;
+    meta.n[0] = p.Nx; meta.n[1] = p.Ny; meta.n[2] = p.Nz;
+    std::vector<std::vector<double>> f;
+    for (size_t k : ck3_sizes_m3(meta.n)) f.emplace_back(k);
+    double* fp[8];
+    for (int k = 0; k < 8; k++) fp[k] = f[k].data();
+    if (int r = m->download(fp)) return r;
+    if (int r = m->get_clock(&meta.t, &meta.steps)) return r;
+    std::string err;
+    if (int r = ck3_save(path, "CCM3DCK1", meta, &p, sizeof(p), f, err)) return fail(h, r, err);
+    return CC_OK;
+}
+
+int cc_mhd3d_checkpoint_load(cc_handle* h, const char* path) {
+    Mhd3dBase* m = m3(h);
+    if (!m || !path) return CC_ERR_ARG;
+    if (int r = set_dev(h)) return r;
+    const cc_mhd3d_params& p = m->params();
+    CkMeta meta;
+    cc_mhd3d_params q;
+    std::vector<std::vector<double>> f;
+    std::string err;
+    if (int r = ck3_load(path, "CCM3DCK1", meta, &q, sizeof(q), ck3_sizes_m3, f, err)) return fail(h, r, err);
+    if (meta.n[0] != p.Nx || meta.n[1] != p.Ny || meta.n[2] != p.Nz || (int)meta.precision != p.precision ||
+        q.x0 != p.x0 || q.x1 != p.x1 || q.y0 != p.y0 || q.y1 != p.y1 || q.z0 != p.z0 || q.z1 != p.z1 ||
+        q.periodic_x != p.periodic_x || q.periodic_y != p.periodic_y || q.periodic_z != p.periodic_z)
+        return fail(h, CC_ERR_ARG, "checkpoint grid, domain, boundaries or precision differ from the handle's");
+    const double* fp[8];
+    for (int k = 0; k < 8; k++) fp[k] = f[k].data();
+    if (int r = m->upload(fp)) return r;
+    return m->set_clock(meta.t, meta.steps);
 }
 
 }  // extern "C"

@@ -14,6 +14,7 @@
 #include <string>
 #include <vector>
 
+#include "checkpoint.h"
 #include "fft_tables.h"
 #include "handle.h"
 #include "ns2d_launch.h"
@@ -37,6 +38,9 @@ struct Ns2dBase {
     virtual int advance(int nsteps, double* t) = 0;
     virtual int diagnostics(cc_diag* d) = 0;
     virtual int derived(double* const* out) = 0;
+    virtual int get_clock(double* t, long long* steps) = 0;
+    virtual int set_clock(double t, long long steps) = 0;
+    virtual const cc_ns2d_params& params() const = 0;
 };
 
 template <class T> struct Ns2d : Ns2dBase {
@@ -397,6 +401,22 @@ template <class T> struct Ns2d : Ns2dBase {
         return CC_OK;
     }
 
+    int get_clock(double* t, long long* steps) override {
+        CC_CUDA(cudaMemcpyAsync(t, t_dev(), sizeof(double), cudaMemcpyDeviceToHost, st()));
+        CC_CUDA(cudaMemcpyAsync(steps, steps_dev, sizeof(long long), cudaMemcpyDeviceToHost, st()));
+        CC_CUDA(cudaStreamSynchronize(st()));
+        return CC_OK;
+    }
+
+    int set_clock(double t, long long steps) override {
+        CC_CUDA(launch_set_scalar(t_dev(), t, st()));
+        CC_CUDA(cudaMemcpyAsync(steps_dev, &steps, sizeof(long long), cudaMemcpyHostToDevice, st()));
+        CC_CUDA(cudaStreamSynchronize(st()));
+        return CC_OK;
+    }
+
+    const cc_ns2d_params& params() const override { return p; }
+
     int diagnostics(cc_diag* d) override {
         if (!loaded) return fail(h, CC_ERR_STATE, "no state uploaded");
         CC_CUDA(NSLaunch<T>::diag(c, U, diag_part, st()));
@@ -529,6 +549,44 @@ int cc_ns2d_derived(cc_handle* h, double* const* out) {
     if (!m || !out) return CC_ERR_ARG;
     if (int r = set_dev(h)) return r;
     return m->derived(out);
+}
+
+// restart files (checkpoint.h): state {rho, mx, my, E} and the clock
+int cc_ns2d_checkpoint_save(cc_handle* h, const char* path) {
+    Ns2dBase* m = ns(h);
+    if (!m || !path) return CC_ERR_ARG;
+    if (int r = set_dev(h)) return r;
+    const cc_ns2d_params& p = m->params();
+    const size_t n = (size_t)p.Nx * p.Ny;
+    std::vector<std::vector<double>> f(4, std::vector<double>(n));
+    double* fp[4] = {f[0].data(), f[1].data(), f[2].data(), f[3].data()};
+    if (int r = m->download(fp)) return r;
+    CkMeta meta;
+    meta.precision = (uint32_t)p.precision;
+    meta.n[0] = p.Nx; meta.n[1] = p.Ny;
+    if (int r = m->get_clock(&meta.t, &meta.steps)) return r;
+    std::string err;
+    if (int r = ck3_save(path, "CCNS2CK1", meta, &p, sizeof(p), f, err)) return fail(h, r, err);
+    return CC_OK;
+}
+
+int cc_ns2d_checkpoint_load(cc_handle* h, const char* path) {
+    Ns2dBase* m = ns(h);
+    if (!m || !path) return CC_ERR_ARG;
+    if (int r = set_dev(h)) return r;
+    const cc_ns2d_params& p = m->params();
+    CkMeta meta;
+    cc_ns2d_params q;
+    std::vector<std::vector<double>> f;
+    std::string err;
+    auto sizes = [](const int32_t* n) { return std::vector<size_t>(4, (size_t)n[0] * n[1]); };
+    if (int r = ck3_load(path, "CCNS2CK1", meta, &q, sizeof(q), sizes, f, err)) return fail(h, r, err);
+    if (meta.n[0] != p.Nx || meta.n[1] != p.Ny || (int)meta.precision != p.precision || q.x0 != p.x0 ||
+        q.x1 != p.x1 || q.y0 != p.y0 || q.y1 != p.y1)
+        return fail(h, CC_ERR_ARG, "checkpoint grid, domain or precision differ from the handle's");
+    const double* fp[4] = {f[0].data(), f[1].data(), f[2].data(), f[3].data()};
+    if (int r = m->upload(fp)) return r;
+    return m->set_clock(meta.t, meta.steps);
 }
 
 }  // extern "C"

@@ -9,7 +9,10 @@
 // <out>/<name>.npy (default out3d_mhd/).
 //
 // Usage: cc_mhd3d_main [--precision fp64|fp32] [--Nx N] [--Ny N] [--Nz N]
-//                      [--t_end T] [--dt_store D] [--out DIR]
+//                      [--t_end T] [--dt_store D] [--out DIR] [--checkpoint FILE] [--restart FILE]
+// --checkpoint writes a restart file at the end of the run; --restart starts
+// from one (same grid) instead of the initial condition; frames then follow
+// the same rule from the restored time (the first after the first step).
 #include <sys/stat.h>
 
 #include <cstdio>
@@ -27,6 +30,7 @@ int main(int argc, char** argv) {
     cc_mhd3d_params p;
     cc_mhd3d_params_default(&p);   // the reference's Params defaults (M3:43-89)
     std::string out = "out3d_mhd";
+    std::string ckpt, restart;
     for (int a = 1; a < argc; a++) {
         const std::string k = argv[a];
         if (a + 1 >= argc) {
@@ -41,6 +45,8 @@ int main(int argc, char** argv) {
         else if (k == "--t_end") p.t_end = std::atof(v.c_str());
         else if (k == "--dt_store") p.dt_store = std::atof(v.c_str());
         else if (k == "--out") out = v;
+        else if (k == "--checkpoint") ckpt = v;
+        else if (k == "--restart") restart = v;
         else {
             std::fprintf(stderr, "unknown option %s\n", k.c_str());
             return 2;
@@ -66,13 +72,21 @@ int main(int argc, char** argv) {
                                           std::vector<double>((size_t)Nx * Ny * (Nz + 1))};
     double* fp[8];
     for (int k = 0; k < 8; k++) fp[k] = f[k].data();
-    cc_mhd3d_ic_knobs kn;
-    cc_mhd3d_ic_knobs_default(&kn);
-    if (cc_ic_mhd3d_reference(&p, &kn, fp) != 0) {
-        std::fprintf(stderr, "initial condition failed\n");
-        return 1;
+    double t = 0.0;
+    if (restart.empty()) {
+        cc_mhd3d_ic_knobs kn;
+        cc_mhd3d_ic_knobs_default(&kn);
+        if (cc_ic_mhd3d_reference(&p, &kn, fp) != 0) {
+            std::fprintf(stderr, "initial condition failed\n");
+            return 1;
+        }
+        if (check(cc_mhd3d_upload(h, fp[0], fp[1], fp[2], fp[3], fp[4], fp[5], fp[6], fp[7]), "upload")) return 1;
+    } else {
+        if (check(cc_mhd3d_checkpoint_load(h, restart.c_str()), "cc_mhd3d_checkpoint_load")) return 1;
+        cc_diag d0;
+        if (check(cc_mhd3d_diagnostics(h, &d0), "diagnostics")) return 1;
+        t = d0.t;
     }
-    if (check(cc_mhd3d_upload(h, fp[0], fp[1], fp[2], fp[3], fp[4], fp[5], fp[6], fp[7]), "upload")) return 1;
 
     const char* names[11] = {"rho", "P", "Mach", "u", "v", "w", "vabs", "Bx", "By", "Bz", "divB"};
     mkdir(out.c_str(), 0755);
@@ -88,7 +102,7 @@ int main(int argc, char** argv) {
     for (int k = 0; k < 11; k++) sp[k] = snap[k].data();
 
     // the main loop (M3:1285-1327)
-    double t = 0.0, tnext = 0.0;
+    double tnext = t;
     while (t < p.t_end) {
         if (check(cc_mhd3d_advance(h, 1, &t), "cc_mhd3d_advance")) return 1;
         if (t >= tnext - 1e-12) {
@@ -100,6 +114,7 @@ int main(int argc, char** argv) {
             tnext += p.dt_store;
         }
     }
+    if (!ckpt.empty() && check(cc_mhd3d_checkpoint_save(h, ckpt.c_str()), "cc_mhd3d_checkpoint_save")) return 1;
     bool ok = true;
     for (int k = 0; k < 11; k++) ok = series[k].finish() && ok;
     ok = write_npy(out + "/x.npy", {Nx}, x.data(), x.size()) && ok;

@@ -9,7 +9,10 @@
 // momy,Phi}.npy (default out_ns2d_poisson/).
 //
 // Usage: cc_ns2d_main [--precision fp64|fp32] [--Nx N] [--Ny N]
-//                     [--t_end T] [--dt_store D] [--out DIR]
+//                     [--t_end T] [--dt_store D] [--out DIR] [--checkpoint FILE] [--restart FILE]
+// --checkpoint writes a restart file at the end of the run; --restart starts
+// from one (same grid) instead of the initial condition, its first snapshot
+// being the restored state at the restored time.
 #include <sys/stat.h>
 
 #include <cstdio>
@@ -27,6 +30,7 @@ int main(int argc, char** argv) {
     cc_ns2d_params p;
     cc_ns2d_params_default(&p);   // the reference's Params defaults (NS:54-86)
     std::string out = "out_ns2d_poisson";
+    std::string ckpt, restart;
     for (int a = 1; a < argc; a++) {
         const std::string k = argv[a];
         if (a + 1 >= argc) {
@@ -40,6 +44,8 @@ int main(int argc, char** argv) {
         else if (k == "--t_end") p.t_end = std::atof(v.c_str());
         else if (k == "--dt_store") p.dt_store = std::atof(v.c_str());
         else if (k == "--out") out = v;
+        else if (k == "--checkpoint") ckpt = v;
+        else if (k == "--restart") restart = v;
         else {
             std::fprintf(stderr, "unknown option %s\n", k.c_str());
             return 2;
@@ -60,11 +66,19 @@ int main(int argc, char** argv) {
     if (check(cc_ns2d_create(&p, &h), "cc_ns2d_create")) return 1;
     std::vector<std::vector<double>> f(4, std::vector<double>(N));
     double* fp[4] = {f[0].data(), f[1].data(), f[2].data(), f[3].data()};
-    if (cc_ic_ns2d_collapse(&p, fp) != 0) {
-        std::fprintf(stderr, "initial condition failed\n");
-        return 1;
+    double t = 0.0;
+    if (restart.empty()) {
+        if (cc_ic_ns2d_collapse(&p, fp) != 0) {
+            std::fprintf(stderr, "initial condition failed\n");
+            return 1;
+        }
+        if (check(cc_ns2d_upload(h, fp[0], fp[1], fp[2], fp[3]), "upload")) return 1;
+    } else {
+        if (check(cc_ns2d_checkpoint_load(h, restart.c_str()), "cc_ns2d_checkpoint_load")) return 1;
+        cc_diag d0;
+        if (check(cc_ns2d_diagnostics(h, &d0), "diagnostics")) return 1;
+        t = d0.t;
     }
-    if (check(cc_ns2d_upload(h, fp[0], fp[1], fp[2], fp[3]), "upload")) return 1;
 
     constexpr int NF = 8;
     const char* names[NF] = {"rho", "P", "Mach", "u", "v", "momx", "momy", "Phi"};
@@ -88,7 +102,7 @@ int main(int argc, char** argv) {
     };
 
     // the main loop (NS:748-792)
-    double t = 0.0, next_store = 0.0;
+    double next_store = t;
     if (!store(t)) return 1;
     next_store += p.dt_store;
     cc_diag d;
@@ -101,6 +115,7 @@ int main(int argc, char** argv) {
             std::fprintf(stderr, "t=%.10g dt=%.10g snapshots=%zu\n", t, d.dt_last, times.size());
         }
     }
+    if (!ckpt.empty() && check(cc_ns2d_checkpoint_save(h, ckpt.c_str()), "cc_ns2d_checkpoint_save")) return 1;
     bool ok = true;
     for (int k = 0; k < NF; k++) ok = series[k].finish() && ok;
     ok = write_npy(out + "/x.npy", {Nx}, x.data(), x.size()) && ok;

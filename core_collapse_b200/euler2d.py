@@ -160,6 +160,15 @@ class Euler2dSolver:
         self._t = tt.value
         return tt.value
 
+    def save_checkpoint(self, path: str):
+        """State, clock and parameters to one file (cc_euler2d_checkpoint_save)."""
+        self._check(self._lib.cc_euler2d_checkpoint_save(self._h, str(path).encode()))
+
+    def load_checkpoint(self, path: str):
+        """Restore state and clock from a checkpoint of the same grid (cc_euler2d_checkpoint_load)."""
+        self._check(self._lib.cc_euler2d_checkpoint_load(self._h, str(path).encode()))
+        self._t = self.diagnostics()["t"]
+
     def diagnostics(self) -> dict:
         d = L.CcDiag()
         self._check(self._lib.cc_euler2d_diagnostics(self._h, C.byref(d)))

@@ -178,6 +178,15 @@ class Ns2dSolver:
     def reset_perf(self):
         self._check(self._lib.cc_reset_perf(self._h))
 
+    def save_checkpoint(self, path: str):
+        """State, clock and parameters to one file (cc_ns2d_checkpoint_save)."""
+        self._check(self._lib.cc_ns2d_checkpoint_save(self._h, str(path).encode()))
+
+    def load_checkpoint(self, path: str):
+        """Restore state and clock from a checkpoint of the same grid (cc_ns2d_checkpoint_load)."""
+        self._check(self._lib.cc_ns2d_checkpoint_load(self._h, str(path).encode()))
+        self._t = self.diagnostics()["t"]
+
     def diagnostics(self) -> dict:
         d = L.CcDiag()
         self._check(self._lib.cc_ns2d_diagnostics(self._h, C.byref(d)))

@@ -286,6 +286,10 @@ int cc_mhd3d_diagnostics(cc_handle* h, cc_diag* d);
  * Mach with the hybrid-EOS sound speed.  The first call allocates
  * 11*Nx*Ny*Nz doubles of device scratch for the handle. */
 int cc_mhd3d_derived(cc_handle* h, double* const* out);
+/* Restart files of the 3D handle: {rho, mx, my, mz, E, Bx_f, By_f, Bz_f}, the
+ * clock and the parameters (as cc_euler2d_checkpoint_*, magic "CCM3DCK1"). */
+int cc_mhd3d_checkpoint_save(cc_handle* h, const char* path);
+int cc_mhd3d_checkpoint_load(cc_handle* h, const char* path);
 
 /* ---- 2D Euler + self-gravity, HLLC (euler2d_gravity_hllc.cpp) ---- */
 
@@ -313,6 +317,13 @@ int cc_euler2d_diagnostics(cc_handle* h, cc_diag* d);
  * floored copy of each cell; Mach = |v| / a, 0 where a <= 0.  The first call
  * allocates 3*Nx*Ny doubles of device scratch for the handle. */
 int cc_euler2d_derived(cc_handle* h, double* const* out);
+/* Restart files of the Euler handle: state {rho, mx, my, E}, the clock and the
+ * parameters in one checksummed file (layout in csrc/checkpoint.h, magic
+ * "CCEH2CK1").  No reference counterpart.  Load checks the grid, domain,
+ * boundaries and precision against the handle's (CC_ERR_ARG otherwise; a
+ * corrupted file: CC_ERR_ARG; an unreadable one: CC_ERR_IO). */
+int cc_euler2d_checkpoint_save(cc_handle* h, const char* path);
+int cc_euler2d_checkpoint_load(cc_handle* h, const char* path);
 
 /* ---- 2D Navier-Stokes + FFT self-gravity, HLLC (navier_stokes_2d_hllc_poisson.cpp) ---- */
 
@@ -345,6 +356,10 @@ int cc_ns2d_diagnostics(cc_handle* h, cc_diag* d);
  * a <= 0; Phi the spectral potential of the state's density (0 with gravity
  * off).  The first call allocates 8*Nx*Ny doubles of device scratch. */
 int cc_ns2d_derived(cc_handle* h, double* const* out);
+/* Restart files of the Navier-Stokes handle (as cc_euler2d_checkpoint_*,
+ * magic "CCNS2CK1"; load checks grid, domain and precision). */
+int cc_ns2d_checkpoint_save(cc_handle* h, const char* path);
+int cc_ns2d_checkpoint_load(cc_handle* h, const char* path);
 
 /* ---- spectral gravity without device allocation ----
  * No counterpart in the reference: an addition for callers that cannot call

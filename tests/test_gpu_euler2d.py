@@ -199,3 +199,50 @@ def test_enclosed_mass_gravity_matches_oracle(name):
         assert O.rel_linf(a, b) <= 1e-12
     for a, b in zip(got5, want5):
         assert O.rel_linf(a, b) <= 1e-11
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+def test_checkpoint_restart_continues_bitwise(tmp_path, precision):
+    """6 steps in one go == 3 steps, checkpoint, load into a fresh handle, 3 more
+    (SOR gravity, so the restart also carries the Poisson state's effect)."""
+    p, s = make_case_eh("periodic_grav")
+    p.precision = precision
+    with Euler2dSolver(p) as g:
+        g.upload(s)
+        t_full = g.advance(6, 0.0)
+        want = g.download()
+        steps_full = g.diagnostics()["steps"]
+    path = tmp_path / "ck.bin"
+    with Euler2dSolver(p) as g:
+        g.upload(s)
+        g.advance(3, 0.0)
+        g.save_checkpoint(path)
+    with Euler2dSolver(p) as g:
+        g.load_checkpoint(path)
+        t = g.advance(3)
+        got = g.download()
+        d = g.diagnostics()
+    assert t == t_full and d["steps"] == steps_full
+    for a, w in zip(got.arrays(), want.arrays()):
+        assert np.array_equal(a, w)
+
+
+def test_checkpoint_rejects_bad_files(tmp_path):
+    p, s = make_case_eh("periodic_grav")
+    path = tmp_path / "ck.bin"
+    with Euler2dSolver(p) as g:
+        g.upload(s)
+        g.save_checkpoint(path)
+    raw = bytearray(path.read_bytes())
+    raw[-20] ^= 0x01
+    bad = tmp_path / "bad.bin"
+    bad.write_bytes(bytes(raw))
+    with Euler2dSolver(p) as g:
+        with pytest.raises(CcError) as e:
+            g.load_checkpoint(bad)
+        assert e.value.code == L.CC_ERR_ARG
+    q, _ = make_case_eh("outflow_grav")   # other boundaries
+    with Euler2dSolver(q) as g:
+        with pytest.raises(CcError) as e:
+            g.load_checkpoint(path)
+        assert e.value.code == L.CC_ERR_ARG

@@ -170,3 +170,35 @@ def test_ns2d_main_matches_wrapper_loop(tmp_path):
         assert got[k].shape == (len(ts), n, n)
         for m, snap in enumerate(snaps):
             assert np.array_equal(got[k][m], snap[k]), f"{k} snapshot {m}"
+
+
+@pytest.mark.parametrize("exe,mod", [("cc_ns2d_main", "ns2d"), ("cc_euler2d_main", "euler2d")])
+def test_2d_drivers_restart_from_checkpoint(tmp_path, exe, mod):
+    """--checkpoint at the end of one run, --restart of a longer one: the
+    restarted run's first snapshot is the checkpointed state at its time and it
+    ends at the same t_end as an uninterrupted run (whose trajectory differs:
+    the first run's last step was clamped to its own t_end)."""
+    import importlib
+    m = importlib.import_module(f"core_collapse_b200.{mod}")
+    Solver = m.Ns2dSolver if mod == "ns2d" else m.Euler2dSolver
+    Par = m.ParamsNS if mod == "ns2d" else m.ParamsEH
+    fields = m.DERIVED_NS_FIELDS if mod == "ns2d" else ("rho", "P", "Mach")
+    prog = EXE.parent / exe
+    n, t1, t2, dts = 32, 0.02, 0.04, 0.01
+    ck, a, b, full = tmp_path / "ck.bin", tmp_path / "a", tmp_path / "b", tmp_path / "full"
+    common = ["--Nx", n, "--Ny", n, "--dt_store", dts]
+    for args in ([*common, "--t_end", t1, "--out", a, "--checkpoint", ck],
+                 [*common, "--t_end", t2, "--out", b, "--restart", ck],
+                 [*common, "--t_end", t2, "--out", full]):
+        r = subprocess.run([str(prog), *map(str, args)], capture_output=True, text=True, timeout=300)
+        assert r.returncode == 0, r.stderr
+    A, B, F = ({k: np.load(d / f"{k}.npy") for k in ("t", *fields)} for d in (a, b, full))
+    with Solver(Par(Nx=n, Ny=n)) as s:
+        s.load_checkpoint(ck)
+        t_ck = s.diagnostics()["t"]
+        want = s.derived()
+    assert B["t"][0] == t_ck == A["t"][-1] and abs(t_ck - t1) < 1e-12
+    assert B["t"][-1] == F["t"][-1]
+    for k in fields:
+        assert np.array_equal(B[k][0], want[k]), k
+        assert B[k].shape[1:] == F[k].shape[1:]

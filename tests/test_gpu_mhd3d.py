@@ -136,3 +136,43 @@ def test_derived_fields_match_oracle(name):
         else:
             scale = np.max(np.abs(want[k])) + 1e-300
             assert np.max(np.abs(a - want[k])) <= 1e-12 * scale, f"{name} {fname}"
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+def test_checkpoint_restart_continues_bitwise(tmp_path, precision):
+    """6 steps in one go == 3 steps, checkpoint, load into a fresh handle, 3 more."""
+    p, s = make_case3("mixed_hybrid", precision=precision)
+    p.t_end = 10.0
+    with Mhd3dSolver(p) as g:
+        g.upload(s)
+        t_full = g.advance(6, 0.0)
+        want = g.download()
+        steps_full = g.diagnostics()["steps"]
+    path = tmp_path / "ck.bin"
+    with Mhd3dSolver(p) as g:
+        g.upload(s)
+        g.advance(3, 0.0)
+        g.save_checkpoint(path)
+    with Mhd3dSolver(p) as g:
+        g.load_checkpoint(path)
+        t = g.advance(3)
+        got = g.download()
+        d = g.diagnostics()
+    assert t == t_full and d["steps"] == steps_full
+    for a, w in zip(got.arrays(), want.arrays()):
+        assert np.array_equal(a, w)
+
+
+def test_checkpoint_rejects_other_grid(tmp_path):
+    from core_collapse_b200 import _lib as L
+    from core_collapse_b200.mhd2d import CcError
+    p, s = make_case3("mixed_hybrid")
+    path = tmp_path / "ck.bin"
+    with Mhd3dSolver(p) as g:
+        g.upload(s)
+        g.save_checkpoint(path)
+    q, _ = make_case3("periodic_ideal")
+    with Mhd3dSolver(q) as g:
+        with pytest.raises(CcError) as e:
+            g.load_checkpoint(path)
+        assert e.value.code == L.CC_ERR_ARG

@@ -193,3 +193,49 @@ def test_errors_are_reported():
         with pytest.raises(CcError) as e:
             g.rk2_step(-1.0)
         assert e.value.code == L.CC_ERR_NONFINITE
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+def test_checkpoint_restart_continues_bitwise(tmp_path, precision):
+    """6 steps in one go == 3 steps, checkpoint, load into a fresh handle, 3 more."""
+    p, s = make_case_ns("kicked_viscous", precision=precision)
+    with Ns2dSolver(p) as g:
+        g.upload(s)
+        t_full = g.advance(6, 0.0)
+        want = g.download()
+        steps_full = g.diagnostics()["steps"]
+    path = tmp_path / "ck.bin"
+    with Ns2dSolver(p) as g:
+        g.upload(s)
+        g.advance(3, 0.0)
+        g.save_checkpoint(path)
+    with Ns2dSolver(p) as g:
+        g.load_checkpoint(path)
+        t = g.advance(3)
+        got = g.download()
+        d = g.diagnostics()
+    assert t == t_full and d["steps"] == steps_full
+    for a, w in zip(got.arrays(), want.arrays()):
+        assert np.array_equal(a, w)
+
+
+def test_checkpoint_rejects_bad_files(tmp_path):
+    p, s = make_case_ns("kicked_viscous")
+    path = tmp_path / "ck.bin"
+    with Ns2dSolver(p) as g:
+        g.upload(s)
+        g.save_checkpoint(path)
+    raw = bytearray(path.read_bytes())
+    raw[200] ^= 0xFF
+    bad = tmp_path / "bad.bin"
+    bad.write_bytes(bytes(raw))
+    with Ns2dSolver(p) as g:
+        for f, code in ((bad, L.CC_ERR_ARG), (tmp_path / "missing.bin", L.CC_ERR_IO)):
+            with pytest.raises(CcError) as e:
+                g.load_checkpoint(f)
+            assert e.value.code == code
+    q, _ = make_case_ns("collapse_ic")   # another grid
+    with Ns2dSolver(q) as g:
+        with pytest.raises(CcError) as e:
+            g.load_checkpoint(path)
+        assert e.value.code == L.CC_ERR_ARG
