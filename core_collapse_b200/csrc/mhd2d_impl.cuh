@@ -53,8 +53,8 @@ cudaError_t M2Launch<T>::prepare(int nx, int ny) {
         }
     }
     constexpr int CW = (sizeof(T) == 8) ? 2 : 4;
-    const int smem_row = (int)(sizeof(Cplx<T>) * (size_t)nx);
-    const int smem_col = (int)(sizeof(Cplx<T>) * (size_t)ny * CW);
+    const int smem_row = (int)(sizeof(Cplx<T>) * (size_t)fft_line_slots(nx));
+    const int smem_col = (int)(sizeof(Cplx<T>) * (size_t)fft_line_slots(ny) * CW);
     if (smem_row <= 227 * 1024 && smem_col <= 227 * 1024) {  // larger lines are rejected by the solver set-up
         CC_ATTR(fft_rows_fwd_kernel<T>, smem_row)
         CC_ATTR(fft_rows_inv_kernel<T>, smem_row)
@@ -136,8 +136,8 @@ cudaError_t M2Launch<T>::fft_solve(const T* rho, int pitch, const double* rho_pa
                                    const Cplx<T>* twy_i, double Lx, double Ly, double G, Cplx<T>* A, T* phi,
                                    const int* active, cudaStream_t s) {
     constexpr int CW = (sizeof(T) == 8) ? 2 : 4;  // 32-byte column strips
-    const size_t smem_row = sizeof(Cplx<T>) * (size_t)nx;
-    const size_t smem_col = sizeof(Cplx<T>) * (size_t)ny * CW;
+    const size_t smem_row = sizeof(Cplx<T>) * (size_t)fft_line_slots(nx);
+    const size_t smem_col = sizeof(Cplx<T>) * (size_t)fft_line_slots(ny) * CW;
     cudaError_t e;
     const int nt_row = nx >= 1024 ? 512 : (nx >= 256 ? 256 : 128);
     fft_rows_fwd_kernel<T><<<ny, nt_row, smem_row, s>>>(rho, pitch, rho_part, RED_BLOCKS, (double)nx * (double)ny, A,

@@ -32,29 +32,73 @@ template <class T> __device__ __forceinline__ Cplx<T> cmul(Cplx<T> x, Cplx<T> w)
 
 __device__ __forceinline__ int bitrev(int i, int logn) { return (int)(__brev((unsigned)i) >> (32 - logn)); }
 
-// In-place radix-2 passes over `lines` independent transforms of length n held
-// in shared memory (line l at a + l*n, already in bit-reversed order).
-// tw: twiddles of all passes, pass with half-length h at tw[h-1 .. 2h-2].
+// Shared-memory slot of element i of a transform line: one spare slot after
+// every 16, so that the strided accesses of the grouped passes below hit
+// distinct banks.  A line of n elements takes fft_line_slots(n) slots.
+__host__ __device__ constexpr int fft_line_slots(int n) { return n + (n >> 4); }
+__device__ __forceinline__ int fpad(int i) { return i + (i >> 4); }
+
+// R consecutive radix-2 stages (half-lengths h0, 2 h0, ..., 2^(R-1) h0) of the
+// reference's DIT transform over `lines` lines of n elements in shared memory.
+// A thread takes the 2^R elements base + m h0 (m < 2^R) of one group, which
+// only exchange data among themselves in these stages, and runs the stages in
+// registers: every butterfly u = a[p], v = a[p+h] * tw[h-1 + (p mod h)],
+// a[p] = u + v, a[p+h] = u - v is the reference's, with the same operands and
+// twiddle, so the result is the same bit for bit as one stage per pass.
+template <class T, int R>
+__device__ __forceinline__ void fft_group_pass(Cplx<T>* a, int n, int lines, int h0,
+                                               const Cplx<T>* __restrict__ tw) {
+    constexpr int M = 1 << R;
+    const int gpl = n >> R;   // groups per line
+    const int L = fft_line_slots(n);
+    for (int g = threadIdx.x; g < lines * gpl; g += blockDim.x) {
+        const int l = g / gpl, gg = g - l * gpl;
+        const int o = gg & (h0 - 1), blk = gg / h0;
+        Cplx<T>* line = a + l * L;
+        const int base = blk * (M * h0) + o;
+        Cplx<T> x[M];
+#pragma unroll
+        for (int m = 0; m < M; m++) x[m] = line[fpad(base + m * h0)];
+#pragma unroll
+        for (int st = 0; st < R; st++) {
+            const int hs = 1 << st, h = h0 << st;
+#pragma unroll
+            for (int m = 0; m < M; m++) {
+                if (m & hs) continue;
+                const Cplx<T> w = tw[h - 1 + o + (m & (hs - 1)) * h0];   // p mod h = o + (m mod hs) h0
+                const Cplx<T> u = x[m];
+                const Cplx<T> v = cmul(x[m + hs], w);
+                x[m].re = u.re + v.re; x[m].im = u.im + v.im;
+                x[m + hs].re = u.re - v.re; x[m + hs].im = u.im - v.im;
+            }
+        }
+#pragma unroll
+        for (int m = 0; m < M; m++) line[fpad(base + m * h0)] = x[m];
+    }
+    __syncthreads();
+}
+
+// All log2(n) stages over `lines` lines already in bit-reversed order (line l
+// at a + l fft_line_slots(n), padded slots), four stages per pass.
+// tw: twiddles of all stages, half-length h at tw[h-1 .. 2h-2].
 template <class T>
 __device__ __forceinline__ void fft_passes(Cplx<T>* a, int n, int lines, const Cplx<T>* __restrict__ tw) {
-    const int nb = lines * (n >> 1);
-    for (int h = 1; h < n; h <<= 1) {
-        for (int b = threadIdx.x; b < nb; b += blockDim.x) {
-            const int l = b / (n >> 1), bb = b % (n >> 1);
-            const int jj = bb & (h - 1);
-            const int i = l * n + ((bb - jj) << 1) + jj;
-            const Cplx<T> u = a[i];
-            const Cplx<T> v = cmul(a[i + h], tw[h - 1 + jj]);
-            a[i].re = u.re + v.re; a[i].im = u.im + v.im;
-            a[i + h].re = u.re - v.re; a[i + h].im = u.im - v.im;
-        }
-        __syncthreads();
+    int h0 = 1;
+    while (h0 < n) {
+        const int left = n / h0;
+        if (left >= 16) { fft_group_pass<T, 4>(a, n, lines, h0, tw); h0 <<= 4; }
+        else if (left == 8) { fft_group_pass<T, 3>(a, n, lines, h0, tw); h0 <<= 3; }
+        else if (left == 4) { fft_group_pass<T, 2>(a, n, lines, h0, tw); h0 <<= 2; }
+        else { fft_group_pass<T, 1>(a, n, lines, h0, tw); h0 <<= 1; }
     }
 }
 
+// the three kernels below run on at most FFT_NT threads
+constexpr int FFT_NT = 512;
+
 // pass 1: one block per row.  rho is a pitched T field; mean = sum/N.
 template <class T>
-__global__ void fft_rows_fwd_kernel(const T* __restrict__ rho, int pitch, const double* __restrict__ rho_part,
+__global__ void __launch_bounds__(FFT_NT) fft_rows_fwd_kernel(const T* __restrict__ rho, int pitch, const double* __restrict__ rho_part,
                                     int nparts, double ncell, Cplx<T>* __restrict__ A, int nx, int logn,
                                     const Cplx<T>* __restrict__ tw, const int* __restrict__ active) {
     if (active && *active == 0) return;
@@ -73,26 +117,27 @@ __global__ void fft_rows_fwd_kernel(const T* __restrict__ rho, int pitch, const 
         Cplx<T> z;
         z.re = rho[(size_t)j * pitch + i] - mean;
         z.im = T(0);
-        a[bitrev(i, logn)] = z;
+        a[fpad(bitrev(i, logn))] = z;
     }
     __syncthreads();
     fft_passes(a, nx, 1, tw);
-    for (int i = threadIdx.x; i < nx; i += blockDim.x) A[(size_t)j * nx + i] = a[i];
+    for (int i = threadIdx.x; i < nx; i += blockDim.x) A[(size_t)j * nx + i] = a[fpad(i)];
 }
 
 // pass 2: CW adjacent columns per block: forward FFT along y, spectral
 // multiply, inverse FFT along y.
 template <class T, int CW>
-__global__ void fft_cols_solve_kernel(Cplx<T>* __restrict__ A, int nx, int ny, int logn,
+__global__ void __launch_bounds__(FFT_NT) fft_cols_solve_kernel(Cplx<T>* __restrict__ A, int nx, int ny, int logn,
                                       const Cplx<T>* __restrict__ twf, const Cplx<T>* __restrict__ twi,
                                       double Lx, double Ly, double G, const int* __restrict__ active) {
     if (active && *active == 0) return;
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    Cplx<T>* a = reinterpret_cast<Cplx<T>*>(smem_raw);   // CW lines of ny
+    Cplx<T>* a = reinterpret_cast<Cplx<T>*>(smem_raw);   // CW padded lines of ny
+    const int L = fft_line_slots(ny);
     const int c0 = blockIdx.x * CW;
     for (int k = threadIdx.x; k < CW * ny; k += blockDim.x) {
         const int cc = k % CW, j = k / CW;
-        a[cc * ny + bitrev(j, logn)] = A[(size_t)j * nx + c0 + cc];
+        a[cc * L + fpad(bitrev(j, logn))] = A[(size_t)j * nx + c0 + cc];
     }
     __syncthreads();
     fft_passes(a, ny, CW, twf);
@@ -105,7 +150,7 @@ __global__ void fft_cols_solve_kernel(Cplx<T>* __restrict__ A, int nx, int ny, i
         const double ky = two_pi * (double)nj / Ly;
         const double kx = two_pi * (double)ni / Lx;
         const double k2 = kx * kx + ky * ky;
-        Cplx<T>& z = a[cc * ny + j];
+        Cplx<T>& z = a[cc * L + fpad(j)];
         if (k2 == 0.0) { z.re = T(0); z.im = T(0); }
         else {
             const T s = (T)(-(4.0 * M_PI * G) / k2);
@@ -116,14 +161,18 @@ __global__ void fft_cols_solve_kernel(Cplx<T>* __restrict__ A, int nx, int ny, i
     // bit-reverse permutation of each line for the inverse DIT transform
     for (int k = threadIdx.x; k < CW * ny; k += blockDim.x) {
         const int cc = k / ny, j = k % ny, r = bitrev(j, logn);
-        if (j < r) { Cplx<T> t = a[cc * ny + j]; a[cc * ny + j] = a[cc * ny + r]; a[cc * ny + r] = t; }
+        if (j < r) {
+            Cplx<T> t = a[cc * L + fpad(j)];
+            a[cc * L + fpad(j)] = a[cc * L + fpad(r)];
+            a[cc * L + fpad(r)] = t;
+        }
     }
     __syncthreads();
     fft_passes(a, ny, CW, twi);
     const T n = (T)ny;
     for (int k = threadIdx.x; k < CW * ny; k += blockDim.x) {
         const int cc = k % CW, j = k / CW;
-        Cplx<T> z = a[cc * ny + j];
+        Cplx<T> z = a[cc * L + fpad(j)];
         z.re = z.re / n; z.im = z.im / n;
         A[(size_t)j * nx + c0 + cc] = z;
     }
@@ -131,17 +180,17 @@ __global__ void fft_cols_solve_kernel(Cplx<T>* __restrict__ A, int nx, int ny, i
 
 // pass 3: inverse FFT along x, real part -> phi (pitched).
 template <class T>
-__global__ void fft_rows_inv_kernel(const Cplx<T>* __restrict__ A, int nx, int logn, const Cplx<T>* __restrict__ tw,
+__global__ void __launch_bounds__(FFT_NT) fft_rows_inv_kernel(const Cplx<T>* __restrict__ A, int nx, int logn, const Cplx<T>* __restrict__ tw,
                                     T* __restrict__ phi, int pitch, const int* __restrict__ active) {
     if (active && *active == 0) return;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     Cplx<T>* a = reinterpret_cast<Cplx<T>*>(smem_raw);
     const int j = blockIdx.x;
-    for (int i = threadIdx.x; i < nx; i += blockDim.x) a[bitrev(i, logn)] = A[(size_t)j * nx + i];
+    for (int i = threadIdx.x; i < nx; i += blockDim.x) a[fpad(bitrev(i, logn))] = A[(size_t)j * nx + i];
     __syncthreads();
     fft_passes(a, nx, 1, tw);
     const T n = (T)nx;
-    for (int i = threadIdx.x; i < nx; i += blockDim.x) phi[(size_t)j * pitch + i] = a[i].re / n;
+    for (int i = threadIdx.x; i < nx; i += blockDim.x) phi[(size_t)j * pitch + i] = a[fpad(i)].re / n;
 }
 
 // ---------------------------------------------------------------------------
