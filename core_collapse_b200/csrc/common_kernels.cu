@@ -8,9 +8,14 @@ namespace ccb {
 __global__ void m2_dt_finalize_kernel(const double* __restrict__ spd_part, int nparts, DtSpec d,
                                       double* __restrict__ dt_out, const double* __restrict__ t_now,
                                       int* __restrict__ active) {
-    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    if (threadIdx.x >= 32 || blockIdx.x != 0) return;
+    // one warp: each lane folds a strided share of the partials into the seed
+    // (a NaN partial never wins), then the lanes' maxima are combined; max is
+    // exact, so the order does not matter
     double maxs = d.seed;
-    for (int b = 0; b < nparts; b++) maxs = vmax(maxs, spd_part[b]);
+    for (int b = threadIdx.x; b < nparts; b += 32) maxs = vmax(maxs, spd_part[b]);
+    for (int o = 16; o > 0; o >>= 1) maxs = vmax(maxs, __shfl_xor_sync(0xffffffffu, maxs, o));
+    if (threadIdx.x != 0) return;
     const double dt_h = d.cfl * d.hmin / maxs;
     double dt = dt_h;
     if (d.cap) {

@@ -98,20 +98,24 @@ __device__ __forceinline__ void ns_hllc(const NSConst<T>& c, T dL, T nL, T tL, T
     F[3] = F[3] + S * (Es - E);
 }
 
+// Tile TX x TY on NT threads, MINB CTAs per SM.  NT covers the larger face
+// count ((TX+1) TY or TX (TY+1)) so that each face loop is one round; the
+// extra threads idle in the update.
 template <class T> struct NSTile;
-template <> struct NSTile<double> { static constexpr int TX = 32, TY = 8; };
-template <> struct NSTile<float> { static constexpr int TX = 32, TY = 16; };
+template <> struct NSTile<double> { static constexpr int TX = 32, TY = 8, NT = 288, MINB = 2; };
+template <> struct NSTile<float> { static constexpr int TX = 32, TY = 16, NT = 544, MINB = 3; };
 
 template <class T> struct NSGeom {
-    static constexpr int TX = NSTile<T>::TX, TY = NSTile<T>::TY;
+    static constexpr int TX = NSTile<T>::TX, TY = NSTile<T>::TY, NT = NSTile<T>::NT, MINB = NSTile<T>::MINB;
     static constexpr int RX = TX + 4, RY = TY + 4, RR = RX * RY;   // primitives, halo 2
     static constexpr int GX = TX + 2, GY = TY + 2, GR = GX * GY;   // gradients, halo 1
-    static constexpr int NFX = (TX + 1) * TY, NGY = TX * (TY + 1), NT = TX * TY;
+    static constexpr int NFX = (TX + 1) * TY, NGY = TX * (TY + 1), NC = TX * TY;
+    static_assert(NT >= NFX && NT >= NGY && NT % 32 == 0, "one round per face loop");
     static constexpr size_t smem = sizeof(T) * (size_t)(4 * RR + 4 * GR + 4 * NFX + 4 * NGY);
 };
 
 template <class T, bool STAGE2>
-__global__ void __launch_bounds__(NSGeom<T>::NT, 2)
+__global__ void __launch_bounds__(NSGeom<T>::NT, NSGeom<T>::MINB)
 ns_stage_kernel(const NSConst<T> c, const NSFields<T> un, const NSFields<T> in, const NSFields<T> k1,
                 const NSFields<T> out, const T* __restrict__ phi, const double* __restrict__ dtp,
                 const int* __restrict__ active) {
@@ -201,6 +205,7 @@ ns_stage_kernel(const NSConst<T> c, const NSFields<T> un, const NSFields<T> in, 
     }
     __syncthreads();
 
+    if (tid >= G::NC) return;
     const int tx = tid % TX, ty = tid / TX;
     const int gi = i0 + tx, gj = j0 + ty;
     if (gi >= c.nx || gj >= c.ny) return;
@@ -320,12 +325,19 @@ template <class D>
 __global__ void ns_dt_kernel(const D* __restrict__ spd_part, const D* __restrict__ rmin_part, int nparts,
                              NSDtSpec d, D* __restrict__ dt_out, const D* __restrict__ t_now,
                              int* __restrict__ active) {
-    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    if (threadIdx.x >= 32 || blockIdx.x != 0) return;
+    // one warp: strided shares of the partials, then the lanes combined (max
+    // and min are exact, so the order does not matter)
     D smax = 0.0, rho_min = 1e300;
-    for (int b = 0; b < nparts; b++) {
+    for (int b = threadIdx.x; b < nparts; b += 32) {
         smax = vmax(smax, spd_part[b]);
         rho_min = vmin(rho_min, rmin_part[b]);
     }
+    for (int o = 16; o > 0; o >>= 1) {
+        smax = vmax(smax, __shfl_xor_sync(0xffffffffu, smax, o));
+        rho_min = vmin(rho_min, __shfl_xor_sync(0xffffffffu, rho_min, o));
+    }
+    if (threadIdx.x != 0) return;
     const D dt_hyp = (smax > 0.0) ? (d.cfl * d.hmin / smax) : 1e-6;
     D dt = dt_hyp;
     if (d.viscous) {
