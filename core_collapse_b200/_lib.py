@@ -25,6 +25,7 @@ CC_POISSON_SOR = 0
 CC_POISSON_FFT = 1
 CC_POISSON_DIRECT = 2
 CC_GRAVITY_ENCLOSED = 3
+CC_GRAVITY_SHELLS = 4
 CC_BATCH_MAX_DIRECT_SIDE = 2048
 
 
@@ -72,6 +73,8 @@ class CcEuler2dParams(C.Structure):
         ("G", C.c_double), ("softening", C.c_double),
         ("sor_tol", C.c_double), ("sor_omega", C.c_double),
         ("poisson_kind", C.c_int32), ("precision", C.c_int32),
+        ("Nr_bins", C.c_int32), ("reserved", C.c_int32),
+        ("xc", C.c_double), ("yc", C.c_double),
     ]
 
 

@@ -60,6 +60,9 @@ template <class T> struct Euler2d : Euler2dBase {
     double* enc_cum = nullptr;
     double* enc_blk = nullptr;
     bool enclosed() const { return p.gravity_on && p.poisson_kind == CC_GRAVITY_ENCLOSED; }
+    bool shells() const { return p.gravity_on && p.poisson_kind == CC_GRAVITY_SHELLS; }
+    bool radial() const { return enclosed() || shells(); }   // gravity as arrays, no Poisson solve
+    double* shl_geo = nullptr;   // shells: per sorted cell rx, ry, (r^2 + softening^2)^(3/2)
     bool loaded = false;
     cudaGraphExec_t graph1 = nullptr;
     cudaStream_t graph_stream = nullptr;
@@ -78,7 +81,7 @@ template <class T> struct Euler2d : Euler2dBase {
         if (graph1) cudaGraphExecDestroy(graph1);
         void* ptrs[] = {block, phi, g2[0], g2[1], rhs, sphi, sor_part, sor_part2, staging, spd_part, rho_part,
                         diag_part, scal, bar, steps_dev, iflags, derived_dev, enc_order, enc_gend, enc_cum,
-                        enc_blk};
+                        enc_blk, shl_geo};
         for (void* q : ptrs)
             if (q) cudaFree(q);
     }
@@ -99,7 +102,8 @@ template <class T> struct Euler2d : Euler2dBase {
         c.gravity_on = p.gravity_on ? 1 : 0;
         plane = (size_t)P * (ny + 1);
         if (p.gravity_on) {
-            if (p.poisson_kind != CC_POISSON_SOR && p.poisson_kind != CC_GRAVITY_ENCLOSED)
+            if (p.poisson_kind != CC_POISSON_SOR && p.poisson_kind != CC_GRAVITY_ENCLOSED &&
+                p.poisson_kind != CC_GRAVITY_SHELLS)
                 return fail(h, CC_ERR_UNSUPPORTED, "the Euler/HLLC solver supports SOR or enclosed-mass gravity");
             if (p.poisson_kind == CC_POISSON_SOR && ((nx & 1) || (ny & 1)))
                 return fail(h, CC_ERR_UNSUPPORTED, "red-black SOR needs even Nx and Ny (periodic)");
@@ -112,12 +116,12 @@ template <class T> struct Euler2d : Euler2dBase {
         U1 = EHFields<T>{b + 4 * plane, b + 5 * plane, b + 6 * plane, b + 7 * plane};
         CC_CUDA(cudaMalloc(&phi, sizeof(T) * plane));
         CC_CUDA(cudaMemsetAsync(phi, 0, sizeof(T) * plane, st()));
-        if (enclosed()) {   // gravity arrays written by every solve, the radius order built once
+        if (radial()) {   // gravity arrays written by every solve, the radius order built once
             CC_CUDA(cudaMalloc(&g2[0], sizeof(T) * plane));
             CC_CUDA(cudaMalloc(&g2[1], sizeof(T) * plane));
             CC_CUDA(cudaMemsetAsync(g2[0], 0, sizeof(T) * plane, st()));
             CC_CUDA(cudaMemsetAsync(g2[1], 0, sizeof(T) * plane, st()));
-            if (int r = enclosed_setup()) return r;
+            if (int r = enclosed() ? enclosed_setup() : shells_setup()) return r;
         }
         CC_CUDA(cudaMalloc(&staging, sizeof(double) * (size_t)(nx + 1) * (ny + 1)));
         CC_CUDA(cudaMalloc(&spd_part, sizeof(double) * RED_BLOCKS));
@@ -208,14 +212,78 @@ template <class T> struct Euler2d : Euler2dBase {
         return CC_OK;
     }
 
-    // gravity arrays of the stage kernel: g2 in the enclosed-mass mode, none for SOR (phi)
-    const T* gxa() const { return enclosed() ? g2[0] : nullptr; }
-    const T* gya() const { return enclosed() ? g2[1] : nullptr; }
+    // shell-binned enclosed mass (gravity_accel_from_enclosed_mass, gravity_enclosed.h:18-96):
+    // the shells depend only on the grid, so each cell's shell is found once and
+    // the cells are ordered by shell (index order inside a shell, the reference's
+    // deposit order); the scan of enclosed_kernels.cuh then gives M(<shell) at
+    // each shell's end.  The geometry factors (the reference's std::pow) are
+    // built here on the host, in the sorted order.
+    int shells_setup() {
+        const int nx = p.Nx, ny = p.Ny, n = nx * ny;
+        const double dx = (p.x1 - p.x0) / nx, dy = (p.y1 - p.y0) / ny;
+        auto xof = [&](int i) { return p.x0 + (i + 0.5) * dx; };
+        auto yof = [&](int j) { return p.y0 + (j + 0.5) * dy; };
+        double rmax = 0.0;
+        for (int j = 0; j < ny; ++j)
+            for (int i = 0; i < nx; ++i) {
+                const double ddx = xof(i) - p.xc, ddy = yof(j) - p.yc;
+                rmax = std::max(rmax, std::sqrt(ddx * ddx + ddy * ddy));
+            }
+        rmax = std::max(rmax, 1e-12);
+        const int nr = std::max(8, p.Nr_bins);
+        const double dr = rmax / (double)nr;
+        std::vector<int> bin(n), count(nr + 1, 0);
+        for (int j = 0; j < ny; ++j)
+            for (int i = 0; i < nx; ++i) {
+                const double ddx = xof(i) - p.xc, ddy = yof(j) - p.yc;
+                int b = (int)std::floor(std::sqrt(ddx * ddx + ddy * ddy) / dr);
+                b = b < 0 ? 0 : (b >= nr ? nr - 1 : b);
+                bin[j * nx + i] = b;
+                count[b + 1]++;
+            }
+        for (int b = 0; b < nr; ++b) count[b + 1] += count[b];   // shell starts
+        std::vector<int> order(n), gend(n), fill(count.begin(), count.end() - 1);
+        for (int k = 0; k < n; ++k) order[fill[bin[k]]++] = k;   // stable: index order inside a shell
+        std::vector<double> geo(3 * (size_t)n);
+        const double eps2 = p.softening * p.softening;
+        for (int t = 0; t < n; ++t) {
+            const int k = order[t], i = k % nx, j = k / nx;
+            gend[t] = count[bin[k] + 1];
+            const double ddx = xof(i) - p.xc, ddy = yof(j) - p.yc;
+            geo[t] = ddx;
+            geo[n + t] = ddy;
+            geo[2 * (size_t)n + t] = std::pow(ddx * ddx + ddy * ddy + eps2, 1.5);
+        }
+        const int nb = (n + ENC_NT - 1) / ENC_NT;
+        CC_CUDA(cudaMalloc(&enc_order, sizeof(int) * n));
+        CC_CUDA(cudaMalloc(&enc_gend, sizeof(int) * n));
+        CC_CUDA(cudaMalloc(&enc_cum, sizeof(double) * n));
+        CC_CUDA(cudaMalloc(&enc_blk, sizeof(double) * nb));
+        CC_CUDA(cudaMalloc(&shl_geo, sizeof(double) * geo.size()));
+        CC_CUDA(cudaMemcpyAsync(enc_order, order.data(), sizeof(int) * n, cudaMemcpyHostToDevice, st()));
+        CC_CUDA(cudaMemcpyAsync(enc_gend, gend.data(), sizeof(int) * n, cudaMemcpyHostToDevice, st()));
+        CC_CUDA(cudaMemcpyAsync(shl_geo, geo.data(), sizeof(double) * geo.size(), cudaMemcpyHostToDevice, st()));
+        CC_CUDA(cudaStreamSynchronize(st()));   // the host vectors go out of scope
+        return CC_OK;
+    }
+
+    // gravity arrays of the stage kernel: g2 in the enclosed-mass modes, none for SOR (phi)
+    const T* gxa() const { return radial() ? g2[0] : nullptr; }
+    const T* gya() const { return radial() ? g2[1] : nullptr; }
 
     // Poisson on a density field whose floored sum is in rho_part -> phi;
     // in the enclosed-mass mode the gravity itself -> g2
     int solve(const T* rho) {
         if (!p.gravity_on) return CC_OK;
+        if (shells()) {
+            h->perf.poisson_solves += 1;
+            const int n = p.Nx * p.Ny;
+            const double dx = (p.x1 - p.x0) / p.Nx, dy = (p.y1 - p.y0) / p.Ny;
+            CC_CUDA(EHLaunch<T>::shells(c, rho, enc_order, enc_gend, n, enc_cum, enc_blk, shl_geo, dx * dy, p.G,
+                                        p.floor_rho, g2[0], g2[1], active(), st()));
+            count(3);
+            return CC_OK;
+        }
         if (enclosed()) {
             h->perf.poisson_solves += 1;
             const int nx = p.Nx, ny = p.Ny;
@@ -269,7 +337,7 @@ template <class T> struct Euler2d : Euler2dBase {
         int one = 1;
         CC_CUDA(cudaMemcpyAsync(iflags, &one, sizeof(int), cudaMemcpyHostToDevice, st()));
         if (p.gravity_on) {
-            if (!enclosed()) {
+            if (!radial()) {
                 CC_CUDA(EHLaunch<T>::rho_sum(c, U.rho, rho_part, st()));
                 count(1);
             }
@@ -279,7 +347,7 @@ template <class T> struct Euler2d : Euler2dBase {
             CC_CUDA(cudaMalloc(&g2[0], sizeof(T) * plane));
             CC_CUDA(cudaMalloc(&g2[1], sizeof(T) * plane));
         }
-        if (enclosed()) {
+        if (radial()) {
             // g2 holds the enclosed-mass gravity from solve()
         } else if (p.gravity_on) {
             CC_CUDA(M2Launch<T>::gravity_from_phi(phi, nx, ny, P, c.pax, c.pay, c.two_dx, c.two_dy, g2[0], g2[1], st()));
@@ -310,7 +378,7 @@ template <class T> struct Euler2d : Euler2dBase {
     // rk2_step (EH:529-550) with dt in dt_dev; the RHS solves Poisson itself (EH:411)
     int step_body() {
         if (p.gravity_on) {
-            if (!enclosed()) {   // the SOR's density mean
+            if (!radial()) {   // the SOR's density mean
                 CC_CUDA(EHLaunch<T>::rho_sum(c, U.rho, rho_part, st()));
                 count(1);
             }
@@ -319,7 +387,7 @@ template <class T> struct Euler2d : Euler2dBase {
         CC_CUDA(EHLaunch<T>::stage(c, U, U, U1, false, phi, gxa(), gya(), dt_dev(), active(), st()));
         count(1);
         if (p.gravity_on) {
-            if (!enclosed()) {
+            if (!radial()) {
                 CC_CUDA(EHLaunch<T>::rho_sum(c, U1.rho, rho_part, st()));
                 count(1);
             }
@@ -474,6 +542,7 @@ void cc_euler2d_params_default(cc_euler2d_params* p) {
     p->G = 1.0; p->softening = 1e-4;
     p->sor_tol = 1e-10; p->sor_omega = 1.7;
     p->poisson_kind = CC_POISSON_SOR; p->precision = CC_FP64;
+    p->Nr_bins = 512; p->xc = 0.5; p->yc = 0.5;
 }
 
 int cc_euler2d_create(const cc_euler2d_params* p, cc_handle** out) {

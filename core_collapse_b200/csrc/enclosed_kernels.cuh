@@ -12,6 +12,8 @@
 //   3. reads M_enc at each group end and writes g            -- enc_gravity_kernel
 // FP64 sums throughout; the association of the scan differs from the
 // reference's running sum (relative differences at the 1e-16 level).
+// The shell-binned provider of gravity_enclosed.h reuses steps 1-2 with the
+// cells ordered by shell (enc_shell_gravity_kernel below).
 #pragma once
 #include "cc_device.cuh"
 
@@ -101,6 +103,34 @@ __global__ void enc_gravity_kernel(const int* __restrict__ order, const int* __r
             vy = gmag * (ry / r);
         }
         const size_t q = (size_t)j * pitch + i;
+        gx[q] = (T)vx;
+        gy[q] = (T)vy;
+    }
+}
+
+// Shell-binned variant (gravity_accel_from_enclosed_mass, gravity_enclosed.h:18-96):
+// cells ordered by shell, gend[t] the end of t's shell, so M(<shell) is the
+// scan at the shell's end; geo (3 n doubles, sorted order) holds each cell's
+// rx, ry and (r^2 + softening^2)^(3/2) from the host.
+// g = -G M(<shell) / denom * (rx, ry); 0 where denom <= 0.
+template <class T>
+__global__ void enc_shell_gravity_kernel(const int* __restrict__ order, const int* __restrict__ gend,
+                                         const double* __restrict__ cum, const double* __restrict__ blk,
+                                         const double* __restrict__ geo, int n, int nx, int pitch, double G,
+                                         T* __restrict__ gx, T* __restrict__ gy, const int* __restrict__ active) {
+    if (active && *active == 0) return;
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
+        const int e = gend[t] - 1;
+        const double menc = cum[e] + blk[e / ENC_NT];
+        const int k = order[t];
+        const double denom = geo[2 * (size_t)n + t];
+        double vx = 0.0, vy = 0.0;
+        if (!(denom <= 0.0)) {
+            const double gcoef = -G * menc / denom;
+            vx = gcoef * geo[t];
+            vy = gcoef * geo[(size_t)n + t];
+        }
+        const size_t q = (size_t)(k / nx) * pitch + (k % nx);
         gx[q] = (T)vx;
         gy[q] = (T)vy;
     }

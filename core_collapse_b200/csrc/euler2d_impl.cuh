@@ -41,6 +41,21 @@ cudaError_t EHLaunch<T>::enclosed(const EHConst<T>& c, const T* rho, const int* 
 }
 
 template <class T>
+cudaError_t EHLaunch<T>::shells(const EHConst<T>& c, const T* rho, const int* order, const int* gend, int n,
+                                double* cum, double* blk, const double* geo, double cell_area, double G,
+                                double floor_rho, T* gx, T* gy, const int* active, cudaStream_t s) {
+    const int nb = (n + ENC_NT - 1) / ENC_NT;
+    enc_scan_kernel<T><<<nb, ENC_NT, 0, s>>>(rho, c.pitch, c.nx, order, n, floor_rho, cell_area, cum, blk, active);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    enc_blocks_kernel<double><<<1, ENC_NT, 0, s>>>(blk, nb, active);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    const int g = nb < 4096 ? nb : 4096;
+    enc_shell_gravity_kernel<T><<<g, ENC_NT, 0, s>>>(order, gend, cum, blk, geo, n, c.nx, c.pitch, G, gx, gy, active);
+    return cudaGetLastError();
+}
+
+template <class T>
 cudaError_t EHLaunch<T>::speeds(const EHConst<T>& c, const EHFields<T>& st, double* spd_part, double* rho_part,
                                 cudaStream_t s) {
     eh_speed_kernel<T, RED_NT><<<RED_BLOCKS, RED_NT, 0, s>>>(c, st, spd_part, rho_part);

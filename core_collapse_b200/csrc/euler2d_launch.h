@@ -23,6 +23,11 @@ template <class T> struct EHLaunch {
                                 double* cum, double* blk, double x0, double y0, double dx, double dy, double cx,
                                 double cy, double G, double soft2, double floor_rho, T* gx, T* gy, const int* active,
                                 cudaStream_t s);
+    // shell-binned enclosed-mass gravity: order / gend by shell, geo the sorted
+    // cells' rx, ry and (r^2 + softening^2)^(3/2) (3 n doubles)
+    static cudaError_t shells(const EHConst<T>& c, const T* rho, const int* order, const int* gend, int n, double* cum,
+                              double* blk, const double* geo, double cell_area, double G, double floor_rho, T* gx,
+                              T* gy, const int* active, cudaStream_t s);
     static cudaError_t speeds(const EHConst<T>& c, const EHFields<T>& st, double* spd_part, double* rho_part,
                               cudaStream_t s);
     static cudaError_t rho_sum(const EHConst<T>& c, const T* rho, double* rho_part, cudaStream_t s);

@@ -52,6 +52,9 @@ extern "C" {
 #define CC_POISSON_DIRECT 2 /* exact solve of the SOR's discrete problem (batched ensemble, cc_batch.h) */
 #define CC_GRAVITY_ENCLOSED 3 /* Euler/HLLC only: enclosed-mass radial gravity, compute_enclosed_mass_gravity
                                  (euler2d_gravity_hllc.cpp:226-286, the rhs's commented-out alternative, EH:411) */
+#define CC_GRAVITY_SHELLS 4   /* Euler/HLLC only: radial gravity from cell masses binned into Nr_bins radial
+                                 shells about (xc, yc), gravity_accel_from_enclosed_mass
+                                 (gravity_enclosed.h:18-96) */
 
 typedef struct cc_handle cc_handle;
 
@@ -129,6 +132,11 @@ typedef struct cc_euler2d_params {
     double sor_omega;       /* 1.7   */
     int32_t poisson_kind;   /* addition */
     int32_t precision;      /* addition */
+    /* the shell-binned provider's knobs (CC_GRAVITY_SHELLS; Params of the
+       solver that includes gravity_enclosed.h, euler2d_h5.cpp:42-45) */
+    int32_t Nr_bins;        /* 512: radial shells (at least 8 are used)    */
+    int32_t reserved;
+    double xc, yc;          /* 0.5, 0.5: gravity centre                     */
 } cc_euler2d_params;
 
 /*

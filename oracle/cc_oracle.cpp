@@ -190,6 +190,55 @@ void enclosed_mass_gravity(const cc_euler2d_params* c, const std::vector<double>
     }
 }
 
+// Shell-binned enclosed-mass gravity (gravity_accel_from_enclosed_mass,
+// gravity_enclosed.h:18-96): r_max over the cell centres (at least 1e-12),
+// Nr = max(8, Nr_bins) shells of width r_max / Nr about (xc, yc); the floored
+// cell masses deposited into shells in index order, their running sum over
+// shells, g = -G M(<shell) r_vec / (r^2 + softening^2)^(3/2).
+void shell_mass_gravity(const cc_euler2d_params* c, const std::vector<double>& rho, std::vector<double>& gx,
+                        std::vector<double>& gy) {
+    const int nx = c->Nx, ny = c->Ny;
+    const size_t N = (size_t)nx * ny;
+    gx.assign(N, 0.0);
+    gy.assign(N, 0.0);
+    const double dx = (c->x1 - c->x0) / nx, dy = (c->y1 - c->y0) / ny;
+    auto xc_of = [&](int i) { return c->x0 + (i + 0.5) * dx; };
+    auto yc_of = [&](int j) { return c->y0 + (j + 0.5) * dy; };
+    double rmax = 0.0;
+    for (int j = 0; j < ny; ++j)
+        for (int i = 0; i < nx; ++i) {
+            const double ddx = xc_of(i) - c->xc, ddy = yc_of(j) - c->yc;
+            rmax = std::max(rmax, std::sqrt(ddx * ddx + ddy * ddy));
+        }
+    rmax = std::max(rmax, 1e-12);
+    const int nr = std::max(8, c->Nr_bins);
+    const double dr = rmax / (double)nr;
+    auto bin = [&](double r) {
+        int b = (int)std::floor(r / dr);
+        return b < 0 ? 0 : (b >= nr ? nr - 1 : b);
+    };
+    std::vector<double> shell((size_t)nr, 0.0), menc((size_t)nr, 0.0);
+    const double dA = dx * dy;
+    for (int j = 0; j < ny; ++j)
+        for (int i = 0; i < nx; ++i) {
+            const double ddx = xc_of(i) - c->xc, ddy = yc_of(j) - c->yc;
+            shell[(size_t)bin(std::sqrt(ddx * ddx + ddy * ddy))] += std::max(rho[(size_t)j * nx + i], c->floor_rho) * dA;
+        }
+    double run = 0.0;
+    for (int b = 0; b < nr; ++b) menc[(size_t)b] = (run += shell[(size_t)b]);
+    const double eps2 = c->softening * c->softening;
+    for (int j = 0; j < ny; ++j)
+        for (int i = 0; i < nx; ++i) {
+            const double ddx = xc_of(i) - c->xc, ddy = yc_of(j) - c->yc;
+            const double r2 = ddx * ddx + ddy * ddy;
+            const double denom = std::pow(r2 + eps2, 1.5);
+            if (denom <= 0.0) continue;
+            const double gcoef = -c->G * menc[(size_t)bin(std::sqrt(r2))] / denom;
+            gx[(size_t)j * nx + i] = gcoef * ddx;
+            gy[(size_t)j * nx + i] = gcoef * ddy;
+        }
+}
+
 PoissonResult eh_gravity(const cc_euler2d_params* c, const std::vector<double>& rho, std::vector<double>& gx,
                          std::vector<double>& gy, int mode) {
     PoissonSpec s = ehspec(c);
@@ -197,6 +246,7 @@ PoissonResult eh_gravity(const cc_euler2d_params* c, const std::vector<double>& 
     size_t N = (size_t)c->Nx * c->Ny;
     if (!c->gravity_on) { gx.assign(N, 0.0); gy.assign(N, 0.0); return r; }
     if (c->poisson_kind == CC_GRAVITY_ENCLOSED) { enclosed_mass_gravity(c, rho, gx, gy); return r; }
+    if (c->poisson_kind == CC_GRAVITY_SHELLS) { shell_mass_gravity(c, rho, gx, gy); return r; }
     std::vector<double> phi;
     if (mode == 2) {
         std::vector<double> fr(rho.begin(), rho.end());

@@ -90,7 +90,7 @@ def oracle() -> C.CDLL:
 
 
 def ref(name: str) -> C.CDLL | None:
-    """The reference solver library `name` in {mhd2d, mhd3d, euler2d, fft}, or None."""
+    """The reference solver library `name` in {mhd2d, mhd3d, euler2d, fft, ge}, or None."""
     if name not in _refs:
         path = REF_DIR / f"libref_{name}.so"
         if not path.exists() and REFERENCE_SRC.exists():
@@ -125,6 +125,9 @@ def ref(name: str) -> C.CDLL | None:
             R.ref_euler2d_enclosed_gravity.argtypes = [P2, _PP, _DP, _DP]
             R.ref_euler2d_init_random_blob.argtypes = [P2, _PP]
             R.ref_euler2d_main_loop.argtypes = [P2, _PP, C.c_int, _DP]
+        if R is not None and name == "ge":
+            R.ref_ge_gravity.argtypes = [C.c_int, C.c_int] + [C.c_double] * 6 + [C.c_int] + [C.c_double] * 3 + \
+                [_DP, _DP, _DP]
         if R is not None and name == "fft":
             R.ref_fft_poisson.argtypes = [C.c_int, C.c_int, C.c_double, C.c_double, C.c_double, C.c_double,
                                           C.c_double, _DP, _DP]
