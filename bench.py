@@ -351,6 +351,8 @@ def run_ours(args) -> None:
         line["mhd3d"] = run_3d(args, stream)
     if world == 1 and not args.skip_ns:
         line["ns2d"] = run_ns2d(args, stream, peaks)
+    if world == 1 and not args.skip_eh:
+        line["euler2d"] = run_euler2d(args, stream, peaks)
     if not args.skip_ensemble:
         line["ensemble"] = run_ensemble(args, stream, rank, world, barrier, max_over_ranks, value32 / world)
     if world == 1 and not args.skip_adjoint:
@@ -399,6 +401,46 @@ def run_3d(args, stream) -> dict:
                      "max_divB_end": d1["max_divB"], "energy_drift_rel": (d1["energy"] - d0["energy"]) / d0["energy"],
                      "mass_drift_rel": (d1["mass"] - d0["mass"]) / d0["mass"]}
     out["fp32_over_fp64"] = out["fp32"]["value"] / out["fp64"]["value"]
+    return out
+
+
+def run_euler2d(args, stream, peaks) -> dict:
+    """2D Euler/HLLC + gravity (euler2d_gravity_hllc.cpp): (1) the reference's
+    own case, init_random_blob (mt19937 seed 42) with its parameters (gamma
+    1.2, CFL 0.45, periodic unit square, G 1) and its red-black SOR to the
+    residual tolerance 1e-10 (omega 1.7), at --grid-eh; (2) the enclosed-mass
+    gravity provider (the rhs's alternative, EH:226-286) on the same IC at
+    --grid-eh-enclosed, where the fused stage kernel dominates.  FP64 and FP32."""
+    import torch
+
+    from core_collapse_b200.euler2d import Euler2dSolver, ParamsEH, ic_random_blob
+    out = {}
+    for tag, n, poisson, steps in (("sor", args.grid_eh, "sor", args.steps_eh_sor),
+                                   ("enclosed", args.grid_eh_enclosed, "enclosed", args.steps_eh)):
+        s0 = ic_random_blob(ParamsEH(Nx=n, Ny=n))
+        blk = {"workload": f"Euler/HLLC random blob (seed 42), {n}^2 periodic, "
+                           + ("red-black SOR to residual 1e-10" if poisson == "sor" else "enclosed-mass gravity"),
+               "steps": steps, "warmup": args.warmup}
+        for prec in ("fp32", "fp64"):
+            p = ParamsEH(Nx=n, Ny=n, precision=prec, poisson=poisson, t_end=1e30)
+            with Euler2dSolver(p) as g:
+                g.set_stream(stream.cuda_stream)
+                g.upload(s0)
+                g.advance(args.warmup, 0.0)
+                g.reset_perf()
+                torch.cuda.synchronize()
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                g.advance(steps)
+                e1.record(stream)
+                torch.cuda.synchronize()
+                ms = e0.elapsed_time(e1)
+                pf = g.perf()
+                d = g.diagnostics()
+            blk[prec] = {"value": n * n * steps / (ms / 1000.0), "unit": UNIT, "ms_per_step": ms / steps,
+                         "gpu_launches": pf["kernel_launches"], "poisson_sweeps_last": d["poisson_iters"],
+                         "nonfinite": d["nonfinite"]}
+        out[tag] = blk
     return out
 
 
@@ -592,6 +634,12 @@ def main():
     ap.add_argument("--grid3d", type=int, default=256)
     ap.add_argument("--steps3d", type=int, default=20)
     ap.add_argument("--skip-ns", action="store_true")
+    ap.add_argument("--skip-eh", action="store_true")
+    ap.add_argument("--grid-eh", type=int, default=512)
+    ap.add_argument("--steps-eh-sor", type=int, default=3)
+    ap.add_argument("--grid-eh-enclosed", type=int, default=4096)
+    ap.add_argument("--steps-eh", type=int, default=20)
+    ap.add_argument("--eh-only", action="store_true", help="time only the Euler/HLLC block (a profiling aid)")
     ap.add_argument("--grid-ns", type=int, default=4096)
     ap.add_argument("--steps-ns", type=int, default=20)
     ap.add_argument("--skip-ensemble", action="store_true")
@@ -611,6 +659,11 @@ def main():
         ap.error("--warmup must be >= 3")
     if args.ensemble_only:
         run_ensemble_only(args)
+        return
+    if args.eh_only:
+        import torch
+        torch.cuda.set_device(0)
+        print(json.dumps(run_euler2d(args, torch.cuda.Stream(), measured_peaks())), flush=True)
         return
     if args.ns_only:
         import torch

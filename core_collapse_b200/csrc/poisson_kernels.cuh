@@ -14,7 +14,8 @@
 //
 // Red-black SOR (the GPU ordering of M2:207-223 / EH:335-368): a persistent
 // cooperative kernel, one grid barrier per colour, deterministic FP64 mean
-// removal after each sweep, optional residual test.
+// removal after each sweep (applied lazily, see sor_rb_kernel), optional
+// residual test.
 #pragma once
 #include "cc_device.cuh"
 
@@ -211,20 +212,35 @@ struct SorArgs {
     const int* active;
 };
 
+// max |lap(phi) - rhs| over the block's cells of the field phi - shift (the
+// stored field with a pending mean removal applied on the fly)
 template <int NT>
-__device__ __forceinline__ double sor_residual_block(const SorArgs& a, double* sh) {
+__device__ __forceinline__ double sor_residual_block(const SorArgs& a, double shift, double* sh) {
     double r = 0.0;
     const int N = a.nx * a.ny;
     for (int k = blockIdx.x * NT + threadIdx.x; k < N; k += gridDim.x * NT) {
         const int i = k % a.nx, j = k / a.nx;
-        const double c = a.phi[k];
-        const double lap = (a.phi[(size_t)j * a.nx + a.ax.cell(i + 1)] - 2.0 * c + a.phi[(size_t)j * a.nx + a.ax.cell(i - 1)]) * a.idx2 +
-                           (a.phi[(size_t)a.ay.cell(j + 1) * a.nx + i] - 2.0 * c + a.phi[(size_t)a.ay.cell(j - 1) * a.nx + i]) * a.idy2;
+        const double c = a.phi[k] - shift;
+        const double pE = a.phi[(size_t)j * a.nx + a.ax.cell(i + 1)] - shift;
+        const double pW = a.phi[(size_t)j * a.nx + a.ax.cell(i - 1)] - shift;
+        const double pN = a.phi[(size_t)a.ay.cell(j + 1) * a.nx + i] - shift;
+        const double pS = a.phi[(size_t)a.ay.cell(j - 1) * a.nx + i] - shift;
+        const double lap = (pE - 2.0 * c + pW) * a.idx2 + (pN - 2.0 * c + pS) * a.idy2;
         r = fmax(r, fabs(lap - a.rhs[k]));
     }
     return block_max<NT>(r, sh);
 }
 
+// One sweep = red update, black update, mean removal, and (tol > 0) the
+// residual test.  The mean removal phi -= mean is not a pass of its own: the
+// mean of a sweep stays pending (`m`) and every read of a value that the
+// sweep has not rewritten subtracts it, which gives the same doubles as
+// subtracting first (x - m is the value the reference stores), and x - 0.0 == x
+// for the values already rewritten.  The density-independent part of the
+// mean (the block partial sums) is formed in the black phase, which also reads
+// the red cell of each of its indices, so a sweep needs two grid barriers
+// (red, black) plus one for the residual when tol > 0.  A final pass applies
+// the last pending mean.
 template <int NT>
 __global__ void __launch_bounds__(NT) sor_rb_kernel(SorArgs a) {
     if (a.active && *a.active == 0) return;
@@ -233,66 +249,91 @@ __global__ void __launch_bounds__(NT) sor_rb_kernel(SorArgs a) {
     const unsigned nb = gridDim.x;
     const int N = a.nx * a.ny;
     const int half = (a.nx + 1) / 2;        // cells of one colour per row (upper bound)
+    const int M = half * a.ny;
     for (int k = blockIdx.x * NT + threadIdx.x; k < N; k += nb * NT) a.phi[k] = 0.0;
     if (!grid_sync(a.bar, nb)) return;
-    int it = 0;
-    double res = 0.0;
-    for (; it < a.max_iter; ++it) {
-        for (int colour = 0; colour < 2; ++colour) {
-            const int M = half * a.ny;
-            for (int k = blockIdx.x * NT + threadIdx.x; k < M; k += nb * NT) {
-                const int j = k / half;
-                const int i = 2 * (k % half) + ((j + colour) & 1);
-                if (i >= a.nx) continue;
-                const size_t q = (size_t)j * a.nx + i;
-                const double pE = a.phi[(size_t)j * a.nx + a.ax.cell(i + 1)];
-                const double pW = a.phi[(size_t)j * a.nx + a.ax.cell(i - 1)];
-                const double pN = a.phi[(size_t)a.ay.cell(j + 1) * a.nx + i];
-                const double pS = a.phi[(size_t)a.ay.cell(j - 1) * a.nx + i];
-                const double pn = ((pE + pW) * a.idx2 + (pN + pS) * a.idy2 - a.rhs[q]) / a.denom;
-                a.phi[q] += a.omega * (pn - a.phi[q]);
-            }
-            if (!grid_sync(a.bar, nb)) return;
-        }
-        // mean removal: block partial sums, then every block adds the partials in block order
-        double s = 0.0;
-        for (int k = blockIdx.x * NT + threadIdx.x; k < N; k += nb * NT) s += a.phi[k];
-        s = block_sum<NT>(s, sh);
-        if (threadIdx.x == 0) a.part[blockIdx.x] = s;
-        if (!grid_sync(a.bar, nb)) return;
+    // the mean of the block partial sums in block order (the same double in every block)
+    auto block_mean = [&]() {
+        __syncthreads();
         if (threadIdx.x == 0) {
             double t = 0.0;
             for (unsigned b = 0; b < nb; b++) t += a.part[b];
             s_val = t / (double)N;
         }
         __syncthreads();
-        const double mean = s_val;
-        for (int k = blockIdx.x * NT + threadIdx.x; k < N; k += nb * NT) a.phi[k] -= mean;
+        return s_val;
+    };
+    double m = 0.0;   // mean removal pending on every cell not yet rewritten in this sweep
+    int it = 0;
+    double res = 0.0;
+    for (; it < a.max_iter; ++it) {
+        // red: every value read is pending
+        for (int k = blockIdx.x * NT + threadIdx.x; k < M; k += nb * NT) {
+            const int j = k / half;
+            const int i = 2 * (k % half) + (j & 1);
+            if (i >= a.nx) continue;
+            const size_t q = (size_t)j * a.nx + i;
+            const double pE = a.phi[(size_t)j * a.nx + a.ax.cell(i + 1)] - m;
+            const double pW = a.phi[(size_t)j * a.nx + a.ax.cell(i - 1)] - m;
+            const double pN = a.phi[(size_t)a.ay.cell(j + 1) * a.nx + i] - m;
+            const double pS = a.phi[(size_t)a.ay.cell(j - 1) * a.nx + i] - m;
+            const double own = a.phi[q] - m;
+            const double pn = ((pE + pW) * a.idx2 + (pN + pS) * a.idy2 - a.rhs[q]) / a.denom;
+            a.phi[q] = own + a.omega * (pn - own);
+        }
         if (!grid_sync(a.bar, nb)) return;
+        // black: the red neighbours are rewritten; a clamped neighbour that is
+        // the cell itself is still pending.  Sum every cell of the new field.
+        double s = 0.0;
+        for (int k = blockIdx.x * NT + threadIdx.x; k < M; k += nb * NT) {
+            const int j = k / half;
+            const int ir = 2 * (k % half) + (j & 1), i = 2 * (k % half) + ((j + 1) & 1);
+            if (ir < a.nx) s += a.phi[(size_t)j * a.nx + ir];
+            if (i >= a.nx) continue;
+            const size_t q = (size_t)j * a.nx + i;
+            const int iE = a.ax.cell(i + 1), iW = a.ax.cell(i - 1), jN = a.ay.cell(j + 1), jS = a.ay.cell(j - 1);
+            const double pE = a.phi[(size_t)j * a.nx + iE] - (iE == i ? m : 0.0);
+            const double pW = a.phi[(size_t)j * a.nx + iW] - (iW == i ? m : 0.0);
+            const double pN = a.phi[(size_t)jN * a.nx + i] - (jN == j ? m : 0.0);
+            const double pS = a.phi[(size_t)jS * a.nx + i] - (jS == j ? m : 0.0);
+            const double own = a.phi[q] - m;
+            const double pn = ((pE + pW) * a.idx2 + (pN + pS) * a.idy2 - a.rhs[q]) / a.denom;
+            const double v = own + a.omega * (pn - own);
+            a.phi[q] = v;
+            s += v;
+        }
+        s = block_sum<NT>(s, sh);
+        if (threadIdx.x == 0) a.part[blockIdx.x] = s;
+        if (!grid_sync(a.bar, nb)) return;
+        m = block_mean();   // this sweep's mean, pending from here on
         if (a.tol > 0.0) {
-            const double r = sor_residual_block<NT>(a, sh);
+            const double r = sor_residual_block<NT>(a, m, sh);
             if (threadIdx.x == 0) a.part2[blockIdx.x] = r;
             if (!grid_sync(a.bar, nb)) return;
             if (threadIdx.x == 0) {
-                double m = 0.0;
-                for (unsigned b = 0; b < nb; b++) m = fmax(m, a.part2[b]);
-                s_val = m;
+                double mx = 0.0;
+                for (unsigned b = 0; b < nb; b++) mx = fmax(mx, a.part2[b]);
+                s_val = mx;
             }
             __syncthreads();
             res = s_val;
-            // part2 is next written after three more grid barriers, so no
-            // barrier is needed here before the blocks' reads of it are done
+            __syncthreads();   // s_val is rewritten by the next block_mean
+            // part and part2 are next written after at least one more grid
+            // barrier, when every block has read them
             if (res < a.tol) { ++it; break; }
         }
     }
+    // apply the last pending mean
+    for (int k = blockIdx.x * NT + threadIdx.x; k < N; k += nb * NT) a.phi[k] -= m;
     if (!(a.tol > 0.0)) {
-        const double r = sor_residual_block<NT>(a, sh);
+        if (!grid_sync(a.bar, nb)) return;
+        const double r = sor_residual_block<NT>(a, 0.0, sh);
         if (threadIdx.x == 0) a.part2[blockIdx.x] = r;
         if (!grid_sync(a.bar, nb)) return;
         if (threadIdx.x == 0) {
-            double m = 0.0;
-            for (unsigned b = 0; b < nb; b++) m = fmax(m, a.part2[b]);
-            res = m;
+            double mx = 0.0;
+            for (unsigned b = 0; b < nb; b++) mx = fmax(mx, a.part2[b]);
+            res = mx;
         }
     }
     if (blockIdx.x == 0 && threadIdx.x == 0) { *a.iters_out = it; *a.res_out = res; }

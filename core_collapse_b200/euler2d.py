@@ -164,6 +164,18 @@ class Euler2dSolver:
         self._t = tt.value
         return tt.value
 
+    def set_stream(self, stream_ptr: int | None):
+        """Queue this handle's work on a caller's cudaStream_t (None: its own stream)."""
+        self._check(self._lib.cc_set_stream(self._h, C.c_void_p(stream_ptr) if stream_ptr else None))
+
+    def perf(self) -> dict:
+        q = L.CcPerf()
+        self._check(self._lib.cc_get_perf(self._h, C.byref(q)))
+        return {f: getattr(q, f) for f, _ in L.CcPerf._fields_}
+
+    def reset_perf(self):
+        self._check(self._lib.cc_reset_perf(self._h))
+
     def save_checkpoint(self, path: str):
         """State, clock and parameters to one file (cc_euler2d_checkpoint_save)."""
         self._check(self._lib.cc_euler2d_checkpoint_save(self._h, str(path).encode()))
