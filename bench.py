@@ -636,7 +636,7 @@ def main():
     ap.add_argument("--skip-ns", action="store_true")
     ap.add_argument("--skip-eh", action="store_true")
     ap.add_argument("--grid-eh", type=int, default=512)
-    ap.add_argument("--steps-eh-sor", type=int, default=3)
+    ap.add_argument("--steps-eh-sor", type=int, default=1)
     ap.add_argument("--grid-eh-enclosed", type=int, default=4096)
     ap.add_argument("--steps-eh", type=int, default=20)
     ap.add_argument("--eh-only", action="store_true", help="time only the Euler/HLLC block (a profiling aid)")
