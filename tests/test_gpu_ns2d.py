@@ -239,3 +239,29 @@ def test_checkpoint_rejects_bad_files(tmp_path):
         with pytest.raises(CcError) as e:
             g.load_checkpoint(path)
         assert e.value.code == L.CC_ERR_ARG
+
+
+def test_reference_configuration_runs_to_t_end():
+    """The reference main()'s whole run (NS:54-86 defaults: 128^2, t_end 10,
+    the collapse IC): about 11 000 Heun steps through cc_ns2d_advance in both
+    precisions; the run reaches t_end exactly, stays finite, conserves mass
+    (FP64 to round-off), and FP32 and FP64 agree on the density extremes."""
+    ext = {}
+    for prec in ("fp64", "fp32"):
+        p = ParamsNS(precision=prec)
+        with Ns2dSolver(p) as g:
+            g.upload(ic_collapse(p))
+            d0 = g.diagnostics()
+            t, chunks = 0.0, 0
+            while t < p.t_end - 1e-14 and chunks < 200:
+                t = g.advance(1000)
+                chunks += 1
+            d1 = g.diagnostics()
+            rho = g.derived()["rho"]
+        assert abs(t - p.t_end) <= 1e-12 and d1["nonfinite"] == 0 and d1["steps"] > 5000
+        drift = abs(d1["mass"] - d0["mass"]) / d0["mass"]
+        assert drift <= (1e-13 if prec == "fp64" else 1e-6), drift
+        ext[prec] = (float(rho.max()), float(rho.min()), d1["steps"])
+    assert ext["fp64"][0] > 3.0   # the central condensation has formed
+    for k in range(2):
+        assert abs(ext["fp32"][k] - ext["fp64"][k]) <= 1e-3 * ext["fp64"][k]
