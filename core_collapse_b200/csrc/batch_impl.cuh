@@ -118,8 +118,8 @@ template <class T, int K = 0> struct ShapeLoop {
     }
 };
 
-// one CTA per reduce tile: the hardware keeps SMs fed while tiles wait on memory
-inline int rgrid(int nrwork) { return nrwork < 1 ? 1 : nrwork; }
+// one warp per reduce tile, RWPB tiles per CTA
+inline int rgrid(int nrwork) { return nrwork < 1 ? 1 : (nrwork + RWPB - 1) / RWPB; }
 
 }  // namespace
 

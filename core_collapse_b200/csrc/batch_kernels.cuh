@@ -12,7 +12,7 @@
 //                 stage body); the persistent stage kernel gives each CTA a
 //                 contiguous run of the list, so consecutive tiles mostly share
 //                 an instance and its record stays in shared memory;
-//   reduce tiles  RTX x RTY cells, one thread per cell, one partial (max CFL
+//   reduce tiles  RTX x RTY cells, one warp per tile (the partial of a one-thread-per-cell block reduction), one partial (max CFL
 //                 speed, density sum) per tile; an instance's partials are a
 //                 contiguous range reduced in a fixed order, so every per-
 //                 instance reduction is deterministic and independent of the
@@ -101,6 +101,32 @@ m2b_stage_kernel(const BatchInst<T>* __restrict__ inst, const int2* __restrict__
 }
 
 // ---------------------------------------------------------------------------
+// Reduce tiles are worked by one warp each (RNT/32 tiles per CTA, no block
+// barriers): lane = column, the RTY rows in turn.  The partials are the same
+// doubles as block_max_sum / block_sum over the tile with one thread per cell
+// (warp = row): each row's values go through that warp shuffle tree, the row
+// results are placed in lanes 0..RTY-1 (the other lanes 0) and go through the
+// same second-level tree.
+// ---------------------------------------------------------------------------
+constexpr int RWPB = RNT / 32;   // reduce tiles per CTA
+static_assert(RTX == 32 && RTY <= 32, "a reduce-tile row is one warp");
+
+__device__ __forceinline__ void rtile_tree(double& m, double& s) {
+    for (int o = 16; o > 0; o >>= 1) {
+        m = fmax(m, __shfl_down_sync(0xffffffffu, m, o));
+        s += __shfl_down_sync(0xffffffffu, s, o);
+    }
+}
+
+// fold row r's (max, sum) into the lane-r slot of the second level
+__device__ __forceinline__ void rtile_row(int r, double m, double s, double& rm, double& rs) {
+    rtile_tree(m, s);
+    m = __shfl_sync(0xffffffffu, m, 0);
+    s = __shfl_sync(0xffffffffu, s, 0);
+    if ((threadIdx.x & 31) == r) { rm = m; rs = s; }
+}
+
+// ---------------------------------------------------------------------------
 // RK average over reduce tiles: U^{n+1} = average(U^n, Joule(S2)) with floors,
 // plus the per-tile CFL-speed max and density sum of U^{n+1}.
 // ---------------------------------------------------------------------------
@@ -109,21 +135,27 @@ __global__ void __launch_bounds__(RNT)
 m2b_average_kernel(const BatchInst<T>* __restrict__ inst, const int2* __restrict__ rwork, int nrwork, int a, int d,
                    int b, const double* __restrict__ dt, const int* __restrict__ active,
                    double* __restrict__ spd_part, double* __restrict__ rho_part) {
-    __shared__ double sh[2 * RNT / 32];
-    for (int w = blockIdx.x; w < nrwork; w += gridDim.x) {
+    const int lane = threadIdx.x & 31;
+    for (int w = blockIdx.x * RWPB + (threadIdx.x >> 5); w < nrwork; w += gridDim.x * RWPB) {
         const int2 it = rwork[w];
         const BatchInst<T>& I = inst[it.x];
         int tx, ty;
         unpack_tile(it, tx, ty);
-        const int i = tx * RTX + (threadIdx.x % RTX), j = ty * RTY + (threadIdx.x / RTX);
-        double smax = 0.0, rsum = 0.0;
-        if (i < I.c.nx && j < I.c.ny) {
-            const double s = average_cell(I.c, I.buf[a], I.buf[d], I.buf[b], (T)dt[it.x], active[it.x] != 0, i, j,
-                                          rsum);
-            if (s > smax) smax = s;
+        const int i = tx * RTX + lane;
+        const bool act = active[it.x] != 0;
+        const T dtv = (T)dt[it.x];
+        double rm = 0.0, rs = 0.0;
+        for (int r = 0; r < RTY; r++) {
+            const int j = ty * RTY + r;
+            double smax = 0.0, rsum = 0.0;
+            if (i < I.c.nx && j < I.c.ny) {
+                const double v = average_cell(I.c, I.buf[a], I.buf[d], I.buf[b], dtv, act, i, j, rsum);
+                if (v > smax) smax = v;
+            }
+            rtile_row(r, smax, rsum, rm, rs);
         }
-        block_max_sum<RNT>(smax, rsum, sh);
-        if (threadIdx.x == 0) { spd_part[w] = smax; rho_part[w] = rsum; }
+        rtile_tree(rm, rs);
+        if (lane == 0) { spd_part[w] = rm; rho_part[w] = rs; }
     }
 }
 
@@ -132,21 +164,26 @@ template <class T>
 __global__ void __launch_bounds__(RNT)
 m2b_speed_kernel(const BatchInst<T>* __restrict__ inst, const int2* __restrict__ rwork, int nrwork, int src,
                  double* __restrict__ spd_part, double* __restrict__ rho_part) {
-    __shared__ double sh[2 * RNT / 32];
-    for (int w = blockIdx.x; w < nrwork; w += gridDim.x) {
+    const int lane = threadIdx.x & 31;
+    for (int w = blockIdx.x * RWPB + (threadIdx.x >> 5); w < nrwork; w += gridDim.x * RWPB) {
         const int2 it = rwork[w];
         const BatchInst<T>& I = inst[it.x];
         int tx, ty;
         unpack_tile(it, tx, ty);
-        const int i = tx * RTX + (threadIdx.x % RTX), j = ty * RTY + (threadIdx.x / RTX);
-        double smax = 0.0, rsum = 0.0;
-        if (i < I.c.nx && j < I.c.ny) {
-            const double v = speed_cell(I.c, I.buf[src], i, j);
-            if (v > smax) smax = v;
-            rsum = (double)I.buf[src].rho[(size_t)j * I.c.pitch + i];
+        const int i = tx * RTX + lane;
+        double rm = 0.0, rs = 0.0;
+        for (int r = 0; r < RTY; r++) {
+            const int j = ty * RTY + r;
+            double smax = 0.0, rsum = 0.0;
+            if (i < I.c.nx && j < I.c.ny) {
+                const double v = speed_cell(I.c, I.buf[src], i, j);
+                if (v > smax) smax = v;
+                rsum = (double)I.buf[src].rho[(size_t)j * I.c.pitch + i];
+            }
+            rtile_row(r, smax, rsum, rm, rs);
         }
-        block_max_sum<RNT>(smax, rsum, sh);
-        if (threadIdx.x == 0) { spd_part[w] = smax; rho_part[w] = rsum; }
+        rtile_tree(rm, rs);
+        if (lane == 0) { spd_part[w] = rm; rho_part[w] = rs; }
     }
 }
 
@@ -155,18 +192,22 @@ template <class T>
 __global__ void __launch_bounds__(RNT)
 m2b_rho_sum_kernel(const BatchInst<T>* __restrict__ inst, const int2* __restrict__ rwork, int nrwork, int src,
                    const int* __restrict__ active, double* __restrict__ rho_part) {
-    __shared__ double sh[RNT / 32];
-    for (int w = blockIdx.x; w < nrwork; w += gridDim.x) {
+    const int lane = threadIdx.x & 31;
+    for (int w = blockIdx.x * RWPB + (threadIdx.x >> 5); w < nrwork; w += gridDim.x * RWPB) {
         const int2 it = rwork[w];
-        if (active[it.x] == 0) continue;
+        if (active[it.x] == 0) continue;   // uniform over the warp
         const BatchInst<T>& I = inst[it.x];
         int tx, ty;
         unpack_tile(it, tx, ty);
-        const int i = tx * RTX + (threadIdx.x % RTX), j = ty * RTY + (threadIdx.x / RTX);
-        double rsum = 0.0;
-        if (i < I.c.nx && j < I.c.ny) rsum = (double)I.buf[src].rho[(size_t)j * I.c.pitch + i];
-        const double bs = block_sum<RNT>(rsum, sh);
-        if (threadIdx.x == 0) rho_part[w] = bs;
+        const int i = tx * RTX + lane;
+        double rm = 0.0, rs = 0.0;
+        for (int r = 0; r < RTY; r++) {
+            const int j = ty * RTY + r;
+            const double rsum = (i < I.c.nx && j < I.c.ny) ? (double)I.buf[src].rho[(size_t)j * I.c.pitch + i] : 0.0;
+            rtile_row(r, 0.0, rsum, rm, rs);
+        }
+        rtile_tree(rm, rs);
+        if (lane == 0) rho_part[w] = rs;
     }
 }
 
