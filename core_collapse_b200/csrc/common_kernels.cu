@@ -58,7 +58,7 @@ cudaError_t launch_set_scalar(double* p, double v, cudaStream_t s) {
     return cudaGetLastError();
 }
 
-constexpr int SOR_NT = 256;
+constexpr int SOR_NT = 1024;
 
 cudaError_t launch_sor(const SorArgs& a, int* nblocks_out, cudaStream_t s) {
     int dev = 0, nsm = 0, per_sm = 0;
@@ -72,7 +72,7 @@ cudaError_t launch_sor(const SorArgs& a, int* nblocks_out, cudaStream_t s) {
     const int ncell = a.nx * a.ny;
     int want = (ncell / 2 + SOR_NT - 1) / SOR_NT;
     if (want < 1) want = 1;
-    int cap = nsm * (per_sm < 2 ? per_sm : 2);
+    int cap = nsm;   // one 1024-thread CTA per SM: the sweeps are grid-barrier bound, and fewer, larger CTAs arrive faster
     int nb = want < cap ? want : cap;
     if (nblocks_out) *nblocks_out = nb;
     SorArgs args = a;
