@@ -79,6 +79,8 @@ template <class T> struct Mhd3d : Mhd3dBase {
 
     int init() override {
         const int nx = p.Nx, ny = p.Ny, nz = p.Nz;
+        if ((long long)(nx + 1) * (ny + 1) * (nz + 1) >= (1ll << 31))
+            return fail(h, CC_ERR_UNSUPPORTED, "3D grids need (Nx+1)(Ny+1)(Nz+1) < 2^31 (32-bit kernel indices)");
         c = m3_make_const<T>(p);
         vol = (size_t)c.PS * (nz + 1);
 

@@ -75,11 +75,16 @@ __device__ __forceinline__ T joule3(const M3Const<T>& c, const Fields3<T>& s, in
     return dt * c.eta * J2;
 }
 
-// grid-stride helper over an (nx, ny, nz) box
+// grid-stride helper over an (nx, ny, nz) box with 32-bit indices (the handle
+// rejects grids whose (Nx+1)(Ny+1)(Nz+1) reaches 2^31)
 #define CC_FOR3(nx_, ny_, nz_)                                                                          \
-    const long long n3_ = (long long)(nx_) * (ny_) * (nz_);                                             \
-    for (long long t_ = (long long)blockIdx.x * blockDim.x + threadIdx.x; t_ < n3_;                     \
-         t_ += (long long)gridDim.x * blockDim.x)
+    const unsigned w3_ = (unsigned)(nx_), h3_ = (unsigned)(ny_);                                        \
+    const unsigned n3_ = w3_ * h3_ * (unsigned)(nz_);                                                   \
+    for (unsigned t_ = blockIdx.x * blockDim.x + threadIdx.x; t_ < n3_; t_ += gridDim.x * blockDim.x)
+// the (i, j, k) of t_ inside CC_FOR3, two 32-bit divisions
+#define CC_IJK3(i, j, k)                                                                                \
+    const unsigned r3_ = t_ / w3_, q3_ = r3_ / h3_;                                                     \
+    const int i = (int)(t_ - r3_ * w3_), j = (int)(r3_ - q3_ * h3_), k = (int)q3_
 
 // ---------------------------------------------------------------------------
 // primitives: 8 planes (rho, u, v, w, P, Bx, By, Bz)
@@ -93,7 +98,7 @@ __global__ void __launch_bounds__(256) m3_prim_kernel(const M3Const<T> c, const 
     if (active && *active == 0) return;
     const T dt = (T)(*dtp);
     CC_FOR3(c.nx, c.ny, c.nz) {
-        const int i = (int)(t_ % c.nx), j = (int)((t_ / c.nx) % c.ny), k = (int)(t_ / ((long long)c.nx * c.ny));
+        CC_IJK3(i, j, k);
         const size_t q = c.idx(i, j, k);
         T rho = s.rho[q], mx = s.mx[q], my = s.my[q], mz = s.mz[q], E = s.E[q];
         const T Bx = bx_cc3(c, s.bx, i, j, k), By = by_cc3(c, s.by, i, j, k), Bz = bz_cc3(c, s.bz, i, j, k);
@@ -138,7 +143,7 @@ __global__ void __launch_bounds__(256) m3_face_kernel(const M3Const<T> c, const 
     if (active && *active == 0) return;
     const int fx = c.nx + (DIR == 0), fy = c.ny + (DIR == 1), fz = c.nz + (DIR == 2);
     CC_FOR3(fx, fy, fz) {
-        const int i = (int)(t_ % fx), j = (int)((t_ / fx) % fy), k = (int)(t_ / ((long long)fx * fy));
+        CC_IJK3(i, j, k);
         int Li = i, Lj = j, Lk = k, Ri = i, Rj = j, Rk = k;
         if (DIR == 0) { Li = c.ax.cell(i - 1); Ri = c.ax.cell(i); }
         if (DIR == 1) { Lj = c.ay.cell(j - 1); Rj = c.ay.cell(j); }
@@ -179,7 +184,7 @@ __global__ void __launch_bounds__(256) m3_update_kernel(const M3Const<T> c, cons
     if (active && *active == 0) return;
     const T dt = (T)(*dtp);
     CC_FOR3(c.nx, c.ny, c.nz) {
-        const int i = (int)(t_ % c.nx), j = (int)((t_ / c.nx) % c.ny), k = (int)(t_ / ((long long)c.nx * c.ny));
+        CC_IJK3(i, j, k);
         const size_t q = c.idx(i, j, k), qx = c.idx(i + 1, j, k), qy = c.idx(i, j + 1, k), qz = c.idx(i, j, k + 1);
         T d[5];
 #pragma unroll
@@ -204,8 +209,7 @@ __global__ void __launch_bounds__(256) m3_edge_kernel(const M3Const<T> c, const 
                                                       const int* __restrict__ active) {
     if (active && *active == 0) return;
     CC_FOR3(c.nx + 1, c.ny + 1, c.nz + 1) {
-        const int i = (int)(t_ % (c.nx + 1)), j = (int)((t_ / (c.nx + 1)) % (c.ny + 1));
-        const int k = (int)(t_ / ((long long)(c.nx + 1) * (c.ny + 1)));
+        CC_IJK3(i, j, k);
         const size_t q = c.idx(i, j, k);
         // x-face EMF planes: X.f[5] = Ey_x, X.f[6] = Ez_x; y: Y.f[5] = Ez_y, Y.f[6] = Ex_y; z: Z.f[5] = Ex_z, Z.f[6] = Ey_z
         auto exy = [&](int a, int b, int d) { return Y.f[6][c.idx(c.ax.cell(a), c.ay.face(b), c.az.cell(d))]; };
@@ -257,8 +261,7 @@ __global__ void __launch_bounds__(256) m3_ct_kernel(const M3Const<T> c, const Fi
     const T dt = (T)(*dtp);
     const T dtdx = dt / c.dx, dtdy = dt / c.dy, dtdz = dt / c.dz;
     CC_FOR3(c.nx + 1, c.ny + 1, c.nz + 1) {
-        const int i = (int)(t_ % (c.nx + 1)), j = (int)((t_ / (c.nx + 1)) % (c.ny + 1));
-        const int k = (int)(t_ / ((long long)(c.nx + 1) * (c.ny + 1)));
+        CC_IJK3(i, j, k);
         const size_t q = c.idx(i, j, k);
         if (j < c.ny && k < c.nz) {  // Bx face (i, j, k)
             const T ezU = Ez[c.idx(i, j + 1, k)], ezD = Ez[q];
@@ -304,8 +307,7 @@ m3_average_kernel(const M3Const<T> c, const Fields3<T> un, const Fields3<T> s2, 
     const T dt = (T)(*dtp);
     double smax = 0.0, rsum = 0.0;
     CC_FOR3(c.nx + 1, c.ny + 1, c.nz + 1) {
-        const int i = (int)(t_ % (c.nx + 1)), j = (int)((t_ / (c.nx + 1)) % (c.ny + 1));
-        const int k = (int)(t_ / ((long long)(c.nx + 1) * (c.ny + 1)));
+        CC_IJK3(i, j, k);
         const size_t q = c.idx(i, j, k);
         auto avx = [&](size_t f) { return act ? T(0.5) * (un.bx[f] + s2.bx[f]) : un.bx[f]; };
         auto avy = [&](size_t f) { return act ? T(0.5) * (un.by[f] + s2.by[f]) : un.by[f]; };
@@ -349,7 +351,7 @@ m3_speed_kernel(const M3Const<T> c, const Fields3<T> s, double* __restrict__ spd
     __shared__ double sh[NT / 32];
     double smax = 0.0;
     CC_FOR3(c.nx, c.ny, c.nz) {
-        const int i = (int)(t_ % c.nx), j = (int)((t_ / c.nx) % c.ny), k = (int)(t_ / ((long long)c.nx * c.ny));
+        CC_IJK3(i, j, k);
         const size_t q = c.idx(i, j, k);
         const Prim<T> W = to_prim(c, s.rho[q], s.mx[q], s.my[q], s.mz[q], s.E[q], bx_cc3(c, s.bx, i, j, k),
                                   by_cc3(c, s.by, i, j, k), bz_cc3(c, s.bz, i, j, k));
@@ -366,7 +368,7 @@ __global__ void __launch_bounds__(NT) m3_diag_kernel(const M3Const<T> c, const F
     __shared__ double sh[NT / 32];
     double acc[5] = {0, 0, 0, 0, 0}, dmax = 0.0, nonf = 0.0;
     CC_FOR3(c.nx, c.ny, c.nz) {
-        const int i = (int)(t_ % c.nx), j = (int)((t_ / c.nx) % c.ny), k = (int)(t_ / ((long long)c.nx * c.ny));
+        CC_IJK3(i, j, k);
         const size_t q = c.idx(i, j, k);
         const double v[5] = {(double)s.rho[q], (double)s.mx[q], (double)s.my[q], (double)s.mz[q], (double)s.E[q]};
         for (int m = 0; m < 5; m++) {
@@ -395,7 +397,7 @@ template <class T>
 __global__ void m3_derived_kernel(const M3Const<T> c, const Fields3<T> s, double* __restrict__ out) {
     const size_t n = (size_t)c.nx * c.ny * c.nz;
     CC_FOR3(c.nx, c.ny, c.nz) {
-        const int i = (int)(t_ % c.nx), j = (int)((t_ / c.nx) % c.ny), k = (int)(t_ / ((long long)c.nx * c.ny));
+        CC_IJK3(i, j, k);
         const size_t q = c.idx(i, j, k), o = (size_t)t_;
         const T Bx = T(0.5) * (s.bx[q] + s.bx[c.idx(i + 1, j, k)]);
         const T By = T(0.5) * (s.by[q] + s.by[c.idx(i, j + 1, k)]);
@@ -419,7 +421,7 @@ template <class T>
 __global__ void pack3_in_kernel(const double* __restrict__ src, T* __restrict__ dst, int w, int h, int d, int P,
                                 long long PS) {
     CC_FOR3(w, h, d) {
-        const int i = (int)(t_ % w), j = (int)((t_ / w) % h), k = (int)(t_ / ((long long)w * h));
+        CC_IJK3(i, j, k);
         dst[(size_t)k * PS + (size_t)j * P + i] = (T)src[t_];
     }
 }
@@ -427,7 +429,7 @@ template <class T>
 __global__ void pack3_out_kernel(const T* __restrict__ src, double* __restrict__ dst, int w, int h, int d, int P,
                                  long long PS) {
     CC_FOR3(w, h, d) {
-        const int i = (int)(t_ % w), j = (int)((t_ / w) % h), k = (int)(t_ / ((long long)w * h));
+        CC_IJK3(i, j, k);
         dst[t_] = (double)src[(size_t)k * PS + (size_t)j * P + i];
     }
 }
