@@ -42,8 +42,8 @@ cudaError_t M3Launch<T>::update(const M3Const<T>& c, const Fields3<T>& in, const
 template <class T>
 cudaError_t M3Launch<T>::edges(const M3Const<T>& c, const Fields3<T>& in, const FaceData<T>& X, const FaceData<T>& Y,
                                const FaceData<T>& Z, T* Ex, T* Ey, T* Ez, const int* active, cudaStream_t st) {
-    m3_edge_kernel<T><<<grid3((long long)(c.nx + 1) * (c.ny + 1) * (c.nz + 1)), 256, 0, st>>>(c, in, X, Y, Z, Ex, Ey,
-                                                                                               Ez, active);
+    const dim3 eg((c.nx + 1 + 31) / 32, (c.ny + 1 + 7) / 8, (c.nz + 1 + M3_EDGE_KCH - 1) / M3_EDGE_KCH);
+    m3_edge_kernel<T><<<eg, 256, 0, st>>>(c, in, X, Y, Z, Ex, Ey, Ez, active);
     return cudaGetLastError();
 }
 

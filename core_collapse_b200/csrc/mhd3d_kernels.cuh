@@ -202,52 +202,79 @@ __global__ void __launch_bounds__(256) m3_update_kernel(const M3Const<T> c, cons
 }
 
 // Edge EMFs (M3:879-939): Ex at (i, jf, kf), Ey at (if, j, kf), Ez at (if, jf, k)
+// Edge EMFs (M3:879-939): Balsara-Spicer average of the four face EMFs plus
+// eta J from cell-centred B differences.  A thread owns one (i, j) edge column
+// and marches k over a chunk of M3_EDGE_KCH planes, carrying what plane k-1
+// loaded (the EMF and cell-centred B at k-1, the z-face Bz at k); every value
+// is the same expression of the same loads as a per-edge evaluation.
+constexpr int M3_EDGE_KCH = 32;
 template <class T>
 __global__ void __launch_bounds__(256) m3_edge_kernel(const M3Const<T> c, const Fields3<T> in, const FaceData<T> X,
                                                       const FaceData<T> Y, const FaceData<T> Z, T* __restrict__ Ex,
                                                       T* __restrict__ Ey, T* __restrict__ Ez,
                                                       const int* __restrict__ active) {
     if (active && *active == 0) return;
-    CC_FOR3(c.nx + 1, c.ny + 1, c.nz + 1) {
-        CC_IJK3(i, j, k);
+    const int i = blockIdx.x * 32 + (threadIdx.x & 31), j = blockIdx.y * 8 + (threadIdx.x >> 5);
+    if (i > c.nx || j > c.ny) return;
+    const int k0 = blockIdx.z * M3_EDGE_KCH, k1 = min(c.nz + 1, k0 + M3_EDGE_KCH);
+    // x-face EMF planes: X.f[5] = Ey_x, X.f[6] = Ez_x; y: Y.f[5] = Ez_y, Y.f[6] = Ex_y; z: Z.f[5] = Ex_z, Z.f[6] = Ey_z
+    const int ci = c.ax.cell(i), cim = c.ax.cell(i - 1), fi = c.ax.face(i), fi1 = c.ax.face(i + 1);
+    const int cj = c.ay.cell(j), cjm = c.ay.cell(j - 1), fj = c.ay.face(j), fj1 = c.ay.face(j + 1);
+    const bool xe = i < c.nx, ye = j < c.ny, res_on = c.resistive != 0;
+    auto at = [&](const T* f, int a, int b, int d) { return f[c.idx(a, b, d)]; };
+    auto bxc = [&](int jj, int kc) { return T(0.5) * (at(in.bx, fi, jj, kc) + at(in.bx, fi1, jj, kc)); };   // bx_cc3(i, jj, kc)
+    auto byc = [&](int ii, int kc) { return T(0.5) * (at(in.by, ii, fj, kc) + at(in.by, ii, fj1, kc)); };   // by_cc3(ii, j, kc)
+    // carried from plane k-1: the Ex_y and Ey_x EMFs, by_cc3(i,j,k-1), bx_cc3(i,j,k-1);
+    // from face k: Bz of the columns (i,j), (i,j-1), (i-1,j)
+    const int ckm = c.az.cell(k0 - 1), fk0 = c.az.face(k0);
+    T exy_p = at(Y.f[6], ci, fj, ckm), eyx_p = at(X.f[5], fi, cj, ckm);
+    T by_p = T(0), bx_p = T(0), bz0 = T(0), bz0s = T(0), bz0w = T(0);
+    if (res_on) {
+        by_p = byc(ci, ckm); bx_p = bxc(cj, ckm);
+        bz0 = at(in.bz, ci, cj, fk0); bz0s = at(in.bz, ci, cjm, fk0); bz0w = at(in.bz, cim, cj, fk0);
+    }
+    for (int k = k0; k < k1; ++k) {
+        const int ck = c.az.cell(k), fk = c.az.face(k), fk1 = c.az.face(k + 1);
         const size_t q = c.idx(i, j, k);
-        // x-face EMF planes: X.f[5] = Ey_x, X.f[6] = Ez_x; y: Y.f[5] = Ez_y, Y.f[6] = Ex_y; z: Z.f[5] = Ex_z, Z.f[6] = Ey_z
-        auto exy = [&](int a, int b, int d) { return Y.f[6][c.idx(c.ax.cell(a), c.ay.face(b), c.az.cell(d))]; };
-        auto exz = [&](int a, int b, int d) { return Z.f[5][c.idx(c.ax.cell(a), c.ay.cell(b), c.az.face(d))]; };
-        auto eyx = [&](int a, int b, int d) { return X.f[5][c.idx(c.ax.face(a), c.ay.cell(b), c.az.cell(d))]; };
-        auto eyz = [&](int a, int b, int d) { return Z.f[6][c.idx(c.ax.cell(a), c.ay.cell(b), c.az.face(d))]; };
-        auto ezx = [&](int a, int b, int d) { return X.f[6][c.idx(c.ax.face(a), c.ay.cell(b), c.az.cell(d))]; };
-        auto ezy = [&](int a, int b, int d) { return Y.f[5][c.idx(c.ax.cell(a), c.ay.face(b), c.az.cell(d))]; };
-        if (i < c.nx) {  // Ex
-            const T ideal = T(0.25) * (exy(i, j, k - 1) + exy(i, j, k) + exz(i, j - 1, k) + exz(i, j, k));
+        const T exy_k = at(Y.f[6], ci, fj, ck), eyx_k = at(X.f[5], fi, cj, ck);
+        T by_k = T(0), bx_k = T(0), bz1 = T(0), bz1s = T(0), bz1w = T(0);
+        if (res_on) {
+            by_k = byc(ci, ck); bx_k = bxc(cj, ck);
+            bz1 = at(in.bz, ci, cj, fk1); bz1s = at(in.bz, ci, cjm, fk1); bz1w = at(in.bz, cim, cj, fk1);
+        }
+        if (xe) {  // Ex
+            const T ideal = T(0.25) * (exy_p + exy_k + at(Z.f[5], ci, cjm, fk) + at(Z.f[5], ci, cj, fk));
             T res = T(0.0);
-            if (c.resistive) {
-                const T dBzdy = (bz_cc3(c, in.bz, i, j, k) - bz_cc3(c, in.bz, i, j - 1, k)) / c.dy;
-                const T dBydz = (by_cc3(c, in.by, i, j, k) - by_cc3(c, in.by, i, j, k - 1)) / c.dz;
+            if (res_on) {
+                const T dBzdy = (T(0.5) * (bz0 + bz1) - T(0.5) * (bz0s + bz1s)) / c.dy;
+                const T dBydz = (by_k - by_p) / c.dz;
                 res = c.eta * (dBzdy - dBydz);
             }
             Ex[q] = ideal + res;
         }
-        if (j < c.ny) {  // Ey
-            const T ideal = T(0.25) * (eyx(i, j, k - 1) + eyx(i, j, k) + eyz(i - 1, j, k) + eyz(i, j, k));
+        if (ye) {  // Ey
+            const T ideal = T(0.25) * (eyx_p + eyx_k + at(Z.f[6], cim, cj, fk) + at(Z.f[6], ci, cj, fk));
             T res = T(0.0);
-            if (c.resistive) {
-                const T dBxdz = (bx_cc3(c, in.bx, i, j, k) - bx_cc3(c, in.bx, i, j, k - 1)) / c.dz;
-                const T dBzdx = (bz_cc3(c, in.bz, i, j, k) - bz_cc3(c, in.bz, i - 1, j, k)) / c.dx;
+            if (res_on) {
+                const T dBxdz = (bx_k - bx_p) / c.dz;
+                const T dBzdx = (T(0.5) * (bz0 + bz1) - T(0.5) * (bz0w + bz1w)) / c.dx;
                 res = c.eta * (dBxdz - dBzdx);
             }
             Ey[q] = ideal + res;
         }
         if (k < c.nz) {  // Ez
-            const T ideal = T(0.25) * (ezx(i, j - 1, k) + ezx(i, j, k) + ezy(i - 1, j, k) + ezy(i, j, k));
+            const T ideal = T(0.25) * (at(X.f[6], fi, cjm, ck) + at(X.f[6], fi, cj, ck) + at(Y.f[5], cim, fj, ck) +
+                                       at(Y.f[5], ci, fj, ck));
             T res = T(0.0);
-            if (c.resistive) {
-                const T dBydx = (by_cc3(c, in.by, i, j, k) - by_cc3(c, in.by, i - 1, j, k)) / c.dx;
-                const T dBxdy = (bx_cc3(c, in.bx, i, j, k) - bx_cc3(c, in.bx, i, j - 1, k)) / c.dy;
+            if (res_on) {
+                const T dBydx = (by_k - byc(cim, ck)) / c.dx;
+                const T dBxdy = (bx_k - bxc(cjm, ck)) / c.dy;
                 res = c.eta * (dBydx - dBxdy);
             }
             Ez[q] = ideal + res;
         }
+        exy_p = exy_k; eyx_p = eyx_k; by_p = by_k; bx_p = bx_k;
+        bz0 = bz1; bz0s = bz1s; bz0w = bz1w;
     }
 }
 
