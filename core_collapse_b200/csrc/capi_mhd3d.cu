@@ -44,6 +44,7 @@ template <class T> struct Mhd3d : Mhd3dBase {
     void* block = nullptr;
     Fields3<T> buf[3];
     PrimData<T> prim{};
+    Bcc3<T> bcc{};   // cell-centred B of the state a Joule pass reads
     FaceData<T> fX{}, fY{}, fZ{};
     T *Ex = nullptr, *Ey = nullptr, *Ez = nullptr;
     double* staging = nullptr;
@@ -84,8 +85,8 @@ template <class T> struct Mhd3d : Mhd3dBase {
         c = m3_make_const<T>(p);
         vol = (size_t)c.PS * (nz + 1);
 
-        // 3 states x 8 + primitives 8 + 3 x 7 face data + 3 edge arrays = 56 fields
-        const size_t nfield = 56;
+        // 3 states x 8 + primitives 8 + 3 x 7 face data + 3 edge arrays + 3 cell-centred B = 59 fields
+        const size_t nfield = 59;
         CC_CUDA(cudaMalloc(&block, sizeof(T) * vol * nfield));
         CC_CUDA(cudaMemsetAsync(block, 0, sizeof(T) * vol * nfield, st()));
         T* base = reinterpret_cast<T*>(block);
@@ -99,6 +100,7 @@ template <class T> struct Mhd3d : Mhd3dBase {
         for (int m = 0; m < 7; m++) fY.f[m] = take();
         for (int m = 0; m < 7; m++) fZ.f[m] = take();
         Ex = take(); Ey = take(); Ez = take();
+        bcc.x = take(); bcc.y = take(); bcc.z = take();
         CC_CUDA(cudaMalloc(&staging, sizeof(double) * (size_t)(nx + 1) * (ny + 1) * (nz + 1)));
         CC_CUDA(cudaMalloc(&spd_part, sizeof(double) * RED_BLOCKS));
         CC_CUDA(cudaMalloc(&rho_part, sizeof(double) * RED_BLOCKS));
@@ -188,12 +190,12 @@ template <class T> struct Mhd3d : Mhd3dBase {
             CC_CUDA(cudaEventCreate(&e1));
             CC_CUDA(cudaEventRecord(e0, st()));
         }
-        CC_CUDA(M3Launch<T>::prim(c, in, prim, defer, dt_dev(), active(), st()));
+        CC_CUDA(M3Launch<T>::prim(c, in, prim, defer, bcc, dt_dev(), active(), st()));
         CC_CUDA(M3Launch<T>::faces(c, in, prim, fX, fY, fZ, active(), st()));
         CC_CUDA(M3Launch<T>::update(c, in, out, fX, fY, fZ, dt_dev(), active(), st()));
         CC_CUDA(M3Launch<T>::edges(c, in, fX, fY, fZ, Ex, Ey, Ez, active(), st()));
         CC_CUDA(M3Launch<T>::ct(c, in, out, Ex, Ey, Ez, dt_dev(), active(), st()));
-        count(7);
+        count(defer && c.resistive ? 8 : 7);
         if (h->profiling) {
             CC_CUDA(cudaEventRecord(e1, st()));
             h->timed.emplace_back(e0, e1);
@@ -205,8 +207,8 @@ template <class T> struct Mhd3d : Mhd3dBase {
         const int a = cur, b = (cur + 1) % 3, d = (cur + 2) % 3;
         if (int r = stage(buf[a], buf[b], false)) return r;
         if (int r = stage(buf[b], buf[d], true)) return r;
-        CC_CUDA(M3Launch<T>::average(c, buf[a], buf[d], buf[b], dt_dev(), active(), spd_part, rho_part, st()));
-        count(1);
+        CC_CUDA(M3Launch<T>::average(c, buf[a], buf[d], buf[b], bcc, dt_dev(), active(), spd_part, rho_part, st()));
+        count(c.resistive ? 2 : 1);
         h->perf.steps += 1;
         cur = b;
         partials_valid = true;

@@ -15,10 +15,15 @@ inline int grid3(long long n) {
 
 template <class T>
 cudaError_t M3Launch<T>::prim(const M3Const<T>& c, const Fields3<T>& s, const PrimData<T>& pr, bool defer,
-                              const double* dt, const int* active, cudaStream_t st) {
+                              const Bcc3<T>& bcc, const double* dt, const int* active, cudaStream_t st) {
     const int g = grid3((long long)c.nx * c.ny * c.nz);
-    if (defer) m3_prim_kernel<T, true><<<g, 256, 0, st>>>(c, s, pr, dt, active);
-    else m3_prim_kernel<T, false><<<g, 256, 0, st>>>(c, s, pr, dt, active);
+    if (defer && c.resistive) {
+        m3_bcc_kernel<T><<<g, 256, 0, st>>>(c, s, bcc, active);
+        cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) return e;
+    }
+    if (defer) m3_prim_kernel<T, true><<<g, 256, 0, st>>>(c, s, pr, bcc, dt, active);
+    else m3_prim_kernel<T, false><<<g, 256, 0, st>>>(c, s, pr, bcc, dt, active);
     return cudaGetLastError();
 }
 
@@ -57,9 +62,14 @@ cudaError_t M3Launch<T>::ct(const M3Const<T>& c, const Fields3<T>& in, const Fie
 
 template <class T>
 cudaError_t M3Launch<T>::average(const M3Const<T>& c, const Fields3<T>& un, const Fields3<T>& s2, const Fields3<T>& out,
-                                 const double* dt, const int* active, double* spd_part, double* rho_part,
-                                 cudaStream_t st) {
-    m3_average_kernel<T, RED_NT><<<RED_BLOCKS, RED_NT, 0, st>>>(c, un, s2, out, dt, active, spd_part, rho_part);
+                                 const Bcc3<T>& bcc, const double* dt, const int* active, double* spd_part,
+                                 double* rho_part, cudaStream_t st) {
+    if (c.resistive) {
+        m3_bcc_kernel<T><<<grid3((long long)c.nx * c.ny * c.nz), 256, 0, st>>>(c, s2, bcc, active);
+        cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) return e;
+    }
+    m3_average_kernel<T, RED_NT><<<RED_BLOCKS, RED_NT, 0, st>>>(c, un, s2, out, bcc, dt, active, spd_part, rho_part);
     return cudaGetLastError();
 }
 

@@ -9,8 +9,9 @@
 namespace ccb {
 
 template <class T> struct M3Launch {
+    // defer: the deferred Joule step first (its cell-centred B of s into bcc, then the pass)
     static cudaError_t prim(const M3Const<T>& c, const Fields3<T>& s, const PrimData<T>& pr, bool defer,
-                            const double* dt, const int* active, cudaStream_t st);
+                            const Bcc3<T>& bcc, const double* dt, const int* active, cudaStream_t st);
     static cudaError_t faces(const M3Const<T>& c, const Fields3<T>& s, const PrimData<T>& pr, const FaceData<T>& X,
                              const FaceData<T>& Y, const FaceData<T>& Z, const int* active, cudaStream_t st);
     static cudaError_t update(const M3Const<T>& c, const Fields3<T>& in, const Fields3<T>& out, const FaceData<T>& X,
@@ -20,9 +21,10 @@ template <class T> struct M3Launch {
                              const FaceData<T>& Z, T* Ex, T* Ey, T* Ez, const int* active, cudaStream_t st);
     static cudaError_t ct(const M3Const<T>& c, const Fields3<T>& in, const Fields3<T>& out, const T* Ex, const T* Ey,
                           const T* Ez, const double* dt, const int* active, cudaStream_t st);
+    // bcc: scratch planes for the cell-centred B of s2 (its Joule step)
     static cudaError_t average(const M3Const<T>& c, const Fields3<T>& un, const Fields3<T>& s2, const Fields3<T>& out,
-                               const double* dt, const int* active, double* spd_part, double* rho_part,
-                               cudaStream_t st);
+                               const Bcc3<T>& bcc, const double* dt, const int* active, double* spd_part,
+                               double* rho_part, cudaStream_t st);
     static cudaError_t speeds(const M3Const<T>& c, const Fields3<T>& s, double* spd_part, cudaStream_t st);
     static cudaError_t diag(const M3Const<T>& c, const Fields3<T>& s, double* part, cudaStream_t st);
     // the 11 snapshot fields of the reference's store, out: 11 planes of nx*ny*nz doubles
