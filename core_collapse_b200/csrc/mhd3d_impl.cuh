@@ -31,8 +31,15 @@ template <class T>
 cudaError_t M3Launch<T>::faces(const M3Const<T>& c, const Fields3<T>& s, const PrimData<T>& pr, const FaceData<T>& X,
                                const FaceData<T>& Y, const FaceData<T>& Z, const int* active, cudaStream_t st) {
     m3_face_kernel<T, 0><<<grid3((long long)(c.nx + 1) * c.ny * c.nz), 256, 0, st>>>(c, s, pr, X, active);
-    m3_face_kernel<T, 1><<<grid3((long long)c.nx * (c.ny + 1) * c.nz), 256, 0, st>>>(c, s, pr, Y, active);
-    m3_face_kernel<T, 2><<<grid3((long long)c.nx * c.ny * (c.nz + 1)), 256, 0, st>>>(c, s, pr, Z, active);
+    if constexpr (sizeof(T) == 4) {   // FP32: y and z faces as marches (FP64's window needs ~170 registers)
+        const dim3 gy((c.nx + 31) / 32, (c.nz + 7) / 8, (c.ny + 1 + M3_FACE_MCH - 1) / M3_FACE_MCH);
+        m3_face_march_kernel<T, 1><<<gy, 256, 0, st>>>(c, s, pr, Y, active);
+        const dim3 gz((c.nx + 31) / 32, (c.ny + 7) / 8, (c.nz + 1 + M3_FACE_MCH - 1) / M3_FACE_MCH);
+        m3_face_march_kernel<T, 2><<<gz, 256, 0, st>>>(c, s, pr, Z, active);
+    } else {
+        m3_face_kernel<T, 1><<<grid3((long long)c.nx * (c.ny + 1) * c.nz), 256, 0, st>>>(c, s, pr, Y, active);
+        m3_face_kernel<T, 2><<<grid3((long long)c.nx * c.ny * (c.nz + 1)), 256, 0, st>>>(c, s, pr, Z, active);
+    }
     return cudaGetLastError();
 }
 

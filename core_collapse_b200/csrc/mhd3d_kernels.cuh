@@ -215,6 +215,90 @@ __global__ void __launch_bounds__(256) m3_face_kernel(const M3Const<T> c, const 
     }
 }
 
+// y (DIR 1) or z (DIR 2) faces as a march: a thread owns the (i, k) or (i, j)
+// column and walks M3_FACE_MCH faces along the normal axis, holding the
+// primitives of cells m-1, m, m+1 and the MC slopes of cells m-1 and m, so a
+// cell's slopes are formed once for its two faces and each step loads one new
+// cell.  Every face state is the same expression of the same values as in
+// m3_face_kernel, where the stencil neighbours of a side's cell are re-mapped
+// from its mapped index: on a periodic axis that equals the window; on a
+// clamped one it differs only at the boundary faces (0 and n), which take the
+// original path.
+constexpr int M3_FACE_MCH = 32;
+template <class T, int DIR>
+__global__ void __launch_bounds__(256) m3_face_march_kernel(const M3Const<T> c, const Fields3<T> s,
+                                                            const PrimData<T> pr, const FaceData<T> out,
+                                                            const int* __restrict__ active) {
+    static_assert(DIR == 1 || DIR == 2, "march along y or z");
+    if (active && *active == 0) return;
+    const int i = blockIdx.x * 32 + (threadIdx.x & 31), o = blockIdx.y * 8 + (threadIdx.x >> 5);
+    const int n = DIR == 1 ? c.ny : c.nz, on = DIR == 1 ? c.nz : c.ny;
+    if (i >= c.nx || o >= on) return;
+    const AxisMap A = DIR == 1 ? c.ay : c.az;
+    const int m0 = blockIdx.z * M3_FACE_MCH, m1 = min(n + 1, m0 + M3_FACE_MCH);
+    auto cq = [&](int m) -> size_t { return DIR == 1 ? c.idx(i, A.cell(m), o) : c.idx(i, o, A.cell(m)); };
+    const T hL = T(0.5) * T(1), hR = T(0.5) * T(-1);
+    T w[3][8];    // cells m-1, m, m+1
+    T sl[2][8];   // slopes of cells m-1, m (the normal B component has none)
+    auto load = [&](T* d, int m) {
+        const size_t q = cq(m);
+#pragma unroll
+        for (int k = 0; k < 8; k++) d[k] = pr.w[k][q];
+    };
+    auto slopes = [&](T* d, const T* a, const T* b, const T* e) {
+#pragma unroll
+        for (int k = 0; k < 8; k++) d[k] = mc_slope(a[k], b[k], e[k]);
+    };
+    T wm2[8];
+    load(wm2, m0 - 2);
+    load(w[0], m0 - 1);
+    load(w[1], m0);
+    load(w[2], m0 + 1);
+    slopes(sl[0], wm2, w[0], w[1]);
+    slopes(sl[1], w[0], w[1], w[2]);
+    for (int m = m0; m < m1; ++m) {
+        Prim<T> WL, WR;
+        if (!A.periodic && (m == 0 || m == n)) {   // the boundary faces of a clamped axis: the original stencil
+            const int Lc = A.cell(m - 1), Rc = A.cell(m);
+            auto at = [&](int mm) -> size_t { return DIR == 1 ? c.idx(i, mm, o) : c.idx(i, o, mm); };
+            WL = face_state3(pr, at(A.cell(Lc - 1)), at(Lc), at(A.cell(Lc + 1)), DIR, T(1), c.floor_rho, c.floor_P);
+            WR = face_state3(pr, at(A.cell(Rc - 1)), at(Rc), at(A.cell(Rc + 1)), DIR, T(-1), c.floor_rho, c.floor_P);
+        } else {
+            auto side = [&](const T* v, const T* d, T h) {
+                Prim<T> W;
+                W.r = v[0] + h * d[0]; W.u = v[1] + h * d[1]; W.v = v[2] + h * d[2]; W.w = v[3] + h * d[3];
+                W.P = v[4] + h * d[4];
+                W.bx = v[5] + h * d[5];
+                W.by = (DIR == 1) ? v[6] : v[6] + h * d[6];
+                W.bz = (DIR == 2) ? v[7] : v[7] + h * d[7];
+                W.r = vmax(W.r, c.floor_rho);
+                W.P = vmax(W.P, c.floor_P);
+                return W;
+            };
+            WL = side(w[0], sl[0], hL);
+            WR = side(w[1], sl[1], hR);
+        }
+        const size_t qf = DIR == 1 ? c.idx(i, m, o) : c.idx(i, o, m);
+        Flux<T> F;
+        T e1, e2;
+        if (DIR == 1) {
+            F = hlld_y(c, WL, WR, s.by[qf]);
+            e1 = F.f5; e2 = -F.f6;
+        } else {
+            F = hlld_z(c, WL, WR, s.bz[qf]);
+            e1 = F.f6; e2 = -F.f5;
+        }
+        out.f[0][qf] = F.f0; out.f[1][qf] = F.f1; out.f[2][qf] = F.f2; out.f[3][qf] = F.f3; out.f[4][qf] = F.f4;
+        out.f[5][qf] = e1; out.f[6][qf] = e2;
+        if (m + 1 < m1) {   // advance the window to face m+1
+#pragma unroll
+            for (int k = 0; k < 8; k++) { w[0][k] = w[1][k]; w[1][k] = w[2][k]; sl[0][k] = sl[1][k]; }
+            load(w[2], m + 2);
+            slopes(sl[1], w[0], w[1], w[2]);
+        }
+    }
+}
+
 // FV update + floors with the stage-input B (M3:803-834)
 template <class T>
 __global__ void __launch_bounds__(256) m3_update_kernel(const M3Const<T> c, const Fields3<T> in, const Fields3<T> out,
