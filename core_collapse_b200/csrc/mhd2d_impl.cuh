@@ -118,15 +118,22 @@ cudaError_t M2Launch<T>::derived(const M2Const<T>& c, const Fields<T>& st, doubl
     return cudaGetLastError();
 }
 
+// grid of the pack kernels: columns in 256-thread blocks, rows up to 65535
+inline dim3 pack_grid(int w, int h) {
+    const unsigned gx = (unsigned)((w + 255) / 256);
+    const unsigned gy = (unsigned)(h < 65535 ? (h < 1 ? 1 : h) : 65535);
+    return dim3(gx < 1 ? 1 : gx, gy);
+}
+
 template <class T>
 cudaError_t M2Launch<T>::pack_in(const double* src, T* dst, int w, int h, int pitch, cudaStream_t s) {
-    pack_in_kernel<T><<<grid_for((size_t)w * h, 256, 4096), 256, 0, s>>>(src, dst, w, h, pitch);
+    pack_in_kernel<T><<<pack_grid(w, h), 256, 0, s>>>(src, dst, w, h, pitch);
     return cudaGetLastError();
 }
 
 template <class T>
 cudaError_t M2Launch<T>::pack_out(const T* src, double* dst, int w, int h, int pitch, cudaStream_t s) {
-    pack_out_kernel<T><<<grid_for((size_t)w * h, 256, 4096), 256, 0, s>>>(src, dst, w, h, pitch);
+    pack_out_kernel<T><<<pack_grid(w, h), 256, 0, s>>>(src, dst, w, h, pitch);
     return cudaGetLastError();
 }
 

@@ -536,21 +536,18 @@ struct DtSpec {
 
 // Host <-> device layout conversion: contiguous FP64 reference layout with row
 // length w and h rows  <->  pitched T field.
+// rows over blockIdx.y, columns over blockIdx.x (no index division)
 template <class T>
 __global__ void pack_in_kernel(const double* __restrict__ src, T* __restrict__ dst, int w, int h, int pitch) {
-    const size_t n = (size_t)w * h;
-    for (size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += (size_t)gridDim.x * blockDim.x) {
-        const int i = (int)(k % w), j = (int)(k / w);
-        dst[(size_t)j * pitch + i] = (T)src[k];
-    }
+    for (int j = blockIdx.y; j < h; j += gridDim.y)
+        for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < w; i += gridDim.x * blockDim.x)
+            dst[(size_t)j * pitch + i] = (T)src[(size_t)j * w + i];
 }
 template <class T>
 __global__ void pack_out_kernel(const T* __restrict__ src, double* __restrict__ dst, int w, int h, int pitch) {
-    const size_t n = (size_t)w * h;
-    for (size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += (size_t)gridDim.x * blockDim.x) {
-        const int i = (int)(k % w), j = (int)(k / w);
-        dst[k] = (double)src[(size_t)j * pitch + i];
-    }
+    for (int j = blockIdx.y; j < h; j += gridDim.y)
+        for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < w; i += gridDim.x * blockDim.x)
+            dst[(size_t)j * w + i] = (double)src[(size_t)j * pitch + i];
 }
 
 }  // namespace ccb
