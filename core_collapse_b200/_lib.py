@@ -211,6 +211,7 @@ SIGNATURES = {
     "cc_batch_compute_dt": (C.c_int, [_H, _DP]),
     "cc_batch_advance": (C.c_int, [_H, C.c_int, _DP]),
     "cc_batch_diagnostics": (C.c_int, [_H, C.c_int, C.POINTER(CcDiag)]),
+    "cc_batch_times": (C.c_int, [_H, _DP]),
     "cc_batch_autotune": (C.c_int, [_H, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_double)]),
     "cc_batch_set_shape": (C.c_int, [_H, C.c_int]),
     "cc_batch_get_info": (C.c_int, [_H, C.POINTER(CcBatchInfo)]),

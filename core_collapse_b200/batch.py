@@ -92,7 +92,13 @@ class BatchSolver:
         ptr = _dp(tt) if t is not None else None
         self._check(self._lib.cc_batch_advance(self._h, int(nsteps), ptr))
         if t is None:
-            tt = np.array([self.diagnostics(i)["t"] for i in range(self.n)])
+            self._check(self._lib.cc_batch_times(self._h, _dp(tt)))
+        return tt
+
+    def times(self) -> np.ndarray:
+        """Every instance's simulated time (one device-to-host copy)."""
+        tt = np.zeros(self.n)
+        self._check(self._lib.cc_batch_times(self._h, _dp(tt)))
         return tt
 
     def diagnostics(self, i: int) -> dict:

@@ -99,6 +99,7 @@ struct BatchBase {
     virtual int compute_dt(double* dt) = 0;
     virtual int advance(int nsteps, double* t) = 0;
     virtual int diagnostics(int inst, cc_diag* d) = 0;
+    virtual int times(double* t) = 0;
     virtual int autotune(int reps, int* shape, double* ms) = 0;
     virtual int set_shape(int shape) = 0;
     virtual int info(cc_batch_info* out) = 0;
@@ -522,6 +523,12 @@ template <class T> struct Batch : BatchBase {
         CC_CUDA(cudaMemcpyAsync(&terr, tcerr, sizeof(int), cudaMemcpyDeviceToHost, st()));
         CC_CUDA(cudaStreamSynchronize(st()));
         if (terr) return fail(h, CC_ERR_CUDA, "tensor-core Poisson transform: an mbarrier wait timed out");
+        return CC_OK;
+    }
+
+    int times(double* t) override {
+        CC_CUDA(cudaMemcpyAsync(t, tclk, sizeof(double) * n, cudaMemcpyDeviceToHost, st()));
+        CC_CUDA(cudaStreamSynchronize(st()));
         return CC_OK;
     }
 

@@ -105,6 +105,13 @@ int cc_batch_diagnostics(cc_handle* h, int inst, cc_diag* d) {
     return b->diagnostics(inst, d);
 }
 
+int cc_batch_times(cc_handle* h, double* t) {
+    BatchBase* b = bt(h);
+    if (!b || !t) return CC_ERR_ARG;
+    if (int r = set_dev(h)) return r;
+    return b->times(t);
+}
+
 int cc_batch_autotune(cc_handle* h, int reps, int* shape, double* ms) {
     BatchBase* b = bt(h);
     if (!b) return CC_ERR_ARG;

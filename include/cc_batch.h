@@ -67,6 +67,9 @@ int cc_batch_compute_dt(cc_handle* h, double* dt);
 int cc_batch_advance(cc_handle* h, int nsteps, double* t);
 
 int cc_batch_diagnostics(cc_handle* h, int inst, cc_diag* d);
+/* Every instance's simulated time (n doubles, instance order): the clocks
+ * cc_batch_advance keeps on the device, read with one copy. */
+int cc_batch_times(cc_handle* h, double* t);
 
 /* Time every stage candidate on the resident state (reps launches each) and
  * keep the fastest; shape / ms (may be NULL) receive the choice and its mean

@@ -205,3 +205,16 @@ def test_create_rejects_sor_gravity():
     with pytest.raises(CcError) as e:
         BatchSolver([p])
     assert e.value.code == L.CC_ERR_UNSUPPORTED
+
+
+def test_times_equal_diagnostics():
+    """cc_batch_times (one copy of the device clocks) == each instance's
+    diagnostics time after advance(nsteps) without start times."""
+    from core_collapse_b200.batch import BatchSolver, collapse_ensemble
+    params, states = collapse_ensemble(6, seed=5, precision="fp64")
+    with BatchSolver(params) as b:
+        for k in range(len(params)):
+            b.upload(k, *states[k])
+        t = b.advance(3)
+        want = np.array([b.diagnostics(i)["t"] for i in range(len(params))])
+        assert np.array_equal(t, want) and np.array_equal(b.times(), want) and np.all(want > 0)
