@@ -239,6 +239,11 @@ def test_checkpoint_rejects_bad_files(tmp_path):
         with pytest.raises(CcError) as e:
             g.load_checkpoint(path)
         assert e.value.code == L.CC_ERR_ARG
+    p32, _ = make_case_ns("kicked_viscous", precision="fp32")   # same grid, other precision
+    with Ns2dSolver(p32) as g:
+        with pytest.raises(CcError) as e:
+            g.load_checkpoint(path)
+        assert e.value.code == L.CC_ERR_ARG
 
 
 def test_reference_configuration_runs_to_t_end():
