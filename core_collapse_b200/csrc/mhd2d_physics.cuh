@@ -64,11 +64,20 @@ __host__ __device__ __forceinline__ Prim<T> to_prim(const M2Const<T>& c, T rho, 
     return W;
 }
 
+// The FP32 bulk path is issue-bound and each of its divisions is several
+// instructions, so where one denominator serves several quotients it takes
+// one reciprocal and multiplies (a rounding change of an ulp); FP64 keeps the
+// reference's divisions operation for operation.
+template <class T> __host__ __device__ constexpr bool fast_recip() { return sizeof(T) == 4; }
+
 // total energy of a primitive state, ideal gas (M2:357, 397, 482, 495)
 template <class T>
 __host__ __device__ __forceinline__ T energy(const M2Const<T>& c, const Prim<T>& W) {
     T B2 = W.bx * W.bx + W.by * W.by + W.bz * W.bz;
-    return W.P / c.gm1 + T(0.5) * W.r * (W.u * W.u + W.v * W.v + W.w * W.w) + T(0.5) * B2;
+    T eint;
+    if constexpr (fast_recip<T>()) eint = W.P * (T(1.0) / c.gm1);   // 1/gm1 shared by every call in a face
+    else eint = W.P / c.gm1;
+    return eint + T(0.5) * W.r * (W.u * W.u + W.v * W.v + W.w * W.w) + T(0.5) * B2;
 }
 
 // fast magnetosonic speed with normal component bn (M2:148-174)
@@ -77,8 +86,15 @@ __host__ __device__ __forceinline__ T fast_speed(const M2Const<T>& c, const Prim
     T a2 = c.gamma * W.P / vmax(W.r, c.floor_rho);
     T b2 = W.bx * W.bx + W.by * W.by + W.bz * W.bz;
     T rho = vmax(W.r, T(1e-300));
-    T vA2 = b2 / rho;
-    T vn2 = (bn * bn) / rho;
+    T vA2, vn2;
+    if constexpr (fast_recip<T>()) {
+        const T ir = T(1.0) / rho;
+        vA2 = b2 * ir;
+        vn2 = (bn * bn) * ir;
+    } else {
+        vA2 = b2 / rho;
+        vn2 = (bn * bn) / rho;
+    }
     T disc = (a2 + vA2) * (a2 + vA2) - T(4.0) * a2 * vn2;
     disc = vmax(T(0.0), disc);
     T cf2 = T(0.5) * ((a2 + vA2) + sqrt(disc));
@@ -153,19 +169,35 @@ __host__ __device__ __forceinline__ Flux<T> hlld_x(const Cst& c, Prim<T> L, Prim
     T vLs = L.v, wLs = L.w, vRs = R.v, wRs = R.w;
     if (fabs(dL) > T(1e-14)) {
         const T num = L.r * sL * (SL - L.u) - bn2;
-        ByLs = L.by * num / dL;
-        BzLs = L.bz * num / dL;
         const T dd = L.r * (SL - L.u) * (SL - SM);
-        vLs = L.v - Bn * (ByLs - L.by) / dd;
-        wLs = L.w - Bn * (BzLs - L.bz) / dd;
+        if constexpr (fast_recip<T>()) {
+            const T q = num / dL, bq = Bn / dd;
+            ByLs = L.by * q;
+            BzLs = L.bz * q;
+            vLs = L.v - (ByLs - L.by) * bq;
+            wLs = L.w - (BzLs - L.bz) * bq;
+        } else {
+            ByLs = L.by * num / dL;
+            BzLs = L.bz * num / dL;
+            vLs = L.v - Bn * (ByLs - L.by) / dd;
+            wLs = L.w - Bn * (BzLs - L.bz) / dd;
+        }
     }
     if (fabs(dR) > T(1e-14)) {
         const T num = R.r * sR * (SR - R.u) - bn2;
-        ByRs = R.by * num / dR;
-        BzRs = R.bz * num / dR;
         const T dd = R.r * (SR - R.u) * (SR - SM);
-        vRs = R.v - Bn * (ByRs - R.by) / dd;
-        wRs = R.w - Bn * (BzRs - R.bz) / dd;
+        if constexpr (fast_recip<T>()) {
+            const T q = num / dR, bq = Bn / dd;
+            ByRs = R.by * q;
+            BzRs = R.bz * q;
+            vRs = R.v - (ByRs - R.by) * bq;
+            wRs = R.w - (BzRs - R.bz) * bq;
+        } else {
+            ByRs = R.by * num / dR;
+            BzRs = R.bz * num / dR;
+            vRs = R.v - Bn * (ByRs - R.by) / dd;
+            wRs = R.w - Bn * (BzRs - R.bz) / dd;
+        }
     }
     const T sqL = sqrt(vmax(rLs, T(1e-300)));
     const T sqR = sqrt(vmax(rRs, T(1e-300)));
@@ -186,10 +218,18 @@ __host__ __device__ __forceinline__ Flux<T> hlld_x(const Cst& c, Prim<T> L, Prim
     } else {
         const T sgn = (Bn >= T(0.0)) ? T(1.0) : T(-1.0);
         const T d2 = sqL + sqR;
-        vs = (sqL * vLs + sqR * vRs + (ByRs - ByLs) * sgn) / d2;
-        ws = (sqL * wLs + sqR * wRs + (BzRs - BzLs) * sgn) / d2;
-        Bys = (sqL * ByRs + sqR * ByLs + sqL * sqR * (vRs - vLs) * sgn) / d2;
-        Bzs = (sqL * BzRs + sqR * BzLs + sqL * sqR * (wRs - wLs) * sgn) / d2;
+        if constexpr (fast_recip<T>()) {
+            const T id2 = T(1.0) / d2;
+            vs = (sqL * vLs + sqR * vRs + (ByRs - ByLs) * sgn) * id2;
+            ws = (sqL * wLs + sqR * wRs + (BzRs - BzLs) * sgn) * id2;
+            Bys = (sqL * ByRs + sqR * ByLs + sqL * sqR * (vRs - vLs) * sgn) * id2;
+            Bzs = (sqL * BzRs + sqR * BzLs + sqL * sqR * (wRs - wLs) * sgn) * id2;
+        } else {
+            vs = (sqL * vLs + sqR * vRs + (ByRs - ByLs) * sgn) / d2;
+            ws = (sqL * wLs + sqR * wRs + (BzRs - BzLs) * sgn) / d2;
+            Bys = (sqL * ByRs + sqR * ByLs + sqL * sqR * (vRs - vLs) * sgn) / d2;
+            Bzs = (sqL * BzRs + sqR * BzLs + sqL * sqR * (wRs - wLs) * sgn) / d2;
+        }
     }
     // U_star (M2:486-505) and the jump F_W + S (U* - U_W) (M2:507-519)
     const T vBs = SM * Bn + vs * Bys + ws * Bzs;
