@@ -86,10 +86,10 @@ __device__ __forceinline__ void joule_cell(const M2Const<T>& c, const Fields<T>&
     const T bzC = Bz;
     const T bzE = s.Bz[(size_t)j * P + iE], bzW = s.Bz[(size_t)j * P + iW];
     const T bzN = s.Bz[(size_t)jN * P + i], bzS = s.Bz[(size_t)jS * P + i];
-    const T dBzdy = (bzN - bzS) / c.two_dy;
-    const T dBzdx = (bzE - bzW) / c.two_dx;
-    const T dBydx = (s.by[(size_t)j * P + iE] - s.by[(size_t)j * P + i]) / c.dx;
-    const T dBxdy = (s.bx[(size_t)jN * P + i] - s.bx[(size_t)j * P + i]) / c.dy;
+    const T dBzdy = div_or_mul(bzN - bzS, c.two_dy, T(0.5) * c.inv_dy);
+    const T dBzdx = div_or_mul(bzE - bzW, c.two_dx, T(0.5) * c.inv_dx);
+    const T dBydx = div_or_mul(s.by[(size_t)j * P + iE] - s.by[(size_t)j * P + i], c.dx, c.inv_dx);
+    const T dBxdy = div_or_mul(s.bx[(size_t)jN * P + i] - s.bx[(size_t)j * P + i], c.dy, c.inv_dy);
     const T Jx = dBzdy, Jy = -dBzdx, Jz = dBydx - dBxdy;
     const T J2 = Jx * Jx + Jy * Jy + Jz * Jz;
     E = E + dt * c.eta * J2;
@@ -257,8 +257,8 @@ __device__ __forceinline__ void m2_stage_tile(const M2Const<T>& c, const Fields<
         if (c.resistive) {
             const int ci = c.ax.cell(ie), cim = c.ax.cell(ie - 1);
             const int cj = c.ay.cell(je), cjm = c.ay.cell(je - 1);
-            const T dBydx = (in.by[(size_t)je * P + ci] - in.by[(size_t)je * P + cim]) / c.dx;
-            const T dBxdy = (in.bx[(size_t)cj * P + ie] - in.bx[(size_t)cjm * P + ie]) / c.dy;
+            const T dBydx = div_or_mul(in.by[(size_t)je * P + ci] - in.by[(size_t)je * P + cim], c.dx, c.inv_dx);
+            const T dBxdy = div_or_mul(in.bx[(size_t)cj * P + ie] - in.bx[(size_t)cjm * P + ie], c.dy, c.inv_dy);
             res = c.eta * (dBydx - dBxdy);
         }
         ez[k] = ideal + res;
@@ -316,11 +316,17 @@ __device__ __forceinline__ void m2_stage_tile(const M2Const<T>& c, const Fields<
             const T* phi = ga;
             const int iE = c.ax.cell(gi + 1), iW = c.ax.cell(gi - 1);
             const int jN = c.ay.cell(gj + 1), jS = c.ay.cell(gj - 1);
-            gxq = -(phi[(size_t)gj * P + iE] - phi[(size_t)gj * P + iW]) / c.two_dx;
-            gyq = -(phi[(size_t)jN * P + gi] - phi[(size_t)jS * P + gi]) / c.two_dy;
+            gxq = div_or_mul(-(phi[(size_t)gj * P + iE] - phi[(size_t)gj * P + iW]), c.two_dx, T(0.5) * c.inv_dx);
+            gyq = div_or_mul(-(phi[(size_t)jN * P + gi] - phi[(size_t)jS * P + gi]), c.two_dy, T(0.5) * c.inv_dy);
         }
-        const T u = mx / vmax(rho, T(1e-300));
-        const T v = my / vmax(rho, T(1e-300));
+        T u, v;
+        if constexpr (fast_recip<T>()) {
+            const T ir = T(1.0) / vmax(rho, T(1e-300));
+            u = mx * ir; v = my * ir;
+        } else {
+            u = mx / vmax(rho, T(1e-300));
+            v = my / vmax(rho, T(1e-300));
+        }
         mx += dt * rho * gxq;
         my += dt * rho * gyq;
         E += dt * rho * (u * gxq + v * gyq);

@@ -36,11 +36,29 @@ __host__ __device__ __forceinline__ Prim<T> prim_select(bool left, const Prim<T>
     return W;
 }
 
+// The FP32 bulk path is issue-bound and each of its divisions is several
+// instructions, so where one denominator serves several quotients it takes
+// one reciprocal and multiplies (a rounding change of an ulp); FP64 keeps the
+// reference's divisions operation for operation.
+template <class T> __host__ __device__ constexpr bool fast_recip() { return sizeof(T) == 4; }
+
+// a / b; a * ib on the fast-reciprocal path (ib = 1/b, precomputed)
+template <class T> __host__ __device__ __forceinline__ T div_or_mul(T a, T b, T ib) {
+    if constexpr (fast_recip<T>()) return a * ib;
+    else return a / b;
+}
+
 // enforce_floors (M2:114-124)
 template <class T>
 __host__ __device__ __forceinline__ void floors(const M2Const<T>& c, T& rho, T mx, T my, T mz, T& E, T Bx, T By, T Bz) {
     rho = vmax(rho, c.floor_rho);
-    T u = mx / rho, v = my / rho, w = mz / rho;
+    T u, v, w;
+    if constexpr (fast_recip<T>()) {
+        const T ir = T(1.0) / rho;
+        u = mx * ir; v = my * ir; w = mz * ir;
+    } else {
+        u = mx / rho; v = my / rho; w = mz / rho;
+    }
     T kin = T(0.5) * rho * (u * u + v * v + w * w);
     T mag = T(0.5) * (Bx * Bx + By * By + Bz * Bz);
     T P = c.gm1 * (E - kin - mag);
@@ -54,7 +72,13 @@ __host__ __device__ __forceinline__ void floors(const M2Const<T>& c, T& rho, T m
 template <class T>
 __host__ __device__ __forceinline__ Prim<T> to_prim(const M2Const<T>& c, T rho, T mx, T my, T mz, T E, T Bx, T By, T Bz) {
     rho = vmax(rho, c.floor_rho);
-    T u = mx / rho, v = my / rho, w = mz / rho;
+    T u, v, w;
+    if constexpr (fast_recip<T>()) {
+        const T ir = T(1.0) / rho;
+        u = mx * ir; v = my * ir; w = mz * ir;
+    } else {
+        u = mx / rho; v = my / rho; w = mz / rho;
+    }
     T kin = T(0.5) * rho * (u * u + v * v + w * w);
     T mag = T(0.5) * (Bx * Bx + By * By + Bz * Bz);
     T P = c.gm1 * (E - kin - mag);
@@ -63,12 +87,6 @@ __host__ __device__ __forceinline__ Prim<T> to_prim(const M2Const<T>& c, T rho, 
     W.r = rho; W.u = u; W.v = v; W.w = w; W.P = P; W.bx = Bx; W.by = By; W.bz = Bz;
     return W;
 }
-
-// The FP32 bulk path is issue-bound and each of its divisions is several
-// instructions, so where one denominator serves several quotients it takes
-// one reciprocal and multiplies (a rounding change of an ulp); FP64 keeps the
-// reference's divisions operation for operation.
-template <class T> __host__ __device__ constexpr bool fast_recip() { return sizeof(T) == 4; }
 
 // total energy of a primitive state, ideal gas (M2:357, 397, 482, 495)
 template <class T>
