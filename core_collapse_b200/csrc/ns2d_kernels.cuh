@@ -39,8 +39,14 @@ template <class T>
 __device__ __forceinline__ NSPrim<T> ns_prim(const NSConst<T>& c, T d, T mx, T my, T E) {
     NSPrim<T> W;
     W.d = vmax(d, c.floor_rho);
-    W.u = mx / W.d;
-    W.v = my / W.d;
+    if constexpr (sizeof(T) == 4) {   // FP32: one reciprocal (an ulp of rounding)
+        const T id = T(1.0) / W.d;
+        W.u = mx * id;
+        W.v = my * id;
+    } else {
+        W.u = mx / W.d;
+        W.v = my / W.d;
+    }
     const T ke = T(0.5) * W.d * (W.u * W.u + W.v * W.v);
     const T eint = E - ke;
     const T P = c.gm1 * eint;
@@ -64,8 +70,11 @@ __device__ __forceinline__ void ns_hllc(const NSConst<T>& c, T dL, T nL, T tL, T
                                         T F[4]) {
     const T aL = sqrt(c.gamma * pL / vmax(dL, c.floor_rho));
     const T aR = sqrt(c.gamma * pR / vmax(dR, c.floor_rho));
-    const T EL = pL / c.gm1 + T(0.5) * dL * (nL * nL + tL * tL);
-    const T ER = pR / c.gm1 + T(0.5) * dR * (nR * nR + tR * tR);
+    // FP32 (issue-bound): 1/gm1 and 1/(S - SM) each formed once
+    constexpr bool F32 = sizeof(T) == 4;
+    const T igm1 = T(1.0) / c.gm1;
+    const T EL = (F32 ? pL * igm1 : pL / c.gm1) + T(0.5) * dL * (nL * nL + tL * tL);
+    const T ER = (F32 ? pR * igm1 : pR / c.gm1) + T(0.5) * dR * (nR * nR + tR * tR);
     const T SL = vmin(nL - aL, nR - aR);
     const T SR = vmax(nL + aL, nR + aR);
     const T num = (pR - pL) + dL * nL * (SL - nL) - dR * nR * (SR - nR);
@@ -82,16 +91,17 @@ __device__ __forceinline__ void ns_hllc(const NSConst<T>& c, T dL, T nL, T tL, T
     if (left) { d = dL; n = nL; t = tL; p = pL; E = EL; S = SL; }
     else { d = dR; n = nR; t = tR; p = pR; E = ER; S = SR; }
     // flux_x_from_prim (NS:198-210)
-    const T Ef = p / c.gm1 + T(0.5) * d * (n * n + t * t);
+    const T Ef = (F32 ? p * igm1 : p / c.gm1) + T(0.5) * d * (n * n + t * t);
     F[0] = d * n;
     F[1] = d * n * n + p;
     F[2] = d * n * t;
     F[3] = (Ef + p) * n;
     if (upL || upR) return;
     // Ustar (NS:235-249): star energy with the star pressure
-    const T fac = d * (S - n) / (S - SM);
+    const T iSS = T(1.0) / (S - SM);
+    const T fac = F32 ? d * (S - n) * iSS : d * (S - n) / (S - SM);
     const T pstar = p + d * (S - n) * (SM - n);
-    const T Es = ((S - n) * E - p * n + pstar * SM) / (S - SM);
+    const T Es = F32 ? ((S - n) * E - p * n + pstar * SM) * iSS : ((S - n) * E - p * n + pstar * SM) / (S - SM);
     F[0] = F[0] + S * (fac - d);
     F[1] = F[1] + S * (fac * SM - d * n);
     F[2] = F[2] + S * (fac * t - d * t);
