@@ -89,12 +89,13 @@ __host__ __device__ __forceinline__ T energy(const M3Const<T>& c, const Prim<T>&
 template <class T>
 __host__ __device__ __forceinline__ void floors(const M3Const<T>& c, T& rho, T mx, T my, T mz, T& E, T Bx, T By, T Bz) {
     rho = vmax(rho, c.floor_rho);
-    const T u = mx / rho, v = my / rho, w = mz / rho;
+    const T ir = T(1.0) / rho;   // used on the FP32 path only (one reciprocal)
+    const T u = div_or_mul(mx, rho, ir), v = div_or_mul(my, rho, ir), w = div_or_mul(mz, rho, ir);
     const T kin = T(0.5) * rho * (u * u + v * v + w * w);
     const T mag = T(0.5) * (Bx * Bx + By * By + Bz * Bz);
     T eint = E - kin - mag;
     if (eint < T(0.0)) eint = T(0.0);
-    const T es = eint / rho;
+    const T es = div_or_mul(eint, rho, ir);
     T P = eos_pressure(c, rho, es);
     if (P < c.floor_P) P = c.floor_P;
     const ColdEos<T> cd = eos_cold(c, rho);
@@ -108,12 +109,13 @@ __host__ __device__ __forceinline__ void floors(const M3Const<T>& c, T& rho, T m
 template <class T>
 __host__ __device__ __forceinline__ Prim<T> to_prim(const M3Const<T>& c, T rho, T mx, T my, T mz, T E, T Bx, T By, T Bz) {
     rho = vmax(rho, c.floor_rho);
-    const T u = mx / rho, v = my / rho, w = mz / rho;
+    const T ir = T(1.0) / rho;   // used on the FP32 path only (one reciprocal)
+    const T u = div_or_mul(mx, rho, ir), v = div_or_mul(my, rho, ir), w = div_or_mul(mz, rho, ir);
     const T kin = T(0.5) * rho * (u * u + v * v + w * w);
     const T mag = T(0.5) * (Bx * Bx + By * By + Bz * Bz);
     T eint = E - kin - mag;
     if (eint < T(0.0)) eint = T(0.0);
-    const T es = eint / rho;
+    const T es = div_or_mul(eint, rho, ir);
     T P = eos_pressure(c, rho, es);
     if (P < c.floor_P) P = c.floor_P;
     Prim<T> W;
@@ -141,8 +143,9 @@ __device__ __forceinline__ T fast_speed(const M3Const<T>& c, const Prim<T>& W, T
     const T a2 = vmax(T(0.0), num / rhof);
     const T b2 = W.bx * W.bx + W.by * W.by + W.bz * W.bz;
     const T rho = vmax(W.r, T(1e-300));
-    const T vA2 = b2 / rho;
-    const T vn2 = (bn * bn) / rho;
+    const T ir = T(1.0) / rho;   // used on the FP32 path only
+    const T vA2 = div_or_mul(b2, rho, ir);
+    const T vn2 = div_or_mul(bn * bn, rho, ir);
     T disc = (a2 + vA2) * (a2 + vA2) - T(4.0) * a2 * vn2;
     disc = vmax(T(0.0), disc);
     const T cf2 = T(0.5) * ((a2 + vA2) + sqrt(disc));
