@@ -31,7 +31,8 @@ template <class T> struct EPrim { T r, u, v, P; };
 template <class T>
 __device__ __forceinline__ void eh_floors(const EHConst<T>& c, T& rho, T mx, T my, T& E) {
     rho = vmax(rho, c.floor_rho);
-    const T u = mx / rho, v = my / rho;
+    const T ir = recip_if_fast(rho);
+    const T u = div_or_mul(mx, rho, ir), v = div_or_mul(my, rho, ir);
     const T kin = T(0.5) * rho * (u * u + v * v);
     const T P = c.gm1 * (E - kin);
     if (P < c.floor_P) {
@@ -44,7 +45,8 @@ __device__ __forceinline__ void eh_floors(const EHConst<T>& c, T& rho, T mx, T m
 template <class T>
 __device__ __forceinline__ EPrim<T> eh_prim(const EHConst<T>& c, T rho, T mx, T my, T E, T* a = nullptr) {
     const T r = vmax(rho, c.floor_rho);
-    const T u = mx / r, v = my / r;
+    const T ir = recip_if_fast(r);
+    const T u = div_or_mul(mx, r, ir), v = div_or_mul(my, r, ir);
     const T kin = T(0.5) * r * (u * u + v * v);
     T P = c.gm1 * (E - kin);
     if (P < c.floor_P) P = c.floor_P;
@@ -66,8 +68,9 @@ __device__ __forceinline__ void eh_hllc(const EHConst<T>& c, const EPrim<T>& L, 
     // prim_to_cons (EH:102-109)
     const T rL = vmax(L.r, c.floor_rho), rR = vmax(R.r, c.floor_rho);
     const T mLx = rL * L.u, mLy = rL * L.v, mRx = rR * R.u, mRy = rR * R.v;
-    const T EL = T(0.5) * rL * (L.u * L.u + L.v * L.v) + L.P / c.gm1;
-    const T ER = T(0.5) * rR * (R.u * R.u + R.v * R.v) + R.P / c.gm1;
+    const T igm1 = recip_if_fast(c.gm1);
+    const T EL = T(0.5) * rL * (L.u * L.u + L.v * L.v) + div_or_mul(L.P, c.gm1, igm1);
+    const T ER = T(0.5) * rR * (R.u * R.u + R.v * R.v) + div_or_mul(R.P, c.gm1, igm1);
     const T num = (R.P - L.P) + rL * nL * (SL - nL) - rR * nR * (SR - nR);
     const T den = rL * (SL - nL) - rR * (SR - nR);
     const T SM = (fabs(den) > T(1e-14)) ? (num / den) : T(0.0);
@@ -80,7 +83,7 @@ __device__ __forceinline__ void eh_hllc(const EHConst<T>& c, const EPrim<T>& L, 
     EPrim<T> W;
     W.r = left ? L.r : R.r; W.u = left ? L.u : R.u; W.v = left ? L.v : R.v; W.P = left ? L.P : R.P;
     const T S = left ? SL : SR;
-    const T Ef = W.P / c.gm1 + T(0.5) * W.r * (W.u * W.u + W.v * W.v);
+    const T Ef = div_or_mul(W.P, c.gm1, igm1) + T(0.5) * W.r * (W.u * W.u + W.v * W.v);
     if (DIR == 0) {
         F[0] = W.r * W.u; F[1] = W.r * W.u * W.u + W.P; F[2] = W.r * W.u * W.v; F[3] = (Ef + W.P) * W.u;
     } else {
@@ -91,9 +94,10 @@ __device__ __forceinline__ void eh_hllc(const EHConst<T>& c, const EPrim<T>& L, 
     const T r = left ? rL : rR, E = left ? EL : ER;
     const T mx = left ? mLx : mRx, my = left ? mLy : mRy;
     const T n = DIR == 0 ? W.u : W.v, t = DIR == 0 ? W.v : W.u;
-    const T rS = r * (S - n) / (S - SM);
+    const T iSS = recip_if_fast(S - SM);
+    const T rS = div_or_mul(r * (S - n), S - SM, iSS);
     const T mn = rS * SM, mt = rS * t;
-    const T ES = ((S - n) * E - W.P * n + W.P * SM) / (S - SM);
+    const T ES = div_or_mul((S - n) * E - W.P * n + W.P * SM, S - SM, iSS);
     const T mxS = DIR == 0 ? mn : mt, myS = DIR == 0 ? mt : mn;
     F[0] = F[0] + S * (rS - r);
     F[1] = F[1] + S * (mxS - mx);
@@ -182,10 +186,12 @@ eh_stage_kernel(const EHConst<T> c, const EHFields<T> un, const EHFields<T> in, 
     const size_t q = (size_t)gj * P + gi;
     // rhs (EH:503-524): flux divergence, then the gravity source with the raw state
     const int kx = ty * (TX + 1) + tx, ky = ty * TX + tx;
+    const T idx = recip_if_fast(c.dx), idy = recip_if_fast(c.dy);
     T d[4];
 #pragma unroll
     for (int m = 0; m < 4; m++)
-        d[m] = -(fx[m * NFX + kx + 1] - fx[m * NFX + kx]) / c.dx - (gy[m * NGY + ky + TX] - gy[m * NGY + ky]) / c.dy;
+        d[m] = -div_or_mul(fx[m * NFX + kx + 1] - fx[m * NFX + kx], c.dx, idx) -
+               div_or_mul(gy[m * NGY + ky + TX] - gy[m * NGY + ky], c.dy, idy);
     const T r0 = in.rho[q], mx0 = in.mx[q], my0 = in.my[q], E0 = in.E[q];
     if (c.gravity_on) {
         T gxq, gyq;
@@ -195,11 +201,12 @@ eh_stage_kernel(const EHConst<T> c, const EHFields<T> un, const EHFields<T> in, 
         } else {
             const int iE = c.pax.cell(gi + 1), iW = c.pax.cell(gi - 1);
             const int jN = c.pay.cell(gj + 1), jS = c.pay.cell(gj - 1);
-            gxq = -(phi[(size_t)gj * P + iE] - phi[(size_t)gj * P + iW]) / c.two_dx;
-            gyq = -(phi[(size_t)jN * P + gi] - phi[(size_t)jS * P + gi]) / c.two_dy;
+            gxq = div_or_mul(-(phi[(size_t)gj * P + iE] - phi[(size_t)gj * P + iW]), c.two_dx, T(0.5) * idx);
+            gyq = div_or_mul(-(phi[(size_t)jN * P + gi] - phi[(size_t)jS * P + gi]), c.two_dy, T(0.5) * idy);
         }
         const T rho = vmax(r0, c.floor_rho);
-        const T u = mx0 / rho, v = my0 / rho;
+        const T ir = recip_if_fast(rho);
+        const T u = div_or_mul(mx0, rho, ir), v = div_or_mul(my0, rho, ir);
         d[1] += rho * gxq;
         d[2] += rho * gyq;
         d[3] += rho * (u * gxq + v * gyq);

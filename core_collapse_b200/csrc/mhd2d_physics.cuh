@@ -42,6 +42,13 @@ __host__ __device__ __forceinline__ Prim<T> prim_select(bool left, const Prim<T>
 // reference's divisions operation for operation.
 template <class T> __host__ __device__ constexpr bool fast_recip() { return sizeof(T) == 4; }
 
+// 1/b on the fast-reciprocal path, else 0 (never read there): the FP64 build
+// forms no division that it does not use
+template <class T> __host__ __device__ __forceinline__ T recip_if_fast(T b) {
+    if constexpr (fast_recip<T>()) return T(1.0) / b;
+    else return T(0.0);
+}
+
 // a / b; a * ib on the fast-reciprocal path (ib = 1/b, precomputed)
 template <class T> __host__ __device__ __forceinline__ T div_or_mul(T a, T b, T ib) {
     if constexpr (fast_recip<T>()) return a * ib;

@@ -89,7 +89,7 @@ __host__ __device__ __forceinline__ T energy(const M3Const<T>& c, const Prim<T>&
 template <class T>
 __host__ __device__ __forceinline__ void floors(const M3Const<T>& c, T& rho, T mx, T my, T mz, T& E, T Bx, T By, T Bz) {
     rho = vmax(rho, c.floor_rho);
-    const T ir = T(1.0) / rho;   // used on the FP32 path only (one reciprocal)
+    const T ir = recip_if_fast(rho);
     const T u = div_or_mul(mx, rho, ir), v = div_or_mul(my, rho, ir), w = div_or_mul(mz, rho, ir);
     const T kin = T(0.5) * rho * (u * u + v * v + w * w);
     const T mag = T(0.5) * (Bx * Bx + By * By + Bz * Bz);
@@ -109,7 +109,7 @@ __host__ __device__ __forceinline__ void floors(const M3Const<T>& c, T& rho, T m
 template <class T>
 __host__ __device__ __forceinline__ Prim<T> to_prim(const M3Const<T>& c, T rho, T mx, T my, T mz, T E, T Bx, T By, T Bz) {
     rho = vmax(rho, c.floor_rho);
-    const T ir = T(1.0) / rho;   // used on the FP32 path only (one reciprocal)
+    const T ir = recip_if_fast(rho);
     const T u = div_or_mul(mx, rho, ir), v = div_or_mul(my, rho, ir), w = div_or_mul(mz, rho, ir);
     const T kin = T(0.5) * rho * (u * u + v * v + w * w);
     const T mag = T(0.5) * (Bx * Bx + By * By + Bz * Bz);
@@ -143,7 +143,7 @@ __device__ __forceinline__ T fast_speed(const M3Const<T>& c, const Prim<T>& W, T
     const T a2 = vmax(T(0.0), num / rhof);
     const T b2 = W.bx * W.bx + W.by * W.by + W.bz * W.bz;
     const T rho = vmax(W.r, T(1e-300));
-    const T ir = T(1.0) / rho;   // used on the FP32 path only
+    const T ir = recip_if_fast(rho);
     const T vA2 = div_or_mul(b2, rho, ir);
     const T vn2 = div_or_mul(bn * bn, rho, ir);
     T disc = (a2 + vA2) * (a2 + vA2) - T(4.0) * a2 * vn2;

@@ -72,7 +72,7 @@ __device__ __forceinline__ void ns_hllc(const NSConst<T>& c, T dL, T nL, T tL, T
     const T aR = sqrt(c.gamma * pR / vmax(dR, c.floor_rho));
     // FP32 (issue-bound): 1/gm1 and 1/(S - SM) each formed once
     constexpr bool F32 = sizeof(T) == 4;
-    const T igm1 = T(1.0) / c.gm1;
+    const T igm1 = recip_if_fast(c.gm1);
     const T EL = (F32 ? pL * igm1 : pL / c.gm1) + T(0.5) * dL * (nL * nL + tL * tL);
     const T ER = (F32 ? pR * igm1 : pR / c.gm1) + T(0.5) * dR * (nR * nR + tR * tR);
     const T SL = vmin(nL - aL, nR - aR);
@@ -98,7 +98,7 @@ __device__ __forceinline__ void ns_hllc(const NSConst<T>& c, T dL, T nL, T tL, T
     F[3] = (Ef + p) * n;
     if (upL || upR) return;
     // Ustar (NS:235-249): star energy with the star pressure
-    const T iSS = T(1.0) / (S - SM);
+    const T iSS = recip_if_fast(S - SM);
     const T fac = F32 ? d * (S - n) * iSS : d * (S - n) / (S - SM);
     const T pstar = p + d * (S - n) * (SM - n);
     const T Es = F32 ? ((S - n) * E - p * n + pstar * SM) * iSS : ((S - n) * E - p * n + pstar * SM) / (S - SM);
