@@ -71,11 +71,10 @@ def cpu_run(sample_n: int, nthreads: int, nsteps: int) -> tuple[float, float]:
     import ctypes as C
 
     import oracle_lib as O
-    from core_collapse_b200.mhd2d import ic_orszag_tang
     p = workload_params(sample_n, "fp64")
-    U, B = ic_orszag_tang(p, core_amp=4.0, core_width=0.1)
+    S0 = ic_orszag_tang_numpy(p, core_amp=4.0, core_width=0.1)
     cp = p.to_c()
-    states = [O.state_list(U, B) for _ in range(nthreads)]
+    states = [[a.copy() for a in S0] for _ in range(nthreads)]
     ptrs = [O.pp(s) for s in states]
     orc = O.oracle()
 
@@ -91,6 +90,38 @@ def cpu_run(sample_n: int, nthreads: int, nsteps: int) -> tuple[float, float]:
         t.join()
     wall = time.perf_counter() - t0
     return wall, float(nthreads) * sample_n * sample_n * nsteps
+
+
+def ic_orszag_tang_numpy(p, core_amp: float, core_width: float) -> list:
+    """The benchmark's initial state in the reference layouts, built with numpy
+    so that the CPU legs never load the GPU library: Orszag-Tang fields, face B
+    from the corner potential Az = B0 (cos(2 pi y) / (2 pi) + cos(4 pi x) / (4 pi)),
+    B0 = 1/sqrt(4 pi), rho = 25/(36 pi) + a Gaussian core, P = 5/(12 pi),
+    conserved through the reference's prim_to_cons (M2:137-146) with B at cell
+    centres from the face averages.  Returns [rho, mx, my, mz, E, Bz, Bx_f, By_f]."""
+    import numpy as np
+    nx, ny = p.Nx, p.Ny
+    dx, dy = (p.x1 - p.x0) / nx, (p.y1 - p.y0) / ny
+    B0 = 1.0 / np.sqrt(4.0 * np.pi)
+    X = p.x0 + np.arange(nx + 1) * dx
+    Y = p.y0 + np.arange(ny + 1) * dy
+    Az = B0 * (np.cos(2.0 * np.pi * Y)[:, None] / (2.0 * np.pi) + np.cos(4.0 * np.pi * X)[None, :] / (4.0 * np.pi))
+    bx = (Az[1:, :] - Az[:-1, :]) / dy            # (ny, nx+1)
+    by = -(Az[:, 1:] - Az[:, :-1]) / dx           # (ny+1, nx)
+    xc = p.x0 + (np.arange(nx) + 0.5) * dx
+    yc = p.y0 + (np.arange(ny) + 0.5) * dy
+    cx, cy = 0.5 * (p.x0 + p.x1), 0.5 * (p.y0 + p.y1)
+    r2 = (xc[None, :] - cx) ** 2 + (yc[:, None] - cy) ** 2
+    rho = np.maximum(25.0 / (36.0 * np.pi) + core_amp * np.exp(-r2 / (2.0 * core_width ** 2)), p.floor_rho)
+    u = np.broadcast_to(-np.sin(2.0 * np.pi * yc)[:, None], (ny, nx))
+    v = np.broadcast_to(np.sin(2.0 * np.pi * xc)[None, :], (ny, nx))
+    P = np.full((ny, nx), max(5.0 / (12.0 * np.pi), p.floor_P))
+    Bxc = 0.5 * (bx[:, :-1] + bx[:, 1:])
+    Byc = 0.5 * (by[:-1, :] + by[1:, :])
+    E = P / (p.gamma - 1.0) + 0.5 * rho * (u * u + v * v) + 0.5 * (Bxc * Bxc + Byc * Byc)
+    z = np.zeros(nx * ny)
+    return [np.ascontiguousarray(a).ravel() for a in (rho, rho * u, rho * v)] + [z.copy(), E.ravel().copy(), z.copy(),
+                                                                                  bx.ravel().copy(), by.ravel().copy()]
 
 
 def cpu_baseline(sample_n: int, nsteps: int) -> dict:
@@ -286,41 +317,38 @@ def run_ours(args) -> None:
     value64 = world * cells * args.steps / (ms64_max / 1000.0)
     stage64_avg_ms = perf64["stage_ms"] / max(1, perf64["stage_launches"])
 
-    # FP32-vs-FP64 L1 error after the same number of steps from the same IC
-    Ua, Ba = s32.download()
-    Ub, Bb = s64.download()
-    names = ["rho", "mx", "my", "mz", "E", "Bz", "Bx_f", "By_f"]
-    l1 = {}
-    for k, (a, b) in enumerate(zip(Ua.arrays() + [Ba.Bx_f, Ba.By_f], Ub.arrays() + [Bb.Bx_f, Bb.By_f])):
-        den = float(np.sum(np.abs(b)))
-        l1[names[k]] = float(np.sum(np.abs(a - b)) / den) if den > 0 else float(np.max(np.abs(a)))
-    d32, d64 = s32.diagnostics(), s64.diagnostics()
-    s64.close()
+    d32 = s32.diagnostics()
 
-    # end to end through the C ABI with pinned host buffers, copies timed every step
+    # end to end through the C ABI with pinned host buffers, copies timed every
+    # step: upload the state, one main-loop step, download the state
     pin = lambda m: torch.empty(m, dtype=torch.float64, pin_memory=True).numpy()
     from core_collapse_b200.mhd2d import Bfaces, Ucc
     Uh = Ucc(*[pin(cells) for _ in range(6)])
     Bh = Bfaces(pin((n + 1) * n), pin(n * (n + 1)))
-    for a, b in zip(Uh.arrays() + [Bh.Bx_f, Bh.By_f], U0.arrays() + [B0.Bx_f, B0.By_f]):
-        a[:] = b
     h2d = sum(a.nbytes for a in Uh.arrays()) + Bh.Bx_f.nbytes + Bh.By_f.nbytes
-    s32.set_profiling(False)
-    s32.reset_perf()
     e2e_steps = max(1, min(args.steps, args.e2e_steps))
-    barrier()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
-    for _ in range(e2e_steps):
-        s32.upload(Uh, Bh)
-        s32.advance(1)
-        s32.download(Uh, Bh)
-    e1.record(stream)
-    torch.cuda.synchronize()
-    barrier()
-    e2e_ms = max_over_ranks(e0.elapsed_time(e1))
-    e2e_value = world * cells * e2e_steps / (e2e_ms / 1000.0)
+
+    def e2e(s) -> float:
+        for a, b in zip(Uh.arrays() + [Bh.Bx_f, Bh.By_f], U0.arrays() + [B0.Bx_f, B0.By_f]):
+            a[:] = b
+        s.set_profiling(False)
+        s.reset_perf()
+        barrier()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(e2e_steps):
+            s.upload(Uh, Bh)
+            s.advance(1)
+            s.download(Uh, Bh)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        barrier()
+        return world * cells * e2e_steps / (max_over_ranks(e0.elapsed_time(e1)) / 1000.0)
+
+    e2e_value = e2e(s32)
+    e2e64_value = e2e(s64)
     s32.close()
+    s64.close()
 
     peaks = measured_peaks()
     achieved = stage_bytes / (stage_avg_ms / 1000.0) / 1e9
@@ -330,11 +358,11 @@ def run_ours(args) -> None:
         "vs_baseline": None, "dtype": "f32", "data": "synthetic", "config": config_block(args),
         "fp64": {"value": value64, "ms_per_step": ms64_max / args.steps, "dtype": "f64",
                  "stage_kernel_ms": stage64_avg_ms,
-                 "stage_kernel_gbs": STAGE_WORDS * 8 * cells / (stage64_avg_ms / 1000.0) / 1e9},
+                 "stage_kernel_gbs": STAGE_WORDS * 8 * cells / (stage64_avg_ms / 1000.0) / 1e9,
+                 "e2e": {"value": e2e64_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": h2d,
+                         "steps": e2e_steps, "api": "cc_mhd2d_upload + cc_mhd2d_advance(1) + cc_mhd2d_download, "
+                                                    "pinned FP64 host"}},
         "fp32_over_fp64": value32 / value64,
-        "l1_err_fp32_vs_fp64": {"max": max(l1.values()), "per_field": l1,
-                                "after_steps": args.warmup + args.steps,
-                                "t_fp32": d32["t"], "t_fp64": d64["t"]},
         "roofline": {"bound": "hbm", "kernel": "m2_stage_kernel<float> (one RK2 stage)",
                      "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
                      "frac": achieved / peaks["hbm_gbs"], "peak_source": peaks["source"],
@@ -347,6 +375,12 @@ def run_ours(args) -> None:
         "clocks": clk,
         "max_divB_fp32": d32["max_divB"],
     }
+    if world == 1 and not args.skip_ladder:
+        lad = run_ladder(args, stream)
+        line["precision_ladder"] = lad
+        big = lad["grids"][str(max(int(g) for g in lad["grids"]))]
+        line["l1_err"] = big["fp32"]["l1_max"]
+        line["linf_err"] = big["fp32"]["linf_max"]
     if world == 1 and not args.skip_3d:
         line["mhd3d"] = run_3d(args, stream)
     if world == 1 and not args.skip_ns:
@@ -366,6 +400,76 @@ def run_ours(args) -> None:
         dist.destroy_process_group()
 
 
+STATE_FIELDS = ["rho", "mx", "my", "mz", "E", "Bz", "Bx_f", "By_f"]
+
+
+def field_errors(got: list, want: list) -> dict:
+    """Per-field relative errors of a state against a reference state:
+    L1 = sum|a - b| / sum|b| and L-inf = max|a - b| / max|b| (absolute where
+    the reference field is identically zero)."""
+    import numpy as np
+    l1, linf = {}, {}
+    for name, a, b in zip(STATE_FIELDS, got, want):
+        d = np.abs(a - b)
+        s1, sm = float(np.sum(np.abs(b))), float(np.max(np.abs(b)))
+        l1[name] = float(np.sum(d)) / s1 if s1 > 0 else float(np.max(d))
+        linf[name] = float(np.max(d)) / sm if sm > 0 else float(np.max(d))
+    return {"l1": l1, "linf": linf, "l1_max": max(l1.values()), "linf_max": max(linf.values())}
+
+
+def run_ladder(args, stream) -> dict:
+    """Precision ladder of the FFT-gravity workload: from the same initial
+    state, FP64 runs --ladder-steps steps to t_final, then FP32 (plain, and
+    with the compensated state update) runs to the same t_final (its own CFL
+    steps, the last one clamped to t_final); each FP32 state is compared with
+    the FP64 one per field (L1, L-inf).  The FP64 GPU path stands in for the
+    oracle here: it matches the CPU restatement of the reference step to
+    <= 1e-12 (tests/test_gpu_config_scale.py runs that comparison at 256^2
+    and 1024^2)."""
+    import torch
+
+    from core_collapse_b200.mhd2d import Mhd2dSolver, ic_orszag_tang
+    import oracle_lib as O
+    out = {"steps": args.ladder_steps, "workload": "the benchmark workload at each grid, from t = 0",
+           "reference": "GPU FP64 path (pinned to the CPU oracle at <= 1e-12 by the config-scale parity tests)",
+           "grids": {}}
+    for n in [int(g) for g in args.ladder_grids.split(",") if g]:
+        p64 = workload_params(n, "fp64")
+        U0, B0 = ic_orszag_tang(p64, core_amp=4.0, core_width=0.1)
+        blk = {}
+
+        def run(p, nsteps):
+            with Mhd2dSolver(p) as s:
+                s.set_stream(stream.cuda_stream)
+                s.upload(U0, B0)
+                torch.cuda.synchronize()
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                t = s.advance(nsteps, 0.0)
+                e1.record(stream)
+                torch.cuda.synchronize()
+                U, B = s.download()
+                d = s.diagnostics()
+            return O.state_list(U, B), t, e0.elapsed_time(e1), d
+
+        S64, t64, ms64, d64 = run(p64, args.ladder_steps)
+        blk["t_final"] = t64
+        blk["fp64"] = {"ms": ms64, "steps": args.ladder_steps, "ms_per_step": ms64 / args.ladder_steps,
+                       "max_divB": d64["max_divB"]}
+        for tag, extra in (("fp32", {}), ("fp32_compensated", {"compensated": True})):
+            p = workload_params(n, "fp32")
+            p.t_end = t64
+            for k, v in extra.items():
+                setattr(p, k, v)
+            S, t, ms, d = run(p, args.ladder_steps + args.ladder_steps // 10 + 2)
+            e = field_errors(S, S64)
+            e.update({"t_final": t, "steps": d["steps"], "ms": ms, "ms_per_step": ms / max(1, d["steps"]),
+                      "max_divB": d["max_divB"]})
+            blk[tag] = e
+        out["grids"][str(n)] = blk
+    return out
+
+
 def run_3d(args, stream) -> dict:
     """3D resistive HLLD+CT workload: 256^3 periodic unit cube, ideal gas
     gamma 5/3 (hybrid EOS with K1 = Kbounce = 0), eta 5e-4, rho 1, p 1/gamma,
@@ -374,7 +478,7 @@ def run_3d(args, stream) -> dict:
 
     from core_collapse_b200.mhd3d import Mhd3dSolver, Params3, ic_turbulence3d
     n = args.grid3d
-    steps = max(1, min(args.steps, args.steps3d))
+    steps = max(1, args.steps3d)
     s0 = ic_turbulence3d(Params3.ideal_gas(Nx=n, Ny=n, Nz=n), seed=1)
     out = {"workload": f"3D resistive MHD HLLD+CT, {n}^3 periodic, random-phase v and A (|k| in [1,4], seed 1), "
                        f"rms v 0.5, rms B 0.3, eta 5e-4, CFL 0.4", "steps": steps, "warmup": args.warmup}
@@ -496,12 +600,16 @@ def run_ensemble(args, stream, rank: int, world: int, barrier, max_over_ranks, s
     with outflow boundaries, side drawn uniformly from {64,96,128,192,256}
     (seed 2), core amplitude U(2,20), width U(0.05,0.2), Bx U(0,0.2), eta
     log-uniform [1e-4,1e-2]; gamma 5/3, G 1, CFL 0.4, direct Poisson; FP32
-    state with FP64 reductions and FP64 Poisson.  Instances are split over
-    the ranks by cell count (no collective inside a step)."""
+    state, FP32 Poisson solve and FP64 reductions.  Instances are split over
+    the ranks by cell count (no collective inside a step).  The single-grid
+    comparison runs one large instance of the same physics and Poisson kind
+    (--ensemble-single-side^2, outflow, direct solve) through the same handle
+    type for the same number of steps."""
     import numpy as np
     import torch
 
     from core_collapse_b200.batch import BatchSolver, collapse_ensemble, partition_by_cells
+    from core_collapse_b200.mhd2d import ic_collapse
     params, states = collapse_ensemble(args.ensemble, seed=2, precision="fp32")
     mine = partition_by_cells(params, world)[rank]
     total_cells = sum(p.Nx * p.Ny for p in params)
@@ -536,8 +644,29 @@ def run_ensemble(args, stream, rank: int, world: int, barrier, max_over_ranks, s
     pf = b.perf()
     b.close()
     value = total_cells * steps / (ms / 1000.0)
+
+    # one large instance, same physics and Poisson kind (rank-local, no collective)
+    from dataclasses import replace as dc_replace
+    ns = args.ensemble_single_side
+    p1 = dc_replace(params[0], Nx=ns, Ny=ns, eta=1e-3)
+    U1, B1 = ic_collapse(p1, core_amp=9.0, core_width=0.1, noise=0.01, seed=0, Bx0=0.05)
+    with BatchSolver([p1]) as b1:
+        b1.set_stream(stream.cuda_stream)
+        b1.upload(0, U1, B1)
+        b1.autotune(reps=3)
+        b1.advance(args.warmup, np.zeros(1))
+        torch.cuda.synchronize()
+        e0.record(stream)
+        b1.advance(steps)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        single_value = ns * ns * steps / (e0.elapsed_time(e1) / 1000.0)
     out.update({"value": value, "unit": UNIT, "ms_per_step": ms / steps,
-                "ensemble_over_single_grid": value / world / single_fp32 if single_fp32 else None,
+                "single_grid": {"workload": f"one {ns}^2 collapse instance (core 9, width 0.1, Bx 0.05, eta 1e-3), "
+                                            "outflow, direct Poisson, FP32, same handle type",
+                                "value": single_value, "unit": UNIT},
+                "ensemble_over_single_grid": value / world / single_value,
+                "ensemble_over_single_fft_grid": value / world / single_fp32 if single_fp32 else None,
                 "tile": [info["tile_x"], info["tile_y"]], "autotune_choice": shape, "autotune_stage_ms": tune_ms,
                 "stage_ctas": info["stage_ctas"], "stage_tiles": info["stage_tiles"],
                 # stage-kernel time per step (events around the stage launches of 3 eager
@@ -545,6 +674,12 @@ def run_ensemble(args, stream, rank: int, world: int, barrier, max_over_ranks, s
                 "stage_share_of_step": (pf["stage_ms"] / 3.0) / (ms / steps) if ms > 0 else None,
                 "nonfinite_instances": nonfinite, "device_bytes_rank0": info["device_bytes"]})
     return out
+
+
+# per-entry finite-difference errors are reported for entries whose central
+# difference exceeds this fraction of the largest gradient: below it the
+# difference quotient's own roundoff (~1e-16 |loss| / h) dominates
+ADJ_FD_FLOOR = 1e-3
 
 
 def run_adjoint(args, stream) -> dict:
@@ -595,6 +730,8 @@ def run_adjoint(args, stream) -> dict:
         cells = rng.choice(n * n, size=args.adjoint_fd, replace=False)
         worst = 0.0
         gscale = float(np.max(np.abs(g.rho)))
+        floor = ADJ_FD_FLOOR * gscale
+        per_entry, n_above = 0.0, 0
         for c in cells:
             vals = []
             for sgn in (1.0, -1.0):
@@ -605,11 +742,16 @@ def run_adjoint(args, stream) -> dict:
                 vals.append(density_loss_adjoint(p, s.download()[0].rho, target)[0])
             fd = (vals[0] - vals[1]) / 2e-6
             worst = max(worst, abs(g.rho[c] - fd) / gscale)
+            if abs(fd) > floor:
+                n_above += 1
+                per_entry = max(per_entry, abs(g.rho[c] - fd) / abs(fd))
     out.update({"forward_ms": fwd_ms, "adjoint_ms": adj_ms, "adjoint_over_forward": adj_ms / fwd_ms,
                 "zone_updates_per_s_forward": n * n * nsteps / (fwd_ms / 1000.0),
                 "loss": loss, "dloss_deta": geta,
                 "fd_check": {"cells": int(args.adjoint_fd), "h": 1e-6,
-                             "max_abs_err_over_max_grad": worst}})
+                             "max_abs_err_over_max_grad": worst,
+                             "max_rel_err_per_entry": per_entry, "entries_above_floor": n_above,
+                             "floor": f"|fd| > {ADJ_FD_FLOOR:g} x max|grad|"}})
     return out
 
 
@@ -631,9 +773,12 @@ def main():
     ap.add_argument("--cpu-sample-grid", type=int, default=512)
     ap.add_argument("--cpu-steps", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--skip-ladder", action="store_true")
+    ap.add_argument("--ladder-steps", type=int, default=500)
+    ap.add_argument("--ladder-grids", default="1024,4096")
     ap.add_argument("--skip-3d", action="store_true")
     ap.add_argument("--grid3d", type=int, default=256)
-    ap.add_argument("--steps3d", type=int, default=20)
+    ap.add_argument("--steps3d", type=int, default=100)
     ap.add_argument("--skip-ns", action="store_true")
     ap.add_argument("--skip-eh", action="store_true")
     ap.add_argument("--grid-eh", type=int, default=512)
@@ -645,11 +790,12 @@ def main():
     ap.add_argument("--steps-ns", type=int, default=20)
     ap.add_argument("--skip-ensemble", action="store_true")
     ap.add_argument("--ensemble", type=int, default=512)
-    ap.add_argument("--ensemble-steps", type=int, default=60)
+    ap.add_argument("--ensemble-steps", type=int, default=300)
+    ap.add_argument("--ensemble-single-side", type=int, default=2048)
     ap.add_argument("--skip-adjoint", action="store_true")
     ap.add_argument("--adjoint-grid", type=int, default=512)
     ap.add_argument("--adjoint-steps", type=int, default=100)
-    ap.add_argument("--adjoint-fd", type=int, default=4)
+    ap.add_argument("--adjoint-fd", type=int, default=64)
     ap.add_argument("--adjoint-only", action="store_true", help="time only the adjoint block (a profiling aid)")
     ap.add_argument("--ns-only", action="store_true",
                     help="time only the Navier-Stokes block (a profiling aid; prints the ns2d block)")

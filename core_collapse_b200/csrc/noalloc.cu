@@ -33,6 +33,10 @@ static __device__ __align__(256) double cc_noalloc_scratch[NA_TOTAL];
 // Twiddles of each radix-2 pass of an n-point transform, one thread per pass,
 // by the recurrence w_{j+1} = w_j * wlen of the reference FFT
 // (navier_stokes_2d_hllc_poisson.cpp:160-171); pass of half-length h at [h-1, 2h-1).
+// wlen comes from the device's cos/sin, where the handle path builds its table
+// on the host with the C library's: the two can differ in the last bit of wlen,
+// so this solve agrees with cc_mhd2d_compute_gravity to about 1e-13 relative,
+// not bit for bit.
 __global__ void na_twiddle_kernel(Cplx<double>* tw, int n, int inverse) {
     const int pass = blockIdx.x * blockDim.x + threadIdx.x;
     if (pass >= 31) return;
@@ -89,7 +93,8 @@ extern "C" int cc_mhd2d_gravity_fft_noalloc(const cc_mhd2d_params* p, const doub
                                             void* stream) {
     if (!p || !rho || !gx || !gy) return CC_ERR_ARG;
     const int nx = p->Nx, ny = p->Ny;
-    if (p->precision != CC_FP64 || !p->periodic_x || !p->periodic_y) return CC_ERR_UNSUPPORTED;
+    if (p->precision != CC_FP64 || p->poisson_kind != CC_POISSON_FFT || !p->periodic_x || !p->periodic_y)
+        return CC_ERR_UNSUPPORTED;
     if (!pow2(nx) || !pow2(ny) || nx < 4 || ny < 4) return CC_ERR_UNSUPPORTED;
     if ((size_t)nx > NA_MAX_SIDE || (size_t)ny > NA_MAX_SIDE || (size_t)nx * (size_t)ny > NA_MAX_CELLS)
         return CC_ERR_TOO_LARGE;

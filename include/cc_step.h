@@ -374,8 +374,10 @@ int cc_ns2d_checkpoint_load(cc_handle* h, const char* path);
  * cudaMalloc -- a host application whose memory manager owns the GPU's
  * memory, or a loop that must not pay cudaMalloc's implicit device
  * synchronisation.  Same result as cc_mhd2d_compute_gravity with
- * poisson_kind == CC_POISSON_FFT and precision == CC_FP64, computed from device
- * arrays: rho (input) and gx, gy (outputs) are caller-owned device pointers,
+ * poisson_kind == CC_POISSON_FFT and precision == CC_FP64 (within 1e-12
+ * relative, not bit for bit: the twiddle tables are built on the device),
+ * computed from device arrays: rho (input) and gx, gy (outputs) are
+ * caller-owned device pointers,
  * FP64, Nx*Ny each, q = j*Nx + i.  Work is queued on `stream`
  * (cudaStream_t, NULL = legacy default stream) and the call returns without
  * waiting for it.
@@ -384,7 +386,9 @@ int cc_ns2d_checkpoint_load(cc_handle* h, const char* path);
  * held by every GPU that loads the library until the process exits); nothing
  * is allocated or freed.  Limits: periodic, Nx and Ny powers of two with
  * 4 <= Nx, Ny <= CC_NOALLOC_MAX_SIDE and Nx*Ny <= CC_NOALLOC_MAX_CELLS;
- * larger grids return CC_ERR_TOO_LARGE.
+ * larger grids return CC_ERR_TOO_LARGE.  Parameters asking for another solver
+ * (poisson_kind other than CC_POISSON_FFT), FP32, or a non-periodic axis
+ * return CC_ERR_UNSUPPORTED.
  * The first call on a device looks up the array's device address and raises
  * the FFT kernels' shared-memory limits; make that first call before any
  * stream capture.  Every call reuses the same array, which keeps the last

@@ -137,4 +137,12 @@ double ref_mhd2d_divB_max(const cc_mhd2d_params* c, double* const* f) {
     return m;
 }
 
+// The reference's own main() (its defaults, initial condition, time loop and
+// snapshot store), run once; its HDF5 datasets are recorded in memory by the
+// recording hdf5.h of this directory (read back through cc_h5rec_*).
+int ref_mhd2d_run_main() {
+    cc_h5rec_clear();
+    return refm2::ref_mhd2d_main();
+}
+
 }  // extern "C"

@@ -118,4 +118,12 @@ double ref_mhd3d_divB_max(const cc_mhd3d_params* c, double* const* f) {
     return m;
 }
 
+// The reference's own main() (its defaults, initial condition, time loop and
+// snapshot store), run once; its HDF5 datasets are recorded in memory by the
+// recording hdf5.h of this directory (read back through cc_h5rec_*).
+int ref_mhd3d_run_main() {
+    cc_h5rec_clear();
+    return refm3::ref_mhd3d_main();
+}
+
 }  // extern "C"

@@ -4,6 +4,7 @@ reference solvers compiled in place).  Built by `make -C oracle`."""
 from __future__ import annotations
 
 import ctypes as C
+import os
 import subprocess
 from pathlib import Path
 
@@ -14,7 +15,8 @@ from core_collapse_b200 import _lib as L
 ROOT = Path(__file__).resolve().parents[1]
 ORACLE_DIR = ROOT / "oracle"
 REF_DIR = ORACLE_DIR / "_ref"
-REFERENCE_SRC = Path("/root/reference")
+# the reference tree: $CC_REFERENCE_DIR, else a checkout named `reference` beside this repository
+REFERENCE_SRC = Path(os.environ.get("CC_REFERENCE_DIR") or ROOT.parent / "reference")
 
 _DP = C.POINTER(C.c_double)
 _PP = C.POINTER(_DP)

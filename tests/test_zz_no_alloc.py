@@ -62,3 +62,12 @@ def test_noalloc_rejects_grids_beyond_its_scratch():
     assert p.Nx * p.Ny > L.CC_NOALLOC_MAX_CELLS
     t = torch.zeros(8, dtype=torch.float64, device="cuda")
     assert _noalloc(p, t, t, t, torch.cuda.current_stream()) == L.CC_ERR_TOO_LARGE
+
+
+def test_noalloc_rejects_other_solvers_and_precisions():
+    import torch
+    t = torch.zeros(64 * 64, dtype=torch.float64, device="cuda")
+    for kw in ({"poisson": "sor"}, {"poisson": "direct"}, {"poisson": "fft", "precision": "fp32"},
+               {"poisson": "fft", "periodic_x": False}):
+        p = Params(**{"Nx": 64, "Ny": 64, "x0": -1, "x1": 1, "y0": -1, "y1": 1, "precision": "fp64", **kw})
+        assert _noalloc(p, t, t, t, torch.cuda.current_stream()) == L.CC_ERR_UNSUPPORTED, kw
