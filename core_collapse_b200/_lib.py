@@ -42,7 +42,7 @@ class CcMhd2dParams(C.Structure):
         ("G", C.c_double), ("softening", C.c_double),
         ("sor_iters", C.c_int32), ("sor_omega", C.c_double),
         ("sor_tol", C.c_double),
-        ("poisson_kind", C.c_int32), ("precision", C.c_int32), ("reserved", C.c_int32),
+        ("poisson_kind", C.c_int32), ("precision", C.c_int32), ("compensated", C.c_int32),
     ]
 
 

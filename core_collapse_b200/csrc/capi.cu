@@ -58,6 +58,10 @@ template <class T> struct Mhd2d : Mhd2dBase {
     size_t plane = 0;
     void* block = nullptr;
     Fields<T> buf[3];
+    // compensated FP32 state (p.compensated): the rounding residual of every plane of buf[b] in lbuf[b]
+    bool comp = false;
+    void* lblock = nullptr;
+    Fields<T> lbuf[3];
     int cur = 0;
     T* phi = nullptr;
     T* gxa = nullptr;
@@ -95,7 +99,7 @@ template <class T> struct Mhd2d : Mhd2dBase {
 
     ~Mhd2d() override {
         if (graph3) cudaGraphExecDestroy(graph3);
-        void* ptrs[] = {block, phi, gxa, gya, fftA, tw[0], tw[1], tw[2], tw[3], rhs, sphi, scal, spd_part, rho_part,
+        void* ptrs[] = {block, lblock, phi, gxa, gya, fftA, tw[0], tw[1], tw[2], tw[3], rhs, sphi, scal, spd_part, rho_part,
                         diag_part, sor_part, sor_part2, staging, bar, iflags, steps_dev, derived_dev};
         for (void* q : ptrs)
             if (q) cudaFree(q);
@@ -123,12 +127,24 @@ template <class T> struct Mhd2d : Mhd2dBase {
         plane = (size_t)P * (ny + 1);
         CC_CUDA(M2Launch<T>::prepare(nx, ny));
 
+        if (p.compensated && sizeof(T) != 4)
+            return fail(h, CC_ERR_UNSUPPORTED, "the compensated update is an option of the FP32 path");
+        comp = p.compensated != 0;
         CC_CUDA(cudaMalloc(&block, sizeof(T) * plane * 24));
         CC_CUDA(cudaMemsetAsync(block, 0, sizeof(T) * plane * 24, st()));
         for (int b = 0; b < 3; b++) {
             T* base = reinterpret_cast<T*>(block) + (size_t)b * 8 * plane;
             buf[b] = Fields<T>{base, base + plane, base + 2 * plane, base + 3 * plane,
                                base + 4 * plane, base + 5 * plane, base + 6 * plane, base + 7 * plane};
+        }
+        if (comp) {
+            CC_CUDA(cudaMalloc(&lblock, sizeof(T) * plane * 24));
+            CC_CUDA(cudaMemsetAsync(lblock, 0, sizeof(T) * plane * 24, st()));
+            for (int b = 0; b < 3; b++) {
+                T* base = reinterpret_cast<T*>(lblock) + (size_t)b * 8 * plane;
+                lbuf[b] = Fields<T>{base, base + plane, base + 2 * plane, base + 3 * plane,
+                                    base + 4 * plane, base + 5 * plane, base + 6 * plane, base + 7 * plane};
+            }
         }
         CC_CUDA(cudaMalloc(&phi, sizeof(T) * plane));
         CC_CUDA(cudaMemsetAsync(phi, 0, sizeof(T) * plane, st()));
@@ -202,10 +218,14 @@ template <class T> struct Mhd2d : Mhd2dBase {
         const int w[8] = {nx, nx, nx, nx, nx, nx, nx + 1, nx};
         const int hh[8] = {ny, ny, ny, ny, ny, ny, ny, ny + 1};
         T* dst[8] = {buf[cur].rho, buf[cur].mx, buf[cur].my, buf[cur].mz, buf[cur].E, buf[cur].Bz, buf[cur].bx, buf[cur].by};
+        T* ldst[8] = {lbuf[cur].rho, lbuf[cur].mx, lbuf[cur].my, lbuf[cur].mz, lbuf[cur].E, lbuf[cur].Bz, lbuf[cur].bx, lbuf[cur].by};
         for (int k = 0; k < 8; k++) {
             if (!f[k]) return fail(h, CC_ERR_ARG, "null state array");
             CC_CUDA(cudaMemcpyAsync(staging, f[k], sizeof(double) * (size_t)w[k] * hh[k], cudaMemcpyHostToDevice, st()));
-            CC_CUDA(M2Launch<T>::pack_in(staging, dst[k], w[k], hh[k], P, st()));
+            if (comp)
+                CC_CUDA(M2Launch<T>::pack_in_split(staging, dst[k], ldst[k], w[k], hh[k], P, st()));
+            else
+                CC_CUDA(M2Launch<T>::pack_in(staging, dst[k], w[k], hh[k], P, st()));
         }
         loaded = true;
         rho_part_valid = false;
@@ -219,9 +239,13 @@ template <class T> struct Mhd2d : Mhd2dBase {
         const int w[8] = {nx, nx, nx, nx, nx, nx, nx + 1, nx};
         const int hh[8] = {ny, ny, ny, ny, ny, ny, ny, ny + 1};
         const T* src[8] = {buf[cur].rho, buf[cur].mx, buf[cur].my, buf[cur].mz, buf[cur].E, buf[cur].Bz, buf[cur].bx, buf[cur].by};
+        const T* lsrc[8] = {lbuf[cur].rho, lbuf[cur].mx, lbuf[cur].my, lbuf[cur].mz, lbuf[cur].E, lbuf[cur].Bz, lbuf[cur].bx, lbuf[cur].by};
         for (int k = 0; k < 8; k++) {
             if (!f[k]) continue;
-            CC_CUDA(M2Launch<T>::pack_out(src[k], staging, w[k], hh[k], P, st()));
+            if (comp)
+                CC_CUDA(M2Launch<T>::pack_out_sum(src[k], lsrc[k], staging, w[k], hh[k], P, st()));
+            else
+                CC_CUDA(M2Launch<T>::pack_out(src[k], staging, w[k], hh[k], P, st()));
             CC_CUDA(cudaMemcpyAsync(f[k], staging, sizeof(double) * (size_t)w[k] * hh[k], cudaMemcpyDeviceToHost, st()));
         }
         CC_CUDA(cudaStreamSynchronize(st()));
@@ -333,15 +357,19 @@ template <class T> struct Mhd2d : Mhd2dBase {
 
     void count(int n) { h->perf.kernel_launches += n; }
 
-    // one stage-kernel launch, bracketed by CUDA events when profiling
-    int stage(const Fields<T>& in, const Fields<T>& out, bool defer, int gmode, const T* ga, const T* gb) {
+    // one stage-kernel launch from buf[bi] to buf[bo], bracketed by CUDA events when profiling
+    int stage(int bi, int bo, bool defer, int gmode, const T* ga, const T* gb) {
         cudaEvent_t e0 = nullptr, e1 = nullptr;
         if (h->profiling) {
             CC_CUDA(cudaEventCreate(&e0));
             CC_CUDA(cudaEventCreate(&e1));
             CC_CUDA(cudaEventRecord(e0, st()));
         }
-        CC_CUDA(M2Launch<T>::stage(c, in, out, defer, gmode, ga, gb, dt_dev, active(), st()));
+        if (comp)
+            CC_CUDA(M2Launch<T>::stage_comp(c, buf[bi], buf[bo], lbuf[bi], lbuf[bo], defer, gmode, ga, gb, dt_dev,
+                                            active(), st()));
+        else
+            CC_CUDA(M2Launch<T>::stage(c, buf[bi], buf[bo], defer, gmode, ga, gb, dt_dev, active(), st()));
         count(1);
         if (h->profiling) {
             CC_CUDA(cudaEventRecord(e1, st()));
@@ -354,8 +382,7 @@ template <class T> struct Mhd2d : Mhd2dBase {
     int step_body(int gmode1) {
         const int a = cur, b = (cur + 1) % 3, d = (cur + 2) % 3;
         const int g2 = p.gravity_on ? GRAV_PHI : GRAV_NONE;
-        int r = stage(buf[a], buf[b], false, gmode1, gmode1 == GRAV_ARRAYS ? gxa : phi,
-                      gmode1 == GRAV_ARRAYS ? gya : nullptr);
+        int r = stage(a, b, false, gmode1, gmode1 == GRAV_ARRAYS ? gxa : phi, gmode1 == GRAV_ARRAYS ? gya : nullptr);
         if (r) return r;
         if (p.gravity_on) {
             CC_CUDA(M2Launch<T>::rho_sum(c, buf[b].rho, rho_part, st()));
@@ -363,9 +390,13 @@ template <class T> struct Mhd2d : Mhd2dBase {
             r = solve(buf[b].rho);
             if (r) return r;
         }
-        r = stage(buf[b], buf[d], true, g2, phi, nullptr);
+        r = stage(b, d, true, g2, phi, nullptr);
         if (r) return r;
-        CC_CUDA(M2Launch<T>::average(c, buf[a], buf[d], buf[b], dt_dev, active(), spd_part, rho_part, st()));
+        if (comp)
+            CC_CUDA(M2Launch<T>::average_comp(c, buf[a], buf[d], buf[b], lbuf[a], lbuf[d], lbuf[b], dt_dev, active(),
+                                              spd_part, rho_part, st()));
+        else
+            CC_CUDA(M2Launch<T>::average(c, buf[a], buf[d], buf[b], dt_dev, active(), spd_part, rho_part, st()));
         count(1);
         h->perf.steps += 1;
         cur = b;

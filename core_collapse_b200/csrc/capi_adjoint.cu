@@ -427,6 +427,7 @@ int cc_adjoint_create(const cc_mhd2d_params* p, int checkpoint_every, int max_st
     std::string why;
     int code = CC_OK;
     if (p->precision != CC_FP64) { code = CC_ERR_UNSUPPORTED; why = "the adjoint runs in FP64"; }
+    else if (p->compensated) { code = CC_ERR_UNSUPPORTED; why = "the adjoint has no compensated update"; }
     else if (checkpoint_every < 1 || max_steps < 1) { code = CC_ERR_ARG; why = "checkpoint_every and max_steps must be >= 1"; }
     else if (p->Nx < 4 || p->Ny < 4 || !(p->x1 > p->x0) || !(p->y1 > p->y0)) { code = CC_ERR_ARG; why = "bad grid"; }
     else if (p->gravity_on && p->poisson_kind != CC_POISSON_DIRECT) {

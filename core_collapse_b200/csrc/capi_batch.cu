@@ -47,6 +47,7 @@ int cc_batch_create(const cc_mhd2d_params* params, int n, cc_handle** out) {
         else if (q.Nx < 4 || q.Ny < 4) { code = CC_ERR_ARG; where += "Nx and Ny must be >= 4"; }
         else if (q.Nx > 65535 * 16 || q.Ny > 65535 * 8) { code = CC_ERR_ARG; where += "grid too large"; }
         else if (!(q.x1 > q.x0) || !(q.y1 > q.y0)) { code = CC_ERR_ARG; where += "empty domain"; }
+        else if (q.compensated) { code = CC_ERR_UNSUPPORTED; where += "the ensemble has no compensated update"; }
         else if (q.gravity_on && q.poisson_kind != CC_POISSON_DIRECT) {
             code = CC_ERR_UNSUPPORTED;
             where += "instances with gravity need poisson_kind == CC_POISSON_DIRECT";

@@ -38,6 +38,15 @@ cudaError_t M2Launch<T>::prepare(int nx, int ny) {
     CC_ATTR((m2_stage_kernel<T, true, GRAV_ARRAYS>), smem)
     CC_ATTR((m2_stage_kernel<T, true, GRAV_PHI>), smem)
     if constexpr (sizeof(T) == 4) {
+        const int smem_c = smem + (int)kahan_smem_extra<T>(StageGeom<T>::NC);
+        CC_ATTR((m2_stage_comp_kernel<T, false, GRAV_NONE>), smem_c)
+        CC_ATTR((m2_stage_comp_kernel<T, false, GRAV_ARRAYS>), smem_c)
+        CC_ATTR((m2_stage_comp_kernel<T, false, GRAV_PHI>), smem_c)
+        CC_ATTR((m2_stage_comp_kernel<T, true, GRAV_NONE>), smem_c)
+        CC_ATTR((m2_stage_comp_kernel<T, true, GRAV_ARRAYS>), smem_c)
+        CC_ATTR((m2_stage_comp_kernel<T, true, GRAV_PHI>), smem_c)
+    }
+    if constexpr (sizeof(T) == 4) {
         if (nx >= 2 && ny >= 2) {
             const int row = (int)(sizeof(float2) * (size_t)fft32_line(nx));
             const int col = (int)(sizeof(float2) * (size_t)fft32_line(ny)) * fft32_cw(ny);
@@ -94,6 +103,46 @@ cudaError_t M2Launch<T>::average(const M2Const<T>& c, const Fields<T>& un, const
 }
 
 template <class T>
+cudaError_t M2Launch<T>::stage_comp(const M2Const<T>& c, const Fields<T>& in, const Fields<T>& out,
+                                    const Fields<T>& lin, const Fields<T>& lout, bool defer, int gmode, const T* ga,
+                                    const T* gb, const double* dt, const int* active, cudaStream_t s) {
+    if constexpr (sizeof(T) != 4) {
+        return cudaErrorNotSupported;
+    } else {
+        using Gm = StageGeom<T>;
+        const size_t smem = m2_stage_smem<T>() + kahan_smem_extra<T>(Gm::NC);
+        dim3 grid((c.nx + Gm::TX - 1) / Gm::TX, (c.ny + Gm::TY - 1) / Gm::TY);
+#define CC_STAGE_CASE(D, G)                                                                                  \
+        if (defer == D && gmode == G) {                                                                      \
+            m2_stage_comp_kernel<T, D, G><<<grid, Gm::NT, smem, s>>>(c, in, out, lin, lout, ga, gb, dt, active); \
+            return cudaGetLastError();                                                                       \
+        }
+        CC_STAGE_CASE(false, GRAV_NONE)
+        CC_STAGE_CASE(false, GRAV_ARRAYS)
+        CC_STAGE_CASE(false, GRAV_PHI)
+        CC_STAGE_CASE(true, GRAV_NONE)
+        CC_STAGE_CASE(true, GRAV_ARRAYS)
+        CC_STAGE_CASE(true, GRAV_PHI)
+#undef CC_STAGE_CASE
+        return cudaErrorInvalidValue;
+    }
+}
+
+template <class T>
+cudaError_t M2Launch<T>::average_comp(const M2Const<T>& c, const Fields<T>& un, const Fields<T>& s2,
+                                      const Fields<T>& out, const Fields<T>& unl, const Fields<T>& s2l,
+                                      const Fields<T>& outl, const double* dt, const int* active, double* spd_part,
+                                      double* rho_part, cudaStream_t s) {
+    if constexpr (sizeof(T) != 4) {
+        return cudaErrorNotSupported;
+    } else {
+        m2_average_comp_kernel<T, RED_NT><<<RED_BLOCKS, RED_NT, 0, s>>>(c, un, s2, out, unl, s2l, outl, dt, active,
+                                                                       spd_part, rho_part);
+        return cudaGetLastError();
+    }
+}
+
+template <class T>
 cudaError_t M2Launch<T>::speeds(const M2Const<T>& c, const Fields<T>& st, double* spd_part, double* rho_part,
                                 cudaStream_t s) {
     m2_speed_kernel<T, RED_NT><<<RED_BLOCKS, RED_NT, 0, s>>>(c, st, spd_part, rho_part);
@@ -134,6 +183,19 @@ cudaError_t M2Launch<T>::pack_in(const double* src, T* dst, int w, int h, int pi
 template <class T>
 cudaError_t M2Launch<T>::pack_out(const T* src, double* dst, int w, int h, int pitch, cudaStream_t s) {
     pack_out_kernel<T><<<pack_grid(w, h), 256, 0, s>>>(src, dst, w, h, pitch);
+    return cudaGetLastError();
+}
+
+template <class T>
+cudaError_t M2Launch<T>::pack_in_split(const double* src, T* hi, T* lo, int w, int h, int pitch, cudaStream_t s) {
+    pack_in_split_kernel<T><<<pack_grid(w, h), 256, 0, s>>>(src, hi, lo, w, h, pitch);
+    return cudaGetLastError();
+}
+
+template <class T>
+cudaError_t M2Launch<T>::pack_out_sum(const T* hi, const T* lo, double* dst, int w, int h, int pitch,
+                                      cudaStream_t s) {
+    pack_out_sum_kernel<T><<<pack_grid(w, h), 256, 0, s>>>(hi, lo, dst, w, h, pitch);
     return cudaGetLastError();
 }
 

@@ -76,14 +76,14 @@ template <class T> constexpr size_t m2_stage_smem() { return StageGeom<T>::smem;
 // (add_joule_heating_and_Bz_resistive, M2:631-686), applied to the stored
 // pre-Joule state s at cell (i,j); the cell's own values are passed in and
 // E, Bz, rho are updated.  Bx, By are the cell-centred stage-output B.
+// |J|^2 and the 5-point Laplacian of Bz of cell (i,j) of the stored state s,
+// whose own Bz is bzC (M2:640-668)
 template <class T>
-__device__ __forceinline__ void joule_cell(const M2Const<T>& c, const Fields<T>& s, int i, int j, T dt,
-                                           T& rho, T mx, T my, T mz, T& E, T& Bz, T Bx, T By) {
-    if (!c.resistive) return;
+__device__ __forceinline__ void joule_terms(const M2Const<T>& c, const Fields<T>& s, int i, int j, T bzC, T& J2,
+                                            T& lap) {
     const int P = c.pitch;
     const int iE = c.ax.cell(i + 1), iW = c.ax.cell(i - 1);
     const int jN = c.ay.cell(j + 1), jS = c.ay.cell(j - 1);
-    const T bzC = Bz;
     const T bzE = s.Bz[(size_t)j * P + iE], bzW = s.Bz[(size_t)j * P + iW];
     const T bzN = s.Bz[(size_t)jN * P + i], bzS = s.Bz[(size_t)jS * P + i];
     const T dBzdy = div_or_mul(bzN - bzS, c.two_dy, T(0.5) * c.inv_dy);
@@ -91,11 +91,74 @@ __device__ __forceinline__ void joule_cell(const M2Const<T>& c, const Fields<T>&
     const T dBydx = div_or_mul(s.by[(size_t)j * P + iE] - s.by[(size_t)j * P + i], c.dx, c.inv_dx);
     const T dBxdy = div_or_mul(s.bx[(size_t)jN * P + i] - s.bx[(size_t)j * P + i], c.dy, c.inv_dy);
     const T Jx = dBzdy, Jy = -dBzdx, Jz = dBydx - dBxdy;
-    const T J2 = Jx * Jx + Jy * Jy + Jz * Jz;
+    J2 = Jx * Jx + Jy * Jy + Jz * Jz;
+    lap = (bzE - T(2) * bzC + bzW) * c.idx2 + (bzN - T(2) * bzC + bzS) * c.idy2;
+}
+
+template <class T>
+__device__ __forceinline__ void joule_cell(const M2Const<T>& c, const Fields<T>& s, int i, int j, T dt,
+                                           T& rho, T mx, T my, T mz, T& E, T& Bz, T Bx, T By) {
+    if (!c.resistive) return;
+    const T bzC = Bz;
+    T J2, lap;
+    joule_terms(c, s, i, j, bzC, J2, lap);
     E = E + dt * c.eta * J2;
-    const T lap = (bzE - T(2) * bzC + bzW) * c.idx2 + (bzN - T(2) * bzC + bzS) * c.idy2;
     Bz = bzC + dt * c.eta * lap;
     floors(c, rho, mx, my, mz, E, Bx, By, Bz);
+}
+
+// ---------------------------------------------------------------------------
+// Compensated (Kahan-style) accumulation of the conserved update, FP32 path.
+// A compensated state stores every field as a pair (h, l): h the FP32 value
+// the physics reads, l the rounding residual of h (|l| <= ulp(h)/2), so that
+// h + l carries about twice FP32's digits between steps.  Every increment of
+// a stage (flux divergence, CT, gravity kick, Joule heating and Bz diffusion)
+// and the RK average are added with an error-free transformation (Knuth's
+// TwoSum), which moves the rounding error of each addition into l instead of
+// dropping it.  A floor that resets a value also resets its residual.
+// ---------------------------------------------------------------------------
+template <class T> __device__ __forceinline__ void comp_add(T& h, T& l, const T inc) {
+    const T y = inc + l;
+    const T s = h + y;
+    const T bb = s - h;
+    l = (h - (s - bb)) + (y - bb);
+    h = s;
+}
+
+// (h, l) = 0.5 * ((ha + la) + (hb + lb)), compensated
+template <class T>
+__device__ __forceinline__ void comp_avg(const T ha, const T la, const T hb, const T lb, T& h, T& l) {
+    const T s = ha + hb;
+    const T bb = s - ha;
+    T e = (ha - (s - bb)) + (hb - bb);
+    e = e + (la + lb);
+    const T r = s + e;            // fast two-sum: |s| >= |e|
+    const T er = e - (r - s);
+    h = T(0.5) * r;
+    l = T(0.5) * er;
+}
+
+// enforce_floors on a compensated cell: a reset value starts a fresh residual
+template <class T>
+__device__ __forceinline__ void floors_comp(const M2Const<T>& c, T& rho, T& lrho, T mx, T my, T mz, T& E, T& lE,
+                                            T Bx, T By, T Bz) {
+    const T r0 = rho, e0 = E;
+    floors(c, rho, mx, my, mz, E, Bx, By, Bz);
+    if (rho != r0) lrho = T(0.0);
+    if (E != e0) lE = T(0.0);
+}
+
+// joule_cell on a compensated cell: the increments of E and Bz go through comp_add
+template <class T>
+__device__ __forceinline__ void joule_cell_comp(const M2Const<T>& c, const Fields<T>& s, int i, int j, T dt,
+                                                T& rho, T& lrho, T mx, T my, T mz, T& E, T& lE, T& Bz, T& lBz,
+                                                T Bx, T By) {
+    if (!c.resistive) return;
+    T J2, lap;
+    joule_terms(c, s, i, j, Bz, J2, lap);
+    comp_add(E, lE, dt * c.eta * J2);
+    comp_add(Bz, lBz, dt * c.eta * lap);
+    floors_comp(c, rho, lrho, mx, my, mz, E, lE, Bx, By, Bz);
 }
 
 // ---------------------------------------------------------------------------
@@ -109,11 +172,17 @@ __device__ __forceinline__ void joule_cell(const M2Const<T>& c, const Fields<T>&
 // E, Bz into rec[0..5], pitched like the state): the record the discrete
 // adjoint replays the floor and gravity-kick branches from.  NT_: threads of
 // the CTA (at least TX * TY); SPLIT_ as in StageGeomT.
+// KAHAN: compensated state (see comp_add): lin / lout hold the residuals of
+// in / out; the tile's own cells read theirs and every increment is added
+// with comp_add.  The physics (primitives, slopes, fluxes, EMFs) reads the
+// FP32 values only, computed exactly as without KAHAN, so neighbouring tiles
+// see identical primitives.  Needs kahan_smem_extra<T>(TX*TY) more bytes.
 template <class T, int TX_, int TY_, bool DEFER, int GMODE, bool REC = false, int NT_ = TX_ * TY_,
-          bool SPLIT_ = false>
+          bool SPLIT_ = false, bool KAHAN = false>
 __device__ __forceinline__ void m2_stage_tile(const M2Const<T>& c, const Fields<T>& in, const Fields<T>& out,
                                               const T* __restrict__ ga, const T* __restrict__ gb, const T dt,
-                                              const int i0, const int j0, T* sm, T* const* rec = nullptr) {
+                                              const int i0, const int j0, T* sm, T* const* rec = nullptr,
+                                              const Fields<T> lin = Fields<T>{}, const Fields<T> lout = Fields<T>{}) {
     using G = StageGeomT<T, TX_, TY_, NT_, SPLIT_>;
     constexpr int TX = G::TX, TY = G::TY, HALO = G::HALO, RX = G::RX, RR = G::RR, NT = G::NT, NC = G::NC;
     constexpr int NFX = G::NFX, NGY = G::NGY, NSL = G::NSL;
@@ -125,6 +194,7 @@ __device__ __forceinline__ void m2_stage_tile(const M2Const<T>& c, const Fields<
     T* gy = fx + 7 * NFX;       // 7 planes of NGY
     T* ez = gy + 7 * NGY;       // NE
     T* own = ez + G::NE;        // 6 planes of NC
+    T* own_lo = own + 6 * NC;   // KAHAN: 6 planes of NC, the residuals of own
 
     const int tid = threadIdx.x;
     const int P = c.pitch;
@@ -138,12 +208,25 @@ __device__ __forceinline__ void m2_stage_tile(const M2Const<T>& c, const Fields<
         T rho = in.rho[q], mx = in.mx[q], my = in.my[q], mz = in.mz[q], E = in.E[q], Bz = in.Bz[q];
         const T Bx = T(0.5) * (in.bx[q] + in.bx[q + 1]);
         const T By = T(0.5) * (in.by[q] + in.by[q + P]);
+        const int ox = rx - HALO, oy = ry - HALO;
+        const bool mine = ox >= 0 && ox < TX && oy >= 0 && oy < TY;
+        if constexpr (KAHAN) {
+            if (mine) {   // the compensated pair of the tile's own cell, Joule sub-step included
+                T h0 = rho, h4 = E, h5 = Bz;
+                T l0 = lin.rho[q], l4 = lin.E[q], l5 = lin.Bz[q];
+                if (DEFER) joule_cell_comp(c, in, ci, cj, dt, h0, l0, mx, my, mz, h4, l4, h5, l5, Bx, By);
+                const int o = oy * TX + ox;
+                own[o] = h0; own[NC + o] = mx; own[2 * NC + o] = my;
+                own[3 * NC + o] = mz; own[4 * NC + o] = h4; own[5 * NC + o] = h5;
+                own_lo[o] = l0; own_lo[NC + o] = lin.mx[q]; own_lo[2 * NC + o] = lin.my[q];
+                own_lo[3 * NC + o] = lin.mz[q]; own_lo[4 * NC + o] = l4; own_lo[5 * NC + o] = l5;
+            }
+        }
         if (DEFER) joule_cell(c, in, ci, cj, dt, rho, mx, my, mz, E, Bz, Bx, By);
         const Prim<T> W = to_prim(c, rho, mx, my, mz, E, Bx, By, Bz);
         s_r[k] = W.r; s_u[k] = W.u; s_v[k] = W.v; s_w[k] = W.w;
         s_P[k] = W.P; s_bx[k] = W.bx; s_by[k] = W.by; s_bz[k] = W.bz;
-        const int ox = rx - HALO, oy = ry - HALO;
-        if (ox >= 0 && ox < TX && oy >= 0 && oy < TY) {
+        if (!KAHAN && mine) {
             const int o = oy * TX + ox;
             own[o] = rho; own[NC + o] = mx; own[2 * NC + o] = my;
             own[3 * NC + o] = mz; own[4 * NC + o] = E; own[5 * NC + o] = Bz;
@@ -274,6 +357,11 @@ __device__ __forceinline__ void m2_stage_tile(const M2Const<T>& c, const Fields<
     const int o = ty * TX + tx;
     T rho = own[o], mx = own[NC + o], my = own[2 * NC + o];
     T mz = own[3 * NC + o], E = own[4 * NC + o], Bz = own[5 * NC + o];
+    T lrho = T(0.0), lmx = T(0.0), lmy = T(0.0), lmz = T(0.0), lE = T(0.0), lBz = T(0.0);
+    if constexpr (KAHAN) {
+        lrho = own_lo[o]; lmx = own_lo[NC + o]; lmy = own_lo[2 * NC + o];
+        lmz = own_lo[3 * NC + o]; lE = own_lo[4 * NC + o]; lBz = own_lo[5 * NC + o];
+    }
     {
         const int kxL = (ty + 1) * (TX + 1) + tx;
         const int kgD = ty * (TX + 2) + tx + 1, kgU = kgD + (TX + 2);
@@ -282,26 +370,50 @@ __device__ __forceinline__ void m2_stage_tile(const M2Const<T>& c, const Fields<
         for (int m = 0; m < 7; m++)
             d[m] = -(fx[m * NFX + kxL + 1] - fx[m * NFX + kxL]) * c.inv_dx -
                    (gy[m * NGY + kgU] - gy[m * NGY + kgD]) * c.inv_dy;
-        rho += dt * d[0];
-        mx += dt * d[1];
-        my += dt * d[2];
-        mz += dt * d[3];
-        E += dt * d[4];
-        Bz += dt * d[6];
-        if (REC) {
-            rec[0][q] = rho; rec[1][q] = mx; rec[2][q] = my; rec[3][q] = mz; rec[4][q] = E; rec[5][q] = Bz;
-        }
         const int kc = ridx(tx, ty);
-        floors(c, rho, mx, my, mz, E, s_bx[kc], s_by[kc], Bz);
+        if constexpr (KAHAN) {
+            comp_add(rho, lrho, dt * d[0]);
+            comp_add(mx, lmx, dt * d[1]);
+            comp_add(my, lmy, dt * d[2]);
+            comp_add(mz, lmz, dt * d[3]);
+            comp_add(E, lE, dt * d[4]);
+            comp_add(Bz, lBz, dt * d[6]);
+            floors_comp(c, rho, lrho, mx, my, mz, E, lE, s_bx[kc], s_by[kc], Bz);
+        } else {
+            rho += dt * d[0];
+            mx += dt * d[1];
+            my += dt * d[2];
+            mz += dt * d[3];
+            E += dt * d[4];
+            Bz += dt * d[6];
+            if (REC) {
+                rec[0][q] = rho; rec[1][q] = mx; rec[2][q] = my; rec[3][q] = mz; rec[4][q] = E; rec[5][q] = Bz;
+            }
+            floors(c, rho, mx, my, mz, E, s_bx[kc], s_by[kc], Bz);
+        }
     }
     // CT (M2:807-830) for this cell's four faces
     const T dtdy = dt / c.dy, dtdx = dt / c.dx;
     const T e00 = ez[ty * (TX + 1) + tx], e10 = ez[ty * (TX + 1) + tx + 1];
     const T e01 = ez[(ty + 1) * (TX + 1) + tx], e11 = ez[(ty + 1) * (TX + 1) + tx + 1];
-    const T bxL = in.bx[q] + -(dtdy) * (e01 - e00);
-    const T bxR = in.bx[q + 1] + -(dtdy) * (e11 - e10);
-    const T byD = in.by[q] + +(dtdx) * (e10 - e00);
-    const T byU = in.by[q + P] + +(dtdx) * (e11 - e01);
+    T bxL, bxR, byD, byU;
+    if constexpr (KAHAN) {
+        T l0 = lin.bx[q], l1 = lin.bx[q + 1], l2 = lin.by[q], l3 = lin.by[q + P];
+        bxL = in.bx[q]; bxR = in.bx[q + 1]; byD = in.by[q]; byU = in.by[q + P];
+        comp_add(bxL, l0, -(dtdy) * (e01 - e00));
+        comp_add(bxR, l1, -(dtdy) * (e11 - e10));
+        comp_add(byD, l2, +(dtdx) * (e10 - e00));
+        comp_add(byU, l3, +(dtdx) * (e11 - e01));
+        lout.bx[q] = l0;
+        if (gi == c.nx - 1) lout.bx[q + 1] = l1;
+        lout.by[q] = l2;
+        if (gj == c.ny - 1) lout.by[q + P] = l3;
+    } else {
+        bxL = in.bx[q] + -(dtdy) * (e01 - e00);
+        bxR = in.bx[q + 1] + -(dtdy) * (e11 - e10);
+        byD = in.by[q] + +(dtdx) * (e10 - e00);
+        byU = in.by[q + P] + +(dtdx) * (e11 - e01);
+    }
     out.bx[q] = bxL;
     if (gi == c.nx - 1) out.bx[q + 1] = bxR;
     out.by[q] = byD;
@@ -327,13 +439,26 @@ __device__ __forceinline__ void m2_stage_tile(const M2Const<T>& c, const Fields<
             u = mx / vmax(rho, T(1e-300));
             v = my / vmax(rho, T(1e-300));
         }
-        mx += dt * rho * gxq;
-        my += dt * rho * gyq;
-        E += dt * rho * (u * gxq + v * gyq);
-        floors(c, rho, mx, my, mz, E, T(0.5) * (bxL + bxR), T(0.5) * (byD + byU), Bz);
+        if constexpr (KAHAN) {
+            comp_add(mx, lmx, dt * rho * gxq);
+            comp_add(my, lmy, dt * rho * gyq);
+            comp_add(E, lE, dt * rho * (u * gxq + v * gyq));
+            floors_comp(c, rho, lrho, mx, my, mz, E, lE, T(0.5) * (bxL + bxR), T(0.5) * (byD + byU), Bz);
+        } else {
+            mx += dt * rho * gxq;
+            my += dt * rho * gyq;
+            E += dt * rho * (u * gxq + v * gyq);
+            floors(c, rho, mx, my, mz, E, T(0.5) * (bxL + bxR), T(0.5) * (byD + byU), Bz);
+        }
     }
     out.rho[q] = rho; out.mx[q] = mx; out.my[q] = my; out.mz[q] = mz; out.E[q] = E; out.Bz[q] = Bz;
+    if constexpr (KAHAN) {
+        lout.rho[q] = lrho; lout.mx[q] = lmx; lout.my[q] = lmy; lout.mz[q] = lmz; lout.E[q] = lE; lout.Bz[q] = lBz;
+    }
 }
+
+// extra shared memory of a KAHAN stage tile of nc cells (the residuals of its own cells)
+template <class T> constexpr size_t kahan_smem_extra(int nc) { return sizeof(T) * 6 * (size_t)nc; }
 
 template <class T, bool DEFER, int GMODE>
 __global__ void __launch_bounds__(StageGeom<T>::NT, StageTile<T>::MINB)
@@ -344,6 +469,20 @@ m2_stage_kernel(const M2Const<T> c, const Fields<T> in, const Fields<T> out, con
     extern __shared__ __align__(16) unsigned char smem_raw[];
     m2_stage_tile<T, TX, TY, DEFER, GMODE, false, StageTile<T>::NT, StageTile<T>::SPLIT>(
         c, in, out, ga, gb, (T)(*dtp), blockIdx.x * TX, blockIdx.y * TY, reinterpret_cast<T*>(smem_raw));
+}
+
+// the same stage on a compensated state (lin / lout: residuals of in / out)
+template <class T, bool DEFER, int GMODE>
+__global__ void __launch_bounds__(StageGeom<T>::NT, StageTile<T>::MINB)
+m2_stage_comp_kernel(const M2Const<T> c, const Fields<T> in, const Fields<T> out, const Fields<T> lin,
+                     const Fields<T> lout, const T* __restrict__ ga, const T* __restrict__ gb,
+                     const double* __restrict__ dtp, const int* __restrict__ active) {
+    constexpr int TX = StageTile<T>::TX, TY = StageTile<T>::TY;
+    if (active && *active == 0) return;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    m2_stage_tile<T, TX, TY, DEFER, GMODE, false, StageTile<T>::NT, StageTile<T>::SPLIT, true>(
+        c, in, out, ga, gb, (T)(*dtp), blockIdx.x * TX, blockIdx.y * TY, reinterpret_cast<T*>(smem_raw), nullptr,
+        lin, lout);
 }
 
 // ---------------------------------------------------------------------------
@@ -395,6 +534,62 @@ __device__ __forceinline__ double average_cell(const M2Const<T>& c, const Fields
     return (double)vmax(sx, sy);
 }
 
+// average_cell on compensated states: unl, s2l, outl hold the residuals of
+// un, s2, out.  The Joule increments of stage 2 and the average go through
+// comp_add / comp_avg; floors reset the residual of a value they reset.
+template <class T>
+__device__ __forceinline__ double average_cell_comp(const M2Const<T>& c, const Fields<T>& un, const Fields<T>& s2,
+                                                    const Fields<T>& out, const Fields<T>& unl,
+                                                    const Fields<T>& s2l, const Fields<T>& outl, const T dt,
+                                                    const bool act, const int i, const int j, double& rsum) {
+    const int P = c.pitch;
+    const size_t q = (size_t)j * P + i;
+    if (!act) {
+        T* dst[8] = {out.rho, out.mx, out.my, out.mz, out.E, out.Bz, out.bx, out.by};
+        T* dstl[8] = {outl.rho, outl.mx, outl.my, outl.mz, outl.E, outl.Bz, outl.bx, outl.by};
+        const T* src[8] = {un.rho, un.mx, un.my, un.mz, un.E, un.Bz, un.bx, un.by};
+        const T* srcl[8] = {unl.rho, unl.mx, unl.my, unl.mz, unl.E, unl.Bz, unl.bx, unl.by};
+#pragma unroll
+        for (int m = 0; m < 8; m++) { dst[m][q] = src[m][q]; dstl[m][q] = srcl[m][q]; }
+        if (i == c.nx - 1) { out.bx[q + 1] = un.bx[q + 1]; outl.bx[q + 1] = unl.bx[q + 1]; }
+        if (j == c.ny - 1) { out.by[q + P] = un.by[q + P]; outl.by[q + P] = unl.by[q + P]; }
+        const T bxl = un.bx[q], bxr = un.bx[q + 1], byd = un.by[q], byu = un.by[q + P];
+        const Prim<T> W = to_prim(c, un.rho[q], un.mx[q], un.my[q], un.mz[q], un.E[q], T(0.5) * (bxl + bxr),
+                                  T(0.5) * (byd + byu), un.Bz[q]);
+        rsum += (double)un.rho[q];
+        return (double)vmax(fabs(W.u) + fast_speed(c, W, W.bx), fabs(W.v) + fast_speed(c, W, W.by));
+    }
+    T rho = s2.rho[q], mx = s2.mx[q], my = s2.my[q], mz = s2.mz[q], E = s2.E[q], Bz = s2.Bz[q];
+    T lrho = s2l.rho[q], lmx = s2l.mx[q], lmy = s2l.my[q], lmz = s2l.mz[q], lE = s2l.E[q], lBz = s2l.Bz[q];
+    const T bxl2 = s2.bx[q], bxr2 = s2.bx[q + 1], byd2 = s2.by[q], byu2 = s2.by[q + P];
+    joule_cell_comp(c, s2, i, j, dt, rho, lrho, mx, my, mz, E, lE, Bz, lBz, T(0.5) * (bxl2 + bxr2),
+                    T(0.5) * (byd2 + byu2));
+    comp_avg(un.rho[q], unl.rho[q], rho, lrho, rho, lrho);
+    comp_avg(un.mx[q], unl.mx[q], mx, lmx, mx, lmx);
+    comp_avg(un.my[q], unl.my[q], my, lmy, my, lmy);
+    comp_avg(un.mz[q], unl.mz[q], mz, lmz, mz, lmz);
+    comp_avg(un.E[q], unl.E[q], E, lE, E, lE);
+    comp_avg(un.Bz[q], unl.Bz[q], Bz, lBz, Bz, lBz);
+    T bxl, bxr, byd, byu, lbxl, lbxr, lbyd, lbyu;
+    comp_avg(un.bx[q], unl.bx[q], bxl2, s2l.bx[q], bxl, lbxl);
+    comp_avg(un.bx[q + 1], unl.bx[q + 1], bxr2, s2l.bx[q + 1], bxr, lbxr);
+    comp_avg(un.by[q], unl.by[q], byd2, s2l.by[q], byd, lbyd);
+    comp_avg(un.by[q + P], unl.by[q + P], byu2, s2l.by[q + P], byu, lbyu);
+    const T Bx = T(0.5) * (bxl + bxr), By = T(0.5) * (byd + byu);
+    floors_comp(c, rho, lrho, mx, my, mz, E, lE, Bx, By, Bz);
+    out.rho[q] = rho; out.mx[q] = mx; out.my[q] = my; out.mz[q] = mz; out.E[q] = E; out.Bz[q] = Bz;
+    outl.rho[q] = lrho; outl.mx[q] = lmx; outl.my[q] = lmy; outl.mz[q] = lmz; outl.E[q] = lE; outl.Bz[q] = lBz;
+    out.bx[q] = bxl; outl.bx[q] = lbxl;
+    if (i == c.nx - 1) { out.bx[q + 1] = bxr; outl.bx[q + 1] = lbxr; }
+    out.by[q] = byd; outl.by[q] = lbyd;
+    if (j == c.ny - 1) { out.by[q + P] = byu; outl.by[q + P] = lbyu; }
+    const Prim<T> W = to_prim(c, rho, mx, my, mz, E, Bx, By, Bz);
+    const T sx = fabs(W.u) + fast_speed(c, W, W.bx);
+    const T sy = fabs(W.v) + fast_speed(c, W, W.by);
+    rsum += (double)rho;
+    return (double)vmax(sx, sy);
+}
+
 // CFL speed of one cell of a state (compute_dt's loop body, M2:585-587)
 template <class T>
 __device__ __forceinline__ double speed_cell(const M2Const<T>& c, const Fields<T>& s, const int i, const int j) {
@@ -421,6 +616,27 @@ m2_average_kernel(const M2Const<T> c, const Fields<T> un, const Fields<T> s2, co
     for (int k = blockIdx.x * NT + threadIdx.x; k < ncell; k += gridDim.x * NT) {
         const double s = average_cell(c, un, s2, out, dt, act, k % c.nx, k / c.nx, rsum);
         if (s > smax) smax = s;   // NaN never wins, as in std::max(maxs, x)
+    }
+    const double bm = block_max<NT>(smax, sh);
+    const double bs = block_sum<NT>(rsum, sh);
+    if (threadIdx.x == 0) { spd_part[blockIdx.x] = bm; rho_part[blockIdx.x] = bs; }
+}
+
+// m2_average_kernel on compensated states
+template <class T, int NT>
+__global__ void __launch_bounds__(NT)
+m2_average_comp_kernel(const M2Const<T> c, const Fields<T> un, const Fields<T> s2, const Fields<T> out,
+                       const Fields<T> unl, const Fields<T> s2l, const Fields<T> outl,
+                       const double* __restrict__ dtp, const int* __restrict__ active,
+                       double* __restrict__ spd_part, double* __restrict__ rho_part) {
+    const bool act = (active == nullptr) || (*active != 0);
+    __shared__ double sh[NT / 32];
+    const T dt = (T)(*dtp);
+    double smax = 0.0, rsum = 0.0;
+    const int ncell = c.nx * c.ny;
+    for (int k = blockIdx.x * NT + threadIdx.x; k < ncell; k += gridDim.x * NT) {
+        const double s = average_cell_comp(c, un, s2, out, unl, s2l, outl, dt, act, k % c.nx, k / c.nx, rsum);
+        if (s > smax) smax = s;
     }
     const double bm = block_max<NT>(smax, sh);
     const double bs = block_sum<NT>(rsum, sh);
@@ -554,6 +770,26 @@ __global__ void pack_out_kernel(const T* __restrict__ src, double* __restrict__ 
     for (int j = blockIdx.y; j < h; j += gridDim.y)
         for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < w; i += gridDim.x * blockDim.x)
             dst[(size_t)j * w + i] = (double)src[(size_t)j * pitch + i];
+}
+// compensated state: hi = the FP64 value rounded to T, lo = the rounding residual (in T)
+template <class T>
+__global__ void pack_in_split_kernel(const double* __restrict__ src, T* __restrict__ hi, T* __restrict__ lo, int w,
+                                     int h, int pitch) {
+    for (int j = blockIdx.y; j < h; j += gridDim.y)
+        for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < w; i += gridDim.x * blockDim.x) {
+            const double v = src[(size_t)j * w + i];
+            const T a = (T)v;
+            hi[(size_t)j * pitch + i] = a;
+            lo[(size_t)j * pitch + i] = (T)(v - (double)a);
+        }
+}
+// compensated state -> FP64: hi + lo (exact in FP64 for FP32 pairs)
+template <class T>
+__global__ void pack_out_sum_kernel(const T* __restrict__ hi, const T* __restrict__ lo, double* __restrict__ dst,
+                                    int w, int h, int pitch) {
+    for (int j = blockIdx.y; j < h; j += gridDim.y)
+        for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < w; i += gridDim.x * blockDim.x)
+            dst[(size_t)j * w + i] = (double)hi[(size_t)j * pitch + i] + (double)lo[(size_t)j * pitch + i];
 }
 
 }  // namespace ccb

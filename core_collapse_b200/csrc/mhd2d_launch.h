@@ -21,6 +21,16 @@ template <class T> struct M2Launch {
     static cudaError_t average(const M2Const<T>& c, const Fields<T>& un, const Fields<T>& s2, const Fields<T>& out,
                                const double* dt, const int* active, double* spd_part, double* rho_part,
                                cudaStream_t s);
+    // the same two kernels on compensated states (FP32 only; l*: the residual planes)
+    static cudaError_t stage_comp(const M2Const<T>& c, const Fields<T>& in, const Fields<T>& out,
+                                  const Fields<T>& lin, const Fields<T>& lout, bool defer, int gmode, const T* ga,
+                                  const T* gb, const double* dt, const int* active, cudaStream_t s);
+    static cudaError_t average_comp(const M2Const<T>& c, const Fields<T>& un, const Fields<T>& s2,
+                                    const Fields<T>& out, const Fields<T>& unl, const Fields<T>& s2l,
+                                    const Fields<T>& outl, const double* dt, const int* active, double* spd_part,
+                                    double* rho_part, cudaStream_t s);
+    static cudaError_t pack_in_split(const double* src, T* hi, T* lo, int w, int h, int pitch, cudaStream_t s);
+    static cudaError_t pack_out_sum(const T* hi, const T* lo, double* dst, int w, int h, int pitch, cudaStream_t s);
     static cudaError_t speeds(const M2Const<T>& c, const Fields<T>& st, double* spd_part, double* rho_part,
                               cudaStream_t s);
     static cudaError_t rho_sum(const M2Const<T>& c, const T* rho, double* rho_part, cudaStream_t s);

@@ -47,6 +47,7 @@ class Params:
     sor_tol: float = 0.0            # > 0: stop SOR once max|lap(phi)-rhs| < sor_tol
     poisson: str = "sor"            # "sor" (red-black), "fft", or "direct" (batched ensemble only)
     precision: str = "fp64"         # "fp64" or "fp32"
+    compensated: bool = False       # FP32 only: compensated (Kahan-style) state update
 
     def to_c(self) -> L.CcMhd2dParams:
         c = L.CcMhd2dParams()

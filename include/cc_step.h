@@ -84,7 +84,13 @@ typedef struct cc_mhd2d_params {
     double sor_tol;         /* > 0: stop once max|lap(phi)-rhs| < sor_tol   */
     int32_t poisson_kind;   /* CC_POISSON_SOR or CC_POISSON_FFT             */
     int32_t precision;      /* CC_FP64 or CC_FP32                           */
-    int32_t reserved;
+    int32_t compensated;    /* FP32 only, 1: compensated (Kahan-style) state
+                               update -- every state plane carries its FP32
+                               rounding residual, each stage increment and
+                               the RK average are added with an error-free
+                               sum; uploads split FP64 values into value +
+                               residual, downloads return their sum.  The
+                               batched ensemble and the adjoint reject it. */
 } cc_mhd2d_params;
 
 /*
