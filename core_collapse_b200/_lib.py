@@ -27,6 +27,8 @@ CC_POISSON_DIRECT = 2
 CC_GRAVITY_ENCLOSED = 3
 CC_GRAVITY_SHELLS = 4
 CC_BATCH_MAX_DIRECT_SIDE = 2048
+CC_STAGE_TILE = 0
+CC_STAGE_MARCH = 1
 
 
 class CcMhd2dParams(C.Structure):
@@ -154,6 +156,7 @@ SIGNATURES = {
     "cc_mhd2d_compute_dt": (C.c_int, [_H, _DP]),
     "cc_mhd2d_rk2_step": (C.c_int, [_H, _DP, _DP, C.c_double]),
     "cc_mhd2d_advance": (C.c_int, [_H, C.c_int, _DP]),
+    "cc_mhd2d_set_stage_kernel": (C.c_int, [_H, C.c_int, C.c_int]),
     "cc_mhd2d_diagnostics": (C.c_int, [_H, C.POINTER(CcDiag)]),
     "cc_mhd2d_derived": (C.c_int, [_H, C.POINTER(C.POINTER(C.c_double))]),
     "cc_mhd2d_checkpoint_save": (C.c_int, [_H, C.c_char_p]),

@@ -48,6 +48,7 @@ struct Mhd2dBase {
     virtual int get_clock(double* t, long long* steps) = 0;
     virtual int set_clock(double t, long long steps) = 0;
     virtual const cc_mhd2d_params& params() const = 0;
+    virtual int set_stage_kernel(int kind, int seg_rows) = 0;
 };
 
 template <class T> struct Mhd2d : Mhd2dBase {
@@ -62,6 +63,9 @@ template <class T> struct Mhd2d : Mhd2dBase {
     bool comp = false;
     void* lblock = nullptr;
     Fields<T> lbuf[3];
+    // stage kernel: CC_STAGE_MARCH (the FP32 default) or CC_STAGE_TILE (FP64, its only form)
+    int stage_kind = sizeof(T) == 4 ? CC_STAGE_MARCH : CC_STAGE_TILE;
+    int march_rows = 128;
     int cur = 0;
     T* phi = nullptr;
     T* gxa = nullptr;
@@ -365,7 +369,11 @@ template <class T> struct Mhd2d : Mhd2dBase {
             CC_CUDA(cudaEventCreate(&e1));
             CC_CUDA(cudaEventRecord(e0, st()));
         }
-        if (comp)
+        if (stage_kind == CC_STAGE_MARCH)
+            CC_CUDA(M2Launch<T>::stage_march(c, buf[bi], buf[bo], comp ? &lbuf[bi] : nullptr,
+                                             comp ? &lbuf[bo] : nullptr, defer, gmode, ga, gb, dt_dev, active(),
+                                             march_rows, st()));
+        else if (comp)
             CC_CUDA(M2Launch<T>::stage_comp(c, buf[bi], buf[bo], lbuf[bi], lbuf[bo], defer, gmode, ga, gb, dt_dev,
                                             active(), st()));
         else
@@ -512,6 +520,17 @@ template <class T> struct Mhd2d : Mhd2dBase {
     }
 
     const cc_mhd2d_params& params() const override { return p; }
+
+    int set_stage_kernel(int kind, int seg_rows) override {
+        if (kind != CC_STAGE_TILE && kind != CC_STAGE_MARCH) return fail(h, CC_ERR_ARG, "unknown stage kernel");
+        if (kind == CC_STAGE_MARCH && sizeof(T) != 4)
+            return fail(h, CC_ERR_UNSUPPORTED, "the column-march stage kernel is an FP32 kernel");
+        if (seg_rows < 1) return fail(h, CC_ERR_ARG, "seg_rows < 1");
+        stage_kind = kind;
+        march_rows = seg_rows;
+        invalidate_graph();
+        return CC_OK;
+    }
 
     int derived(double* const* out) override {
         if (!loaded) return fail(h, CC_ERR_STATE, "no state uploaded");
@@ -724,6 +743,12 @@ int cc_mhd2d_rk2_step(cc_handle* h, const double* gx, const double* gy, double d
     if (!std::isfinite(dt) || dt < 0.0) return fail(h, CC_ERR_NONFINITE, "dt not finite or negative");
     if (int r = set_dev(h)) return r;
     return m->rk2_step(gx, gy, dt);
+}
+
+int cc_mhd2d_set_stage_kernel(cc_handle* h, int kind, int seg_rows) {
+    Mhd2dBase* m = m2(h);
+    if (!m) return CC_ERR_ARG;
+    return m->set_stage_kernel(kind, seg_rows);
 }
 
 int cc_mhd2d_advance(cc_handle* h, int nsteps, double* t) {

@@ -38,6 +38,17 @@ cudaError_t M2Launch<T>::prepare(int nx, int ny) {
     CC_ATTR((m2_stage_kernel<T, true, GRAV_ARRAYS>), smem)
     CC_ATTR((m2_stage_kernel<T, true, GRAV_PHI>), smem)
     if constexpr (sizeof(T) == 4) {
+        const int sm0 = (int)MarchG32::smem(false), sm1 = (int)MarchG32::smem(true);
+#define CC_MARCH_ATTR(D, G)                                                  \
+        CC_ATTR((m2_march_kernel<T, MARCH_W, MARCH_R, D, G, false>), sm0) \
+        CC_ATTR((m2_march_kernel<T, MARCH_W, MARCH_R, D, G, true>), sm1)
+        CC_MARCH_ATTR(false, GRAV_NONE)
+        CC_MARCH_ATTR(false, GRAV_ARRAYS)
+        CC_MARCH_ATTR(false, GRAV_PHI)
+        CC_MARCH_ATTR(true, GRAV_NONE)
+        CC_MARCH_ATTR(true, GRAV_ARRAYS)
+        CC_MARCH_ATTR(true, GRAV_PHI)
+#undef CC_MARCH_ATTR
         const int smem_c = smem + (int)kahan_smem_extra<T>(StageGeom<T>::NC);
         CC_ATTR((m2_stage_comp_kernel<T, false, GRAV_NONE>), smem_c)
         CC_ATTR((m2_stage_comp_kernel<T, false, GRAV_ARRAYS>), smem_c)
@@ -124,6 +135,40 @@ cudaError_t M2Launch<T>::stage_comp(const M2Const<T>& c, const Fields<T>& in, co
         CC_STAGE_CASE(true, GRAV_ARRAYS)
         CC_STAGE_CASE(true, GRAV_PHI)
 #undef CC_STAGE_CASE
+        return cudaErrorInvalidValue;
+    }
+}
+
+template <class T>
+cudaError_t M2Launch<T>::stage_march(const M2Const<T>& c, const Fields<T>& in, const Fields<T>& out,
+                                     const Fields<T>* lin, const Fields<T>* lout, bool defer, int gmode,
+                                     const T* ga, const T* gb, const double* dt, const int* active, int seg_rows,
+                                     cudaStream_t s) {
+    if constexpr (sizeof(T) != 4) {
+        return cudaErrorNotSupported;
+    } else {
+        if (seg_rows < 1) return cudaErrorInvalidValue;
+        const bool kahan = lin && lout;
+        const Fields<T> li = kahan ? *lin : Fields<T>{}, lo = kahan ? *lout : Fields<T>{};
+        const dim3 grid((c.nx + MARCH_W - 1) / MARCH_W, (c.ny + seg_rows - 1) / seg_rows);
+        const size_t smem = MarchG32::smem(kahan);
+#define CC_MARCH_CASE(D, G)                                                                                   \
+        if (defer == D && gmode == G) {                                                                       \
+            if (kahan)                                                                                        \
+                m2_march_kernel<T, MARCH_W, MARCH_R, D, G, true><<<grid, MarchG32::NT, smem, s>>>(           \
+                    c, in, out, li, lo, ga, gb, dt, active, seg_rows);                                        \
+            else                                                                                              \
+                m2_march_kernel<T, MARCH_W, MARCH_R, D, G, false><<<grid, MarchG32::NT, smem, s>>>(          \
+                    c, in, out, li, lo, ga, gb, dt, active, seg_rows);                                        \
+            return cudaGetLastError();                                                                        \
+        }
+        CC_MARCH_CASE(false, GRAV_NONE)
+        CC_MARCH_CASE(false, GRAV_ARRAYS)
+        CC_MARCH_CASE(false, GRAV_PHI)
+        CC_MARCH_CASE(true, GRAV_NONE)
+        CC_MARCH_CASE(true, GRAV_ARRAYS)
+        CC_MARCH_CASE(true, GRAV_PHI)
+#undef CC_MARCH_CASE
         return cudaErrorInvalidValue;
     }
 }

@@ -6,6 +6,7 @@
 
 #include "fft32_kernels.cuh"
 #include "mhd2d_kernels.cuh"
+#include "mhd2d_march.cuh"
 #include "poisson_kernels.cuh"
 
 namespace ccb {
@@ -29,6 +30,11 @@ template <class T> struct M2Launch {
                                     const Fields<T>& out, const Fields<T>& unl, const Fields<T>& s2l,
                                     const Fields<T>& outl, const double* dt, const int* active, double* spd_part,
                                     double* rho_part, cudaStream_t s);
+    // FP32 column-march stage (mhd2d_march.cuh): segments of seg_rows rows;
+    // lin / lout non-null: compensated state
+    static cudaError_t stage_march(const M2Const<T>& c, const Fields<T>& in, const Fields<T>& out,
+                                   const Fields<T>* lin, const Fields<T>* lout, bool defer, int gmode, const T* ga,
+                                   const T* gb, const double* dt, const int* active, int seg_rows, cudaStream_t s);
     static cudaError_t pack_in_split(const double* src, T* hi, T* lo, int w, int h, int pitch, cudaStream_t s);
     static cudaError_t pack_out_sum(const T* hi, const T* lo, double* dst, int w, int h, int pitch, cudaStream_t s);
     static cudaError_t speeds(const M2Const<T>& c, const Fields<T>& st, double* spd_part, double* rho_part,

@@ -208,6 +208,11 @@ class Mhd2dSolver:
         self._t = tt.value
         return tt.value
 
+    def set_stage_kernel(self, kind: str, seg_rows: int = 128):
+        """"tile" or "march" (FP32 only; the FP32 default): cc_mhd2d_set_stage_kernel."""
+        k = {"tile": L.CC_STAGE_TILE, "march": L.CC_STAGE_MARCH}[kind]
+        self._check(self._lib.cc_mhd2d_set_stage_kernel(self._h, k, int(seg_rows)))
+
     def set_stream(self, stream_ptr: int | None):
         """Issue work on a caller's cudaStream_t (e.g. torch's current stream)."""
         self._check(self._lib.cc_set_stream(self._h, C.c_void_p(stream_ptr) if stream_ptr else None))

@@ -250,6 +250,16 @@ int cc_mhd2d_rk2_step(cc_handle* h, const double* gx, const double* gy, double d
  * the handle's clock).  dt never leaves the device. */
 int cc_mhd2d_advance(cc_handle* h, int nsteps, double* t);
 
+/* Choice of the stage kernel (no counterpart in the reference, whose
+ * advance_stage M2:690-834 is one function): CC_STAGE_TILE, one CTA per tile
+ * of cells with a recomputed halo (the only form for FP64), or
+ * CC_STAGE_MARCH, FP32 only and the FP32 default, a CTA per column strip that
+ * marches up a segment of seg_rows rows carrying the rows below it.  Both
+ * evaluate the same expressions; a tuning and testing switch. */
+#define CC_STAGE_TILE 0
+#define CC_STAGE_MARCH 1
+int cc_mhd2d_set_stage_kernel(cc_handle* h, int kind, int seg_rows);
+
 /* Diagnostics of the resident state. */
 int cc_mhd2d_diagnostics(cc_handle* h, cc_diag* d);
 
