@@ -29,12 +29,15 @@ def _ptrs(U: Ucc, B: Bfaces):
 
 
 class AdjointSolver:
-    """One FP64 grid with a recorded, checkpointed forward run and its adjoint."""
+    """One grid with a recorded, checkpointed forward run and its adjoint, in
+    the precision of `p` ("fp64", or "fp32": FP32 forward and FP32 reverse
+    kernels, eta's adjoint summed in FP64); states and adjoints cross the API
+    as FP64 arrays."""
 
     def __init__(self, p: Params, checkpoint_every: int = 10, max_steps: int = 100):
         if p.gravity_on and p.poisson != "direct":
             p = replace(p, poisson="direct")
-        self.p = replace(p, precision="fp64")
+        self.p = replace(p, compensated=False)
         self._lib = L.lib()
         self._cp = self.p.to_c()
         self._h = C.c_void_p()

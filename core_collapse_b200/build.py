@@ -9,12 +9,13 @@ Translation units and their floating-point contract:
                                      the reference's x86-64 build (no FMA)
   dpoisson.cu                        -fmad=false, explicit fma() only: the batched
                                      direct Poisson solve, reproducible on the CPU
-  capi_adjoint.cu                    -fmad=false: the adjoint kernels recompute FP64
-                                     forward intermediates and must round like them
+  capi_adjoint.cu                    -fmad=false: the FP64 adjoint's kernels recompute
+                                     FP64 forward intermediates and must round like them
   ic3d.cu                            -fmad=false: host IC of the 3D driver through the
                                      solver's EOS functions
   mhd2d_f32.cu, mhd3d_f32.cu, ns2d_f32.cu,
-  euler2d_f32.cu, batch_f32.cu       FMA contraction on, approximate FP32 division
+  euler2d_f32.cu, batch_f32.cu,
+  adjoint_f32.cu                     FMA contraction on, approximate FP32 division
                                      and square root, flush-to-zero (the FP32 bulk path)
   capi*.cu, ic.cpp                   host code
 and the host programs of MAINS (g++, linked against the library):
@@ -59,6 +60,7 @@ UNITS = [
     ("euler2d_f32.cu", ["-prec-div=false", "-prec-sqrt=false", "-ftz=true"]),
     ("ns2d_f32.cu", ["-prec-div=false", "-prec-sqrt=false", "-ftz=true"]),
     ("batch_f32.cu", ["-prec-div=false", "-prec-sqrt=false", "-ftz=true"]),
+    ("adjoint_f32.cu", ["-prec-div=false", "-prec-sqrt=false", "-ftz=true"]),
     ("capi.cu", []),
     ("capi_mhd3d.cu", []),
     ("capi_euler2d.cu", []),

@@ -1,4 +1,6 @@
-// Discrete adjoint of one RK2 step of the 2D resistive-MHD solver (FP64).
+// Discrete adjoint of one RK2 step of the 2D resistive-MHD solver, templated on
+// the arithmetic type T of the forward it reverses (FP64, or FP32 with eta's
+// adjoint accumulated in FP64).
 //
 // The forward step (mhd2d_kernels.cuh; M2:838-869) is
 //   phi0 = P(U^n.rho)               S1' = Stage(U^n, phi0)        (pre-Joule)
@@ -12,7 +14,7 @@
 // the stage tile), so every branch is the forward's.  Contributions that one
 // thread scatters to cells or faces it does not own (slopes, face states,
 // cell-centred B, the potential gradient, Joule neighbours, EMF averages) are
-// FP64 atomic adds; eta's adjoint is block-reduced, then one atomic per block.
+// atomic adds in T; eta's adjoint is block-reduced in FP64, then one atomic per block.
 //
 // Adjoint arrays share the pitched layout of the state (pitch P, ny+1 rows).
 #pragma once
@@ -23,8 +25,9 @@ namespace ccb {
 
 constexpr int ADJ_NT = 256;
 
-__device__ __forceinline__ void aadd(double* p, double v) {
-    if (v != 0.0) atomicAdd(p, v);
+template <class T>
+__device__ __forceinline__ void aadd(T* p, T v) {
+    if (v != T(0)) atomicAdd(p, v);
 }
 
 __device__ __forceinline__ void eta_commit(double v, double* lam_eta) {
@@ -34,17 +37,20 @@ __device__ __forceinline__ void eta_commit(double v, double* lam_eta) {
 }
 
 // cell-centred B of a state at cell q (M2:278-286)
-__device__ __forceinline__ double bxcc(const Fields<double>& s, size_t q) { return 0.5 * (s.bx[q] + s.bx[q + 1]); }
-__device__ __forceinline__ double bycc(const Fields<double>& s, size_t q, int P) {
-    return 0.5 * (s.by[q] + s.by[q + P]);
+template <class T>
+__device__ __forceinline__ T bxcc(const Fields<T>& s, size_t q) { return T(0.5) * (s.bx[q] + s.bx[q + 1]); }
+template <class T>
+__device__ __forceinline__ T bycc(const Fields<T>& s, size_t q, int P) {
+    return T(0.5) * (s.by[q] + s.by[q + P]);
 }
 
 // Joule input of cell (i, j) of a stored stage output s (joule_cell's reads)
-__device__ __forceinline__ JouleIn<double> joule_in(const M2Const<double>& c, const Fields<double>& s, int i, int j) {
+template <class T>
+__device__ __forceinline__ JouleIn<T> joule_in(const M2Const<T>& c, const Fields<T>& s, int i, int j) {
     const int P = c.pitch;
     const size_t q = (size_t)j * P + i;
     const int iE = c.ax.cell(i + 1), iW = c.ax.cell(i - 1), jN = c.ay.cell(j + 1), jS = c.ay.cell(j - 1);
-    JouleIn<double> J;
+    JouleIn<T> J;
     J.rho = s.rho[q]; J.mx = s.mx[q]; J.my = s.my[q]; J.mz = s.mz[q]; J.E = s.E[q]; J.Bz = s.Bz[q];
     J.Bx = bxcc(s, q); J.By = bycc(s, q, P);
     J.bzE = s.Bz[(size_t)j * P + iE]; J.bzW = s.Bz[(size_t)j * P + iW];
@@ -55,8 +61,9 @@ __device__ __forceinline__ JouleIn<double> joule_in(const M2Const<double>& c, co
 }
 
 // Scatter the adjoint of Joule's inputs at cell (i, j) into lam (a state-shaped adjoint).
-__device__ __forceinline__ void joule_scatter(const M2Const<double>& c, const Fields<double>& lam, int i, int j,
-                                              const JouleAdj<double>& a) {
+template <class T>
+__device__ __forceinline__ void joule_scatter(const M2Const<T>& c, const Fields<T>& lam, int i, int j,
+                                              const JouleAdj<T>& a) {
     const int P = c.pitch;
     const size_t q = (size_t)j * P + i;
     const int iE = c.ax.cell(i + 1), iW = c.ax.cell(i - 1), jN = c.ay.cell(j + 1), jS = c.ay.cell(j - 1);
@@ -64,43 +71,44 @@ __device__ __forceinline__ void joule_scatter(const M2Const<double>& c, const Fi
     aadd(lam.mz + q, a.l[3]); aadd(lam.E + q, a.l[4]); aadd(lam.Bz + q, a.l[5]);
     aadd(lam.Bz + (size_t)j * P + iE, a.bzE); aadd(lam.Bz + (size_t)j * P + iW, a.bzW);
     aadd(lam.Bz + (size_t)jN * P + i, a.bzN); aadd(lam.Bz + (size_t)jS * P + i, a.bzS);
-    aadd(lam.by + (size_t)j * P + iE, a.byE); aadd(lam.by + q, a.byC + 0.5 * a.By);
-    aadd(lam.by + q + P, 0.5 * a.By);
-    aadd(lam.bx + (size_t)jN * P + i, a.bxN); aadd(lam.bx + q, a.bxC + 0.5 * a.Bx);
-    aadd(lam.bx + q + 1, 0.5 * a.Bx);
+    aadd(lam.by + (size_t)j * P + iE, a.byE); aadd(lam.by + q, a.byC + T(0.5) * a.By);
+    aadd(lam.by + q + P, T(0.5) * a.By);
+    aadd(lam.bx + (size_t)jN * P + i, a.bxN); aadd(lam.bx + q, a.bxC + T(0.5) * a.Bx);
+    aadd(lam.bx + q + 1, T(0.5) * a.Bx);
 }
 
 // ---------------------------------------------------------------------------
 // RK average (M2:848-868 with the deferred stage-2 Joule), reverse.
 // lnext: adjoint of U^{n+1}; lun (cells, plain store), ls2 and lbavg (atomics).
 // ---------------------------------------------------------------------------
+template <class T>
 __global__ void __launch_bounds__(ADJ_NT)
-adj_average_kernel(const M2Const<double> c, const Fields<double> un, const Fields<double> s2, double dt,
-                   const Fields<double> lnext, const Fields<double> lun, const Fields<double> ls2,
-                   double* __restrict__ lbavg_x, double* __restrict__ lbavg_y, double* __restrict__ lam_eta) {
+adj_average_kernel(const M2Const<T> c, const Fields<T> un, const Fields<T> s2, T dt,
+                   const Fields<T> lnext, const Fields<T> lun, const Fields<T> ls2,
+                   T* __restrict__ lbavg_x, T* __restrict__ lbavg_y, double* __restrict__ lam_eta) {
     const int P = c.pitch;
     double leta = 0.0;
     for (int k = blockIdx.x * ADJ_NT + threadIdx.x; k < c.nx * c.ny; k += gridDim.x * ADJ_NT) {
         const int i = k % c.nx, j = k / c.nx;
         const size_t q = (size_t)j * P + i;
         // forward: Joule(S2') at this cell, then the average and floors
-        const JouleIn<double> J = joule_in(c, s2, i, j);
-        double rho = J.rho, mx = J.mx, my = J.my, mz = J.mz, E = J.E, Bz = J.Bz;
+        const JouleIn<T> J = joule_in(c, s2, i, j);
+        T rho = J.rho, mx = J.mx, my = J.my, mz = J.mz, E = J.E, Bz = J.Bz;
         joule_cell(c, s2, i, j, dt, rho, mx, my, mz, E, Bz, J.Bx, J.By);
-        const double ar = 0.5 * (un.rho[q] + rho), amx = 0.5 * (un.mx[q] + mx), amy = 0.5 * (un.my[q] + my);
-        const double amz = 0.5 * (un.mz[q] + mz), aE = 0.5 * (un.E[q] + E), aBz = 0.5 * (un.Bz[q] + Bz);
-        const double bxl = 0.5 * (un.bx[q] + s2.bx[q]), bxr = 0.5 * (un.bx[q + 1] + s2.bx[q + 1]);
-        const double byd = 0.5 * (un.by[q] + s2.by[q]), byu = 0.5 * (un.by[q + P] + s2.by[q + P]);
-        const double Bx = 0.5 * (bxl + bxr), By = 0.5 * (byd + byu);
-        double l0 = lnext.rho[q], l1 = lnext.mx[q], l2 = lnext.my[q], l3 = lnext.mz[q], l4 = lnext.E[q];
-        double l5 = lnext.Bz[q], lBx = 0.0, lBy = 0.0;
+        const T ar = T(0.5) * (un.rho[q] + rho), amx = T(0.5) * (un.mx[q] + mx), amy = T(0.5) * (un.my[q] + my);
+        const T amz = T(0.5) * (un.mz[q] + mz), aE = T(0.5) * (un.E[q] + E), aBz = T(0.5) * (un.Bz[q] + Bz);
+        const T bxl = T(0.5) * (un.bx[q] + s2.bx[q]), bxr = T(0.5) * (un.bx[q + 1] + s2.bx[q + 1]);
+        const T byd = T(0.5) * (un.by[q] + s2.by[q]), byu = T(0.5) * (un.by[q + P] + s2.by[q + P]);
+        const T Bx = T(0.5) * (bxl + bxr), By = T(0.5) * (byd + byu);
+        T l0 = lnext.rho[q], l1 = lnext.mx[q], l2 = lnext.my[q], l3 = lnext.mz[q], l4 = lnext.E[q];
+        T l5 = lnext.Bz[q], lBx = 0.0, lBy = 0.0;
         floors_vjp(c, ar, amx, amy, amz, aE, Bx, By, aBz, l0, l1, l2, l3, l4, lBx, lBy, l5);
-        aadd(lbavg_x + q, 0.5 * lBx); aadd(lbavg_x + q + 1, 0.5 * lBx);
-        aadd(lbavg_y + q, 0.5 * lBy); aadd(lbavg_y + q + P, 0.5 * lBy);
-        lun.rho[q] = 0.5 * l0; lun.mx[q] = 0.5 * l1; lun.my[q] = 0.5 * l2;
-        lun.mz[q] = 0.5 * l3; lun.E[q] = 0.5 * l4; lun.Bz[q] = 0.5 * l5;
-        JouleAdj<double> a{};
-        a.l[0] = 0.5 * l0; a.l[1] = 0.5 * l1; a.l[2] = 0.5 * l2; a.l[3] = 0.5 * l3; a.l[4] = 0.5 * l4; a.l[5] = 0.5 * l5;
+        aadd(lbavg_x + q, T(0.5) * lBx); aadd(lbavg_x + q + 1, T(0.5) * lBx);
+        aadd(lbavg_y + q, T(0.5) * lBy); aadd(lbavg_y + q + P, T(0.5) * lBy);
+        lun.rho[q] = T(0.5) * l0; lun.mx[q] = T(0.5) * l1; lun.my[q] = T(0.5) * l2;
+        lun.mz[q] = T(0.5) * l3; lun.E[q] = T(0.5) * l4; lun.Bz[q] = T(0.5) * l5;
+        JouleAdj<T> a{};
+        a.l[0] = T(0.5) * l0; a.l[1] = T(0.5) * l1; a.l[2] = T(0.5) * l2; a.l[3] = T(0.5) * l3; a.l[4] = T(0.5) * l4; a.l[5] = T(0.5) * l5;
         if (c.resistive) joule_vjp(c, dt, J, a);
         joule_scatter(c, ls2, i, j, a);
         leta += a.eta;
@@ -109,21 +117,22 @@ adj_average_kernel(const M2Const<double> c, const Fields<double> un, const Field
 }
 
 // faces of the average: B^{n+1} = 0.5 (B^n + B2'); lbavg holds the floors' share
-__global__ void adj_average_face_kernel(const M2Const<double> c, const Fields<double> lnext,
-                                        const double* __restrict__ lbavg_x, const double* __restrict__ lbavg_y,
-                                        const Fields<double> lun, const Fields<double> ls2) {
+template <class T>
+__global__ void adj_average_face_kernel(const M2Const<T> c, const Fields<T> lnext,
+                                        const T* __restrict__ lbavg_x, const T* __restrict__ lbavg_y,
+                                        const Fields<T> lun, const Fields<T> ls2) {
     const int P = c.pitch;
     const int n = (c.nx + 1) * (c.ny + 1);
     for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
         const int i = k % (c.nx + 1), j = k / (c.nx + 1);
         const size_t q = (size_t)j * P + i;
         if (j < c.ny) {   // Bx face (i, j), i <= nx
-            const double l = 0.5 * (lnext.bx[q] + lbavg_x[q]);
+            const T l = T(0.5) * (lnext.bx[q] + lbavg_x[q]);
             lun.bx[q] = l;
             ls2.bx[q] += l;
         }
         if (i < c.nx) {   // By face (i, j), j <= ny
-            const double l = 0.5 * (lnext.by[q] + lbavg_y[q]);
+            const T l = T(0.5) * (lnext.by[q] + lbavg_y[q]);
             lun.by[q] = l;
             ls2.by[q] += l;
         }
@@ -134,17 +143,18 @@ __global__ void adj_average_face_kernel(const M2Const<double> c, const Fields<do
 // Stage reverse, step A: stage inputs after the deferred Joule (ut) and their
 // primitives (wp), recomputed once per cell.
 // ---------------------------------------------------------------------------
-__global__ void adj_prep_kernel(const M2Const<double> c, const Fields<double> sin, bool defer, double dt,
-                                double* const* ut, double* const* wp) {
+template <class T>
+__global__ void adj_prep_kernel(const M2Const<T> c, const Fields<T> sin, bool defer, T dt,
+                                T* const* ut, T* const* wp) {
     const int P = c.pitch;
     for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < c.nx * c.ny; k += gridDim.x * blockDim.x) {
         const int i = k % c.nx, j = k / c.nx;
         const size_t q = (size_t)j * P + i;
-        double rho = sin.rho[q], mx = sin.mx[q], my = sin.my[q], mz = sin.mz[q], E = sin.E[q], Bz = sin.Bz[q];
-        const double Bx = bxcc(sin, q), By = bycc(sin, q, P);
+        T rho = sin.rho[q], mx = sin.mx[q], my = sin.my[q], mz = sin.mz[q], E = sin.E[q], Bz = sin.Bz[q];
+        const T Bx = bxcc(sin, q), By = bycc(sin, q, P);
         if (defer) joule_cell(c, sin, i, j, dt, rho, mx, my, mz, E, Bz, Bx, By);
         ut[0][q] = rho; ut[1][q] = mx; ut[2][q] = my; ut[3][q] = mz; ut[4][q] = E; ut[5][q] = Bz;
-        const Prim<double> W = to_prim(c, rho, mx, my, mz, E, Bx, By, Bz);
+        const Prim<T> W = to_prim(c, rho, mx, my, mz, E, Bx, By, Bz);
         wp[0][q] = W.r; wp[1][q] = W.u; wp[2][q] = W.v; wp[3][q] = W.w;
         wp[4][q] = W.P; wp[5][q] = W.bx; wp[6][q] = W.by; wp[7][q] = W.bz;
     }
@@ -159,54 +169,55 @@ __global__ void adj_prep_kernel(const M2Const<double> c, const Fields<double> si
 // ld: dt * adjoint of the pre-floor update (plain store, 6 planes).
 // lphi: adjoint of the potential (atomics).
 // ---------------------------------------------------------------------------
+template <class T>
 __global__ void __launch_bounds__(ADJ_NT)
-adj_update_kernel(const M2Const<double> c, const Fields<double> sin, const Fields<double> sout,
-                  const double* __restrict__ phi, const double* const* rec, double dt, bool grav,
-                  const Fields<double> lout, double* __restrict__ lb1x, double* __restrict__ lb1y,
-                  const Fields<double> lin, double* const* ld, double* __restrict__ lphi) {
+adj_update_kernel(const M2Const<T> c, const Fields<T> sin, const Fields<T> sout,
+                  const T* __restrict__ phi, const T* const* rec, T dt, bool grav,
+                  const Fields<T> lout, T* __restrict__ lb1x, T* __restrict__ lb1y,
+                  const Fields<T> lin, T* const* ld, T* __restrict__ lphi) {
     const int P = c.pitch;
     for (int k = blockIdx.x * ADJ_NT + threadIdx.x; k < c.nx * c.ny; k += gridDim.x * ADJ_NT) {
         const int i = k % c.nx, j = k / c.nx;
         const size_t q = (size_t)j * P + i;
         // forward: the pre-floor update, its floors with the stage-input B
-        const double rr = rec[0][q], rmx = rec[1][q], rmy = rec[2][q], rmz = rec[3][q], rE = rec[4][q];
-        const double rBz = rec[5][q];
-        const double Bx0 = bxcc(sin, q), By0 = bycc(sin, q, P);
-        double rho = rr, E = rE;
+        const T rr = rec[0][q], rmx = rec[1][q], rmy = rec[2][q], rmz = rec[3][q], rE = rec[4][q];
+        const T rBz = rec[5][q];
+        const T Bx0 = bxcc(sin, q), By0 = bycc(sin, q, P);
+        T rho = rr, E = rE;
         floors(c, rho, rmx, rmy, rmz, E, Bx0, By0, rBz);
-        double l0 = lout.rho[q], l1 = lout.mx[q], l2 = lout.my[q], l3 = lout.mz[q], l4 = lout.E[q], l5 = lout.Bz[q];
+        T l0 = lout.rho[q], l1 = lout.mx[q], l2 = lout.my[q], l3 = lout.mz[q], l4 = lout.E[q], l5 = lout.Bz[q];
         if (grav && c.gravity_on) {
             const int iE = c.ax.cell(i + 1), iW = c.ax.cell(i - 1), jN = c.ay.cell(j + 1), jS = c.ay.cell(j - 1);
-            const double gx = -(phi[(size_t)j * P + iE] - phi[(size_t)j * P + iW]) / c.two_dx;
-            const double gy = -(phi[(size_t)jN * P + i] - phi[(size_t)jS * P + i]) / c.two_dy;
-            const double rv = vmax(rho, 1e-300);
-            const double u = rmx / rv, v = rmy / rv;
-            const double kmx = rmx + dt * rho * gx, kmy = rmy + dt * rho * gy;
-            const double kE = E + dt * rho * (u * gx + v * gy);
-            const double B1x = bxcc(sout, q), B1y = bycc(sout, q, P);
-            double lBx = 0.0, lBy = 0.0;
+            const T gx = -(phi[(size_t)j * P + iE] - phi[(size_t)j * P + iW]) / c.two_dx;
+            const T gy = -(phi[(size_t)jN * P + i] - phi[(size_t)jS * P + i]) / c.two_dy;
+            const T rv = vmax(rho, T(1e-300));
+            const T u = rmx / rv, v = rmy / rv;
+            const T kmx = rmx + dt * rho * gx, kmy = rmy + dt * rho * gy;
+            const T kE = E + dt * rho * (u * gx + v * gy);
+            const T B1x = bxcc(sout, q), B1y = bycc(sout, q, P);
+            T lBx = 0.0, lBy = 0.0;
             floors_vjp(c, rho, kmx, kmy, rmz, kE, B1x, B1y, rBz, l0, l1, l2, l3, l4, lBx, lBy, l5);
-            aadd(lb1x + q, 0.5 * lBx); aadd(lb1x + q + 1, 0.5 * lBx);
-            aadd(lb1y + q, 0.5 * lBy); aadd(lb1y + q + P, 0.5 * lBy);
+            aadd(lb1x + q, T(0.5) * lBx); aadd(lb1x + q + 1, T(0.5) * lBx);
+            aadd(lb1y + q, T(0.5) * lBy); aadd(lb1y + q + P, T(0.5) * lBy);
             // kick (rho, mz, Bz pass through)
-            const double lkmx = l1, lkmy = l2, lkE = l4;
+            const T lkmx = l1, lkmy = l2, lkE = l4;
             l0 += dt * gx * lkmx + dt * gy * lkmy + dt * (u * gx + v * gy) * lkE;
-            const double lu = dt * rho * gx * lkE, lv = dt * rho * gy * lkE;
-            const double lgx = dt * rho * lkmx + dt * rho * u * lkE;
-            const double lgy = dt * rho * lkmy + dt * rho * v * lkE;
+            const T lu = dt * rho * gx * lkE, lv = dt * rho * gy * lkE;
+            const T lgx = dt * rho * lkmx + dt * rho * u * lkE;
+            const T lgy = dt * rho * lkmy + dt * rho * v * lkE;
             l1 = lkmx + lu / rv;
             l2 = lkmy + lv / rv;
-            if (!(rho < 1e-300)) l0 -= (lu * u + lv * v) / rv;
+            if (!(rho < T(1e-300))) l0 -= (lu * u + lv * v) / rv;
             aadd(lphi + (size_t)j * P + iE, -lgx / c.two_dx);
             aadd(lphi + (size_t)j * P + iW, lgx / c.two_dx);
             aadd(lphi + (size_t)jN * P + i, -lgy / c.two_dy);
             aadd(lphi + (size_t)jS * P + i, lgy / c.two_dy);
         }
         // update floors with the stage-input B
-        double lBx = 0.0, lBy = 0.0;
+        T lBx = 0.0, lBy = 0.0;
         floors_vjp(c, rr, rmx, rmy, rmz, rE, Bx0, By0, rBz, l0, l1, l2, l3, l4, lBx, lBy, l5);
-        aadd(lin.bx + q, 0.5 * lBx); aadd(lin.bx + q + 1, 0.5 * lBx);
-        aadd(lin.by + q, 0.5 * lBy); aadd(lin.by + q + P, 0.5 * lBy);
+        aadd(lin.bx + q, T(0.5) * lBx); aadd(lin.bx + q + 1, T(0.5) * lBx);
+        aadd(lin.by + q, T(0.5) * lBy); aadd(lin.by + q + P, T(0.5) * lBy);
         // U1 = Ut + dt d
         aadd(lin.rho + q, l0); aadd(lin.mx + q, l1); aadd(lin.my + q, l2);
         aadd(lin.mz + q, l3); aadd(lin.E + q, l4); aadd(lin.Bz + q, l5);
@@ -221,17 +232,18 @@ adj_update_kernel(const M2Const<double> c, const Fields<double> sin, const Field
 // adjoint through CT to the input face it owns (Bx face (ie, je), By face
 // (ie, je)).
 // ---------------------------------------------------------------------------
+template <class T>
 __global__ void __launch_bounds__(ADJ_NT)
-adj_edge_kernel(const M2Const<double> c, const Fields<double> sin, double dt, const double* __restrict__ lb1x,
-                const double* __restrict__ lb1y, double* __restrict__ lf5x, double* __restrict__ lg5y,
-                const Fields<double> lin, double* __restrict__ lam_eta) {
+adj_edge_kernel(const M2Const<T> c, const Fields<T> sin, T dt, const T* __restrict__ lb1x,
+                const T* __restrict__ lb1y, T* __restrict__ lf5x, T* __restrict__ lg5y,
+                const Fields<T> lin, double* __restrict__ lam_eta) {
     const int P = c.pitch;
-    const double dtdy = dt / c.dy, dtdx = dt / c.dx;
+    const T dtdy = dt / c.dy, dtdx = dt / c.dx;
     double leta = 0.0;
     const int n = (c.nx + 1) * (c.ny + 1);
     for (int k = blockIdx.x * ADJ_NT + threadIdx.x; k < n; k += gridDim.x * ADJ_NT) {
         const int ie = k % (c.nx + 1), je = k / (c.nx + 1);
-        double lez = 0.0;
+        T lez = 0.0;
         if (je < c.ny) lez += dtdy * lb1x[(size_t)je * P + ie];
         if (je >= 1) lez -= dtdy * lb1x[(size_t)(je - 1) * P + ie];
         if (ie < c.nx) lez -= dtdx * lb1y[(size_t)je * P + ie];
@@ -241,15 +253,15 @@ adj_edge_kernel(const M2Const<double> c, const Fields<double> sin, double dt, co
         if (ie < c.nx) aadd(lin.by + (size_t)je * P + ie, lb1y[(size_t)je * P + ie]);
         if (lez == 0.0) continue;
         const int cj = c.ay.cell(je), cjm = c.ay.cell(je - 1), ci = c.ax.cell(ie), cim = c.ax.cell(ie - 1);
-        aadd(lf5x + (size_t)cjm * P + ie, -0.25 * lez);
-        aadd(lf5x + (size_t)cj * P + ie, -0.25 * lez);
-        aadd(lg5y + (size_t)je * P + cim, 0.25 * lez);
-        aadd(lg5y + (size_t)je * P + ci, 0.25 * lez);
+        aadd(lf5x + (size_t)cjm * P + ie, T(-0.25) * lez);
+        aadd(lf5x + (size_t)cj * P + ie, T(-0.25) * lez);
+        aadd(lg5y + (size_t)je * P + cim, T(0.25) * lez);
+        aadd(lg5y + (size_t)je * P + ci, T(0.25) * lez);
         if (c.resistive) {
-            const double dBydx = (sin.by[(size_t)je * P + ci] - sin.by[(size_t)je * P + cim]) / c.dx;
-            const double dBxdy = (sin.bx[(size_t)cj * P + ie] - sin.bx[(size_t)cjm * P + ie]) / c.dy;
+            const T dBydx = (sin.by[(size_t)je * P + ci] - sin.by[(size_t)je * P + cim]) / c.dx;
+            const T dBxdy = (sin.bx[(size_t)cj * P + ie] - sin.bx[(size_t)cjm * P + ie]) / c.dy;
             leta += lez * (dBydx - dBxdy);
-            const double e = c.eta * lez;
+            const T e = c.eta * lez;
             aadd(lin.by + (size_t)je * P + ci, e / c.dx);
             aadd(lin.by + (size_t)je * P + cim, -e / c.dx);
             aadd(lin.bx + (size_t)cj * P + ie, -e / c.dy);
@@ -262,19 +274,20 @@ adj_edge_kernel(const M2Const<double> c, const Fields<double> sin, double dt, co
 // face-state reconstruction (M2:295-311) of one side of a face, reverse:
 // scatter the adjoint of the floored face state lf (7 reconstructed
 // components, prim planes comp[k]) into lw at the mapped cells.
-__device__ __forceinline__ void face_state_scatter(const M2Const<double>& c, double* const* wp, double* const* lw,
-                                                   const int comp[7], size_t qm, size_t q0, size_t qp, double h,
-                                                   const double lf[7]) {
+template <class T>
+__device__ __forceinline__ void face_state_scatter(const M2Const<T>& c, T* const* wp, T* const* lw,
+                                                   const int comp[7], size_t qm, size_t q0, size_t qp, T h,
+                                                   const T lf[7]) {
 #pragma unroll
     for (int k = 0; k < 7; k++) {
         const int m = comp[k];
-        const double wm = wp[m][qm], wc = wp[m][q0], wq = wp[m][qp];
-        const double s = mc_slope(wm, wc, wq);
-        double l = lf[k];
+        const T wm = wp[m][qm], wc = wp[m][q0], wq = wp[m][qp];
+        const T s = mc_slope(wm, wc, wq);
+        T l = lf[k];
         if (k == 0 && (wc + h * s) < c.floor_rho) l = 0.0;   // r = vmax(r, floor_rho)
         if (k == 4 && (wc + h * s) < c.floor_P) l = 0.0;     // P = vmax(P, floor_P)
         if (l == 0.0) continue;
-        double lm = 0.0, lc = l, lp = 0.0;
+        T lm = 0.0, lc = l, lp = 0.0;
         mc_slope_vjp(wm, wc, wq, h * l, lm, lc, lp);
         aadd(lw[m] + qm, lm);
         aadd(lw[m] + q0, lc);
@@ -282,10 +295,11 @@ __device__ __forceinline__ void face_state_scatter(const M2Const<double>& c, dou
     }
 }
 
-__device__ __forceinline__ Prim<double> face_state_fwd(const M2Const<double>& c, double* const* wp, size_t qm,
-                                                       size_t q0, size_t qp, double h, bool ydir) {
-    Prim<double> W;
-    double v[8];
+template <class T>
+__device__ __forceinline__ Prim<T> face_state_fwd(const M2Const<T>& c, T* const* wp, size_t qm,
+                                                       size_t q0, size_t qp, T h, bool ydir) {
+    Prim<T> W;
+    T v[8];
 #pragma unroll
     for (int m = 0; m < 8; m++) v[m] = wp[m][q0];
     const int rc[7] = {0, 1, 2, 3, 4, ydir ? 5 : 6, 7};
@@ -305,10 +319,10 @@ __device__ __forceinline__ Prim<double> face_state_fwd(const M2Const<double>& c,
 // then HLLD, face states and MC slopes in reverse; lw (primitive adjoints)
 // and the normal-B adjoint of the input face by atomics.
 // ---------------------------------------------------------------------------
-template <bool YDIR>
+template <class T, bool YDIR>
 __global__ void __launch_bounds__(ADJ_NT)
-adj_face_kernel(const M2Const<double> c, const Fields<double> sin, double* const* wp, double* const* ld,
-                const double* __restrict__ lf5, double* const* lw, const Fields<double> lin) {
+adj_face_kernel(const M2Const<T> c, const Fields<T> sin, T* const* wp, T* const* ld,
+                const T* __restrict__ lf5, T* const* lw, const Fields<T> lin) {
     const int P = c.pitch;
     const int nf = YDIR ? c.nx * (c.ny + 1) : (c.nx + 1) * c.ny;
     const int rc[7] = {0, 1, 2, 3, 4, YDIR ? 5 : 6, 7};
@@ -325,13 +339,13 @@ adj_face_kernel(const M2Const<double> c, const Fields<double> sin, double* const
         const size_t qLm = cq(f - 2), qL = cq(f - 1), qR = cq(f), qRp = cq(f + 1);
         const size_t qface = YDIR ? (size_t)f * P + r : (size_t)r * P + f;
         // flux adjoint: d(cell) = -(F(face+1) - F(face)) / h; ld = dt * adj(U1raw)
-        const double ih = YDIR ? c.inv_dy : c.inv_dx;
-        double lF[7];
+        const T ih = YDIR ? c.inv_dy : c.inv_dx;
+        T lF[7];
         const int dmap[7] = {0, 1, 2, 3, 4, -1, 5};
 #pragma unroll
         for (int m = 0; m < 7; m++) {
             if (dmap[m] < 0) { lF[m] = lf5[qface]; continue; }
-            double v = 0.0;
+            T v = 0.0;
             if (f < nn) v += ld[dmap[m]][YDIR ? (size_t)f * P + r : (size_t)r * P + f];
             if (f >= 1) v -= ld[dmap[m]][YDIR ? (size_t)(f - 1) * P + r : (size_t)r * P + f - 1];
             lF[m] = ih * v;
@@ -340,46 +354,47 @@ adj_face_kernel(const M2Const<double> c, const Fields<double> sin, double* const
 #pragma unroll
         for (int m = 0; m < 7; m++) any = any || (lF[m] != 0.0);
         if (!any) continue;
-        Flux<double> g;
+        Flux<T> g;
         g.f0 = lF[0]; g.f1 = lF[1]; g.f2 = lF[2]; g.f3 = lF[3]; g.f4 = lF[4]; g.f5 = lF[5]; g.f6 = lF[6];
-        const Prim<double> WL = face_state_fwd(c, wp, qLm, qL, qR, 0.5, YDIR);
-        const Prim<double> WR = face_state_fwd(c, wp, qL, qR, qRp, -0.5, YDIR);
-        const double Bn = YDIR ? sin.by[qface] : sin.bx[qface];
-        Prim<double> lL = prim_zero<double>(), lR = prim_zero<double>();
-        double lBn = 0.0;
+        const Prim<T> WL = face_state_fwd(c, wp, qLm, qL, qR, T(0.5), YDIR);
+        const Prim<T> WR = face_state_fwd(c, wp, qL, qR, qRp, T(-0.5), YDIR);
+        const T Bn = YDIR ? sin.by[qface] : sin.bx[qface];
+        Prim<T> lL = prim_zero<T>(), lR = prim_zero<T>();
+        T lBn = 0.0;
         if (YDIR) hlld_y_vjp(c, WL, WR, Bn, g, lL, lR, lBn);
         else hlld_x_vjp(c, WL, WR, Bn, g, lL, lR, lBn);
         aadd((YDIR ? lin.by : lin.bx) + qface, lBn);
-        const double aL[8] = {lL.r, lL.u, lL.v, lL.w, lL.P, lL.bx, lL.by, lL.bz};
-        const double aR[8] = {lR.r, lR.u, lR.v, lR.w, lR.P, lR.bx, lR.by, lR.bz};
-        double fl[7], fr[7];
+        const T aL[8] = {lL.r, lL.u, lL.v, lL.w, lL.P, lL.bx, lL.by, lL.bz};
+        const T aR[8] = {lR.r, lR.u, lR.v, lR.w, lR.P, lR.bx, lR.by, lR.bz};
+        T fl[7], fr[7];
 #pragma unroll
         for (int m = 0; m < 7; m++) { fl[m] = aL[rc[m]]; fr[m] = aR[rc[m]]; }
-        face_state_scatter(c, wp, lw, rc, qLm, qL, qR, 0.5, fl);
-        face_state_scatter(c, wp, lw, rc, qL, qR, qRp, -0.5, fr);
+        face_state_scatter(c, wp, lw, rc, qLm, qL, qR, T(0.5), fl);
+        face_state_scatter(c, wp, lw, rc, qL, qR, qRp, T(-0.5), fr);
     }
 }
 
 // ---------------------------------------------------------------------------
 // Stage reverse, step E (cells): primitives (M2:126-135) in reverse.
 // ---------------------------------------------------------------------------
+template <class T>
 __global__ void __launch_bounds__(ADJ_NT)
-adj_prim_kernel(const M2Const<double> c, const Fields<double> sin, double* const* ut, double* const* lw,
-                const Fields<double> lin) {
+adj_prim_kernel(const M2Const<T> c, const Fields<T> sin, T* const* ut, T* const* lw,
+                const Fields<T> lin) {
     const int P = c.pitch;
     for (int k = blockIdx.x * ADJ_NT + threadIdx.x; k < c.nx * c.ny; k += gridDim.x * ADJ_NT) {
         const int i = k % c.nx, j = k / c.nx;
         const size_t q = (size_t)j * P + i;
-        Prim<double> l;
+        Prim<T> l;
         l.r = lw[0][q]; l.u = lw[1][q]; l.v = lw[2][q]; l.w = lw[3][q];
         l.P = lw[4][q]; l.bx = lw[5][q]; l.by = lw[6][q]; l.bz = lw[7][q];
-        double a0 = 0, a1 = 0, a2 = 0, a3 = 0, a4 = 0, aBx = 0, aBy = 0, aBz = 0;
+        T a0 = 0, a1 = 0, a2 = 0, a3 = 0, a4 = 0, aBx = 0, aBy = 0, aBz = 0;
         to_prim_vjp(c, ut[0][q], ut[1][q], ut[2][q], ut[3][q], ut[4][q], bxcc(sin, q), bycc(sin, q, P), ut[5][q], l,
                     a0, a1, a2, a3, a4, aBx, aBy, aBz);
         aadd(lin.rho + q, a0); aadd(lin.mx + q, a1); aadd(lin.my + q, a2);
         aadd(lin.mz + q, a3); aadd(lin.E + q, a4); aadd(lin.Bz + q, aBz);
-        aadd(lin.bx + q, 0.5 * aBx); aadd(lin.bx + q + 1, 0.5 * aBx);
-        aadd(lin.by + q, 0.5 * aBy); aadd(lin.by + q + P, 0.5 * aBy);
+        aadd(lin.bx + q, T(0.5) * aBx); aadd(lin.bx + q + 1, T(0.5) * aBx);
+        aadd(lin.by + q, T(0.5) * aBy); aadd(lin.by + q + P, T(0.5) * aBy);
     }
 }
 
@@ -387,15 +402,16 @@ adj_prim_kernel(const M2Const<double> c, const Fields<double> sin, double* const
 // Stage-2 input: Ut = Joule(S1') (deferred Joule, M2:631-686), reverse.
 // lin: adjoint of Ut (cells) and of the input faces; ls1 += adjoint of S1'.
 // ---------------------------------------------------------------------------
+template <class T>
 __global__ void __launch_bounds__(ADJ_NT)
-adj_joule_kernel(const M2Const<double> c, const Fields<double> s1, double dt, const Fields<double> lin,
-                 const Fields<double> ls1, double* __restrict__ lam_eta) {
+adj_joule_kernel(const M2Const<T> c, const Fields<T> s1, T dt, const Fields<T> lin,
+                 const Fields<T> ls1, double* __restrict__ lam_eta) {
     const int P = c.pitch;
     double leta = 0.0;
     for (int k = blockIdx.x * ADJ_NT + threadIdx.x; k < c.nx * c.ny; k += gridDim.x * ADJ_NT) {
         const int i = k % c.nx, j = k / c.nx;
         const size_t q = (size_t)j * P + i;
-        JouleAdj<double> a{};
+        JouleAdj<T> a{};
         a.l[0] = lin.rho[q]; a.l[1] = lin.mx[q]; a.l[2] = lin.my[q];
         a.l[3] = lin.mz[q]; a.l[4] = lin.E[q]; a.l[5] = lin.Bz[q];
         if (c.resistive) joule_vjp(c, dt, joule_in(c, s1, i, j), a);
@@ -406,7 +422,8 @@ adj_joule_kernel(const M2Const<double> c, const Fields<double> s1, double dt, co
 }
 
 // dst += src over the cells (if `cells`) and faces of a state-shaped adjoint
-__global__ void adj_add_state_kernel(const M2Const<double> c, const Fields<double> dst, const Fields<double> src,
+template <class T>
+__global__ void adj_add_state_kernel(const M2Const<T> c, const Fields<T> dst, const Fields<T> src,
                                      bool cells) {
     const int P = c.pitch;
     const int n = (c.nx + 1) * (c.ny + 1);
@@ -422,18 +439,19 @@ __global__ void adj_add_state_kernel(const M2Const<double> c, const Fields<doubl
     }
 }
 
-// zero nplanes planes of `plane` doubles each (one launch for a whole set)
-__global__ void adj_zero_kernel(double* const* planes, int nplanes, size_t plane) {
-    const size_t n2 = plane / 2;   // planes hold an even number of doubles (pitch is a multiple of 32)
+// zero nplanes planes of `plane` values each (one launch for a whole set)
+template <class T>
+__global__ void adj_zero_kernel(T* const* planes, int nplanes, size_t plane) {
     for (int k = 0; k < nplanes; k++) {
-        double2* q = reinterpret_cast<double2*>(planes[k]);
-        for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n2; i += (size_t)gridDim.x * blockDim.x)
-            q[i] = make_double2(0.0, 0.0);
+        T* q = planes[k];
+        for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < plane; i += (size_t)gridDim.x * blockDim.x)
+            q[i] = T(0);
     }
 }
 
 // dst[q] += src[q] over the cells of a pitched plane
-__global__ void adj_add_plane_kernel(int nx, int ny, int P, double* __restrict__ dst, const double* __restrict__ src) {
+template <class T>
+__global__ void adj_add_plane_kernel(int nx, int ny, int P, T* __restrict__ dst, const T* __restrict__ src) {
     for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < nx * ny; k += gridDim.x * blockDim.x) {
         const size_t q = (size_t)(k / nx) * P + (k % nx);
         dst[q] += src[q];

@@ -1,7 +1,7 @@
 /*
  * cc_adjoint.h -- discrete adjoint (vector-Jacobian product) of n steps of the
  * 2D resistive-MHD step (mhd2d_resistive_hlld_ct_gravity.cpp, rk2_step
- * M2:838-869 with compute_dt M2:579-598), FP64, one grid.
+ * M2:838-869 with compute_dt M2:579-598), one grid, FP64 or FP32.
  *
  * No reference counterpart: the reference has no derivatives.  The forward
  * map is the step of cc_batch.h / cc_step.h: RK2 stages of MUSCL-MC + HLLD +
@@ -29,8 +29,11 @@
 extern "C" {
 #endif
 
-/* p: FP64; gravity_on requires poisson_kind == CC_POISSON_DIRECT.  Device
- * memory: about 40 planes of (Nx+1)*(Ny+1) doubles per step of a checkpoint
+/* p: precision CC_FP64, or CC_FP32 (an FP32 forward run reversed by the same
+ * kernels in FP32, eta's adjoint summed in FP64; states and adjoints cross
+ * the API as FP64 arrays); gravity_on requires poisson_kind ==
+ * CC_POISSON_DIRECT; compensated must be 0.  Device
+ * memory: about 40 planes of (Nx+1)*(Ny+1) values per step of a checkpoint
  * block, plus 8 planes per checkpoint of max_steps. */
 int cc_adjoint_create(const cc_mhd2d_params* p, int checkpoint_every, int max_steps, cc_handle** out);
 int cc_adjoint_upload(cc_handle* h, const double* const* f);
