@@ -9,7 +9,12 @@ that tests/test_golden.py can pin the CPU oracle to the reference on a
 machine without the reference tree.  Every stored output is the reference's
 own result; nothing here is computed by the oracle or the library.
 
-    python tests/golden/make_golden.py          (from the repository root)
+    python tests/golden/make_golden.py [--mains-only | --no-mains]   (from the repository root)
+
+main_mhd2d.json / main_mhd3d.json hold what the reference's own main() wrote
+(its HDF5 datasets, recorded in memory): dataset names and dimensions, the
+rank-1 datasets (x, y, [z,] t) in full, and of every field the SHA-256 digest
+and sum of its first two stored frames and its last one.
 """
 from __future__ import annotations
 
@@ -133,15 +138,84 @@ def fft():
     _save("fft", **out)
 
 
+def frame_digest(a: np.ndarray) -> str:
+    """SHA-256 of a frame's FP64 values (little-endian bytes)."""
+    import hashlib
+    return hashlib.sha256(np.ascontiguousarray(a, dtype="<f8").tobytes()).hexdigest()
+
+
+def read_record(path: Path) -> dict:
+    """The datasets the reference's writer produced, as written by
+    oracle/_ref/ref_main_record: name -> {file, dims, values (rank 1) or the
+    SHA-256 digest, sum and max |value| of the first two frames and the last
+    one (rank >= 2)}."""
+    b = path.read_bytes()
+    assert b[:8] == b"CCH5REC1"
+    off = 8
+
+    def take(nbytes, dtype, n):
+        nonlocal off
+        a = np.frombuffer(b, dtype=dtype, count=n, offset=off)
+        off += nbytes * n
+        return a
+
+    out = {}
+    n = int(take(4, "<i4", 1)[0])
+    for _ in range(n):
+        strs = []
+        for _k in range(2):
+            ln = int(take(4, "<i4", 1)[0])
+            strs.append(b[off:off + ln].decode())
+            off += ln
+        rank = int(take(4, "<i4", 1)[0])
+        dims = [int(d) for d in take(8, "<u8", rank)]
+        head = take(8, "<f8", int(take(8, "<i8", 1)[0]))
+        last = take(8, "<f8", int(take(8, "<i8", 1)[0]))
+        ent = {"file": strs[1], "dims": dims}
+        if rank == 1:
+            ent["values"] = [float(v).hex() for v in head]
+        else:
+            frame = int(np.prod(dims[1:]))
+            frames = [head[k * frame:(k + 1) * frame] for k in range(len(head) // frame)] + [last]
+            ent["frames"] = [{"sha256": frame_digest(a), "sum": float(np.sum(a)), "absmax": float(np.max(np.abs(a)))}
+                             for a in frames]
+            ent["frame_index"] = list(range(len(frames) - 1)) + [dims[0] - 1]
+        out[strs[0]] = ent
+    return out
+
+
+def write_main_fixture(name: str, record: Path):
+    (HERE / f"main_{name}.json").write_text(json.dumps(read_record(record), indent=1) + "\n")
+
+
+def mains():
+    """The reference's own main() of the 2D and 3D MHD solvers, run once with
+    their defaults in a plain process (oracle/_ref/ref_main_record; the 2D run
+    takes most of an hour of CPU): their HDF5 datasets, recorded in memory by
+    oracle/hdf5_stub/hdf5.h, go to main_mhd2d.json / main_mhd3d.json."""
+    import subprocess
+    import tempfile
+    runner = O.REF_DIR / "ref_main_record"
+    for name in ("mhd2d", "mhd3d"):
+        with tempfile.TemporaryDirectory() as tmp:
+            rec = Path(tmp) / "rec.bin"
+            subprocess.run([str(runner), str(O.REF_DIR / f"libref_{name}.so"), f"ref_{name}_run_main", str(rec)],
+                           check=True, stdout=subprocess.DEVNULL, cwd=tmp)
+            write_main_fixture(name, rec)
+
+
 def main():
     for name in ("mhd2d", "mhd3d", "euler2d", "fft"):
         if O.ref(name) is None:
             raise SystemExit(f"compiled reference libref_{name}.so is missing: run make -C oracle")
-    mhd2d()
-    mhd3d()
-    euler2d()
-    fft()
-    print("wrote", sorted(p.name for p in HERE.glob("*.npz")))
+    if "--mains-only" not in sys.argv:
+        mhd2d()
+        mhd3d()
+        euler2d()
+        fft()
+    if "--no-mains" not in sys.argv:
+        mains()
+    print("wrote", sorted(p.name for p in HERE.glob("*.npz")) + sorted(p.name for p in HERE.glob("main_*.json")))
 
 
 if __name__ == "__main__":
