@@ -776,6 +776,29 @@ def run_adjoint(args, stream) -> dict:
         e3.record(stream)
         torch.cuda.synchronize()
         f32, a32 = e0.elapsed_time(e1), e2.elapsed_time(e3)
+    # the same workload with the single-grid red-black SOR instead of the direct
+    # solve (the reference M2's fixed 600 sweeps, omega 1.9), FP64
+    with AdjointSolver(dc_replace(p, poisson="sor", sor_iters=args.adjoint_sor_sweeps, sor_omega=1.9), k,
+                       nsteps) as s:
+        s.set_stream(stream.cuda_stream)
+        s.upload(U, B)
+        s.forward(nsteps)
+        e0, e1, e2, e3 = (torch.cuda.Event(enable_timing=True) for _ in range(4))
+        torch.cuda.synchronize()
+        e0.record(stream)
+        s.forward(nsteps)
+        e1.record(stream)
+        UT, _ = s.download()
+        loss_s, lamU, lamB = density_loss_adjoint(p, UT.rho, target)
+        torch.cuda.synchronize()
+        e2.record(stream)
+        gs, _, geta_s = s.vjp(lamU, lamB)
+        e3.record(stream)
+        torch.cuda.synchronize()
+        fs, as_ = e0.elapsed_time(e1), e2.elapsed_time(e3)
+    out["sor"] = {"forward_ms": fs, "adjoint_ms": as_, "adjoint_over_forward": as_ / fs, "loss": loss_s,
+                  "dloss_deta": geta_s, "sweeps_per_solve": args.adjoint_sor_sweeps,
+                  "note": "red-black SOR gravity (omega 1.9, fixed sweeps), reversed sweep by sweep; FP64"}
     out["fp32"] = {"forward_ms": f32, "adjoint_ms": a32, "adjoint_over_forward": a32 / f32,
                    "zone_updates_per_s_forward": n * n * nsteps / (f32 / 1000.0), "loss": loss32,
                    "dloss_deta": geta32,
@@ -825,6 +848,7 @@ def main():
     ap.add_argument("--adjoint-grid", type=int, default=512)
     ap.add_argument("--adjoint-steps", type=int, default=100)
     ap.add_argument("--adjoint-fd", type=int, default=64)
+    ap.add_argument("--adjoint-sor-sweeps", type=int, default=600)
     ap.add_argument("--adjoint-only", action="store_true", help="time only the adjoint block (a profiling aid)")
     ap.add_argument("--ns-only", action="store_true",
                     help="time only the Navier-Stokes block (a profiling aid; prints the ns2d block)")

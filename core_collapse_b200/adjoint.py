@@ -32,10 +32,12 @@ class AdjointSolver:
     """One grid with a recorded, checkpointed forward run and its adjoint, in
     the precision of `p` ("fp64", or "fp32": FP32 forward and FP32 reverse
     kernels, eta's adjoint summed in FP64); states and adjoints cross the API
-    as FP64 arrays."""
+    as FP64 arrays.  Gravity: the direct Poisson solve, or "sor" (the
+    single-grid red-black SOR with its recorded sweep counts, reversed sweep
+    by sweep); "fft" is replaced by the direct solve."""
 
     def __init__(self, p: Params, checkpoint_every: int = 10, max_steps: int = 100):
-        if p.gravity_on and p.poisson != "direct":
+        if p.gravity_on and p.poisson not in ("direct", "sor"):
             p = replace(p, poisson="direct")
         self.p = replace(p, compensated=False)
         self._lib = L.lib()

@@ -9,7 +9,9 @@
 // one (adj2d_kernels.cuh).  dt is a recorded constant of the step (its
 // dependence on the state through the CFL maximum is not differentiated), and
 // gravity uses the direct Poisson solve, whose adjoint is the same solve
-// (the discrete Laplacian is symmetric).
+// (the discrete Laplacian is symmetric), or the red-black SOR of the single-
+// grid solver with its recorded sweep count, reversed sweep by sweep
+// (adj_sor_kernels.cuh).
 //
 // Instantiated for double in capi_adjoint.cu (-fmad=false: the reverse
 // kernels recompute forward intermediates and must round like the FP64
@@ -22,6 +24,8 @@
 
 #include "../../include/cc_adjoint.h"
 #include "adj2d_kernels.cuh"
+#include "adj_sor_kernels.cuh"
+#include "mhd2d_launch.h"
 #include "batch_host.h"
 
 namespace ccb {
@@ -62,6 +66,15 @@ template <class T> struct Adjoint : AdjointBase, Batch<T> {
     int P = 0;
     size_t plane = 0;
     bool grav = false;
+    // red-black SOR gravity (poisson_kind CC_POISSON_SOR): forward solve
+    // buffers, the sweep count of every solve (two per step), reverse buffers
+    bool sor = false;
+    double *srhs = nullptr, *sphi = nullptr, *spart = nullptr, *spart2 = nullptr, *sres = nullptr;
+    double *smu0 = nullptr, *smu1 = nullptr, *srhat = nullptr, *sapart = nullptr;
+    unsigned int* sbar = nullptr;
+    int* sflags = nullptr;            // [barrier error, sweep count of the last solve]
+    int* sor_iters_dev = nullptr;     // 2 per step
+    std::vector<int> sor_iters_h;
     std::vector<Fields<T>> St, S1, S2, ckpt;
     std::vector<T*> Phi0, Phi1;
     std::vector<std::vector<T*>> Rec1, Rec2;
@@ -109,6 +122,22 @@ template <class T> struct Adjoint : AdjointBase, Batch<T> {
         P = pitch[0];
         plane = (size_t)P * (p[0].Ny + 1);
         grav = p[0].gravity_on != 0;
+        sor = grav && p[0].poisson_kind == CC_POISSON_SOR;
+        if (sor) {
+            const size_t N = (size_t)p[0].Nx * p[0].Ny;
+            for (double** q : {&srhs, &sphi, &smu0, &smu1, &srhat})
+                if (int r = dalloc(q, N)) return r;
+            if (int r = dalloc(&spart, 4096)) return r;
+            if (int r = dalloc(&spart2, 4096)) return r;
+            if (int r = dalloc(&sapart, ASOR_BLOCKS)) return r;
+            if (int r = dalloc(&sres, 1)) return r;
+            if (int r = dalloc(&sbar, 2)) return r;
+            if (int r = dalloc(&sflags, 2)) return r;
+            if (int r = dalloc(&sor_iters_dev, 2 * (size_t)max_steps)) return r;
+            CC_CUDA(cudaMemsetAsync(sbar, 0, sizeof(unsigned int) * 2, st()));
+            CC_CUDA(cudaMemsetAsync(sflags, 0, sizeof(int) * 2, st()));
+            sor_iters_h.assign(2 * (size_t)max_steps, 0);
+        }
         St.resize(K + 1); S1.resize(K); S2.resize(K);
         Phi0.resize(K); Phi1.resize(K);
         Rec1.assign(K, std::vector<T*>(6));
@@ -239,6 +268,56 @@ template <class T> struct Adjoint : AdjointBase, Batch<T> {
         return CC_OK;
     }
 
+    SorAdjArgs sor_adj_args() const {
+        const double dx = (p[0].x1 - p[0].x0) / p[0].Nx, dy = (p[0].y1 - p[0].y0) / p[0].Ny;
+        SorAdjArgs a;
+        a.nx = p[0].Nx; a.ny = p[0].Ny;
+        a.ax = AxisMap{p[0].Nx, p[0].periodic_x ? 1 : 0};
+        a.ay = AxisMap{p[0].Ny, p[0].periodic_y ? 1 : 0};
+        a.idx2 = 1.0 / (dx * dx); a.idy2 = 1.0 / (dy * dy);
+        a.denom = 2.0 * (a.idx2 + a.idy2);
+        a.omega = p[0].sor_omega;
+        a.rhat = srhat; a.part = sapart;
+        return a;
+    }
+
+    // forward red-black SOR of the density rho into the potential plane phi
+    // (the single-grid solver's M2 solve: rhs from the density mean, phi = 0
+    // start, sor_iters sweeps or the tolerance), its sweep count kept as
+    // solve number `which`
+    int sor_forward(const T* rho, T* phi, int which) {
+        const int nx = p[0].Nx, ny = p[0].Ny;
+        const int g = adj_grid(nx * ny);
+        adj_sor_rhs_kernel<T><<<g, ADJ_NT, 0, st()>>>(rho, nx, ny, P, rho_mean, 4.0 * M_PI * p[0].G, srhs, active);
+        CC_CUDA(cudaGetLastError());
+        const SorAdjArgs b = sor_adj_args();
+        SorArgs a;
+        a.nx = nx; a.ny = ny; a.ax = b.ax; a.ay = b.ay;
+        a.idx2 = b.idx2; a.idy2 = b.idy2; a.denom = b.denom;
+        a.omega = p[0].sor_omega; a.tol = p[0].sor_tol; a.max_iter = p[0].sor_iters;
+        a.rhs = srhs; a.phi = sphi; a.part = spart; a.part2 = spart2;
+        a.bar = GridBarrier{sbar, sbar + 1, sflags};
+        a.iters_out = sflags + 1; a.res_out = sres; a.active = active;
+        int nb = 0;
+        CC_CUDA(launch_sor(a, &nb, st()));
+        phi_to_field_kernel<T><<<g, ADJ_NT, 0, st()>>>(sphi, nx, ny, phi, P, active);
+        CC_CUDA(cudaGetLastError());
+        CC_CUDA(cudaMemcpyAsync(sor_iters_dev + which, sflags + 1, sizeof(int), cudaMemcpyDeviceToDevice, st()));
+        return CC_OK;
+    }
+
+    // host copy of the sweep counts of steps [s0, s0 + L); a timed-out grid barrier is an error
+    int sor_counts(int s0, int L) {
+        if (!sor) return CC_OK;
+        int err = 0;
+        CC_CUDA(cudaMemcpyAsync(&err, sflags, sizeof(int), cudaMemcpyDeviceToHost, st()));
+        CC_CUDA(cudaMemcpyAsync(sor_iters_h.data() + 2 * s0, sor_iters_dev + 2 * s0, sizeof(int) * 2 * L,
+                                cudaMemcpyDeviceToHost, st()));
+        CC_CUDA(cudaStreamSynchronize(st()));
+        if (err) return fail(h, CC_ERR_CUDA, "SOR grid barrier timed out");
+        return CC_OK;
+    }
+
     // mode 0: dt from the CFL condition (recorded); 1: recorded dt; 2: recorded dt + stage records
     int step(int l, int s, int mode) {
         const BatchInst<T>* A = recA + l;
@@ -246,8 +325,12 @@ template <class T> struct Adjoint : AdjointBase, Batch<T> {
         const BatchInst<T>* Cc = recC + l;
         if (grav) {
             CC_CUDA(launch_batch_finalize(dred, 1, spd_part, rho_part, BF_MEAN, dt, tclk, active, rho_mean, st()));
-            CC_CUDA(DPoissonLaunch<T>::solve(A, gwork, ngwork, gtile, nullptr, 0, ywork, nywork, 0, rho_mean,
-                                                  active, tcerr, st()));
+            if (sor) {
+                if (int r = sor_forward(St[l].rho, Phi0[l], 2 * s)) return r;
+            } else {
+                CC_CUDA(DPoissonLaunch<T>::solve(A, gwork, ngwork, gtile, nullptr, 0, ywork, nywork, 0, rho_mean,
+                                                 active, tcerr, st()));
+            }
         }
         if (mode == 0) {
             CC_CUDA(launch_batch_finalize(dred, 1, spd_part, rho_part, BF_DT | BF_CLAMP, dt, tclk, active, rho_mean,
@@ -268,8 +351,12 @@ template <class T> struct Adjoint : AdjointBase, Batch<T> {
         if (grav) {
             CC_CUDA(BatchLaunch<T>::rho_sum(B, rwork, nrwork, 1, active, rho_part, st()));
             CC_CUDA(launch_batch_finalize(dred, 1, spd_part, rho_part, BF_MEAN, dt, tclk, active, rho_mean, st()));
-            CC_CUDA(DPoissonLaunch<T>::solve(B, gwork, ngwork, gtile, nullptr, 0, ywork, nywork, 1, rho_mean,
-                                                  active, tcerr, st()));
+            if (sor) {
+                if (int r = sor_forward(S1[l].rho, Phi1[l], 2 * s + 1)) return r;
+            } else {
+                CC_CUDA(DPoissonLaunch<T>::solve(B, gwork, ngwork, gtile, nullptr, 0, ywork, nywork, 1, rho_mean,
+                                                 active, tcerr, st()));
+            }
         }
         if (int r = stage(B, 1, 2, true)) return r;
         CC_CUDA(BatchLaunch<T>::average(Cc, rwork, nrwork, 0, 2, 1, dt, active, spd_part, rho_part, st()));
@@ -305,6 +392,7 @@ template <class T> struct Adjoint : AdjointBase, Batch<T> {
         }
         if (int r = copy_state(fin, ckpt[(nsteps + K - 1) / K])) return r;
         if (int r = copy_state(St[0], ckpt[0])) return r;   // initial state again, for the next run
+        if (int r = sor_counts(0, nsteps)) return r;
         if (!replay) {
             nrec = nsteps;
             dts.assign(nsteps, 0.0);
@@ -329,6 +417,24 @@ template <class T> struct Adjoint : AdjointBase, Batch<T> {
     }
 
     // ---- reverse ----
+    // SOR solve number `which` in reverse: LamPhi -> adjoint of its density, added to ltarget.rho
+    int sor_adjoint(const Fields<T>& ltarget, int which) {
+        const int K = sor_iters_h[which];
+        const SorAdjArgs a = sor_adj_args();
+        adj_sor_start_kernel<T><<<ASOR_BLOCKS, ASOR_NT, 0, st()>>>(a, LamPhi, P, smu0);
+        CC_CUDA(cudaGetLastError());
+        for (int k = 0; k < K; k++) {
+            adj_sor_half_kernel<1, true, false><<<ASOR_BLOCKS, ASOR_NT, 0, st()>>>(a, smu0, smu1);
+            adj_sor_half_kernel<0, false, true><<<ASOR_BLOCKS, ASOR_NT, 0, st()>>>(a, smu1, smu0);
+        }
+        CC_CUDA(cudaGetLastError());
+        adj_sor_rhat_sum_kernel<ASOR_NT><<<ASOR_BLOCKS, ASOR_NT, 0, st()>>>(a);
+        adj_sor_finish_kernel<T><<<ASOR_BLOCKS, ASOR_NT, 0, st()>>>(a, 4.0 * M_PI * p[0].G, ltarget.rho, P);
+        CC_CUDA(cudaGetLastError());
+        h->perf.kernel_launches += 3 + 2 * K;
+        return CC_OK;
+    }
+
     // LamPhi -> 4 pi G L^+ LamPhi (the same direct solve), added to ltarget.rho
     int poisson_adjoint(const Fields<T>& ltarget) {
         CC_CUDA(BatchLaunch<T>::rho_sum(recP, rwork, nrwork, 0, active, rho_part, st()));
@@ -395,13 +501,13 @@ template <class T> struct Adjoint : AdjointBase, Batch<T> {
         adj_add_state_kernel<<<adj_grid(nedge), ADJ_NT, 0, st()>>>(c, LamS1, LamIn, false);
         CC_CUDA(cudaGetLastError());
         if (grav)
-            if (int r = poisson_adjoint(LamS1)) return r;
+            if (int r = sor ? sor_adjoint(LamS1, 2 * s + 1) : poisson_adjoint(LamS1)) return r;
         // stage 1: U^n -> S1'
         if (int r = stage_reverse(St[l], S1[l], Phi0[l], dRec1[l], false, dtv, LamS1)) return r;
         adj_add_state_kernel<<<adj_grid(nedge), ADJ_NT, 0, st()>>>(c, lun, LamIn, true);
         CC_CUDA(cudaGetLastError());
         if (grav)
-            if (int r = poisson_adjoint(lun)) return r;
+            if (int r = sor ? sor_adjoint(lun, 2 * s) : poisson_adjoint(lun)) return r;
         h->perf.kernel_launches += 5;
         return CC_OK;
     }
@@ -419,6 +525,7 @@ template <class T> struct Adjoint : AdjointBase, Batch<T> {
             const int s0 = b * K, L = std::min(K, n - s0);
             if (int r = copy_state(St[0], ckpt[b])) return r;
             if (int r = run_block(s0, L, 2)) return r;
+            if (int r = sor_counts(s0, L)) return r;
             for (int l = L - 1; l >= 0; l--) {
                 if (int r = step_reverse(l, s0 + l, lnext, lun)) return r;
                 std::swap(lnext, lun);

@@ -39,9 +39,13 @@ int cc_adjoint_create(const cc_mhd2d_params* p, int checkpoint_every, int max_st
     else if (p->compensated) { code = CC_ERR_UNSUPPORTED; why = "the adjoint has no compensated update"; }
     else if (checkpoint_every < 1 || max_steps < 1) { code = CC_ERR_ARG; why = "checkpoint_every and max_steps must be >= 1"; }
     else if (p->Nx < 4 || p->Ny < 4 || !(p->x1 > p->x0) || !(p->y1 > p->y0)) { code = CC_ERR_ARG; why = "bad grid"; }
-    else if (p->gravity_on && p->poisson_kind != CC_POISSON_DIRECT) {
+    else if (p->gravity_on && p->poisson_kind != CC_POISSON_DIRECT && p->poisson_kind != CC_POISSON_SOR) {
         code = CC_ERR_UNSUPPORTED;
-        why = "gravity needs poisson_kind == CC_POISSON_DIRECT (its adjoint is the same solve)";
+        why = "gravity needs poisson_kind CC_POISSON_DIRECT or CC_POISSON_SOR";
+    } else if (p->gravity_on && p->poisson_kind == CC_POISSON_SOR &&
+               ((p->periodic_x && (p->Nx & 1)) || (p->periodic_y && (p->Ny & 1)))) {
+        code = CC_ERR_UNSUPPORTED;
+        why = "red-black SOR needs an even extent along periodic axes";
     } else if (p->gravity_on && (p->Nx > CC_BATCH_MAX_DIRECT_SIDE || p->Ny > CC_BATCH_MAX_DIRECT_SIDE)) {
         code = CC_ERR_UNSUPPORTED;
         why = "direct Poisson side above CC_BATCH_MAX_DIRECT_SIDE";

@@ -7,7 +7,7 @@
  * map is the step of cc_batch.h / cc_step.h: RK2 stages of MUSCL-MC + HLLD +
  * CT + resistive EMF + gravity kick + Joule/Bz diffusion, floors, RK
  * average; with gravity on, the Poisson solve is the direct solve
- * (CC_POISSON_DIRECT).  Each step's dt is computed by the CFL rule in the
+ * (CC_POISSON_DIRECT) or the red-black SOR (CC_POISSON_SOR).  Each step's dt is computed by the CFL rule in the
  * recorded forward run and then treated as a constant (replayed in the
  * recomputation and in any finite-difference check); the derivative of a
  * floor, limiter or Riemann-solver branch is that of the branch taken.
@@ -31,8 +31,11 @@ extern "C" {
 
 /* p: precision CC_FP64, or CC_FP32 (an FP32 forward run reversed by the same
  * kernels in FP32, eta's adjoint summed in FP64; states and adjoints cross
- * the API as FP64 arrays); gravity_on requires poisson_kind ==
- * CC_POISSON_DIRECT; compensated must be 0.  Device
+ * the API as FP64 arrays); with gravity_on, poisson_kind is CC_POISSON_DIRECT
+ * (the direct solve, its own adjoint) or CC_POISSON_SOR (the red-black SOR
+ * of cc_mhd2d_*, sor_iters sweeps or the tolerance; reversed with the sweep
+ * count each solve took; even extents along periodic axes); compensated must
+ * be 0.  Device
  * memory: about 40 planes of (Nx+1)*(Ny+1) values per step of a checkpoint
  * block, plus 8 planes per checkpoint of max_steps. */
 int cc_adjoint_create(const cc_mhd2d_params* p, int checkpoint_every, int max_steps, cc_handle** out);
