@@ -284,6 +284,8 @@ def run_ours(args) -> None:
         p = workload_params(n, precision)
         s = Mhd2dSolver(p)
         s.set_stream(stream.cuda_stream)
+        if precision == "fp32":
+            s.set_stage_kernel(args.stage_kernel, args.march_rows)
         s.upload(U0, B0)
         s.advance(args.warmup, 0.0)
         s.set_profiling(profile)
@@ -363,7 +365,8 @@ def run_ours(args) -> None:
                          "steps": e2e_steps, "api": "cc_mhd2d_upload + cc_mhd2d_advance(1) + cc_mhd2d_download, "
                                                     "pinned FP64 host"}},
         "fp32_over_fp64": value32 / value64,
-        "roofline": {"bound": "hbm", "kernel": "m2_stage_kernel<float> (one RK2 stage)",
+        "roofline": {"bound": "hbm", "kernel": ("m2_march_kernel<float>" if args.stage_kernel == "march"
+                                                else "m2_stage_kernel<float>") + " (one RK2 stage)",
                      "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
                      "frac": achieved / peaks["hbm_gbs"], "peak_source": peaks["source"],
                      "traffic": traffic_per_launch(n), "algorithmic_bytes_per_launch": stage_bytes,
@@ -825,6 +828,9 @@ def main():
     ap.add_argument("--cpu-sample-grid", type=int, default=512)
     ap.add_argument("--cpu-steps", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--stage-kernel", choices=["march", "tile"], default="march",
+                    help="FP32 stage kernel of the headline run")
+    ap.add_argument("--march-rows", type=int, default=0, help="rows per march segment (0: from the grid)")
     ap.add_argument("--skip-ladder", action="store_true")
     ap.add_argument("--ladder-steps", type=int, default=500)
     ap.add_argument("--ladder-grids", default="1024,4096")

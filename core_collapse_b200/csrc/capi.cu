@@ -29,6 +29,19 @@ using namespace ccb;
 namespace {
 
 bool is_pow2(int n) { return n > 0 && (n & (n - 1)) == 0; }
+
+// Rows per segment of the column-march stage kernel: as long as possible (each
+// segment pays a half step to build its carried rows), but short enough that
+// the strips x segments fill 148 SMs x 4 resident CTAs about twice; a
+// multiple of the 8-row march step, 16 to 128 rows.
+int default_march_rows(int nx, int ny) {
+    const long strips = (nx + 31) / 32;
+    long rows = (long)ny * strips / (148L * 4 * 2);
+    rows = rows / 8 * 8;
+    if (rows < 16) rows = 16;
+    if (rows > 128) rows = 128;
+    return (int)rows;
+}
 int ilog2(int n) { int l = 0; while ((1 << l) < n) ++l; return l; }
 
 // --------------------------------------------------------------------------
@@ -65,7 +78,7 @@ template <class T> struct Mhd2d : Mhd2dBase {
     Fields<T> lbuf[3];
     // stage kernel: CC_STAGE_MARCH (the FP32 default) or CC_STAGE_TILE (FP64, its only form)
     int stage_kind = sizeof(T) == 4 ? CC_STAGE_MARCH : CC_STAGE_TILE;
-    int march_rows = 128;
+    int march_rows = 0;   // 0: from the grid (init)
     int cur = 0;
     T* phi = nullptr;
     T* gxa = nullptr;
@@ -129,6 +142,7 @@ template <class T> struct Mhd2d : Mhd2dBase {
         c.gravity_on = p.gravity_on ? 1 : 0;
         c.resistive = (p.eta > 0.0) ? 1 : 0;
         plane = (size_t)P * (ny + 1);
+        march_rows = default_march_rows(nx, ny);
         CC_CUDA(M2Launch<T>::prepare(nx, ny));
 
         if (p.compensated && sizeof(T) != 4)
@@ -525,9 +539,9 @@ template <class T> struct Mhd2d : Mhd2dBase {
         if (kind != CC_STAGE_TILE && kind != CC_STAGE_MARCH) return fail(h, CC_ERR_ARG, "unknown stage kernel");
         if (kind == CC_STAGE_MARCH && sizeof(T) != 4)
             return fail(h, CC_ERR_UNSUPPORTED, "the column-march stage kernel is an FP32 kernel");
-        if (seg_rows < 1) return fail(h, CC_ERR_ARG, "seg_rows < 1");
+        if (seg_rows < 0) return fail(h, CC_ERR_ARG, "seg_rows < 0");
         stage_kind = kind;
-        march_rows = seg_rows;
+        march_rows = seg_rows > 0 ? seg_rows : default_march_rows(p.Nx, p.Ny);
         invalidate_graph();
         return CC_OK;
     }

@@ -254,8 +254,9 @@ int cc_mhd2d_advance(cc_handle* h, int nsteps, double* t);
  * advance_stage M2:690-834 is one function): CC_STAGE_TILE, one CTA per tile
  * of cells with a recomputed halo (the only form for FP64), or
  * CC_STAGE_MARCH, FP32 only and the FP32 default, a CTA per column strip that
- * marches up a segment of seg_rows rows carrying the rows below it.  Both
- * evaluate the same expressions; a tuning and testing switch. */
+ * marches up a segment of seg_rows rows carrying the rows below it (0: a
+ * length chosen from the grid so the segments fill the GPU).  Both evaluate
+ * the same expressions; a tuning and testing switch. */
 #define CC_STAGE_TILE 0
 #define CC_STAGE_MARCH 1
 int cc_mhd2d_set_stage_kernel(cc_handle* h, int kind, int seg_rows);

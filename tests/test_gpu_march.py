@@ -18,7 +18,7 @@ pytestmark = pytest.mark.gpu
 TOL = 2e-5   # relative L-inf per field after a few steps, FP32
 
 
-def _run(p, U, B, nsteps, kind, seg=128):
+def _run(p, U, B, nsteps, kind, seg=0):
     with Mhd2dSolver(p) as s:
         s.set_stage_kernel(kind, seg)
         s.upload(U, B)
@@ -34,7 +34,7 @@ def _compare(a_list, b_list, what):
 
 
 @pytest.mark.parametrize("name", sorted(CASES))
-@pytest.mark.parametrize("seg", [128, 5, 1])
+@pytest.mark.parametrize("seg", [0, 128, 5, 1])
 def test_march_matches_tile_cases(name, seg):
     p, U, B = make_case(name, precision="fp32")
     p.t_end = 10.0
