@@ -828,7 +828,7 @@ def main():
     ap.add_argument("--cpu-sample-grid", type=int, default=512)
     ap.add_argument("--cpu-steps", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--stage-kernel", choices=["march", "tile"], default="march",
+    ap.add_argument("--stage-kernel", choices=["march", "tile"], default="tile",
                     help="FP32 stage kernel of the headline run")
     ap.add_argument("--march-rows", type=int, default=0, help="rows per march segment (0: from the grid)")
     ap.add_argument("--skip-ladder", action="store_true")

@@ -57,7 +57,7 @@ template <class T> struct Adjoint : AdjointBase, Batch<T> {
     using B::gwork; using B::ngwork; using B::gtile; using B::ywork; using B::nywork; using B::tcerr;
     using B::swork; using B::nswork; using B::spd_part; using B::rho_part; using B::dt; using B::tclk;
     using B::rho_mean; using B::active; using B::steps; using B::staging; using B::st; using B::dalloc;
-    using B::upload_vec; using B::this_handle;
+    using B::upload_vec; using B::this_handle; using B::tcwork; using B::ntcwork;
     int K;
     int max_steps;
     double t0 = 0.0;
@@ -328,7 +328,7 @@ template <class T> struct Adjoint : AdjointBase, Batch<T> {
             if (sor) {
                 if (int r = sor_forward(St[l].rho, Phi0[l], 2 * s)) return r;
             } else {
-                CC_CUDA(DPoissonLaunch<T>::solve(A, gwork, ngwork, gtile, nullptr, 0, ywork, nywork, 0, rho_mean,
+                CC_CUDA(DPoissonLaunch<T>::solve(A, gwork, ngwork, gtile, tcwork, ntcwork, ywork, nywork, 0, rho_mean,
                                                  active, tcerr, st()));
             }
         }
@@ -354,7 +354,7 @@ template <class T> struct Adjoint : AdjointBase, Batch<T> {
             if (sor) {
                 if (int r = sor_forward(S1[l].rho, Phi1[l], 2 * s + 1)) return r;
             } else {
-                CC_CUDA(DPoissonLaunch<T>::solve(B, gwork, ngwork, gtile, nullptr, 0, ywork, nywork, 1, rho_mean,
+                CC_CUDA(DPoissonLaunch<T>::solve(B, gwork, ngwork, gtile, tcwork, ntcwork, ywork, nywork, 1, rho_mean,
                                                  active, tcerr, st()));
             }
         }
@@ -439,7 +439,7 @@ template <class T> struct Adjoint : AdjointBase, Batch<T> {
     int poisson_adjoint(const Fields<T>& ltarget) {
         CC_CUDA(BatchLaunch<T>::rho_sum(recP, rwork, nrwork, 0, active, rho_part, st()));
         CC_CUDA(launch_batch_finalize(dred, 1, spd_part, rho_part, BF_MEAN, dt, tclk, active, rho_mean, st()));
-        CC_CUDA(DPoissonLaunch<T>::solve(recP, gwork, ngwork, gtile, nullptr, 0, ywork, nywork, 0, rho_mean,
+        CC_CUDA(DPoissonLaunch<T>::solve(recP, gwork, ngwork, gtile, tcwork, ntcwork, ywork, nywork, 0, rho_mean,
                                               active, tcerr, st()));
         adj_add_plane_kernel<<<adj_grid(p[0].Nx * p[0].Ny), ADJ_NT, 0, st()>>>(p[0].Nx, p[0].Ny, P, ltarget.rho,
                                                                                 PoisOut);

@@ -76,8 +76,8 @@ template <class T> struct Mhd2d : Mhd2dBase {
     bool comp = false;
     void* lblock = nullptr;
     Fields<T> lbuf[3];
-    // stage kernel: CC_STAGE_MARCH (the FP32 default) or CC_STAGE_TILE (FP64, its only form)
-    int stage_kind = sizeof(T) == 4 ? CC_STAGE_MARCH : CC_STAGE_TILE;
+    // stage kernel: CC_STAGE_TILE (the default; FP64's only form) or CC_STAGE_MARCH (FP32)
+    int stage_kind = CC_STAGE_TILE;
     int march_rows = 0;   // 0: from the grid (init)
     int cur = 0;
     T* phi = nullptr;

@@ -55,9 +55,11 @@ int main(int argc, char** argv) {
     const int Nx = p.Nx, Ny = p.Ny, Nz = p.Nz;
     const size_t N = (size_t)Nx * Ny * Nz;
     std::vector<double> x(Nx), y(Ny), z(Nz);
-    for (int i = 0; i < Nx; i++) x[i] = p.x0 + (i + 0.5) * (p.x1 - p.x0) / Nx;
-    for (int j = 0; j < Ny; j++) y[j] = p.y0 + (j + 0.5) * (p.y1 - p.y0) / Ny;
-    for (int k = 0; k < Nz; k++) z[k] = p.z0 + (k + 0.5) * (p.z1 - p.z0) / Nz;
+    // cell centres as the reference forms them (M3:1134-1143): x0 + (i + 0.5) * dx
+    const double dx = (p.x1 - p.x0) / Nx, dy = (p.y1 - p.y0) / Ny, dz = (p.z1 - p.z0) / Nz;
+    for (int i = 0; i < Nx; i++) x[i] = p.x0 + (i + 0.5) * dx;
+    for (int j = 0; j < Ny; j++) y[j] = p.y0 + (j + 0.5) * dy;
+    for (int k = 0; k < Nz; k++) z[k] = p.z0 + (k + 0.5) * dz;
 
     cc_handle* h = nullptr;
     auto check = [&](int r, const char* what) {

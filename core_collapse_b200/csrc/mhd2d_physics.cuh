@@ -108,15 +108,19 @@ __host__ __device__ __forceinline__ T energy(const M2Const<T>& c, const Prim<T>&
 // fast magnetosonic speed with normal component bn (M2:148-174)
 template <class T>
 __host__ __device__ __forceinline__ T fast_speed(const M2Const<T>& c, const Prim<T>& W, T bn) {
-    T a2 = c.gamma * W.P / vmax(W.r, c.floor_rho);
     T b2 = W.bx * W.bx + W.by * W.by + W.bz * W.bz;
-    T rho = vmax(W.r, T(1e-300));
-    T vA2, vn2;
+    T a2, vA2, vn2;
     if constexpr (fast_recip<T>()) {
-        const T ir = T(1.0) / rho;
+        // every caller passes a floored density (face states, cons_to_prim), so
+        // the two floors of the reference's expression select the same value and
+        // one reciprocal serves the three quotients
+        const T ir = T(1.0) / vmax(W.r, c.floor_rho);
+        a2 = c.gamma * W.P * ir;
         vA2 = b2 * ir;
         vn2 = (bn * bn) * ir;
     } else {
+        a2 = c.gamma * W.P / vmax(W.r, c.floor_rho);
+        const T rho = vmax(W.r, T(1e-300));
         vA2 = b2 / rho;
         vn2 = (bn * bn) / rho;
     }
@@ -135,6 +139,23 @@ __host__ __device__ __forceinline__ Flux<T> ideal_flux(const Cst& c, const Prim<
     T B2 = Bx * Bx + By * By + Bz * Bz;
     T pt = P + T(0.5) * B2;
     T E = energy(c, W);
+    T vdotB = u * Bx + v * By + w * Bz;
+    Flux<T> F;
+    F.f0 = rho * u;
+    F.f1 = rho * u * u + pt - Bx * Bx;
+    F.f2 = rho * u * v - Bx * By;
+    F.f3 = rho * u * w - Bx * Bz;
+    F.f4 = (E + pt) * u - Bx * vdotB;
+    F.f5 = u * By - v * Bx;
+    F.f6 = u * Bz - w * Bx;
+    return F;
+}
+
+// ideal_flux of a state whose total energy E and total pressure pt are known
+// (the same expressions as ideal_flux forms them, so the same values)
+template <class T>
+__host__ __device__ __forceinline__ Flux<T> ideal_flux_ep(const Prim<T>& W, T E, T pt) {
+    T rho = W.r, u = W.u, v = W.v, w = W.w, Bx = W.bx, By = W.by, Bz = W.bz;
     T vdotB = u * Bx + v * By + w * Bz;
     Flux<T> F;
     F.f0 = rho * u;
@@ -224,10 +245,22 @@ __host__ __device__ __forceinline__ Flux<T> hlld_x(const Cst& c, Prim<T> L, Prim
             wRs = R.w - Bn * (BzRs - R.bz) / dd;
         }
     }
-    const T sqL = sqrt(vmax(rLs, T(1e-300)));
-    const T sqR = sqrt(vmax(rRs, T(1e-300)));
-    const T SLL = SM - fabs(Bn) / sqL;
-    const T SRR = SM + fabs(Bn) / sqR;
+    T sqL, sqR, SLL, SRR;
+    if constexpr (fast_recip<T>()) {
+        // one reciprocal square root each: sqrt(r) = r / sqrt(r), |Bn| / sqrt(r)
+        const T rl = vmax(rLs, T(1e-30)), rr = vmax(rRs, T(1e-30));
+        const T iqL = rsqrt(rl), iqR = rsqrt(rr);
+        sqL = rl * iqL;
+        sqR = rr * iqR;
+        // explicit fused multiply-adds: the same rounding in every kernel that inlines this
+        SLL = __fmaf_rn(-fabs(Bn), iqL, SM);
+        SRR = __fmaf_rn(fabs(Bn), iqR, SM);
+    } else {
+        sqL = sqrt(vmax(rLs, T(1e-300)));
+        sqR = sqrt(vmax(rRs, T(1e-300)));
+        SLL = SM - fabs(Bn) / sqL;
+        SRR = SM + fabs(Bn) / sqR;
+    }
 
     // pick the region first, then build only the state it needs
     const bool left = (T(0.0) < SM);
@@ -260,7 +293,7 @@ __host__ __device__ __forceinline__ Flux<T> hlld_x(const Cst& c, Prim<T> L, Prim
     const T vBs = SM * Bn + vs * Bys + ws * Bzs;
     const T vBw = W.u * W.bx + W.v * W.by + W.w * W.bz;
     const T Es = ((S - W.u) * EW - (ptW * W.u - Bn * vBw) + (pts * SM - Bn * vBs)) / (S - SM);
-    Flux<T> F = ideal_flux(c, W);
+    Flux<T> F = ideal_flux_ep(W, EW, ptW);
     F.f0 = F.f0 + S * (rs - W.r);
     F.f1 = F.f1 + S * (rs * SM - W.r * W.u);
     F.f2 = F.f2 + S * (rs * vs - W.r * W.v);

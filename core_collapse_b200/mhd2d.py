@@ -209,8 +209,8 @@ class Mhd2dSolver:
         return tt.value
 
     def set_stage_kernel(self, kind: str, seg_rows: int = 0):
-        """"tile" or "march" (FP32 only; the FP32 default), seg_rows 0: chosen
-        from the grid (cc_mhd2d_set_stage_kernel)."""
+        """"tile" (the default) or "march" (FP32 only), seg_rows 0: chosen from
+        the grid (cc_mhd2d_set_stage_kernel)."""
         k = {"tile": L.CC_STAGE_TILE, "march": L.CC_STAGE_MARCH}[kind]
         self._check(self._lib.cc_mhd2d_set_stage_kernel(self._h, k, int(seg_rows)))
 

@@ -251,9 +251,9 @@ int cc_mhd2d_rk2_step(cc_handle* h, const double* gx, const double* gy, double d
 int cc_mhd2d_advance(cc_handle* h, int nsteps, double* t);
 
 /* Choice of the stage kernel (no counterpart in the reference, whose
- * advance_stage M2:690-834 is one function): CC_STAGE_TILE, one CTA per tile
- * of cells with a recomputed halo (the only form for FP64), or
- * CC_STAGE_MARCH, FP32 only and the FP32 default, a CTA per column strip that
+ * advance_stage M2:690-834 is one function): CC_STAGE_TILE, the default, one
+ * CTA per tile of cells with a recomputed halo (the only form for FP64), or
+ * CC_STAGE_MARCH, FP32 only, a CTA per column strip that
  * marches up a segment of seg_rows rows carrying the rows below it (0: a
  * length chosen from the grid so the segments fill the GPU).  Both evaluate
  * the same expressions; a tuning and testing switch. */
