@@ -15,7 +15,7 @@ default parameters:
   /x /y /z bit for bit, shapes (Nt, Nz, Ny, Nx), /t[0] within 1e-13, the
   first frame (stored after one step) of every field within 1e-12 of the
   reference's by its sum and maximum (the hybrid EOS's pow runs on the
-  device)."""
+  device; div B, roundoff itself, relative to |B| / dx)."""
 from __future__ import annotations
 
 import hashlib
@@ -85,10 +85,13 @@ def test_mhd3d_driver_output_pinned_to_reference_main(tmp_path):
         assert np.array_equal(got[k], _values(fx["/" + k]))
     nt = len(got["t"])
     assert nt >= 2 and abs(got["t"][0] - t_ref[0]) <= 1e-13 * t_ref[0]
+    # div B is roundoff itself: its scale is |B| / dx, not its own size
+    bscale = max(fx["/" + b]["frames"][0]["absmax"] for b in ("Bx", "By", "Bz"))
+    hmin = min(float(got[a][1] - got[a][0]) for a in ("x", "y", "z"))
     for k in names[4:]:
         ent = fx["/" + k]
         assert list(got[k].shape) == [nt] + ent["dims"][1:], k
         f0 = ent["frames"][0]
-        scale = max(f0["absmax"], 1e-300)
+        scale = bscale / hmin if k == "divB" else max(f0["absmax"], 1e-300)
         assert abs(float(np.sum(got[k][0])) - f0["sum"]) <= 1e-12 * scale * got[k][0].size, k
         assert abs(float(np.max(np.abs(got[k][0]))) - f0["absmax"]) <= 1e-12 * scale, k
