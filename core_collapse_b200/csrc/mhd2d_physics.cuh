@@ -293,7 +293,12 @@ __host__ __device__ __forceinline__ Flux<T> hlld_x(const Cst& c, Prim<T> L, Prim
     const T vBs = SM * Bn + vs * Bys + ws * Bzs;
     const T vBw = W.u * W.bx + W.v * W.by + W.w * W.bz;
     const T Es = ((S - W.u) * EW - (ptW * W.u - Bn * vBw) + (pts * SM - Bn * vBs)) / (S - SM);
-    Flux<T> F = ideal_flux_ep(W, EW, ptW);
+    // FP64: the flux from the known energy and total pressure (the same values);
+    // FP32 forms them again, which keeps its rounding the same in every kernel
+    // that inlines this (the batched tile shapes give bit-identical results)
+    Flux<T> F;
+    if constexpr (fast_recip<T>()) F = ideal_flux(c, W);
+    else F = ideal_flux_ep(W, EW, ptW);
     F.f0 = F.f0 + S * (rs - W.r);
     F.f1 = F.f1 + S * (rs * SM - W.r * W.u);
     F.f2 = F.f2 + S * (rs * vs - W.r * W.v);
