@@ -664,12 +664,40 @@ def run_ensemble(args, stream, rank: int, world: int, barrier, max_over_ranks, s
         e1.record(stream)
         torch.cuda.synchronize()
         single_value = ns * ns * steps / (e0.elapsed_time(e1) / 1000.0)
+
+    # batching efficiency of the step machinery alone: the same ensemble and one
+    # large instance, both without gravity (the direct solve's cost per cell
+    # grows with the side, so with gravity a large grid is slower per cell)
+    def timed_batch(plist, slist, nsteps):
+        with BatchSolver(plist) as bb:
+            bb.set_stream(stream.cuda_stream)
+            for kk, st_ in enumerate(slist):
+                bb.upload(kk, *st_)
+            bb.autotune(reps=3)
+            bb.advance(args.warmup, np.zeros(len(plist)))
+            torch.cuda.synchronize()
+            e0.record(stream)
+            bb.advance(nsteps)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            return sum(q.Nx * q.Ny for q in plist) * nsteps / (e0.elapsed_time(e1) / 1000.0)
+
+    ng_steps = max(1, min(steps, 60))
+    ens_nograv = timed_batch([dc_replace(params[i], gravity_on=False) for i in mine], [states[i] for i in mine],
+                             ng_steps)
+    big = args.ensemble_nograv_side
+    pb = dc_replace(params[0], Nx=big, Ny=big, eta=1e-3, gravity_on=False)
+    single_nograv = timed_batch([pb], [ic_collapse(pb, core_amp=9.0, core_width=0.1, noise=0.01, seed=0, Bx0=0.05)],
+                                ng_steps)
     out.update({"value": value, "unit": UNIT, "ms_per_step": ms / steps,
                 "single_grid": {"workload": f"one {ns}^2 collapse instance (core 9, width 0.1, Bx 0.05, eta 1e-3), "
                                             "outflow, direct Poisson, FP32, same handle type",
                                 "value": single_value, "unit": UNIT},
                 "ensemble_over_single_grid": value / world / single_value,
                 "ensemble_over_single_fft_grid": value / world / single_fp32 if single_fp32 else None,
+                "no_gravity": {"steps": ng_steps, "ensemble_value": ens_nograv,
+                               "single_grid": f"one {big}^2 instance, same handle type",
+                               "single_value": single_nograv, "ensemble_over_single_grid": ens_nograv / single_nograv},
                 "tile": [info["tile_x"], info["tile_y"]], "autotune_choice": shape, "autotune_stage_ms": tune_ms,
                 "stage_ctas": info["stage_ctas"], "stage_tiles": info["stage_tiles"],
                 # stage-kernel time per step (events around the stage launches of 3 eager
@@ -850,6 +878,7 @@ def main():
     ap.add_argument("--ensemble", type=int, default=512)
     ap.add_argument("--ensemble-steps", type=int, default=300)
     ap.add_argument("--ensemble-single-side", type=int, default=2048)
+    ap.add_argument("--ensemble-nograv-side", type=int, default=4096)
     ap.add_argument("--skip-adjoint", action="store_true")
     ap.add_argument("--adjoint-grid", type=int, default=512)
     ap.add_argument("--adjoint-steps", type=int, default=100)
