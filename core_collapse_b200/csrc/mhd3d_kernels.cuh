@@ -225,10 +225,10 @@ __global__ void __launch_bounds__(256) m3_face_kernel(const M3Const<T> c, const 
 // clamped one it differs only at the boundary faces (0 and n), which take the
 // original path.
 constexpr int M3_FACE_MCH = 32;
-template <class T, int DIR>
 // (FP32 only) capped at 64 registers, four CTAs per SM: a few spilled values
 // cost less than the latency a 98-register, two-CTA launch leaves exposed
 // (256^3 FP32 step 7.26 -> 6.74 ms; 80 registers without spills: 6.80 ms)
+template <class T, int DIR>
 __global__ void __launch_bounds__(256, 4) m3_face_march_kernel(const M3Const<T> c, const Fields3<T> s,
                                                             const PrimData<T> pr, const FaceData<T> out,
                                                             const int* __restrict__ active) {
