@@ -232,17 +232,35 @@ class ClockSampler:
 
 # ---------------------------------------------------------------- GPU arm
 
-def traffic_per_launch(grid: int):
-    """DRAM bytes per stage-kernel launch from the committed ncu capture,
-    scaled to the benchmark grid by cell count (traffic grows with cells)."""
+def stage_capture(grid: int, key: str):
+    """A per-launch figure of the stage kernel (DRAM bytes, warp instructions)
+    from the committed ncu capture, scaled to the benchmark grid by cell count
+    (both grow with the cells: every tile reads its halo once and runs the same
+    work per cell)."""
     f = ROOT / "profiles" / "stage_kernel_traffic.json"
     if not f.exists():
         return None
     d = json.loads(f.read_text())
     try:
-        return float(d["dram_bytes_per_launch"]) * (grid * grid) / float(d["cells"])
+        return float(d[key]) * (grid * grid) / float(d["cells"])
     except Exception:
         return None
+
+
+def traffic_per_launch(grid: int):
+    return stage_capture(grid, "dram_bytes_per_launch")
+
+
+def issue_roofline(grid: int, launch_ms: float, clk) -> dict | None:
+    """The stage kernel's instruction-issue bound: its warp instructions per
+    launch (ncu capture, scaled to the grid) over 148 SMs x 4 schedulers x one
+    instruction per cycle at the SM clock sampled during the timed region."""
+    inst = stage_capture(grid, "warp_instructions_per_launch")
+    mhz = (clk or {}).get("sm_mhz") or (clk or {}).get("sm_max_mhz") or 1965
+    if not inst or not launch_ms:
+        return None
+    ms = inst / (148 * 4 * mhz * 1e6) * 1e3
+    return {"warp_instructions_per_launch": inst, "sm_mhz": mhz, "bound_ms": ms, "frac": ms / launch_ms}
 
 
 def run_ours(args) -> None:
@@ -371,7 +389,8 @@ def run_ours(args) -> None:
                      "frac": achieved / peaks["hbm_gbs"], "peak_source": peaks["source"],
                      "traffic": traffic_per_launch(n), "algorithmic_bytes_per_launch": stage_bytes,
                      "launch_ms": stage_avg_ms,
-                     "step_roofline_frac": STEP_WORDS * 4 * value32 / world / 1e9 / peaks["hbm_gbs"]},
+                     "step_roofline_frac": STEP_WORDS * 4 * value32 / world / 1e9 / peaks["hbm_gbs"],
+                     "issue": issue_roofline(n, stage_avg_ms, clk)},
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": h2d,
                 "steps": e2e_steps, "api": "cc_mhd2d_upload + cc_mhd2d_advance(1) + cc_mhd2d_download, pinned FP64 host"},
         "gpu_launches": perf32["kernel_launches"],
