@@ -190,7 +190,7 @@ adj_update_kernel(const M2Const<T> c, const Fields<T> sin, const Fields<T> sout,
             const int iE = c.ax.cell(i + 1), iW = c.ax.cell(i - 1), jN = c.ay.cell(j + 1), jS = c.ay.cell(j - 1);
             const T gx = -(phi[(size_t)j * P + iE] - phi[(size_t)j * P + iW]) / c.two_dx;
             const T gy = -(phi[(size_t)jN * P + i] - phi[(size_t)jS * P + i]) / c.two_dy;
-            const T rv = vmax(rho, T(1e-300));
+            const T rv = vmax(rho, tiny_pos<T>());
             const T u = rmx / rv, v = rmy / rv;
             const T kmx = rmx + dt * rho * gx, kmy = rmy + dt * rho * gy;
             const T kE = E + dt * rho * (u * gx + v * gy);
@@ -207,7 +207,7 @@ adj_update_kernel(const M2Const<T> c, const Fields<T> sin, const Fields<T> sout,
             const T lgy = dt * rho * lkmy + dt * rho * v * lkE;
             l1 = lkmx + lu / rv;
             l2 = lkmy + lv / rv;
-            if (!(rho < T(1e-300))) l0 -= (lu * u + lv * v) / rv;
+            if (!(rho < tiny_pos<T>())) l0 -= (lu * u + lv * v) / rv;
             aadd(lphi + (size_t)j * P + iE, -lgx / c.two_dx);
             aadd(lphi + (size_t)j * P + iW, lgx / c.two_dx);
             aadd(lphi + (size_t)jN * P + i, -lgy / c.two_dy);

@@ -62,7 +62,9 @@ adj_sor_start_kernel(SorAdjArgs a, const T* __restrict__ lphi, int P, double* __
 }
 
 // one transposed half-sweep of colour COLOR ((i + j) & 1 == COLOR updated);
-// MEAN: read mu_in minus the mean of the partial sums; SUMS: partial sums of mu_out
+// MEAN: read mu_in minus the mean of the partial sums; SUMS: partial sums of
+// mu_out.  A block works whole rows (coalesced, no index division), the
+// updated cells of a row and then the others (no divergence between them).
 template <int COLOR, bool MEAN, bool SUMS>
 __global__ void __launch_bounds__(ASOR_NT)
 adj_sor_half_kernel(SorAdjArgs a, const double* __restrict__ mu_in, double* __restrict__ mu_out) {
@@ -70,40 +72,53 @@ adj_sor_half_kernel(SorAdjArgs a, const double* __restrict__ mu_in, double* __re
     __shared__ double s_m;
     double m = 0.0;
     if constexpr (MEAN) {
-        if (threadIdx.x == 0) {
+        if (threadIdx.x < 32) {   // one warp sums the partials (fixed order)
             double t = 0.0;
-            for (int b = 0; b < (int)gridDim.x; b++) t += a.part[b];
-            s_m = t / ((double)a.nx * (double)a.ny);
+            for (int b = threadIdx.x; b < (int)gridDim.x; b += 32) t += a.part[b];
+            for (int o = 16; o > 0; o >>= 1) t += __shfl_down_sync(0xffffffffu, t, o);
+            if (threadIdx.x == 0) s_m = t / ((double)a.nx * (double)a.ny);
         }
         __syncthreads();
         m = s_m;
         __syncthreads();   // every block reads part before any block writes it (SUMS is off here)
     }
     const double k1 = a.omega / a.denom;
+    const int nh = (a.nx + 1) / 2;
     double s = 0.0;
-    for (int k = blockIdx.x * ASOR_NT + threadIdx.x; k < a.nx * a.ny; k += gridDim.x * ASOR_NT) {
-        const int i = k % a.nx, j = k / a.nx;
-        const double mq = mu_in[k] - m;
-        const int iE = a.ax.cell(i + 1), iW = a.ax.cell(i - 1), jN = a.ay.cell(j + 1), jS = a.ay.cell(j - 1);
-        double v;
-        if (((i + j) & 1) == COLOR) {
-            double self = 0.0;
-            if (iE == i) self += a.idx2;
-            if (iW == i) self += a.idx2;
-            if (jN == j) self += a.idy2;
-            if (jS == j) self += a.idy2;
-            v = (1.0 - a.omega) * mq + k1 * self * mq;
-            a.rhat[k] -= k1 * mq;
-        } else {
-            double acc = 0.0;
-            if (iE != i) acc += a.idx2 * (mu_in[(size_t)j * a.nx + iE] - m);
-            if (iW != i) acc += a.idx2 * (mu_in[(size_t)j * a.nx + iW] - m);
-            if (jN != j) acc += a.idy2 * (mu_in[(size_t)jN * a.nx + i] - m);
-            if (jS != j) acc += a.idy2 * (mu_in[(size_t)jS * a.nx + i] - m);
-            v = mq + k1 * acc;
+    for (int j = blockIdx.x; j < a.ny; j += gridDim.x) {
+        const int jN = a.ay.cell(j + 1), jS = a.ay.cell(j - 1);
+        const double* rowC = mu_in + (size_t)j * a.nx;
+        const double* rowN = mu_in + (size_t)jN * a.nx;
+        const double* rowS = mu_in + (size_t)jS * a.nx;
+        double* out = mu_out + (size_t)j * a.nx;
+        double* rh = a.rhat + (size_t)j * a.nx;
+        const double yself = (jN == j ? a.idy2 : 0.0) + (jS == j ? a.idy2 : 0.0);
+        // updated cells: (1 - omega + omega w_self / den) mu, and -omega/den mu into rhat
+        for (int t = threadIdx.x; t < nh; t += ASOR_NT) {
+            const int i = 2 * t + ((COLOR + j) & 1);
+            if (i >= a.nx) continue;
+            const int iE = a.ax.cell(i + 1), iW = a.ax.cell(i - 1);
+            const double self = yself + (iE == i ? a.idx2 : 0.0) + (iW == i ? a.idx2 : 0.0);
+            const double mq = rowC[i] - m;
+            const double v = (1.0 - a.omega) * mq + k1 * self * mq;
+            rh[i] -= k1 * mq;
+            out[i] = v;
+            s += v;
         }
-        mu_out[k] = v;
-        s += v;
+        // the other cells gather the updated neighbours that read them
+        for (int t = threadIdx.x; t < nh; t += ASOR_NT) {
+            const int i = 2 * t + ((COLOR + j + 1) & 1);
+            if (i >= a.nx) continue;
+            const int iE = a.ax.cell(i + 1), iW = a.ax.cell(i - 1);
+            double acc = 0.0;
+            if (iE != i) acc += a.idx2 * (rowC[iE] - m);
+            if (iW != i) acc += a.idx2 * (rowC[iW] - m);
+            if (jN != j) acc += a.idy2 * (rowN[i] - m);
+            if (jS != j) acc += a.idy2 * (rowS[i] - m);
+            const double v = (rowC[i] - m) + k1 * acc;
+            out[i] = v;
+            s += v;
+        }
     }
     if constexpr (SUMS) {
         s = block_sum<ASOR_NT>(s, sh);

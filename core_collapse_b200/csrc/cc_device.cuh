@@ -13,6 +13,11 @@ namespace ccb {
 template <class T> __host__ __device__ __forceinline__ T vmax(T a, T b) { return (a < b) ? b : a; }
 template <class T> __host__ __device__ __forceinline__ T vmin(T a, T b) { return (b < a) ? b : a; }
 
+// The reference's positive guard 1e-300 (a division or square-root floor); FP32
+// cannot hold it and its instantiations use 1e-30, a normal FP32 value far
+// below every density floor
+template <class T> __host__ __device__ constexpr T tiny_pos() { return sizeof(T) == 4 ? T(1e-30f) : T(1e-300); }
+
 __host__ __device__ __forceinline__ int wrap_idx(int i, int n) { int r = i % n; return (r < 0) ? r + n : r; }
 __host__ __device__ __forceinline__ int clamp_idx(int i, int lo, int hi) { return i < lo ? lo : (i > hi ? hi : i); }
 

@@ -47,7 +47,7 @@ CC_HD void fast_speed_vjp(const M2Const<T>& c, const Prim<T>& W, T bn, T lcf, Pr
     const T rf = vmax(W.r, c.floor_rho);
     const T a2 = c.gamma * W.P / rf;
     const T b2 = W.bx * W.bx + W.by * W.by + W.bz * W.bz;
-    const T rr = vmax(W.r, T(1e-300));
+    const T rr = vmax(W.r, tiny_pos<T>());
     const T vA2 = b2 / rr;
     const T vn2 = (bn * bn) / rr;
     const T s = a2 + vA2;
@@ -69,7 +69,7 @@ CC_HD void fast_speed_vjp(const M2Const<T>& c, const Prim<T>& W, T bn, T lcf, Pr
     const T lb2 = lvA2 * i_rr;
     const T lrr = -(lvA2 * vA2 + lvn2 * vn2) * i_rr;
     lbn += T(2) * bn * lvn2 * i_rr;
-    if (!(W.r < T(1e-300))) lW.r += lrr;
+    if (!(W.r < tiny_pos<T>())) lW.r += lrr;
     lW.P += c.gamma * la2 * i_rf;
     const T lrf = -la2 * a2 * i_rf;
     if (!(W.r < c.floor_rho)) lW.r += lrf;
@@ -203,8 +203,8 @@ CC_HD void hlld_x_vjp(const M2Const<T>& c, Prim<T> L, Prim<T> R, const T Bn, con
                 vRs = R.v - Bn * (ByRs - R.by) / ddR;
                 wRs = R.w - Bn * (BzRs - R.bz) / ddR;
             }
-            const T sqL = sqrt(vmax(rLs, T(1e-300)));
-            const T sqR = sqrt(vmax(rRs, T(1e-300)));
+            const T sqL = sqrt(vmax(rLs, tiny_pos<T>()));
+            const T sqR = sqrt(vmax(rRs, tiny_pos<T>()));
             const T SLL = SM - fabs(Bn) / sqL;
             const T SRR = SM + fabs(Bn) / sqR;
             const bool left = (T(0.0) < SM);
@@ -316,8 +316,8 @@ CC_HD void hlld_x_vjp(const M2Const<T>& c, Prim<T> L, Prim<T> R, const T Bn, con
                 lsqL += ld2;
                 lsqR += ld2;
             }
-            if (!(rLs < T(1e-300)) && sqL > T(0)) lrLs += lsqL / (T(2) * sqL);
-            if (!(rRs < T(1e-300)) && sqR > T(0)) lrRs += lsqR / (T(2) * sqR);
+            if (!(rLs < tiny_pos<T>()) && sqL > T(0)) lrLs += lsqL / (T(2) * sqL);
+            if (!(rRs < tiny_pos<T>()) && sqR > T(0)) lrRs += lsqR / (T(2) * sqR);
             // star states of each side (M2:424-442)
             T ldL = T(0), ldR = T(0), lbn2 = T(0), lsL = T(0), lsR = T(0);
             if (starL) {

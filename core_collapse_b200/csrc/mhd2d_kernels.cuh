@@ -268,6 +268,32 @@ __device__ __forceinline__ void m2_stage_tile(const M2Const<T>& c, const Fields<
         W.P = vmax(W.P, c.floor_P);
         return W;
     };
+    // FP32: the two face states of a face (cell kl's high side, cell kr's low
+    // side) as packed pairs, already in hlld_x orientation (for a y face the
+    // (u,v)/(Bx,By) swap of hlld_y; its Bx slot is set to Bn by hlld_x2)
+    // (generic, so that only the FP32 instantiation forms it)
+    auto face_pair = [&](auto kl, int ol, int kr, int orr, bool ydir) {
+        const T* sl = ydir ? sly : slx;
+        const float2 h = pk(0.5f, -0.5f);
+        auto rec = [&](const T* v, int m) {
+            return pfma(h, pk(sl[m * NSL + ol], sl[m * NSL + orr]), pk(v[kl], v[kr]));
+        };
+        auto ctr = [&](const T* v) { return pk(v[kl], v[kr]); };
+        Prim2 S;
+        S.r = rec(s_r, 0);
+        S.P = rec(s_P, 4);
+        S.w = rec(s_w, 3);
+        S.bz = rec(s_bz, 6);
+        if (ydir) {
+            S.u = rec(s_v, 2); S.v = rec(s_u, 1); S.by = rec(s_bx, 5); S.bx = ctr(s_by);
+        } else {
+            S.u = rec(s_u, 1); S.v = rec(s_v, 2); S.by = rec(s_by, 5); S.bx = ctr(s_bx);
+        }
+        const float fr = (float)c.floor_rho, fp = (float)c.floor_P;
+        S.r.x = vmax(S.r.x, fr); S.r.y = vmax(S.r.y, fr);
+        S.P.x = vmax(S.P.x, fp); S.P.y = vmax(S.P.y, fp);
+        return S;
+    };
 
     auto x_slopes = [&](int k) {
         const int lx = k % (TX + 2) - 1, ly = k / (TX + 2) - 1;
@@ -283,9 +309,15 @@ __device__ __forceinline__ void m2_stage_tile(const M2Const<T>& c, const Fields<
         const int gi = i0 + f;
         if (gi > c.nx) return;
         const int cj = c.ay.cell(j0 + r);
-        const Prim<T> WL = face_state(ridx(f - 1, r), sidx(f - 1, r), false, T(1));
-        const Prim<T> WR = face_state(ridx(f, r), sidx(f, r), false, T(-1));
-        const Flux<T> F = hlld_x(c, WL, WR, in.bx[(size_t)cj * P + gi]);
+        Flux<T> F;
+        if constexpr (std::is_same<T, float>::value) {
+            F = hlld_x2(c, face_pair(ridx(f - 1, r), sidx(f - 1, r), ridx(f, r), sidx(f, r), false),
+                        in.bx[(size_t)cj * P + gi]);
+        } else {
+            const Prim<T> WL = face_state(ridx(f - 1, r), sidx(f - 1, r), false, T(1));
+            const Prim<T> WR = face_state(ridx(f, r), sidx(f, r), false, T(-1));
+            F = hlld_x(c, WL, WR, in.bx[(size_t)cj * P + gi]);
+        }
         fx[k] = F.f0; fx[NFX + k] = F.f1; fx[2 * NFX + k] = F.f2; fx[3 * NFX + k] = F.f3;
         fx[4 * NFX + k] = F.f4; fx[5 * NFX + k] = F.f5; fx[6 * NFX + k] = F.f6;
     };
@@ -295,9 +327,16 @@ __device__ __forceinline__ void m2_stage_tile(const M2Const<T>& c, const Fields<
         const int gj = j0 + g;
         if (gj > c.ny) return;
         const int ci = c.ax.cell(i0 + col);
-        const Prim<T> WL = face_state(ridx(col, g - 1), sidx(col, g - 1), true, T(1));
-        const Prim<T> WR = face_state(ridx(col, g), sidx(col, g), true, T(-1));
-        const Flux<T> Gf = hlld_y(c, WL, WR, in.by[(size_t)gj * P + ci]);
+        Flux<T> Gf;
+        if constexpr (std::is_same<T, float>::value) {
+            Gf = hlld_x2(c, face_pair(ridx(col, g - 1), sidx(col, g - 1), ridx(col, g), sidx(col, g), true),
+                         in.by[(size_t)gj * P + ci]);
+            const T t = Gf.f1; Gf.f1 = Gf.f2; Gf.f2 = t;   // hlld_y's swap back
+        } else {
+            const Prim<T> WL = face_state(ridx(col, g - 1), sidx(col, g - 1), true, T(1));
+            const Prim<T> WR = face_state(ridx(col, g), sidx(col, g), true, T(-1));
+            Gf = hlld_y(c, WL, WR, in.by[(size_t)gj * P + ci]);
+        }
         gy[k] = Gf.f0; gy[NGY + k] = Gf.f1; gy[2 * NGY + k] = Gf.f2; gy[3 * NGY + k] = Gf.f3;
         gy[4 * NGY + k] = Gf.f4; gy[5 * NGY + k] = Gf.f5; gy[6 * NGY + k] = Gf.f6;
     };
@@ -433,11 +472,11 @@ __device__ __forceinline__ void m2_stage_tile(const M2Const<T>& c, const Fields<
         }
         T u, v;
         if constexpr (fast_recip<T>()) {
-            const T ir = T(1.0) / vmax(rho, T(1e-300));
+            const T ir = T(1.0) / vmax(rho, tiny_pos<T>());
             u = mx * ir; v = my * ir;
         } else {
-            u = mx / vmax(rho, T(1e-300));
-            v = my / vmax(rho, T(1e-300));
+            u = mx / vmax(rho, tiny_pos<T>());
+            v = my / vmax(rho, tiny_pos<T>());
         }
         if constexpr (KAHAN) {
             comp_add(mx, lmx, dt * rho * gxq);

@@ -321,11 +321,11 @@ m2_march_kernel(const M2Const<T> c, const Fields<T> in, const Fields<T> out, con
                 }
                 T u, v;
                 if constexpr (fast_recip<T>()) {
-                    const T ir = T(1.0) / vmax(rho, T(1e-300));
+                    const T ir = T(1.0) / vmax(rho, tiny_pos<T>());
                     u = mx * ir; v = my * ir;
                 } else {
-                    u = mx / vmax(rho, T(1e-300));
-                    v = my / vmax(rho, T(1e-300));
+                    u = mx / vmax(rho, tiny_pos<T>());
+                    v = my / vmax(rho, tiny_pos<T>());
                 }
                 if constexpr (KAHAN) {
                     comp_add(mx, lmx, dt * rho * gxq);

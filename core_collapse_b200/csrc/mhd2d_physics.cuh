@@ -5,6 +5,8 @@
 // (cited M2:<line>); the double instantiation is compiled with -fmad=false so
 // that it rounds exactly like the reference's x86-64 build.
 #pragma once
+#include <type_traits>
+
 #include "cc_device.cuh"
 
 namespace ccb {
@@ -120,7 +122,7 @@ __host__ __device__ __forceinline__ T fast_speed(const M2Const<T>& c, const Prim
         vn2 = (bn * bn) * ir;
     } else {
         a2 = c.gamma * W.P / vmax(W.r, c.floor_rho);
-        const T rho = vmax(W.r, T(1e-300));
+        const T rho = vmax(W.r, tiny_pos<T>());
         vA2 = b2 / rho;
         vn2 = (bn * bn) / rho;
     }
@@ -172,7 +174,7 @@ __host__ __device__ __forceinline__ Flux<T> ideal_flux_ep(const Prim<T>& W, T E,
 // degenerate guards at 1e-14, HLL fallback for |Bn| < 1e-12, double-star
 // fluxes jumped from the outer state with the outer speed.
 template <class T, class Cst>
-__host__ __device__ __forceinline__ Flux<T> hlld_x(const Cst& c, Prim<T> L, Prim<T> R, T Bn) {
+__host__ __device__ __forceinline__ Flux<T> hlld_x_scalar(const Cst& c, Prim<T> L, Prim<T> R, T Bn) {
     L.bx = Bn; R.bx = Bn;
     const T cfL = fast_speed(c, L, Bn), cfR = fast_speed(c, R, Bn);
     const T SL = vmin(L.u - cfL, R.u - cfR);
@@ -256,8 +258,8 @@ __host__ __device__ __forceinline__ Flux<T> hlld_x(const Cst& c, Prim<T> L, Prim
         SLL = __fmaf_rn(-fabs(Bn), iqL, SM);
         SRR = __fmaf_rn(fabs(Bn), iqR, SM);
     } else {
-        sqL = sqrt(vmax(rLs, T(1e-300)));
-        sqR = sqrt(vmax(rRs, T(1e-300)));
+        sqL = sqrt(vmax(rLs, tiny_pos<T>()));
+        sqR = sqrt(vmax(rRs, tiny_pos<T>()));
         SLL = SM - fabs(Bn) / sqL;
         SRR = SM + fabs(Bn) / sqR;
     }
@@ -307,6 +309,156 @@ __host__ __device__ __forceinline__ Flux<T> hlld_x(const Cst& c, Prim<T> L, Prim
     F.f5 = F.f5 + S * (Bys - W.by);
     F.f6 = F.f6 + S * (Bzs - W.bz);
     return F;
+}
+
+// ---------------------------------------------------------------------------
+// HLLD of the 2D FP32 path on packed FP32 pairs.  sm_100 executes add, mul
+// and fma on a float2 (.f32x2) as one instruction; HLLD forms the same
+// quantities for its left and right states (fast speeds, energies, total
+// pressures, star states, Alfven speeds), so the FP32 path keeps each such
+// pair in one float2, .x the left state and .y the right, and spends one
+// issue slot where the scalar code spends two.  Each lane rounds like the
+// scalar FP32 code with its multiply-adds contracted (divisions, square roots
+// and comparisons stay scalar).  The region logic and the flux of the chosen
+// state follow hlld_x_scalar line for line.
+// ---------------------------------------------------------------------------
+struct Prim2 { float2 r, u, v, w, P, bx, by, bz; };   // .x left state, .y right state
+
+__device__ __forceinline__ float2 pk(float a, float b) { return make_float2(a, b); }
+__device__ __forceinline__ float2 pbc(float a) { return make_float2(a, a); }
+__device__ __forceinline__ float2 padd(float2 a, float2 b) { return __fadd2_rn(a, b); }
+// a - b as fma(b, -1, a): one rounding, the exact difference rounded
+__device__ __forceinline__ float2 psub(float2 a, float2 b) { return __ffma2_rn(b, pbc(-1.0f), a); }
+__device__ __forceinline__ float2 pmul(float2 a, float2 b) { return __fmul2_rn(a, b); }
+__device__ __forceinline__ float2 pfma(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+
+__device__ __forceinline__ Prim<float> lane_x(const Prim2& S) {
+    return Prim<float>{S.r.x, S.u.x, S.v.x, S.w.x, S.P.x, S.bx.x, S.by.x, S.bz.x};
+}
+__device__ __forceinline__ Prim<float> lane_y(const Prim2& S) {
+    return Prim<float>{S.r.y, S.u.y, S.v.y, S.w.y, S.P.y, S.bx.y, S.by.y, S.bz.y};
+}
+
+__device__ __forceinline__ Flux<float> hlld_x2(const M2Const<float>& c, Prim2 S, const float Bn) {
+    const float2 bn = pbc(Bn);
+    S.bx = bn;
+    // fast_speed of both states (M2:148-174)
+    const float2 bn2p = pmul(bn, bn);
+    const float2 b2 = pfma(S.bz, S.bz, pfma(S.by, S.by, bn2p));
+    const float2 ir = pk(1.0f / vmax(S.r.x, c.floor_rho), 1.0f / vmax(S.r.y, c.floor_rho));
+    const float2 a2 = pmul(pmul(pbc(c.gamma), S.P), ir);
+    const float2 vA2 = pmul(b2, ir);
+    const float2 vn2 = pmul(bn2p, ir);
+    const float2 sa = padd(a2, vA2);
+    const float2 disc = pfma(sa, sa, pmul(pmul(pbc(-4.0f), a2), vn2));
+    const float2 sd = pk(sqrtf(vmax(0.0f, disc.x)), sqrtf(vmax(0.0f, disc.y)));
+    const float2 cf2 = pmul(pbc(0.5f), padd(sa, sd));
+    const float2 cf = pk(sqrtf(vmax(0.0f, cf2.x)), sqrtf(vmax(0.0f, cf2.y)));
+    const float2 um = psub(S.u, cf), up = padd(S.u, cf);
+    const float SL = vmin(um.x, um.y);
+    const float SR = vmax(up.x, up.y);
+    if (0.0f <= SL) return ideal_flux(c, lane_x(S));
+    if (0.0f >= SR) return ideal_flux(c, lane_y(S));
+
+    // energies and total pressures (M2:357, 482, 495)
+    const float2 ksum = pfma(S.w, S.w, pfma(S.v, S.v, pmul(S.u, S.u)));
+    const float2 eint = pmul(S.P, pbc(1.0f / c.gm1));
+    const float2 E = pfma(pbc(0.5f), b2, pfma(pmul(pbc(0.5f), S.r), ksum, eint));
+    const float2 pt = pfma(pbc(0.5f), b2, S.P);
+
+    if (fabsf(Bn) < 1e-12f) {  // HLL (M2:449-467)
+        const Prim<float> L = lane_x(S), R = lane_y(S);
+        const Flux<float> FL = ideal_flux(c, L), FR = ideal_flux(c, R);
+        const float inv = 1.0f / (SR - SL);
+        const float s2 = SL * SR;
+        Flux<float> F;
+        F.f0 = (SR * FL.f0 - SL * FR.f0 + s2 * (R.r - L.r)) * inv;
+        F.f1 = (SR * FL.f1 - SL * FR.f1 + s2 * (R.r * R.u - L.r * L.u)) * inv;
+        F.f2 = (SR * FL.f2 - SL * FR.f2 + s2 * (R.r * R.v - L.r * L.v)) * inv;
+        F.f3 = (SR * FL.f3 - SL * FR.f3 + s2 * (R.r * R.w - L.r * L.w)) * inv;
+        F.f4 = (SR * FL.f4 - SL * FR.f4 + s2 * (E.y - E.x)) * inv;
+        F.f5 = (SR * FL.f5 - SL * FR.f5 + s2 * (R.by - L.by)) * inv;
+        F.f6 = (SR * FL.f6 - SL * FR.f6 + s2 * (R.bz - L.bz)) * inv;
+        return F;
+    }
+
+    // contact speed and star states (M2:470-505)
+    const float2 SLR = pk(SL, SR);
+    const float2 sLR = psub(SLR, S.u);          // SL - uL, SR - uR
+    const float2 rsd = pmul(S.r, sLR);          // rho (S - u) of each side
+    const float den = rsd.x - rsd.y;
+    float SM = 0.0f;
+    if (fabsf(den) > 1e-14f) {
+        const float2 m = pmul(pmul(S.r, S.u), sLR);
+        SM = (pt.y - pt.x + m.x - m.y) / den;
+    }
+    const float2 SmM = psub(SLR, pbc(SM));     // S - SM of each side
+    const float2 rst = pk(rsd.x / SmM.x, rsd.y / SmM.y);
+    const float pts = pt.x + rsd.x * (SM - S.u.x);
+    const float bn2 = Bn * Bn;
+    const float2 dLR = pfma(rsd, SmM, pbc(-bn2));
+    const float2 num = pfma(rsd, sLR, pbc(-bn2));
+    const float2 dd = pmul(rsd, SmM);
+    const float2 q = pk(num.x / dLR.x, num.y / dLR.y);
+    const float2 bq = pk(Bn / dd.x, Bn / dd.y);
+    float2 Bys2 = pmul(S.by, q), Bzs2 = pmul(S.bz, q);
+    float2 vs2 = pfma(psub(S.by, Bys2), bq, S.v);
+    float2 ws2 = pfma(psub(S.bz, Bzs2), bq, S.w);
+    if (!(fabsf(dLR.x) > 1e-14f)) { Bys2.x = S.by.x; Bzs2.x = S.bz.x; vs2.x = S.v.x; ws2.x = S.w.x; }
+    if (!(fabsf(dLR.y) > 1e-14f)) { Bys2.y = S.by.y; Bzs2.y = S.bz.y; vs2.y = S.v.y; ws2.y = S.w.y; }
+    const float2 rl = pk(vmax(rst.x, 1e-30f), vmax(rst.y, 1e-30f));
+    const float2 iq = pk(rsqrtf(rl.x), rsqrtf(rl.y));
+    const float2 sq = pmul(rl, iq);                                  // sqrt(rho*) of each side
+    const float2 SAl = pfma(pk(-fabsf(Bn), fabsf(Bn)), iq, pbc(SM));  // SL*, SR*
+
+    // the region, then only the state it needs (as hlld_x_scalar)
+    const bool left = (0.0f < SM);
+    const bool outer = left ? (0.0f < SAl.x) : !(0.0f < SAl.y);
+    const Prim<float> W = prim_select(left, lane_x(S), lane_y(S));
+    const float Sw = left ? SL : SR;
+    const float EW = left ? E.x : E.y;
+    const float ptW = left ? pt.x : pt.y;
+    const float rs = left ? rst.x : rst.y;
+    float vs, ws, Bys, Bzs;
+    if (outer) {
+        vs = left ? vs2.x : vs2.y; ws = left ? ws2.x : ws2.y;
+        Bys = left ? Bys2.x : Bys2.y; Bzs = left ? Bzs2.x : Bzs2.y;
+    } else {
+        const float sgn = (Bn >= 0.0f) ? 1.0f : -1.0f;
+        const float id2 = 1.0f / (sq.x + sq.y);
+        vs = (sq.x * vs2.x + sq.y * vs2.y + (Bys2.y - Bys2.x) * sgn) * id2;
+        ws = (sq.x * ws2.x + sq.y * ws2.y + (Bzs2.y - Bzs2.x) * sgn) * id2;
+        Bys = (sq.x * Bys2.y + sq.y * Bys2.x + sq.x * sq.y * (vs2.y - vs2.x) * sgn) * id2;
+        Bzs = (sq.x * Bzs2.y + sq.y * Bzs2.x + sq.x * sq.y * (ws2.y - ws2.x) * sgn) * id2;
+    }
+    const float vBs = SM * Bn + vs * Bys + ws * Bzs;
+    const float vBw = W.u * W.bx + W.v * W.by + W.w * W.bz;
+    const float Es = ((Sw - W.u) * EW - (ptW * W.u - Bn * vBw) + (pts * SM - Bn * vBs)) / (Sw - SM);
+    Flux<float> F = ideal_flux(c, W);
+    F.f0 = F.f0 + Sw * (rs - W.r);
+    F.f1 = F.f1 + Sw * (rs * SM - W.r * W.u);
+    F.f2 = F.f2 + Sw * (rs * vs - W.r * W.v);
+    F.f3 = F.f3 + Sw * (rs * ws - W.r * W.w);
+    F.f4 = F.f4 + Sw * (Es - EW);
+    F.f5 = F.f5 + Sw * (Bys - W.by);
+    F.f6 = F.f6 + Sw * (Bzs - W.bz);
+    return F;
+}
+
+// HLLD of a face: the packed form on the 2D FP32 device path, else the scalar one
+template <class T, class Cst>
+__host__ __device__ __forceinline__ Flux<T> hlld_x(const Cst& c, const Prim<T>& L, const Prim<T>& R, T Bn) {
+#if defined(__CUDA_ARCH__)
+    if constexpr (std::is_same<Cst, M2Const<float>>::value) {
+        const Prim2 S{pk(L.r, R.r), pk(L.u, R.u), pk(L.v, R.v), pk(L.w, R.w),
+                      pk(L.P, R.P), pk(L.bx, R.bx), pk(L.by, R.by), pk(L.bz, R.bz)};
+        return hlld_x2(c, S, Bn);
+    } else {
+        return hlld_x_scalar(c, L, R, Bn);
+    }
+#else
+    return hlld_x_scalar(c, L, R, Bn);
+#endif
 }
 
 // y-normal HLLD through the (u,v)/(Bx,By) swap (M2:540-561).  Returns

@@ -142,7 +142,7 @@ __device__ __forceinline__ T fast_speed(const M3Const<T>& c, const Prim<T>& W, T
     const T num = cd.g * cd.P + c.gth * Pth;
     const T a2 = vmax(T(0.0), num / rhof);
     const T b2 = W.bx * W.bx + W.by * W.by + W.bz * W.bz;
-    const T rho = vmax(W.r, T(1e-300));
+    const T rho = vmax(W.r, tiny_pos<T>());
     const T ir = recip_if_fast(rho);
     const T vA2 = div_or_mul(b2, rho, ir);
     const T vn2 = div_or_mul(bn * bn, rho, ir);
