@@ -145,8 +145,105 @@ __device__ __forceinline__ void f32_fft_line(float2* a, int n, const float2* __r
     }
 }
 
+// ---------------------------------------------------------------------------
+// Register hand-offs (lines of n >= 256 points, every thread of the CTA
+// active, tl = n / 16 threads per line).  The first pass of the transform
+// (radix 16, Ns = 1) reads x[lt + r tl], r < 16: exactly the values a thread
+// fetches with coalesced global loads, so it can start from registers.  The
+// last pass (radix RL) leaves X[lt + fft32_fmap<RL>(q) tl] in the thread's
+// register q: coalesced again, so the last pass can feed the next step (the
+// spectral factor, the inverse transform's first pass, the global store)
+// from registers.  This removes the staging round trips through shared
+// memory and their barriers; the arithmetic, and so every value, is that of
+// f32_fft_line.
+// ---------------------------------------------------------------------------
+template <int RL> __host__ __device__ constexpr int fft32_fmap(int q) { return q / RL + (q % RL) * (16 / RL); }
+// radix of the last pass of an n-point transform (16 when n is a power of 16)
+__host__ __device__ constexpr int fft32_last_radix(int n) {
+    int l = 0;
+    while ((1 << l) < n) ++l;
+    return (l % 4 == 0) ? 16 : (1 << (l % 4));
+}
+
+// One Stockham pass as f32_pass (V = 16), with its input from registers
+// (IN_REG: v[g R + r] = x[j + r n / R], j = lt + g tl) and / or its output
+// left in registers (OUT_REG: v[g R + s] = X[base + s Ns]).  Barriers: one
+// after the shared-memory writes; one between the reads and the writes of an
+// in-place pass.  A pass that reads from registers writes without a barrier
+// first, so the caller makes sure nobody still reads the line.
+template <int R, bool INV, bool IN_REG, bool OUT_REG>
+__device__ __forceinline__ void f32_pass_rw(float2* a, float2 (&v)[16], int n, int Ns,
+                                            const float2* __restrict__ roots, int lt, int tl) {
+    constexpr int G = 16 / R;
+    const int nb = n / R;
+    if constexpr (!IN_REG) {
+#pragma unroll
+        for (int g = 0; g < G; g++) {
+            const int j = lt + g * tl;
+#pragma unroll
+            for (int r = 0; r < R; r++) v[g * R + r] = a[fft32_pad(j + r * nb)];
+        }
+        if constexpr (!OUT_REG) __syncthreads();
+    }
+    const int span = n / (Ns * R);
+#pragma unroll
+    for (int g = 0; g < G; g++) {
+        const int j = lt + g * tl;
+        const int k = j & (Ns - 1);
+        if (Ns > 1) {
+#pragma unroll
+            for (int r = 1; r < R; r++) v[g * R + r] = f2twiddle<INV>(v[g * R + r], __ldg(&roots[r * k * span]));
+        }
+        f32_dft<R, INV>(&v[g * R]);
+        if constexpr (!OUT_REG) {
+            const int base = (j - k) * R + k;
+#pragma unroll
+            for (int s = 0; s < R; s++) a[fft32_pad(base + s * Ns)] = v[g * R + s];
+        }
+    }
+    if constexpr (!OUT_REG) __syncthreads();
+}
+
+// Whole transform of a line, ending in registers: v[q] = X[lt + fft32_fmap<RL>(q) tl]
+// on exit.  IN_REG: v[r] = x[lt + r tl] on entry, else the line is in shared memory.
+// RL = fft32_last_radix(n).
+template <int RL, bool INV, bool IN_REG>
+__device__ __forceinline__ void f32_fft_regs(float2* a, float2 (&v)[16], int n, const float2* __restrict__ roots,
+                                             int lt) {
+    const int tl = n / 16;
+    int Ns = 1;
+    if constexpr (IN_REG) {
+        f32_pass_rw<16, INV, true, false>(a, v, n, 1, roots, lt, tl);
+        Ns = 16;
+    }
+    while (n / Ns > RL) {
+        f32_pass_rw<16, INV, false, false>(a, v, n, Ns, roots, lt, tl);
+        Ns *= 16;
+    }
+    f32_pass_rw<RL, INV, false, true>(a, v, n, Ns, roots, lt, tl);
+}
+
+// Whole transform of a line from registers (v[r] = x[lt + r tl]) into shared
+// memory (natural order), the rest as f32_fft_line.
+template <bool INV>
+__device__ __forceinline__ void f32_fft_from_regs(float2* a, float2 (&v)[16], int n, const float2* __restrict__ roots,
+                                                  int lt) {
+    const int tl = n / 16;
+    f32_pass_rw<16, INV, true, false>(a, v, n, 1, roots, lt, tl);
+    int Ns = 16;
+    while (n / Ns >= 16) {
+        f32_pass<16, 16, INV>(a, n, Ns, roots, lt, tl, true);
+        Ns *= 16;
+    }
+    const int rem = n / Ns;
+    if (rem == 8) f32_pass<8, 16, INV>(a, n, Ns, roots, lt, tl, true);
+    else if (rem == 4) f32_pass<4, 16, INV>(a, n, Ns, roots, lt, tl, true);
+    else if (rem == 2) f32_pass<2, 16, INV>(a, n, Ns, roots, lt, tl, true);
+}
+
 // pass 1: rows 2b and 2b+1 -> half spectra.  rho pitched; mean = sum/N.
-template <class F>   // F = float (a template so that only the FP32 unit instantiates it)
+// REG: the first pass starts from the loaded registers (blockDim = nx / 16).
+template <class F, bool REG>   // F = float (a template so that only the FP32 unit instantiates it)
 __global__ void __maxnreg__(80)   // three 256-thread CTAs per SM; blocks of up to FFT32_MAXT threads
 f32_rows_fwd_kernel(const F* __restrict__ rho, int pitch, const double* __restrict__ rho_part, int nparts,
                     double ncell, float2* __restrict__ A, int nx, int ny, const float2* __restrict__ roots,
@@ -173,14 +270,21 @@ f32_rows_fwd_kernel(const F* __restrict__ rho, int pitch, const double* __restri
     }
     __syncthreads();
     const float mean = (float)s_mean;
+    if constexpr (REG) {
+        float2 v[16];
 #pragma unroll
-    for (int q = 0; q < 16; q++) {
-        const int i = threadIdx.x + q * blockDim.x;
-        if (i < nx) a[fft32_pad(i)] = make_float2(ra[q] - mean, rb[q] - mean);
+        for (int q = 0; q < 16; q++) v[q] = make_float2(ra[q] - mean, rb[q] - mean);
+        f32_fft_from_regs<false>(a, v, nx, roots, (int)threadIdx.x);
+    } else {
+#pragma unroll
+        for (int q = 0; q < 16; q++) {
+            const int i = threadIdx.x + q * blockDim.x;
+            if (i < nx) a[fft32_pad(i)] = make_float2(ra[q] - mean, rb[q] - mean);
+        }
+        __syncthreads();
+        const int tl = fft32_tpl(nx);
+        f32_fft_line<false>(a, nx, roots, (int)threadIdx.x, (int)threadIdx.x < tl);
     }
-    __syncthreads();
-    const int tl = fft32_tpl(nx);
-    f32_fft_line<false>(a, nx, roots, (int)threadIdx.x, (int)threadIdx.x < tl);
     // Z = FFT(x_a + i x_b):  X_a[k] = (Z[k] + conj Z[-k]) / 2,  X_b[k] = (Z[k] - conj Z[-k]) / (2 i)
     for (int k = threadIdx.x; k <= nx / 2; k += blockDim.x) {
         const float2 z = a[fft32_pad(k)], m = a[fft32_pad((nx - k) & (nx - 1))];
@@ -249,9 +353,64 @@ f32_cols_solve_kernel(float2* __restrict__ A, int nx, int ny, const float2* __re
     }
 }
 
+// pass 2 with register hand-offs (ny >= 256, blockDim = CW ny / 16): the
+// column's values go from global loads into the forward transform's first
+// pass, the forward transform's last pass hands its registers to the spectral
+// factor and on to the inverse transform's first pass, and the inverse's last
+// pass stores from registers (coalesced).  RL = fft32_last_radix(ny).
+// Two 256-thread CTAs per SM (up to 128 registers): the 16 values of a line
+// stay live across the hand-offs; at three CTAs (80 registers) they spill and
+// the pass is slower (4096^2 step 3.534 against 3.555 ms).
+template <int CW, int RL>
+__global__ void __launch_bounds__(CW == 1 && RL == 2 ? 512 : 256, CW == 1 && RL == 2 ? 1 : 2)
+f32_cols_rk_kernel(float2* __restrict__ A, int nx, int ny, const float2* __restrict__ roots, double Lx, double Ly,
+                   double G, const int* __restrict__ active) {
+    if (active && *active == 0) return;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    float2* a = reinterpret_cast<float2*>(smem_raw);
+    const int tl = ny / 16;
+    const int l = (int)threadIdx.x / tl, lt = (int)threadIdx.x % tl;
+    const int kx = blockIdx.x * CW + l;
+    const bool live = kx < nx / 2 + 1;
+    float2* line = a + l * fft32_line(ny);
+    float2* col = A + (size_t)kx * ny;
+    float2 v[16];
+#pragma unroll
+    for (int r = 0; r < 16; r++) v[r] = live ? col[lt + r * tl] : make_float2(0.0f, 0.0f);
+    f32_fft_regs<RL, false, true>(line, v, ny, roots, lt);
+    // spectral kernel (NS:308-322) on the registers, as in f32_cols_solve_kernel
+    const float fy = (float)(2.0 * M_PI / Ly), fx = (float)(2.0 * M_PI / Lx), g4 = (float)(4.0 * M_PI * G);
+    float2 w[16];
+#pragma unroll
+    for (int q = 0; q < 16; q++) {
+        const int j = lt + fft32_fmap<RL>(q) * tl;
+        const int nj = (j <= ny / 2) ? j : j - ny;
+        const float ky = fy * (float)nj, kxf = fx * (float)kx;
+        const float k2 = kxf * kxf + ky * ky;
+        float2 z = v[q];
+        if (k2 == 0.0f) {
+            z = make_float2(0.0f, 0.0f);
+        } else {
+            const float sf = -g4 / k2;
+            z.x = z.x * sf;
+            z.y = z.y * sf;
+        }
+        w[fft32_fmap<RL>(q)] = z;   // the inverse's first-pass order: w[r] = Z[lt + r tl]
+    }
+    __syncthreads();   // every thread's last forward reads of the line are done
+    f32_fft_regs<RL, true, true>(line, w, ny, roots, lt);
+    if (live) {
+        const float n = (float)ny;
+#pragma unroll
+        for (int q = 0; q < 16; q++) col[lt + fft32_fmap<RL>(q) * tl] = make_float2(w[q].x / n, w[q].y / n);
+    }
+}
+
 // pass 3: half spectra of rows 2b, 2b+1 -> Z = X_a + i X_b over all kx
 // (Hermitian completion), inverse FFT, phi_a = Re / nx, phi_b = Im / nx.
-template <class F>   // F = float (a template so that only the FP32 unit instantiates it)
+// RL > 0: the last pass stores phi from registers (blockDim = nx / 16,
+// RL = fft32_last_radix(nx)).
+template <class F, int RL>   // F = float (a template so that only the FP32 unit instantiates it)
 __global__ void __launch_bounds__(FFT32_MAXT)
 f32_rows_inv_kernel(const float2* __restrict__ A, int nx, int ny, const float2* __restrict__ roots,
                     F* __restrict__ phi, int pitch, const int* __restrict__ active) {
@@ -276,13 +435,25 @@ f32_rows_inv_kernel(const float2* __restrict__ A, int nx, int ny, const float2* 
         if (k > 0 && k < nx / 2) a[fft32_pad(nx - k)] = make_float2(xa.x + xb.y, xb.x - xa.y);
     }
     __syncthreads();
-    const int tl = fft32_tpl(nx);
-    f32_fft_line<true>(a, nx, roots, (int)threadIdx.x, (int)threadIdx.x < tl);
     const float n = (float)nx;
-    for (int i = threadIdx.x; i < nx; i += blockDim.x) {
-        const float2 z = a[fft32_pad(i)];
-        phi[(size_t)ja * pitch + i] = z.x / n;
-        phi[(size_t)jb * pitch + i] = z.y / n;
+    if constexpr (RL > 0) {
+        float2 v[16];
+        f32_fft_regs<RL, true, false>(a, v, nx, roots, (int)threadIdx.x);
+        const int tl = nx / 16;
+#pragma unroll
+        for (int q = 0; q < 16; q++) {
+            const int i = (int)threadIdx.x + fft32_fmap<RL>(q) * tl;
+            phi[(size_t)ja * pitch + i] = v[q].x / n;
+            phi[(size_t)jb * pitch + i] = v[q].y / n;
+        }
+    } else {
+        const int tl = fft32_tpl(nx);
+        f32_fft_line<true>(a, nx, roots, (int)threadIdx.x, (int)threadIdx.x < tl);
+        for (int i = threadIdx.x; i < nx; i += blockDim.x) {
+            const float2 z = a[fft32_pad(i)];
+            phi[(size_t)ja * pitch + i] = z.x / n;
+            phi[(size_t)jb * pitch + i] = z.y / n;
+        }
     }
 }
 

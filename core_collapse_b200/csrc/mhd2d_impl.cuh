@@ -62,8 +62,19 @@ cudaError_t M2Launch<T>::prepare(int nx, int ny) {
             const int row = (int)(sizeof(float2) * (size_t)fft32_line(nx));
             const int col = (int)(sizeof(float2) * (size_t)fft32_line(ny)) * fft32_cw(ny);
             if (row <= 227 * 1024 && col <= 227 * 1024) {
-                CC_ATTR(f32_rows_fwd_kernel<T>, row)
-                CC_ATTR(f32_rows_inv_kernel<T>, row)
+                CC_ATTR((f32_rows_fwd_kernel<T, false>), row)
+                CC_ATTR((f32_rows_fwd_kernel<T, true>), row)
+                CC_ATTR((f32_rows_inv_kernel<T, 0>), row)
+                CC_ATTR((f32_rows_inv_kernel<T, 2>), row)
+                CC_ATTR((f32_rows_inv_kernel<T, 4>), row)
+                CC_ATTR((f32_rows_inv_kernel<T, 8>), row)
+                CC_ATTR((f32_rows_inv_kernel<T, 16>), row)
+                CC_ATTR((f32_cols_rk_kernel<16, 16>), col)
+                CC_ATTR((f32_cols_rk_kernel<8, 2>), col)
+                CC_ATTR((f32_cols_rk_kernel<4, 4>), col)
+                CC_ATTR((f32_cols_rk_kernel<2, 8>), col)
+                CC_ATTR((f32_cols_rk_kernel<1, 16>), col)
+                CC_ATTR((f32_cols_rk_kernel<1, 2>), col)
                 CC_ATTR(f32_cols_solve_kernel<1>, col)
                 CC_ATTR(f32_cols_solve_kernel<2>, col)
                 CC_ATTR(f32_cols_solve_kernel<4>, col)
@@ -277,20 +288,44 @@ cudaError_t M2Launch<T>::fft32_solve(const T* rho, int pitch, const double* rho_
         const int cw = fft32_cw(ny);
         const size_t col = sizeof(float2) * (size_t)fft32_line(ny) * cw;
         cudaError_t e;
-        f32_rows_fwd_kernel<T><<<ny / 2, round32(fft32_tpl(nx)), row, s>>>(rho, pitch, rho_part, RED_BLOCKS,
-                                                                        (double)nx * (double)ny, A, nx, ny,
-                                                                        rootx, active);
+        // register hand-offs where every thread of a row / column CTA is busy
+        // (lines of at least 512 / 256 points); the staged forms below that
+        const int rt = round32(fft32_tpl(nx));
+        const bool reg_rows = nx >= 512;
+        if (reg_rows)
+            f32_rows_fwd_kernel<T, true><<<ny / 2, rt, row, s>>>(rho, pitch, rho_part, RED_BLOCKS,
+                                                                 (double)nx * (double)ny, A, nx, ny, rootx, active);
+        else
+            f32_rows_fwd_kernel<T, false><<<ny / 2, rt, row, s>>>(rho, pitch, rho_part, RED_BLOCKS,
+                                                                  (double)nx * (double)ny, A, nx, ny, rootx, active);
         if ((e = cudaGetLastError()) != cudaSuccess) return e;
         const int nt = round32(cw * fft32_tpl(ny)), nb = nhl / cw;
-        switch (cw) {
-            case 16: f32_cols_solve_kernel<16><<<nb, nt, col, s>>>(A, nx, ny, rooty, Lx, Ly, G, active); break;
-            case 8: f32_cols_solve_kernel<8><<<nb, nt, col, s>>>(A, nx, ny, rooty, Lx, Ly, G, active); break;
-            case 4: f32_cols_solve_kernel<4><<<nb, nt, col, s>>>(A, nx, ny, rooty, Lx, Ly, G, active); break;
-            case 2: f32_cols_solve_kernel<2><<<nb, nt, col, s>>>(A, nx, ny, rooty, Lx, Ly, G, active); break;
-            default: f32_cols_solve_kernel<1><<<nb, nt, col, s>>>(A, nx, ny, rooty, Lx, Ly, G, active); break;
+        const int rly = fft32_last_radix(ny);
+        if (ny >= 256 && nt == cw * fft32_tpl(ny)) {
+            if (cw == 16 && rly == 16) f32_cols_rk_kernel<16, 16><<<nb, nt, col, s>>>(A, nx, ny, rooty, Lx, Ly, G, active);
+            else if (cw == 8 && rly == 2) f32_cols_rk_kernel<8, 2><<<nb, nt, col, s>>>(A, nx, ny, rooty, Lx, Ly, G, active);
+            else if (cw == 4 && rly == 4) f32_cols_rk_kernel<4, 4><<<nb, nt, col, s>>>(A, nx, ny, rooty, Lx, Ly, G, active);
+            else if (cw == 2 && rly == 8) f32_cols_rk_kernel<2, 8><<<nb, nt, col, s>>>(A, nx, ny, rooty, Lx, Ly, G, active);
+            else if (cw == 1 && rly == 16) f32_cols_rk_kernel<1, 16><<<nb, nt, col, s>>>(A, nx, ny, rooty, Lx, Ly, G, active);
+            else if (cw == 1 && rly == 2) f32_cols_rk_kernel<1, 2><<<nb, nt, col, s>>>(A, nx, ny, rooty, Lx, Ly, G, active);
+            else return cudaErrorInvalidConfiguration;   // no (columns per CTA, last radix) pair for this ny
+        } else {
+            switch (cw) {
+                case 16: f32_cols_solve_kernel<16><<<nb, nt, col, s>>>(A, nx, ny, rooty, Lx, Ly, G, active); break;
+                case 8: f32_cols_solve_kernel<8><<<nb, nt, col, s>>>(A, nx, ny, rooty, Lx, Ly, G, active); break;
+                case 4: f32_cols_solve_kernel<4><<<nb, nt, col, s>>>(A, nx, ny, rooty, Lx, Ly, G, active); break;
+                case 2: f32_cols_solve_kernel<2><<<nb, nt, col, s>>>(A, nx, ny, rooty, Lx, Ly, G, active); break;
+                default: f32_cols_solve_kernel<1><<<nb, nt, col, s>>>(A, nx, ny, rooty, Lx, Ly, G, active); break;
+            }
         }
         if ((e = cudaGetLastError()) != cudaSuccess) return e;
-        f32_rows_inv_kernel<T><<<ny / 2, round32(fft32_tpl(nx)), row, s>>>(A, nx, ny, rootx, phi, pitch, active);
+        switch (reg_rows ? fft32_last_radix(nx) : 0) {
+            case 16: f32_rows_inv_kernel<T, 16><<<ny / 2, rt, row, s>>>(A, nx, ny, rootx, phi, pitch, active); break;
+            case 8: f32_rows_inv_kernel<T, 8><<<ny / 2, rt, row, s>>>(A, nx, ny, rootx, phi, pitch, active); break;
+            case 4: f32_rows_inv_kernel<T, 4><<<ny / 2, rt, row, s>>>(A, nx, ny, rootx, phi, pitch, active); break;
+            case 2: f32_rows_inv_kernel<T, 2><<<ny / 2, rt, row, s>>>(A, nx, ny, rootx, phi, pitch, active); break;
+            default: f32_rows_inv_kernel<T, 0><<<ny / 2, rt, row, s>>>(A, nx, ny, rootx, phi, pitch, active); break;
+        }
         return cudaGetLastError();
     }
 }
