@@ -5,7 +5,7 @@
 //   "CCH5REC1", int32 count, then per dataset: int32 name length, name,
 //   int32 file-name length, file name, int32 rank, uint64 dims[rank],
 //   int64 n_head, double head[n_head], int64 n_last, double last[n_last].
-// Read by tests/golden/make_golden.py.
+// Read by tests/golden/make_golden.py, which also reads the printed lines.
 //   usage: ref_main_record <libref_X.so> <run-main symbol> <out.bin>
 #include <dlfcn.h>
 
@@ -38,6 +38,10 @@ int main(int argc, char** argv) {
         std::fprintf(stderr, "missing symbols in %s\n", argv[1]);
         return 1;
     }
+    // line-buffered stdout: the reference's per-snapshot lines (t, dt, max
+    // |div B|) reach a reader as they are printed, also from a run that is
+    // stopped before its HDF5 write
+    std::setvbuf(stdout, nullptr, _IOLBF, 0);
     if (int r = run()) return r;
     std::FILE* f = std::fopen(argv[3], "wb");
     if (!f) return 1;

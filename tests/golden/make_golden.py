@@ -9,12 +9,17 @@ that tests/test_golden.py can pin the CPU oracle to the reference on a
 machine without the reference tree.  Every stored output is the reference's
 own result; nothing here is computed by the oracle or the library.
 
-    python tests/golden/make_golden.py [--mains-only | --no-mains]   (from the repository root)
+    python tests/golden/make_golden.py [--mains-only | --no-mains | --main2d-log-only]
+    (from the repository root)
 
-main_mhd2d.json / main_mhd3d.json hold what the reference's own main() wrote
-(its HDF5 datasets, recorded in memory): dataset names and dimensions, the
-rank-1 datasets (x, y, [z,] t) in full, and of every field the SHA-256 digest
-and sum of its first two stored frames and its last one.
+main_mhd3d.json holds what the reference's own 3D main() wrote (its HDF5
+datasets, recorded in memory): dataset names and dimensions, the rank-1
+datasets (x, y, z, t) in full, and of every field the SHA-256 digest and sum
+of its first two stored frames and its last one.  The 2D main() does not
+reach its HDF5 write with its default parameters (its core collapses and dt
+falls by orders of magnitude near t = 0.275): main_mhd2d_log.json holds the
+lines it printed per stored snapshot until it was stopped, and the dataset
+list of its writer.
 """
 from __future__ import annotations
 
@@ -188,26 +193,90 @@ def write_main_fixture(name: str, record: Path):
     (HERE / f"main_{name}.json").write_text(json.dumps(read_record(record), indent=1) + "\n")
 
 
+MAIN2D_SECONDS = 1200   # wall time allowed to the reference's 2D main() (see main2d_log)
+
+
+def _writer_datasets(src: Path, writer: str) -> list[list]:
+    """[name, rank] of every dataset the reference's HDF5 writer `writer`
+    writes, in order, read from its source (write1 -> rank 1, write3 -> rank 3)."""
+    import re
+    text = src.read_text()
+    body = text[text.index(f"static void {writer}("):]
+    body = body[:body.index("H5Fclose(file);")]
+    return [[name, 1 if kind == "1" else 3] for kind, name in re.findall(r'write([13])\("(/\w+)"', body)]
+
+
+def main2d_log(seconds: int = MAIN2D_SECONDS):
+    """The reference's own 2D main() (mhd2d_resistive_hlld_ct_gravity.cpp
+    main(), M2:929-1139) with its default parameters, run in a plain process
+    (oracle/_ref/ref_main_record): every line it prints, one per stored
+    snapshot ("t=... dt=... max|divB|=...", M2:1119-1125, t and dt to 7
+    significant digits, div B to 12).  With its defaults the core collapses
+    near t = 0.275 and dt falls by orders of magnitude, so the run does not
+    reach t_end = 0.35 (nor its HDF5 write) in hours; it is stopped after
+    `seconds` of wall time and the lines printed so far are kept, with the
+    dataset list of its writer (write_h5, M2:881-925) read from the source."""
+    import subprocess
+    import tempfile
+    import threading
+    import time
+    runner = O.REF_DIR / "ref_main_record"
+    lines, init = [], None
+    t0 = time.time()
+    with tempfile.TemporaryDirectory() as tmp:
+        proc = subprocess.Popen([str(runner), str(O.REF_DIR / "libref_mhd2d.so"), "ref_mhd2d_run_main",
+                                 str(Path(tmp) / "rec.bin")], cwd=tmp, stdout=subprocess.PIPE, text=True, bufsize=1)
+        timer = threading.Timer(seconds, proc.kill)
+        timer.start()
+        try:
+            for ln in proc.stdout:
+                ln = ln.strip()
+                if ln.startswith("init max|divB|="):
+                    init = ln.split("=", 1)[1]
+                elif ln.startswith("t="):
+                    kv = dict(part.split("=", 1) for part in ln.split())
+                    lines.append([kv["t"], kv["dt"], kv["max|divB|"], round(time.time() - t0, 1)])
+        finally:
+            timer.cancel()
+            proc.wait()
+    fx = {
+        "source": "mhd2d_resistive_hlld_ct_gravity.cpp main() with its default Params, stdout",
+        "finished": proc.returncode == 0,
+        "wall_seconds_allowed": seconds,
+        "seconds_to_last_line": lines[-1][3] if lines else None,
+        "init_max_divB": init,
+        "columns": ["t", "dt", "max|divB|"],
+        "lines": [ln[:3] for ln in lines],
+        "datasets": _writer_datasets(O.REFERENCE_SRC / "mhd2d_resistive_hlld_ct_gravity.cpp", "write_h5"),
+    }
+    (HERE / "main_mhd2d_log.json").write_text(json.dumps(fx, indent=0) + "\n")
+
+
 def mains():
-    """The reference's own main() of the 2D and 3D MHD solvers, run once with
-    their defaults in a plain process (oracle/_ref/ref_main_record; the 2D run
-    takes most of an hour of CPU): their HDF5 datasets, recorded in memory by
-    oracle/hdf5_stub/hdf5.h, go to main_mhd2d.json / main_mhd3d.json."""
+    """The reference's own main() of the 3D MHD solver, run once with its
+    defaults in a plain process (oracle/_ref/ref_main_record): its HDF5
+    datasets, recorded in memory by oracle/hdf5_stub/hdf5.h, go to
+    main_mhd3d.json.  The 2D main() does not finish with its defaults (see
+    main2d_log): its printed lines go to main_mhd2d_log.json."""
     import subprocess
     import tempfile
     runner = O.REF_DIR / "ref_main_record"
-    for name in ("mhd2d", "mhd3d"):
+    for name in ("mhd3d",):
         with tempfile.TemporaryDirectory() as tmp:
             rec = Path(tmp) / "rec.bin"
             subprocess.run([str(runner), str(O.REF_DIR / f"libref_{name}.so"), f"ref_{name}_run_main", str(rec)],
                            check=True, stdout=subprocess.DEVNULL, cwd=tmp)
             write_main_fixture(name, rec)
+    main2d_log()
 
 
 def main():
     for name in ("mhd2d", "mhd3d", "euler2d", "fft"):
         if O.ref(name) is None:
             raise SystemExit(f"compiled reference libref_{name}.so is missing: run make -C oracle")
+    if "--main2d-log-only" in sys.argv:
+        main2d_log()
+        return
     if "--mains-only" not in sys.argv:
         mhd2d()
         mhd3d()
