@@ -24,6 +24,7 @@ CC_FP32 = 1
 CC_POISSON_SOR = 0
 CC_POISSON_FFT = 1
 CC_POISSON_DIRECT = 2
+CC_POISSON_SOR_LEX = 5
 CC_GRAVITY_ENCLOSED = 3
 CC_GRAVITY_SHELLS = 4
 CC_BATCH_MAX_DIRECT_SIDE = 2048

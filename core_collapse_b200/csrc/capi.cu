@@ -210,6 +210,9 @@ template <class T> struct Mhd2d : Mhd2dBase {
                         CC_CUDA(cudaMemcpyAsync(tw[k], tt.data(), sizeof(T) * tt.size(), cudaMemcpyHostToDevice, st()));
                     }
                 }
+            } else if (p.poisson_kind == CC_POISSON_SOR_LEX) {
+                CC_CUDA(cudaMalloc(&rhs, sizeof(double) * (size_t)nx * ny));
+                CC_CUDA(cudaMalloc(&sphi, sizeof(double) * (size_t)nx * ny));
             } else if (p.poisson_kind == CC_POISSON_SOR) {
                 if ((p.periodic_x && (nx & 1)) || (p.periodic_y && (ny & 1)))
                     return fail(h, CC_ERR_UNSUPPORTED, "red-black SOR needs an even extent along periodic axes");
@@ -300,6 +303,17 @@ template <class T> struct Mhd2d : Mhd2dBase {
                 CC_CUDA(M2Launch<T>::fft_solve(rho, P, rho_part, nx, ny, ilog2(nx), ilog2(ny), tw[0], tw[1], tw[2],
                                                tw[3], p.x1 - p.x0, p.y1 - p.y0, p.G, fftA, phi, active(), st()));
             count(3);
+        } else if (p.poisson_kind == CC_POISSON_SOR_LEX) {
+            const double dx = (p.x1 - p.x0) / nx, dy = (p.y1 - p.y0) / ny;
+            SorLexArgs a;
+            a.nx = nx; a.ny = ny; a.pitch = P; a.ax = c.ax; a.ay = c.ay;
+            a.idx2 = 1.0 / (dx * dx); a.idy2 = 1.0 / (dy * dy);
+            a.denom = 2.0 * (a.idx2 + a.idy2);
+            a.omega = p.sor_omega; a.fourpiG = 4.0 * M_PI * p.G; a.tol = p.sor_tol; a.max_iter = p.sor_iters;
+            a.rhs = rhs; a.phi = sphi; a.iters_out = iflags + 2; a.res_out = sor_res; a.active = active();
+            CC_CUDA(launch_sor_lex<T>(a, rho, st()));
+            CC_CUDA(M2Launch<T>::phi_to_field(sphi, nx, ny, phi, P, active(), st()));
+            count(2);
         } else {
             CC_CUDA(M2Launch<T>::sor_rhs(rho, nx, ny, P, rho_part, 4.0 * M_PI * p.G, -1.0, rhs, active(), st()));
             const double dx = (p.x1 - p.x0) / nx, dy = (p.y1 - p.y0) / ny;

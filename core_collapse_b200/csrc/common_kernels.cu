@@ -80,4 +80,14 @@ cudaError_t launch_sor(const SorArgs& a, int* nblocks_out, cudaStream_t s) {
     return cudaLaunchCooperativeKernel((const void*)sor_rb_kernel<SOR_NT>, dim3(nb), dim3(SOR_NT), params, 0, s);
 }
 
+constexpr int SOR_LEX_NT = 1024;
+
+template <class T>
+cudaError_t launch_sor_lex(const SorLexArgs& a, const T* rho, cudaStream_t s) {
+    sor_lex_kernel<T, SOR_LEX_NT><<<1, SOR_LEX_NT, 0, s>>>(a, rho);
+    return cudaGetLastError();
+}
+template cudaError_t launch_sor_lex<float>(const SorLexArgs&, const float*, cudaStream_t);
+template cudaError_t launch_sor_lex<double>(const SorLexArgs&, const double*, cudaStream_t);
+
 }  // namespace ccb

@@ -14,11 +14,17 @@
 // Field files grow one snapshot at a time; their headers are rewritten with
 // the final Nt at the end.
 //
-// Usage: cc_mhd2d_main [--precision fp64|fp32] [--poisson sor|fft]
+// Usage: cc_mhd2d_main [--precision fp64|fp32] [--poisson sor|fft|lex]
 //                      [--Nx N] [--Ny N] [--t_end T] [--dt_store D]
 //                      [--out DIR] [--checkpoint FILE] [--restart FILE]
+//                      [--max_steps N]
 // --checkpoint writes a restart file at the end of the run; --restart starts
-// from one (same grid) instead of the initial condition.
+// from one (same grid) instead of the initial condition.  --poisson lex runs
+// the reference's own lexicographic SOR (CC_POISSON_SOR_LEX: its sweep order
+// and sums, slow; the default red-black SOR is the production solve).
+// --max_steps ends the loop after N steps even before t_end (the output then
+// holds the snapshots stored so far): with its default parameters the
+// reference's collapse makes dt fall by orders of magnitude near t = 0.275.
 #include <sys/stat.h>
 
 #include <cinttypes>
@@ -50,6 +56,7 @@ int main(int argc, char** argv) {
     cc_mhd2d_params p;
     cc_mhd2d_params_default(&p);   // the reference's Params defaults (M2:44-86)
     std::string out = "out2d_mhd", ckpt, restart;
+    long long max_steps = -1;
     for (int a = 1; a < argc; a++) {
         const std::string k = argv[a];
         const char* v = (a + 1 < argc) ? argv[a + 1] : nullptr;
@@ -62,7 +69,10 @@ int main(int argc, char** argv) {
             return std::string(v);
         };
         if (k == "--precision") p.precision = need() == "fp32" ? CC_FP32 : CC_FP64;
-        else if (k == "--poisson") p.poisson_kind = need() == "fft" ? CC_POISSON_FFT : CC_POISSON_SOR;
+        else if (k == "--poisson") {
+            const std::string kind = need();
+            p.poisson_kind = kind == "fft" ? CC_POISSON_FFT : kind == "lex" ? CC_POISSON_SOR_LEX : CC_POISSON_SOR;
+        }
         else if (k == "--Nx") p.Nx = std::atoi(need().c_str());
         else if (k == "--Ny") p.Ny = std::atoi(need().c_str());
         else if (k == "--t_end") p.t_end = std::atof(need().c_str());
@@ -70,6 +80,7 @@ int main(int argc, char** argv) {
         else if (k == "--out") out = need();
         else if (k == "--checkpoint") ckpt = need();
         else if (k == "--restart") restart = need();
+        else if (k == "--max_steps") max_steps = std::atoll(need().c_str());
         else {
             std::fprintf(stderr, "unknown option %s\n", k.c_str());
             return 2;
@@ -132,8 +143,15 @@ int main(int argc, char** argv) {
     // the main loop (M2:1111-1129)
     double next_store = t;
     if (!store(t)) return 1;
+    long long steps = 0;
     while (t < p.t_end) {
+        if (max_steps >= 0 && steps >= max_steps) {
+            if (check(h, cc_mhd2d_diagnostics(h, &d), "diagnostics")) return 1;
+            std::printf("stopped after %lld steps: t=%.7g dt=%.7g\n", steps, t, d.dt_last);
+            break;
+        }
         if (check(h, cc_mhd2d_advance(h, 1, &t), "cc_mhd2d_advance")) return 1;
+        steps++;
         if (t >= next_store - 1e-15) {
             if (check(h, cc_mhd2d_diagnostics(h, &d), "diagnostics")) return 1;
             std::printf("t=%.7g dt=%.7g max|divB|=%.12g\n", t, d.dt_last, d.max_divB);

@@ -69,5 +69,7 @@ cudaError_t launch_dt_finalize(const double* spd_part, DtSpec d, double* dt_out,
 cudaError_t launch_clock(double* t, const double* dt, const int* active, long long* steps, cudaStream_t s);
 // cooperative launch of the red-black SOR; nblocks must all be co-resident
 cudaError_t launch_sor(const SorArgs& a, int* nblocks_out, cudaStream_t s);
+// the lexicographic SOR of the reference (one CTA, sor_lex_kernel); rho pitched
+template <class T> cudaError_t launch_sor_lex(const SorLexArgs& a, const T* rho, cudaStream_t s);
 
 }  // namespace ccb

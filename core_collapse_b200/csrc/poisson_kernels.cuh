@@ -212,6 +212,106 @@ struct SorArgs {
     const int* active;
 };
 
+// Lexicographic SOR, the reference's own solve (compute_poisson_gravity_periodic,
+// M2:178-237) in its own order, for parity runs of the drop-in driver.  One
+// CTA.  A sweep runs as anti-diagonal wavefronts: the cells with i + j = d
+// update together, d = 0 .. nx + ny - 2, with a barrier between diagonals.
+// Of a cell's neighbours, west and south lie on diagonal d - 1 (already
+// updated in this sweep), east and north on d + 1 (not yet), and a periodic
+// wrap neighbour on d +- (n - 1): (0, j) reads (nx - 1, j) before this sweep
+// updates it and (nx - 1, j) reads (0, j) after, as the row-major loop does;
+// a clamped neighbour that is the cell itself is read before its update.  So
+// every cell sees exactly the values the reference's loop sees.  The density
+// mean and each sweep's mean of phi are summed by one thread in the
+// reference's row-major order, and the update is the reference's expression,
+// so phi is the reference's to the last bit.  Slow by design (nx + ny - 1
+// barriers and an N-term sequential sum per sweep); the red-black kernel is
+// the production solve.  tol > 0: stop after the first sweep whose max
+// |lap(phi) - rhs|, taken inside the sweep from each cell's update as
+// EH:335-368 does, is below tol.
+struct SorLexArgs {
+    int nx, ny, pitch;
+    AxisMap ax, ay;
+    double idx2, idy2, denom, omega, fourpiG, tol;
+    int max_iter;
+    double* rhs;            // nx*ny contiguous (written)
+    double* phi;            // nx*ny contiguous (written)
+    int* iters_out;
+    double* res_out;
+    const int* active;
+};
+
+template <class T, int NT>
+__global__ void __launch_bounds__(NT) sor_lex_kernel(SorLexArgs a, const T* __restrict__ rho) {
+    if (a.active && *a.active == 0) return;
+    __shared__ double sh[NT / 32];
+    __shared__ double s_val;
+    const int nx = a.nx, ny = a.ny, N = nx * ny, tid = threadIdx.x;
+    double* __restrict__ phi = a.phi;
+    // rhobar and rhs = 4 pi G (rho - rhobar) (M2:187-194)
+    if (tid == 0) {
+        double s = 0.0;
+        for (int j = 0; j < ny; j++)
+            for (int i = 0; i < nx; i++) s += (double)rho[(size_t)j * a.pitch + i];
+        s_val = s / (double)N;
+    }
+    __syncthreads();
+    const double rhobar = s_val;
+    for (int j = 0; j < ny; j++)
+        for (int i = tid; i < nx; i += NT) {
+            const size_t q = (size_t)j * nx + i;
+            a.rhs[q] = a.fourpiG * ((double)rho[(size_t)j * a.pitch + i] - rhobar);
+            phi[q] = 0.0;
+        }
+    __syncthreads();
+    int it = 0;
+    double res = 0.0;
+    for (; it < a.max_iter; ++it) {
+        double r = 0.0;   // tol > 0: the residual taken inside the sweep (EH:335-368)
+        for (int d = 0; d <= nx + ny - 2; ++d) {
+            const int i0 = d - (ny - 1) > 0 ? d - (ny - 1) : 0, i1 = d < nx - 1 ? d : nx - 1;
+            for (int i = i0 + tid; i <= i1; i += NT) {
+                const int j = d - i;
+                const size_t k = (size_t)j * nx + i;
+                const double phiE = phi[(size_t)j * nx + a.ax.cell(i + 1)];
+                const double phiW = phi[(size_t)j * nx + a.ax.cell(i - 1)];
+                const double phiN = phi[(size_t)a.ay.cell(j + 1) * nx + i];
+                const double phiS = phi[(size_t)a.ay.cell(j - 1) * nx + i];
+                const double phi_new = ((phiE + phiW) * a.idx2 + (phiN + phiS) * a.idy2 - a.rhs[k]) / a.denom;
+                const double v = phi[k] + a.omega * (phi_new - phi[k]);
+                phi[k] = v;
+                if (a.tol > 0.0) {
+                    const double lap = (phiE - 2.0 * v + phiW) * a.idx2 + (phiN - 2.0 * v + phiS) * a.idy2;
+                    r = fmax(r, fabs(lap - a.rhs[k]));
+                }
+            }
+            __syncthreads();
+        }
+        // phibar in row-major order (M2:219-222)
+        if (tid == 0) {
+            double s = 0.0;
+            for (int q = 0; q < N; q++) s += phi[q];
+            s_val = s / (double)N;
+        }
+        __syncthreads();
+        const double phibar = s_val;
+        for (int q = tid; q < N; q += NT) phi[q] -= phibar;
+        __syncthreads();
+        if (a.tol > 0.0) {
+            const double r0 = block_max<NT>(r, sh);   // valid in thread 0
+            if (tid == 0) s_val = r0;
+            __syncthreads();
+            res = s_val;
+            __syncthreads();   // s_val is rewritten by the next sweep's mean
+            if (res < a.tol) { ++it; break; }
+        }
+    }
+    if (tid == 0) {
+        if (a.iters_out) *a.iters_out = it;
+        if (a.res_out) *a.res_out = res;
+    }
+}
+
 // max |lap(phi) - rhs| over the block's cells of the field phi - shift (the
 // stored field with a pending mean removal applied on the fly)
 template <int NT>

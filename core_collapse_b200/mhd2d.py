@@ -45,7 +45,8 @@ class Params:
     sor_omega: float = 1.8
     # additions
     sor_tol: float = 0.0            # > 0: stop SOR once max|lap(phi)-rhs| < sor_tol
-    poisson: str = "sor"            # "sor" (red-black), "fft", or "direct" (batched ensemble only)
+    poisson: str = "sor"            # "sor" (red-black), "fft", "sor_lex" (the reference's lexicographic
+    #                                 SOR, a parity mode) or "direct" (batched ensemble only)
     precision: str = "fp64"         # "fp64" or "fp32"
     compensated: bool = False       # FP32 only: compensated (Kahan-style) state update
 
@@ -56,7 +57,8 @@ class Params:
                 continue
             v = getattr(self, f.name)
             setattr(c, f.name, int(v) if isinstance(v, bool) else v)
-        c.poisson_kind = {"sor": L.CC_POISSON_SOR, "fft": L.CC_POISSON_FFT, "direct": L.CC_POISSON_DIRECT}[self.poisson]
+        c.poisson_kind = {"sor": L.CC_POISSON_SOR, "fft": L.CC_POISSON_FFT, "direct": L.CC_POISSON_DIRECT,
+                          "sor_lex": L.CC_POISSON_SOR_LEX}[self.poisson]
         c.precision = {"fp64": L.CC_FP64, "fp32": L.CC_FP32}[self.precision]
         return c
 

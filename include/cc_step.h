@@ -55,6 +55,10 @@ extern "C" {
 #define CC_GRAVITY_SHELLS 4   /* Euler/HLLC only: radial gravity from cell masses binned into Nr_bins radial
                                  shells about (xc, yc), gravity_accel_from_enclosed_mass
                                  (gravity_enclosed.h:18-96) */
+#define CC_POISSON_SOR_LEX 5 /* 2D MHD: the reference's lexicographic SOR (M2:178-237) in its own sweep order,
+                                with its sequential density and phi means: the same phi bit for bit (FP64).
+                                A parity mode for drop-in runs: one CTA, nx+ny-1 barriers and an N-term
+                                sequential sum per sweep */
 
 typedef struct cc_handle cc_handle;
 
