@@ -310,6 +310,7 @@ template <class T> struct Mhd2d : Mhd2dBase {
             a.idx2 = 1.0 / (dx * dx); a.idy2 = 1.0 / (dy * dy);
             a.denom = 2.0 * (a.idx2 + a.idy2);
             a.omega = p.sor_omega; a.fourpiG = 4.0 * M_PI * p.G; a.tol = p.sor_tol; a.max_iter = p.sor_iters;
+            a.floor_rho = -1.0;   // M2 solves with the stored density (M2:187-194)
             a.rhs = rhs; a.phi = sphi; a.iters_out = iflags + 2; a.res_out = sor_res; a.active = active();
             CC_CUDA(launch_sor_lex<T>(a, rho, st()));
             CC_CUDA(M2Launch<T>::phi_to_field(sphi, nx, ny, phi, P, active(), st()));

@@ -102,8 +102,8 @@ template <class T> struct Euler2d : Euler2dBase {
         c.gravity_on = p.gravity_on ? 1 : 0;
         plane = (size_t)P * (ny + 1);
         if (p.gravity_on) {
-            if (p.poisson_kind != CC_POISSON_SOR && p.poisson_kind != CC_GRAVITY_ENCLOSED &&
-                p.poisson_kind != CC_GRAVITY_SHELLS)
+            if (p.poisson_kind != CC_POISSON_SOR && p.poisson_kind != CC_POISSON_SOR_LEX &&
+                p.poisson_kind != CC_GRAVITY_ENCLOSED && p.poisson_kind != CC_GRAVITY_SHELLS)
                 return fail(h, CC_ERR_UNSUPPORTED, "the Euler/HLLC solver supports SOR or enclosed-mass gravity");
             if (p.poisson_kind == CC_POISSON_SOR && ((nx & 1) || (ny & 1)))
                 return fail(h, CC_ERR_UNSUPPORTED, "red-black SOR needs even Nx and Ny (periodic)");
@@ -296,6 +296,20 @@ template <class T> struct Euler2d : Euler2dBase {
         }
         h->perf.poisson_solves += 1;
         const int nx = p.Nx, ny = p.Ny;
+        if (p.poisson_kind == CC_POISSON_SOR_LEX) {   // the reference's own order (parity mode)
+            const double dx = (p.x1 - p.x0) / nx, dy = (p.y1 - p.y0) / ny;
+            SorLexArgs a;
+            a.nx = nx; a.ny = ny; a.pitch = P; a.ax = c.pax; a.ay = c.pay;
+            a.idx2 = 1.0 / (dx * dx); a.idy2 = 1.0 / (dy * dy);
+            a.denom = 2.0 * (a.idx2 + a.idy2);
+            a.omega = p.sor_omega; a.fourpiG = 4.0 * M_PI * p.G; a.tol = p.sor_tol; a.max_iter = p.sor_max_iter;
+            a.floor_rho = p.floor_rho;
+            a.rhs = rhs; a.phi = sphi; a.iters_out = iflags + 2; a.res_out = res_dev(); a.active = active();
+            CC_CUDA(launch_sor_lex<T>(a, rho, st()));
+            CC_CUDA(M2Launch<T>::phi_to_field(sphi, nx, ny, phi, P, active(), st()));
+            count(2);
+            return CC_OK;
+        }
         CC_CUDA(M2Launch<T>::sor_rhs(rho, nx, ny, P, rho_part, 4.0 * M_PI * p.G, p.floor_rho, rhs, active(), st()));
         const double dx = (p.x1 - p.x0) / nx, dy = (p.y1 - p.y0) / ny;
         SorArgs a;

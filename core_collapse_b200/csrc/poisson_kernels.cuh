@@ -213,7 +213,7 @@ struct SorArgs {
 };
 
 // Lexicographic SOR, the reference's own solve (compute_poisson_gravity_periodic,
-// M2:178-237) in its own order, for parity runs of the drop-in driver.  One
+// M2:178-237 and EH:288-386) in its own order, for parity runs.  One
 // CTA.  A sweep runs as anti-diagonal wavefronts: the cells with i + j = d
 // update together, d = 0 .. nx + ny - 2, with a barrier between diagonals.
 // Of a cell's neighbours, west and south lie on diagonal d - 1 (already
@@ -233,6 +233,7 @@ struct SorLexArgs {
     int nx, ny, pitch;
     AxisMap ax, ay;
     double idx2, idy2, denom, omega, fourpiG, tol;
+    double floor_rho;       // >= 0: density floored at it first (EH:307-313); < 0: as read (M2)
     int max_iter;
     double* rhs;            // nx*ny contiguous (written)
     double* phi;            // nx*ny contiguous (written)
@@ -248,11 +249,15 @@ __global__ void __launch_bounds__(NT) sor_lex_kernel(SorLexArgs a, const T* __re
     __shared__ double s_val;
     const int nx = a.nx, ny = a.ny, N = nx * ny, tid = threadIdx.x;
     double* __restrict__ phi = a.phi;
-    // rhobar and rhs = 4 pi G (rho - rhobar) (M2:187-194)
+    // rhobar and rhs = 4 pi G (rho - rhobar) (M2:187-194; EH:307-321 with the floor)
+    auto dens = [&](int i, int j) {
+        const double r = (double)rho[(size_t)j * a.pitch + i];
+        return (a.floor_rho >= 0.0 && r < a.floor_rho) ? a.floor_rho : r;   // std::max(rho, floor_rho)
+    };
     if (tid == 0) {
         double s = 0.0;
         for (int j = 0; j < ny; j++)
-            for (int i = 0; i < nx; i++) s += (double)rho[(size_t)j * a.pitch + i];
+            for (int i = 0; i < nx; i++) s += dens(i, j);
         s_val = s / (double)N;
     }
     __syncthreads();
@@ -260,7 +265,7 @@ __global__ void __launch_bounds__(NT) sor_lex_kernel(SorLexArgs a, const T* __re
     for (int j = 0; j < ny; j++)
         for (int i = tid; i < nx; i += NT) {
             const size_t q = (size_t)j * nx + i;
-            a.rhs[q] = a.fourpiG * ((double)rho[(size_t)j * a.pitch + i] - rhobar);
+            a.rhs[q] = a.fourpiG * (dens(i, j) - rhobar);
             phi[q] = 0.0;
         }
     __syncthreads();

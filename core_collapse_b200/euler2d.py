@@ -41,7 +41,8 @@ class ParamsEH:
     softening: float = 1e-4
     sor_tol: float = 1e-10
     sor_omega: float = 1.7
-    poisson: str = "sor"       # "enclosed": enclosed-mass radial gravity (EH:226-286);
+    poisson: str = "sor"       # "sor": red-black SOR; "sor_lex": the reference's lexicographic SOR
+    #                            (a parity mode); "enclosed": enclosed-mass radial gravity (EH:226-286);
     #                            "shells": shell-binned enclosed mass (gravity_enclosed.h:18-96)
     precision: str = "fp64"
     Nr_bins: int = 512         # shell count of "shells" (euler2d_h5.cpp:43)
@@ -55,7 +56,7 @@ class ParamsEH:
                 continue
             v = getattr(self, f.name)
             setattr(c, f.name, int(v) if isinstance(v, bool) else v)
-        c.poisson_kind = {"sor": L.CC_POISSON_SOR, "fft": L.CC_POISSON_FFT,
+        c.poisson_kind = {"sor": L.CC_POISSON_SOR, "fft": L.CC_POISSON_FFT, "sor_lex": L.CC_POISSON_SOR_LEX,
                           "enclosed": L.CC_GRAVITY_ENCLOSED, "shells": L.CC_GRAVITY_SHELLS}[self.poisson]
         c.precision = {"fp64": L.CC_FP64, "fp32": L.CC_FP32}[self.precision]
         return c

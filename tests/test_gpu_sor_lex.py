@@ -6,12 +6,19 @@ gravity field and the main-loop steps are the same doubles, on every seeded
 gravity case (periodic, outflow and mixed axes, the reference IC, the HLL
 fallback case) and on odd periodic extents, which the red-black ordering
 cannot take.  FP32 (density read as FP32, the solve in FP64) is checked
-against the same oracle with the FP32 bound of the other gravity tests."""
+against the same oracle with the FP32 bound of the other gravity tests.
+Euler/HLLC (EH:288-386: floored density, the reference's residual tolerance
+1e-10 taken inside the sweep, an always-periodic stencil): the same gravity,
+sweep count and residual, and the same RK2 step, bit for bit."""
+import ctypes as C
+
 import numpy as np
 import pytest
 
 import oracle_lib as O
+from cases_euler2d import CASES_EH, make_case_eh
 from cases_mhd2d import CASES, make_case
+from core_collapse_b200.euler2d import Euler2dSolver
 from core_collapse_b200.mhd2d import Mhd2dSolver, Params, ic_collapse
 
 pytestmark = pytest.mark.gpu
@@ -75,3 +82,40 @@ def test_gravity_lex_fp32():
     gx, gy, _, _ = O.m2_gravity_oracle(p.to_c(), U.rho, mode=0)
     g, _ = _gravity(p, U, B)
     assert O.rel_linf(g.gx, gx) <= 2e-5 and O.rel_linf(g.gy, gy) <= 2e-5
+
+
+# ---- Euler/HLLC ----
+
+EH_GRAV = [n for n in sorted(CASES_EH) if CASES_EH[n][0].get("gravity_on")]
+
+
+@pytest.mark.parametrize("name", EH_GRAV)
+def test_euler_gravity_lex_bit_identical(name):
+    p, s = make_case_eh(name, poisson="sor_lex")   # the reference's tolerance 1e-10
+    cp = p.to_c()
+    n = p.Nx * p.Ny
+    gx, gy = np.zeros(n), np.zeros(n)
+    it, res = C.c_int(), C.c_double()
+    O.oracle().or_euler2d_gravity(C.byref(cp), O.dp(s.rho), O.dp(gx), O.dp(gy), 0, C.byref(it), C.byref(res))
+    with Euler2dSolver(p) as g:
+        g.upload(s)
+        x, y = g.compute_gravity()
+        d = g.diagnostics()
+    assert d["poisson_iters"] == it.value and d["poisson_residual"] == res.value
+    assert np.array_equal(x, gx) and np.array_equal(y, gy)
+
+
+@pytest.mark.parametrize("name", EH_GRAV)
+def test_euler_rk2_step_lex_bit_identical(name):
+    p, s = make_case_eh(name, poisson="sor_lex")
+    cp = p.to_c()
+    S = [a.copy() for a in s.arrays()]
+    dt = O.oracle().or_euler2d_compute_dt(C.byref(cp), O.pp(S))
+    want = O.copy_state(S)
+    O.oracle().or_euler2d_rk2_step(C.byref(cp), O.pp(want), dt, 0)
+    with Euler2dSolver(p) as g:
+        g.upload(s)
+        g.rk2_step(dt)
+        got = g.download().arrays()
+    for a, b in zip(got, want):
+        assert np.array_equal(a, b)
