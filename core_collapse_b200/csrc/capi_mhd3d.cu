@@ -2,7 +2,7 @@
 // transfer, compute_dt, rk2_step and the device-resident main-loop body.
 //
 // Per step (M3:1285-1291, 1034-1066): dt = finalize(CFL partials), clamped to
-// t_end; stage 1 (prim, x/y/z faces, update, edges, CT): U^n -> S1;
+// t_end; stage 1 (prim, x/y/z faces, update, edge EMFs + CT in one pass): U^n -> S1;
 // stage 2 (prim applies S1's deferred Joule sub-step in place): S1 -> S2;
 // average: U^{n+1} = floors(0.5 (U^n + Joule(S2))) with the CFL partials of
 // U^{n+1}; t += dt.  Three state buffers rotate; three steps are one CUDA graph.
@@ -46,7 +46,6 @@ template <class T> struct Mhd3d : Mhd3dBase {
     PrimData<T> prim{};
     Bcc3<T> bcc{};   // cell-centred B of the state a Joule pass reads
     FaceData<T> fX{}, fY{}, fZ{};
-    T *Ex = nullptr, *Ey = nullptr, *Ez = nullptr;
     double* staging = nullptr;
     double* spd_part = nullptr;
     double* rho_part = nullptr;
@@ -85,8 +84,8 @@ template <class T> struct Mhd3d : Mhd3dBase {
         c = m3_make_const<T>(p);
         vol = (size_t)c.PS * (nz + 1);
 
-        // 3 states x 8 + primitives 8 + 3 x 7 face data + 3 edge arrays + 3 cell-centred B = 59 fields
-        const size_t nfield = 59;
+        // 3 states x 8 + primitives 8 + 3 x 7 face data + 3 cell-centred B = 56 fields
+        const size_t nfield = 56;
         CC_CUDA(cudaMalloc(&block, sizeof(T) * vol * nfield));
         CC_CUDA(cudaMemsetAsync(block, 0, sizeof(T) * vol * nfield, st()));
         T* base = reinterpret_cast<T*>(block);
@@ -99,7 +98,6 @@ template <class T> struct Mhd3d : Mhd3dBase {
         for (int m = 0; m < 7; m++) fX.f[m] = take();
         for (int m = 0; m < 7; m++) fY.f[m] = take();
         for (int m = 0; m < 7; m++) fZ.f[m] = take();
-        Ex = take(); Ey = take(); Ez = take();
         bcc.x = take(); bcc.y = take(); bcc.z = take();
         CC_CUDA(cudaMalloc(&staging, sizeof(double) * (size_t)(nx + 1) * (ny + 1) * (nz + 1)));
         CC_CUDA(cudaMalloc(&spd_part, sizeof(double) * RED_BLOCKS));
@@ -193,9 +191,8 @@ template <class T> struct Mhd3d : Mhd3dBase {
         CC_CUDA(M3Launch<T>::prim(c, in, prim, defer, bcc, dt_dev(), active(), st()));
         CC_CUDA(M3Launch<T>::faces(c, in, prim, fX, fY, fZ, active(), st()));
         CC_CUDA(M3Launch<T>::update(c, in, out, fX, fY, fZ, dt_dev(), active(), st()));
-        CC_CUDA(M3Launch<T>::edges(c, in, fX, fY, fZ, Ex, Ey, Ez, active(), st()));
-        CC_CUDA(M3Launch<T>::ct(c, in, out, Ex, Ey, Ez, dt_dev(), active(), st()));
-        count(defer && c.resistive ? 8 : 7);
+        CC_CUDA(M3Launch<T>::emf_ct(c, in, out, fX, fY, fZ, dt_dev(), active(), st()));
+        count(defer && c.resistive ? 7 : 6);
         if (h->profiling) {
             CC_CUDA(cudaEventRecord(e1, st()));
             h->timed.emplace_back(e0, e1);

@@ -52,18 +52,11 @@ cudaError_t M3Launch<T>::update(const M3Const<T>& c, const Fields3<T>& in, const
 }
 
 template <class T>
-cudaError_t M3Launch<T>::edges(const M3Const<T>& c, const Fields3<T>& in, const FaceData<T>& X, const FaceData<T>& Y,
-                               const FaceData<T>& Z, T* Ex, T* Ey, T* Ez, const int* active, cudaStream_t st) {
-    const dim3 eg((c.nx + 1 + 31) / 32, (c.ny + 1 + 7) / 8, (c.nz + 1 + M3_EDGE_KCH - 1) / M3_EDGE_KCH);
-    m3_edge_kernel<T><<<eg, 256, 0, st>>>(c, in, X, Y, Z, Ex, Ey, Ez, active);
-    return cudaGetLastError();
-}
-
-template <class T>
-cudaError_t M3Launch<T>::ct(const M3Const<T>& c, const Fields3<T>& in, const Fields3<T>& out, const T* Ex, const T* Ey,
-                            const T* Ez, const double* dt, const int* active, cudaStream_t st) {
-    m3_ct_kernel<T><<<grid3((long long)(c.nx + 1) * (c.ny + 1) * (c.nz + 1)), 256, 0, st>>>(c, in, out, Ex, Ey, Ez,
-                                                                                             dt, active);
+cudaError_t M3Launch<T>::emf_ct(const M3Const<T>& c, const Fields3<T>& in, const Fields3<T>& out, const FaceData<T>& X,
+                                const FaceData<T>& Y, const FaceData<T>& Z, const double* dt, const int* active,
+                                cudaStream_t st) {
+    const dim3 g((c.nx + 1 + 30) / 31, (c.ny + 1 + 6) / 7, (c.nz + 1 + M3_EDGE_KCH - 1) / M3_EDGE_KCH);
+    m3_emf_ct_kernel<T><<<g, 256, 0, st>>>(c, in, out, X, Y, Z, dt, active);
     return cudaGetLastError();
 }
 

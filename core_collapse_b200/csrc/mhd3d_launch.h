@@ -17,10 +17,10 @@ template <class T> struct M3Launch {
     static cudaError_t update(const M3Const<T>& c, const Fields3<T>& in, const Fields3<T>& out, const FaceData<T>& X,
                               const FaceData<T>& Y, const FaceData<T>& Z, const double* dt, const int* active,
                               cudaStream_t st);
-    static cudaError_t edges(const M3Const<T>& c, const Fields3<T>& in, const FaceData<T>& X, const FaceData<T>& Y,
-                             const FaceData<T>& Z, T* Ex, T* Ey, T* Ez, const int* active, cudaStream_t st);
-    static cudaError_t ct(const M3Const<T>& c, const Fields3<T>& in, const Fields3<T>& out, const T* Ex, const T* Ey,
-                          const T* Ez, const double* dt, const int* active, cudaStream_t st);
+    // edge EMFs and the CT face update in one pass (m3_emf_ct_kernel)
+    static cudaError_t emf_ct(const M3Const<T>& c, const Fields3<T>& in, const Fields3<T>& out, const FaceData<T>& X,
+                              const FaceData<T>& Y, const FaceData<T>& Z, const double* dt, const int* active,
+                              cudaStream_t st);
     // bcc: scratch planes for the cell-centred B of s2 (its Joule step)
     static cudaError_t average(const M3Const<T>& c, const Fields3<T>& un, const Fields3<T>& s2, const Fields3<T>& out,
                                const Bcc3<T>& bcc, const double* dt, const int* active, double* spd_part,

@@ -123,9 +123,10 @@ def test_mhd2d_driver_trajectory_tracks_reference_main(tmp_path):
     rd = np.array([float(ln[1]) for ln in fx["lines"]])
     r = _run("cc_mhd2d_main", "--dt_store", 0.01, "--t_end", 0.15, "--out", tmp_path / "out")
     _, lines = _driver_lines(r.stdout)
-    assert len(lines) == 15
+    # the first step (next_store starts at t = 0), t >= 0.01 .. 0.14, and the clamped last step at 0.15
+    assert len(lines) == 16 and lines[-1][0] == "0.15"
     worst = 0.0
-    for ln in lines:
+    for ln in lines[:-1]:
         t, dt = float(ln[0]), float(ln[1])
         worst = max(worst, abs(dt / np.interp(t, rt, rd) - 1.0))
         assert float(ln[2]) < 1e-10, ln
