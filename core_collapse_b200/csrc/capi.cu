@@ -96,7 +96,7 @@ template <class T> struct Mhd2d : Mhd2dBase {
     double* sor_part2 = nullptr;
     double* staging = nullptr;
     unsigned int* bar = nullptr;  // count, gen
-    int* iflags = nullptr;        // active, bar_err, sor_iters
+    int* iflags = nullptr;        // active, bar_err, sor_iters, fft_copy_err
     double* dt_dev = nullptr;
     double* t_dev = nullptr;
     double* sor_res = nullptr;
@@ -277,6 +277,7 @@ template <class T> struct Mhd2d : Mhd2dBase {
         int fl[4];
         CC_CUDA(cudaMemcpy(fl, iflags, sizeof(fl), cudaMemcpyDeviceToHost));
         if (fl[1]) return fail(h, CC_ERR_CUDA, "SOR grid barrier timed out");
+        if (fl[3]) return fail(h, CC_ERR_CUDA, "FFT column pass: a bulk-copy wait timed out");
         return CC_OK;
     }
 
@@ -298,7 +299,8 @@ template <class T> struct Mhd2d : Mhd2dBase {
             if constexpr (sizeof(T) == 4)
                 CC_CUDA(M2Launch<T>::fft32_solve(rho, P, rho_part, nx, ny, reinterpret_cast<const float2*>(tw[0]),
                                                  reinterpret_cast<const float2*>(tw[2]), p.x1 - p.x0, p.y1 - p.y0,
-                                                 p.G, reinterpret_cast<float2*>(fftA), phi, active(), st()));
+                                                 p.G, reinterpret_cast<float2*>(fftA), phi, active(), st(),
+                                                 iflags + 3));
             else
                 CC_CUDA(M2Launch<T>::fft_solve(rho, P, rho_part, nx, ny, ilog2(nx), ilog2(ny), tw[0], tw[1], tw[2],
                                                tw[3], p.x1 - p.x0, p.y1 - p.y0, p.G, fftA, phi, active(), st()));
@@ -617,6 +619,7 @@ template <class T> struct Mhd2d : Mhd2dBase {
         d->poisson_residual = sc[2];
         d->nonfinite = nonf > 0.0 ? 1 : 0;
         if (fl[1]) return fail(h, CC_ERR_CUDA, "SOR grid barrier timed out");
+        if (fl[3]) return fail(h, CC_ERR_CUDA, "FFT column pass: a bulk-copy wait timed out");
         return CC_OK;
     }
 };

@@ -19,6 +19,8 @@
 //   * shared-memory lines padded by one element per 16 so that the stride-16
 //     writes of the first pass hit distinct banks.
 #pragma once
+#include <cstdint>
+
 #include <cuda_runtime.h>
 
 namespace ccb {
@@ -403,6 +405,134 @@ f32_cols_rk_kernel(float2* __restrict__ A, int nx, int ny, const float2* __restr
         const float n = (float)ny;
 #pragma unroll
         for (int q = 0; q < 16; q++) col[lt + fft32_fmap<RL>(q) * tl] = make_float2(w[q].x / n, w[q].y / n);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Bulk-copy (TMA) staging for the column pass.  A line group (CW contiguous kx
+// lines, CW ny float2, 16-byte aligned, a multiple of 16 bytes) is one
+// cp.async.bulk copy from global into shared memory, completed on an
+// mbarrier with its byte count; no multicast, this GPU's memory only.  Every
+// wait is bounded: after FFT32_WAIT_POLLS polls the kernel records the timeout
+// in *err, waits (bounded again) for its copies still in flight and returns.
+// ---------------------------------------------------------------------------
+constexpr unsigned FFT32_WAIT_POLLS = 1u << 22;
+
+__device__ __forceinline__ uint32_t f32_smem_addr(const void* p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void f32_mbar_init(uint32_t mbar) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(mbar) : "memory");
+}
+// one elected thread: expect `bytes` on the mbarrier and start the copy
+__device__ __forceinline__ void f32_bulk_load(uint32_t dst, const void* src, uint32_t bytes, uint32_t mbar) {
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");   // earlier generic reads of dst come first
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(mbar), "r"(bytes) : "memory");
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
+                 "l"(src), "r"(bytes), "r"(mbar)
+                 : "memory");
+}
+// true once phase `parity` of the mbarrier has completed; false after the poll limit
+__device__ __forceinline__ bool f32_mbar_wait(uint32_t mbar, uint32_t parity) {
+    for (unsigned it = 0; it < FFT32_WAIT_POLLS; ++it) {
+        uint32_t done;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\tmbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+            "selp.u32 %0, 1, 0, p;\n\t}\n"
+            : "=r"(done)
+            : "r"(mbar), "r"(parity)
+            : "memory");
+        if (done) return true;
+        __nanosleep(32);
+    }
+    return false;
+}
+
+// shared memory of f32_cols_tma_kernel: two staging buffers, the padded work
+// lines, two mbarriers
+__host__ __device__ constexpr size_t fft32_cols_tma_smem(int cw, int ny) {
+    return sizeof(float2) * (2 * (size_t)cw * ny + (size_t)cw * fft32_line(ny)) + 16;
+}
+
+// Pass 2 as f32_cols_rk_kernel, persistent: a CTA takes line groups
+// blockIdx.x, blockIdx.x + gridDim.x, ...; while it transforms one group the
+// bulk copy of its next group is in flight into the other staging buffer, so
+// the global load latency of the column pass is hidden behind the transform.
+// The first forward pass reads the staged line (coalesced shared loads); the
+// rest, and every value, is f32_cols_rk_kernel's.
+template <int CW, int RL>
+__global__ void __launch_bounds__(CW == 1 && RL == 2 ? 512 : 256, CW == 1 && RL == 2 ? 1 : 2)
+f32_cols_tma_kernel(float2* __restrict__ A, int nx, int ny, const float2* __restrict__ roots, double Lx, double Ly,
+                    double G, const int* __restrict__ active, int* __restrict__ err) {
+    if (active && *active == 0) return;
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    const int tl = ny / 16;
+    const int l = (int)threadIdx.x / tl, lt = (int)threadIdx.x % tl;
+    const int ncol = nx / 2 + 1, ngroups = (ncol + CW - 1) / CW;
+    const int gsz = CW * ny;                                   // float2 per group
+    float2* stage = reinterpret_cast<float2*>(smem_raw);       // 2 x gsz
+    float2* work = stage + 2 * gsz;                            // CW padded lines
+    uint64_t* mbar = reinterpret_cast<uint64_t*>(work + CW * fft32_line(ny));
+    const uint32_t mb[2] = {f32_smem_addr(&mbar[0]), f32_smem_addr(&mbar[1])};
+    const uint32_t st[2] = {f32_smem_addr(stage), f32_smem_addr(stage + gsz)};
+    const uint32_t bytes = (uint32_t)(sizeof(float2) * gsz);
+    if (threadIdx.x == 0) {
+        f32_mbar_init(mb[0]);
+        f32_mbar_init(mb[1]);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+    int g = blockIdx.x;
+    if (threadIdx.x == 0 && g < ngroups) f32_bulk_load(st[0], A + (size_t)g * gsz, bytes, mb[0]);
+    const float fy = (float)(2.0 * M_PI / Ly), fx = (float)(2.0 * M_PI / Lx), g4 = (float)(4.0 * M_PI * G);
+    float2* line = work + l * fft32_line(ny);
+    for (int it = 0; g < ngroups; g += gridDim.x, ++it) {
+        const int buf = it & 1;
+        const bool next = g + (int)gridDim.x < ngroups;
+        if (threadIdx.x == 0 && next)
+            f32_bulk_load(st[buf ^ 1], A + (size_t)(g + gridDim.x) * gsz, bytes, mb[buf ^ 1]);
+        const bool ok = f32_mbar_wait(mb[buf], (it >> 1) & 1);
+        if (!__syncthreads_and(ok)) {
+            if (threadIdx.x == 0) {
+                atomicExch(err, 1);
+                f32_mbar_wait(mb[buf], (it >> 1) & 1);                   // let the copies in flight land
+                if (next) f32_mbar_wait(mb[buf ^ 1], ((it + 1) >> 1) & 1);
+            }
+            __syncthreads();
+            return;
+        }
+        const float2* src = stage + buf * gsz + l * ny;
+        float2 v[16];
+#pragma unroll
+        for (int r = 0; r < 16; r++) v[r] = src[lt + r * tl];
+        const int kx = g * CW + l;
+        f32_fft_regs<RL, false, true>(line, v, ny, roots, lt);
+        float2 w[16];
+#pragma unroll
+        for (int q = 0; q < 16; q++) {
+            const int j = lt + fft32_fmap<RL>(q) * tl;
+            const int nj = (j <= ny / 2) ? j : j - ny;
+            const float ky = fy * (float)nj, kxf = fx * (float)kx;
+            const float k2 = kxf * kxf + ky * ky;
+            float2 z = v[q];
+            if (k2 == 0.0f) {
+                z = make_float2(0.0f, 0.0f);
+            } else {
+                const float sf = -g4 / k2;
+                z.x = z.x * sf;
+                z.y = z.y * sf;
+            }
+            w[fft32_fmap<RL>(q)] = z;
+        }
+        __syncthreads();   // every thread's last forward reads of the line are done
+        f32_fft_regs<RL, true, true>(line, w, ny, roots, lt);
+        if (kx < ncol) {
+            float2* col = A + (size_t)kx * ny;
+            const float n = (float)ny;
+#pragma unroll
+            for (int q = 0; q < 16; q++) col[lt + fft32_fmap<RL>(q) * tl] = make_float2(w[q].x / n, w[q].y / n);
+        }
+        __syncthreads();   // the line's last reads are done before the next group's first pass writes it
     }
 }
 

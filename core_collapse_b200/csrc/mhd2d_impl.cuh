@@ -75,6 +75,17 @@ cudaError_t M2Launch<T>::prepare(int nx, int ny) {
                 CC_ATTR((f32_cols_rk_kernel<2, 8>), col)
                 CC_ATTR((f32_cols_rk_kernel<1, 16>), col)
                 CC_ATTR((f32_cols_rk_kernel<1, 2>), col)
+                if (ny >= 256) {
+                    const int tsm = (int)fft32_cols_tma_smem(fft32_cw(ny), ny);
+                    if (tsm <= 227 * 1024) {
+                        CC_ATTR((f32_cols_tma_kernel<16, 16>), tsm)
+                        CC_ATTR((f32_cols_tma_kernel<8, 2>), tsm)
+                        CC_ATTR((f32_cols_tma_kernel<4, 4>), tsm)
+                        CC_ATTR((f32_cols_tma_kernel<2, 8>), tsm)
+                        CC_ATTR((f32_cols_tma_kernel<1, 16>), tsm)
+                        CC_ATTR((f32_cols_tma_kernel<1, 2>), tsm)
+                    }
+                }
                 CC_ATTR(f32_cols_solve_kernel<1>, col)
                 CC_ATTR(f32_cols_solve_kernel<2>, col)
                 CC_ATTR(f32_cols_solve_kernel<4>, col)
@@ -278,7 +289,7 @@ cudaError_t M2Launch<T>::fft_solve(const T* rho, int pitch, const double* rho_pa
 template <class T>
 cudaError_t M2Launch<T>::fft32_solve(const T* rho, int pitch, const double* rho_part, int nx, int ny,
                                      const float2* rootx, const float2* rooty, double Lx, double Ly, double G,
-                                     float2* A, T* phi, const int* active, cudaStream_t s) {
+                                     float2* A, T* phi, const int* active, cudaStream_t s, int* err) {
     if constexpr (sizeof(T) != 4) {
         return cudaErrorNotSupported;
     } else {
@@ -301,7 +312,24 @@ cudaError_t M2Launch<T>::fft32_solve(const T* rho, int pitch, const double* rho_
         if ((e = cudaGetLastError()) != cudaSuccess) return e;
         const int nt = round32(cw * fft32_tpl(ny)), nb = nhl / cw;
         const int rly = fft32_last_radix(ny);
-        if (ny >= 256 && nt == cw * fft32_tpl(ny)) {
+        if (ny >= 256 && nt == cw * fft32_tpl(ny) && err) {
+            static int nsm = 0;
+            if (nsm == 0) {
+                int dev = 0;
+                if ((e = cudaGetDevice(&dev)) != cudaSuccess) return e;
+                if ((e = cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return e;
+            }
+            const size_t sm = fft32_cols_tma_smem(cw, ny);
+            const int per_sm = (cw == 1 && rly == 2) ? 1 : 2;
+            const int g = nb < nsm * per_sm ? nb : nsm * per_sm;
+            if (cw == 16 && rly == 16) f32_cols_tma_kernel<16, 16><<<g, nt, sm, s>>>(A, nx, ny, rooty, Lx, Ly, G, active, err);
+            else if (cw == 8 && rly == 2) f32_cols_tma_kernel<8, 2><<<g, nt, sm, s>>>(A, nx, ny, rooty, Lx, Ly, G, active, err);
+            else if (cw == 4 && rly == 4) f32_cols_tma_kernel<4, 4><<<g, nt, sm, s>>>(A, nx, ny, rooty, Lx, Ly, G, active, err);
+            else if (cw == 2 && rly == 8) f32_cols_tma_kernel<2, 8><<<g, nt, sm, s>>>(A, nx, ny, rooty, Lx, Ly, G, active, err);
+            else if (cw == 1 && rly == 16) f32_cols_tma_kernel<1, 16><<<g, nt, sm, s>>>(A, nx, ny, rooty, Lx, Ly, G, active, err);
+            else if (cw == 1 && rly == 2) f32_cols_tma_kernel<1, 2><<<g, nt, sm, s>>>(A, nx, ny, rooty, Lx, Ly, G, active, err);
+            else return cudaErrorInvalidConfiguration;
+        } else if (ny >= 256 && nt == cw * fft32_tpl(ny)) {
             if (cw == 16 && rly == 16) f32_cols_rk_kernel<16, 16><<<nb, nt, col, s>>>(A, nx, ny, rooty, Lx, Ly, G, active);
             else if (cw == 8 && rly == 2) f32_cols_rk_kernel<8, 2><<<nb, nt, col, s>>>(A, nx, ny, rooty, Lx, Ly, G, active);
             else if (cw == 4 && rly == 4) f32_cols_rk_kernel<4, 4><<<nb, nt, col, s>>>(A, nx, ny, rooty, Lx, Ly, G, active);

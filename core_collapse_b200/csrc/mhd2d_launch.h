@@ -53,9 +53,11 @@ template <class T> struct M2Launch {
     // FP32 spectral solve (fft32_kernels.cuh), T = float only: rootx / rooty
     // the nx-th / ny-th roots of unity W^e = (cos 2 pi e/n, -sin 2 pi e/n),
     // A: fft32_half_lines(nx) x ny complex work array; needs nx, ny powers of two.
+    // err (device int): given, the column pass stages its lines by bulk copies
+    // (f32_cols_tma_kernel) and records a timed-out copy wait there.
     static cudaError_t fft32_solve(const T* rho, int pitch, const double* rho_part, int nx, int ny,
                                    const float2* rootx, const float2* rooty, double Lx, double Ly, double G,
-                                   float2* A, T* phi, const int* active, cudaStream_t s);
+                                   float2* A, T* phi, const int* active, cudaStream_t s, int* err = nullptr);
     static cudaError_t sor_rhs(const T* rho, int nx, int ny, int pitch, const double* rho_part, double fourpiG,
                                double floor_rho, double* rhs, const int* active, cudaStream_t s);
     static cudaError_t phi_to_field(const double* phi, int nx, int ny, T* out, int pitch, const int* active,
