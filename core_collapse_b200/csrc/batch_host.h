@@ -126,7 +126,9 @@ template <class T> struct Batch : BatchBase {
     int2* rwork = nullptr; int nrwork = 0;
     int2* gwork = nullptr; int ngwork = 0; int gtile = 64;
     int2* tcwork = nullptr; int ntcwork = 0;   // FP32 instances with 16-byte rows: tcgen05 transforms
-    int* tcerr = nullptr;            // timed-out waits of the tensor-core transforms
+    int* tcerr = nullptr;            // timed-out waits of the tensor-core transforms (bit 0; bit 1: the final
+                                     // wait for the MMAs gave up too)
+    bool tc_fatal = false;           // bit 1 was seen: MMAs may have outlived their TMEM, no further work
     int2* ywork = nullptr; int nywork = 0;
     // per-instance device scalars and partials
     double* spd_part = nullptr;
@@ -367,6 +369,7 @@ template <class T> struct Batch : BatchBase {
     }
 
     int upload(int i, const double* const* f) override {
+        if (tc_fatal) return fail(h, CC_ERR_CUDA, "handle unusable: an earlier tensor-core transform gave up on its MMAs");
         if (i < 0 || i >= n || !f) return fail(h, CC_ERR_ARG, "bad instance index or null state");
         int w[8], hh[8];
         layout(i, w, hh);
@@ -417,6 +420,7 @@ template <class T> struct Batch : BatchBase {
     }
 
     int compute_dt(double* out) override {
+        if (tc_fatal) return fail(h, CC_ERR_CUDA, "handle unusable: an earlier tensor-core transform gave up on its MMAs");
         if (!all_loaded()) return fail(h, CC_ERR_STATE, "not every instance has an uploaded state");
         if (int r = ensure_partials()) return r;
         CC_CUDA(launch_batch_finalize(dred, n, spd_part, rho_part, BF_DT, dt, tclk, active, rho_mean, st()));
@@ -478,6 +482,7 @@ template <class T> struct Batch : BatchBase {
     }
 
     int advance(int nsteps, double* t) override {
+        if (tc_fatal) return fail(h, CC_ERR_CUDA, "handle unusable: an earlier tensor-core transform gave up on its MMAs");
         if (!all_loaded()) return fail(h, CC_ERR_STATE, "not every instance has an uploaded state");
         if (nsteps < 0) return fail(h, CC_ERR_ARG, "nsteps < 0");
         if (t) CC_CUDA(cudaMemcpyAsync(tclk, t, sizeof(double) * n, cudaMemcpyHostToDevice, st()));
@@ -522,6 +527,7 @@ template <class T> struct Batch : BatchBase {
         int terr = 0;
         CC_CUDA(cudaMemcpyAsync(&terr, tcerr, sizeof(int), cudaMemcpyDeviceToHost, st()));
         CC_CUDA(cudaStreamSynchronize(st()));
+        if (terr & 2) tc_fatal = true;
         if (terr) return fail(h, CC_ERR_CUDA, "tensor-core Poisson transform: an mbarrier wait timed out");
         return CC_OK;
     }
@@ -566,6 +572,7 @@ template <class T> struct Batch : BatchBase {
     }
 
     int autotune(int reps, int* out_shape, double* out_ms) override {
+        if (tc_fatal) return fail(h, CC_ERR_CUDA, "handle unusable: an earlier tensor-core transform gave up on its MMAs");
         if (!all_loaded()) return fail(h, CC_ERR_STATE, "not every instance has an uploaded state");
         if (reps < 1) reps = 1;
         if (int r = ensure_partials()) return r;

@@ -26,8 +26,10 @@
 //     chunk c+1 overlap the MMAs of chunk c;
 //   * epilogue: each warp reads 32 accumulator lanes (rows) x 64 columns with
 //     tcgen05.ld and stores them (float4) to ah or phi.
-// Every mbarrier wait is bounded; on a timeout the kernel records it in *err,
-// waits (bounded) for its own MMAs, frees its TMEM and returns.
+// Every mbarrier wait is bounded; on a timeout the kernel sets bit 0 of *err,
+// waits (bounded) for its own MMAs, frees its TMEM and returns.  If that last
+// wait gives up too, MMAs may still be writing the TMEM it frees: the kernel
+// then also sets bit 1, and the handle refuses all further work.
 #pragma once
 #include <cstdint>
 
@@ -243,6 +245,7 @@ dp_gemm_tc_kernel(const BatchInst<float>* __restrict__ inst, const int2* __restr
             const int c = issued - 1;
             done = tc_mbar_wait((c & 1) ? mb1 : mb0, (uint32_t)((c >> 1) & 1));
         }
+        if (!done) atomicOr(err, 3);   // the MMAs may outlive this CTA's TMEM
         *sok = (ok && done) ? 1 : 0;
     }
     __syncthreads();
