@@ -35,9 +35,9 @@ enum GravMode { GRAV_NONE = 0, GRAV_ARRAYS = 1, GRAV_PHI = 2 };
 // phase is a loop of its items over the NT threads between two barriers, so
 // a phase whose item count is just above NT costs a second, nearly empty
 // round while the CTA's other warps wait at the barrier.  The FP32 tile is
-// sized so that slopes, x faces, y faces, edges and cells each fit one round:
-// 32 x 14 cells, 544 threads = 34 x 16 slope cells, 33 x 16 x faces,
-// 34 x 15 y faces.
+// sized so that slopes, x faces, y faces, edges and cells each fit one round
+// and each warp works one row of a phase (ROW32): 30 x 15 cells, 544 threads
+// = 17 rows of 32 slope cells, 17 rows of 31 x faces, 16 rows of 32 y faces.
 // SPLIT: separate x and y slope buffers (7 NSL more shared memory), so that
 // the x and y slopes form one phase and the x and y face fluxes another
 // (4 barriers per tile instead of 6; each item range padded to whole warps so
@@ -48,7 +48,7 @@ template <> struct StageTile<double> {
     static constexpr bool SPLIT = false;
 };
 template <> struct StageTile<float> {
-    static constexpr int TX = 32, TY = 14, NT = 544, MINB = 2;
+    static constexpr int TX = 30, TY = 15, NT = 544, MINB = 2;
     static constexpr bool SPLIT = false;
 };
 
@@ -58,7 +58,13 @@ template <class T, int TX_, int TY_, int NT_ = TX_ * TY_, bool SPLIT_ = false> s
     static constexpr int NT = NT_;        // threads
     static constexpr int NC = TX * TY;    // cells
     static constexpr bool SPLIT = SPLIT_;
+    // ROW32: a tile TX = 30 wide, so that slope and y-face rows are 32 items
+    // wide; x faces, edges and cells are then also mapped one row per warp
+    // (a lane per column, the last lanes idle), so no warp straddles two rows
+    // and the shared-memory reads of a phase hit 32 distinct banks
+    static constexpr bool ROW32 = (TX + 2 == 32);
     static_assert(NT >= NC && NT % 32 == 0, "one thread per cell in the update phase, whole warps");
+    static_assert(!ROW32 || (32 * TY <= NT && !SPLIT), "ROW32: a row of threads per tile row of cells, no split");
     static constexpr int NFX = (TX + 1) * (TY + 2);  // x faces: TX+1 per row, rows -1..TY
     static constexpr int NGY = (TX + 2) * (TY + 1);  // y faces: cols -1..TX, TY+1 per col
     static constexpr int NE = (TX + 1) * (TY + 1);   // edges
@@ -304,8 +310,15 @@ __device__ __forceinline__ void m2_stage_tile(const M2Const<T>& c, const Fields<
         slopes(ridx(lx, ly), RX, true, k);
     };
     // x faces i0..i0+TX, rows j0-1..j0+TY (M2:706-725)
-    auto x_face = [&](int k) {
-        const int f = k % (TX + 1), r = k / (TX + 1) - 1;
+    auto x_face = [&](int kk) {
+        int f, r, k;
+        if constexpr (G::ROW32) {   // kk = a lane of row r + 1
+            f = kk % 32; r = kk / 32 - 1;
+            if (f > TX) return;
+            k = (r + 1) * (TX + 1) + f;
+        } else {
+            f = kk % (TX + 1); r = kk / (TX + 1) - 1; k = kk;
+        }
         const int gi = i0 + f;
         if (gi > c.nx) return;
         const int cj = c.ay.cell(j0 + r);
@@ -357,7 +370,7 @@ __device__ __forceinline__ void m2_stage_tile(const M2Const<T>& c, const Fields<
         // ---- B: x slopes, then x faces; C: y slopes (same buffer), then y faces ----
         for (int k = tid; k < NSL; k += NT) x_slopes(k);
         __syncthreads();
-        for (int k = tid; k < NFX; k += NT) x_face(k);
+        for (int k = tid; k < (G::ROW32 ? 32 * (TY + 2) : NFX); k += NT) x_face(k);
         __syncthreads();
         for (int k = tid; k < NSL; k += NT) y_slopes(k);
         __syncthreads();
@@ -366,8 +379,10 @@ __device__ __forceinline__ void m2_stage_tile(const M2Const<T>& c, const Fields<
     }
 
     // ---- E: edge EMFs, edges i0..i0+TX x j0..j0+TY (M2:782-804, 565-575) ----
-    for (int k = tid; k < G::NE; k += NT) {
-        const int ei = k % (TX + 1), ej = k / (TX + 1);
+    for (int kk = tid; kk < (G::ROW32 ? 32 * (TY + 1) : G::NE); kk += NT) {
+        const int ei = G::ROW32 ? kk % 32 : kk % (TX + 1), ej = G::ROW32 ? kk / 32 : kk / (TX + 1);
+        if (G::ROW32 && ei > TX) continue;
+        const int k = ej * (TX + 1) + ei;
         const int ie = i0 + ei, je = j0 + ej;
         if (ie > c.nx || je > c.ny) continue;
         const T exm = -fx[5 * NFX + ej * (TX + 1) + ei];        // x face ie, row je-1
@@ -388,8 +403,8 @@ __device__ __forceinline__ void m2_stage_tile(const M2Const<T>& c, const Fields<
     __syncthreads();
 
     // ---- D+F: FV update, floors, CT, gravity kick, store (M2:750-779, 807-832) ----
-    if (tid >= NC) return;
-    const int tx = tid % TX, ty = tid / TX;
+    const int tx = G::ROW32 ? tid % 32 : tid % TX, ty = G::ROW32 ? tid / 32 : tid / TX;
+    if (tx >= TX || ty >= TY) return;
     const int gi = i0 + tx, gj = j0 + ty;
     if (gi >= c.nx || gj >= c.ny) return;
     const size_t q = (size_t)gj * P + gi;
