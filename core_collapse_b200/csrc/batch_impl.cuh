@@ -4,7 +4,7 @@
 // for, split x/y slope buffers):
 //   FP64: 32x8/256 (2), 16x16/256 (2)
 //   FP32: 32x16/512 (2, split), 32x8/256 (4), 64x8/512 (2), 32x14/544 (2, split),
-//         30x15/544 (2, one row per warp in every phase)
+//         30x15/544 (2, one row per warp in every phase), 30x6/256 (4, the same)
 // The autotuner of the batch handle times each on the actual work-list.
 #pragma once
 #include "batch_launch.h"
@@ -23,7 +23,7 @@ template <> template <> struct BatchShapes<double>::S<1> {
     static constexpr int TX = 16, TY = 16, NT = 256, MINB = 2; static constexpr bool SPLIT = false;
 };
 template <> struct BatchShapes<float> {
-    static constexpr int N = 5;
+    static constexpr int N = 6;
     template <int K> struct S;
 };
 template <> template <> struct BatchShapes<float>::S<0> {
@@ -40,6 +40,9 @@ template <> template <> struct BatchShapes<float>::S<3> {
 };
 template <> template <> struct BatchShapes<float>::S<4> {   // one row per warp in every phase (ROW32)
     static constexpr int TX = 30, TY = 15, NT = 544, MINB = 2; static constexpr bool SPLIT = false;
+};
+template <> template <> struct BatchShapes<float>::S<5> {   // the same on 8 warps, four CTAs per SM
+    static constexpr int TX = 30, TY = 6, NT = 256, MINB = 4; static constexpr bool SPLIT = false;
 };
 
 namespace {

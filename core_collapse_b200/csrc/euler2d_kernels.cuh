@@ -105,14 +105,23 @@ __device__ __forceinline__ void eh_hllc(const EHConst<T>& c, const EPrim<T>& L, 
     F[3] = F[3] + S * (ES - E);
 }
 
+// FP64 tiles are 31 cells wide (ROWW): a row of x faces is then 32 wide, and
+// the y faces and cells are also mapped one row per warp (a lane per column,
+// the last one idle), so no warp straddles two rows and every face loop is
+// one round.  At 4096^2 that took the FP64 step from 4.16 to 3.81 ms; the same
+// for FP32 (31 x 15 on 512 threads) made it slower (2.11 -> 2.39 ms: the
+// FP32 stage is bound by the tile's loads, and its 10% more, smaller tiles
+// cost more than the rounds and bank conflicts saved), so FP32 keeps 32 x 16.
 template <class T> struct EHTile;
-template <> struct EHTile<double> { static constexpr int TX = 32, TY = 8; };
-template <> struct EHTile<float> { static constexpr int TX = 32, TY = 16; };
+template <> struct EHTile<double> { static constexpr int TX = 31, TY = 8, NT = 288; };
+template <> struct EHTile<float> { static constexpr int TX = 32, TY = 16, NT = 512; };
 
 template <class T> struct EHGeom {
     static constexpr int TX = EHTile<T>::TX, TY = EHTile<T>::TY, HALO = 2;
-    static constexpr int RX = TX + 2 * HALO, RY = TY + 2 * HALO, RR = RX * RY, NT = TX * TY;
+    static constexpr int RX = TX + 2 * HALO, RY = TY + 2 * HALO, RR = RX * RY, NT = EHTile<T>::NT;
     static constexpr int NFX = (TX + 1) * TY, NGY = TX * (TY + 1);
+    static constexpr bool ROWW = (TX == 31);
+    static_assert(NT % 32 == 0 && (ROWW ? NT >= 32 * (TY + 1) : NT == TX * TY), "a thread per cell, whole warps");
     static constexpr size_t smem = sizeof(T) * (size_t)(4 * RR + 4 * NFX + 4 * NGY);
 };
 
@@ -169,9 +178,10 @@ eh_stage_kernel(const EHConst<T> c, const EHFields<T> un, const EHFields<T> in, 
         eh_hllc<T, 0>(c, L, R, F);
         fx[k] = F[0]; fx[NFX + k] = F[1]; fx[2 * NFX + k] = F[2]; fx[3 * NFX + k] = F[3];
     }
-    for (int k = tid; k < NGY; k += NT) {  // y faces j0..j0+TY of columns i0..i0+TX-1
-        const int col = k % TX, g = k / TX;
-        if (j0 + g > c.ny || i0 + col >= c.nx) continue;
+    for (int kk = tid; kk < (G::ROWW ? 32 * (TY + 1) : NGY); kk += NT) {  // y faces j0..j0+TY of columns i0..i0+TX-1
+        const int w = G::ROWW ? 32 : TX;
+        const int col = kk % w, g = kk / w, k = g * TX + col;
+        if (col >= TX || j0 + g > c.ny || i0 + col >= c.nx) continue;
         EPrim<T> L, R;
         face(ridx(col, g - 2), ridx(col, g - 1), ridx(col, g), ridx(col, g + 1), L, R);
         T F[4];
@@ -180,9 +190,9 @@ eh_stage_kernel(const EHConst<T> c, const EHFields<T> un, const EHFields<T> in, 
     }
     __syncthreads();
 
-    const int tx = tid % TX, ty = tid / TX;
+    const int tx = tid % (G::ROWW ? 32 : TX), ty = tid / (G::ROWW ? 32 : TX);
     const int gi = i0 + tx, gj = j0 + ty;
-    if (gi >= c.nx || gj >= c.ny) return;
+    if (tx >= TX || ty >= TY || gi >= c.nx || gj >= c.ny) return;
     const size_t q = (size_t)gj * P + gi;
     // rhs (EH:503-524): flux divergence, then the gravity source with the raw state
     const int kx = ty * (TX + 1) + tx, ky = ty * TX + tx;
