@@ -66,6 +66,11 @@ template <class T, int TX_, int TY_, int NT_ = TX_ * TY_, bool SPLIT_ = false> s
     // (a lane per column, the last lanes idle), so no warp straddles two rows
     // and the shared-memory reads of a phase hit 32 distinct banks
     static constexpr bool ROW32 = (TX + 2 == 32);
+    // ROWSYNC: one warp per slope row (NT = 32 (TY + 2) threads).  A warp then
+    // writes the x slopes of its row, reads them for the x faces of the same
+    // row and writes the y slopes of that row into the same slots: no other
+    // warp touches them, so these phases are separated by __syncwarp only
+    static constexpr bool ROWSYNC = ROW32 && NT == 32 * (TY + 2);
     static_assert(NT >= NC && NT % 32 == 0, "one thread per cell in the update phase, whole warps");
     static_assert(!ROW32 || (32 * TY <= NT && !SPLIT), "ROW32: a row of threads per tile row of cells, no split");
     static constexpr int NFX = (TX + 1) * (TY + 2);  // x faces: TX+1 per row, rows -1..TY
@@ -372,9 +377,9 @@ __device__ __forceinline__ void m2_stage_tile(const M2Const<T>& c, const Fields<
     } else {
         // ---- B: x slopes, then x faces; C: y slopes (same buffer), then y faces ----
         for (int k = tid; k < NSL; k += NT) x_slopes(k);
-        __syncthreads();
+        if constexpr (G::ROWSYNC) __syncwarp(); else __syncthreads();
         for (int k = tid; k < (G::ROW32 ? 32 * (TY + 2) : NFX); k += NT) x_face(k);
-        __syncthreads();
+        if constexpr (G::ROWSYNC) __syncwarp(); else __syncthreads();
         for (int k = tid; k < NSL; k += NT) y_slopes(k);
         __syncthreads();
         for (int k = tid; k < NGY; k += NT) y_face(k);
