@@ -69,7 +69,8 @@ template <class T, int TX_, int TY_, int NT_ = TX_ * TY_, bool SPLIT_ = false> s
     // ROWSYNC: one warp per slope row (NT = 32 (TY + 2) threads).  A warp then
     // writes the x slopes of its row, reads them for the x faces of the same
     // row and writes the y slopes of that row into the same slots: no other
-    // warp touches them, so these phases are separated by __syncwarp only
+    // warp touches them, so these phases are separated by __syncwarp only;
+    // likewise its y-face row and then its edge row
     static constexpr bool ROWSYNC = ROW32 && NT == 32 * (TY + 2);
     static_assert(NT >= NC && NT % 32 == 0, "one thread per cell in the update phase, whole warps");
     static_assert(!ROW32 || (32 * TY <= NT && !SPLIT), "ROW32: a row of threads per tile row of cells, no split");
@@ -383,7 +384,9 @@ __device__ __forceinline__ void m2_stage_tile(const M2Const<T>& c, const Fields<
         for (int k = tid; k < NSL; k += NT) y_slopes(k);
         __syncthreads();
         for (int k = tid; k < NGY; k += NT) y_face(k);
-        __syncthreads();
+        // ROWSYNC: warp w computes y-face row w and then edge row w, which reads
+        // that y-face row and the x faces (written before the last barrier)
+        if constexpr (G::ROWSYNC) __syncwarp(); else __syncthreads();
     }
 
     // ---- E: edge EMFs, edges i0..i0+TX x j0..j0+TY (M2:782-804, 565-575) ----
