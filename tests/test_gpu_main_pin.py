@@ -156,3 +156,12 @@ def test_mhd3d_driver_output_pinned_to_reference_main(tmp_path):
         scale = bscale / hmin if k == "divB" else max(f0["absmax"], 1e-300)
         assert abs(float(np.sum(got[k][0])) - f0["sum"]) <= 1e-12 * scale * got[k][0].size, k
         assert abs(float(np.max(np.abs(got[k][0]))) - f0["absmax"]) <= 1e-12 * scale, k
+
+
+def test_mhd2d_driver_max_steps_ends_the_loop(tmp_path):
+    """--max_steps ends the main loop before t_end and keeps what was stored."""
+    out = tmp_path / "out"
+    r = _run("cc_mhd2d_main", "--max_steps", 3, "--out", out)
+    assert "stopped after 3 steps: t=" in r.stdout
+    t = np.load(out / "t.npy")
+    assert len(t) == 4 and t[0] == 0.0 and np.all(np.diff(t) > 0)   # the t = 0 store and one per step
