@@ -493,7 +493,17 @@ template <class T> __host__ __device__ __forceinline__ T minmod(T a, T b) {
 }
 template <class T> __host__ __device__ __forceinline__ T mc_slope(T wm, T wc, T wp) {
     const T dm = wc - wm, dp = wp - wc;
-    return minmod(T(0.5) * (dm + dp), minmod(T(2.0) * dm, T(2.0) * dp));
+    if constexpr (sizeof(T) == 4) {
+        // FP32: the same limiter in fewer compare / select instructions (the
+        // stage kernel's ALU pipe is its busiest): 0 when dm dp <= 0, else the
+        // smallest of |dm + dp| / 2, 2 |dm|, 2 |dp|, with the sign of dm, which
+        // is the value the two minmods select (ties have equal values)
+        const T sc = T(0.5) * (dm + dp);
+        const T m = fminf(fabsf(sc), fminf(fabsf(T(2.0) * dm), fabsf(T(2.0) * dp)));
+        return (dm * dp <= T(0.0)) ? T(0.0) : copysignf(m, dm);
+    } else {
+        return minmod(T(0.5) * (dm + dp), minmod(T(2.0) * dm, T(2.0) * dp));
+    }
 }
 
 }  // namespace ccb
