@@ -305,8 +305,8 @@ __device__ __forceinline__ void m2_stage_tile(const M2Const<T>& c, const Fields<
             S.u = rec(s_u, 1); S.v = rec(s_v, 2); S.by = rec(s_by, 5); S.bx = ctr(s_bx);
         }
         const float fr = (float)c.floor_rho, fp = (float)c.floor_P;
-        S.r.x = vmax(S.r.x, fr); S.r.y = vmax(S.r.y, fr);
-        S.P.x = vmax(S.P.x, fp); S.P.y = vmax(S.P.y, fp);
+        S.r.x = fmaxf(S.r.x, fr); S.r.y = fmaxf(S.r.y, fr);
+        S.P.x = fmaxf(S.P.x, fp); S.P.y = fmaxf(S.P.y, fp);
         return S;
     };
 

@@ -320,7 +320,9 @@ __host__ __device__ __forceinline__ Flux<T> hlld_x_scalar(const Cst& c, Prim<T> 
 // issue slot where the scalar code spends two.  Each lane rounds like the
 // scalar FP32 code with its multiply-adds contracted (divisions, square roots
 // and comparisons stay scalar).  The region logic and the flux of the chosen
-// state follow hlld_x_scalar line for line.
+// state follow hlld_x_scalar line for line; its max / min are fmaxf / fminf
+// (one instruction where (a < b) ? b : a takes a compare and a select; the
+// same value for every operand that is not NaN).
 // ---------------------------------------------------------------------------
 struct Prim2 { float2 r, u, v, w, P, bx, by, bz; };   // .x left state, .y right state
 
@@ -345,18 +347,18 @@ __device__ __forceinline__ Flux<float> hlld_x2(const M2Const<float>& c, Prim2 S,
     // fast_speed of both states (M2:148-174)
     const float2 bn2p = pmul(bn, bn);
     const float2 b2 = pfma(S.bz, S.bz, pfma(S.by, S.by, bn2p));
-    const float2 ir = pk(1.0f / vmax(S.r.x, c.floor_rho), 1.0f / vmax(S.r.y, c.floor_rho));
+    const float2 ir = pk(1.0f / fmaxf(S.r.x, c.floor_rho), 1.0f / fmaxf(S.r.y, c.floor_rho));
     const float2 a2 = pmul(pmul(pbc(c.gamma), S.P), ir);
     const float2 vA2 = pmul(b2, ir);
     const float2 vn2 = pmul(bn2p, ir);
     const float2 sa = padd(a2, vA2);
     const float2 disc = pfma(sa, sa, pmul(pmul(pbc(-4.0f), a2), vn2));
-    const float2 sd = pk(sqrtf(vmax(0.0f, disc.x)), sqrtf(vmax(0.0f, disc.y)));
+    const float2 sd = pk(sqrtf(fmaxf(0.0f, disc.x)), sqrtf(fmaxf(0.0f, disc.y)));
     const float2 cf2 = pmul(pbc(0.5f), padd(sa, sd));
-    const float2 cf = pk(sqrtf(vmax(0.0f, cf2.x)), sqrtf(vmax(0.0f, cf2.y)));
+    const float2 cf = pk(sqrtf(fmaxf(0.0f, cf2.x)), sqrtf(fmaxf(0.0f, cf2.y)));
     const float2 um = psub(S.u, cf), up = padd(S.u, cf);
-    const float SL = vmin(um.x, um.y);
-    const float SR = vmax(up.x, up.y);
+    const float SL = fminf(um.x, um.y);
+    const float SR = fmaxf(up.x, up.y);
     if (0.0f <= SL) return ideal_flux(c, lane_x(S));
     if (0.0f >= SR) return ideal_flux(c, lane_y(S));
 
@@ -406,7 +408,7 @@ __device__ __forceinline__ Flux<float> hlld_x2(const M2Const<float>& c, Prim2 S,
     float2 ws2 = pfma(psub(S.bz, Bzs2), bq, S.w);
     if (!(fabsf(dLR.x) > 1e-14f)) { Bys2.x = S.by.x; Bzs2.x = S.bz.x; vs2.x = S.v.x; ws2.x = S.w.x; }
     if (!(fabsf(dLR.y) > 1e-14f)) { Bys2.y = S.by.y; Bzs2.y = S.bz.y; vs2.y = S.v.y; ws2.y = S.w.y; }
-    const float2 rl = pk(vmax(rst.x, 1e-30f), vmax(rst.y, 1e-30f));
+    const float2 rl = pk(fmaxf(rst.x, 1e-30f), fmaxf(rst.y, 1e-30f));
     const float2 iq = pk(rsqrtf(rl.x), rsqrtf(rl.y));
     const float2 sq = pmul(rl, iq);                                  // sqrt(rho*) of each side
     const float2 SAl = pfma(pk(-fabsf(Bn), fabsf(Bn)), iq, pbc(SM));  // SL*, SR*
